@@ -1,0 +1,234 @@
+/*
+ * mojoalign_b200.h - C ABI of the B200 linear bisulfite seed-and-extend path.
+ *
+ * This library replaces the FM engine of the mojo-align linear mapper
+ * (align.linear.mojo, the bwa-meth method class).  Every entry point below
+ * names the reference interface it stands in for.  Reference paths are
+ * relative to the mojo-align source tree.
+ *
+ * Conventions
+ *   - Every call returns MA_OK (0) or a negative MA_ERR_* code.  No C++
+ *     exception crosses this boundary.  ma_last_error() returns the message
+ *     of the last failing call made on a context (thread-local for calls
+ *     that take no context).
+ *   - One ma_ctx per host thread.  The caller owns every host buffer; the
+ *     library owns device buffers it allocates.
+ *   - Host pointers are plain pageable or pinned memory.  "_device" entry
+ *     points take device pointers and a cudaStream_t passed as void*.
+ *   - The CUDA kernels are the only compute path: with no usable sm_100
+ *     device every mapping call fails with MA_ERR_CUDA.
+ */
+#ifndef MOJOALIGN_B200_H
+#define MOJOALIGN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define MA_OK 0
+#define MA_ERR_ARG -1         /* invalid argument / size                    */
+#define MA_ERR_IO -2          /* file missing or unreadable                 */
+#define MA_ERR_FORMAT -3      /* malformed bwa index / FASTA / FASTQ        */
+#define MA_ERR_CUDA -4        /* CUDA runtime failure or no device          */
+#define MA_ERR_NOMEM -5       /* HBM admission budget exceeded / OOM        */
+#define MA_ERR_UNSUPPORTED -6 /* input outside what this build handles      */
+#define MA_ERR_TIMEOUT -7     /* a bounded device wait ran out              */
+#define MA_ERR_INTERNAL -8    /* device-side consistency check failed       */
+
+/* bisulfite conversion modes, fq2bam-meth/src/linear_fastq.mojo:29-34 */
+#define MA_BS_NONE 0
+#define MA_BS_C2T 1
+#define MA_BS_G2A 2
+
+typedef struct ma_ctx ma_ctx;
+typedef struct ma_index ma_index;
+
+/*
+ * Mapping parameters.  Field names and defaults follow the env knobs read at
+ * fq2bam-meth/src/linear_gpu_fm.mojo:2074-2082 (METHYLGRAPHER_FM_*).
+ */
+typedef struct ma_params {
+    int32_t seed_len;    /* METHYLGRAPHER_FM_SEED_LEN     default 18   */
+    int32_t seed_stride; /* METHYLGRAPHER_FM_SEED_STRIDE  default 2    */
+    int32_t max_occ;     /* METHYLGRAPHER_FM_MAX_OCC      default 4096 */
+    int32_t max_diff;    /* METHYLGRAPHER_FM_MAX_DIFF     default 12   */
+    int32_t max_soft;    /* METHYLGRAPHER_FM_MAX_SOFT     default 20   */
+    int32_t max_adj;     /* METHYLGRAPHER_FM_ADJ          default 8    */
+    int32_t rescue_win;  /* METHYLGRAPHER_FM_RESCUE_WIN   default 512  */
+} ma_params;
+
+/* Fills the reference defaults (linear_gpu_fm.mojo:2074-2082). */
+void ma_params_default(ma_params* p);
+
+/*
+ * Per-read outputs, structure of arrays, each [n_seq] (R1 rows then R2 rows).
+ * Same fields and meaning as the seven output buffers of
+ * fm_seed_extend_kernel (linear_gpu_fm.mojo:1183-1189): rid is the index of
+ * the f<name>/r<name> contig of the .ann (-1 unmapped), pos is 0-based and
+ * contig-local, flag is 4 (unmapped) or 16*is_rev, sl/sr soft clips.
+ */
+typedef struct ma_hits {
+    int32_t* rid;
+    uint32_t* pos;
+    uint32_t* mapq;
+    int32_t* flag;
+    uint32_t* sl;
+    uint32_t* sr;
+    uint32_t* nm;
+} ma_hits;
+
+/*
+ * Optional side outputs (not emitted by the reference kernel, which keeps
+ * them in locals at linear_gpu_fm.mojo:1238-1240,1369-1385).  For the
+ * candidate that won the best-hit selection: the SA interval [uk, ul], its
+ * left read offset us and its right endpoint e; us = e = -1 when the seed
+ * kernel chose no hit.  score = (qlen - sl - sr) - 5*nm for a mapped read
+ * (match +1 / mismatch -4 over the aligned part), 0 for an unmapped one.
+ * Any pointer may be NULL.
+ */
+typedef struct ma_debug {
+    uint64_t* uk;
+    uint64_t* ul;
+    int32_t* us;
+    int32_t* e;
+    int32_t* score;
+} ma_debug;
+
+typedef struct ma_index_info {
+    uint64_t seq_len;      /* BWT length 2*l_pac (linear_fm_index.mojo:126) */
+    uint64_t l_pac;        /* forward pac length (.ann line 1)               */
+    uint64_t primary;      /* BWT row of the whole text                      */
+    uint64_t L2[5];        /* cumulative symbol counts                       */
+    int64_t sa_intv;       /* SA sampling interval of the .sa file           */
+    int64_t n_sa;          /* (seq_len + sa_intv) / sa_intv                  */
+    int64_t n_contigs;     /* .ann records (f<name> and r<name>)             */
+    uint64_t sa_reject_below; /* smallest text position reachable by the
+                                 reference's sampled-SA walk (see DESIGN) */
+    int32_t kmer_k;        /* k of the resident k-mer interval table         */
+    uint64_t device_bytes; /* HBM held by this index                         */
+} ma_index_info;
+
+/* ---- context ------------------------------------------------------- */
+
+/* Opens a CUDA context on device `device_ordinal` (select_device,
+ * gpu-common/src/gpu_device.mojo:19-64; DeviceContext(api),
+ * linear_gpu_fm.mojo:2014).  Fails with MA_ERR_CUDA without an sm_100 GPU. */
+int ma_ctx_create(int device_ordinal, ma_ctx** out);
+void ma_ctx_destroy(ma_ctx* ctx);
+const char* ma_last_error(const ma_ctx* ctx);
+/* Free / total HBM of the context's device (replaces the nvidia-smi probe
+ * hbm_info, gpu-common/python/gpu_mem.py:28-57). */
+int ma_hbm_info(ma_ctx* ctx, uint64_t* free_bytes, uint64_t* total_bytes);
+
+/* ---- index --------------------------------------------------------- */
+
+/*
+ * Builds a bwa-0.7-format FM-index (.bwt/.sa/.pac/.ann/.amb) of `fasta`.
+ * bwameth_c2t != 0 first writes the bwa-meth dual-strand text (r<name> =
+ * G->A, f<name> = C->T) as `out_prefix` itself (fq2bam_meth.py:91-93) and
+ * indexes that, replacing `bwameth.py index` + `bwa index`
+ * (fq2bam-meth/scripts/ensure_bwameth_index.sh:23-50).  sa_intv is the SA
+ * sampling interval written to .sa (bwa default 32).  device_ordinal >= 0
+ * sorts suffixes on that GPU; -1 sorts on the host.
+ */
+int ma_index_build(const char* fasta, const char* out_prefix, int bwameth_c2t,
+                   int sa_intv, int device_ordinal);
+
+/*
+ * Loads prefix.{bwt,sa,pac,ann} with the header checks of
+ * FmIndex.load (fq2bam-meth/src/linear_fm_index.mojo:88-175) and makes the
+ * index resident in HBM (upload at linear_gpu_fm.mojo:2034-2069) in this
+ * library's own layout.  The HBM preflight (_require_hbm,
+ * linear_gpu_locate.mojo:211-214; gpu_mem.require_index_capacity) becomes a
+ * cudaMemGetInfo check against hbm_budget_bytes (0 = all free HBM).
+ * kmer_k selects the k-mer interval table (0 = none, 1..14; must not exceed
+ * the seed length used later).
+ */
+int ma_index_open(ma_ctx* ctx, const char* prefix, int kmer_k,
+                  uint64_t hbm_budget_bytes, ma_index** out);
+void ma_index_close(ma_index* idx);
+int ma_index_get_info(const ma_index* idx, ma_index_info* out);
+/* Contig record i of the .ann (FmIndex.contig_name/offset/length,
+ * linear_fm_index.mojo:337-347).  *name stays valid until ma_index_close. */
+int ma_index_contig(const ma_index* idx, int64_t i, const char** name,
+                    uint64_t* offset, uint64_t* length);
+
+/* ---- mapping ------------------------------------------------------- */
+
+/*
+ * One batch through the plain single-launch form, synchronous.  Replaces
+ * _fm_fire_batch (linear_gpu_fm.mojo:2279-2417): H2D of bases and lengths,
+ * then on-device conversion + 2-bit pack (pack_bases_kernel L1136-1154 and
+ * _cvt, linear_fastq.mojo:37-46), the seed/extend kernel
+ * (fm_seed_extend_kernel L1156-1837), the mate rescue kernel when paired
+ * (fm_mate_rescue_kernel L1839-2011), D2H of the outputs.
+ *
+ *   bases   ASCII, row-major [n_seq][max_len]; R1 rows 0..n1-1, then R2
+ *           rows n1..2*n1-1 when paired (fq_pack_bases layout,
+ *           linear_fastq.mojo:454-492).  Bytes past a read's length are
+ *           ignored.
+ *   lens    [n_seq] read lengths, each <= max_len <= 1024.
+ *   bs_r1 / bs_r2   MA_BS_* conversion applied on the device to R1 / R2.
+ *   out     host arrays [n_seq]; dbg may be NULL.
+ */
+int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases,
+                 const uint32_t* lens, uint32_t n1, int paired,
+                 uint32_t max_len, int bs_r1, int bs_r2, const ma_params* p,
+                 ma_hits* out, ma_debug* dbg);
+
+/*
+ * Same computation on device-resident buffers, asynchronous on `stream`
+ * (a cudaStream_t, NULL = the context's stream).  Scratch comes from the
+ * context's pool, sized on first use for (n_seq, max_len).
+ */
+int ma_map_batch_device(ma_ctx* ctx, const ma_index* idx,
+                        const uint8_t* d_bases, const uint32_t* d_lens,
+                        uint32_t n1, int paired, uint32_t max_len, int bs_r1,
+                        int bs_r2, const ma_params* p, ma_hits* d_out,
+                        ma_debug* d_dbg, void* stream);
+
+/* Number of kernel launches the last mapping call on ctx issued. */
+int ma_last_launch_count(const ma_ctx* ctx);
+
+/* ---- synthetic workloads (bench and tests; no reference counterpart) -- */
+
+/*
+ * Writes a FASTA of total_len bases split into n_contigs contigs, from a
+ * first-order base model with GC fraction gc and CpG frequency cpg.
+ */
+int ma_synth_reference(const char* fasta_out, uint64_t total_len,
+                       int n_contigs, double gc, double cpg, uint64_t seed);
+
+typedef struct ma_read_model {
+    uint32_t len_fixed;     /* >0: every read this long                       */
+    double len_lognorm_median; /* used when len_fixed == 0                    */
+    double len_lognorm_sigma;
+    uint32_t len_min, len_max;
+    double frag_mean, frag_sd; /* paired fragments                            */
+    double conv_non_cpg;    /* P(non-CpG C converted)                         */
+    double cpg_retain;      /* P(CpG C retained)                              */
+    double sub_rate;        /* uniform substitution error rate                */
+    double random_frac;     /* fraction of fully random reads                 */
+    double non_directional; /* fraction of CTOT/CTOB reads                    */
+} ma_read_model;
+
+/*
+ * Simulates bisulfite reads from `fasta` into padded row-major ASCII
+ * buffers (the ma_map_batch layout).  bases must hold n_seq*max_len bytes,
+ * lens n_seq entries, where n_seq = n1 * (paired ? 2 : 1).  truth_pos /
+ * truth_rev (optional, [n_seq]) receive the forward text coordinate and
+ * strand each read was drawn from (UINT64_MAX for random reads).
+ */
+int ma_synth_reads(const char* fasta, const ma_read_model* m, uint32_t n1,
+                   int paired, uint32_t max_len, uint64_t seed,
+                   uint8_t* bases, uint32_t* lens, uint64_t* truth_pos,
+                   uint8_t* truth_rev);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MOJOALIGN_B200_H */

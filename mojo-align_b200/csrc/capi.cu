@@ -1,0 +1,397 @@
+// capi.cu - the C ABI of libmojoalign_b200 (declared in
+// include/mojoalign_b200.h).  Every entry point catches ma::Error and
+// returns its code; the message is kept on the context (or thread-locally
+// for calls without one).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "ma_device.cuh"
+#include "ma_internal.h"
+
+namespace ma {
+int launch_pack(const uint8_t* d_bases, const uint32_t* d_lens, int64_t n_seq, int64_t n1, int max_len, int words,
+                int bs_r1, int bs_r2, uint64_t* d_packed, int* d_err, cudaStream_t st);
+int launch_seed_extend(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
+                       cudaStream_t st);
+int launch_rescue(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int64_t n_pairs,
+                  cudaStream_t st);
+}  // namespace ma
+
+extern "C" int ma_synth_reference_impl(const char*, uint64_t, int, double, double, uint64_t, char*, size_t);
+extern "C" int ma_synth_reads_impl(const char*, const ma_read_model*, uint32_t, int, uint32_t, uint64_t, uint8_t*,
+                                   uint32_t*, uint64_t*, uint8_t*, char*, size_t);
+
+using namespace ma;
+
+namespace {
+
+thread_local std::string t_err;
+
+void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) fail(MA_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// A grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    void ensure(size_t n) {
+        if (n <= cap) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        ck(cudaMalloc(&p, n ? n : 1), "cudaMalloc scratch");
+        cap = n;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <typename T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+}  // namespace
+
+struct ma_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int last_launches = 0;
+    DevBuf bases, lens, packed, err_flag;
+    DevBuf o_rid, o_pos, o_mapq, o_flag, o_sl, o_sr, o_nm;
+    DevBuf d_uk, d_ul, d_us, d_e, d_score;
+};
+
+struct ma_index {
+    ma_ctx* ctx = nullptr;
+    DevIndex dix{};
+    DeviceIndexBuffers bufs;
+    ma_index_info info{};
+    std::vector<Contig> contigs;
+};
+
+namespace {
+
+template <typename F>
+int guarded(ma_ctx* ctx, F&& f) {
+    try {
+        f();
+        if (ctx) ctx->err.clear();
+        return MA_OK;
+    } catch (const Error& e) {
+        if (ctx) ctx->err = e.what();
+        t_err = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        if (ctx) ctx->err = "host out of memory";
+        t_err = "host out of memory";
+        return MA_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        if (ctx) ctx->err = e.what();
+        t_err = e.what();
+        return MA_ERR_INTERNAL;
+    }
+}
+
+void use_device(ma_ctx* ctx) { ck(cudaSetDevice(ctx->device), "cudaSetDevice"); }
+
+void validate_params(const ma_params* p) {
+    if (!p) fail(MA_ERR_ARG, "params must not be NULL");
+    if (p->seed_len < 1 || p->seed_len > MAX_READ_LEN) fail(MA_ERR_ARG, "seed_len must be in 1..1024");
+    if (p->seed_stride < 1) fail(MA_ERR_ARG, "seed_stride must be >= 1");
+    if (p->max_occ < 1) fail(MA_ERR_ARG, "max_occ must be >= 1");
+}
+
+DevParams to_dev(const ma_params* p) {
+    DevParams d;
+    d.seed_len = p->seed_len;
+    d.seed_stride = p->seed_stride;
+    d.max_occ = p->max_occ;
+    d.max_diff = p->max_diff;
+    d.max_soft = p->max_soft;
+    d.max_adj = p->max_adj;
+    d.rescue_win = p->rescue_win;
+    return d;
+}
+
+// Enqueues pack -> seed/extend -> rescue for device-resident inputs.
+void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const uint32_t* d_lens, uint32_t n1,
+                 int paired, uint32_t max_len, int bs_r1, int bs_r2, const ma_params* p, const DevOut& out,
+                 cudaStream_t st) {
+    const int64_t n_seq = paired ? 2 * static_cast<int64_t>(n1) : n1;
+    const int words = static_cast<int>((max_len + 31) / 32);
+    ctx->packed.ensure(static_cast<size_t>(n_seq) * 4 * words * 8);
+    ctx->err_flag.ensure(sizeof(int));
+    ck(cudaMemsetAsync(ctx->err_flag.p, 0, sizeof(int), st), "memset");
+    int launches = 0;
+    launches += launch_pack(d_bases, d_lens, n_seq, n1, static_cast<int>(max_len), words, bs_r1, bs_r2,
+                            ctx->packed.as<uint64_t>(), ctx->err_flag.as<int>(), st);
+    DevReads R{ctx->packed.as<uint64_t>(), d_lens, words, n_seq};
+    DevParams P = to_dev(p);
+    launches += launch_seed_extend(idx->dix, R, P, out, st);
+    if (paired && p->rescue_win > 0) launches += launch_rescue(idx->dix, R, P, out, n1, st);
+    ck(cudaGetLastError(), "kernel launch");
+    ctx->last_launches = launches;
+}
+
+void check_err_flag(ma_ctx* ctx, cudaStream_t st) {
+    int h = 0;
+    ck(cudaMemcpyAsync(&h, ctx->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H err");
+    ck(cudaStreamSynchronize(st), "mapping kernels");
+    if (h == 1) fail(MA_ERR_ARG, "a read length exceeds max_len");
+    if (h) fail(MA_ERR_INTERNAL, "device error flag " + std::to_string(h));
+}
+
+}  // namespace
+
+extern "C" {
+
+void ma_params_default(ma_params* p) {
+    if (!p) return;
+    p->seed_len = 18;
+    p->seed_stride = 2;
+    p->max_occ = 4096;
+    p->max_diff = 12;
+    p->max_soft = 20;
+    p->max_adj = 8;
+    p->rescue_win = 512;
+}
+
+const char* ma_last_error(const ma_ctx* ctx) { return ctx ? ctx->err.c_str() : t_err.c_str(); }
+
+int ma_ctx_create(int device_ordinal, ma_ctx** out) {
+    if (!out) return MA_ERR_ARG;
+    *out = nullptr;
+    ma_ctx* ctx = new ma_ctx();
+    int rc = guarded(nullptr, [&] {
+        int n = 0;
+        cudaError_t e = cudaGetDeviceCount(&n);
+        if (e != cudaSuccess || n == 0) fail(MA_ERR_CUDA, "no CUDA device available");
+        if (device_ordinal < 0 || device_ordinal >= n) fail(MA_ERR_ARG, "device ordinal out of range");
+        cudaDeviceProp prop;
+        ck(cudaGetDeviceProperties(&prop, device_ordinal), "cudaGetDeviceProperties");
+        if (prop.major != 10)
+            fail(MA_ERR_CUDA, "this library is built for sm_100a (B200); device reports sm_" +
+                                  std::to_string(prop.major) + std::to_string(prop.minor));
+        ctx->device = device_ordinal;
+        ck(cudaSetDevice(device_ordinal), "cudaSetDevice");
+        ck(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    });
+    if (rc != MA_OK) {
+        delete ctx;
+        return rc;
+    }
+    *out = ctx;
+    return MA_OK;
+}
+
+void ma_ctx_destroy(ma_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    for (DevBuf* b : {&ctx->bases, &ctx->lens, &ctx->packed, &ctx->err_flag, &ctx->o_rid, &ctx->o_pos, &ctx->o_mapq,
+                      &ctx->o_flag, &ctx->o_sl, &ctx->o_sr, &ctx->o_nm, &ctx->d_uk, &ctx->d_ul, &ctx->d_us,
+                      &ctx->d_e, &ctx->d_score})
+        b->release();
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+int ma_hbm_info(ma_ctx* ctx, uint64_t* free_bytes, uint64_t* total_bytes) {
+    if (!ctx || !free_bytes || !total_bytes) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        use_device(ctx);
+        size_t f = 0, t = 0;
+        ck(cudaMemGetInfo(&f, &t), "cudaMemGetInfo");
+        *free_bytes = f;
+        *total_bytes = t;
+    });
+}
+
+int ma_index_build(const char* fasta, const char* out_prefix, int bwameth_c2t, int sa_intv, int device_ordinal) {
+    if (!fasta || !out_prefix) {
+        t_err = "null path";
+        return MA_ERR_ARG;
+    }
+    return guarded(nullptr, [&] { build_index(fasta, out_prefix, bwameth_c2t != 0, sa_intv, device_ordinal); });
+}
+
+int ma_index_open(ma_ctx* ctx, const char* prefix, int kmer_k, uint64_t hbm_budget_bytes, ma_index** out) {
+    if (!ctx || !prefix || !out) return MA_ERR_ARG;
+    *out = nullptr;
+    ma_index* idx = new ma_index();
+    int rc = guarded(ctx, [&] {
+        use_device(ctx);
+        BwaIndexHost h = load_bwa_index(prefix);
+        const uint64_t need = device_index_bytes(h, kmer_k);
+        size_t f = 0, t = 0;
+        ck(cudaMemGetInfo(&f, &t), "cudaMemGetInfo");
+        // fail-closed admission like gpu_mem.require_index_capacity: the
+        // resident index plus staging (bwt, pac, samples) must fit
+        const uint64_t staging = h.bwt.size() * 4 + h.pac.size() + h.sa.size() * 8;
+        const uint64_t budget = hbm_budget_bytes ? std::min<uint64_t>(hbm_budget_bytes, f) : f;
+        if (need + staging > budget)
+            fail(MA_ERR_NOMEM, "index needs " + std::to_string((need + staging) >> 20) + " MiB of HBM, budget " +
+                                   std::to_string(budget >> 20) + " MiB");
+        uint64_t p0 = 0;
+        idx->dix = build_device_index(h, kmer_k, ctx->stream, idx->bufs, &p0);
+        idx->ctx = ctx;
+        idx->contigs = h.contigs;
+        ma_index_info& I = idx->info;
+        I.seq_len = h.seq_len;
+        I.l_pac = h.l_pac;
+        I.primary = h.primary;
+        for (int c = 0; c < 5; ++c) I.L2[c] = h.L2[c];
+        I.sa_intv = h.sa_intv;
+        I.n_sa = h.n_sa;
+        I.n_contigs = static_cast<int64_t>(h.contigs.size());
+        I.sa_reject_below = p0;
+        I.kmer_k = kmer_k;
+        I.device_bytes = idx->bufs.bytes;
+    });
+    if (rc != MA_OK) {
+        free_device_index(idx->bufs);
+        delete idx;
+        return rc;
+    }
+    *out = idx;
+    return MA_OK;
+}
+
+void ma_index_close(ma_index* idx) {
+    if (!idx) return;
+    if (idx->ctx) cudaSetDevice(idx->ctx->device);
+    free_device_index(idx->bufs);
+    delete idx;
+}
+
+int ma_index_get_info(const ma_index* idx, ma_index_info* out) {
+    if (!idx || !out) return MA_ERR_ARG;
+    *out = idx->info;
+    return MA_OK;
+}
+
+int ma_index_contig(const ma_index* idx, int64_t i, const char** name, uint64_t* offset, uint64_t* length) {
+    if (!idx || i < 0 || i >= static_cast<int64_t>(idx->contigs.size())) return MA_ERR_ARG;
+    if (name) *name = idx->contigs[static_cast<size_t>(i)].name.c_str();
+    if (offset) *offset = idx->contigs[static_cast<size_t>(i)].offset;
+    if (length) *length = idx->contigs[static_cast<size_t>(i)].len;
+    return MA_OK;
+}
+
+int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const uint32_t* lens, uint32_t n1,
+                 int paired, uint32_t max_len, int bs_r1, int bs_r2, const ma_params* p, ma_hits* out,
+                 ma_debug* dbg) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (!idx || !out || (n1 && (!bases || !lens))) fail(MA_ERR_ARG, "null argument");
+        if (idx->ctx != ctx) fail(MA_ERR_ARG, "index belongs to another context");
+        validate_params(p);
+        if (max_len < 1 || max_len > MAX_READ_LEN) fail(MA_ERR_ARG, "max_len must be in 1..1024");
+        if (bs_r1 < 0 || bs_r1 > 2 || bs_r2 < 0 || bs_r2 > 2) fail(MA_ERR_ARG, "bad bisulfite mode");
+        ctx->last_launches = 0;
+        if (n1 == 0) return;
+        const int64_t n_seq = paired ? 2 * static_cast<int64_t>(n1) : n1;
+        for (int64_t i = 0; i < n_seq; ++i)
+            if (lens[i] > max_len) fail(MA_ERR_ARG, "read " + std::to_string(i) + " longer than max_len");
+        if (!out->rid || !out->pos || !out->mapq || !out->flag || !out->sl || !out->sr || !out->nm)
+            fail(MA_ERR_ARG, "null output array");
+        use_device(ctx);
+        cudaStream_t st = ctx->stream;
+        const size_t nb = static_cast<size_t>(n_seq) * max_len;
+        ctx->bases.ensure(nb);
+        ctx->lens.ensure(n_seq * 4);
+        for (DevBuf* b : {&ctx->o_rid, &ctx->o_pos, &ctx->o_mapq, &ctx->o_flag, &ctx->o_sl, &ctx->o_sr, &ctx->o_nm,
+                          &ctx->d_us, &ctx->d_e, &ctx->d_score})
+            b->ensure(n_seq * 4);
+        ctx->d_uk.ensure(n_seq * 8);
+        ctx->d_ul.ensure(n_seq * 8);
+        ck(cudaMemcpyAsync(ctx->bases.p, bases, nb, cudaMemcpyHostToDevice, st), "H2D bases");
+        ck(cudaMemcpyAsync(ctx->lens.p, lens, n_seq * 4, cudaMemcpyHostToDevice, st), "H2D lens");
+        DevOut o{ctx->o_rid.as<int32_t>(), ctx->o_pos.as<uint32_t>(), ctx->o_mapq.as<uint32_t>(),
+                 ctx->o_flag.as<int32_t>(), ctx->o_sl.as<uint32_t>(), ctx->o_sr.as<uint32_t>(),
+                 ctx->o_nm.as<uint32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr};
+        const bool want_dbg = dbg && (dbg->uk || dbg->ul || dbg->us || dbg->e || dbg->score);
+        if (want_dbg) {
+            o.uk = ctx->d_uk.as<uint64_t>();
+            o.ul = ctx->d_ul.as<uint64_t>();
+            o.us = ctx->d_us.as<int32_t>();
+            o.e = ctx->d_e.as<int32_t>();
+            o.score = ctx->d_score.as<int32_t>();
+        }
+        enqueue_map(ctx, idx, ctx->bases.as<uint8_t>(), ctx->lens.as<uint32_t>(), n1, paired, max_len, bs_r1, bs_r2,
+                    p, o, st);
+        const size_t n4 = n_seq * 4;
+        ck(cudaMemcpyAsync(out->rid, o.rid, n4, cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaMemcpyAsync(out->pos, o.pos, n4, cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaMemcpyAsync(out->mapq, o.mapq, n4, cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaMemcpyAsync(out->flag, o.flag, n4, cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaMemcpyAsync(out->sl, o.sl, n4, cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaMemcpyAsync(out->sr, o.sr, n4, cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaMemcpyAsync(out->nm, o.nm, n4, cudaMemcpyDeviceToHost, st), "D2H");
+        if (want_dbg) {
+            if (dbg->uk) ck(cudaMemcpyAsync(dbg->uk, o.uk, n_seq * 8, cudaMemcpyDeviceToHost, st), "D2H");
+            if (dbg->ul) ck(cudaMemcpyAsync(dbg->ul, o.ul, n_seq * 8, cudaMemcpyDeviceToHost, st), "D2H");
+            if (dbg->us) ck(cudaMemcpyAsync(dbg->us, o.us, n4, cudaMemcpyDeviceToHost, st), "D2H");
+            if (dbg->e) ck(cudaMemcpyAsync(dbg->e, o.e, n4, cudaMemcpyDeviceToHost, st), "D2H");
+            if (dbg->score) ck(cudaMemcpyAsync(dbg->score, o.score, n4, cudaMemcpyDeviceToHost, st), "D2H");
+        }
+        check_err_flag(ctx, st);
+    });
+}
+
+int ma_map_batch_device(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const uint32_t* d_lens,
+                        uint32_t n1, int paired, uint32_t max_len, int bs_r1, int bs_r2, const ma_params* p,
+                        ma_hits* d_out, ma_debug* d_dbg, void* stream) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (!idx || !d_out || (n1 && (!d_bases || !d_lens))) fail(MA_ERR_ARG, "null argument");
+        if (idx->ctx != ctx) fail(MA_ERR_ARG, "index belongs to another context");
+        validate_params(p);
+        if (max_len < 1 || max_len > MAX_READ_LEN) fail(MA_ERR_ARG, "max_len must be in 1..1024");
+        if (bs_r1 < 0 || bs_r1 > 2 || bs_r2 < 0 || bs_r2 > 2) fail(MA_ERR_ARG, "bad bisulfite mode");
+        ctx->last_launches = 0;
+        if (n1 == 0) return;
+        use_device(ctx);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+        DevOut o{d_out->rid, d_out->pos, d_out->mapq, d_out->flag, d_out->sl, d_out->sr, d_out->nm,
+                 nullptr, nullptr, nullptr, nullptr, nullptr};
+        if (d_dbg) {
+            if (!d_dbg->uk || !d_dbg->ul || !d_dbg->us || !d_dbg->e || !d_dbg->score)
+                fail(MA_ERR_ARG, "device debug outputs must be all set or NULL");
+            o.uk = d_dbg->uk;
+            o.ul = d_dbg->ul;
+            o.us = d_dbg->us;
+            o.e = d_dbg->e;
+            o.score = d_dbg->score;
+        }
+        enqueue_map(ctx, idx, d_bases, d_lens, n1, paired, max_len, bs_r1, bs_r2, p, o, st);
+        check_err_flag(ctx, st);
+    });
+}
+
+int ma_last_launch_count(const ma_ctx* ctx) { return ctx ? ctx->last_launches : 0; }
+
+int ma_synth_reference(const char* fasta_out, uint64_t total_len, int n_contigs, double gc, double cpg,
+                       uint64_t seed) {
+    char err[512] = {0};
+    int rc = ma_synth_reference_impl(fasta_out, total_len, n_contigs, gc, cpg, seed, err, sizeof err);
+    if (rc != MA_OK) t_err = err;
+    return rc;
+}
+
+int ma_synth_reads(const char* fasta, const ma_read_model* m, uint32_t n1, int paired, uint32_t max_len,
+                   uint64_t seed, uint8_t* bases, uint32_t* lens, uint64_t* truth_pos, uint8_t* truth_rev) {
+    char err[512] = {0};
+    int rc = ma_synth_reads_impl(fasta, m, n1, paired, max_len, seed, bases, lens, truth_pos, truth_rev, err,
+                                 sizeof err);
+    if (rc != MA_OK) t_err = err;
+    return rc;
+}
+
+}  // extern "C"

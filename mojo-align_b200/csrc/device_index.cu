@@ -1,0 +1,285 @@
+// device_index.cu - builds the HBM-resident index from bwa 0.7 files.
+//
+// The reference uploads the bwa words as they are and walks the sampled SA
+// on every lookup (linear_gpu_fm.mojo:2034-2069, 1390-1508).  Here the
+// upload is followed by one-time device passes that re-lay the index for
+// random 32-byte gathers:
+//   relayout_occ      bwa 64-B blocks of 128 positions -> 32-B lines of 64
+//   relayout_pac      MSB-first pac bytes -> LSB-first u64 words, padded
+//   reconstruct_sa    sampled SA -> full SA, one LF chain per sampled row
+//   build_kmer        k-mer -> backward-search interval table
+// Every kernel's loops are bounded; a chain that runs past its bound (only
+// possible on an inconsistent index) raises a device error flag instead of
+// spinning.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+
+#include "ma_device.cuh"
+#include "ma_internal.h"
+
+namespace ma {
+
+namespace {
+
+__device__ __forceinline__ uint32_t rev2(uint32_t v) {
+    // reverse the order of the 16 2-bit symbols of a word
+    v = __brev(v);
+    return ((v >> 1) & 0x55555555u) | ((v & 0x55555555u) << 1);
+}
+
+__device__ __forceinline__ uint32_t count_sym32(uint32_t w_lsb, int c, int nbases) {
+    // occurrences of c among the first nbases symbols (LSB first) of w
+    uint32_t pat = static_cast<uint32_t>(c) * 0x55555555u;
+    uint32_t t = w_lsb ^ pat;
+    uint32_t m = ~(t | (t >> 1)) & 0x55555555u;
+    if (nbases < 16) m &= (1u << (2 * nbases)) - 1;
+    return __popc(m);
+}
+
+__global__ void relayout_occ_kernel(const uint32_t* __restrict__ bwa, uint64_t seq_len, uint64_t n_lines,
+                                    OccLine* __restrict__ out) {
+    uint64_t L = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (L >= n_lines) return;
+    uint64_t blk = L >> 1;
+    int half = static_cast<int>(L & 1);
+    const uint32_t* b = bwa + blk * 16;
+    uint64_t cnt[4];
+    for (int c = 0; c < 4; ++c) cnt[c] = static_cast<uint64_t>(b[2 * c]) | (static_cast<uint64_t>(b[2 * c + 1]) << 32);
+    if (half) {
+        for (int i = 0; i < 4; ++i) {
+            uint32_t w = rev2(b[8 + i]);
+            for (int c = 0; c < 4; ++c) cnt[c] += count_sym32(w, c, 16);
+        }
+    }
+    OccLine o;
+    for (int c = 0; c < 4; ++c) o.cnt[c] = static_cast<uint32_t>(cnt[c]);
+    for (int i = 0; i < 4; ++i) {
+        uint64_t p0 = L * 64 + 16 * i;  // first position held by word i
+        uint32_t w = 0;
+        if (p0 < seq_len) {
+            w = rev2(b[8 + 4 * half + i]);
+            uint64_t valid = seq_len - p0;
+            if (valid < 16) w &= (1u << (2 * valid)) - 1;
+        }
+        o.w[i] = w;
+    }
+    out[L] = o;
+}
+
+__global__ void relayout_pac_kernel(const uint8_t* __restrict__ pac, uint64_t l_pac, uint64_t n_words,
+                                    uint64_t* __restrict__ out) {
+    uint64_t w = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (w >= n_words) return;  // n_words covers the text plus padding on both sides
+    int64_t tw = static_cast<int64_t>(w) - PAC_PAD;  // text word index
+    uint64_t v = 0;
+    if (tw >= 0) {
+        for (int i = 0; i < 32; ++i) {
+            uint64_t p = static_cast<uint64_t>(tw) * 32 + i;
+            if (p >= l_pac) break;
+            uint64_t sym = (pac[p >> 2] >> ((~p & 3) << 1)) & 3;
+            v |= sym << (2 * i);
+        }
+    }
+    out[w] = v;
+}
+
+// One chain per sampled row i (i % intv == 0, i <= seq_len): SA[i] is known
+// (row 0 is the sentinel suffix, SA[0] = seq_len).  LF steps from i visit
+// the rows of text positions SA[i]-1, SA[i]-2, ... until a sampled row or
+// text position 0; every row visited gets its SA value.
+__global__ void reconstruct_sa_kernel(DevIndex ix, const uint64_t* __restrict__ samples, uint64_t n_chains,
+                                      uint64_t intv, uint32_t* __restrict__ sa, uint64_t max_steps,
+                                      int* __restrict__ err) {
+    uint64_t ci = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (ci >= n_chains) return;
+    uint64_t r = ci * intv;
+    uint64_t s = ci == 0 ? ix.seq_len : samples[ci - 1];
+    if (s > ix.seq_len) {
+        atomicExch(err, 1);
+        return;
+    }
+    sa[r] = static_cast<uint32_t>(s);
+    for (uint64_t step = 0; step < max_steps; ++step) {
+        if (s == 0) return;
+        if (r == ix.primary) {  // position 0 reached through a bad sample
+            atomicExch(err, 2);
+            return;
+        }
+        uint64_t x = r - (r > ix.primary ? 1 : 0);
+        int c = bwt_sym(ix.occ, x);
+        r = ix.L2[c] + occ_row(ix, r, c);
+        s -= 1;
+        if (r > ix.seq_len) {
+            atomicExch(err, 3);
+            return;
+        }
+        if (r % intv == 0) return;
+        sa[r] = static_cast<uint32_t>(s);
+    }
+    atomicExch(err, 4);  // chain longer than any consistent index allows
+}
+
+__global__ void count_unset_kernel(const uint32_t* __restrict__ sa, uint64_t n, unsigned long long* cnt) {
+    uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    unsigned long long local = 0;
+    for (; i < n; i += stride) local += sa[i] == 0xFFFFFFFFu;
+    if (local) atomicAdd(cnt, local);
+}
+
+__global__ void build_kmer_kernel(DevIndex ix, int K, uint64_t n_kmers, uint2* __restrict__ out) {
+    uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (idx >= n_kmers) return;
+    uint64_t k = 0, l = ix.seq_len;
+    for (int t = 0; t < K; ++t) {
+        int c = static_cast<int>((idx >> (2 * t)) & 3);  // last base of W first
+        uint64_t ok = k != 0 ? occ_row(ix, k - 1, c) : 0;
+        uint64_t ol = occ_row(ix, l, c);
+        k = ix.L2[c] + ok + 1;
+        l = ix.L2[c] + ol;
+        if (k > l) {
+            out[idx] = make_uint2(1u, 0u);
+            return;
+        }
+    }
+    out[idx] = make_uint2(static_cast<uint32_t>(k), static_cast<uint32_t>(l));
+}
+
+void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) fail(MA_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+unsigned grid_for(uint64_t n, unsigned block) {
+    uint64_t g = (n + block - 1) / block;
+    return static_cast<unsigned>(g ? g : 1);
+}
+
+}  // namespace
+
+uint64_t device_index_bytes(const BwaIndexHost& h, int kmer_k) {
+    uint64_t n_lines = (h.seq_len + 63) / 64;
+    uint64_t b = n_lines * sizeof(OccLine);
+    b += (h.seq_len + 1) * 4;
+    b += ((h.l_pac + 31) / 32 + 2 * PAC_PAD) * 8;
+    if (kmer_k > 0) b += (1ull << (2 * kmer_k)) * 8;
+    b += h.contigs.size() * 12;
+    return b;
+}
+
+// Builds the resident index on the current device; returns its DevIndex and
+// fills `bufs`.  Temporary upload buffers are freed before returning.
+DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, cudaStream_t st, DeviceIndexBuffers& bufs,
+                            uint64_t* reject_below) {
+    if (h.seq_len + 1 >= 0xFFFFFFFFull)
+        fail(MA_ERR_UNSUPPORTED, "resident layout stores SA rows as u32; texts of 2^32 symbols or more are not supported yet");
+    if (kmer_k < 0 || kmer_k > 14) fail(MA_ERR_ARG, "kmer_k must be in 0..14");
+    const uint64_t n_lines = (h.seq_len + 63) / 64;
+    const uint64_t n_pacw = (h.l_pac + 31) / 32 + 2 * PAC_PAD;
+    DevIndex ix{};
+    ix.seq_len = h.seq_len;
+    ix.l_pac = h.l_pac;
+    ix.primary = h.primary;
+    for (int c = 0; c < 5; ++c) ix.L2[c] = h.L2[c];
+    ix.n_contigs = static_cast<int64_t>(h.contigs.size());
+    ix.kmer_k = kmer_k;
+
+    uint32_t* d_bwa = nullptr;
+    uint8_t* d_pac = nullptr;
+    uint64_t* d_samples = nullptr;
+    int* d_err = nullptr;
+    unsigned long long* d_cnt = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(d_bwa);
+        cudaFree(d_pac);
+        cudaFree(d_samples);
+        cudaFree(d_err);
+        cudaFree(d_cnt);
+    };
+    try {
+        check(cudaMalloc(&bufs.occ, n_lines * sizeof(OccLine)), "cudaMalloc occ");
+        check(cudaMalloc(&bufs.sa, (h.seq_len + 1) * 4), "cudaMalloc sa");
+        check(cudaMalloc(&bufs.pacw, n_pacw * 8), "cudaMalloc pac");
+        check(cudaMalloc(&bufs.coff, (h.contigs.size() + 1) * 8), "cudaMalloc contig_off");
+        check(cudaMalloc(&bufs.clen, (h.contigs.size() + 1) * 4), "cudaMalloc contig_len");
+        if (kmer_k > 0) check(cudaMalloc(&bufs.kmer, (1ull << (2 * kmer_k)) * 8), "cudaMalloc kmer");
+        check(cudaMalloc(&d_bwa, h.bwt.size() * 4), "cudaMalloc bwt staging");
+        check(cudaMalloc(&d_pac, h.pac.size() + 8), "cudaMalloc pac staging");
+        check(cudaMalloc(&d_samples, (h.sa.size() + 1) * 8), "cudaMalloc sa staging");
+        check(cudaMalloc(&d_err, sizeof(int)), "cudaMalloc err");
+        check(cudaMalloc(&d_cnt, sizeof(unsigned long long)), "cudaMalloc cnt");
+        check(cudaMemsetAsync(d_err, 0, sizeof(int), st), "memset");
+        check(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st), "memset");
+        check(cudaMemcpyAsync(d_bwa, h.bwt.data(), h.bwt.size() * 4, cudaMemcpyHostToDevice, st), "H2D bwt");
+        check(cudaMemsetAsync(d_pac, 0, h.pac.size() + 8, st), "memset");
+        check(cudaMemcpyAsync(d_pac, h.pac.data(), h.pac.size(), cudaMemcpyHostToDevice, st), "H2D pac");
+        if (!h.sa.empty())
+            check(cudaMemcpyAsync(d_samples, h.sa.data(), h.sa.size() * 8, cudaMemcpyHostToDevice, st), "H2D sa");
+        std::vector<uint64_t> coff(h.contigs.size());
+        std::vector<uint32_t> clen(h.contigs.size());
+        for (size_t i = 0; i < h.contigs.size(); ++i) {
+            coff[i] = h.contigs[i].offset;
+            clen[i] = h.contigs[i].len;
+        }
+        if (!coff.empty()) {
+            check(cudaMemcpyAsync(bufs.coff, coff.data(), coff.size() * 8, cudaMemcpyHostToDevice, st), "H2D coff");
+            check(cudaMemcpyAsync(bufs.clen, clen.data(), clen.size() * 4, cudaMemcpyHostToDevice, st), "H2D clen");
+        }
+        relayout_occ_kernel<<<grid_for(n_lines, 256), 256, 0, st>>>(d_bwa, h.seq_len, n_lines, bufs.occ);
+        relayout_pac_kernel<<<grid_for(n_pacw, 256), 256, 0, st>>>(d_pac, h.l_pac, n_pacw, bufs.pacw);
+        check(cudaGetLastError(), "relayout launch");
+        ix.occ = bufs.occ;
+        ix.pacw = bufs.pacw;
+        ix.coff = bufs.coff;
+        ix.clen = bufs.clen;
+        // full SA from the samples
+        check(cudaMemsetAsync(bufs.sa, 0xFF, (h.seq_len + 1) * 4, st), "memset sa");
+        const uint64_t intv = static_cast<uint64_t>(h.sa_intv);
+        const uint64_t n_chains = h.seq_len / intv + 1;  // rows 0, intv, ..., <= seq_len
+        if (h.sa.size() + 1 < n_chains) fail(MA_ERR_FORMAT, "FmIndex .sa holds fewer samples than seq_len implies");
+        reconstruct_sa_kernel<<<grid_for(n_chains, 128), 128, 0, st>>>(ix, d_samples, n_chains, intv, bufs.sa,
+                                                                       1ull << 20, d_err);
+        check(cudaGetLastError(), "reconstruct_sa launch");
+        count_unset_kernel<<<1184, 256, 0, st>>>(bufs.sa, h.seq_len + 1, d_cnt);
+        int herr = 0;
+        unsigned long long hcnt = 0;
+        check(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H err");
+        check(cudaMemcpyAsync(&hcnt, d_cnt, sizeof(hcnt), cudaMemcpyDeviceToHost, st), "D2H cnt");
+        check(cudaStreamSynchronize(st), "index preparation");
+        if (herr) fail(MA_ERR_FORMAT, "FmIndex BWT and SA samples are inconsistent (code " + std::to_string(herr) + ")");
+        if (hcnt) fail(MA_ERR_FORMAT, "FmIndex SA reconstruction left " + std::to_string(hcnt) + " rows unset");
+        ix.sa = bufs.sa;
+        // rejection bound of the reference's sampled walk: the smallest text
+        // position whose BWT row is sampled (rows >= intv; row 0 is the
+        // sentinel suffix and is never reached by a walk)
+        uint64_t p0 = h.seq_len;
+        for (uint64_t v : h.sa) p0 = v < p0 ? v : p0;
+        ix.sa_reject_below = p0;
+        *reject_below = p0;
+        if (kmer_k > 0) {
+            const uint64_t nk = 1ull << (2 * kmer_k);
+            build_kmer_kernel<<<grid_for(nk, 256), 256, 0, st>>>(ix, kmer_k, nk, bufs.kmer);
+            check(cudaGetLastError(), "build_kmer launch");
+            ix.kmer = bufs.kmer;
+        }
+        check(cudaStreamSynchronize(st), "index preparation");
+    } catch (...) {
+        cleanup();
+        throw;
+    }
+    cleanup();
+    bufs.bytes = device_index_bytes(h, kmer_k);
+    return ix;
+}
+
+void free_device_index(DeviceIndexBuffers& b) {
+    cudaFree(b.occ);
+    cudaFree(b.sa);
+    cudaFree(b.pacw);
+    cudaFree(b.kmer);
+    cudaFree(b.coff);
+    cudaFree(b.clen);
+    b = DeviceIndexBuffers{};
+}
+
+}  // namespace ma

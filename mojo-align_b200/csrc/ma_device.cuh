@@ -1,0 +1,156 @@
+// ma_device.cuh - HBM layout of the resident index and the device helpers
+// shared by the index-preparation and mapping kernels (sm_100a).
+//
+// Layout (all resident in HBM, built once per index by device_index.cu):
+//   occ   one 32-byte line per 64 BWT positions of the stored BWT string
+//         (the sentinel removed, as in bwa): u32 cnt[4] = symbols c in
+//         positions [0, 64*line), then 4 u32 words of 2-bit symbols, 16 per
+//         word, least significant first.  An Occ query is one 32-B sector.
+//   sa    the full suffix array, u32 per row, rows 0..seq_len.
+//   pacw  the forward text, 32 bases per u64 word, least significant first,
+//         with PAC_PAD zero words before text position 0 and after the end,
+//         so that a 32-base window starting anywhere in [-512, l_pac + 480)
+//         is two aligned loads and a funnel shift.
+//   kmer  for every k-mer W (first base most significant, 2 bits per base)
+//         the backward-search interval (k, l) after the k steps that consume
+//         W; k > l when W does not occur.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/mojoalign_b200.h"
+
+namespace ma {
+
+constexpr int PAC_PAD = 16;           // u64 words of zero padding each side
+constexpr int MAX_READ_LEN = 1024;    // linear_gpu_fm.mojo:2192,2447
+constexpr int MAX_WORDS = MAX_READ_LEN / 32;
+
+struct __align__(32) OccLine {
+    uint32_t cnt[4];
+    uint32_t w[4];
+};
+
+struct DevIndex {
+    const OccLine* occ;
+    const uint32_t* sa;
+    const uint64_t* pacw;
+    const uint2* kmer;
+    const uint64_t* coff;
+    const uint32_t* clen;
+    int64_t n_contigs;
+    uint64_t seq_len, l_pac, primary;
+    uint64_t L2[5];
+    uint64_t sa_reject_below;  // sa_pos below this is rejected (see seed kernel)
+    int32_t kmer_k;
+};
+
+// Mapping parameters after the reference's clamps are applied per read.
+struct DevParams {
+    int32_t seed_len, seed_stride, max_occ, max_diff, max_soft, max_adj, rescue_win;
+};
+
+// Packed read batch: per read r, 4 arrays of `words` u64 at
+// base + r * 4 * words: forward codes, reverse-complement codes, N mask of
+// the forward codes, N mask of the reverse complement.  Codes are 2 bits
+// per base, base j of a word at bits 2*(j%32); an N mask has bit 2*(j%32)
+// set where base j is not A/C/G/T.
+struct DevReads {
+    const uint64_t* packed;
+    const uint32_t* lens;
+    int32_t words;
+    int64_t n_seq;
+};
+
+struct DevOut {
+    int32_t* rid;
+    uint32_t* pos;
+    uint32_t* mapq;
+    int32_t* flag;
+    uint32_t* sl;
+    uint32_t* sr;
+    uint32_t* nm;
+    uint64_t* uk;  // debug outputs, may be null
+    uint64_t* ul;
+    int32_t* us;
+    int32_t* e;
+    int32_t* score;
+};
+
+constexpr uint64_t kEven = 0x5555555555555555ull;
+
+__device__ __forceinline__ uint64_t ldg64(const uint64_t* p) { return __ldg(p); }
+
+// Count of symbol c in stored-BWT positions [0 .. x] (x < seq_len).
+__device__ __forceinline__ uint64_t occ_at(const OccLine* __restrict__ occ, uint64_t x, int c) {
+    const uint4* p = reinterpret_cast<const uint4*>(occ + (x >> 6));
+    uint4 cnt = __ldg(p);
+    uint4 bw = __ldg(p + 1);
+    uint32_t base = c == 0 ? cnt.x : c == 1 ? cnt.y : c == 2 ? cnt.z : cnt.w;
+    uint64_t lo = static_cast<uint64_t>(bw.x) | (static_cast<uint64_t>(bw.y) << 32);
+    uint64_t hi = static_cast<uint64_t>(bw.z) | (static_cast<uint64_t>(bw.w) << 32);
+    uint64_t pat = static_cast<uint64_t>(c) * kEven;
+    uint64_t tl = lo ^ pat, th = hi ^ pat;
+    uint64_t ml = ~(tl | (tl >> 1)) & kEven;
+    uint64_t mh = ~(th | (th >> 1)) & kEven;
+    uint32_t w = static_cast<uint32_t>(x & 63);
+    uint64_t keep_lo = w >= 31 ? ~0ull : ((1ull << (2 * w + 2)) - 1);
+    uint64_t keep_hi = w < 32 ? 0ull : (w >= 63 ? ~0ull : ((1ull << (2 * (w - 32) + 2)) - 1));
+    return static_cast<uint64_t>(base) + __popcll(ml & keep_lo) + __popcll(mh & keep_hi);
+}
+
+// Occ(k, c) of the reference: count of c in BWT rows [0..k] (k a row index
+// in [0, seq_len]), with the sentinel row `primary` removed
+// (linear_gpu_fm.mojo:1261-1345).
+__device__ __forceinline__ uint64_t occ_row(const DevIndex& ix, uint64_t k, int c) {
+    if (k == ix.seq_len) return ix.L2[c + 1] - ix.L2[c];
+    uint64_t x = k - (k >= ix.primary ? 1 : 0);
+    return occ_at(ix.occ, x, c);
+}
+
+// Symbol of the stored BWT at position x.
+__device__ __forceinline__ int bwt_sym(const OccLine* __restrict__ occ, uint64_t x) {
+    uint32_t w = __ldg(&occ[x >> 6].w[(x >> 4) & 3]);
+    return static_cast<int>((w >> (2 * (x & 15))) & 3);
+}
+
+// 32 text bases starting at forward text position p, p in [-512, l_pac+480).
+__device__ __forceinline__ uint64_t ref_window(const uint64_t* __restrict__ pacw, int64_t p) {
+    int64_t q = p + 32 * PAC_PAD;
+    uint64_t wi = static_cast<uint64_t>(q) >> 5;
+    int sh = static_cast<int>(q & 31) * 2;
+    uint64_t lo = ldg64(pacw + wi), hi = ldg64(pacw + wi + 1);
+    return sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
+}
+
+// Even-bit mask for read positions [a, b) inside the word starting at 32*w.
+__device__ __forceinline__ uint64_t range_mask(int w, int a, int b) {
+    int lo = a - 32 * w, hi = b - 32 * w;
+    if (lo < 0) lo = 0;
+    if (hi > 32) hi = 32;
+    if (hi <= lo) return 0;
+    uint64_t m_hi = hi >= 32 ? ~0ull : ((1ull << (2 * hi)) - 1);
+    uint64_t m_lo = (1ull << (2 * lo)) - 1;
+    return m_hi & ~m_lo & kEven;
+}
+
+// Device buffers of one resident index (owned by an ma_index).
+struct DeviceIndexBuffers {
+    OccLine* occ = nullptr;
+    uint32_t* sa = nullptr;
+    uint64_t* pacw = nullptr;
+    uint2* kmer = nullptr;
+    uint64_t* coff = nullptr;
+    uint32_t* clen = nullptr;
+    uint64_t bytes = 0;
+};
+
+struct BwaIndexHost;
+uint64_t device_index_bytes(const BwaIndexHost& h, int kmer_k);
+DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, cudaStream_t st, DeviceIndexBuffers& bufs,
+                            uint64_t* reject_below);
+void free_device_index(DeviceIndexBuffers& b);
+
+}  // namespace ma

@@ -1,0 +1,69 @@
+// ma_internal.h - host-side types shared by the C++ and CUDA sources of
+// libmojoalign_b200.  Nothing here crosses the C ABI.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/mojoalign_b200.h"
+
+namespace ma {
+
+// Error carrying an MA_ERR_* code; converted to a status at the C ABI.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+[[noreturn]] inline void fail(int code, const std::string& msg) { throw Error(code, msg); }
+
+// One .ann record (bwa bntann1_t): name, annotation, offset and length.
+struct Contig {
+    std::string name;
+    std::string anno;
+    uint64_t offset = 0;
+    uint32_t len = 0;
+    int32_t n_ambs = 0;
+};
+
+// A run of ambiguous bases replaced in the pac (bwa bntamb1_t).
+struct Hole {
+    uint64_t offset = 0;
+    uint32_t len = 0;
+    char amb = 'N';
+};
+
+// A bwa 0.7 FM-index as the reference reads it
+// (fq2bam-meth/src/linear_fm_index.mojo:88-175).
+struct BwaIndexHost {
+    uint64_t primary = 0, seq_len = 0, l_pac = 0;
+    uint64_t L2[5] = {0, 0, 0, 0, 0};
+    int64_t sa_intv = 32, n_sa = 0;
+    std::vector<uint32_t> bwt;  // interleaved words after the 40-byte header
+    std::vector<uint64_t> sa;   // sa[1..n_sa-1]: element i = SA[(i+1)*sa_intv]
+    std::vector<uint8_t> pac;   // forward text, 4 bases per byte, MSB first
+    std::vector<Contig> contigs;
+};
+
+// Reads prefix.{bwt,sa,pac,ann} with FmIndex.load's checks.
+BwaIndexHost load_bwa_index(const std::string& prefix);
+
+// FASTA records (name = first word of the header, anno = the rest).
+struct FastaRecord {
+    std::string name;
+    std::string anno;
+    std::string seq;
+};
+std::vector<FastaRecord> read_fasta(const std::string& path);
+
+// Suffix array of text[0..n) over {0,1,2,3} with a virtual smallest
+// sentinel at n: returns SA[0..n] (SA[0] == n).  n must be < 2^32 - 1.
+std::vector<uint32_t> suffix_array_cpu(const uint8_t* text, uint64_t n);
+// Same, sorted on GPU `device` (prefix doubling over CUB radix sorts).
+std::vector<uint32_t> suffix_array_gpu(const uint8_t* text, uint64_t n, int device);
+
+void build_index(const std::string& fasta, const std::string& out_prefix, bool bwameth_c2t,
+                 int sa_intv, int device);
+
+}  // namespace ma

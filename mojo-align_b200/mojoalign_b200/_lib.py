@@ -1,0 +1,175 @@
+"""ctypes binding of libmojoalign_b200.so (the C ABI in include/mojoalign_b200.h).
+
+The shared library is the only compute path: importing this module fails
+loudly when it is missing, and every mapping call fails when no sm_100 GPU
+is present.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libmojoalign_b200.so"
+
+MA_OK = 0
+MA_ERR_ARG = -1
+MA_ERR_IO = -2
+MA_ERR_FORMAT = -3
+MA_ERR_CUDA = -4
+MA_ERR_NOMEM = -5
+MA_ERR_UNSUPPORTED = -6
+MA_ERR_TIMEOUT = -7
+MA_ERR_INTERNAL = -8
+
+MA_BS_NONE, MA_BS_C2T, MA_BS_G2A = 0, 1, 2
+
+ERR_NAMES = {
+    MA_ERR_ARG: "MA_ERR_ARG",
+    MA_ERR_IO: "MA_ERR_IO",
+    MA_ERR_FORMAT: "MA_ERR_FORMAT",
+    MA_ERR_CUDA: "MA_ERR_CUDA",
+    MA_ERR_NOMEM: "MA_ERR_NOMEM",
+    MA_ERR_UNSUPPORTED: "MA_ERR_UNSUPPORTED",
+    MA_ERR_TIMEOUT: "MA_ERR_TIMEOUT",
+    MA_ERR_INTERNAL: "MA_ERR_INTERNAL",
+}
+
+
+class MojoAlignError(RuntimeError):
+    """A failed C ABI call; `code` is the MA_ERR_* status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERR_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+class ma_params(C.Structure):
+    _fields_ = [
+        ("seed_len", C.c_int32),
+        ("seed_stride", C.c_int32),
+        ("max_occ", C.c_int32),
+        ("max_diff", C.c_int32),
+        ("max_soft", C.c_int32),
+        ("max_adj", C.c_int32),
+        ("rescue_win", C.c_int32),
+    ]
+
+
+class ma_hits(C.Structure):
+    _fields_ = [
+        ("rid", C.c_void_p),
+        ("pos", C.c_void_p),
+        ("mapq", C.c_void_p),
+        ("flag", C.c_void_p),
+        ("sl", C.c_void_p),
+        ("sr", C.c_void_p),
+        ("nm", C.c_void_p),
+    ]
+
+
+class ma_debug(C.Structure):
+    _fields_ = [
+        ("uk", C.c_void_p),
+        ("ul", C.c_void_p),
+        ("us", C.c_void_p),
+        ("e", C.c_void_p),
+        ("score", C.c_void_p),
+    ]
+
+
+class ma_index_info(C.Structure):
+    _fields_ = [
+        ("seq_len", C.c_uint64),
+        ("l_pac", C.c_uint64),
+        ("primary", C.c_uint64),
+        ("L2", C.c_uint64 * 5),
+        ("sa_intv", C.c_int64),
+        ("n_sa", C.c_int64),
+        ("n_contigs", C.c_int64),
+        ("sa_reject_below", C.c_uint64),
+        ("kmer_k", C.c_int32),
+        ("device_bytes", C.c_uint64),
+    ]
+
+
+class ma_read_model(C.Structure):
+    _fields_ = [
+        ("len_fixed", C.c_uint32),
+        ("len_lognorm_median", C.c_double),
+        ("len_lognorm_sigma", C.c_double),
+        ("len_min", C.c_uint32),
+        ("len_max", C.c_uint32),
+        ("frag_mean", C.c_double),
+        ("frag_sd", C.c_double),
+        ("conv_non_cpg", C.c_double),
+        ("cpg_retain", C.c_double),
+        ("sub_rate", C.c_double),
+        ("random_frac", C.c_double),
+        ("non_directional", C.c_double),
+    ]
+
+
+# (name, restype, argtypes) of every exported entry point of the header.
+SIGNATURES = [
+    ("ma_params_default", None, [C.POINTER(ma_params)]),
+    ("ma_ctx_create", C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    ("ma_ctx_destroy", None, [C.c_void_p]),
+    ("ma_last_error", C.c_char_p, [C.c_void_p]),
+    ("ma_hbm_info", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("ma_index_build", C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_int]),
+    ("ma_index_open", C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
+    ("ma_index_close", None, [C.c_void_p]),
+    ("ma_index_get_info", C.c_int, [C.c_void_p, C.POINTER(ma_index_info)]),
+    ("ma_index_contig", C.c_int,
+     [C.c_void_p, C.c_int64, C.POINTER(C.c_char_p), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("ma_map_batch", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_uint32, C.c_int, C.c_int,
+      C.POINTER(ma_params), C.POINTER(ma_hits), C.POINTER(ma_debug)]),
+    ("ma_map_batch_device", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_uint32, C.c_int, C.c_int,
+      C.POINTER(ma_params), C.POINTER(ma_hits), C.POINTER(ma_debug), C.c_void_p]),
+    ("ma_last_launch_count", C.c_int, [C.c_void_p]),
+    ("ma_synth_reference", C.c_int, [C.c_char_p, C.c_uint64, C.c_int, C.c_double, C.c_double, C.c_uint64]),
+    ("ma_synth_reads", C.c_int,
+     [C.c_char_p, C.POINTER(ma_read_model), C.c_uint32, C.c_int, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p,
+      C.c_void_p, C.c_void_p]),
+]
+
+
+def _load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python mojo-align_b200/build_lib.py` "
+            "(or __graft_entry__.build()); there is no fallback implementation"
+        )
+    lib = C.CDLL(str(LIB_PATH))
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def last_error(ctx=None) -> str:
+    msg = lib.ma_last_error(ctx)
+    return msg.decode() if msg else ""
+
+
+def check(rc: int, ctx=None) -> None:
+    if rc != MA_OK:
+        raise MojoAlignError(rc, last_error(ctx))
+
+
+def ptr(a) -> int | None:
+    """Address of a numpy array (or None)."""
+    if a is None:
+        return None
+    return a.ctypes.data
+
+
+def fspath(p) -> bytes:
+    return os.fsencode(os.fspath(p))

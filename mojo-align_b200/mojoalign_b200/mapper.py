@@ -1,0 +1,187 @@
+"""GPU mapping through the C ABI: contexts, resident indexes, batches.
+
+This is the function-level drop-in for the FM engine's batch step
+(_fm_fire_batch, fq2bam-meth/src/linear_gpu_fm.mojo:2279-2417): one call
+converts + packs the reads on the device, runs seed/extend and (paired)
+mate rescue, and returns the seven per-read output arrays of
+fm_seed_extend_kernel (L1183-1189) plus optional side outputs.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import MA_BS_C2T, MA_BS_G2A, MA_BS_NONE, check, fspath, lib, ma_debug, ma_hits, ma_index_info, ptr
+from .params import FmParams
+
+BS_MODES = {"": MA_BS_NONE, "C2T": MA_BS_C2T, "G2A": MA_BS_G2A}
+
+
+def bs_mode(mode) -> int:
+    """_bs_mode (fq2bam-meth/src/linear_fastq.mojo:29-34); ints pass through."""
+    if isinstance(mode, int):
+        return mode
+    return BS_MODES.get(mode, MA_BS_NONE)
+
+
+class GpuContext:
+    """One CUDA device context (one per host thread)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib.ma_ctx_create(device, C.byref(h)))
+        self.handle = h
+        self.device = device
+
+    def hbm_info(self) -> tuple[int, int]:
+        f, t = C.c_uint64(), C.c_uint64()
+        check(lib.ma_hbm_info(self.handle, C.byref(f), C.byref(t)), self.handle)
+        return f.value, t.value
+
+    def last_launch_count(self) -> int:
+        return lib.ma_last_launch_count(self.handle)
+
+    def close(self) -> None:
+        if self.handle:
+            lib.ma_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class Contig:
+    name: str
+    offset: int
+    length: int
+
+
+class GpuIndex:
+    """A bwa 0.7 FM-index made resident in HBM (FmIndex.load + upload)."""
+
+    def __init__(self, ctx: GpuContext, prefix, kmer_k: int = 12, hbm_budget_bytes: int = 0):
+        h = C.c_void_p()
+        check(lib.ma_index_open(ctx.handle, fspath(prefix), kmer_k, hbm_budget_bytes, C.byref(h)), ctx.handle)
+        self.handle = h
+        self.ctx = ctx
+        info = ma_index_info()
+        check(lib.ma_index_get_info(h, C.byref(info)))
+        self.info = info
+        self.contigs = []
+        for i in range(info.n_contigs):
+            nm, off, ln = C.c_char_p(), C.c_uint64(), C.c_uint64()
+            check(lib.ma_index_contig(h, i, C.byref(nm), C.byref(off), C.byref(ln)))
+            self.contigs.append(Contig(nm.value.decode(), off.value, ln.value))
+
+    def close(self) -> None:
+        if self.handle:
+            lib.ma_index_close(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class MapResult:
+    rid: np.ndarray
+    pos: np.ndarray
+    mapq: np.ndarray
+    flag: np.ndarray
+    sl: np.ndarray
+    sr: np.ndarray
+    nm: np.ndarray
+    uk: np.ndarray | None = None
+    ul: np.ndarray | None = None
+    us: np.ndarray | None = None
+    e: np.ndarray | None = None
+    score: np.ndarray | None = None
+
+    FIELDS = ("rid", "pos", "mapq", "flag", "sl", "sr", "nm")
+    DEBUG = ("uk", "ul", "us", "e", "score")
+
+    @classmethod
+    def empty(cls, n: int, debug: bool) -> "MapResult":
+        r = cls(np.empty(n, np.int32), np.empty(n, np.uint32), np.empty(n, np.uint32), np.empty(n, np.int32),
+                np.empty(n, np.uint32), np.empty(n, np.uint32), np.empty(n, np.uint32))
+        if debug:
+            r.uk = np.empty(n, np.uint64)
+            r.ul = np.empty(n, np.uint64)
+            r.us = np.empty(n, np.int32)
+            r.e = np.empty(n, np.int32)
+            r.score = np.empty(n, np.int32)
+        return r
+
+    def hits(self) -> ma_hits:
+        return ma_hits(*[ptr(getattr(self, f)) for f in self.FIELDS])
+
+    def debug(self) -> ma_debug | None:
+        if self.uk is None:
+            return None
+        return ma_debug(*[ptr(getattr(self, f)) for f in self.DEBUG])
+
+
+def map_batch(ctx: GpuContext, index: GpuIndex, bases: np.ndarray, lens: np.ndarray, n1: int, paired: bool,
+              max_len: int, bs_r1="C2T", bs_r2="G2A", params: FmParams | None = None, debug: bool = False,
+              out: MapResult | None = None) -> MapResult:
+    """Maps one batch of padded ASCII reads (R1 rows, then R2 rows)."""
+    params = params or FmParams()
+    n_seq = n1 * (2 if paired else 1)
+    bases = np.ascontiguousarray(bases, dtype=np.uint8)
+    lens = np.ascontiguousarray(lens, dtype=np.uint32)
+    if bases.size < n_seq * max_len or lens.size < n_seq:
+        raise ValueError("bases / lens smaller than the batch")
+    res = out if out is not None else MapResult.empty(n_seq, debug)
+    p = params.to_c()
+    hits = res.hits()
+    dbg = res.debug()
+    rc = lib.ma_map_batch(ctx.handle, index.handle, ptr(bases), ptr(lens), n1, int(paired), max_len,
+                          bs_mode(bs_r1), bs_mode(bs_r2), C.byref(p), C.byref(hits),
+                          C.byref(dbg) if dbg is not None else None)
+    check(rc, ctx.handle)
+    return res
+
+
+def map_batch_device(ctx: GpuContext, index: GpuIndex, d_bases: int, d_lens: int, n1: int, paired: bool,
+                     max_len: int, d_out: dict, bs_r1="C2T", bs_r2="G2A", params: FmParams | None = None,
+                     d_debug: dict | None = None, stream: int | None = None) -> None:
+    """Same on device pointers (ints); d_out / d_debug map field -> pointer."""
+    params = params or FmParams()
+    p = params.to_c()
+    hits = ma_hits(*[d_out[f] for f in MapResult.FIELDS])
+    dbg = ma_debug(*[d_debug[f] for f in MapResult.DEBUG]) if d_debug else None
+    rc = lib.ma_map_batch_device(ctx.handle, index.handle, d_bases, d_lens, n1, int(paired), max_len,
+                                 bs_mode(bs_r1), bs_mode(bs_r2), C.byref(p), C.byref(hits),
+                                 C.byref(dbg) if dbg is not None else None, stream)
+    check(rc, ctx.handle)
+
+
+def build_index(fasta, out_prefix, bwameth_c2t: bool = True, sa_intv: int = 32, device: int = -1) -> None:
+    """Writes a bwa-0.7 FM-index (optionally of the bwa-meth c2t text)."""
+    check(lib.ma_index_build(fspath(fasta), fspath(out_prefix), int(bwameth_c2t), sa_intv, device))
+
+
+__all__ = ["GpuContext", "GpuIndex", "MapResult", "map_batch", "map_batch_device", "build_index", "bs_mode",
+           "_lib"]

@@ -1,0 +1,207 @@
+"""GPU path (through the C ABI) against the oracle, bit-exact.
+
+Every output of the reference kernel (rid, pos, mapq, flag, sl, sr, nm) and
+the side outputs (uk, ul, us, e, score) must be identical to the oracle's
+restatement of fm_seed_extend_kernel + fm_mate_rescue_kernel
+(fq2bam-meth/src/linear_gpu_fm.mojo:1156-2011) on the same reads.  Integer
+work: the tolerance is zero.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from mojoalign_b200 import BENCH_PARAMS, FmParams, GpuContext, GpuIndex, MojoAlignError, map_batch, synth
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("rid", "pos", "mapq", "flag", "sl", "sr", "nm", "uk", "ul", "us", "e", "score")
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = GpuContext(0)
+    yield c
+    c.close()
+
+
+_INDEX_CACHE = {}
+
+
+def gpu_index(ctx, prefix, k):
+    key = (str(prefix), k)
+    if key not in _INDEX_CACHE:
+        _INDEX_CACHE[key] = GpuIndex(ctx, prefix, kmer_k=k)
+    return _INDEX_CACHE[key]
+
+
+def compare(prefix, ctx, bases, lens, n1, paired, max_len, params, k=12, bs=(1, 2)):
+    gi = gpu_index(ctx, prefix, k)
+    g = map_batch(ctx, gi, bases, lens, n1, paired, max_len, bs[0], bs[1], params, debug=True)
+    o = oracle.OracleIndex(prefix).map(bases, lens, n1, paired, max_len, bs[0], bs[1], params.as_list())
+    for f in FIELDS:
+        a, b = getattr(g, f), o[f]
+        bad = np.nonzero(a != b)[0]
+        assert bad.size == 0, (
+            f"{f}: {bad.size} of {a.size} reads differ; first read {bad[0]}: gpu {a[bad[0]]} oracle {b[bad[0]]}; "
+            + ", ".join(f"{x}=({getattr(g, x)[bad[0]]},{o[x][bad[0]]})" for x in FIELDS)
+        )
+    return g
+
+
+def sim(fa, n1, paired, max_len=150, seed=1, **model):
+    return synth.simulate_reads(fa, synth.ReadModel(**model), n1, paired, max_len, seed=seed)
+
+
+def test_single_end_default_model(ctx, small_ref):
+    fa, prefix = small_ref
+    rb = sim(fa, 20000, False)
+    g = compare(prefix, ctx, rb.bases, rb.lens, rb.n1, False, 150, BENCH_PARAMS)
+    assert (g.rid >= 0).mean() > 0.9
+
+
+def test_paired_end_with_rescue(ctx, small_ref):
+    fa, prefix = small_ref
+    rb = sim(fa, 10000, True, seed=2, sub_rate=0.02)
+    compare(prefix, ctx, rb.bases, rb.lens, rb.n1, True, 150, BENCH_PARAMS)
+
+
+@pytest.mark.parametrize("k", [0, 10, 12])
+def test_kmer_table_is_exact(ctx, small_ref, k):
+    fa, prefix = small_ref
+    rb = sim(fa, 5000, False, seed=3, sub_rate=0.01)
+    compare(prefix, ctx, rb.bases, rb.lens, rb.n1, False, 150, BENCH_PARAMS, k=k)
+
+
+def test_high_error_soft_clips_and_deletions(ctx, small_ref):
+    fa, prefix = small_ref
+    rb = sim(fa, 8000, True, seed=4, sub_rate=0.04, conv_non_cpg=0.9)
+    g = compare(prefix, ctx, rb.bases, rb.lens, rb.n1, True, 150, FmParams(seed_len=19, max_occ=500, max_diff=8))
+    assert (g.sl > 0).any() or (g.sr > 0).any()
+
+
+def test_contig_edges(ctx, edgy_ref):
+    fa, prefix = edgy_ref
+    for paired in (False, True):
+        rb = sim(fa, 6000, paired, seed=5, sub_rate=0.01, frag_mean=300)
+        compare(prefix, ctx, rb.bases, rb.lens, rb.n1, paired, 150, BENCH_PARAMS)
+
+
+def test_uneven_and_short_reads(ctx, small_ref):
+    fa, prefix = small_ref
+    rb = sim(fa, 8000, False, max_len=300, seed=6, len_fixed=0, len_lognorm_median=60, len_lognorm_sigma=0.8,
+             len_min=1, len_max=300)
+    assert rb.lens.min() < 19
+    compare(prefix, ctx, rb.bases, rb.lens, rb.n1, False, 300, BENCH_PARAMS)
+
+
+def test_long_reads_max_len(ctx, small_ref):
+    fa, prefix = small_ref
+    rb = sim(fa, 1500, False, max_len=1024, seed=7, len_fixed=0, len_lognorm_median=700, len_lognorm_sigma=0.3,
+             len_min=300, len_max=1024, sub_rate=0.01)
+    assert rb.lens.max() == 1024 or rb.lens.max() > 900
+    compare(prefix, ctx, rb.bases, rb.lens, rb.n1, False, 1024, BENCH_PARAMS)
+
+
+def test_reads_with_ambiguous_bases(ctx, small_ref):
+    fa, prefix = small_ref
+    rb = sim(fa, 6000, True, seed=8)
+    rng = np.random.default_rng(8)
+    for r in rng.choice(rb.n_seq, size=rb.n_seq // 4, replace=False):
+        L = int(rb.lens[r])
+        for p in rng.integers(0, L, size=int(rng.integers(1, 8))):
+            rb.bases[r, p] = rng.choice([ord("N"), ord("n"), ord("R"), ord(".")])
+    compare(prefix, ctx, rb.bases, rb.lens, rb.n1, True, 150, BENCH_PARAMS)
+
+
+PARAM_SETS = [
+    FmParams(),
+    FmParams(seed_len=12, seed_stride=1, max_occ=5),
+    FmParams(seed_len=25, seed_stride=3, max_occ=4096, max_diff=30),
+    FmParams(seed_len=19, max_occ=500, max_diff=2, max_soft=0, max_adj=0),
+    FmParams(seed_len=19, max_occ=500, max_soft=300, max_adj=12, rescue_win=5000),
+    FmParams(seed_len=8, seed_stride=5, max_occ=64, max_adj=20, rescue_win=10),
+    FmParams(seed_len=19, max_occ=1, max_diff=1, max_soft=5, max_adj=3, rescue_win=32),
+]
+
+
+@pytest.mark.parametrize("params", PARAM_SETS, ids=lambda p: "-".join(map(str, p.as_list())))
+def test_parameter_sweep(ctx, edgy_ref, params):
+    fa, prefix = edgy_ref
+    rb = sim(fa, 3000, True, seed=9, sub_rate=0.02)
+    compare(prefix, ctx, rb.bases, rb.lens, rb.n1, True, 150, params)
+
+
+def test_unconverted_reads_all_modes(ctx, small_ref):
+    fa, prefix = small_ref
+    rb = sim(fa, 4000, True, seed=10, conv_non_cpg=0.0, cpg_retain=1.0)
+    for bs in ((0, 0), (2, 1), (1, 1)):
+        compare(prefix, ctx, rb.bases, rb.lens, rb.n1, True, 150, BENCH_PARAMS, bs=bs)
+
+
+def _ref_text(fa):
+    seqs = []
+    for block in open(fa).read().split(">")[1:]:
+        lines = block.splitlines()
+        seqs.append("".join(lines[1:]).upper())
+    return seqs
+
+
+def test_deletions_and_text_start(ctx, small_ref):
+    """Reads with a 1-bp deletion (deletion probe) and reads overhanging the
+    first contig's start (negative text positions in the probe)."""
+    fa, prefix = small_ref
+    chrom = _ref_text(fa)[0].replace("C", "T")  # f-strand-like reads (C->T)
+    rng = np.random.default_rng(11)
+    reads = []
+    for _ in range(3000):
+        p = int(rng.integers(0, len(chrom) - 200))
+        s = chrom[p:p + 151]
+        g = int(rng.integers(10, 140))
+        reads.append(s[:g] + s[g + 1:])
+    for _ in range(600):
+        pre = "".join(rng.choice(list("AGT"), size=int(rng.integers(1, 30))))
+        reads.append((pre + chrom[: 150])[:150])
+    n = len(reads)
+    bases = np.full((n, 150), ord("N"), np.uint8)
+    lens = np.zeros(n, np.uint32)
+    for i, s in enumerate(reads):
+        bases[i, : len(s)] = np.frombuffer(s.encode(), np.uint8)
+        lens[i] = len(s)
+    for params in (BENCH_PARAMS, FmParams(seed_len=19, max_occ=500, max_diff=3, max_soft=30)):
+        compare(prefix, ctx, bases, lens, n, False, 150, params)
+
+
+def test_empty_batch_and_errors(ctx, small_ref):
+    fa, prefix = small_ref
+    gi = gpu_index(ctx, prefix, 12)
+    bases = np.zeros((0, 150), np.uint8)
+    lens = np.zeros(0, np.uint32)
+    r = map_batch(ctx, gi, bases, lens, 0, False, 150)
+    assert r.rid.size == 0
+    bases = np.full((2, 8), ord("A"), np.uint8)
+    with pytest.raises(MojoAlignError) as e:
+        map_batch(ctx, gi, bases, np.array([8, 9], np.uint32), 2, False, 8)
+    assert e.value.code == -1
+    with pytest.raises(MojoAlignError):
+        map_batch(ctx, gi, bases, np.array([8, 8], np.uint32), 2, False, 8, params=FmParams(seed_stride=0))
+    # the context still works after a rejected call
+    rb = sim(fa, 500, False, seed=12)
+    compare(prefix, ctx, rb.bases, rb.lens, rb.n1, False, 150, BENCH_PARAMS)
+
+
+def test_toy_fixture_shape(ctx, tmp_path):
+    """The reference's toy fixture shape (fq2bam-meth/tests/data/fq2bam_fixture):
+    a 64-bp A/T-alternating chr1 and two exact 32-bp PE reads."""
+    from mojoalign_b200 import build_index
+
+    fa = tmp_path / "ref.fa"
+    fa.write_text(">chr1\n" + "AT" * 32 + "\n")
+    prefix = tmp_path / "ref.fa.bwameth.c2t"
+    build_index(fa, prefix, bwameth_c2t=True, sa_intv=32)
+    read = np.frombuffer(("AT" * 16).encode(), np.uint8)
+    bases = np.stack([read, read])
+    lens = np.array([32, 32], np.uint32)
+    for p in (FmParams(), FmParams(seed_len=19), FmParams(seed_len=8, max_occ=4096)):
+        compare(prefix, ctx, bases, lens, 1, True, 32, p, k=0)
