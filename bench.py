@@ -1,0 +1,420 @@
+#!/usr/bin/env python
+"""Benchmark of the linear bisulfite seed-and-extend path (reads/s).
+
+Workload (per GPU): a synthetic 250 Mbp reference (GC 0.41, CpG ~1%, seed 0)
+indexed as the bwa-meth dual-strand text, and 10M bisulfite read pairs of
+2x150 bp (fragments N(350, 50), non-CpG conversion 0.99, CpG retention 0.75,
+0.5% substitutions, 5% random reads, seed 1 + rank).  Parameters: the
+reference defaults with seed_len 19 and max_occ 500.  One step maps the
+whole batch through the plain single-launch form (pack -> seed/extend ->
+mate rescue), counting each mate as one read.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` is measured with the reads already
+in HBM; `e2e` through the host API (ma_map_batch) with pinned host buffers,
+copies included.  `--impl reference` times the CPU restatement of the
+reference kernels (the oracle; the Mojo reference cannot run here) on all
+host cores over a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+for p in (ROOT, ROOT / "mojo-align_b200"):
+    if str(p) not in sys.path:
+        sys.path.insert(0, str(p))
+
+import numpy as np  # noqa: E402
+
+METRIC = "reads/s seed+extend"
+READ_LEN = 150
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--genome-mb", type=int, default=250)
+    ap.add_argument("--pairs", type=int, default=10_000_000, help="read pairs per GPU")
+    ap.add_argument("--kmer", type=int, default=12)
+    ap.add_argument("--workdir", default=os.environ.get("MOJOALIGN_BENCH_DIR", tempfile.gettempdir()))
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the oracle timing (profiling runs)")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Dist:
+    """Barrier / max-reduce over ranks (torch.distributed when world > 1)."""
+
+    def __init__(self, world: int, backend: str):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=1800))
+            self.dist = dist
+            self.pg = True
+        self.backend = backend
+
+    def barrier(self):
+        if self.pg:
+            if self.backend == "nccl":
+                import torch
+
+                self.dist.barrier(device_ids=[torch.cuda.current_device()])
+            else:
+                self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.dist.destroy_process_group()
+
+
+def prepare_reference(args, rank, dist: Dist, device: int):
+    """Synthetic reference + bwa-meth index, built once per node by rank 0."""
+    from mojoalign_b200 import build_index, synth
+
+    d = Path(args.workdir) / f"mojoalign_bench_{args.genome_mb}mb"
+    d.mkdir(parents=True, exist_ok=True)
+    fa = d / "ref.fa"
+    prefix = Path(str(fa) + ".bwameth.c2t")
+    done = d / "index.ok"
+    t0 = time.time()
+    if rank == 0 and not done.exists():
+        try:
+            import torch
+
+            device = device if torch.cuda.is_available() else -1
+        except ImportError:
+            device = -1
+        n_contigs = max(1, args.genome_mb // 50)
+        synth.write_reference(fa, args.genome_mb * 1_000_000, n_contigs=n_contigs, gc=0.41, cpg=0.01, seed=0)
+        build_index(fa, prefix, bwameth_c2t=True, sa_intv=32, device=device)
+        done.write_text("ok\n")
+    dist.barrier()
+    return fa, prefix, time.time() - t0
+
+
+def simulate(args, fa, rank, bases_out=None):
+    from mojoalign_b200 import synth
+
+    model = synth.ReadModel(len_fixed=READ_LEN, frag_mean=350, frag_sd=50, conv_non_cpg=0.99, cpg_retain=0.75,
+                            sub_rate=0.005, random_frac=0.05)
+    return synth.simulate_reads(fa, model, args.pairs, True, READ_LEN, seed=1 + rank, bases_out=bases_out)
+
+
+def sample_pairs(rb, n):
+    """First n pairs of a paired batch, as a smaller paired batch."""
+    b = np.concatenate([rb.bases[:n], rb.bases[rb.n1:rb.n1 + n]])
+    l = np.concatenate([rb.lens[:n], rb.lens[rb.n1:rb.n1 + n]])
+    return b, l
+
+
+def time_oracle(prefix, rb, params, target_s, probe_pairs=20000):
+    """Times the oracle on a bounded sample sized to about target_s seconds."""
+    import oracle
+
+    ix = oracle.OracleIndex(prefix)
+    b, l = sample_pairs(rb, probe_pairs)
+    t = time.perf_counter()
+    ix.map(b, l, probe_pairs, True, READ_LEN, 1, 2, params.as_list())
+    rate = 2 * probe_pairs / (time.perf_counter() - t)
+    n = int(min(rb.n1, max(probe_pairs, rate * target_s / 2)))
+    b, l = sample_pairs(rb, n)
+    t = time.perf_counter()
+    out = ix.map(b, l, n, True, READ_LEN, 1, 2, params.as_list())
+    dt = time.perf_counter() - t
+    return ix, out, n, 2 * n / dt, dt
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        rows = [r.split(",") for r in self.path.read_text().splitlines() if r.count(",") >= 8]
+        self.path.unlink(missing_ok=True)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.strip() == "Active"})
+        busy = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {"hbm_gbs": 6650.0, "_fallback": True}
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = Dist(world, "nccl")
+    from mojoalign_b200 import BENCH_PARAMS, GpuContext, GpuIndex, MapResult, map_batch, map_batch_device
+    from mojoalign_b200 import _lib
+
+    params = BENCH_PARAMS
+    fa, prefix, prep_s = prepare_reference(args, rank, dist, local)
+    n_seq = 2 * args.pairs
+    pinned = torch.empty((n_seq, READ_LEN), dtype=torch.uint8, pin_memory=True)
+    t = time.time()
+    rb = simulate(args, fa, rank, bases_out=pinned.numpy())
+    sim_s = time.time() - t
+    lens_pinned = torch.from_numpy(rb.lens.view(np.int32)).pin_memory()
+
+    ctx = GpuContext(local)
+    t = time.time()
+    gi = GpuIndex(ctx, prefix, kmer_k=args.kmer)
+    open_s = time.time() - t
+
+    # ---- device-resident inputs and outputs ----
+    d_bases = pinned.to(f"cuda:{local}").reshape(-1)
+    d_lens = lens_pinned.to(f"cuda:{local}")
+    d_out = {f: torch.empty(n_seq, dtype=torch.int32, device=f"cuda:{local}") for f in MapResult.FIELDS}
+    out_ptrs = {f: t_.data_ptr() for f, t_ in d_out.items()}
+    stream = torch.cuda.current_stream()
+
+    def step():
+        map_batch_device(ctx, gi, d_bases.data_ptr(), d_lens.data_ptr(), args.pairs, True, READ_LEN, out_ptrs,
+                         "C2T", "G2A", params, stream=stream.cuda_stream)
+
+    # traffic accounting: one untimed pass of the counting kernel
+    _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 2), ctx.handle)
+    step()
+    tally = (_lib.C.c_uint64 * 8)()
+    _lib.lib.ma_ctx_traffic(ctx.handle, tally)
+    tally = list(tally)
+    _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 1), ctx.handle)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    seed_ms = []
+    kms = (_lib.C.c_float * 3)()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+        _lib.lib.ma_ctx_kernel_ms(ctx.handle, kms)
+        seed_ms.append(float(kms[1]))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    clk = clocks.stop()
+    dist.barrier()
+    launches = ctx.last_launch_count() * args.steps
+    ms_max = dist.max(ms)
+    value = n_seq * world / (ms_max / 1000.0)
+
+    # ---- end to end through the host API (pinned host in, host out) ----
+    host_out = MapResult.empty(n_seq, debug=False)
+    pin_out = {f: torch.empty(n_seq, dtype=torch.int32, pin_memory=True) for f in MapResult.FIELDS}
+    res = MapResult(*[pin_out[f].numpy().view(getattr(host_out, f).dtype) for f in MapResult.FIELDS])
+    bases_np = pinned.numpy()
+    lens_np = rb.lens
+    map_batch(ctx, gi, bases_np, lens_np, args.pairs, True, READ_LEN, "C2T", "G2A", params, out=res)
+    dist.barrier()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        map_batch(ctx, gi, bases_np, lens_np, args.pairs, True, READ_LEN, "C2T", "G2A", params, out=res)
+    e2e_s = dist.max((time.perf_counter() - t) / args.steps)
+    e2e_value = n_seq * world / e2e_s
+    mapped = float((res.rid >= 0).mean())
+
+    # ---- roofline of the dominant kernel (seed/extend) ----
+    peaks = measured_peaks()
+    words = (READ_LEN + 31) // 32
+    alg_bytes = 32 * (tally[0] + tally[1] + tally[2] + tally[3]) + n_seq * (4 * words * 8 + 4) + n_seq * 28
+    seed_avg_ms = statistics.mean(seed_ms)
+    achieved = alg_bytes / (seed_avg_ms / 1000.0) / 1e9
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+            "frac": round(achieved / peaks.get("hbm_gbs"), 4), "traffic": None,
+            "peak_source": "fallback" if peaks.get("_fallback") else "measured (MEASURED_PEAKS.json hbm_gbs)",
+            "kernel": "seed_extend_kernel", "kernel_ms": round(seed_avg_ms, 3),
+            "alg_bytes_per_launch": int(alg_bytes),
+            "tally_per_read": {k: round(v / n_seq, 3) for k, v in zip(
+                ["occ_lines_32B", "kmer_loads", "sa_loads", "pac_sectors_32B", "backward_steps", "endpoints",
+                 "loci_evaluated", "read_words"], tally)}}
+    line = {"metric": METRIC, "value": round(value, 1), "unit": "reads/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"plain single-launch, {args.genome_mb} Mbp synthetic bisulfite reference "
+                                   f"(bwa-meth c2t index), {args.pairs} PE 2x{READ_LEN} read pairs per GPU",
+                       "form": "plain single-launch", "genome_bp": args.genome_mb * 1_000_000,
+                       "reads_per_gpu": n_seq, "read_len": READ_LEN, "paired": True,
+                       "params": dict(zip(["seed_len", "seed_stride", "max_occ", "max_diff", "max_soft", "max_adj",
+                                           "rescue_win"], params.as_list())),
+                       "kmer_k": args.kmer, "l2": "inputs larger than L2 (reads and index several GB)",
+                       "mapped_frac": round(mapped, 4)},
+            "e2e": {"value": round(e2e_value, 1), "unit": "reads/s",
+                    "h2d_bytes_per_step": int(n_seq * READ_LEN + n_seq * 4),
+                    "d2h_bytes_per_step": int(n_seq * 28)},
+            "gpu_launches": launches, "roofline": roof, "clocks": clk,
+            "setup_s": {"reference_and_index": round(prep_s, 1), "reads": round(sim_s, 1),
+                        "index_open": round(open_s, 1)}}
+    if rank == 0:
+        line["gather_roofline"] = {}
+        for lb in (32, 64):
+            g = _lib.C.c_double()
+            _lib.check(_lib.lib.ma_bench_gather(ctx.handle, 8 << 30, lb, 1 << 30, _lib.C.byref(g)), ctx.handle)
+            line["gather_roofline"][f"hbm_{lb}B_GBs"] = round(g.value, 1)
+        g = _lib.C.c_double()
+        _lib.check(_lib.lib.ma_bench_gather(ctx.handle, 64 << 20, 32, 1 << 30, _lib.C.byref(g)), ctx.handle)
+        line["gather_roofline"]["l2_32B_GBs"] = round(g.value, 1)
+        line["roofline"]["frac_of_gather32"] = round(achieved / line["gather_roofline"]["hbm_32B_GBs"], 4)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ix, o, n, rate, dt = time_oracle(prefix, rb, params, args.cpu_seconds)
+        import oracle
+
+        line["cpu_baseline"] = {"value": round(rate, 1), "unit": "reads/s", "cores": oracle.max_threads(),
+                                "kind": "port", "sample": f"first {n} pairs ({2 * n} reads) of the GPU workload, "
+                                                          f"{dt:.1f} s", "cpu": _cpu_model()}
+        # full-size parity: the GPU's outputs for those reads against the oracle
+        bad = 0
+        for f in MapResult.FIELDS:
+            g = getattr(res, f)
+            g = np.concatenate([g[:n], g[args.pairs:args.pairs + n]])
+            bad += int((g != o[f]).sum())
+        line["parity_sample"] = {"reads": 2 * n, "mismatched_fields": bad}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    gi.close()
+    ctx.close()
+    dist.close()
+
+
+def _cpu_model() -> str:
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args, rank, world, local):
+    """The oracle (CPU restatement of the reference kernels) on all host cores."""
+    if rank != 0:
+        return
+    import oracle
+    from mojoalign_b200 import BENCH_PARAMS
+
+    class _Solo(Dist):
+        def __init__(self):
+            super().__init__(1, "gloo")
+
+    dist = _Solo()
+    fa, prefix, _ = prepare_reference(args, 0, dist, local)
+    rb = simulate(args, fa, 0)
+    params = BENCH_PARAMS
+    ix = oracle.OracleIndex(prefix)
+    # size one step to about cpu_seconds / (steps + warmup) * 2
+    probe = 10000
+    b, l = sample_pairs(rb, probe)
+    t = time.perf_counter()
+    ix.map(b, l, probe, True, READ_LEN, 1, 2, params.as_list())
+    rate = 2 * probe / (time.perf_counter() - t)
+    per_step_s = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    n = int(min(rb.n1, max(probe, rate * per_step_s / 2)))
+    b, l = sample_pairs(rb, n)
+    for _ in range(args.warmup):
+        ix.map(b, l, n, True, READ_LEN, 1, 2, params.as_list())
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        ix.map(b, l, n, True, READ_LEN, 1, 2, params.as_list())
+    dt = (time.perf_counter() - t) / args.steps
+    value = 2 * n / dt
+    line = {"metric": METRIC, "value": round(value, 1), "unit": "reads/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(dt * 1000, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"plain single-launch, {args.genome_mb} Mbp synthetic bisulfite reference "
+                                   f"(bwa-meth c2t index), {args.pairs} PE 2x{READ_LEN} read pairs per GPU",
+                       "form": "plain single-launch", "genome_bp": args.genome_mb * 1_000_000,
+                       "reads_per_gpu": 2 * args.pairs, "read_len": READ_LEN, "paired": True},
+            "cpu_baseline": {"value": round(value, 1), "unit": "reads/s", "cores": oracle.max_threads(),
+                             "kind": "port", "cpu": _cpu_model(),
+                             "sample": f"first {n} pairs ({2 * n} reads) of the workload per step"},
+            "e2e": {"value": round(value, 1), "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world, local)
+    else:
+        run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -194,6 +194,23 @@ int ma_map_batch_device(ma_ctx* ctx, const ma_index* idx,
 /* Number of kernel launches the last mapping call on ctx issued. */
 int ma_last_launch_count(const ma_ctx* ctx);
 
+/* ---- measurement (no reference counterpart; the reference only prints
+ * perf_counter stage timers, linear_gpu_fm.mojo:2270-2273,3317-3340) ---- */
+
+/* flags bit 0: time each kernel of a mapping call with CUDA events on its
+ * stream; bit 1: run the counting instantiation of the seed kernel, which
+ * tallies its index and text accesses (slower; for traffic accounting). */
+int ma_ctx_set_profiling(ma_ctx* ctx, int flags);
+/* Device time (ms) of pack, seed/extend and rescue in the last call. */
+int ma_ctx_kernel_ms(const ma_ctx* ctx, float* out3);
+/* Tallies of the last counting call: 32-B Occ lines, k-mer entries, SA
+ * entries, 32-B pac sectors, backward steps, endpoints searched, loci
+ * evaluated, read words read. */
+int ma_ctx_traffic(const ma_ctx* ctx, uint64_t* out8);
+/* Random aligned `line_bytes` (32 or 64) gathers over a buffer of
+ * buffer_bytes: achieved GB/s (the random-gather roofline). */
+int ma_bench_gather(ma_ctx* ctx, uint64_t buffer_bytes, int line_bytes, uint64_t n_loads, double* gbps);
+
 /* ---- synthetic workloads (bench and tests; no reference counterpart) -- */
 
 /*

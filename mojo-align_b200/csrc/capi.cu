@@ -16,7 +16,8 @@ namespace ma {
 int launch_pack(const uint8_t* d_bases, const uint32_t* d_lens, int64_t n_seq, int64_t n1, int max_len, int words,
                 int bs_r1, int bs_r2, uint64_t* d_packed, int* d_err, cudaStream_t st);
 int launch_seed_extend(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
-                       cudaStream_t st);
+                       unsigned long long* d_tally, cudaStream_t st);
+double run_gather_bench(uint64_t buffer_bytes, int line_bytes, uint64_t n_loads, int sm_count, cudaStream_t st);
 int launch_rescue(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int64_t n_pairs,
                   cudaStream_t st);
 }  // namespace ma
@@ -63,6 +64,12 @@ struct ma_ctx {
     cudaStream_t stream = nullptr;
     std::string err;
     int last_launches = 0;
+    int profiling = 0;           // bit 0: per-kernel events, bit 1: traffic tally
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    float kernel_ms[3] = {0, 0, 0};
+    uint64_t traffic[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    bool rescue_ran = false;
+    DevBuf tally;
     DevBuf bases, lens, packed, err_flag;
     DevBuf o_rid, o_pos, o_mapq, o_flag, o_sl, o_sr, o_nm;
     DevBuf d_uk, d_ul, d_us, d_e, d_score;
@@ -130,12 +137,24 @@ void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const
     ctx->err_flag.ensure(sizeof(int));
     ck(cudaMemsetAsync(ctx->err_flag.p, 0, sizeof(int), st), "memset");
     int launches = 0;
+    const bool timed = ctx->profiling & 1;
+    unsigned long long* d_tally = nullptr;
+    if (ctx->profiling & 2) {
+        ctx->tally.ensure(8 * sizeof(unsigned long long));
+        d_tally = ctx->tally.as<unsigned long long>();
+        ck(cudaMemsetAsync(d_tally, 0, 8 * sizeof(unsigned long long), st), "memset");
+    }
+    if (timed) ck(cudaEventRecord(ctx->ev[0], st), "event");
     launches += launch_pack(d_bases, d_lens, n_seq, n1, static_cast<int>(max_len), words, bs_r1, bs_r2,
                             ctx->packed.as<uint64_t>(), ctx->err_flag.as<int>(), st);
+    if (timed) ck(cudaEventRecord(ctx->ev[1], st), "event");
     DevReads R{ctx->packed.as<uint64_t>(), d_lens, words, n_seq};
     DevParams P = to_dev(p);
-    launches += launch_seed_extend(idx->dix, R, P, out, st);
-    if (paired && p->rescue_win > 0) launches += launch_rescue(idx->dix, R, P, out, n1, st);
+    launches += launch_seed_extend(idx->dix, R, P, out, d_tally, st);
+    if (timed) ck(cudaEventRecord(ctx->ev[2], st), "event");
+    ctx->rescue_ran = paired && p->rescue_win > 0;
+    if (ctx->rescue_ran) launches += launch_rescue(idx->dix, R, P, out, n1, st);
+    if (timed) ck(cudaEventRecord(ctx->ev[3], st), "event");
     ck(cudaGetLastError(), "kernel launch");
     ctx->last_launches = launches;
 }
@@ -146,6 +165,15 @@ void check_err_flag(ma_ctx* ctx, cudaStream_t st) {
     ck(cudaStreamSynchronize(st), "mapping kernels");
     if (h == 1) fail(MA_ERR_ARG, "a read length exceeds max_len");
     if (h) fail(MA_ERR_INTERNAL, "device error flag " + std::to_string(h));
+    if (ctx->profiling & 1) {
+        for (int i = 0; i < 3; ++i) ck(cudaEventElapsedTime(&ctx->kernel_ms[i], ctx->ev[i], ctx->ev[i + 1]), "elapsed");
+        if (!ctx->rescue_ran) ctx->kernel_ms[2] = 0;
+    }
+    if (ctx->profiling & 2) {
+        unsigned long long t[8];
+        ck(cudaMemcpy(t, ctx->tally.p, sizeof t, cudaMemcpyDeviceToHost), "D2H tally");
+        for (int i = 0; i < 8; ++i) ctx->traffic[i] = t[i];
+    }
 }
 
 }  // namespace
@@ -194,6 +222,9 @@ int ma_ctx_create(int device_ordinal, ma_ctx** out) {
 void ma_ctx_destroy(ma_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
+    for (cudaEvent_t& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    ctx->tally.release();
     for (DevBuf* b : {&ctx->bases, &ctx->lens, &ctx->packed, &ctx->err_flag, &ctx->o_rid, &ctx->o_pos, &ctx->o_mapq,
                       &ctx->o_flag, &ctx->o_sl, &ctx->o_sr, &ctx->o_nm, &ctx->d_uk, &ctx->d_ul, &ctx->d_us,
                       &ctx->d_e, &ctx->d_score})
@@ -376,6 +407,38 @@ int ma_map_batch_device(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases
 }
 
 int ma_last_launch_count(const ma_ctx* ctx) { return ctx ? ctx->last_launches : 0; }
+
+int ma_ctx_set_profiling(ma_ctx* ctx, int flags) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        use_device(ctx);
+        if ((flags & 1) && !ctx->ev[0])
+            for (cudaEvent_t& e : ctx->ev) ck(cudaEventCreate(&e), "cudaEventCreate");
+        ctx->profiling = flags;
+    });
+}
+
+int ma_ctx_kernel_ms(const ma_ctx* ctx, float* out3) {
+    if (!ctx || !out3) return MA_ERR_ARG;
+    for (int i = 0; i < 3; ++i) out3[i] = ctx->kernel_ms[i];
+    return MA_OK;
+}
+
+int ma_ctx_traffic(const ma_ctx* ctx, uint64_t* out8) {
+    if (!ctx || !out8) return MA_ERR_ARG;
+    for (int i = 0; i < 8; ++i) out8[i] = ctx->traffic[i];
+    return MA_OK;
+}
+
+int ma_bench_gather(ma_ctx* ctx, uint64_t buffer_bytes, int line_bytes, uint64_t n_loads, double* gbps) {
+    if (!ctx || !gbps) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        use_device(ctx);
+        int sms = 0;
+        ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device), "attribute");
+        *gbps = run_gather_bench(buffer_bytes, line_bytes, n_loads, sms, ctx->stream);
+    });
+}
 
 int ma_synth_reference(const char* fasta_out, uint64_t total_len, int n_contigs, double gc, double cpg,
                        uint64_t seed) {

@@ -23,6 +23,7 @@
 #include <fstream>
 #include <random>
 #include <sstream>
+#include <thread>
 
 #include "ma_internal.h"
 
@@ -261,6 +262,18 @@ void build_index(const std::string& fasta, const std::string& out_prefix, bool b
     uint64_t L2[5] = {0, 0, 0, 0, 0};
     for (uint64_t i = 0; i < n; ++i) L2[text[i] + 1]++;
     for (int c = 1; c <= 4; ++c) L2[c] += L2[c - 1];
+    // BWT symbol of every row (4 = the sentinel row), gathered in parallel
+    std::vector<uint8_t> bsym(n + 1);
+    {
+        const unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < nt; ++t)
+            pool.emplace_back([&, t] {
+                const uint64_t r0 = (n + 1) * t / nt, r1 = (n + 1) * (t + 1) / nt;
+                for (uint64_t row = r0; row < r1; ++row) bsym[row] = sa[row] ? text[sa[row] - 1] : 4;
+            });
+        for (auto& th : pool) th.join();
+    }
     // stored BWT: rows 0..n without the sentinel row
     const uint64_t n_occ = (n + 127) / 128 + 1;
     std::vector<uint32_t> bwt((n + 15) / 16 + 8 * n_occ, 0);
@@ -269,11 +282,11 @@ void build_index(const std::string& fasta, const std::string& out_prefix, bool b
         uint64_t k = 0;       // stored position
         uint64_t wbase = 0;   // word index of current block start
         for (uint64_t row = 0; row <= n; ++row) {
-            if (sa[row] == 0) {
+            if (bsym[row] == 4) {
                 primary = row;
                 continue;
             }
-            uint8_t c = text[sa[row] - 1];
+            uint8_t c = bsym[row];
             if (k % 128 == 0) {
                 wbase = (k / 128) * 16;
                 for (int cc = 0; cc < 4; ++cc) {

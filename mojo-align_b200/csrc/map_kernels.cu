@@ -77,43 +77,60 @@ __device__ __forceinline__ int code_at(const ReadView& v, int s) {
     return static_cast<int>((__ldg(v.fwd + w) >> sh) & 3);
 }
 
+// Per-thread traffic tally of the counting kernel variant (S = true).  The
+// timed kernel is the S = false instantiation, where every tally compiles
+// away.
+struct Tally {
+    uint32_t occ_lines, kmer_loads, sa_loads, pac_sectors, steps, endpoints, loci, read_words;
+};
+
 // Mismatch bits (even positions) of read word w against the text at
 // bstart + 32*w; N bases always mismatch.
+template <bool S>
 __device__ __forceinline__ uint64_t mm_word(const uint64_t* __restrict__ pacw, const uint64_t* q,
-                                            const uint64_t* qn, int64_t bstart, int w) {
+                                            const uint64_t* qn, int64_t bstart, int w, Tally& t) {
+    if constexpr (S) {
+        // the window reads 16 bytes at word (bstart + 32w + 32*PAC_PAD) >> 5
+        const uint64_t wi = static_cast<uint64_t>(bstart + 32 * w + 32 * PAC_PAD) >> 5;
+        t.pac_sectors += ((wi * 8) >> 5) == ((wi * 8 + 15) >> 5) ? 1 : 2;
+        t.read_words += 2;
+    }
     uint64_t x = __ldg(q + w) ^ ref_window(pacw, bstart + 32 * w);
     return ((x | (x >> 1)) & kEven) | __ldg(qn + w);
 }
 
 // min(mismatches over read positions [a, b), cap): the reference's counting
 // loops stop as soon as the count exceeds their budget.
+template <bool S>
 __device__ __forceinline__ int count_mm(const uint64_t* __restrict__ pacw, const uint64_t* q, const uint64_t* qn,
-                                        int64_t bstart, int a, int b, int cap) {
+                                        int64_t bstart, int a, int b, int cap, Tally& t) {
     if (a >= b) return 0;
     int n = 0;
     for (int w = a >> 5; w <= (b - 1) >> 5; ++w) {
-        n += __popcll(mm_word(pacw, q, qn, bstart, w) & range_mask(w, a, b));
+        n += __popcll(mm_word<S>(pacw, q, qn, bstart, w, t) & range_mask(w, a, b));
         if (n >= cap) return cap;
     }
     return n;
 }
 
 // First / last read position in [a, b) whose base matches the text.
+template <bool S>
 __device__ __forceinline__ int first_match(const uint64_t* __restrict__ pacw, const uint64_t* q,
-                                           const uint64_t* qn, int64_t bstart, int a, int b) {
+                                           const uint64_t* qn, int64_t bstart, int a, int b, Tally& t) {
     if (a >= b) return -1;
     for (int w = a >> 5; w <= (b - 1) >> 5; ++w) {
-        uint64_t m = ~mm_word(pacw, q, qn, bstart, w) & range_mask(w, a, b);
+        uint64_t m = ~mm_word<S>(pacw, q, qn, bstart, w, t) & range_mask(w, a, b);
         if (m) return 32 * w + (__ffsll(static_cast<long long>(m)) - 1) / 2;
     }
     return -1;
 }
 
+template <bool S>
 __device__ __forceinline__ int last_match(const uint64_t* __restrict__ pacw, const uint64_t* q,
-                                          const uint64_t* qn, int64_t bstart, int a, int b) {
+                                          const uint64_t* qn, int64_t bstart, int a, int b, Tally& t) {
     if (a >= b) return -1;
     for (int w = (b - 1) >> 5; w >= (a >> 5); --w) {
-        uint64_t m = ~mm_word(pacw, q, qn, bstart, w) & range_mask(w, a, b);
+        uint64_t m = ~mm_word<S>(pacw, q, qn, bstart, w, t) & range_mask(w, a, b);
         if (m) return 32 * w + (63 - __clzll(static_cast<long long>(m))) / 2;
     }
     return -1;
@@ -152,14 +169,14 @@ __device__ __forceinline__ int64_t contig_of(const DevIndex& ix, int64_t probe) 
 // nm_d(g) = min(1 + mismatches(read[0,g) vs text at bstart) +
 //           mismatches(read[g,qlen) vs text at bstart+1), budget+1).
 // Text positions below 0 read as "not a base" (a mismatch).
-template <typename Visit>
+template <bool S, typename Visit>
 __device__ __forceinline__ void deletion_scan(const uint64_t* __restrict__ pacw, const uint64_t* q,
                                               const uint64_t* qn, int64_t bstart, int qlen, int budget,
-                                              Visit visit) {
+                                              Tally& t, Visit visit) {
     const int nw = (qlen + 31) >> 5;
     int R = 0;
     for (int w = 0; w < nw; ++w) {
-        uint64_t m1 = mm_word(pacw, q, qn, bstart + 1, w);
+        uint64_t m1 = mm_word<S>(pacw, q, qn, bstart + 1, w, t);
         if (bstart + 1 < 0) m1 |= range_mask(w, 0, static_cast<int>(-(bstart + 1)));
         R += __popcll(m1 & range_mask(w, 0, qlen));
     }
@@ -174,8 +191,8 @@ __device__ __forceinline__ void deletion_scan(const uint64_t* __restrict__ pacw,
             int w = g >> 5;
             if (w != cw) {
                 cw = w;
-                m0 = mm_word(pacw, q, qn, bstart, w);
-                m1 = mm_word(pacw, q, qn, bstart + 1, w);
+                m0 = mm_word<S>(pacw, q, qn, bstart, w, t);
+                m1 = mm_word<S>(pacw, q, qn, bstart + 1, w, t);
                 if (bstart < 0) m0 |= range_mask(w, 0, static_cast<int>(-bstart));
                 if (bstart + 1 < 0) m1 |= range_mask(w, 0, static_cast<int>(-(bstart + 1)));
                 uint64_t in = range_mask(w, 0, qlen);
@@ -191,9 +208,11 @@ __device__ __forceinline__ void deletion_scan(const uint64_t* __restrict__ pacw,
 
 // Evaluates every shift adj of one locus (b0, strand): the body of the
 // reference's adj loop, L1526-1826.
+template <bool S>
 __device__ void eval_locus(const DevIndex& ix, const ReadView& rd, int64_t b0, int is_rev, int adj_cap,
                            int budget, int clip_cap, uint32_t ord_row, Best& best, uint64_t uk, uint64_t ul,
-                           int us, int e) {
+                           int us, int e, Tally& t) {
+    if constexpr (S) t.loci++;
     const int qlen = rd.qlen;
     const uint64_t* q = is_rev ? rd.rc : rd.fwd;
     const uint64_t* qn = is_rev ? rd.nr : rd.nf;
@@ -210,26 +229,26 @@ __device__ void eval_locus(const DevIndex& ix, const ReadView& rd, int64_t b0, i
         const int64_t sr0 = local + qlen > clen ? local + qlen - clen : 0;
         if (!(sl0 + sr0 < qlen && sl0 <= clip_cap && sr0 <= clip_cap)) continue;
         const uint32_t ord = (ord_row + static_cast<uint32_t>(adj + 12)) * KIND_SPAN;
-        int nm = count_mm(ix.pacw, q, qn, bstart, static_cast<int>(sl0), static_cast<int>(qlen - sr0), budget + 1);
+        int nm = count_mm<S>(ix.pacw, q, qn, bstart, static_cast<int>(sl0), static_cast<int>(qlen - sr0), budget + 1, t);
         int sl = static_cast<int>(sl0), sr = static_cast<int>(sr0);
         if (nm > budget && clip_cap > 0) {
             // soft-clip retry, L1591-1694: grow sl to the first matching
             // in-contig base below clip_cap, sr likewise from the right
             int64_t lim = clen - local;
             if (lim > clip_cap) lim = clip_cap;
-            int j = first_match(ix.pacw, q, qn, bstart, sl, static_cast<int>(lim));
+            int j = first_match<S>(ix.pacw, q, qn, bstart, sl, static_cast<int>(lim), t);
             sl = j >= 0 ? j : clip_cap;
             int64_t jlo = sl > qlen - 1 - clip_cap ? sl : qlen - 1 - clip_cap;
             int64_t jhi = qlen - 1 - sr0;
             if (jhi > clen - local - 1) jhi = clen - local - 1;
-            int j2 = last_match(ix.pacw, q, qn, bstart, static_cast<int>(jlo + 1), static_cast<int>(jhi + 1));
+            int j2 = last_match<S>(ix.pacw, q, qn, bstart, static_cast<int>(jlo + 1), static_cast<int>(jhi + 1), t);
             if (j2 >= 0) {
                 sr = qlen - 1 - j2;
             } else {
                 int64_t sstar = sr0 > qlen - 1 - sl ? sr0 : qlen - 1 - sl;
                 sr = static_cast<int>(sstar < clip_cap ? sstar : clip_cap);
             }
-            nm = count_mm(ix.pacw, q, qn, bstart, sl, qlen - sr, budget + 1);
+            nm = count_mm<S>(ix.pacw, q, qn, bstart, sl, qlen - sr, budget + 1, t);
         }
         const int alen = qlen - sl - sr;
         if (nm <= budget && alen >= 24) {
@@ -249,7 +268,7 @@ __device__ void eval_locus(const DevIndex& ix, const ReadView& rd, int64_t b0, i
             }
         } else if (adj == 0 && is_rev == 0) {
             if (bstart + qlen + 1 <= coff + clen) {
-                deletion_scan(ix.pacw, q, qn, bstart, qlen, budget, [&](int g, int nmd) {
+                deletion_scan<S>(ix.pacw, q, qn, bstart, qlen, budget, t, [&](int g, int nmd) {
                     if (nmd > budget) return;
                     const uint64_t key = (static_cast<uint64_t>(nmd) << ORD_SHIFT) | (ord + 1 + g / 4);
                     if (key < best.key) {
@@ -278,7 +297,10 @@ struct Seed {
 };
 
 // Unique-SMEM left extension from right endpoint e (L1235-1385).
-__device__ __forceinline__ Seed search_endpoint(const DevIndex& ix, const ReadView& rd, int e, const DevParams& P) {
+template <bool S>
+__device__ __forceinline__ Seed search_endpoint(const DevIndex& ix, const ReadView& rd, int e, const DevParams& P,
+                                                Tally& t) {
+    if constexpr (S) t.endpoints++;
     uint64_t k = 0, l = ix.seq_len, last_k = 0, last_l = 0;
     int s = e, last_s = -1;
     Seed res{0, 0, -1, false};
@@ -293,6 +315,7 @@ __device__ __forceinline__ Seed search_endpoint(const DevIndex& ix, const ReadVi
             idx = (idx << 2) | static_cast<uint32_t>(c);
         }
         const uint2 kl = __ldg(ix.kmer + idx);
+        if constexpr (S) t.kmer_loads++;
         k = kl.x;
         l = kl.y;
         if (k > l) return res;
@@ -313,6 +336,12 @@ __device__ __forceinline__ Seed search_endpoint(const DevIndex& ix, const ReadVi
             const int cc = code_at(rd, s);
             if (cc > 3) break;
             uint64_t ok = 0;
+            if constexpr (S) {
+                t.steps++;
+                const int64_t lk = k != 0 ? static_cast<int64_t>((k - 1 - (k - 1 >= ix.primary)) >> 6) : -1;
+                const int64_t ll = l != ix.seq_len ? static_cast<int64_t>((l - (l >= ix.primary)) >> 6) : -2;
+                t.occ_lines += (lk >= 0) + (ll >= 0 && ll != lk);
+            }
             if (k != 0) ok = occ_row(ix, k - 1, cc);
             const uint64_t ol = occ_row(ix, l, cc);
             const uint64_t Lc = ix.L2[cc];
@@ -371,9 +400,12 @@ __global__ void __launch_bounds__(256) pack_reads_kernel(const uint8_t* __restri
     out[3 * words + w] = rn;
 }
 
-__global__ void __launch_bounds__(256) seed_extend_kernel(DevIndex ix, DevReads R, DevParams P, DevOut out) {
+template <bool S>
+__global__ void __launch_bounds__(256) seed_extend_kernel(DevIndex ix, DevReads R, DevParams P, DevOut out,
+                                                          unsigned long long* __restrict__ tally_out) {
     const int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (r >= R.n_seq) return;
+    Tally t{};
     const ReadView rd = read_view(R, r);
     const int qlen = rd.qlen;
     Best best;
@@ -398,12 +430,13 @@ __global__ void __launch_bounds__(256) seed_extend_kernel(DevIndex ix, DevReads 
         const int64_t l_pac = static_cast<int64_t>(ix.l_pac);
         int ei = 0;
         for (int e = P.seed_len - 1; e < qlen; e += P.seed_stride, ++ei) {
-            const Seed sd = search_endpoint(ix, rd, e, P);
+            const Seed sd = search_endpoint<S>(ix, rd, e, P, t);
             if (!sd.found) continue;
             const int us = sd.s;
             const int64_t plen = e - us + 1;
             for (uint64_t hi = sd.k; hi <= sd.l; ++hi) {
                 const uint64_t sa_pos = __ldg(ix.sa + hi);
+                if constexpr (S) t.sa_loads++;
                 if (sa_pos < ix.sa_reject_below) continue;
                 int64_t b0;
                 int is_rev;
@@ -426,7 +459,7 @@ __global__ void __launch_bounds__(256) seed_extend_kernel(DevIndex ix, DevReads 
                 memo_b0[memo_n % MEMO] = tag;
                 ++memo_n;
                 const uint32_t ord_row = (static_cast<uint32_t>(ei) * 16 + static_cast<uint32_t>(hi - sd.k)) * ADJ_SPAN;
-                eval_locus(ix, rd, b0, is_rev, adj_cap, budget, clip_cap, ord_row, best, sd.k, sd.l, us, e);
+                eval_locus<S>(ix, rd, b0, is_rev, adj_cap, budget, clip_cap, ord_row, best, sd.k, sd.l, us, e, t);
                 if ((best.key >> ORD_SHIFT) == 0) goto done;  // nm == 0 returns (L1708-1728)
             }
         }
@@ -457,6 +490,12 @@ done:
         out.ul[r] = best.ul;
         out.us[r] = best.us;
         out.e[r] = best.e;
+    }
+    if constexpr (S) {
+        const uint32_t v[8] = {t.occ_lines, t.kmer_loads, t.sa_loads, t.pac_sectors, t.steps, t.endpoints, t.loci,
+                               t.read_words};
+        for (int i = 0; i < 8; ++i)
+            if (v[i]) atomicAdd(tally_out + i, static_cast<unsigned long long>(v[i]));
     }
 }
 
@@ -492,6 +531,7 @@ __global__ void __launch_bounds__(256) mate_rescue_kernel(DevIndex ix, DevReads 
     if (budget > qlen / 2) budget = qlen / 2;
     const bool mate_rev = (out.flag[src] & 16) != 0;
     const int span = static_cast<int>(hi - lo + 1);
+    Tally tz{};
     uint32_t scan_key = 0xFFFFFFFFu, best_key = 0xFFFFFFFFu;
     for (int pass = 0; pass < 2; ++pass) {
         const int is_rev = pass == 0 ? (mate_rev ? 0 : 1) : (mate_rev ? 1 : 0);
@@ -500,7 +540,7 @@ __global__ void __launch_bounds__(256) mate_rescue_kernel(DevIndex ix, DevReads 
         for (int i = lane; i < span; i += 32) {
             const int64_t bstart = coff + lo + i;
             if (bstart < 0 || static_cast<uint64_t>(bstart + qlen) > ix.l_pac) continue;
-            const int nm = count_mm(ix.pacw, q, qn, bstart, 0, qlen, budget + 5);
+            const int nm = count_mm<false>(ix.pacw, q, qn, bstart, 0, qlen, budget + 5, tz);
             const uint32_t key = (static_cast<uint32_t>(nm) << 13) | (static_cast<uint32_t>(pass) << 12) |
                                  static_cast<uint32_t>(i);
             scan_key = key < scan_key ? key : scan_key;
@@ -528,7 +568,7 @@ __global__ void __launch_bounds__(256) mate_rescue_kernel(DevIndex ix, DevReads 
             const uint64_t* qn = scan_rev ? rd.nr : rd.nf;
             uint32_t dkey = 0xFFFFFFFFu;
             if (lane == 0) {
-                deletion_scan(ix.pacw, q, qn, bstart, qlen, budget, [&](int g, int nmd) {
+                deletion_scan<false>(ix.pacw, q, qn, bstart, qlen, budget, tz, [&](int g, int nmd) {
                     if (nmd > budget) return;
                     const uint32_t k2 = (static_cast<uint32_t>(nmd) << 13) | static_cast<uint32_t>(g / 4);
                     dkey = k2 < dkey ? k2 : dkey;
@@ -571,8 +611,11 @@ int launch_pack(const uint8_t* d_bases, const uint32_t* d_lens, int64_t n_seq, i
 }
 
 int launch_seed_extend(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
-                       cudaStream_t st) {
-    seed_extend_kernel<<<grid_for(R.n_seq, 128), 128, 0, st>>>(ix, R, P, out);
+                       unsigned long long* d_tally, cudaStream_t st) {
+    if (d_tally)
+        seed_extend_kernel<true><<<grid_for(R.n_seq, 128), 128, 0, st>>>(ix, R, P, out, d_tally);
+    else
+        seed_extend_kernel<false><<<grid_for(R.n_seq, 128), 128, 0, st>>>(ix, R, P, out, nullptr);
     return 1;
 }
 

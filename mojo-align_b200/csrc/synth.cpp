@@ -7,6 +7,7 @@
 #include <cstring>
 #include <random>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "ma_internal.h"
@@ -175,10 +176,18 @@ extern "C" int ma_synth_reads_impl(const char* fasta, const ma_read_model* m, ui
             tot += r.seq.size();
             seqs.push_back(std::move(r.seq));
         }
-        Rng rng(seed);
         const uint64_t n_seq = paired ? 2ull * n1 : n1;
         std::memset(bases, 'N', n_seq * max_len);
-        for (uint32_t i = 0; i < n1; ++i) {
+        // 16 fixed chunks, each with its own generator: the output depends on
+        // the seed only, not on how many host threads run the chunks.
+        constexpr uint32_t kChunks = 16;
+        std::vector<std::string> errors(kChunks);
+        auto work = [&](uint32_t chunk) {
+          try {
+            Rng rng(seed * 1000003ull + chunk);
+            const uint32_t i0 = static_cast<uint32_t>(static_cast<uint64_t>(n1) * chunk / kChunks);
+            const uint32_t i1 = static_cast<uint32_t>(static_cast<uint64_t>(n1) * (chunk + 1) / kChunks);
+        for (uint32_t i = i0; i < i1; ++i) {
             uint32_t l1 = draw_len(m, rng), l2 = paired ? draw_len(m, rng) : 0;
             if (l1 > max_len) l1 = max_len;
             if (l2 > max_len) l2 = max_len;
@@ -245,6 +254,15 @@ extern "C" int ma_synth_reads_impl(const char* fasta, const ma_read_model* m, ui
                 if (truth_rev) truth_rev[j] = tr2;
             }
         }
+          } catch (const std::exception& ex) {
+            errors[chunk] = ex.what();
+          }
+        };
+        std::vector<std::thread> pool;
+        for (uint32_t c = 0; c < kChunks; ++c) pool.emplace_back(work, c);
+        for (auto& t : pool) t.join();
+        for (const auto& m : errors)
+            if (!m.empty()) fail(MA_ERR_ARG, m);
         return MA_OK;
     } catch (const Error& e) {
         std::snprintf(err, err_cap, "%s", e.what());

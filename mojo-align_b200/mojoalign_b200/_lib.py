@@ -130,6 +130,10 @@ SIGNATURES = [
      [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_uint32, C.c_int, C.c_int,
       C.POINTER(ma_params), C.POINTER(ma_hits), C.POINTER(ma_debug), C.c_void_p]),
     ("ma_last_launch_count", C.c_int, [C.c_void_p]),
+    ("ma_ctx_set_profiling", C.c_int, [C.c_void_p, C.c_int]),
+    ("ma_ctx_kernel_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    ("ma_ctx_traffic", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    ("ma_bench_gather", C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_uint64, C.POINTER(C.c_double)]),
     ("ma_synth_reference", C.c_int, [C.c_char_p, C.c_uint64, C.c_int, C.c_double, C.c_double, C.c_uint64]),
     ("ma_synth_reads", C.c_int,
      [C.c_char_p, C.POINTER(ma_read_model), C.c_uint32, C.c_int, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p,
