@@ -194,6 +194,26 @@ int ma_map_batch_device(ma_ctx* ctx, const ma_index* idx,
 /* Number of kernel launches the last mapping call on ctx issued. */
 int ma_last_launch_count(const ma_ctx* ctx);
 
+/*
+ * Result-neutral execution choices (every setting gives identical outputs).
+ *   seed_kernel           0: one thread per read over all right endpoints
+ *                         (the reference's launch shape, L2336-2382);
+ *                         1: two stages (default): one thread per read over
+ *                         the first stage1_endpoints endpoints, then one
+ *                         warp per remaining read in a persistent kernel
+ *                         fed by a work queue.
+ *   stage1_endpoints      endpoints stage 1 covers (default 1).
+ *   stage2_blocks_per_sm  persistent blocks per SM for stage 2 (0 = the
+ *                         occupancy maximum).
+ */
+typedef struct ma_tuning {
+    int32_t seed_kernel;
+    int32_t stage1_endpoints;
+    int32_t stage2_blocks_per_sm;
+} ma_tuning;
+int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t);
+int ma_ctx_get_tuning(const ma_ctx* ctx, ma_tuning* t);
+
 /* ---- measurement (no reference counterpart; the reference only prints
  * perf_counter stage timers, linear_gpu_fm.mojo:2270-2273,3317-3340) ---- */
 

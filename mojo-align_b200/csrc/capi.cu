@@ -18,6 +18,11 @@ int launch_pack(const uint8_t* d_bases, const uint32_t* d_lens, int64_t n_seq, i
 int launch_seed_extend(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
                        unsigned long long* d_tally, cudaStream_t st);
 double run_gather_bench(uint64_t buffer_bytes, int line_bytes, uint64_t n_loads, int sm_count, cudaStream_t st);
+size_t two_stage_scratch_bytes(int64_t n_seq);
+int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
+                          int stage1_endpoints, int stage2_blocks, void* scratch, unsigned long long* d_tally,
+                          cudaStream_t st);
+int stage2_blocks_per_sm();
 int launch_rescue(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int64_t n_pairs,
                   cudaStream_t st);
 }  // namespace ma
@@ -70,6 +75,9 @@ struct ma_ctx {
     uint64_t traffic[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     bool rescue_ran = false;
     DevBuf tally;
+    ma_tuning tuning{1, 1, 0};
+    int sm_count = 0;
+    DevBuf seed_scratch;
     DevBuf bases, lens, packed, err_flag;
     DevBuf o_rid, o_pos, o_mapq, o_flag, o_sl, o_sr, o_nm;
     DevBuf d_uk, d_ul, d_us, d_e, d_score;
@@ -150,7 +158,14 @@ void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const
     if (timed) ck(cudaEventRecord(ctx->ev[1], st), "event");
     DevReads R{ctx->packed.as<uint64_t>(), d_lens, words, n_seq};
     DevParams P = to_dev(p);
-    launches += launch_seed_extend(idx->dix, R, P, out, d_tally, st);
+    if (ctx->tuning.seed_kernel == 0) {
+        launches += launch_seed_extend(idx->dix, R, P, out, d_tally, st);
+    } else {
+        ctx->seed_scratch.ensure(two_stage_scratch_bytes(n_seq));
+        const int bps = ctx->tuning.stage2_blocks_per_sm > 0 ? ctx->tuning.stage2_blocks_per_sm : stage2_blocks_per_sm();
+        launches += launch_seed_two_stage(idx->dix, R, P, out, ctx->tuning.stage1_endpoints, bps * ctx->sm_count,
+                                          ctx->seed_scratch.p, d_tally, st);
+    }
     if (timed) ck(cudaEventRecord(ctx->ev[2], st), "event");
     ctx->rescue_ran = paired && p->rescue_win > 0;
     if (ctx->rescue_ran) launches += launch_rescue(idx->dix, R, P, out, n1, st);
@@ -210,6 +225,7 @@ int ma_ctx_create(int device_ordinal, ma_ctx** out) {
         ctx->device = device_ordinal;
         ck(cudaSetDevice(device_ordinal), "cudaSetDevice");
         ck(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ctx->sm_count = prop.multiProcessorCount;
     });
     if (rc != MA_OK) {
         delete ctx;
@@ -225,6 +241,7 @@ void ma_ctx_destroy(ma_ctx* ctx) {
     for (cudaEvent_t& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     ctx->tally.release();
+    ctx->seed_scratch.release();
     for (DevBuf* b : {&ctx->bases, &ctx->lens, &ctx->packed, &ctx->err_flag, &ctx->o_rid, &ctx->o_pos, &ctx->o_mapq,
                       &ctx->o_flag, &ctx->o_sl, &ctx->o_sr, &ctx->o_nm, &ctx->d_uk, &ctx->d_ul, &ctx->d_us,
                       &ctx->d_e, &ctx->d_score})
@@ -416,6 +433,22 @@ int ma_ctx_set_profiling(ma_ctx* ctx, int flags) {
             for (cudaEvent_t& e : ctx->ev) ck(cudaEventCreate(&e), "cudaEventCreate");
         ctx->profiling = flags;
     });
+}
+
+int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t) {
+    if (!ctx || !t) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (t->seed_kernel < 0 || t->seed_kernel > 1) fail(MA_ERR_ARG, "seed_kernel must be 0 or 1");
+        if (t->stage1_endpoints < 1) fail(MA_ERR_ARG, "stage1_endpoints must be >= 1");
+        if (t->stage2_blocks_per_sm < 0 || t->stage2_blocks_per_sm > 64) fail(MA_ERR_ARG, "bad stage2_blocks_per_sm");
+        ctx->tuning = *t;
+    });
+}
+
+int ma_ctx_get_tuning(const ma_ctx* ctx, ma_tuning* t) {
+    if (!ctx || !t) return MA_ERR_ARG;
+    *t = ctx->tuning;
+    return MA_OK;
 }
 
 int ma_ctx_kernel_ms(const ma_ctx* ctx, float* out3) {

@@ -71,10 +71,11 @@ __device__ __forceinline__ ReadView read_view(const DevReads& R, int64_t r) {
     return v;
 }
 
+// Read words may live in global or shared memory (generic loads).
 __device__ __forceinline__ int code_at(const ReadView& v, int s) {
     int w = s >> 5, sh = 2 * (s & 31);
-    if ((__ldg(v.nf + w) >> sh) & 1) return 4;
-    return static_cast<int>((__ldg(v.fwd + w) >> sh) & 3);
+    if ((v.nf[w] >> sh) & 1) return 4;
+    return static_cast<int>((v.fwd[w] >> sh) & 3);
 }
 
 // Per-thread traffic tally of the counting kernel variant (S = true).  The
@@ -95,8 +96,8 @@ __device__ __forceinline__ uint64_t mm_word(const uint64_t* __restrict__ pacw, c
         t.pac_sectors += ((wi * 8) >> 5) == ((wi * 8 + 15) >> 5) ? 1 : 2;
         t.read_words += 2;
     }
-    uint64_t x = __ldg(q + w) ^ ref_window(pacw, bstart + 32 * w);
-    return ((x | (x >> 1)) & kEven) | __ldg(qn + w);
+    uint64_t x = q[w] ^ ref_window(pacw, bstart + 32 * w);
+    return ((x | (x >> 1)) & kEven) | qn[w];
 }
 
 // min(mismatches over read positions [a, b), cap): the reference's counting
@@ -149,6 +150,16 @@ struct Best {
 };
 
 constexpr int ORD_SHIFT = 27;
+constexpr int MEMO1 = 8;  // loci handed from stage 1 to stage 2 per read
+
+// State of reads that stage 1 hands to stage 2 (scratch, sized n_seq).
+struct Handoff {
+    uint64_t* key;       // running best key
+    uint64_t* memo;      // [n_seq][MEMO1] loci already evaluated (b0*2+strand)
+    uint8_t* memo_n;     // entries used in memo
+    uint32_t* pending;   // read ids handed over
+    uint32_t* counters;  // [0] pending count, [1] stage-2 work cursor
+};
 constexpr uint32_t KIND_SPAN = 260;  // full compare + up to 257 deletion offsets
 constexpr uint32_t ADJ_SPAN = 25;    // 2*12+1 shifts
 
@@ -206,88 +217,96 @@ __device__ __forceinline__ void deletion_scan(const uint64_t* __restrict__ pacw,
     }
 }
 
-// Evaluates every shift adj of one locus (b0, strand): the body of the
-// reference's adj loop, L1526-1826.
+// One shift adj of one locus (b0, strand): the body of the reference's adj
+// loop, linear_gpu_fm.mojo:1528-1826.  Folds the candidate (full compare,
+// or the deletion probe's offsets) into `best` by its (nm, ordinal) key.
+template <bool S>
+__device__ void eval_adj(const DevIndex& ix, const ReadView& rd, int64_t b0, int is_rev, int adj, int budget,
+                         int clip_cap, uint32_t ord_row, Best& best, uint64_t uk, uint64_t ul, int us, int e,
+                         Tally& t) {
+    const int qlen = rd.qlen;
+    const uint64_t* q = is_rev ? rd.rc : rd.fwd;
+    const uint64_t* qn = is_rev ? rd.nr : rd.nf;
+    const int64_t bstart = b0 + adj;
+    int64_t probe = bstart < 0 ? 0 : bstart;
+    if (probe >= static_cast<int64_t>(ix.l_pac)) probe = static_cast<int64_t>(ix.l_pac) - 1;
+    const int64_t crid = contig_of(ix, probe);
+    if (crid < 0) return;
+    const int64_t coff = static_cast<int64_t>(__ldg(ix.coff + crid));
+    const int64_t clen = static_cast<int64_t>(__ldg(ix.clen + crid));
+    const int64_t local = bstart - coff;
+    const int64_t sl0 = local < 0 ? -local : 0;
+    const int64_t sr0 = local + qlen > clen ? local + qlen - clen : 0;
+    if (!(sl0 + sr0 < qlen && sl0 <= clip_cap && sr0 <= clip_cap)) return;
+    const uint32_t ord = (ord_row + static_cast<uint32_t>(adj + 12)) * KIND_SPAN;
+    int nm = count_mm<S>(ix.pacw, q, qn, bstart, static_cast<int>(sl0), static_cast<int>(qlen - sr0), budget + 1, t);
+    int sl = static_cast<int>(sl0), sr = static_cast<int>(sr0);
+    if (nm > budget && clip_cap > 0) {
+        // soft-clip retry, L1591-1694: grow sl to the first matching
+        // in-contig base below clip_cap, sr likewise from the right
+        int64_t lim = clen - local;
+        if (lim > clip_cap) lim = clip_cap;
+        int j = first_match<S>(ix.pacw, q, qn, bstart, sl, static_cast<int>(lim), t);
+        sl = j >= 0 ? j : clip_cap;
+        int64_t jlo = sl > qlen - 1 - clip_cap ? sl : qlen - 1 - clip_cap;
+        int64_t jhi = qlen - 1 - sr0;
+        if (jhi > clen - local - 1) jhi = clen - local - 1;
+        int j2 = last_match<S>(ix.pacw, q, qn, bstart, static_cast<int>(jlo + 1), static_cast<int>(jhi + 1), t);
+        if (j2 >= 0) {
+            sr = qlen - 1 - j2;
+        } else {
+            int64_t sstar = sr0 > qlen - 1 - sl ? sr0 : qlen - 1 - sl;
+            sr = static_cast<int>(sstar < clip_cap ? sstar : clip_cap);
+        }
+        nm = count_mm<S>(ix.pacw, q, qn, bstart, sl, qlen - sr, budget + 1, t);
+    }
+    const int alen = qlen - sl - sr;
+    if (nm <= budget && alen >= 24) {
+        const uint64_t key = (static_cast<uint64_t>(nm) << ORD_SHIFT) | ord;
+        if (key < best.key) {
+            best.key = key;
+            best.crid = static_cast<int32_t>(crid);
+            best.pos = static_cast<uint32_t>(local + sl);
+            best.sl = sl;
+            best.sr = sr;
+            best.mapq = nm == 0 ? 60u : 20u;
+            best.flag = is_rev * 16;
+            best.uk = uk;
+            best.ul = ul;
+            best.us = us;
+            best.e = e;
+        }
+    } else if (adj == 0 && is_rev == 0) {
+        if (bstart + qlen + 1 <= coff + clen) {
+            deletion_scan<S>(ix.pacw, q, qn, bstart, qlen, budget, t, [&](int g, int nmd) {
+                if (nmd > budget) return;
+                const uint64_t key = (static_cast<uint64_t>(nmd) << ORD_SHIFT) | (ord + 1 + g / 4);
+                if (key < best.key) {
+                    best.key = key;
+                    best.crid = static_cast<int32_t>(crid);
+                    best.pos = static_cast<uint32_t>(local);
+                    best.sl = 0;
+                    best.sr = 0;
+                    best.mapq = 20u;
+                    best.flag = 0;
+                    best.uk = uk;
+                    best.ul = ul;
+                    best.us = us;
+                    best.e = e;
+                }
+            });
+        }
+    }
+}
+
+// Every shift of one locus, in adj order (L1526-1827).
 template <bool S>
 __device__ void eval_locus(const DevIndex& ix, const ReadView& rd, int64_t b0, int is_rev, int adj_cap,
                            int budget, int clip_cap, uint32_t ord_row, Best& best, uint64_t uk, uint64_t ul,
                            int us, int e, Tally& t) {
     if constexpr (S) t.loci++;
-    const int qlen = rd.qlen;
-    const uint64_t* q = is_rev ? rd.rc : rd.fwd;
-    const uint64_t* qn = is_rev ? rd.nr : rd.nf;
-    for (int adj = -adj_cap; adj <= adj_cap; ++adj) {
-        const int64_t bstart = b0 + adj;
-        int64_t probe = bstart < 0 ? 0 : bstart;
-        if (probe >= static_cast<int64_t>(ix.l_pac)) probe = static_cast<int64_t>(ix.l_pac) - 1;
-        const int64_t crid = contig_of(ix, probe);
-        if (crid < 0) continue;
-        const int64_t coff = static_cast<int64_t>(__ldg(ix.coff + crid));
-        const int64_t clen = static_cast<int64_t>(__ldg(ix.clen + crid));
-        const int64_t local = bstart - coff;
-        const int64_t sl0 = local < 0 ? -local : 0;
-        const int64_t sr0 = local + qlen > clen ? local + qlen - clen : 0;
-        if (!(sl0 + sr0 < qlen && sl0 <= clip_cap && sr0 <= clip_cap)) continue;
-        const uint32_t ord = (ord_row + static_cast<uint32_t>(adj + 12)) * KIND_SPAN;
-        int nm = count_mm<S>(ix.pacw, q, qn, bstart, static_cast<int>(sl0), static_cast<int>(qlen - sr0), budget + 1, t);
-        int sl = static_cast<int>(sl0), sr = static_cast<int>(sr0);
-        if (nm > budget && clip_cap > 0) {
-            // soft-clip retry, L1591-1694: grow sl to the first matching
-            // in-contig base below clip_cap, sr likewise from the right
-            int64_t lim = clen - local;
-            if (lim > clip_cap) lim = clip_cap;
-            int j = first_match<S>(ix.pacw, q, qn, bstart, sl, static_cast<int>(lim), t);
-            sl = j >= 0 ? j : clip_cap;
-            int64_t jlo = sl > qlen - 1 - clip_cap ? sl : qlen - 1 - clip_cap;
-            int64_t jhi = qlen - 1 - sr0;
-            if (jhi > clen - local - 1) jhi = clen - local - 1;
-            int j2 = last_match<S>(ix.pacw, q, qn, bstart, static_cast<int>(jlo + 1), static_cast<int>(jhi + 1), t);
-            if (j2 >= 0) {
-                sr = qlen - 1 - j2;
-            } else {
-                int64_t sstar = sr0 > qlen - 1 - sl ? sr0 : qlen - 1 - sl;
-                sr = static_cast<int>(sstar < clip_cap ? sstar : clip_cap);
-            }
-            nm = count_mm<S>(ix.pacw, q, qn, bstart, sl, qlen - sr, budget + 1, t);
-        }
-        const int alen = qlen - sl - sr;
-        if (nm <= budget && alen >= 24) {
-            const uint64_t key = (static_cast<uint64_t>(nm) << ORD_SHIFT) | ord;
-            if (key < best.key) {
-                best.key = key;
-                best.crid = static_cast<int32_t>(crid);
-                best.pos = static_cast<uint32_t>(local + sl);
-                best.sl = sl;
-                best.sr = sr;
-                best.mapq = nm == 0 ? 60u : 20u;
-                best.flag = is_rev * 16;
-                best.uk = uk;
-                best.ul = ul;
-                best.us = us;
-                best.e = e;
-            }
-        } else if (adj == 0 && is_rev == 0) {
-            if (bstart + qlen + 1 <= coff + clen) {
-                deletion_scan<S>(ix.pacw, q, qn, bstart, qlen, budget, t, [&](int g, int nmd) {
-                    if (nmd > budget) return;
-                    const uint64_t key = (static_cast<uint64_t>(nmd) << ORD_SHIFT) | (ord + 1 + g / 4);
-                    if (key < best.key) {
-                        best.key = key;
-                        best.crid = static_cast<int32_t>(crid);
-                        best.pos = static_cast<uint32_t>(local);
-                        best.sl = 0;
-                        best.sr = 0;
-                        best.mapq = 20u;
-                        best.flag = 0;
-                        best.uk = uk;
-                        best.ul = ul;
-                        best.us = us;
-                        best.e = e;
-                    }
-                });
-            }
-        }
-    }
+    for (int adj = -adj_cap; adj <= adj_cap; ++adj)
+        eval_adj<S>(ix, rd, b0, is_rev, adj, budget, clip_cap, ord_row, best, uk, ul, us, e, t);
 }
 
 struct Seed {
@@ -400,8 +419,93 @@ __global__ void __launch_bounds__(256) pack_reads_kernel(const uint8_t* __restri
     out[3 * words + w] = rn;
 }
 
+// Per-read clamps of linear_gpu_fm.mojo:1204-1216.
+struct Clamps {
+    int budget, clip_cap, adj_cap;
+};
+
+__device__ __forceinline__ Clamps clamps_for(const DevParams& P, int qlen) {
+    Clamps c;
+    c.budget = P.max_diff;
+    if (c.budget < 2) c.budget = 2;
+    if (c.budget > qlen / 2) c.budget = qlen / 2;
+    c.clip_cap = P.max_soft;
+    if (c.clip_cap > qlen / 4) c.clip_cap = qlen / 4;
+    c.adj_cap = P.max_adj;
+    if (c.adj_cap < 0) c.adj_cap = 0;
+    if (c.adj_cap > 12) c.adj_cap = 12;
+    return c;
+}
+
+// Number of right endpoints e = seed_len-1 + j*stride below qlen.
+__device__ __forceinline__ int endpoint_count(const DevParams& P, int qlen) {
+    return qlen >= P.seed_len ? (qlen - P.seed_len) / P.seed_stride + 1 : 0;
+}
+
+// SA row -> candidate locus (b0, strand) of L1503-1524; false = rejected.
+__device__ __forceinline__ bool locus_of_row(const DevIndex& ix, uint64_t sa_pos, int us, int e, int qlen,
+                                             int64_t& b0, int& is_rev) {
+    if (sa_pos < ix.sa_reject_below) return false;  // the sampled walk would hit the first row
+    const int64_t plen = e - us + 1;
+    if (sa_pos < ix.l_pac) {
+        b0 = static_cast<int64_t>(sa_pos) - us;
+        is_rev = 0;
+        return true;
+    }
+    if (sa_pos + static_cast<uint64_t>(plen) - 1 >= 2 * ix.l_pac) return false;
+    const int64_t fp_end = 2 * static_cast<int64_t>(ix.l_pac) - 1 - static_cast<int64_t>(sa_pos);
+    const int64_t fp_start = fp_end - (plen - 1);
+    b0 = fp_start - (qlen - 1 - e);
+    is_rev = 1;
+    return true;
+}
+
+__device__ __forceinline__ void write_hit(const DevOut& out, int64_t r, const Best& b, int qlen) {
+    if (b.crid >= 0) {
+        const int nm = static_cast<int>(b.key >> ORD_SHIFT);
+        out.rid[r] = b.crid;
+        out.pos[r] = b.pos;
+        out.mapq[r] = b.mapq;
+        out.flag[r] = b.flag;
+        out.sl[r] = static_cast<uint32_t>(b.sl);
+        out.sr[r] = static_cast<uint32_t>(b.sr);
+        out.nm[r] = static_cast<uint32_t>(nm);
+        if (out.score) out.score[r] = qlen - b.sl - b.sr - 5 * nm;
+    } else {  // defaults of L1194-1200
+        out.rid[r] = -1;
+        out.pos[r] = 0;
+        out.mapq[r] = 0;
+        out.flag[r] = 4;
+        out.sl[r] = 0;
+        out.sr[r] = 0;
+        out.nm[r] = 0;
+        if (out.score) out.score[r] = 0;
+    }
+    if (out.us) {
+        out.uk[r] = b.uk;
+        out.ul[r] = b.ul;
+        out.us[r] = b.us;
+        out.e[r] = b.e;
+    }
+}
+
 template <bool S>
-__global__ void __launch_bounds__(256) seed_extend_kernel(DevIndex ix, DevReads R, DevParams P, DevOut out,
+__device__ __forceinline__ void flush_tally(const Tally& t, unsigned long long* tally_out) {
+    if constexpr (S) {
+        const uint32_t v[8] = {t.occ_lines, t.kmer_loads, t.sa_loads, t.pac_sectors, t.steps, t.endpoints, t.loci,
+                               t.read_words};
+        for (int i = 0; i < 8; ++i)
+            if (v[i]) atomicAdd(tally_out + i, static_cast<unsigned long long>(v[i]));
+    }
+}
+
+// Stage 1: one thread per read, right endpoints [0, ep_limit).  A read
+// whose best hit is not nm == 0 and that has endpoints left is handed to
+// stage 2 with its running best and the loci it evaluated.  With
+// ep_limit >= every read's endpoint count this is the whole algorithm.
+template <bool S>
+__global__ void __launch_bounds__(128) seed_stage1_kernel(DevIndex ix, DevReads R, DevParams P, DevOut out,
+                                                          int ep_limit, Handoff h,
                                                           unsigned long long* __restrict__ tally_out) {
     const int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (r >= R.n_seq) return;
@@ -414,42 +518,23 @@ __global__ void __launch_bounds__(256) seed_extend_kernel(DevIndex ix, DevReads 
     best.us = -1;
     best.e = -1;
     best.uk = best.ul = 0;
-    if (qlen >= P.seed_len) {
-        // clamps of L1204-1216
-        int budget = P.max_diff;
-        if (budget < 2) budget = 2;
-        if (budget > qlen / 2) budget = qlen / 2;
-        int clip_cap = P.max_soft;
-        if (clip_cap > qlen / 4) clip_cap = qlen / 4;
-        int adj_cap = P.max_adj;
-        if (adj_cap < 0) adj_cap = 0;
-        if (adj_cap > 12) adj_cap = 12;
-        constexpr int MEMO = 16;
-        int64_t memo_b0[MEMO];
-        int memo_n = 0;
-        const int64_t l_pac = static_cast<int64_t>(ix.l_pac);
-        int ei = 0;
-        for (int e = P.seed_len - 1; e < qlen; e += P.seed_stride, ++ei) {
+    constexpr int MEMO = 16;
+    int64_t memo_b0[MEMO];
+    int memo_n = 0;
+    const int n_end = endpoint_count(P, qlen);
+    const int n_run = n_end < ep_limit ? n_end : ep_limit;
+    if (n_run > 0) {
+        const Clamps cl = clamps_for(P, qlen);
+        for (int ei = 0; ei < n_run; ++ei) {
+            const int e = P.seed_len - 1 + ei * P.seed_stride;
             const Seed sd = search_endpoint<S>(ix, rd, e, P, t);
             if (!sd.found) continue;
-            const int us = sd.s;
-            const int64_t plen = e - us + 1;
             for (uint64_t hi = sd.k; hi <= sd.l; ++hi) {
                 const uint64_t sa_pos = __ldg(ix.sa + hi);
                 if constexpr (S) t.sa_loads++;
-                if (sa_pos < ix.sa_reject_below) continue;
                 int64_t b0;
                 int is_rev;
-                if (sa_pos < ix.l_pac) {  // L1509-1524
-                    b0 = static_cast<int64_t>(sa_pos) - us;
-                    is_rev = 0;
-                } else {
-                    if (sa_pos + static_cast<uint64_t>(plen) - 1 >= 2 * ix.l_pac) continue;
-                    const int64_t fp_end = 2 * l_pac - 1 - static_cast<int64_t>(sa_pos);
-                    const int64_t fp_start = fp_end - (plen - 1);
-                    b0 = fp_start - (qlen - 1 - e);
-                    is_rev = 1;
-                }
+                if (!locus_of_row(ix, sa_pos, sd.s, e, qlen, b0, is_rev)) continue;
                 // shortcut 1: a locus already evaluated cannot win again
                 const int64_t tag = b0 * 2 + is_rev;
                 bool seen = false;
@@ -459,44 +544,201 @@ __global__ void __launch_bounds__(256) seed_extend_kernel(DevIndex ix, DevReads 
                 memo_b0[memo_n % MEMO] = tag;
                 ++memo_n;
                 const uint32_t ord_row = (static_cast<uint32_t>(ei) * 16 + static_cast<uint32_t>(hi - sd.k)) * ADJ_SPAN;
-                eval_locus<S>(ix, rd, b0, is_rev, adj_cap, budget, clip_cap, ord_row, best, sd.k, sd.l, us, e, t);
+                eval_locus<S>(ix, rd, b0, is_rev, cl.adj_cap, cl.budget, cl.clip_cap, ord_row, best, sd.k, sd.l,
+                              sd.s, e, t);
                 if ((best.key >> ORD_SHIFT) == 0) goto done;  // nm == 0 returns (L1708-1728)
             }
         }
     }
 done:
-    if (best.crid >= 0) {
-        const int nm = static_cast<int>(best.key >> ORD_SHIFT);
-        out.rid[r] = best.crid;
-        out.pos[r] = best.pos;
-        out.mapq[r] = best.mapq;
-        out.flag[r] = best.flag;
-        out.sl[r] = static_cast<uint32_t>(best.sl);
-        out.sr[r] = static_cast<uint32_t>(best.sr);
-        out.nm[r] = static_cast<uint32_t>(nm);
-        if (out.score) out.score[r] = qlen - best.sl - best.sr - 5 * nm;
-    } else {
-        out.rid[r] = -1;
-        out.pos[r] = 0;
-        out.mapq[r] = 0;
-        out.flag[r] = 4;
-        out.sl[r] = 0;
-        out.sr[r] = 0;
-        out.nm[r] = 0;
-        if (out.score) out.score[r] = 0;
+    write_hit(out, r, best, qlen);
+    {
+        const bool pend = h.pending && (best.key >> ORD_SHIFT) != 0 && n_end > n_run;
+        if (pend) {
+            h.key[r] = best.key;
+            const int mn = memo_n < MEMO1 ? memo_n : MEMO1;
+            for (int i = 0; i < mn; ++i) h.memo[r * MEMO1 + i] = static_cast<uint64_t>(memo_b0[i]);
+            h.memo_n[r] = static_cast<uint8_t>(mn);
+        }
+        const unsigned m = __activemask();
+        const unsigned b = __ballot_sync(m, pend);
+        if (b) {
+            const int lane = threadIdx.x & 31;
+            const int leader = __ffs(b) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(h.counters, static_cast<uint32_t>(__popc(b)));
+            base = __shfl_sync(m, base, leader);
+            if (pend) h.pending[base + __popc(b & ((1u << lane) - 1))] = static_cast<uint32_t>(r);
+        }
     }
-    if (out.us) {
-        out.uk[r] = best.uk;
-        out.ul[r] = best.ul;
-        out.us[r] = best.us;
-        out.e[r] = best.e;
+    flush_tally<S>(t, tally_out);
+}
+
+// A locus staged for the warp's shift evaluations.
+struct Locus {
+    int64_t b0;
+    uint64_t uk, ul;
+    uint32_t ord_row;
+    int32_t us, e, rev;
+};
+
+constexpr int S2_WARPS = 8;   // warps per block of the stage-2 kernel
+constexpr int MEMO2 = 64;     // loci remembered per read in stage 2
+
+__device__ __forceinline__ uint64_t warp_min64(uint64_t v) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const uint64_t w = __shfl_xor_sync(0xFFFFFFFFu, v, o);
+        v = w < v ? w : v;
     }
-    if constexpr (S) {
-        const uint32_t v[8] = {t.occ_lines, t.kmer_loads, t.sa_loads, t.pac_sectors, t.steps, t.endpoints, t.loci,
-                               t.read_words};
-        for (int i = 0; i < 8; ++i)
-            if (v[i]) atomicAdd(tally_out + i, static_cast<unsigned long long>(v[i]));
+    return v;
+}
+
+// Stage 2: one warp per pending read, persistent over the pending list.
+// Lanes search 32 right endpoints at a time; the candidate rows of those
+// endpoints, in the reference's order (endpoint, then row), are resolved
+// 32 at a time, de-duplicated (within the group by __match_any_sync,
+// against earlier groups and stage 1 through the memo), and every (locus,
+// shift) pair is evaluated by one lane.  The warp minimum of the (nm,
+// ordinal) keys is folded into the read's running best.  The read stops
+// after the group of endpoints in which an nm == 0 hit appears.
+template <bool S>
+__global__ void __launch_bounds__(S2_WARPS * 32) seed_stage2_kernel(DevIndex ix, DevReads R, DevParams P,
+                                                                    DevOut out, int ep_start, Handoff h,
+                                                                    unsigned long long* __restrict__ tally_out) {
+    __shared__ uint64_t s_words_all[S2_WARPS][4 * MAX_WORDS];
+    __shared__ uint64_t s_memo_all[S2_WARPS][MEMO2];
+    __shared__ Locus s_loci_all[S2_WARPS][32];
+    constexpr unsigned FULL = 0xFFFFFFFFu;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint64_t* s_words = s_words_all[warp];
+    uint64_t* s_memo = s_memo_all[warp];
+    Locus* s_loci = s_loci_all[warp];
+    Tally t{};
+    const uint32_t n_pending = *reinterpret_cast<volatile uint32_t*>(h.counters);
+    for (;;) {
+        uint32_t qi = 0;
+        if (lane == 0) qi = atomicAdd(h.counters + 1, 1u);
+        qi = __shfl_sync(FULL, qi, 0);
+        if (qi >= n_pending) break;
+        const int64_t r = h.pending[qi];
+        const int words = R.words;
+        const uint64_t* g = R.packed + r * 4 * static_cast<int64_t>(words);
+        for (int i = lane; i < 4 * words; i += 32) s_words[i] = g[i];
+        const int qlen = static_cast<int>(R.lens[r]);
+        int n_memo = h.memo_n[r];
+        for (int i = lane; i < n_memo; i += 32) s_memo[i] = h.memo[r * MEMO1 + i];
+        __syncwarp();
+        ReadView rd;
+        rd.fwd = s_words;
+        rd.rc = s_words + words;
+        rd.nf = s_words + 2 * words;
+        rd.nr = s_words + 3 * words;
+        rd.qlen = qlen;
+        const Clamps cl = clamps_for(P, qlen);
+        const int A = 2 * cl.adj_cap + 1;
+        const int n_end = endpoint_count(P, qlen);
+        uint64_t best_key = h.key[r];
+        Best win;  // valid when improved
+        win.crid = -1;
+        bool improved = false;
+        for (int j0 = ep_start; j0 < n_end; j0 += 32) {
+            const int j = j0 + lane;
+            const int e = P.seed_len - 1 + j * P.seed_stride;
+            Seed sd{0, 0, -1, false};
+            if (j < n_end) sd = search_endpoint<S>(ix, rd, e, P, t);
+            const int nrows = sd.found ? static_cast<int>(sd.l - sd.k + 1) : 0;
+            int incl = nrows;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int total = __shfl_sync(FULL, incl, 31);
+            for (int c0 = 0; c0 < total; c0 += 32) {
+                const int idx = c0 + lane;
+                int owner = 0;  // lanes whose rows end at or before idx
+                for (int step = 16; step >= 1; step >>= 1) {
+                    const int v = __shfl_sync(FULL, incl, owner + step - 1);
+                    if (v <= idx) owner += step;
+                }
+                const int own = owner < 32 ? owner : 31;
+                const uint64_t o_k = __shfl_sync(FULL, sd.k, own);
+                const uint64_t o_l = __shfl_sync(FULL, sd.l, own);
+                const int o_s = __shfl_sync(FULL, sd.s, own);
+                const int o_first = __shfl_sync(FULL, incl - nrows, own);
+                const bool valid = idx < total;
+                const int o_e = P.seed_len - 1 + (j0 + own) * P.seed_stride;
+                const uint64_t hi = o_k + static_cast<uint64_t>(idx - o_first);
+                uint64_t tag = 0x8000000000000000ull | static_cast<uint64_t>(lane);
+                int64_t b0 = 0;
+                int rev = 0;
+                bool ok = false;
+                if (valid) {
+                    const uint64_t sa_pos = __ldg(ix.sa + hi);
+                    if constexpr (S) t.sa_loads++;
+                    ok = locus_of_row(ix, sa_pos, o_s, o_e, qlen, b0, rev);
+                    if (ok) tag = static_cast<uint64_t>(b0 * 2 + rev);
+                }
+                const unsigned peers = __match_any_sync(FULL, tag);
+                bool keep = ok && (__ffs(peers) - 1) == lane;
+                if (keep)
+                    for (int m = 0; m < n_memo; ++m)
+                        if (s_memo[m] == tag) {
+                            keep = false;
+                            break;
+                        }
+                const unsigned kb = __ballot_sync(FULL, keep);
+                const int rank = __popc(kb & ((1u << lane) - 1));
+                if (keep) {
+                    if (n_memo + rank < MEMO2) s_memo[n_memo + rank] = tag;
+                    Locus L;
+                    L.b0 = b0;
+                    L.uk = o_k;
+                    L.ul = o_l;
+                    L.ord_row = (static_cast<uint32_t>(j0 + own) * 16 + static_cast<uint32_t>(hi - o_k)) * ADJ_SPAN;
+                    L.us = o_s;
+                    L.e = o_e;
+                    L.rev = rev;
+                    s_loci[rank] = L;
+                    if constexpr (S) t.loci++;
+                }
+                n_memo += __popc(kb);
+                if (n_memo > MEMO2) n_memo = MEMO2;
+                __syncwarp();
+                const int U = __popc(kb);
+                Best lb;
+                lb.key = ~0ull;
+                lb.crid = -1;
+                for (int it = lane; it < U * A; it += 32) {
+                    const int u = it / A, a = it - u * A;
+                    const Locus L = s_loci[u];
+                    eval_adj<S>(ix, rd, L.b0, L.rev, a - cl.adj_cap, cl.budget, cl.clip_cap, L.ord_row, lb, L.uk,
+                                L.ul, L.us, L.e, t);
+                }
+                const uint64_t wmin = warp_min64(lb.key);
+                if (wmin < best_key) {
+                    const int wl = __ffs(__ballot_sync(FULL, lb.key == wmin)) - 1;
+                    best_key = wmin;
+                    win.key = wmin;
+                    win.crid = __shfl_sync(FULL, lb.crid, wl);
+                    win.pos = __shfl_sync(FULL, lb.pos, wl);
+                    win.sl = __shfl_sync(FULL, lb.sl, wl);
+                    win.sr = __shfl_sync(FULL, lb.sr, wl);
+                    win.mapq = __shfl_sync(FULL, lb.mapq, wl);
+                    win.flag = __shfl_sync(FULL, lb.flag, wl);
+                    win.uk = __shfl_sync(FULL, lb.uk, wl);
+                    win.ul = __shfl_sync(FULL, lb.ul, wl);
+                    win.us = __shfl_sync(FULL, lb.us, wl);
+                    win.e = __shfl_sync(FULL, lb.e, wl);
+                    improved = true;
+                }
+                __syncwarp();
+            }
+            if ((best_key >> ORD_SHIFT) == 0) break;
+        }
+        if (improved && lane == 0) write_hit(out, r, win, qlen);
+        __syncwarp();
     }
+    flush_tally<S>(t, tally_out);
 }
 
 // One warp per pair.  Keys are 32-bit: nm (<= budget+5 <= 517) << 13 |
@@ -612,11 +854,54 @@ int launch_pack(const uint8_t* d_bases, const uint32_t* d_lens, int64_t n_seq, i
 
 int launch_seed_extend(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
                        unsigned long long* d_tally, cudaStream_t st) {
+    Handoff none{};
     if (d_tally)
-        seed_extend_kernel<true><<<grid_for(R.n_seq, 128), 128, 0, st>>>(ix, R, P, out, d_tally);
+        seed_stage1_kernel<true><<<grid_for(R.n_seq, 128), 128, 0, st>>>(ix, R, P, out, 1 << 30, none, d_tally);
     else
-        seed_extend_kernel<false><<<grid_for(R.n_seq, 128), 128, 0, st>>>(ix, R, P, out, nullptr);
+        seed_stage1_kernel<false><<<grid_for(R.n_seq, 128), 128, 0, st>>>(ix, R, P, out, 1 << 30, none, nullptr);
     return 1;
+}
+
+// Two-stage form: stage 1 over every read for the first `stage1_endpoints`
+// right endpoints, then the persistent stage-2 warps over the reads left.
+// `scratch` must hold two_stage_scratch_bytes(n_seq) bytes.
+size_t two_stage_scratch_bytes(int64_t n_seq) {
+    const size_t n = static_cast<size_t>(n_seq);
+    return 256 + n * 8 + n * 8 * MEMO1 + ((n + 255) / 256) * 256 + n * 4 + 256;
+}
+
+int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
+                          int stage1_endpoints, int stage2_blocks, void* scratch, unsigned long long* d_tally,
+                          cudaStream_t st) {
+    const size_t n = static_cast<size_t>(R.n_seq);
+    char* p = static_cast<char*>(scratch);
+    Handoff h;
+    h.counters = reinterpret_cast<uint32_t*>(p);
+    p += 256;
+    h.key = reinterpret_cast<uint64_t*>(p);
+    p += n * 8;
+    h.memo = reinterpret_cast<uint64_t*>(p);
+    p += n * 8 * MEMO1;
+    h.memo_n = reinterpret_cast<uint8_t*>(p);
+    p += ((n + 255) / 256) * 256;
+    h.pending = reinterpret_cast<uint32_t*>(p);
+    cudaMemsetAsync(h.counters, 0, 256, st);
+    if (d_tally) {
+        seed_stage1_kernel<true><<<grid_for(R.n_seq, 128), 128, 0, st>>>(ix, R, P, out, stage1_endpoints, h, d_tally);
+        seed_stage2_kernel<true><<<stage2_blocks, S2_WARPS * 32, 0, st>>>(ix, R, P, out, stage1_endpoints, h, d_tally);
+    } else {
+        seed_stage1_kernel<false><<<grid_for(R.n_seq, 128), 128, 0, st>>>(ix, R, P, out, stage1_endpoints, h,
+                                                                         nullptr);
+        seed_stage2_kernel<false><<<stage2_blocks, S2_WARPS * 32, 0, st>>>(ix, R, P, out, stage1_endpoints, h,
+                                                                          nullptr);
+    }
+    return 2;
+}
+
+int stage2_blocks_per_sm() {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, seed_stage2_kernel<false>, S2_WARPS * 32, 0);
+    return nb > 0 ? nb : 1;
 }
 
 int launch_rescue(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int64_t n_pairs,

@@ -93,6 +93,10 @@ class ma_index_info(C.Structure):
     ]
 
 
+class ma_tuning(C.Structure):
+    _fields_ = [("seed_kernel", C.c_int32), ("stage1_endpoints", C.c_int32), ("stage2_blocks_per_sm", C.c_int32)]
+
+
 class ma_read_model(C.Structure):
     _fields_ = [
         ("len_fixed", C.c_uint32),
@@ -131,6 +135,8 @@ SIGNATURES = [
       C.POINTER(ma_params), C.POINTER(ma_hits), C.POINTER(ma_debug), C.c_void_p]),
     ("ma_last_launch_count", C.c_int, [C.c_void_p]),
     ("ma_ctx_set_profiling", C.c_int, [C.c_void_p, C.c_int]),
+    ("ma_ctx_set_tuning", C.c_int, [C.c_void_p, C.POINTER(ma_tuning)]),
+    ("ma_ctx_get_tuning", C.c_int, [C.c_void_p, C.POINTER(ma_tuning)]),
     ("ma_ctx_kernel_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     ("ma_ctx_traffic", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     ("ma_bench_gather", C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_uint64, C.POINTER(C.c_double)]),

@@ -44,6 +44,34 @@ class GpuContext:
     def last_launch_count(self) -> int:
         return lib.ma_last_launch_count(self.handle)
 
+    def set_tuning(self, seed_kernel: int = 1, stage1_endpoints: int = 1, stage2_blocks_per_sm: int = 0) -> None:
+        """Result-neutral kernel choices (see ma_tuning in the C header)."""
+        t = _lib.ma_tuning(seed_kernel, stage1_endpoints, stage2_blocks_per_sm)
+        check(lib.ma_ctx_set_tuning(self.handle, C.byref(t)), self.handle)
+
+    def tuning(self) -> dict:
+        t = _lib.ma_tuning()
+        check(lib.ma_ctx_get_tuning(self.handle, C.byref(t)), self.handle)
+        return {f: getattr(t, f) for f, _ in t._fields_}
+
+    def set_profiling(self, flags: int) -> None:
+        check(lib.ma_ctx_set_profiling(self.handle, flags), self.handle)
+
+    def kernel_ms(self) -> list[float]:
+        v = (C.c_float * 3)()
+        check(lib.ma_ctx_kernel_ms(self.handle, v), self.handle)
+        return list(v)
+
+    def traffic(self) -> list[int]:
+        v = (C.c_uint64 * 8)()
+        check(lib.ma_ctx_traffic(self.handle, v), self.handle)
+        return list(v)
+
+    def gather_gbps(self, buffer_bytes: int, line_bytes: int, n_loads: int = 1 << 30) -> float:
+        g = C.c_double()
+        check(lib.ma_bench_gather(self.handle, buffer_bytes, line_bytes, n_loads, C.byref(g)), self.handle)
+        return g.value
+
     def close(self) -> None:
         if self.handle:
             lib.ma_ctx_destroy(self.handle)

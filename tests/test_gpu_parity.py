@@ -36,17 +36,27 @@ def gpu_index(ctx, prefix, k):
     return _INDEX_CACHE[key]
 
 
-def compare(prefix, ctx, bases, lens, n1, paired, max_len, params, k=12, bs=(1, 2)):
+# Result-neutral kernel forms: one thread per read; two stages with the
+# first 1 or 3 right endpoints in stage 1.
+TUNINGS = [(0, 1, 0), (1, 1, 0), (1, 3, 1)]
+
+
+def compare(prefix, ctx, bases, lens, n1, paired, max_len, params, k=12, bs=(1, 2), tunings=TUNINGS):
     gi = gpu_index(ctx, prefix, k)
-    g = map_batch(ctx, gi, bases, lens, n1, paired, max_len, bs[0], bs[1], params, debug=True)
     o = oracle.OracleIndex(prefix).map(bases, lens, n1, paired, max_len, bs[0], bs[1], params.as_list())
-    for f in FIELDS:
-        a, b = getattr(g, f), o[f]
-        bad = np.nonzero(a != b)[0]
-        assert bad.size == 0, (
-            f"{f}: {bad.size} of {a.size} reads differ; first read {bad[0]}: gpu {a[bad[0]]} oracle {b[bad[0]]}; "
-            + ", ".join(f"{x}=({getattr(g, x)[bad[0]]},{o[x][bad[0]]})" for x in FIELDS)
-        )
+    g = None
+    for tu in tunings:
+        ctx.set_tuning(*tu)
+        g = map_batch(ctx, gi, bases, lens, n1, paired, max_len, bs[0], bs[1], params, debug=True)
+        for f in FIELDS:
+            a, b = getattr(g, f), o[f]
+            bad = np.nonzero(a != b)[0]
+            assert bad.size == 0, (
+                f"tuning {tu} {f}: {bad.size} of {a.size} reads differ; first read {bad[0]}: "
+                f"gpu {a[bad[0]]} oracle {b[bad[0]]}; "
+                + ", ".join(f"{x}=({getattr(g, x)[bad[0]]},{o[x][bad[0]]})" for x in FIELDS)
+            )
+    ctx.set_tuning()
     return g
 
 
