@@ -257,14 +257,16 @@ def run_ours(args, rank, world, local):
     clocks = ClockSampler(local)
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    seed_ms = []
-    kms = (_lib.C.c_float * 3)()
+    seed_ms, stage1_ms, other_ms = [], [], []
+    kms = (_lib.C.c_float * 4)()
     torch.cuda.synchronize()
     ev0.record(stream)
     for _ in range(args.steps):
         step()
         _lib.lib.ma_ctx_kernel_ms(ctx.handle, kms)
         seed_ms.append(float(kms[1]))
+        stage1_ms.append(float(kms[3]))
+        other_ms.append((float(kms[0]), float(kms[2])))
     ev1.record(stream)
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1) / args.steps
@@ -298,7 +300,10 @@ def run_ours(args, rank, world, local):
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
             "frac": round(achieved / peaks.get("hbm_gbs"), 4), "traffic": None,
             "peak_source": "fallback" if peaks.get("_fallback") else "measured (MEASURED_PEAKS.json hbm_gbs)",
-            "kernel": "seed_extend_kernel", "kernel_ms": round(seed_avg_ms, 3),
+            "kernel": "seed/extend (seed_stage1_kernel + seed_stage2_kernel)", "kernel_ms": round(seed_avg_ms, 3),
+            "stage1_ms": round(statistics.mean(stage1_ms), 3),
+            "pack_ms": round(statistics.mean(x[0] for x in other_ms), 3),
+            "rescue_ms": round(statistics.mean(x[1] for x in other_ms), 3),
             "alg_bytes_per_launch": int(alg_bytes),
             "tally_per_read": {k: round(v / n_seq, 3) for k, v in zip(
                 ["occ_lines_32B", "kmer_loads", "sa_loads", "pac_sectors_32B", "backward_steps", "endpoints",

@@ -221,8 +221,9 @@ int ma_ctx_get_tuning(const ma_ctx* ctx, ma_tuning* t);
  * stream; bit 1: run the counting instantiation of the seed kernel, which
  * tallies its index and text accesses (slower; for traffic accounting). */
 int ma_ctx_set_profiling(ma_ctx* ctx, int flags);
-/* Device time (ms) of pack, seed/extend and rescue in the last call. */
-int ma_ctx_kernel_ms(const ma_ctx* ctx, float* out3);
+/* Device time (ms) in the last call of: pack, seed/extend (both stages),
+ * rescue, and stage 1 alone (equal to seed/extend for seed_kernel 0). */
+int ma_ctx_kernel_ms(const ma_ctx* ctx, float* out4);
 /* Tallies of the last counting call: 32-B Occ lines, k-mer entries, SA
  * entries, 32-B pac sectors, backward steps, endpoints searched, loci
  * evaluated, read words read. */

@@ -21,7 +21,7 @@ double run_gather_bench(uint64_t buffer_bytes, int line_bytes, uint64_t n_loads,
 size_t two_stage_scratch_bytes(int64_t n_seq);
 int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
                           int stage1_endpoints, int stage2_blocks, void* scratch, unsigned long long* d_tally,
-                          cudaStream_t st);
+                          cudaEvent_t mid, cudaStream_t st);
 int stage2_blocks_per_sm();
 int launch_rescue(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int64_t n_pairs,
                   cudaStream_t st);
@@ -70,8 +70,8 @@ struct ma_ctx {
     std::string err;
     int last_launches = 0;
     int profiling = 0;           // bit 0: per-kernel events, bit 1: traffic tally
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    float kernel_ms[3] = {0, 0, 0};
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // pack | stage 1 | stage 2 | rescue
+    float kernel_ms[4] = {0, 0, 0, 0};  // pack, seed (both stages), rescue, stage 1 alone
     uint64_t traffic[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     bool rescue_ran = false;
     DevBuf tally;
@@ -164,7 +164,7 @@ void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const
         ctx->seed_scratch.ensure(two_stage_scratch_bytes(n_seq));
         const int bps = ctx->tuning.stage2_blocks_per_sm > 0 ? ctx->tuning.stage2_blocks_per_sm : stage2_blocks_per_sm();
         launches += launch_seed_two_stage(idx->dix, R, P, out, ctx->tuning.stage1_endpoints, bps * ctx->sm_count,
-                                          ctx->seed_scratch.p, d_tally, st);
+                                          ctx->seed_scratch.p, d_tally, timed ? ctx->ev[4] : nullptr, st);
     }
     if (timed) ck(cudaEventRecord(ctx->ev[2], st), "event");
     ctx->rescue_ran = paired && p->rescue_win > 0;
@@ -183,6 +183,8 @@ void check_err_flag(ma_ctx* ctx, cudaStream_t st) {
     if (ctx->profiling & 1) {
         for (int i = 0; i < 3; ++i) ck(cudaEventElapsedTime(&ctx->kernel_ms[i], ctx->ev[i], ctx->ev[i + 1]), "elapsed");
         if (!ctx->rescue_ran) ctx->kernel_ms[2] = 0;
+        ctx->kernel_ms[3] = ctx->kernel_ms[1];
+        if (ctx->tuning.seed_kernel == 1) ck(cudaEventElapsedTime(&ctx->kernel_ms[3], ctx->ev[1], ctx->ev[4]), "elapsed");
     }
     if (ctx->profiling & 2) {
         unsigned long long t[8];
@@ -451,9 +453,9 @@ int ma_ctx_get_tuning(const ma_ctx* ctx, ma_tuning* t) {
     return MA_OK;
 }
 
-int ma_ctx_kernel_ms(const ma_ctx* ctx, float* out3) {
-    if (!ctx || !out3) return MA_ERR_ARG;
-    for (int i = 0; i < 3; ++i) out3[i] = ctx->kernel_ms[i];
+int ma_ctx_kernel_ms(const ma_ctx* ctx, float* out4) {
+    if (!ctx || !out4) return MA_ERR_ARG;
+    for (int i = 0; i < 4; ++i) out4[i] = ctx->kernel_ms[i];
     return MA_OK;
 }
 

@@ -23,19 +23,21 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
 }
 
 template <int LINE>
-__global__ void __launch_bounds__(256) gather_kernel(const uint4* __restrict__ buf, uint64_t n_lines,
+__global__ void __launch_bounds__(256) gather_kernel(const uint4* __restrict__ buf, uint64_t line_mask,
                                                      uint32_t iters, uint64_t seed, uint32_t* __restrict__ sink) {
     constexpr int V = LINE / 16;  // uint4 per line
-    constexpr int INFLIGHT = 4;
+    constexpr int INFLIGHT = 8;
     const uint64_t tid = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-    uint64_t state = mix64(seed ^ (tid * 0x9E3779B97F4A7C15ull));
+    uint64_t state = mix64(seed ^ (tid * 0x9E3779B97F4A7C15ull)) | 1;
     uint32_t acc = 0;
     for (uint32_t it = 0; it < iters; it += INFLIGHT) {
         uint4 v[INFLIGHT][V];
 #pragma unroll
         for (int j = 0; j < INFLIGHT; ++j) {
-            state = mix64(state + 0x9E3779B97F4A7C15ull);
-            const uint4* p = buf + (state % n_lines) * V;
+            state ^= state << 13;  // xorshift64
+            state ^= state >> 7;
+            state ^= state << 17;
+            const uint4* p = buf + (state & line_mask) * V;
 #pragma unroll
             for (int q = 0; q < V; ++q) v[j][q] = __ldg(p + q);
         }
@@ -57,7 +59,8 @@ void ck(cudaError_t e, const char* what) {
 double run_gather_bench(uint64_t buffer_bytes, int line_bytes, uint64_t n_loads, int sm_count, cudaStream_t st) {
     if (line_bytes != 32 && line_bytes != 64) fail(MA_ERR_ARG, "line_bytes must be 32 or 64");
     if (buffer_bytes < 1024) fail(MA_ERR_ARG, "buffer too small");
-    const uint64_t n_lines = buffer_bytes / line_bytes;
+    uint64_t n_lines = 1;  // a power of two, at most buffer_bytes / line_bytes
+    while (n_lines * 2 * line_bytes <= buffer_bytes) n_lines *= 2;
     void* buf = nullptr;
     uint32_t* sink = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -71,13 +74,13 @@ double run_gather_bench(uint64_t buffer_bytes, int line_bytes, uint64_t n_loads,
         const int block = 256;
         const uint64_t threads = static_cast<uint64_t>(sm_count) * 8 * block;  // 8 blocks per SM
         uint32_t iters = static_cast<uint32_t>((n_loads + threads - 1) / threads);
-        iters = (iters + 3) & ~3u;
+        iters = (iters + 7) & ~7u;
         const unsigned grid = static_cast<unsigned>(threads / block);
         auto launch = [&](uint64_t seed) {
             if (line_bytes == 32)
-                gather_kernel<32><<<grid, block, 0, st>>>(static_cast<const uint4*>(buf), n_lines, iters, seed, sink);
+                gather_kernel<32><<<grid, block, 0, st>>>(static_cast<const uint4*>(buf), n_lines - 1, iters, seed, sink);
             else
-                gather_kernel<64><<<grid, block, 0, st>>>(static_cast<const uint4*>(buf), n_lines, iters, seed, sink);
+                gather_kernel<64><<<grid, block, 0, st>>>(static_cast<const uint4*>(buf), n_lines - 1, iters, seed, sink);
         };
         launch(1);  // warm-up
         ck(cudaEventRecord(e0, st), "record");

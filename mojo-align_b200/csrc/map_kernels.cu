@@ -90,12 +90,7 @@ struct Tally {
 template <bool S>
 __device__ __forceinline__ uint64_t mm_word(const uint64_t* __restrict__ pacw, const uint64_t* q,
                                             const uint64_t* qn, int64_t bstart, int w, Tally& t) {
-    if constexpr (S) {
-        // the window reads 16 bytes at word (bstart + 32w + 32*PAC_PAD) >> 5
-        const uint64_t wi = static_cast<uint64_t>(bstart + 32 * w + 32 * PAC_PAD) >> 5;
-        t.pac_sectors += ((wi * 8) >> 5) == ((wi * 8 + 15) >> 5) ? 1 : 2;
-        t.read_words += 2;
-    }
+    if constexpr (S) t.read_words += 2;
     uint64_t x = q[w] ^ ref_window(pacw, bstart + 32 * w);
     return ((x | (x >> 1)) & kEven) | qn[w];
 }
@@ -239,6 +234,11 @@ __device__ void eval_adj(const DevIndex& ix, const ReadView& rd, int64_t b0, int
     const int64_t sr0 = local + qlen > clen ? local + qlen - clen : 0;
     if (!(sl0 + sr0 < qlen && sl0 <= clip_cap && sr0 <= clip_cap)) return;
     const uint32_t ord = (ord_row + static_cast<uint32_t>(adj + 12)) * KIND_SPAN;
+    if constexpr (S) {
+        // text bytes of the window [bstart, bstart + qlen], 4 bases a byte
+        const int64_t lo = (bstart < 0 ? 0 : bstart) >> 2, hi = (bstart + qlen) >> 2;
+        t.pac_sectors += static_cast<uint32_t>((hi >> 5) - (lo >> 5) + 1);
+    }
     int nm = count_mm<S>(ix.pacw, q, qn, bstart, static_cast<int>(sl0), static_cast<int>(qlen - sr0), budget + 1, t);
     int sl = static_cast<int>(sl0), sr = static_cast<int>(sr0);
     if (nm > budget && clip_cap > 0) {
@@ -872,7 +872,7 @@ size_t two_stage_scratch_bytes(int64_t n_seq) {
 
 int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
                           int stage1_endpoints, int stage2_blocks, void* scratch, unsigned long long* d_tally,
-                          cudaStream_t st) {
+                          cudaEvent_t mid, cudaStream_t st) {
     const size_t n = static_cast<size_t>(R.n_seq);
     char* p = static_cast<char*>(scratch);
     Handoff h;
@@ -888,10 +888,12 @@ int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams
     cudaMemsetAsync(h.counters, 0, 256, st);
     if (d_tally) {
         seed_stage1_kernel<true><<<grid_for(R.n_seq, 128), 128, 0, st>>>(ix, R, P, out, stage1_endpoints, h, d_tally);
+        if (mid) cudaEventRecord(mid, st);
         seed_stage2_kernel<true><<<stage2_blocks, S2_WARPS * 32, 0, st>>>(ix, R, P, out, stage1_endpoints, h, d_tally);
     } else {
         seed_stage1_kernel<false><<<grid_for(R.n_seq, 128), 128, 0, st>>>(ix, R, P, out, stage1_endpoints, h,
                                                                          nullptr);
+        if (mid) cudaEventRecord(mid, st);
         seed_stage2_kernel<false><<<stage2_blocks, S2_WARPS * 32, 0, st>>>(ix, R, P, out, stage1_endpoints, h,
                                                                           nullptr);
     }

@@ -58,7 +58,7 @@ class GpuContext:
         check(lib.ma_ctx_set_profiling(self.handle, flags), self.handle)
 
     def kernel_ms(self) -> list[float]:
-        v = (C.c_float * 3)()
+        v = (C.c_float * 4)()
         check(lib.ma_ctx_kernel_ms(self.handle, v), self.handle)
         return list(v)
 
