@@ -49,6 +49,7 @@ def parse_args():
     ap.add_argument("--genome-mb", type=int, default=250)
     ap.add_argument("--pairs", type=int, default=10_000_000, help="read pairs per GPU")
     ap.add_argument("--kmer", type=int, default=12)
+    ap.add_argument("--kmer3", type=int, default=19, help="converted-alphabet k-mer tables (<= seed_len)")
     ap.add_argument("--workdir", default=os.environ.get("MOJOALIGN_BENCH_DIR", tempfile.gettempdir()))
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the oracle timing (profiling runs)")
@@ -228,7 +229,7 @@ def run_ours(args, rank, world, local):
 
     ctx = GpuContext(local)
     t = time.time()
-    gi = GpuIndex(ctx, prefix, kmer_k=args.kmer)
+    gi = GpuIndex(ctx, prefix, kmer_k=args.kmer, kmer3_k=args.kmer3)
     open_s = time.time() - t
 
     # ---- device-resident inputs and outputs ----
@@ -317,7 +318,8 @@ def run_ours(args, rank, world, local):
                        "reads_per_gpu": n_seq, "read_len": READ_LEN, "paired": True,
                        "params": dict(zip(["seed_len", "seed_stride", "max_occ", "max_diff", "max_soft", "max_adj",
                                            "rescue_win"], params.as_list())),
-                       "kmer_k": args.kmer, "l2": "inputs larger than L2 (reads and index several GB)",
+                       "kmer_k": args.kmer, "kmer3_k": args.kmer3, "index_hbm_bytes": int(gi.info.device_bytes),
+                       "l2": "inputs larger than L2 (reads and index several GB)",
                        "mapped_frac": round(mapped, 4)},
             "e2e": {"value": round(e2e_value, 1), "unit": "reads/s",
                     "h2d_bytes_per_step": int(n_seq * READ_LEN + n_seq * 4),

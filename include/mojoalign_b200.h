@@ -109,8 +109,27 @@ typedef struct ma_index_info {
     uint64_t sa_reject_below; /* smallest text position reachable by the
                                  reference's sampled-SA walk (see DESIGN) */
     int32_t kmer_k;        /* k of the resident k-mer interval table         */
+    int32_t kmer3_k;       /* k of the converted-alphabet k-mer tables       */
     uint64_t device_bytes; /* HBM held by this index                         */
 } ma_index_info;
+
+/*
+ * Resident-index options (all result-neutral).
+ *   kmer_k    k-mer interval table over A/C/G/T, 4^k entries of 8 bytes
+ *             (0 = none, 1..14; default 12).
+ *   kmer3_k   interval tables over the converted-read alphabets A/G/T
+ *             (C->T reads) and A/C/T (G->A reads), 2 * 3^k entries of 8
+ *             bytes (0 = none, 1..20; default 0).  k = seed_len replaces
+ *             the first seed_len backward-search steps with one lookup.
+ *   hbm_budget_bytes  admission budget (0 = all free HBM).
+ * A table is used by a mapping call only when its k <= seed_len.
+ */
+typedef struct ma_index_options {
+    int32_t kmer_k;
+    int32_t kmer3_k;
+    uint64_t hbm_budget_bytes;
+} ma_index_options;
+void ma_index_options_default(ma_index_options* o);
 
 /* ---- context ------------------------------------------------------- */
 
@@ -144,12 +163,11 @@ int ma_index_build(const char* fasta, const char* out_prefix, int bwameth_c2t,
  * index resident in HBM (upload at linear_gpu_fm.mojo:2034-2069) in this
  * library's own layout.  The HBM preflight (_require_hbm,
  * linear_gpu_locate.mojo:211-214; gpu_mem.require_index_capacity) becomes a
- * cudaMemGetInfo check against hbm_budget_bytes (0 = all free HBM).
- * kmer_k selects the k-mer interval table (0 = none, 1..14; must not exceed
- * the seed length used later).
+ * cudaMemGetInfo check of the resident bytes plus staging against
+ * opt->hbm_budget_bytes, failing with MA_ERR_NOMEM.  opt may be NULL.
  */
-int ma_index_open(ma_ctx* ctx, const char* prefix, int kmer_k,
-                  uint64_t hbm_budget_bytes, ma_index** out);
+int ma_index_open(ma_ctx* ctx, const char* prefix, const ma_index_options* opt,
+                  ma_index** out);
 void ma_index_close(ma_index* idx);
 int ma_index_get_info(const ma_index* idx, ma_index_info* out);
 /* Contig record i of the .ann (FmIndex.contig_name/offset/length,

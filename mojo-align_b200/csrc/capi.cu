@@ -271,25 +271,35 @@ int ma_index_build(const char* fasta, const char* out_prefix, int bwameth_c2t, i
     return guarded(nullptr, [&] { build_index(fasta, out_prefix, bwameth_c2t != 0, sa_intv, device_ordinal); });
 }
 
-int ma_index_open(ma_ctx* ctx, const char* prefix, int kmer_k, uint64_t hbm_budget_bytes, ma_index** out) {
+void ma_index_options_default(ma_index_options* o) {
+    if (!o) return;
+    o->kmer_k = 12;
+    o->kmer3_k = 0;
+    o->hbm_budget_bytes = 0;
+}
+
+int ma_index_open(ma_ctx* ctx, const char* prefix, const ma_index_options* opt, ma_index** out) {
     if (!ctx || !prefix || !out) return MA_ERR_ARG;
     *out = nullptr;
+    ma_index_options o;
+    ma_index_options_default(&o);
+    if (opt) o = *opt;
     ma_index* idx = new ma_index();
     int rc = guarded(ctx, [&] {
         use_device(ctx);
         BwaIndexHost h = load_bwa_index(prefix);
-        const uint64_t need = device_index_bytes(h, kmer_k);
+        const uint64_t need = device_index_bytes(h, o.kmer_k, o.kmer3_k);
         size_t f = 0, t = 0;
         ck(cudaMemGetInfo(&f, &t), "cudaMemGetInfo");
         // fail-closed admission like gpu_mem.require_index_capacity: the
-        // resident index plus staging (bwt, pac, samples) must fit
-        const uint64_t staging = h.bwt.size() * 4 + h.pac.size() + h.sa.size() * 8;
-        const uint64_t budget = hbm_budget_bytes ? std::min<uint64_t>(hbm_budget_bytes, f) : f;
+        // resident index plus the preparation passes' staging must fit
+        const uint64_t staging = device_index_staging_bytes(h, o.kmer3_k);
+        const uint64_t budget = o.hbm_budget_bytes ? std::min<uint64_t>(o.hbm_budget_bytes, f) : f;
         if (need + staging > budget)
             fail(MA_ERR_NOMEM, "index needs " + std::to_string((need + staging) >> 20) + " MiB of HBM, budget " +
                                    std::to_string(budget >> 20) + " MiB");
         uint64_t p0 = 0;
-        idx->dix = build_device_index(h, kmer_k, ctx->stream, idx->bufs, &p0);
+        idx->dix = build_device_index(h, o.kmer_k, o.kmer3_k, ctx->stream, idx->bufs, &p0);
         idx->ctx = ctx;
         idx->contigs = h.contigs;
         ma_index_info& I = idx->info;
@@ -301,7 +311,8 @@ int ma_index_open(ma_ctx* ctx, const char* prefix, int kmer_k, uint64_t hbm_budg
         I.n_sa = h.n_sa;
         I.n_contigs = static_cast<int64_t>(h.contigs.size());
         I.sa_reject_below = p0;
-        I.kmer_k = kmer_k;
+        I.kmer_k = o.kmer_k;
+        I.kmer3_k = o.kmer3_k;
         I.device_bytes = idx->bufs.bytes;
     });
     if (rc != MA_OK) {

@@ -8,11 +8,13 @@
 //   relayout_pac      MSB-first pac bytes -> LSB-first u64 words, padded
 //   reconstruct_sa    sampled SA -> full SA, one LF chain per sampled row
 //   build_kmer        k-mer -> backward-search interval table
+//   kmer3_rows/bounds 3-letter k-mer tables from one pass over the full SA
 // Every kernel's loops are bounded; a chain that runs past its bound (only
 // possible on an inconsistent index) raises a device error flag instead of
 // spinning.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 
 #include "ma_device.cuh"
@@ -146,6 +148,69 @@ __global__ void build_kmer_kernel(DevIndex ix, int K, uint64_t n_kmers, uint2* _
     out[idx] = make_uint2(static_cast<uint32_t>(k), static_cast<uint32_t>(l));
 }
 
+// 2-bit codes of text T[p, p+K) (T = the pac followed by its reverse
+// complement), first base most significant; ~0 when p + K > seq_len.
+__device__ uint64_t text_kmer(const DevIndex& ix, uint64_t p, int K) {
+    if (p + K > ix.seq_len) return ~0ull;
+    const uint64_t L = ix.l_pac;
+    const uint64_t mask = (1ull << (2 * K)) - 1;
+    uint64_t v = 0;
+    if (p + K <= L) {
+        const uint64_t w = ref_window(ix.pacw, static_cast<int64_t>(p));  // base p at bits 0-1
+        for (int i = 0; i < K; ++i) v = (v << 2) | ((w >> (2 * i)) & 3);
+    } else if (p >= L) {
+        // T[p+i] = 3 - pac[2L-1-p-i]: the forward window [q0, q0+K) read
+        // backwards and complemented, which is the LSB-first window itself
+        const uint64_t q0 = 2 * L - p - K;
+        v = (ref_window(ix.pacw, static_cast<int64_t>(q0)) & mask) ^ mask;
+    } else {
+        for (int i = 0; i < K; ++i) {
+            const uint64_t q = p + i;
+            const uint64_t f = q < L ? q : 2 * L - 1 - q;
+            const uint64_t c = (ix.pacw[(f >> 5) + PAC_PAD] >> (2 * (f & 31))) & 3;
+            v = (v << 2) | (q < L ? c : 3 - c);
+        }
+    }
+    return v;
+}
+
+__global__ void kmer3_rows_kernel(DevIndex ix, int K, uint64_t n_rows, uint64_t* __restrict__ codes) {
+    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n_rows) return;
+    codes[i] = text_kmer(ix, ix.sa[i], K);
+}
+
+__global__ void fill_empty_kernel(uint2* __restrict__ t, uint64_t n) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n; i += stride)
+        t[i] = make_uint2(0xFFFFFFFFu, 0u);
+}
+
+// Rows with the same k-mer are contiguous in SA order; the first and last
+// row of each run are the interval (k, l) of that k-mer.
+__global__ void kmer3_bounds_kernel(const uint64_t* __restrict__ codes, uint64_t n_rows, int K,
+                                    uint2* __restrict__ t_agt, uint2* __restrict__ t_act) {
+    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n_rows) return;
+    const uint64_t c = codes[i];
+    if (c == ~0ull) return;
+    const bool start = i == 0 || codes[i - 1] != c;
+    const bool end = i + 1 == n_rows || codes[i + 1] != c;
+    if (!start && !end) return;
+    const uint64_t lo = c & kEven, hi = (c >> 1) & kEven;
+    const bool has_c = (lo & ~hi) != 0, has_g = (hi & ~lo) != 0;
+    uint32_t idx = 0;
+    for (int j = K - 1; j >= 0; --j) idx = idx * 3 + static_cast<uint32_t>(__popcll((c >> (2 * j)) & 3));
+    if (!has_c) {
+        if (start) t_agt[idx].x = static_cast<uint32_t>(i);
+        if (end) t_agt[idx].y = static_cast<uint32_t>(i);
+    }
+    if (!has_g) {
+        if (start) t_act[idx].x = static_cast<uint32_t>(i);
+        if (end) t_act[idx].y = static_cast<uint32_t>(i);
+    }
+}
+
 void check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) fail(MA_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
@@ -157,23 +222,38 @@ unsigned grid_for(uint64_t n, unsigned block) {
 
 }  // namespace
 
-uint64_t device_index_bytes(const BwaIndexHost& h, int kmer_k) {
+uint64_t pow3(int k) {
+    uint64_t v = 1;
+    for (int i = 0; i < k; ++i) v *= 3;
+    return v;
+}
+
+uint64_t device_index_bytes(const BwaIndexHost& h, int kmer_k, int kmer3_k) {
     uint64_t n_lines = (h.seq_len + 63) / 64;
     uint64_t b = n_lines * sizeof(OccLine);
     b += (h.seq_len + 1) * 4;
     b += ((h.l_pac + 31) / 32 + 2 * PAC_PAD) * 8;
     if (kmer_k > 0) b += (1ull << (2 * kmer_k)) * 8;
+    if (kmer3_k > 0) b += 2 * pow3(kmer3_k) * 8;
     b += h.contigs.size() * 12;
+    return b;
+}
+
+// Temporary device memory of the preparation passes.
+uint64_t device_index_staging_bytes(const BwaIndexHost& h, int kmer3_k) {
+    uint64_t b = h.bwt.size() * 4 + h.pac.size() + h.sa.size() * 8;
+    if (kmer3_k > 0) b = std::max<uint64_t>(b, (h.seq_len + 1) * 8);
     return b;
 }
 
 // Builds the resident index on the current device; returns its DevIndex and
 // fills `bufs`.  Temporary upload buffers are freed before returning.
-DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, cudaStream_t st, DeviceIndexBuffers& bufs,
-                            uint64_t* reject_below) {
+DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, int kmer3_k, cudaStream_t st,
+                            DeviceIndexBuffers& bufs, uint64_t* reject_below) {
     if (h.seq_len + 1 >= 0xFFFFFFFFull)
         fail(MA_ERR_UNSUPPORTED, "resident layout stores SA rows as u32; texts of 2^32 symbols or more are not supported yet");
     if (kmer_k < 0 || kmer_k > 14) fail(MA_ERR_ARG, "kmer_k must be in 0..14");
+    if (kmer3_k < 0 || kmer3_k > 20) fail(MA_ERR_ARG, "kmer3_k must be in 0..20");
     const uint64_t n_lines = (h.seq_len + 63) / 64;
     const uint64_t n_pacw = (h.l_pac + 31) / 32 + 2 * PAC_PAD;
     DevIndex ix{};
@@ -183,6 +263,7 @@ DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, cudaStream_t st, 
     for (int c = 0; c < 5; ++c) ix.L2[c] = h.L2[c];
     ix.n_contigs = static_cast<int64_t>(h.contigs.size());
     ix.kmer_k = kmer_k;
+    ix.kmer3_k = 0;  // set once the tables are built
 
     uint32_t* d_bwa = nullptr;
     uint8_t* d_pac = nullptr;
@@ -262,13 +343,33 @@ DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, cudaStream_t st, 
             check(cudaGetLastError(), "build_kmer launch");
             ix.kmer = bufs.kmer;
         }
+        if (kmer3_k > 0) {
+            const uint64_t n3 = pow3(kmer3_k), n_rows = h.seq_len + 1;
+            check(cudaMalloc(&bufs.kmer3[0], n3 * 8), "cudaMalloc kmer3");
+            check(cudaMalloc(&bufs.kmer3[1], n3 * 8), "cudaMalloc kmer3");
+            uint64_t* d_codes = nullptr;
+            check(cudaMalloc(&d_codes, n_rows * 8), "cudaMalloc kmer3 staging");
+            fill_empty_kernel<<<4096, 256, 0, st>>>(bufs.kmer3[0], n3);
+            fill_empty_kernel<<<4096, 256, 0, st>>>(bufs.kmer3[1], n3);
+            kmer3_rows_kernel<<<grid_for(n_rows, 256), 256, 0, st>>>(ix, kmer3_k, n_rows, d_codes);
+            kmer3_bounds_kernel<<<grid_for(n_rows, 256), 256, 0, st>>>(d_codes, n_rows, kmer3_k, bufs.kmer3[0],
+                                                                       bufs.kmer3[1]);
+            cudaError_t le = cudaGetLastError();
+            cudaError_t se = cudaStreamSynchronize(st);
+            cudaFree(d_codes);
+            check(le, "kmer3 launch");
+            check(se, "kmer3 tables");
+            ix.kmer3[0] = bufs.kmer3[0];
+            ix.kmer3[1] = bufs.kmer3[1];
+            ix.kmer3_k = kmer3_k;
+        }
         check(cudaStreamSynchronize(st), "index preparation");
     } catch (...) {
         cleanup();
         throw;
     }
     cleanup();
-    bufs.bytes = device_index_bytes(h, kmer_k);
+    bufs.bytes = device_index_bytes(h, kmer_k, kmer3_k);
     return ix;
 }
 
@@ -277,6 +378,8 @@ void free_device_index(DeviceIndexBuffers& b) {
     cudaFree(b.sa);
     cudaFree(b.pacw);
     cudaFree(b.kmer);
+    cudaFree(b.kmer3[0]);
+    cudaFree(b.kmer3[1]);
     cudaFree(b.coff);
     cudaFree(b.clen);
     b = DeviceIndexBuffers{};

@@ -14,6 +14,10 @@
 //   kmer  for every k-mer W (first base most significant, 2 bits per base)
 //         the backward-search interval (k, l) after the k steps that consume
 //         W; k > l when W does not occur.
+//   kmer3 the same intervals for k-mers over the alphabets of converted
+//         reads, indexed in base 3: table 0 holds the words without C
+//         (A, G, T -> digits 0, 1, 2; C->T reads), table 1 the words
+//         without G (A, C, T -> 0, 1, 2; G->A reads).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -38,6 +42,7 @@ struct DevIndex {
     const uint32_t* sa;
     const uint64_t* pacw;
     const uint2* kmer;
+    const uint2* kmer3[2];
     const uint64_t* coff;
     const uint32_t* clen;
     int64_t n_contigs;
@@ -45,6 +50,7 @@ struct DevIndex {
     uint64_t L2[5];
     uint64_t sa_reject_below;  // sa_pos below this is rejected (see seed kernel)
     int32_t kmer_k;
+    int32_t kmer3_k;
 };
 
 // Mapping parameters after the reference's clamps are applied per read.
@@ -142,15 +148,18 @@ struct DeviceIndexBuffers {
     uint32_t* sa = nullptr;
     uint64_t* pacw = nullptr;
     uint2* kmer = nullptr;
+    uint2* kmer3[2] = {nullptr, nullptr};
     uint64_t* coff = nullptr;
     uint32_t* clen = nullptr;
     uint64_t bytes = 0;
 };
 
 struct BwaIndexHost;
-uint64_t device_index_bytes(const BwaIndexHost& h, int kmer_k);
-DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, cudaStream_t st, DeviceIndexBuffers& bufs,
-                            uint64_t* reject_below);
+uint64_t pow3(int k);
+uint64_t device_index_bytes(const BwaIndexHost& h, int kmer_k, int kmer3_k);
+uint64_t device_index_staging_bytes(const BwaIndexHost& h, int kmer3_k);
+DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, int kmer3_k, cudaStream_t st,
+                            DeviceIndexBuffers& bufs, uint64_t* reject_below);
 void free_device_index(DeviceIndexBuffers& b);
 
 }  // namespace ma

@@ -78,6 +78,15 @@ __device__ __forceinline__ int code_at(const ReadView& v, int s) {
     return static_cast<int>((v.fwd[w] >> sh) & 3);
 }
 
+// 2*n bits (n <= 32 bases) of packed read words starting at base s, base s
+// in the lowest two bits.  Reads only words that hold bases of the window.
+__device__ __forceinline__ uint64_t window_bits(const uint64_t* words, int s, int n) {
+    const int w = s >> 5, off = s & 31;
+    uint64_t v = words[w] >> (2 * off);
+    if (off && off + n > 32) v |= words[w + 1] << (64 - 2 * off);
+    return n >= 32 ? v : (v & ((1ull << (2 * n)) - 1));
+}
+
 // Per-thread traffic tally of the counting kernel variant (S = true).  The
 // timed kernel is the S = false instantiation, where every tally compiles
 // away.
@@ -215,10 +224,13 @@ __device__ __forceinline__ void deletion_scan(const uint64_t* __restrict__ pacw,
 // One shift adj of one locus (b0, strand): the body of the reference's adj
 // loop, linear_gpu_fm.mojo:1528-1826.  Folds the candidate (full compare,
 // or the deletion probe's offsets) into `best` by its (nm, ordinal) key.
+// prune_nm: a candidate of this call can only matter when its nm is below
+// prune_nm (every candidate of the call comes after the current best in the
+// reference's order); 1 << 20 disables pruning.
 template <bool S>
 __device__ void eval_adj(const DevIndex& ix, const ReadView& rd, int64_t b0, int is_rev, int adj, int budget,
                          int clip_cap, uint32_t ord_row, Best& best, uint64_t uk, uint64_t ul, int us, int e,
-                         Tally& t) {
+                         int prune_nm, Tally& t) {
     const int qlen = rd.qlen;
     const uint64_t* q = is_rev ? rd.rc : rd.fwd;
     const uint64_t* qn = is_rev ? rd.nr : rd.nf;
@@ -238,6 +250,39 @@ __device__ void eval_adj(const DevIndex& ix, const ReadView& rd, int64_t b0, int
         // text bytes of the window [bstart, bstart + qlen], 4 bases a byte
         const int64_t lo = (bstart < 0 ? 0 : bstart) >> 2, hi = (bstart + qlen) >> 2;
         t.pac_sectors += static_cast<uint32_t>((hi >> 5) - (lo >> 5) + 1);
+    }
+    const bool del_probe = adj == 0 && is_rev == 0;
+    {
+        // Exact pruning.  sl0, sr0 and every soft clip are at most clip_cap,
+        // so the full compare and any clipped recount both span read
+        // positions [clip_cap, qlen - clip_cap); their mismatches bound nm.
+        const int core = count_mm<S>(ix.pacw, q, qn, bstart, clip_cap, qlen - clip_cap, budget + 1, t);
+        if (core > budget) {
+            // neither compare is accepted: only the deletion probe remains
+            if (del_probe && prune_nm > 1 && bstart + qlen + 1 <= coff + clen) {
+                deletion_scan<S>(ix.pacw, q, qn, bstart, qlen, budget, t, [&](int g, int nmd) {
+                    if (nmd > budget) return;
+                    const uint64_t key = (static_cast<uint64_t>(nmd) << ORD_SHIFT) | (ord + 1 + g / 4);
+                    if (key < best.key) {
+                        best.key = key;
+                        best.crid = static_cast<int32_t>(crid);
+                        best.pos = static_cast<uint32_t>(local);
+                        best.sl = 0;
+                        best.sr = 0;
+                        best.mapq = 20u;
+                        best.flag = 0;
+                        best.uk = uk;
+                        best.ul = ul;
+                        best.us = us;
+                        best.e = e;
+                    }
+                });
+            }
+            return;
+        }
+        // whether the compare is accepted decides the deletion probe, so
+        // only shifts without one can stop here
+        if (core >= prune_nm && !del_probe) return;
     }
     int nm = count_mm<S>(ix.pacw, q, qn, bstart, static_cast<int>(sl0), static_cast<int>(qlen - sr0), budget + 1, t);
     int sl = static_cast<int>(sl0), sr = static_cast<int>(sr0);
@@ -276,8 +321,8 @@ __device__ void eval_adj(const DevIndex& ix, const ReadView& rd, int64_t b0, int
             best.us = us;
             best.e = e;
         }
-    } else if (adj == 0 && is_rev == 0) {
-        if (bstart + qlen + 1 <= coff + clen) {
+    } else if (del_probe) {
+        if (prune_nm > 1 && bstart + qlen + 1 <= coff + clen) {
             deletion_scan<S>(ix.pacw, q, qn, bstart, qlen, budget, t, [&](int g, int nmd) {
                 if (nmd > budget) return;
                 const uint64_t key = (static_cast<uint64_t>(nmd) << ORD_SHIFT) | (ord + 1 + g / 4);
@@ -305,8 +350,11 @@ __device__ void eval_locus(const DevIndex& ix, const ReadView& rd, int64_t b0, i
                            int budget, int clip_cap, uint32_t ord_row, Best& best, uint64_t uk, uint64_t ul,
                            int us, int e, Tally& t) {
     if constexpr (S) t.loci++;
-    for (int adj = -adj_cap; adj <= adj_cap; ++adj)
-        eval_adj<S>(ix, rd, b0, is_rev, adj, budget, clip_cap, ord_row, best, uk, ul, us, e, t);
+    for (int adj = -adj_cap; adj <= adj_cap; ++adj) {
+        const uint64_t bn = best.key >> ORD_SHIFT;
+        eval_adj<S>(ix, rd, b0, is_rev, adj, budget, clip_cap, ord_row, best, uk, ul, us, e,
+                    bn < (1u << 20) ? static_cast<int>(bn) : (1 << 20), t);
+    }
 }
 
 struct Seed {
@@ -323,20 +371,46 @@ __device__ __forceinline__ Seed search_endpoint(const DevIndex& ix, const ReadVi
     uint64_t k = 0, l = ix.seq_len, last_k = 0, last_l = 0;
     int s = e, last_s = -1;
     Seed res{0, 0, -1, false};
-    const int K = ix.kmer_k;
     bool stop = false;
-    if (K > 0 && K <= P.seed_len) {
-        const int s0 = e - K + 1;
-        uint32_t idx = 0;
-        for (int t = s0; t <= e; ++t) {
-            int c = code_at(rd, t);
-            if (c > 3) return res;  // a non-ACGT before mlen reaches seed_len
-            idx = (idx << 2) | static_cast<uint32_t>(c);
+    bool have = false;  // a table gave the interval after the first K steps
+    int K = 0;
+    // Steps before mlen reaches seed_len record nothing, so with K <= seed_len
+    // a window holding a non-ACGT base, or an empty interval, ends the search
+    // with no seed, and otherwise the interval after K steps is all that is
+    // kept from them.
+    const int K3 = ix.kmer3_k;
+    if (K3 > 0 && K3 <= P.seed_len) {
+        const int s0 = e - K3 + 1;
+        if (window_bits(rd.nf, s0, K3) != 0) return res;
+        const uint64_t win = window_bits(rd.fwd, s0, K3);
+        const uint64_t lo = win & kEven, hi = (win >> 1) & kEven;
+        const bool has_c = (lo & ~hi) != 0, has_g = (hi & ~lo) != 0;
+        if (!(has_c && has_g)) {
+            uint32_t idx = 0;
+            for (int i = 0; i < K3; ++i) idx = idx * 3 + static_cast<uint32_t>(__popcll((win >> (2 * i)) & 3));
+            const uint2 kl = __ldg(ix.kmer3[has_c ? 1 : 0] + idx);
+            if constexpr (S) t.kmer_loads++;
+            k = kl.x;
+            l = kl.y;
+            have = true;
+            K = K3;
         }
+    }
+    if (!have && ix.kmer_k > 0 && ix.kmer_k <= P.seed_len) {
+        K = ix.kmer_k;
+        const int s0 = e - K + 1;
+        if (window_bits(rd.nf, s0, K) != 0) return res;
+        const uint64_t win = window_bits(rd.fwd, s0, K);
+        uint32_t idx = 0;
+        for (int i = 0; i < K; ++i) idx = (idx << 2) | static_cast<uint32_t>((win >> (2 * i)) & 3);
         const uint2 kl = __ldg(ix.kmer + idx);
         if constexpr (S) t.kmer_loads++;
         k = kl.x;
         l = kl.y;
+        have = true;
+    }
+    if (have) {
+        const int s0 = e - K + 1;
         if (k > l) return res;
         if (K >= P.seed_len) {
             const int64_t occ_n = static_cast<int64_t>(l - k + 1);
@@ -708,11 +782,13 @@ __global__ void __launch_bounds__(S2_WARPS * 32) seed_stage2_kernel(DevIndex ix,
                 Best lb;
                 lb.key = ~0ull;
                 lb.crid = -1;
+                const uint64_t bn = best_key >> ORD_SHIFT;
+                const int prune = bn < (1u << 20) ? static_cast<int>(bn) : (1 << 20);
                 for (int it = lane; it < U * A; it += 32) {
                     const int u = it / A, a = it - u * A;
                     const Locus L = s_loci[u];
                     eval_adj<S>(ix, rd, L.b0, L.rev, a - cl.adj_cap, cl.budget, cl.clip_cap, L.ord_row, lb, L.uk,
-                                L.ul, L.us, L.e, t);
+                                L.ul, L.us, L.e, prune, t);
                 }
                 const uint64_t wmin = warp_min64(lb.key);
                 if (wmin < best_key) {

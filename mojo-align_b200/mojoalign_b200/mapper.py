@@ -100,9 +100,10 @@ class Contig:
 class GpuIndex:
     """A bwa 0.7 FM-index made resident in HBM (FmIndex.load + upload)."""
 
-    def __init__(self, ctx: GpuContext, prefix, kmer_k: int = 12, hbm_budget_bytes: int = 0):
+    def __init__(self, ctx: GpuContext, prefix, kmer_k: int = 12, kmer3_k: int = 0, hbm_budget_bytes: int = 0):
         h = C.c_void_p()
-        check(lib.ma_index_open(ctx.handle, fspath(prefix), kmer_k, hbm_budget_bytes, C.byref(h)), ctx.handle)
+        opt = _lib.ma_index_options(kmer_k, kmer3_k, hbm_budget_bytes)
+        check(lib.ma_index_open(ctx.handle, fspath(prefix), C.byref(opt), C.byref(h)), ctx.handle)
         self.handle = h
         self.ctx = ctx
         info = ma_index_info()

@@ -29,10 +29,10 @@ def ctx():
 _INDEX_CACHE = {}
 
 
-def gpu_index(ctx, prefix, k):
-    key = (str(prefix), k)
+def gpu_index(ctx, prefix, k, k3=0):
+    key = (str(prefix), k, k3)
     if key not in _INDEX_CACHE:
-        _INDEX_CACHE[key] = GpuIndex(ctx, prefix, kmer_k=k)
+        _INDEX_CACHE[key] = GpuIndex(ctx, prefix, kmer_k=k, kmer3_k=k3)
     return _INDEX_CACHE[key]
 
 
@@ -41,8 +41,8 @@ def gpu_index(ctx, prefix, k):
 TUNINGS = [(0, 1, 0), (1, 1, 0), (1, 3, 1)]
 
 
-def compare(prefix, ctx, bases, lens, n1, paired, max_len, params, k=12, bs=(1, 2), tunings=TUNINGS):
-    gi = gpu_index(ctx, prefix, k)
+def compare(prefix, ctx, bases, lens, n1, paired, max_len, params, k=12, bs=(1, 2), tunings=TUNINGS, k3=12):
+    gi = gpu_index(ctx, prefix, k, k3)
     o = oracle.OracleIndex(prefix).map(bases, lens, n1, paired, max_len, bs[0], bs[1], params.as_list())
     g = None
     for tu in tunings:
@@ -77,11 +77,11 @@ def test_paired_end_with_rescue(ctx, small_ref):
     compare(prefix, ctx, rb.bases, rb.lens, rb.n1, True, 150, BENCH_PARAMS)
 
 
-@pytest.mark.parametrize("k", [0, 10, 12])
-def test_kmer_table_is_exact(ctx, small_ref, k):
+@pytest.mark.parametrize("k,k3", [(0, 0), (10, 0), (12, 0), (0, 12), (12, 9), (0, 19)])
+def test_kmer_tables_are_exact(ctx, small_ref, k, k3):
     fa, prefix = small_ref
-    rb = sim(fa, 5000, False, seed=3, sub_rate=0.01)
-    compare(prefix, ctx, rb.bases, rb.lens, rb.n1, False, 150, BENCH_PARAMS, k=k)
+    rb = sim(fa, 5000, True, seed=3, sub_rate=0.01)
+    compare(prefix, ctx, rb.bases, rb.lens, rb.n1, True, 150, BENCH_PARAMS, k=k, k3=k3)
 
 
 def test_high_error_soft_clips_and_deletions(ctx, small_ref):
@@ -214,4 +214,5 @@ def test_toy_fixture_shape(ctx, tmp_path):
     bases = np.stack([read, read])
     lens = np.array([32, 32], np.uint32)
     for p in (FmParams(), FmParams(seed_len=19), FmParams(seed_len=8, max_occ=4096)):
-        compare(prefix, ctx, bases, lens, 1, True, 32, p, k=0)
+        compare(prefix, ctx, bases, lens, 1, True, 32, p, k=0, k3=0)
+        compare(prefix, ctx, bases, lens, 1, True, 32, p, k=4, k3=8)
