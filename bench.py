@@ -232,6 +232,15 @@ def run_ours(args, rank, world, local):
     gi = GpuIndex(ctx, prefix, kmer_k=args.kmer, kmer3_k=args.kmer3)
     open_s = time.time() - t
 
+    # ---- result-neutral kernel choices picked on a sample of the batch ----
+    from mojoalign_b200.autotune import autotune
+
+    ns = min(args.pairs, 1_000_000)
+    tb = np.concatenate([rb.bases[:ns], rb.bases[args.pairs:args.pairs + ns]])
+    tl = np.concatenate([rb.lens[:ns], rb.lens[args.pairs:args.pairs + ns]])
+    tune = autotune(ctx, gi, tb, tl, ns, True, READ_LEN, "C2T", "G2A", params)
+    del tb, tl
+
     # ---- device-resident inputs and outputs ----
     d_bases = pinned.to(f"cuda:{local}").reshape(-1)
     d_lens = lens_pinned.to(f"cuda:{local}")
@@ -318,6 +327,7 @@ def run_ours(args, rank, world, local):
                        "reads_per_gpu": n_seq, "read_len": READ_LEN, "paired": True,
                        "params": dict(zip(["seed_len", "seed_stride", "max_occ", "max_diff", "max_soft", "max_adj",
                                            "rescue_win"], params.as_list())),
+                       "tuning": tune.tuning, "autotune_sample_reads": 2 * ns,
                        "kmer_k": args.kmer, "kmer3_k": args.kmer3, "index_hbm_bytes": int(gi.info.device_bytes),
                        "l2": "inputs larger than L2 (reads and index several GB)",
                        "mapped_frac": round(mapped, 4)},
@@ -327,6 +337,7 @@ def run_ours(args, rank, world, local):
             "gpu_launches": launches, "roofline": roof, "clocks": clk,
             "setup_s": {"reference_and_index": round(prep_s, 1), "reads": round(sim_s, 1),
                         "index_open": round(open_s, 1)}}
+    line["autotune"] = tune.all_ms
     if rank == 0:
         line["gather_roofline"] = {}
         for lb in (32, 64):

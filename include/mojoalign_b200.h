@@ -223,11 +223,15 @@ int ma_last_launch_count(const ma_ctx* ctx);
  *   stage1_endpoints      endpoints stage 1 covers (default 1).
  *   stage2_blocks_per_sm  persistent blocks per SM for stage 2 (0 = the
  *                         occupancy maximum).
+ *   reg_level             register budget of the seed kernels: 0 = the
+ *                         compiler's choice, 1 = 80 registers (default),
+ *                         2 = 64 registers.
  */
 typedef struct ma_tuning {
     int32_t seed_kernel;
     int32_t stage1_endpoints;
     int32_t stage2_blocks_per_sm;
+    int32_t reg_level;
 } ma_tuning;
 int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t);
 int ma_ctx_get_tuning(const ma_ctx* ctx, ma_tuning* t);

@@ -16,13 +16,13 @@ namespace ma {
 int launch_pack(const uint8_t* d_bases, const uint32_t* d_lens, int64_t n_seq, int64_t n1, int max_len, int words,
                 int bs_r1, int bs_r2, uint64_t* d_packed, int* d_err, cudaStream_t st);
 int launch_seed_extend(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
-                       unsigned long long* d_tally, cudaStream_t st);
+                       unsigned long long* d_tally, int level, cudaStream_t st);
 double run_gather_bench(uint64_t buffer_bytes, int line_bytes, uint64_t n_loads, int sm_count, cudaStream_t st);
 size_t two_stage_scratch_bytes(int64_t n_seq);
 int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
-                          int stage1_endpoints, int stage2_blocks, void* scratch, unsigned long long* d_tally,
-                          cudaEvent_t mid, cudaStream_t st);
-int stage2_blocks_per_sm();
+                          int stage1_endpoints, int stage2_blocks, int level, void* scratch,
+                          unsigned long long* d_tally, cudaEvent_t mid, cudaStream_t st);
+int stage2_blocks_per_sm(int level, bool counting);
 int launch_rescue(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int64_t n_pairs,
                   cudaStream_t st);
 }  // namespace ma
@@ -75,7 +75,7 @@ struct ma_ctx {
     uint64_t traffic[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     bool rescue_ran = false;
     DevBuf tally;
-    ma_tuning tuning{1, 1, 0};
+    ma_tuning tuning{1, 1, 0, 1};
     int sm_count = 0;
     DevBuf seed_scratch;
     DevBuf bases, lens, packed, err_flag;
@@ -158,13 +158,15 @@ void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const
     if (timed) ck(cudaEventRecord(ctx->ev[1], st), "event");
     DevReads R{ctx->packed.as<uint64_t>(), d_lens, words, n_seq};
     DevParams P = to_dev(p);
+    const int level = ctx->tuning.reg_level;
     if (ctx->tuning.seed_kernel == 0) {
-        launches += launch_seed_extend(idx->dix, R, P, out, d_tally, st);
+        launches += launch_seed_extend(idx->dix, R, P, out, d_tally, level, st);
     } else {
         ctx->seed_scratch.ensure(two_stage_scratch_bytes(n_seq));
-        const int bps = ctx->tuning.stage2_blocks_per_sm > 0 ? ctx->tuning.stage2_blocks_per_sm : stage2_blocks_per_sm();
+        const int bps = ctx->tuning.stage2_blocks_per_sm > 0 ? ctx->tuning.stage2_blocks_per_sm
+                                                             : stage2_blocks_per_sm(level, d_tally != nullptr);
         launches += launch_seed_two_stage(idx->dix, R, P, out, ctx->tuning.stage1_endpoints, bps * ctx->sm_count,
-                                          ctx->seed_scratch.p, d_tally, timed ? ctx->ev[4] : nullptr, st);
+                                          level, ctx->seed_scratch.p, d_tally, timed ? ctx->ev[4] : nullptr, st);
     }
     if (timed) ck(cudaEventRecord(ctx->ev[2], st), "event");
     ctx->rescue_ran = paired && p->rescue_win > 0;
@@ -454,6 +456,7 @@ int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t) {
         if (t->seed_kernel < 0 || t->seed_kernel > 1) fail(MA_ERR_ARG, "seed_kernel must be 0 or 1");
         if (t->stage1_endpoints < 1) fail(MA_ERR_ARG, "stage1_endpoints must be >= 1");
         if (t->stage2_blocks_per_sm < 0 || t->stage2_blocks_per_sm > 64) fail(MA_ERR_ARG, "bad stage2_blocks_per_sm");
+        if (t->reg_level < 0 || t->reg_level > 2) fail(MA_ERR_ARG, "reg_level must be 0, 1 or 2");
         ctx->tuning = *t;
     });
 }

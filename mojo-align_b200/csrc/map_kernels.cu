@@ -577,8 +577,8 @@ __device__ __forceinline__ void flush_tally(const Tally& t, unsigned long long* 
 // whose best hit is not nm == 0 and that has endpoints left is handed to
 // stage 2 with its running best and the loci it evaluated.  With
 // ep_limit >= every read's endpoint count this is the whole algorithm.
-template <bool S>
-__global__ void __launch_bounds__(128) seed_stage1_kernel(DevIndex ix, DevReads R, DevParams P, DevOut out,
+template <bool S, int MINB>
+__global__ void __launch_bounds__(128, MINB) seed_stage1_kernel(DevIndex ix, DevReads R, DevParams P, DevOut out,
                                                           int ep_limit, Handoff h,
                                                           unsigned long long* __restrict__ tally_out) {
     const int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
@@ -675,8 +675,8 @@ __device__ __forceinline__ uint64_t warp_min64(uint64_t v) {
 // shift) pair is evaluated by one lane.  The warp minimum of the (nm,
 // ordinal) keys is folded into the read's running best.  The read stops
 // after the group of endpoints in which an nm == 0 hit appears.
-template <bool S>
-__global__ void __launch_bounds__(S2_WARPS * 32) seed_stage2_kernel(DevIndex ix, DevReads R, DevParams P,
+template <bool S, int MINB>
+__global__ void __launch_bounds__(S2_WARPS * 32, MINB) seed_stage2_kernel(DevIndex ix, DevReads R, DevParams P,
                                                                     DevOut out, int ep_start, Handoff h,
                                                                     unsigned long long* __restrict__ tally_out) {
     __shared__ uint64_t s_words_all[S2_WARPS][4 * MAX_WORDS];
@@ -928,13 +928,52 @@ int launch_pack(const uint8_t* d_bases, const uint32_t* d_lens, int64_t n_seq, i
     return 1;
 }
 
+// Register budgets of the seed kernels (result-neutral): level 0 leaves the
+// compiler free (about 120 registers), level 1 asks for 3 stage-2 / 6
+// stage-1 blocks per SM (80 registers), level 2 for 4 / 8 (64 registers,
+// with spills to L1).
+template <bool S, int L>
+struct SeedKernels {
+    static constexpr int B1 = L == 0 ? 1 : (L == 1 ? 6 : 8);
+    static constexpr int B2 = L == 0 ? 1 : (L == 1 ? 3 : 4);
+    static void stage1(dim3 g, cudaStream_t st, const DevIndex& ix, const DevReads& R, const DevParams& P,
+                       const DevOut& out, int ep, const Handoff& h, unsigned long long* tally) {
+        seed_stage1_kernel<S, B1><<<g, 128, 0, st>>>(ix, R, P, out, ep, h, tally);
+    }
+    static void stage2(dim3 g, cudaStream_t st, const DevIndex& ix, const DevReads& R, const DevParams& P,
+                       const DevOut& out, int ep, const Handoff& h, unsigned long long* tally) {
+        seed_stage2_kernel<S, B2><<<g, S2_WARPS * 32, 0, st>>>(ix, R, P, out, ep, h, tally);
+    }
+    static int stage2_occupancy() {
+        int nb = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, seed_stage2_kernel<S, B2>, S2_WARPS * 32, 0);
+        return nb > 0 ? nb : 1;
+    }
+};
+
+template <bool S>
+void launch_levels(int level, bool second, dim3 g, cudaStream_t st, const DevIndex& ix, const DevReads& R,
+                   const DevParams& P, const DevOut& out, int ep, const Handoff& h, unsigned long long* tally) {
+    if (level == 1) {
+        second ? SeedKernels<S, 1>::stage2(g, st, ix, R, P, out, ep, h, tally)
+               : SeedKernels<S, 1>::stage1(g, st, ix, R, P, out, ep, h, tally);
+    } else if (level == 2) {
+        second ? SeedKernels<S, 2>::stage2(g, st, ix, R, P, out, ep, h, tally)
+               : SeedKernels<S, 2>::stage1(g, st, ix, R, P, out, ep, h, tally);
+    } else {
+        second ? SeedKernels<S, 0>::stage2(g, st, ix, R, P, out, ep, h, tally)
+               : SeedKernels<S, 0>::stage1(g, st, ix, R, P, out, ep, h, tally);
+    }
+}
+
 int launch_seed_extend(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
-                       unsigned long long* d_tally, cudaStream_t st) {
+                       unsigned long long* d_tally, int level, cudaStream_t st) {
     Handoff none{};
+    const dim3 g(grid_for(R.n_seq, 128));
     if (d_tally)
-        seed_stage1_kernel<true><<<grid_for(R.n_seq, 128), 128, 0, st>>>(ix, R, P, out, 1 << 30, none, d_tally);
+        SeedKernels<true, 0>::stage1(g, st, ix, R, P, out, 1 << 30, none, d_tally);
     else
-        seed_stage1_kernel<false><<<grid_for(R.n_seq, 128), 128, 0, st>>>(ix, R, P, out, 1 << 30, none, nullptr);
+        launch_levels<false>(level, false, g, st, ix, R, P, out, 1 << 30, none, nullptr);
     return 1;
 }
 
@@ -947,8 +986,8 @@ size_t two_stage_scratch_bytes(int64_t n_seq) {
 }
 
 int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
-                          int stage1_endpoints, int stage2_blocks, void* scratch, unsigned long long* d_tally,
-                          cudaEvent_t mid, cudaStream_t st) {
+                          int stage1_endpoints, int stage2_blocks, int level, void* scratch,
+                          unsigned long long* d_tally, cudaEvent_t mid, cudaStream_t st) {
     const size_t n = static_cast<size_t>(R.n_seq);
     char* p = static_cast<char*>(scratch);
     Handoff h;
@@ -962,24 +1001,24 @@ int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams
     p += ((n + 255) / 256) * 256;
     h.pending = reinterpret_cast<uint32_t*>(p);
     cudaMemsetAsync(h.counters, 0, 256, st);
+    const dim3 g1(grid_for(R.n_seq, 128)), g2(stage2_blocks);
     if (d_tally) {
-        seed_stage1_kernel<true><<<grid_for(R.n_seq, 128), 128, 0, st>>>(ix, R, P, out, stage1_endpoints, h, d_tally);
+        SeedKernels<true, 0>::stage1(g1, st, ix, R, P, out, stage1_endpoints, h, d_tally);
         if (mid) cudaEventRecord(mid, st);
-        seed_stage2_kernel<true><<<stage2_blocks, S2_WARPS * 32, 0, st>>>(ix, R, P, out, stage1_endpoints, h, d_tally);
+        SeedKernels<true, 0>::stage2(g2, st, ix, R, P, out, stage1_endpoints, h, d_tally);
     } else {
-        seed_stage1_kernel<false><<<grid_for(R.n_seq, 128), 128, 0, st>>>(ix, R, P, out, stage1_endpoints, h,
-                                                                         nullptr);
+        launch_levels<false>(level, false, g1, st, ix, R, P, out, stage1_endpoints, h, nullptr);
         if (mid) cudaEventRecord(mid, st);
-        seed_stage2_kernel<false><<<stage2_blocks, S2_WARPS * 32, 0, st>>>(ix, R, P, out, stage1_endpoints, h,
-                                                                          nullptr);
+        launch_levels<false>(level, true, g2, st, ix, R, P, out, stage1_endpoints, h, nullptr);
     }
     return 2;
 }
 
-int stage2_blocks_per_sm() {
-    int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, seed_stage2_kernel<false>, S2_WARPS * 32, 0);
-    return nb > 0 ? nb : 1;
+int stage2_blocks_per_sm(int level, bool counting) {
+    if (counting) return SeedKernels<true, 0>::stage2_occupancy();
+    if (level == 1) return SeedKernels<false, 1>::stage2_occupancy();
+    if (level == 2) return SeedKernels<false, 2>::stage2_occupancy();
+    return SeedKernels<false, 0>::stage2_occupancy();
 }
 
 int launch_rescue(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int64_t n_pairs,

@@ -1,0 +1,73 @@
+"""Autotuner for the result-neutral execution choices of the seed kernels.
+
+Sweeps the kernel form (one thread per read, or two stages), the number of
+right endpoints stage 1 covers, the seed kernels' register budget and the
+persistent stage-2 grid, on a sample batch.  Every candidate must produce
+identical outputs (checked here); the fastest by device time wins.
+
+The seed stride is not swept: it decides which right endpoints are tried
+(linear_gpu_fm.mojo:1828) and so changes results.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .mapper import GpuContext, GpuIndex, MapResult, map_batch
+from .params import FmParams
+
+DEFAULT_CANDIDATES = [
+    (0, 1, 0, 0),
+    (0, 1, 0, 1),
+    (1, 1, 0, 0),
+    (1, 1, 0, 1),
+    (1, 1, 0, 2),
+    (1, 2, 0, 0),
+    (1, 2, 0, 1),
+    (1, 2, 0, 2),
+    (1, 3, 0, 1),
+    (1, 1, 2, 1),
+    (1, 2, 2, 1),
+]
+FIELDS = ("seed_kernel", "stage1_endpoints", "stage2_blocks_per_sm", "reg_level")
+
+
+@dataclass
+class TuneResult:
+    tuning: dict
+    seed_ms: float
+    all_ms: list
+
+
+def autotune(ctx: GpuContext, index: GpuIndex, bases: np.ndarray, lens: np.ndarray, n1: int, paired: bool,
+             max_len: int, bs_r1="C2T", bs_r2="G2A", params: FmParams | None = None, candidates=None,
+             reps: int = 2) -> TuneResult:
+    params = params or FmParams()
+    candidates = candidates or DEFAULT_CANDIDATES
+    n_seq = n1 * (2 if paired else 1)
+    ref = None
+    timings = []
+    ctx.set_profiling(1)
+    try:
+        for cand in candidates:
+            ctx.set_tuning(*cand)
+            res = MapResult.empty(n_seq, debug=True)
+            map_batch(ctx, index, bases, lens, n1, paired, max_len, bs_r1, bs_r2, params, out=res)
+            if ref is None:
+                ref = res
+            else:
+                for f in MapResult.FIELDS + MapResult.DEBUG:
+                    if not np.array_equal(getattr(res, f), getattr(ref, f)):
+                        raise AssertionError(f"tuning {cand} changed output {f}; the kernels are not result-neutral")
+            ms = []
+            for _ in range(reps):
+                map_batch(ctx, index, bases, lens, n1, paired, max_len, bs_r1, bs_r2, params, out=res)
+                ms.append(ctx.kernel_ms()[1])
+            timings.append((min(ms), cand))
+    finally:
+        ctx.set_profiling(0)
+    best_ms, best = min(timings)
+    ctx.set_tuning(*best)
+    return TuneResult(dict(zip(FIELDS, best)), best_ms,
+                      [{"tuning": dict(zip(FIELDS, c)), "seed_ms": round(t, 3)} for t, c in timings])

@@ -36,9 +36,10 @@ def gpu_index(ctx, prefix, k, k3=0):
     return _INDEX_CACHE[key]
 
 
-# Result-neutral kernel forms: one thread per read; two stages with the
-# first 1 or 3 right endpoints in stage 1.
-TUNINGS = [(0, 1, 0), (1, 1, 0), (1, 3, 1)]
+# Result-neutral kernel forms (seed_kernel, stage1_endpoints,
+# stage2_blocks_per_sm, reg_level): one thread per read; two stages with
+# the first 1, 2 or 3 right endpoints in stage 1, at each register budget.
+TUNINGS = [(0, 1, 0, 0), (1, 1, 0, 1), (1, 3, 1, 2), (1, 2, 0, 0)]
 
 
 def compare(prefix, ctx, bases, lens, n1, paired, max_len, params, k=12, bs=(1, 2), tunings=TUNINGS, k3=12):
