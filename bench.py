@@ -53,6 +53,8 @@ def parse_args():
     ap.add_argument("--workdir", default=os.environ.get("MOJOALIGN_BENCH_DIR", tempfile.gettempdir()))
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the oracle timing (profiling runs)")
+    ap.add_argument("--tuning", default="", help="fixed kernel choice 'seed_kernel,stage1_endpoints,"
+                    "stage2_blocks_per_sm,reg_level' instead of the autotuner")
     return ap.parse_args()
 
 
@@ -238,7 +240,15 @@ def run_ours(args, rank, world, local):
     ns = min(args.pairs, 1_000_000)
     tb = np.concatenate([rb.bases[:ns], rb.bases[args.pairs:args.pairs + ns]])
     tl = np.concatenate([rb.lens[:ns], rb.lens[args.pairs:args.pairs + ns]])
-    tune = autotune(ctx, gi, tb, tl, ns, True, READ_LEN, "C2T", "G2A", params)
+    if args.tuning:
+        from mojoalign_b200.autotune import FIELDS, TuneResult
+
+        fixed = [int(x) for x in args.tuning.split(",")]
+        ctx.set_tuning(*fixed)
+        tune = TuneResult(dict(zip(FIELDS, fixed)), float("nan"), [])
+        ns = 0
+    else:
+        tune = autotune(ctx, gi, tb, tl, ns, True, READ_LEN, "C2T", "G2A", params)
     del tb, tl
 
     # ---- device-resident inputs and outputs ----
