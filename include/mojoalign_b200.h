@@ -106,8 +106,9 @@ typedef struct ma_index_info {
     int64_t sa_intv;       /* SA sampling interval of the .sa file           */
     int64_t n_sa;          /* (seq_len + sa_intv) / sa_intv                  */
     int64_t n_contigs;     /* .ann records (f<name> and r<name>)             */
-    uint64_t sa_reject_below; /* smallest text position reachable by the
-                                 reference's sampled-SA walk (see DESIGN) */
+    uint64_t sa_reject_below; /* text positions below this are rejected by
+                                 the reference's sampled-SA walk (it reaches
+                                 the first text row unsampled) */
     int32_t kmer_k;        /* k of the resident k-mer interval table         */
     int32_t kmer3_k;       /* k of the converted-alphabet k-mer tables       */
     uint64_t device_bytes; /* HBM held by this index                         */
