@@ -210,6 +210,28 @@ int ma_map_batch_device(ma_ctx* ctx, const ma_index* idx,
                         int bs_r2, const ma_params* p, ma_hits* d_out,
                         ma_debug* d_dbg, void* stream);
 
+/*
+ * Same computation as ma_map_batch_device, with no device allocation.  No
+ * counterpart in the reference (its batch step allocates through its
+ * DeviceContext).  For callers that must not let the library call
+ * cudaMalloc: a framework whose caching allocator already holds the free
+ * HBM, or a latency-bound serving loop sharing the GPU with other streams,
+ * where cudaMalloc's implicit device synchronisation would stall them.
+ * Inputs and outputs stay the caller's device buffers; scratch comes from
+ * one fixed file-scope device array (about 11 MiB, held on every GPU that
+ * loads the library until exit).  Limits: at most 32768 reads per call
+ * (16384 pairs) of at most 256 bases; larger calls fail with MA_ERR_ARG.
+ * The first call on a device looks up the array's device address; make it
+ * before any stream capture.  Calls share the array: calls whose kernels
+ * overlap on the GPU race.  Synchronous on `stream` (a cudaStream_t, NULL
+ * = the legacy default stream); errors are reported by ma_last_error(NULL).
+ */
+int ma_map_batch_device_noalloc(const ma_index* idx, const uint8_t* d_bases,
+                                const uint32_t* d_lens, uint32_t n1,
+                                int paired, uint32_t max_len, int bs_r1,
+                                int bs_r2, const ma_params* p, ma_hits* d_out,
+                                ma_debug* d_dbg, void* stream);
+
 /* Number of kernel launches the last mapping call on ctx issued. */
 int ma_last_launch_count(const ma_ctx* ctx);
 

@@ -35,8 +35,6 @@ using namespace ma;
 
 namespace {
 
-thread_local std::string t_err;
-
 void ck(cudaError_t e, const char* what) {
     if (e != cudaSuccess) fail(MA_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
@@ -90,6 +88,25 @@ struct ma_index {
     ma_index_info info{};
     std::vector<Contig> contigs;
 };
+
+namespace ma {
+// Device view and device ordinal of a resident index, for entry points
+// defined in other translation units.
+const DevIndex* index_device_view(const ma_index* idx, int* device) {
+    if (!idx || !idx->ctx) return nullptr;
+    if (device) *device = idx->ctx->device;
+    return &idx->dix;
+}
+}  // namespace ma
+
+namespace {
+thread_local std::string t_err;
+}  // namespace
+
+namespace ma {
+// Message returned by ma_last_error(NULL) on this thread.
+void set_thread_error(const std::string& msg) { t_err = msg; }
+}  // namespace ma
 
 namespace {
 

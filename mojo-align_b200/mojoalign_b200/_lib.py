@@ -140,6 +140,9 @@ SIGNATURES = [
     ("ma_map_batch_device", C.c_int,
      [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_uint32, C.c_int, C.c_int,
       C.POINTER(ma_params), C.POINTER(ma_hits), C.POINTER(ma_debug), C.c_void_p]),
+    ("ma_map_batch_device_noalloc", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_uint32, C.c_int, C.c_int,
+      C.POINTER(ma_params), C.POINTER(ma_hits), C.POINTER(ma_debug), C.c_void_p]),
     ("ma_last_launch_count", C.c_int, [C.c_void_p]),
     ("ma_ctx_set_profiling", C.c_int, [C.c_void_p, C.c_int]),
     ("ma_ctx_set_tuning", C.c_int, [C.c_void_p, C.POINTER(ma_tuning)]),
