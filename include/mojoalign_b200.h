@@ -249,12 +249,16 @@ int ma_last_launch_count(const ma_ctx* ctx);
  *   reg_level             register budget of the seed kernels: 0 = the
  *                         compiler's choice, 1 = 80 registers (default),
  *                         2 = 64 registers.
+ *   stage1_max_rows       stage 1 hands a read to stage 2 as soon as one of
+ *                         its seeds has more SA rows than this (1..16,
+ *                         default 2; 16 = never).
  */
 typedef struct ma_tuning {
     int32_t seed_kernel;
     int32_t stage1_endpoints;
     int32_t stage2_blocks_per_sm;
     int32_t reg_level;
+    int32_t stage1_max_rows;
 } ma_tuning;
 int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t);
 int ma_ctx_get_tuning(const ma_ctx* ctx, ma_tuning* t);

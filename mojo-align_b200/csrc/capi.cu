@@ -20,7 +20,7 @@ int launch_seed_extend(const DevIndex& ix, const DevReads& R, const DevParams& P
 double run_gather_bench(uint64_t buffer_bytes, int line_bytes, uint64_t n_loads, int sm_count, cudaStream_t st);
 size_t two_stage_scratch_bytes(int64_t n_seq);
 int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
-                          int stage1_endpoints, int stage2_blocks, int level, void* scratch,
+                          int stage1_endpoints, int stage1_max_rows, int stage2_blocks, int level, void* scratch,
                           unsigned long long* d_tally, cudaEvent_t mid, cudaStream_t st);
 int stage2_blocks_per_sm(int level, bool counting);
 int launch_rescue(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int64_t n_pairs,
@@ -73,7 +73,7 @@ struct ma_ctx {
     uint64_t traffic[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     bool rescue_ran = false;
     DevBuf tally;
-    ma_tuning tuning{1, 1, 0, 1};
+    ma_tuning tuning{1, 1, 0, 1, 2};
     int sm_count = 0;
     DevBuf seed_scratch;
     DevBuf bases, lens, packed, err_flag;
@@ -182,8 +182,9 @@ void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const
         ctx->seed_scratch.ensure(two_stage_scratch_bytes(n_seq));
         const int bps = ctx->tuning.stage2_blocks_per_sm > 0 ? ctx->tuning.stage2_blocks_per_sm
                                                              : stage2_blocks_per_sm(level, d_tally != nullptr);
-        launches += launch_seed_two_stage(idx->dix, R, P, out, ctx->tuning.stage1_endpoints, bps * ctx->sm_count,
-                                          level, ctx->seed_scratch.p, d_tally, timed ? ctx->ev[4] : nullptr, st);
+        launches += launch_seed_two_stage(idx->dix, R, P, out, ctx->tuning.stage1_endpoints,
+                                          ctx->tuning.stage1_max_rows, bps * ctx->sm_count, level,
+                                          ctx->seed_scratch.p, d_tally, timed ? ctx->ev[4] : nullptr, st);
     }
     if (timed) ck(cudaEventRecord(ctx->ev[2], st), "event");
     ctx->rescue_ran = paired && p->rescue_win > 0;
@@ -474,6 +475,7 @@ int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t) {
         if (t->stage1_endpoints < 1) fail(MA_ERR_ARG, "stage1_endpoints must be >= 1");
         if (t->stage2_blocks_per_sm < 0 || t->stage2_blocks_per_sm > 64) fail(MA_ERR_ARG, "bad stage2_blocks_per_sm");
         if (t->reg_level < 0 || t->reg_level > 2) fail(MA_ERR_ARG, "reg_level must be 0, 1 or 2");
+        if (t->stage1_max_rows < 1 || t->stage1_max_rows > 16) fail(MA_ERR_ARG, "stage1_max_rows must be in 1..16");
         ctx->tuning = *t;
     });
 }

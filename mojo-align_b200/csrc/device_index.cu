@@ -189,7 +189,8 @@ __global__ void fill_empty_kernel(uint2* __restrict__ t, uint64_t n) {
 // Rows with the same k-mer are contiguous in SA order; the first and last
 // row of each run are the interval (k, l) of that k-mer.
 __global__ void kmer3_bounds_kernel(const uint64_t* __restrict__ codes, uint64_t n_rows, int K,
-                                    uint2* __restrict__ t_agt, uint2* __restrict__ t_act) {
+                                    uint2* __restrict__ t_agt, uint2* __restrict__ t_act,
+                                    const uint32_t* __restrict__ sa, uint32_t* __restrict__ uniq) {
     const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     if (i >= n_rows) return;
     const uint64_t c = codes[i];
@@ -197,6 +198,10 @@ __global__ void kmer3_bounds_kernel(const uint64_t* __restrict__ codes, uint64_t
     const bool start = i == 0 || codes[i - 1] != c;
     const bool end = i + 1 == n_rows || codes[i + 1] != c;
     if (!start && !end) return;
+    if (start && end) {  // a k-mer with a single occurrence
+        const uint32_t p = sa[i];
+        atomicOr(uniq + (p >> 5), 1u << (p & 31));
+    }
     const uint64_t lo = c & kEven, hi = (c >> 1) & kEven;
     const bool has_c = (lo & ~hi) != 0, has_g = (hi & ~lo) != 0;
     uint32_t idx = 0;
@@ -234,7 +239,7 @@ uint64_t device_index_bytes(const BwaIndexHost& h, int kmer_k, int kmer3_k) {
     b += (h.seq_len + 1) * 4;
     b += ((h.l_pac + 31) / 32 + 2 * PAC_PAD) * 8;
     if (kmer_k > 0) b += (1ull << (2 * kmer_k)) * 8;
-    if (kmer3_k > 0) b += 2 * pow3(kmer3_k) * 8;
+    if (kmer3_k > 0) b += 2 * pow3(kmer3_k) * 8 + ((h.seq_len + 31) / 32) * 4;
     b += h.contigs.size() * 12;
     return b;
 }
@@ -347,13 +352,15 @@ DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, int kmer3_k, cuda
             const uint64_t n3 = pow3(kmer3_k), n_rows = h.seq_len + 1;
             check(cudaMalloc(&bufs.kmer3[0], n3 * 8), "cudaMalloc kmer3");
             check(cudaMalloc(&bufs.kmer3[1], n3 * 8), "cudaMalloc kmer3");
+            check(cudaMalloc(&bufs.uniq, ((h.seq_len + 31) / 32) * 4), "cudaMalloc uniq");
+            check(cudaMemsetAsync(bufs.uniq, 0, ((h.seq_len + 31) / 32) * 4, st), "memset uniq");
             uint64_t* d_codes = nullptr;
             check(cudaMalloc(&d_codes, n_rows * 8), "cudaMalloc kmer3 staging");
             fill_empty_kernel<<<4096, 256, 0, st>>>(bufs.kmer3[0], n3);
             fill_empty_kernel<<<4096, 256, 0, st>>>(bufs.kmer3[1], n3);
             kmer3_rows_kernel<<<grid_for(n_rows, 256), 256, 0, st>>>(ix, kmer3_k, n_rows, d_codes);
             kmer3_bounds_kernel<<<grid_for(n_rows, 256), 256, 0, st>>>(d_codes, n_rows, kmer3_k, bufs.kmer3[0],
-                                                                       bufs.kmer3[1]);
+                                                                       bufs.kmer3[1], bufs.sa, bufs.uniq);
             cudaError_t le = cudaGetLastError();
             cudaError_t se = cudaStreamSynchronize(st);
             cudaFree(d_codes);
@@ -361,6 +368,7 @@ DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, int kmer3_k, cuda
             check(se, "kmer3 tables");
             ix.kmer3[0] = bufs.kmer3[0];
             ix.kmer3[1] = bufs.kmer3[1];
+            ix.uniq = bufs.uniq;
             ix.kmer3_k = kmer3_k;
         }
         check(cudaStreamSynchronize(st), "index preparation");
@@ -380,6 +388,7 @@ void free_device_index(DeviceIndexBuffers& b) {
     cudaFree(b.kmer);
     cudaFree(b.kmer3[0]);
     cudaFree(b.kmer3[1]);
+    cudaFree(b.uniq);
     cudaFree(b.coff);
     cudaFree(b.clen);
     b = DeviceIndexBuffers{};

@@ -18,6 +18,8 @@
 //         reads, indexed in base 3: table 0 holds the words without C
 //         (A, G, T -> digits 0, 1, 2; C->T reads), table 1 the words
 //         without G (A, C, T -> 0, 1, 2; G->A reads).
+//   uniq  one bit per text position p of T (pac + reverse complement): the
+//         kmer3_k-mer T[p, p+k) occurs exactly once in T.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -43,6 +45,7 @@ struct DevIndex {
     const uint64_t* pacw;
     const uint2* kmer;
     const uint2* kmer3[2];
+    const uint32_t* uniq;  // bit p: the kmer3_k-mer at text position p occurs once
     const uint64_t* coff;
     const uint32_t* clen;
     int64_t n_contigs;
@@ -149,6 +152,7 @@ struct DeviceIndexBuffers {
     uint64_t* pacw = nullptr;
     uint2* kmer = nullptr;
     uint2* kmer3[2] = {nullptr, nullptr};
+    uint32_t* uniq = nullptr;
     uint64_t* coff = nullptr;
     uint32_t* clen = nullptr;
     uint64_t bytes = 0;

@@ -161,6 +161,7 @@ struct Handoff {
     uint64_t* key;       // running best key
     uint64_t* memo;      // [n_seq][MEMO1] loci already evaluated (b0*2+strand)
     uint8_t* memo_n;     // entries used in memo
+    uint16_t* resume;    // first right endpoint stage 2 searches
     uint32_t* pending;   // read ids handed over
     uint32_t* counters;  // [0] pending count, [1] stage-2 work cursor
 };
@@ -579,7 +580,7 @@ __device__ __forceinline__ void flush_tally(const Tally& t, unsigned long long* 
 // ep_limit >= every read's endpoint count this is the whole algorithm.
 template <bool S, int MINB>
 __global__ void __launch_bounds__(128, MINB) seed_stage1_kernel(DevIndex ix, DevReads R, DevParams P, DevOut out,
-                                                          int ep_limit, Handoff h,
+                                                          int ep_limit, int max_rows, Handoff h,
                                                           unsigned long long* __restrict__ tally_out) {
     const int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (r >= R.n_seq) return;
@@ -597,12 +598,18 @@ __global__ void __launch_bounds__(128, MINB) seed_stage1_kernel(DevIndex ix, Dev
     int memo_n = 0;
     const int n_end = endpoint_count(P, qlen);
     const int n_run = n_end < ep_limit ? n_end : ep_limit;
+    int resume = n_run;  // first endpoint stage 2 searches
     if (n_run > 0) {
         const Clamps cl = clamps_for(P, qlen);
         for (int ei = 0; ei < n_run; ++ei) {
             const int e = P.seed_len - 1 + ei * P.seed_stride;
             const Seed sd = search_endpoint<S>(ix, rd, e, P, t);
             if (!sd.found) continue;
+            if (h.pending && sd.l - sd.k >= static_cast<uint64_t>(max_rows)) {
+                // many SA rows: stage 2 spreads them over a warp
+                resume = ei;
+                break;
+            }
             for (uint64_t hi = sd.k; hi <= sd.l; ++hi) {
                 const uint64_t sa_pos = __ldg(ix.sa + hi);
                 if constexpr (S) t.sa_loads++;
@@ -627,9 +634,10 @@ __global__ void __launch_bounds__(128, MINB) seed_stage1_kernel(DevIndex ix, Dev
 done:
     write_hit(out, r, best, qlen);
     {
-        const bool pend = h.pending && (best.key >> ORD_SHIFT) != 0 && n_end > n_run;
+        const bool pend = h.pending && (best.key >> ORD_SHIFT) != 0 && n_end > resume;
         if (pend) {
             h.key[r] = best.key;
+            h.resume[r] = static_cast<uint16_t>(resume);
             const int mn = memo_n < MEMO1 ? memo_n : MEMO1;
             for (int i = 0; i < mn; ++i) h.memo[r * MEMO1 + i] = static_cast<uint64_t>(memo_b0[i]);
             h.memo_n[r] = static_cast<uint8_t>(mn);
@@ -675,9 +683,38 @@ __device__ __forceinline__ uint64_t warp_min64(uint64_t v) {
 // shift) pair is evaluated by one lane.  The warp minimum of the (nm,
 // ordinal) keys is folded into the read's running best.  The read stops
 // after the group of endpoints in which an nm == 0 hit appears.
+// An endpoint whose seed window (seed_len bases ending at e) matches the
+// text exactly at an evaluated locus, and whose kmer3_k-mer there occurs
+// once in the text, would give the reference a unique interval at
+// mlen = seed_len resolving to that same locus: a duplicate that cannot win.
+// Such endpoints are skipped without touching the index.
+__device__ __forceinline__ bool predicted_duplicate(const DevIndex& ix, const ReadView& rd, int e, int seed_len,
+                                                    const uint64_t* memo, int n_check) {
+    const int n = seed_len, qlen = rd.qlen;
+    const int s0 = e - n + 1;
+    if (window_bits(rd.nf, s0, n) != 0) return false;
+    const uint64_t mask = n >= 32 ? ~0ull : ((1ull << (2 * n)) - 1);
+    const uint64_t wf = window_bits(rd.fwd, s0, n);
+    const uint64_t wr = window_bits(rd.rc, qlen - 1 - e, n);
+    const int64_t L = static_cast<int64_t>(ix.l_pac);
+    const int Ku = ix.kmer3_k;
+    for (int m = 0; m < n_check; ++m) {
+        const int64_t tag = static_cast<int64_t>(memo[m]);
+        const int64_t b0 = tag >> 1;
+        const int rev = static_cast<int>(tag & 1);
+        const int64_t tpos = rev ? b0 + qlen - 1 - e : b0 + s0;  // forward text start of the window
+        if (tpos < 0 || tpos + n > L) continue;
+        if (((ref_window(ix.pacw, tpos) & mask) ^ (rev ? wr : wf)) != 0) continue;
+        const uint64_t pu = rev ? static_cast<uint64_t>(2 * L - tpos - Ku)
+                                : static_cast<uint64_t>(b0 + e - Ku + 1);
+        return (__ldg(ix.uniq + (pu >> 5)) >> (pu & 31)) & 1;
+    }
+    return false;
+}
+
 template <bool S, int MINB>
 __global__ void __launch_bounds__(S2_WARPS * 32, MINB) seed_stage2_kernel(DevIndex ix, DevReads R, DevParams P,
-                                                                    DevOut out, int ep_start, Handoff h,
+                                                                    DevOut out, Handoff h,
                                                                     unsigned long long* __restrict__ tally_out) {
     __shared__ uint64_t s_words_all[S2_WARPS][4 * MAX_WORDS];
     __shared__ uint64_t s_memo_all[S2_WARPS][MEMO2];
@@ -715,11 +752,16 @@ __global__ void __launch_bounds__(S2_WARPS * 32, MINB) seed_stage2_kernel(DevInd
         Best win;  // valid when improved
         win.crid = -1;
         bool improved = false;
-        for (int j0 = ep_start; j0 < n_end; j0 += 32) {
+        const bool can_predict = ix.uniq && ix.kmer3_k > 0 && ix.kmer3_k <= P.seed_len && P.seed_len <= 32;
+        for (int j0 = h.resume[r]; j0 < n_end; j0 += 32) {
             const int j = j0 + lane;
             const int e = P.seed_len - 1 + j * P.seed_stride;
             Seed sd{0, 0, -1, false};
-            if (j < n_end) sd = search_endpoint<S>(ix, rd, e, P, t);
+            if (j < n_end) {
+                const bool dup = can_predict && predicted_duplicate(ix, rd, e, P.seed_len, s_memo,
+                                                                    n_memo < 8 ? n_memo : 8);
+                if (!dup) sd = search_endpoint<S>(ix, rd, e, P, t);
+            }
             const int nrows = sd.found ? static_cast<int>(sd.l - sd.k + 1) : 0;
             int incl = nrows;
             for (int o = 1; o < 32; o <<= 1) {
@@ -937,12 +979,12 @@ struct SeedKernels {
     static constexpr int B1 = L == 0 ? 1 : (L == 1 ? 6 : 8);
     static constexpr int B2 = L == 0 ? 1 : (L == 1 ? 3 : 4);
     static void stage1(dim3 g, cudaStream_t st, const DevIndex& ix, const DevReads& R, const DevParams& P,
-                       const DevOut& out, int ep, const Handoff& h, unsigned long long* tally) {
-        seed_stage1_kernel<S, B1><<<g, 128, 0, st>>>(ix, R, P, out, ep, h, tally);
+                       const DevOut& out, int ep, int max_rows, const Handoff& h, unsigned long long* tally) {
+        seed_stage1_kernel<S, B1><<<g, 128, 0, st>>>(ix, R, P, out, ep, max_rows, h, tally);
     }
     static void stage2(dim3 g, cudaStream_t st, const DevIndex& ix, const DevReads& R, const DevParams& P,
-                       const DevOut& out, int ep, const Handoff& h, unsigned long long* tally) {
-        seed_stage2_kernel<S, B2><<<g, S2_WARPS * 32, 0, st>>>(ix, R, P, out, ep, h, tally);
+                       const DevOut& out, int, int, const Handoff& h, unsigned long long* tally) {
+        seed_stage2_kernel<S, B2><<<g, S2_WARPS * 32, 0, st>>>(ix, R, P, out, h, tally);
     }
     static int stage2_occupancy() {
         int nb = 0;
@@ -953,16 +995,17 @@ struct SeedKernels {
 
 template <bool S>
 void launch_levels(int level, bool second, dim3 g, cudaStream_t st, const DevIndex& ix, const DevReads& R,
-                   const DevParams& P, const DevOut& out, int ep, const Handoff& h, unsigned long long* tally) {
+                   const DevParams& P, const DevOut& out, int ep, int max_rows, const Handoff& h,
+                   unsigned long long* tally) {
     if (level == 1) {
-        second ? SeedKernels<S, 1>::stage2(g, st, ix, R, P, out, ep, h, tally)
-               : SeedKernels<S, 1>::stage1(g, st, ix, R, P, out, ep, h, tally);
+        second ? SeedKernels<S, 1>::stage2(g, st, ix, R, P, out, ep, max_rows, h, tally)
+               : SeedKernels<S, 1>::stage1(g, st, ix, R, P, out, ep, max_rows, h, tally);
     } else if (level == 2) {
-        second ? SeedKernels<S, 2>::stage2(g, st, ix, R, P, out, ep, h, tally)
-               : SeedKernels<S, 2>::stage1(g, st, ix, R, P, out, ep, h, tally);
+        second ? SeedKernels<S, 2>::stage2(g, st, ix, R, P, out, ep, max_rows, h, tally)
+               : SeedKernels<S, 2>::stage1(g, st, ix, R, P, out, ep, max_rows, h, tally);
     } else {
-        second ? SeedKernels<S, 0>::stage2(g, st, ix, R, P, out, ep, h, tally)
-               : SeedKernels<S, 0>::stage1(g, st, ix, R, P, out, ep, h, tally);
+        second ? SeedKernels<S, 0>::stage2(g, st, ix, R, P, out, ep, max_rows, h, tally)
+               : SeedKernels<S, 0>::stage1(g, st, ix, R, P, out, ep, max_rows, h, tally);
     }
 }
 
@@ -971,9 +1014,9 @@ int launch_seed_extend(const DevIndex& ix, const DevReads& R, const DevParams& P
     Handoff none{};
     const dim3 g(grid_for(R.n_seq, 128));
     if (d_tally)
-        SeedKernels<true, 0>::stage1(g, st, ix, R, P, out, 1 << 30, none, d_tally);
+        SeedKernels<true, 0>::stage1(g, st, ix, R, P, out, 1 << 30, 16, none, d_tally);
     else
-        launch_levels<false>(level, false, g, st, ix, R, P, out, 1 << 30, none, nullptr);
+        launch_levels<false>(level, false, g, st, ix, R, P, out, 1 << 30, 16, none, nullptr);
     return 1;
 }
 
@@ -982,11 +1025,11 @@ int launch_seed_extend(const DevIndex& ix, const DevReads& R, const DevParams& P
 // `scratch` must hold two_stage_scratch_bytes(n_seq) bytes.
 size_t two_stage_scratch_bytes(int64_t n_seq) {
     const size_t n = static_cast<size_t>(n_seq);
-    return 256 + n * 8 + n * 8 * MEMO1 + ((n + 255) / 256) * 256 + n * 4 + 256;
+    return 256 + n * 8 + n * 8 * MEMO1 + ((n + 255) / 256) * 256 + ((2 * n + 255) / 256) * 256 + n * 4 + 256;
 }
 
 int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
-                          int stage1_endpoints, int stage2_blocks, int level, void* scratch,
+                          int stage1_endpoints, int stage1_max_rows, int stage2_blocks, int level, void* scratch,
                           unsigned long long* d_tally, cudaEvent_t mid, cudaStream_t st) {
     const size_t n = static_cast<size_t>(R.n_seq);
     char* p = static_cast<char*>(scratch);
@@ -999,17 +1042,19 @@ int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams
     p += n * 8 * MEMO1;
     h.memo_n = reinterpret_cast<uint8_t*>(p);
     p += ((n + 255) / 256) * 256;
+    h.resume = reinterpret_cast<uint16_t*>(p);
+    p += ((2 * n + 255) / 256) * 256;
     h.pending = reinterpret_cast<uint32_t*>(p);
     cudaMemsetAsync(h.counters, 0, 256, st);
     const dim3 g1(grid_for(R.n_seq, 128)), g2(stage2_blocks);
     if (d_tally) {
-        SeedKernels<true, 0>::stage1(g1, st, ix, R, P, out, stage1_endpoints, h, d_tally);
+        SeedKernels<true, 0>::stage1(g1, st, ix, R, P, out, stage1_endpoints, stage1_max_rows, h, d_tally);
         if (mid) cudaEventRecord(mid, st);
-        SeedKernels<true, 0>::stage2(g2, st, ix, R, P, out, stage1_endpoints, h, d_tally);
+        SeedKernels<true, 0>::stage2(g2, st, ix, R, P, out, stage1_endpoints, stage1_max_rows, h, d_tally);
     } else {
-        launch_levels<false>(level, false, g1, st, ix, R, P, out, stage1_endpoints, h, nullptr);
+        launch_levels<false>(level, false, g1, st, ix, R, P, out, stage1_endpoints, stage1_max_rows, h, nullptr);
         if (mid) cudaEventRecord(mid, st);
-        launch_levels<false>(level, true, g2, st, ix, R, P, out, stage1_endpoints, h, nullptr);
+        launch_levels<false>(level, true, g2, st, ix, R, P, out, stage1_endpoints, stage1_max_rows, h, nullptr);
     }
     return 2;
 }

@@ -18,19 +18,17 @@ from .mapper import GpuContext, GpuIndex, MapResult, map_batch
 from .params import FmParams
 
 DEFAULT_CANDIDATES = [
-    (0, 1, 0, 0),
-    (0, 1, 0, 1),
-    (1, 1, 0, 0),
-    (1, 1, 0, 1),
-    (1, 1, 0, 2),
-    (1, 2, 0, 0),
-    (1, 2, 0, 1),
-    (1, 2, 0, 2),
-    (1, 3, 0, 1),
-    (1, 1, 2, 1),
-    (1, 2, 2, 1),
+    (0, 1, 0, 1, 16),
+    (1, 1, 0, 1, 2),
+    (1, 1, 0, 2, 2),
+    (1, 1, 0, 2, 1),
+    (1, 1, 0, 2, 4),
+    (1, 1, 0, 2, 16),
+    (1, 2, 0, 2, 2),
+    (1, 1, 0, 0, 2),
+    (1, 1, 3, 2, 2),
 ]
-FIELDS = ("seed_kernel", "stage1_endpoints", "stage2_blocks_per_sm", "reg_level")
+FIELDS = ("seed_kernel", "stage1_endpoints", "stage2_blocks_per_sm", "reg_level", "stage1_max_rows")
 
 
 @dataclass

@@ -45,9 +45,9 @@ class GpuContext:
         return lib.ma_last_launch_count(self.handle)
 
     def set_tuning(self, seed_kernel: int = 1, stage1_endpoints: int = 1, stage2_blocks_per_sm: int = 0,
-                   reg_level: int = 1) -> None:
+                   reg_level: int = 1, stage1_max_rows: int = 2) -> None:
         """Result-neutral kernel choices (see ma_tuning in the C header)."""
-        t = _lib.ma_tuning(seed_kernel, stage1_endpoints, stage2_blocks_per_sm, reg_level)
+        t = _lib.ma_tuning(seed_kernel, stage1_endpoints, stage2_blocks_per_sm, reg_level, stage1_max_rows)
         check(lib.ma_ctx_set_tuning(self.handle, C.byref(t)), self.handle)
 
     def tuning(self) -> dict:
