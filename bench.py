@@ -54,7 +54,7 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the oracle timing (profiling runs)")
     ap.add_argument("--tuning", default="", help="fixed kernel choice 'seed_kernel,stage1_endpoints,"
-                    "stage2_blocks_per_sm,reg_level' instead of the autotuner")
+                    "stage2_blocks_per_sm,reg_level,stage1_max_rows,stage2_first_wave' instead of the autotuner")
     return ap.parse_args()
 
 
@@ -265,7 +265,7 @@ def run_ours(args, rank, world, local):
     # traffic accounting: one untimed pass of the counting kernel
     _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 2), ctx.handle)
     step()
-    tally = (_lib.C.c_uint64 * 8)()
+    tally = (_lib.C.c_uint64 * 9)()
     _lib.lib.ma_ctx_traffic(ctx.handle, tally)
     tally = list(tally)
     _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 1), ctx.handle)
@@ -327,7 +327,7 @@ def run_ours(args, rank, world, local):
             "alg_bytes_per_launch": int(alg_bytes),
             "tally_per_read": {k: round(v / n_seq, 3) for k, v in zip(
                 ["occ_lines_32B", "kmer_loads", "sa_loads", "pac_sectors_32B", "backward_steps", "endpoints",
-                 "loci_evaluated", "read_words"], tally)}}
+                 "loci_evaluated", "read_words", "endpoints_skipped"], tally)}}
     line = {"metric": METRIC, "value": round(value, 1), "unit": "reads/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",

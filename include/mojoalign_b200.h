@@ -252,6 +252,9 @@ int ma_last_launch_count(const ma_ctx* ctx);
  *   stage1_max_rows       stage 1 hands a read to stage 2 as soon as one of
  *                         its seeds has more SA rows than this (1..16,
  *                         default 2; 16 = never).
+ *   stage2_first_wave     right endpoints stage 2 searches in its first
+ *                         group for a read (1..32, default 32); later groups
+ *                         take 32.
  */
 typedef struct ma_tuning {
     int32_t seed_kernel;
@@ -259,6 +262,7 @@ typedef struct ma_tuning {
     int32_t stage2_blocks_per_sm;
     int32_t reg_level;
     int32_t stage1_max_rows;
+    int32_t stage2_first_wave;
 } ma_tuning;
 int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t);
 int ma_ctx_get_tuning(const ma_ctx* ctx, ma_tuning* t);
@@ -275,8 +279,8 @@ int ma_ctx_set_profiling(ma_ctx* ctx, int flags);
 int ma_ctx_kernel_ms(const ma_ctx* ctx, float* out4);
 /* Tallies of the last counting call: 32-B Occ lines, k-mer entries, SA
  * entries, 32-B pac sectors, backward steps, endpoints searched, loci
- * evaluated, read words read. */
-int ma_ctx_traffic(const ma_ctx* ctx, uint64_t* out8);
+ * evaluated, read words read, endpoints skipped as predicted duplicates. */
+int ma_ctx_traffic(const ma_ctx* ctx, uint64_t* out9);
 /* Random aligned `line_bytes` (32 or 64) gathers over a buffer of
  * buffer_bytes: achieved GB/s (the random-gather roofline). */
 int ma_bench_gather(ma_ctx* ctx, uint64_t buffer_bytes, int line_bytes, uint64_t n_loads, double* gbps);

@@ -20,8 +20,9 @@ int launch_seed_extend(const DevIndex& ix, const DevReads& R, const DevParams& P
 double run_gather_bench(uint64_t buffer_bytes, int line_bytes, uint64_t n_loads, int sm_count, cudaStream_t st);
 size_t two_stage_scratch_bytes(int64_t n_seq);
 int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
-                          int stage1_endpoints, int stage1_max_rows, int stage2_blocks, int level, void* scratch,
-                          unsigned long long* d_tally, cudaEvent_t mid, cudaStream_t st);
+                          int stage1_endpoints, int stage1_max_rows, int stage2_blocks, int level,
+                          int first_wave, void* scratch, unsigned long long* d_tally, cudaEvent_t mid,
+                          cudaStream_t st);
 int stage2_blocks_per_sm(int level, bool counting);
 int launch_rescue(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int64_t n_pairs,
                   cudaStream_t st);
@@ -70,10 +71,10 @@ struct ma_ctx {
     int profiling = 0;           // bit 0: per-kernel events, bit 1: traffic tally
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // pack | stage 1 | stage 2 | rescue
     float kernel_ms[4] = {0, 0, 0, 0};  // pack, seed (both stages), rescue, stage 1 alone
-    uint64_t traffic[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint64_t traffic[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     bool rescue_ran = false;
     DevBuf tally;
-    ma_tuning tuning{1, 1, 0, 1, 2};
+    ma_tuning tuning{1, 1, 0, 1, 2, 32};
     int sm_count = 0;
     DevBuf seed_scratch;
     DevBuf bases, lens, packed, err_flag;
@@ -165,9 +166,9 @@ void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const
     const bool timed = ctx->profiling & 1;
     unsigned long long* d_tally = nullptr;
     if (ctx->profiling & 2) {
-        ctx->tally.ensure(8 * sizeof(unsigned long long));
+        ctx->tally.ensure(9 * sizeof(unsigned long long));
         d_tally = ctx->tally.as<unsigned long long>();
-        ck(cudaMemsetAsync(d_tally, 0, 8 * sizeof(unsigned long long), st), "memset");
+        ck(cudaMemsetAsync(d_tally, 0, 9 * sizeof(unsigned long long), st), "memset");
     }
     if (timed) ck(cudaEventRecord(ctx->ev[0], st), "event");
     launches += launch_pack(d_bases, d_lens, n_seq, n1, static_cast<int>(max_len), words, bs_r1, bs_r2,
@@ -184,7 +185,8 @@ void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const
                                                              : stage2_blocks_per_sm(level, d_tally != nullptr);
         launches += launch_seed_two_stage(idx->dix, R, P, out, ctx->tuning.stage1_endpoints,
                                           ctx->tuning.stage1_max_rows, bps * ctx->sm_count, level,
-                                          ctx->seed_scratch.p, d_tally, timed ? ctx->ev[4] : nullptr, st);
+                                          ctx->tuning.stage2_first_wave, ctx->seed_scratch.p, d_tally,
+                                          timed ? ctx->ev[4] : nullptr, st);
     }
     if (timed) ck(cudaEventRecord(ctx->ev[2], st), "event");
     ctx->rescue_ran = paired && p->rescue_win > 0;
@@ -207,9 +209,9 @@ void check_err_flag(ma_ctx* ctx, cudaStream_t st) {
         if (ctx->tuning.seed_kernel == 1) ck(cudaEventElapsedTime(&ctx->kernel_ms[3], ctx->ev[1], ctx->ev[4]), "elapsed");
     }
     if (ctx->profiling & 2) {
-        unsigned long long t[8];
+        unsigned long long t[9];
         ck(cudaMemcpy(t, ctx->tally.p, sizeof t, cudaMemcpyDeviceToHost), "D2H tally");
-        for (int i = 0; i < 8; ++i) ctx->traffic[i] = t[i];
+        for (int i = 0; i < 9; ++i) ctx->traffic[i] = t[i];
     }
 }
 
@@ -476,6 +478,8 @@ int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t) {
         if (t->stage2_blocks_per_sm < 0 || t->stage2_blocks_per_sm > 64) fail(MA_ERR_ARG, "bad stage2_blocks_per_sm");
         if (t->reg_level < 0 || t->reg_level > 2) fail(MA_ERR_ARG, "reg_level must be 0, 1 or 2");
         if (t->stage1_max_rows < 1 || t->stage1_max_rows > 16) fail(MA_ERR_ARG, "stage1_max_rows must be in 1..16");
+        if (t->stage2_first_wave < 1 || t->stage2_first_wave > 32)
+            fail(MA_ERR_ARG, "stage2_first_wave must be in 1..32");
         ctx->tuning = *t;
     });
 }
@@ -492,9 +496,9 @@ int ma_ctx_kernel_ms(const ma_ctx* ctx, float* out4) {
     return MA_OK;
 }
 
-int ma_ctx_traffic(const ma_ctx* ctx, uint64_t* out8) {
-    if (!ctx || !out8) return MA_ERR_ARG;
-    for (int i = 0; i < 8; ++i) out8[i] = ctx->traffic[i];
+int ma_ctx_traffic(const ma_ctx* ctx, uint64_t* out9) {
+    if (!ctx || !out9) return MA_ERR_ARG;
+    for (int i = 0; i < 9; ++i) out9[i] = ctx->traffic[i];
     return MA_OK;
 }
 

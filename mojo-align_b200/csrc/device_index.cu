@@ -9,6 +9,8 @@
 //   reconstruct_sa    sampled SA -> full SA, one LF chain per sampled row
 //   build_kmer        k-mer -> backward-search interval table
 //   kmer3_rows/bounds 3-letter k-mer tables from one pass over the full SA
+//   lcp / summary     capped LCPs of adjacent SA rows -> per-position
+//                     shortest-unique lengths and k-mer counts
 // Every kernel's loops are bounded; a chain that runs past its bound (only
 // possible on an inconsistent index) raises a device error flag instead of
 // spinning.
@@ -189,8 +191,7 @@ __global__ void fill_empty_kernel(uint2* __restrict__ t, uint64_t n) {
 // Rows with the same k-mer are contiguous in SA order; the first and last
 // row of each run are the interval (k, l) of that k-mer.
 __global__ void kmer3_bounds_kernel(const uint64_t* __restrict__ codes, uint64_t n_rows, int K,
-                                    uint2* __restrict__ t_agt, uint2* __restrict__ t_act,
-                                    const uint32_t* __restrict__ sa, uint32_t* __restrict__ uniq) {
+                                    uint2* __restrict__ t_agt, uint2* __restrict__ t_act) {
     const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     if (i >= n_rows) return;
     const uint64_t c = codes[i];
@@ -198,10 +199,6 @@ __global__ void kmer3_bounds_kernel(const uint64_t* __restrict__ codes, uint64_t
     const bool start = i == 0 || codes[i - 1] != c;
     const bool end = i + 1 == n_rows || codes[i + 1] != c;
     if (!start && !end) return;
-    if (start && end) {  // a k-mer with a single occurrence
-        const uint32_t p = sa[i];
-        atomicOr(uniq + (p >> 5), 1u << (p & 31));
-    }
     const uint64_t lo = c & kEven, hi = (c >> 1) & kEven;
     const bool has_c = (lo & ~hi) != 0, has_g = (hi & ~lo) != 0;
     uint32_t idx = 0;
@@ -214,6 +211,77 @@ __global__ void kmer3_bounds_kernel(const uint64_t* __restrict__ codes, uint64_t
         if (start) t_act[idx].x = static_cast<uint32_t>(i);
         if (end) t_act[idx].y = static_cast<uint32_t>(i);
     }
+}
+
+// 32 symbols of T from position p (T[p] in bits 0-1); symbols past the end
+// of T read as 0 (callers bound comparisons by the suffix lengths).
+__device__ uint64_t text_window32(const DevIndex& ix, uint64_t p) {
+    const uint64_t L = ix.l_pac;
+    if (p + 32 <= L) return ref_window(ix.pacw, static_cast<int64_t>(p));
+    if (p >= L && p + 32 <= 2 * L) {
+        // T[p+i] = 3 - pac[2L-1-p-i]: the forward window [2L-p-32, 2L-p)
+        // complemented, with its 32 symbols in reverse order
+        uint64_t w = ~ref_window(ix.pacw, static_cast<int64_t>(2 * L - p - 32));
+        w = __brevll(w);
+        return ((w >> 1) & kEven) | ((w & kEven) << 1);
+    }
+    uint64_t v = 0;
+    for (int i = 0; i < 32; ++i) {
+        const uint64_t q = p + i;
+        if (q >= 2 * L) break;
+        const uint64_t f = q < L ? q : 2 * L - 1 - q;
+        const uint64_t c = (ix.pacw[(f >> 5) + PAC_PAD] >> (2 * (f & 31))) & 3;
+        v |= (q < L ? c : 3 - c) << (2 * i);
+    }
+    return v;
+}
+
+constexpr int LCP_CAP = 255;
+
+// lcp[i] = min(common prefix of the suffixes of rows i-1 and i, 255).
+__global__ void lcp_kernel(DevIndex ix, uint64_t n_rows, uint8_t* __restrict__ lcp) {
+    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n_rows) return;
+    if (i == 0) {
+        lcp[0] = 0;
+        return;
+    }
+    const uint64_t n = ix.seq_len;
+    const uint64_t a = ix.sa[i - 1], b = ix.sa[i];
+    uint64_t maxl = n - (a > b ? a : b);  // the shorter suffix
+    if (maxl > LCP_CAP) maxl = LCP_CAP;
+    uint64_t l = 0;
+    while (l < maxl) {
+        const uint64_t x = text_window32(ix, a + l) ^ text_window32(ix, b + l);
+        const uint64_t d = (x | (x >> 1)) & kEven;
+        if (d) {
+            l += static_cast<uint64_t>(__ffsll(static_cast<long long>(d)) - 1) / 2;
+            break;
+        }
+        l += 32;
+    }
+    lcp[i] = static_cast<uint8_t>(l < maxl ? l : maxl);
+}
+
+// Row i holds the suffix starting at y = SA[i]; its shortest unique prefix
+// is 1 + max(lcp[i], lcp[i+1]) and its K-mer occurs as often as the run of
+// adjacent rows with lcp >= K around i.  Stored at x = 2L-1-y.
+__global__ void summary_kernel(DevIndex ix, uint64_t n_rows, int K, const uint8_t* __restrict__ lcp,
+                               uint16_t* __restrict__ summary) {
+    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (i == 0 || i >= n_rows) return;  // row 0 is the sentinel suffix
+    const uint64_t n = ix.seq_len;
+    const uint64_t y = ix.sa[i];
+    const int l1 = lcp[i], l2 = i + 1 < n_rows ? lcp[i + 1] : 0;
+    const uint64_t m = 1 + static_cast<uint64_t>(l1 > l2 ? l1 : l2);
+    const uint32_t mul = (m < LCP_CAP && y + m <= n) ? static_cast<uint32_t>(m) : 255u;
+    uint32_t occ = 255;
+    if (y + K <= n) {
+        occ = 1;
+        for (uint64_t j = i; j >= 1 && lcp[j] >= K && occ < 255; --j) ++occ;
+        for (uint64_t j = i + 1; j < n_rows && lcp[j] >= K && occ < 255; ++j) ++occ;
+    }
+    summary[n - 1 - y] = static_cast<uint16_t>(mul | (occ << 8));
 }
 
 void check(cudaError_t e, const char* what) {
@@ -239,7 +307,7 @@ uint64_t device_index_bytes(const BwaIndexHost& h, int kmer_k, int kmer3_k) {
     b += (h.seq_len + 1) * 4;
     b += ((h.l_pac + 31) / 32 + 2 * PAC_PAD) * 8;
     if (kmer_k > 0) b += (1ull << (2 * kmer_k)) * 8;
-    if (kmer3_k > 0) b += 2 * pow3(kmer3_k) * 8 + ((h.seq_len + 31) / 32) * 4;
+    if (kmer3_k > 0) b += 2 * pow3(kmer3_k) * 8 + h.seq_len * 2;
     b += h.contigs.size() * 12;
     return b;
 }
@@ -352,15 +420,18 @@ DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, int kmer3_k, cuda
             const uint64_t n3 = pow3(kmer3_k), n_rows = h.seq_len + 1;
             check(cudaMalloc(&bufs.kmer3[0], n3 * 8), "cudaMalloc kmer3");
             check(cudaMalloc(&bufs.kmer3[1], n3 * 8), "cudaMalloc kmer3");
-            check(cudaMalloc(&bufs.uniq, ((h.seq_len + 31) / 32) * 4), "cudaMalloc uniq");
-            check(cudaMemsetAsync(bufs.uniq, 0, ((h.seq_len + 31) / 32) * 4, st), "memset uniq");
+            check(cudaMalloc(&bufs.summary, h.seq_len * 2), "cudaMalloc summary");
             uint64_t* d_codes = nullptr;
             check(cudaMalloc(&d_codes, n_rows * 8), "cudaMalloc kmer3 staging");
             fill_empty_kernel<<<4096, 256, 0, st>>>(bufs.kmer3[0], n3);
             fill_empty_kernel<<<4096, 256, 0, st>>>(bufs.kmer3[1], n3);
             kmer3_rows_kernel<<<grid_for(n_rows, 256), 256, 0, st>>>(ix, kmer3_k, n_rows, d_codes);
             kmer3_bounds_kernel<<<grid_for(n_rows, 256), 256, 0, st>>>(d_codes, n_rows, kmer3_k, bufs.kmer3[0],
-                                                                       bufs.kmer3[1], bufs.sa, bufs.uniq);
+                                                                       bufs.kmer3[1]);
+            // the codes buffer (8 B per row) is reused for the u8 LCPs
+            uint8_t* d_lcp = reinterpret_cast<uint8_t*>(d_codes);
+            lcp_kernel<<<grid_for(n_rows, 256), 256, 0, st>>>(ix, n_rows, d_lcp);
+            summary_kernel<<<grid_for(n_rows, 256), 256, 0, st>>>(ix, n_rows, kmer3_k, d_lcp, bufs.summary);
             cudaError_t le = cudaGetLastError();
             cudaError_t se = cudaStreamSynchronize(st);
             cudaFree(d_codes);
@@ -368,7 +439,7 @@ DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, int kmer3_k, cuda
             check(se, "kmer3 tables");
             ix.kmer3[0] = bufs.kmer3[0];
             ix.kmer3[1] = bufs.kmer3[1];
-            ix.uniq = bufs.uniq;
+            ix.summary = bufs.summary;
             ix.kmer3_k = kmer3_k;
         }
         check(cudaStreamSynchronize(st), "index preparation");
@@ -388,7 +459,7 @@ void free_device_index(DeviceIndexBuffers& b) {
     cudaFree(b.kmer);
     cudaFree(b.kmer3[0]);
     cudaFree(b.kmer3[1]);
-    cudaFree(b.uniq);
+    cudaFree(b.summary);
     cudaFree(b.coff);
     cudaFree(b.clen);
     b = DeviceIndexBuffers{};

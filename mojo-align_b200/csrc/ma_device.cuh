@@ -18,8 +18,12 @@
 //         reads, indexed in base 3: table 0 holds the words without C
 //         (A, G, T -> digits 0, 1, 2; C->T reads), table 1 the words
 //         without G (A, C, T -> 0, 1, 2; G->A reads).
-//   uniq  one bit per text position p of T (pac + reverse complement): the
-//         kmer3_k-mer T[p, p+k) occurs exactly once in T.
+//   summary  per position x of T (pac + reverse complement), for the
+//         substrings of T that end at x: bits 0-7 the smallest length m with
+//         T[x-m+1, x] occurring once in T (255: none up to 254), bits 8-15 the
+//         occurrences of the kmer3_k-mer ending at x (capped at 255).  T is
+//         its own reverse complement, so these are the shortest unique prefix
+//         and the k-mer count of the suffix starting at 2*l_pac-1-x.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -45,7 +49,7 @@ struct DevIndex {
     const uint64_t* pacw;
     const uint2* kmer;
     const uint2* kmer3[2];
-    const uint32_t* uniq;  // bit p: the kmer3_k-mer at text position p occurs once
+    const uint16_t* summary;  // per text end position x: see "summary" above
     const uint64_t* coff;
     const uint32_t* clen;
     int64_t n_contigs;
@@ -152,7 +156,7 @@ struct DeviceIndexBuffers {
     uint64_t* pacw = nullptr;
     uint2* kmer = nullptr;
     uint2* kmer3[2] = {nullptr, nullptr};
-    uint32_t* uniq = nullptr;
+    uint16_t* summary = nullptr;
     uint64_t* coff = nullptr;
     uint32_t* clen = nullptr;
     uint64_t bytes = 0;

@@ -91,8 +91,9 @@ __device__ __forceinline__ uint64_t window_bits(const uint64_t* words, int s, in
 // timed kernel is the S = false instantiation, where every tally compiles
 // away.
 struct Tally {
-    uint32_t occ_lines, kmer_loads, sa_loads, pac_sectors, steps, endpoints, loci, read_words;
+    uint32_t occ_lines, kmer_loads, sa_loads, pac_sectors, steps, endpoints, loci, read_words, skipped;
 };
+constexpr int TALLY_N = 9;
 
 // Mismatch bits (even positions) of read word w against the text at
 // bstart + 32*w; N bases always mismatch.
@@ -567,9 +568,9 @@ __device__ __forceinline__ void write_hit(const DevOut& out, int64_t r, const Be
 template <bool S>
 __device__ __forceinline__ void flush_tally(const Tally& t, unsigned long long* tally_out) {
     if constexpr (S) {
-        const uint32_t v[8] = {t.occ_lines, t.kmer_loads, t.sa_loads, t.pac_sectors, t.steps, t.endpoints, t.loci,
-                               t.read_words};
-        for (int i = 0; i < 8; ++i)
+        const uint32_t v[TALLY_N] = {t.occ_lines, t.kmer_loads, t.sa_loads, t.pac_sectors, t.steps,
+                                     t.endpoints, t.loci, t.read_words, t.skipped};
+        for (int i = 0; i < TALLY_N; ++i)
             if (v[i]) atomicAdd(tally_out + i, static_cast<unsigned long long>(v[i]));
     }
 }
@@ -683,38 +684,52 @@ __device__ __forceinline__ uint64_t warp_min64(uint64_t v) {
 // shift) pair is evaluated by one lane.  The warp minimum of the (nm,
 // ordinal) keys is folded into the read's running best.  The read stops
 // after the group of endpoints in which an nm == 0 hit appears.
-// An endpoint whose seed window (seed_len bases ending at e) matches the
-// text exactly at an evaluated locus, and whose kmer3_k-mer there occurs
-// once in the text, would give the reference a unique interval at
-// mlen = seed_len resolving to that same locus: a duplicate that cannot win.
-// Such endpoints are skipped without touching the index.
-__device__ __forceinline__ bool predicted_duplicate(const DevIndex& ix, const ReadView& rd, int e, int seed_len,
-                                                    const uint64_t* memo, int n_check) {
-    const int n = seed_len, qlen = rd.qlen;
-    const int s0 = e - n + 1;
-    if (window_bits(rd.nf, s0, n) != 0) return false;
-    const uint64_t mask = n >= 32 ? ~0ull : ((1ull << (2 * n)) - 1);
-    const uint64_t wf = window_bits(rd.fwd, s0, n);
-    const uint64_t wr = window_bits(rd.rc, qlen - 1 - e, n);
+// Duplicate prediction.  Let the read's bases ending at right endpoint e
+// match the text exactly at an evaluated locus (b0, strand), over the
+// length mlen = max(seed_len, m), m the shortest unique length of the text
+// substring ending there (summary).  Then the reference's backward search
+// from e only ever follows that text (no empty interval, no non-ACGT base),
+// occ never exceeds its value at mlen = seed_len (<= max_occ, from the
+// summary's k-mer count, or 1 when m <= seed_len), and it stops at mlen with
+// a single SA row whose text position resolves to b0: the locus again, which
+// cannot win.  Such endpoints are skipped without touching the index.
+template <bool S>
+__device__ __forceinline__ bool predicted_duplicate(const DevIndex& ix, const ReadView& rd, int e,
+                                                    const DevParams& P, const uint64_t* memo, int n_check,
+                                                    Tally& t) {
+    const int qlen = rd.qlen;
     const int64_t L = static_cast<int64_t>(ix.l_pac);
-    const int Ku = ix.kmer3_k;
     for (int m = 0; m < n_check; ++m) {
         const int64_t tag = static_cast<int64_t>(memo[m]);
         const int64_t b0 = tag >> 1;
         const int rev = static_cast<int>(tag & 1);
-        const int64_t tpos = rev ? b0 + qlen - 1 - e : b0 + s0;  // forward text start of the window
-        if (tpos < 0 || tpos + n > L) continue;
-        if (((ref_window(ix.pacw, tpos) & mask) ^ (rev ? wr : wf)) != 0) continue;
-        const uint64_t pu = rev ? static_cast<uint64_t>(2 * L - tpos - Ku)
-                                : static_cast<uint64_t>(b0 + e - Ku + 1);
-        return (__ldg(ix.uniq + (pu >> 5)) >> (pu & 31)) & 1;
+        // text position (in T) of the window's right end
+        const int64_t x = rev ? 2 * L - 1 - (b0 + qlen - 1 - e) : b0 + e;
+        if (rev ? (b0 + qlen - 1 - e < 0 || b0 + qlen - 1 - e >= L) : (x < 0 || x >= L)) continue;
+        const uint32_t sm = __ldg(ix.summary + x);
+        const int mul = static_cast<int>(sm & 0xFF), occ = static_cast<int>(sm >> 8);
+        if (mul == 255) continue;
+        const int mlen = mul > P.seed_len ? mul : P.seed_len;
+        if (mlen > e + 1) continue;
+        if (mul > P.seed_len && (occ == 255 || occ > P.max_occ)) continue;
+        const int sA = e - mlen + 1;
+        int mm;
+        if (!rev) {
+            if (b0 + sA < 0) continue;
+            mm = count_mm<S>(ix.pacw, rd.fwd, rd.nf, b0, sA, e + 1, 1, t);
+        } else {
+            const int a = qlen - 1 - e, bb = qlen - sA;  // reverse-complement read positions
+            if (b0 + bb - 1 >= L) continue;
+            mm = count_mm<S>(ix.pacw, rd.rc, rd.nr, b0, a, bb, 1, t);
+        }
+        if (mm == 0) return true;
     }
     return false;
 }
 
 template <bool S, int MINB>
 __global__ void __launch_bounds__(S2_WARPS * 32, MINB) seed_stage2_kernel(DevIndex ix, DevReads R, DevParams P,
-                                                                    DevOut out, Handoff h,
+                                                                    DevOut out, Handoff h, int first_wave,
                                                                     unsigned long long* __restrict__ tally_out) {
     __shared__ uint64_t s_words_all[S2_WARPS][4 * MAX_WORDS];
     __shared__ uint64_t s_memo_all[S2_WARPS][MEMO2];
@@ -752,14 +767,16 @@ __global__ void __launch_bounds__(S2_WARPS * 32, MINB) seed_stage2_kernel(DevInd
         Best win;  // valid when improved
         win.crid = -1;
         bool improved = false;
-        const bool can_predict = ix.uniq && ix.kmer3_k > 0 && ix.kmer3_k <= P.seed_len && P.seed_len <= 32;
-        for (int j0 = h.resume[r]; j0 < n_end; j0 += 32) {
+        const bool can_predict = ix.summary && ix.kmer3_k > 0 && ix.kmer3_k <= P.seed_len;
+        int width = first_wave;
+        for (int j0 = h.resume[r]; j0 < n_end; j0 += width, width = 32) {
             const int j = j0 + lane;
             const int e = P.seed_len - 1 + j * P.seed_stride;
             Seed sd{0, 0, -1, false};
-            if (j < n_end) {
-                const bool dup = can_predict && predicted_duplicate(ix, rd, e, P.seed_len, s_memo,
-                                                                    n_memo < 8 ? n_memo : 8);
+            if (lane < width && j < n_end) {
+                const bool dup = can_predict && predicted_duplicate<S>(ix, rd, e, P, s_memo,
+                                                                       n_memo < 8 ? n_memo : 8, t);
+                if constexpr (S) t.skipped += dup;
                 if (!dup) sd = search_endpoint<S>(ix, rd, e, P, t);
             }
             const int nrows = sd.found ? static_cast<int>(sd.l - sd.k + 1) : 0;
@@ -983,8 +1000,8 @@ struct SeedKernels {
         seed_stage1_kernel<S, B1><<<g, 128, 0, st>>>(ix, R, P, out, ep, max_rows, h, tally);
     }
     static void stage2(dim3 g, cudaStream_t st, const DevIndex& ix, const DevReads& R, const DevParams& P,
-                       const DevOut& out, int, int, const Handoff& h, unsigned long long* tally) {
-        seed_stage2_kernel<S, B2><<<g, S2_WARPS * 32, 0, st>>>(ix, R, P, out, h, tally);
+                       const DevOut& out, int first_wave, int, const Handoff& h, unsigned long long* tally) {
+        seed_stage2_kernel<S, B2><<<g, S2_WARPS * 32, 0, st>>>(ix, R, P, out, h, first_wave, tally);
     }
     static int stage2_occupancy() {
         int nb = 0;
@@ -1029,8 +1046,9 @@ size_t two_stage_scratch_bytes(int64_t n_seq) {
 }
 
 int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
-                          int stage1_endpoints, int stage1_max_rows, int stage2_blocks, int level, void* scratch,
-                          unsigned long long* d_tally, cudaEvent_t mid, cudaStream_t st) {
+                          int stage1_endpoints, int stage1_max_rows, int stage2_blocks, int level,
+                          int first_wave, void* scratch, unsigned long long* d_tally, cudaEvent_t mid,
+                          cudaStream_t st) {
     const size_t n = static_cast<size_t>(R.n_seq);
     char* p = static_cast<char*>(scratch);
     Handoff h;
@@ -1050,11 +1068,11 @@ int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams
     if (d_tally) {
         SeedKernels<true, 0>::stage1(g1, st, ix, R, P, out, stage1_endpoints, stage1_max_rows, h, d_tally);
         if (mid) cudaEventRecord(mid, st);
-        SeedKernels<true, 0>::stage2(g2, st, ix, R, P, out, stage1_endpoints, stage1_max_rows, h, d_tally);
+        SeedKernels<true, 0>::stage2(g2, st, ix, R, P, out, first_wave, stage1_max_rows, h, d_tally);
     } else {
         launch_levels<false>(level, false, g1, st, ix, R, P, out, stage1_endpoints, stage1_max_rows, h, nullptr);
         if (mid) cudaEventRecord(mid, st);
-        launch_levels<false>(level, true, g2, st, ix, R, P, out, stage1_endpoints, stage1_max_rows, h, nullptr);
+        launch_levels<false>(level, true, g2, st, ix, R, P, out, first_wave, stage1_max_rows, h, nullptr);
     }
     return 2;
 }

@@ -33,8 +33,9 @@ int launch_pack(const uint8_t* d_bases, const uint32_t* d_lens, int64_t n_seq, i
                 int bs_r1, int bs_r2, uint64_t* d_packed, int* d_err, cudaStream_t st);
 size_t two_stage_scratch_bytes(int64_t n_seq);
 int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
-                          int stage1_endpoints, int stage1_max_rows, int stage2_blocks, int level, void* scratch,
-                          unsigned long long* d_tally, cudaEvent_t mid, cudaStream_t st);
+                          int stage1_endpoints, int stage1_max_rows, int stage2_blocks, int level,
+                          int first_wave, void* scratch, unsigned long long* d_tally, cudaEvent_t mid,
+                          cudaStream_t st);
 int stage2_blocks_per_sm(int level, bool counting);
 int launch_rescue(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int64_t n_pairs,
                   cudaStream_t st);
@@ -123,7 +124,7 @@ extern "C" int ma_map_batch_device_noalloc(const ma_index* idx, const uint8_t* d
         launch_pack(d_bases, d_lens, n_seq, n1, static_cast<int>(max_len), words, bs_r1, bs_r2, packed, err, st);
         DevReads R{packed, d_lens, words, n_seq};
         const int level = 2;
-        launch_seed_two_stage(*ix, R, P, o, 1, 2, stage2_blocks_per_sm(level, false) * sms, level, handoff,
+        launch_seed_two_stage(*ix, R, P, o, 1, 2, stage2_blocks_per_sm(level, false) * sms, level, 32, handoff,
                               nullptr, nullptr, st);
         if (paired && p->rescue_win > 0) launch_rescue(*ix, R, P, o, n1, st);
         ck(cudaGetLastError(), "kernel launch");

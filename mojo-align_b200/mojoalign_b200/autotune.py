@@ -18,17 +18,19 @@ from .mapper import GpuContext, GpuIndex, MapResult, map_batch
 from .params import FmParams
 
 DEFAULT_CANDIDATES = [
-    (0, 1, 0, 1, 16),
-    (1, 1, 0, 1, 2),
-    (1, 1, 0, 2, 2),
-    (1, 1, 0, 2, 1),
-    (1, 1, 0, 2, 4),
-    (1, 1, 0, 2, 16),
-    (1, 2, 0, 2, 2),
-    (1, 1, 0, 0, 2),
-    (1, 1, 3, 2, 2),
+    (0, 1, 0, 1, 16, 32),
+    (1, 1, 0, 2, 16, 32),
+    (1, 1, 0, 2, 2, 32),
+    (1, 1, 0, 2, 1, 32),
+    (1, 1, 0, 2, 1, 1),
+    (1, 1, 0, 2, 1, 4),
+    (1, 1, 0, 2, 1, 8),
+    (1, 1, 0, 1, 1, 1),
+    (1, 1, 0, 1, 1, 4),
+    (1, 2, 0, 2, 2, 4),
 ]
-FIELDS = ("seed_kernel", "stage1_endpoints", "stage2_blocks_per_sm", "reg_level", "stage1_max_rows")
+FIELDS = ("seed_kernel", "stage1_endpoints", "stage2_blocks_per_sm", "reg_level", "stage1_max_rows",
+          "stage2_first_wave")
 
 
 @dataclass

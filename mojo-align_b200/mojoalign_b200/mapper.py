@@ -45,9 +45,10 @@ class GpuContext:
         return lib.ma_last_launch_count(self.handle)
 
     def set_tuning(self, seed_kernel: int = 1, stage1_endpoints: int = 1, stage2_blocks_per_sm: int = 0,
-                   reg_level: int = 1, stage1_max_rows: int = 2) -> None:
+                   reg_level: int = 1, stage1_max_rows: int = 2, stage2_first_wave: int = 32) -> None:
         """Result-neutral kernel choices (see ma_tuning in the C header)."""
-        t = _lib.ma_tuning(seed_kernel, stage1_endpoints, stage2_blocks_per_sm, reg_level, stage1_max_rows)
+        t = _lib.ma_tuning(seed_kernel, stage1_endpoints, stage2_blocks_per_sm, reg_level, stage1_max_rows,
+                           stage2_first_wave)
         check(lib.ma_ctx_set_tuning(self.handle, C.byref(t)), self.handle)
 
     def tuning(self) -> dict:
@@ -64,7 +65,7 @@ class GpuContext:
         return list(v)
 
     def traffic(self) -> list[int]:
-        v = (C.c_uint64 * 8)()
+        v = (C.c_uint64 * 9)()
         check(lib.ma_ctx_traffic(self.handle, v), self.handle)
         return list(v)
 

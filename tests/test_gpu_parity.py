@@ -37,9 +37,9 @@ def gpu_index(ctx, prefix, k, k3=0):
 
 
 # Result-neutral kernel forms (seed_kernel, stage1_endpoints,
-# stage2_blocks_per_sm, reg_level, stage1_max_rows): one thread per read; two stages with
+# stage2_blocks_per_sm, reg_level, stage1_max_rows, stage2_first_wave): one thread per read; two stages with
 # the first 1, 2 or 3 right endpoints in stage 1, at each register budget.
-TUNINGS = [(0, 1, 0, 0, 16), (1, 1, 0, 1, 2), (1, 3, 1, 2, 1), (1, 2, 0, 0, 16), (1, 1, 0, 2, 4)]
+TUNINGS = [(0, 1, 0, 0, 16, 32), (1, 1, 0, 1, 2, 32), (1, 3, 1, 2, 1, 1), (1, 2, 0, 0, 16, 4), (1, 1, 0, 2, 1, 7)]
 
 
 def compare(prefix, ctx, bases, lens, n1, paired, max_len, params, k=12, bs=(1, 2), tunings=TUNINGS, k3=12):
