@@ -226,23 +226,117 @@ __device__ __forceinline__ void deletion_scan(const uint64_t* __restrict__ pacw,
 // One shift adj of one locus (b0, strand): the body of the reference's adj
 // loop, linear_gpu_fm.mojo:1528-1826.  Folds the candidate (full compare,
 // or the deletion probe's offsets) into `best` by its (nm, ordinal) key.
+// Contig of a locus, looked up once for all of its shifts.
+struct ContigHint {
+    int64_t crid, coff, clen;
+};
+
+__device__ __forceinline__ ContigHint contig_hint(const DevIndex& ix, int64_t b0) {
+    int64_t probe = b0 < 0 ? 0 : b0;
+    if (probe >= static_cast<int64_t>(ix.l_pac)) probe = static_cast<int64_t>(ix.l_pac) - 1;
+    ContigHint h{contig_of(ix, probe), 0, 0};
+    if (h.crid >= 0) {
+        h.coff = static_cast<int64_t>(__ldg(ix.coff + h.crid));
+        h.clen = static_cast<int64_t>(__ldg(ix.clen + h.crid));
+    }
+    return h;
+}
+
+__device__ __forceinline__ void set_best(Best& best, uint64_t key, int64_t crid, int64_t pos, int sl, int sr,
+                                         uint32_t mapq, int flag, uint64_t uk, uint64_t ul, int us, int e) {
+    best.key = key;
+    best.crid = static_cast<int32_t>(crid);
+    best.pos = static_cast<uint32_t>(pos);
+    best.sl = sl;
+    best.sr = sr;
+    best.mapq = mapq;
+    best.flag = flag;
+    best.uk = uk;
+    best.ul = ul;
+    best.us = us;
+    best.e = e;
+}
+
+// The deletion probe of a failed forward shift (L1729-1825), kept out of
+// line: it is rare on the hot path.  Every read position mismatches under
+// shift 0 or under shift +1 for every g unless it matches under one of
+// them, so nm_d(g) >= 1 + popc(M0 & M1) for all g; when that bound already
+// exceeds the budget or cannot beat the best so far, no offset is tried.
+template <bool S>
+__device__ __noinline__ void deletion_candidates(const uint64_t* __restrict__ pacw, const uint64_t* q,
+                                                 const uint64_t* qn, int64_t bstart, int qlen, int budget,
+                                                 int prune_nm, uint32_t ord, int64_t crid, int64_t local,
+                                                 Best& best, uint64_t uk, uint64_t ul, int us, int e, Tally& t) {
+    const int nw = (qlen + 31) >> 5;
+    const int stop = prune_nm < budget + 1 ? prune_nm : budget + 1;  // 1 + bound >= stop: nothing to gain
+    int both = 0;
+    for (int w = 0; w < nw; ++w) {
+        uint64_t m0 = mm_word<S>(pacw, q, qn, bstart, w, t);
+        uint64_t m1 = mm_word<S>(pacw, q, qn, bstart + 1, w, t);
+        if (bstart < 0) m0 |= range_mask(w, 0, static_cast<int>(-bstart));
+        if (bstart + 1 < 0) m1 |= range_mask(w, 0, static_cast<int>(-(bstart + 1)));
+        both += __popcll(m0 & m1 & range_mask(w, 0, qlen));
+        if (1 + both >= stop) return;
+    }
+    deletion_scan<S>(pacw, q, qn, bstart, qlen, budget, t, [&](int g, int nmd) {
+        if (nmd > budget) return;
+        const uint64_t key = (static_cast<uint64_t>(nmd) << ORD_SHIFT) | (ord + 1 + g / 4);
+        if (key < best.key) set_best(best, key, crid, local, 0, 0, 20u, 0, uk, ul, us, e);
+    });
+}
+
+// Soft-clip retry of L1591-1694: sl grows to the first matching in-contig
+// base below clip_cap, sr likewise from the right; then the recount.
+template <bool S>
+__device__ __noinline__ int soft_clip_recount(const uint64_t* __restrict__ pacw, const uint64_t* q,
+                                              const uint64_t* qn, int64_t bstart, int qlen, int64_t local,
+                                              int64_t clen, int sl0, int sr0, int clip_cap, int budget, int* sl_out,
+                                              int* sr_out, Tally& t) {
+    int64_t lim = clen - local;
+    if (lim > clip_cap) lim = clip_cap;
+    const int j = first_match<S>(pacw, q, qn, bstart, sl0, static_cast<int>(lim), t);
+    const int sl = j >= 0 ? j : clip_cap;
+    const int64_t jlo = sl > qlen - 1 - clip_cap ? sl : qlen - 1 - clip_cap;
+    int64_t jhi = qlen - 1 - sr0;
+    if (jhi > clen - local - 1) jhi = clen - local - 1;
+    const int j2 = last_match<S>(pacw, q, qn, bstart, static_cast<int>(jlo + 1), static_cast<int>(jhi + 1), t);
+    int sr;
+    if (j2 >= 0) {
+        sr = qlen - 1 - j2;
+    } else {
+        const int64_t sstar = sr0 > qlen - 1 - sl ? sr0 : qlen - 1 - sl;
+        sr = static_cast<int>(sstar < clip_cap ? sstar : clip_cap);
+    }
+    *sl_out = sl;
+    *sr_out = sr;
+    return count_mm<S>(pacw, q, qn, bstart, sl, qlen - sr, budget + 1, t);
+}
+
+// One shift adj of one locus (b0, strand): the body of the reference's adj
+// loop, linear_gpu_fm.mojo:1528-1826.  Folds the candidate (full compare,
+// or the deletion probe's offsets) into `best` by its (nm, ordinal) key.
 // prune_nm: a candidate of this call can only matter when its nm is below
 // prune_nm (every candidate of the call comes after the current best in the
-// reference's order); 1 << 20 disables pruning.
+// reference's order); 1 << 20 disables pruning.  `hint` is the contig of
+// b0; a shift that stays inside it needs no contig search.
 template <bool S>
 __device__ void eval_adj(const DevIndex& ix, const ReadView& rd, int64_t b0, int is_rev, int adj, int budget,
                          int clip_cap, uint32_t ord_row, Best& best, uint64_t uk, uint64_t ul, int us, int e,
-                         int prune_nm, Tally& t) {
+                         int prune_nm, const ContigHint& hint, Tally& t) {
     const int qlen = rd.qlen;
     const uint64_t* q = is_rev ? rd.rc : rd.fwd;
     const uint64_t* qn = is_rev ? rd.nr : rd.nf;
     const int64_t bstart = b0 + adj;
-    int64_t probe = bstart < 0 ? 0 : bstart;
-    if (probe >= static_cast<int64_t>(ix.l_pac)) probe = static_cast<int64_t>(ix.l_pac) - 1;
-    const int64_t crid = contig_of(ix, probe);
-    if (crid < 0) return;
-    const int64_t coff = static_cast<int64_t>(__ldg(ix.coff + crid));
-    const int64_t clen = static_cast<int64_t>(__ldg(ix.clen + crid));
+    int64_t crid = hint.crid, coff = hint.coff, clen = hint.clen;
+    if (crid < 0 || bstart < coff || bstart >= coff + clen) {
+        // the contig holding the clamped probe (binary search, L1536-1549)
+        int64_t probe = bstart < 0 ? 0 : bstart;
+        if (probe >= static_cast<int64_t>(ix.l_pac)) probe = static_cast<int64_t>(ix.l_pac) - 1;
+        crid = contig_of(ix, probe);
+        if (crid < 0) return;
+        coff = static_cast<int64_t>(__ldg(ix.coff + crid));
+        clen = static_cast<int64_t>(__ldg(ix.clen + crid));
+    }
     const int64_t local = bstart - coff;
     const int64_t sl0 = local < 0 ? -local : 0;
     const int64_t sr0 = local + qlen > clen ? local + qlen - clen : 0;
@@ -254,95 +348,33 @@ __device__ void eval_adj(const DevIndex& ix, const ReadView& rd, int64_t b0, int
         t.pac_sectors += static_cast<uint32_t>((hi >> 5) - (lo >> 5) + 1);
     }
     const bool del_probe = adj == 0 && is_rev == 0;
-    {
-        // Exact pruning.  sl0, sr0 and every soft clip are at most clip_cap,
-        // so the full compare and any clipped recount both span read
-        // positions [clip_cap, qlen - clip_cap); their mismatches bound nm.
-        const int core = count_mm<S>(ix.pacw, q, qn, bstart, clip_cap, qlen - clip_cap, budget + 1, t);
-        if (core > budget) {
-            // neither compare is accepted: only the deletion probe remains
-            if (del_probe && prune_nm > 1 && bstart + qlen + 1 <= coff + clen) {
-                deletion_scan<S>(ix.pacw, q, qn, bstart, qlen, budget, t, [&](int g, int nmd) {
-                    if (nmd > budget) return;
-                    const uint64_t key = (static_cast<uint64_t>(nmd) << ORD_SHIFT) | (ord + 1 + g / 4);
-                    if (key < best.key) {
-                        best.key = key;
-                        best.crid = static_cast<int32_t>(crid);
-                        best.pos = static_cast<uint32_t>(local);
-                        best.sl = 0;
-                        best.sr = 0;
-                        best.mapq = 20u;
-                        best.flag = 0;
-                        best.uk = uk;
-                        best.ul = ul;
-                        best.us = us;
-                        best.e = e;
-                    }
-                });
-            }
-            return;
-        }
-        // whether the compare is accepted decides the deletion probe, so
-        // only shifts without one can stop here
-        if (core >= prune_nm && !del_probe) return;
+    const bool del_room = del_probe && prune_nm > 1 && bstart + qlen + 1 <= coff + clen;
+    // Exact pruning.  sl0, sr0 and every soft clip are at most clip_cap, so
+    // the full compare and any clipped recount both span read positions
+    // [clip_cap, qlen - clip_cap); their mismatches bound nm from below.
+    const int core = count_mm<S>(ix.pacw, q, qn, bstart, clip_cap, qlen - clip_cap, budget + 1, t);
+    if (core > budget) {
+        // neither compare is accepted: only the deletion probe remains
+        if (del_room)
+            deletion_candidates<S>(ix.pacw, q, qn, bstart, qlen, budget, prune_nm, ord, crid, local, best, uk, ul,
+                                   us, e, t);
+        return;
     }
+    // whether the compare is accepted decides the deletion probe, so only
+    // shifts without one can stop here
+    if (core >= prune_nm && !del_probe) return;
     int nm = count_mm<S>(ix.pacw, q, qn, bstart, static_cast<int>(sl0), static_cast<int>(qlen - sr0), budget + 1, t);
     int sl = static_cast<int>(sl0), sr = static_cast<int>(sr0);
-    if (nm > budget && clip_cap > 0) {
-        // soft-clip retry, L1591-1694: grow sl to the first matching
-        // in-contig base below clip_cap, sr likewise from the right
-        int64_t lim = clen - local;
-        if (lim > clip_cap) lim = clip_cap;
-        int j = first_match<S>(ix.pacw, q, qn, bstart, sl, static_cast<int>(lim), t);
-        sl = j >= 0 ? j : clip_cap;
-        int64_t jlo = sl > qlen - 1 - clip_cap ? sl : qlen - 1 - clip_cap;
-        int64_t jhi = qlen - 1 - sr0;
-        if (jhi > clen - local - 1) jhi = clen - local - 1;
-        int j2 = last_match<S>(ix.pacw, q, qn, bstart, static_cast<int>(jlo + 1), static_cast<int>(jhi + 1), t);
-        if (j2 >= 0) {
-            sr = qlen - 1 - j2;
-        } else {
-            int64_t sstar = sr0 > qlen - 1 - sl ? sr0 : qlen - 1 - sl;
-            sr = static_cast<int>(sstar < clip_cap ? sstar : clip_cap);
-        }
-        nm = count_mm<S>(ix.pacw, q, qn, bstart, sl, qlen - sr, budget + 1, t);
-    }
+    if (nm > budget && clip_cap > 0)
+        nm = soft_clip_recount<S>(ix.pacw, q, qn, bstart, qlen, local, clen, sl, sr, clip_cap, budget, &sl, &sr, t);
     const int alen = qlen - sl - sr;
     if (nm <= budget && alen >= 24) {
         const uint64_t key = (static_cast<uint64_t>(nm) << ORD_SHIFT) | ord;
-        if (key < best.key) {
-            best.key = key;
-            best.crid = static_cast<int32_t>(crid);
-            best.pos = static_cast<uint32_t>(local + sl);
-            best.sl = sl;
-            best.sr = sr;
-            best.mapq = nm == 0 ? 60u : 20u;
-            best.flag = is_rev * 16;
-            best.uk = uk;
-            best.ul = ul;
-            best.us = us;
-            best.e = e;
-        }
-    } else if (del_probe) {
-        if (prune_nm > 1 && bstart + qlen + 1 <= coff + clen) {
-            deletion_scan<S>(ix.pacw, q, qn, bstart, qlen, budget, t, [&](int g, int nmd) {
-                if (nmd > budget) return;
-                const uint64_t key = (static_cast<uint64_t>(nmd) << ORD_SHIFT) | (ord + 1 + g / 4);
-                if (key < best.key) {
-                    best.key = key;
-                    best.crid = static_cast<int32_t>(crid);
-                    best.pos = static_cast<uint32_t>(local);
-                    best.sl = 0;
-                    best.sr = 0;
-                    best.mapq = 20u;
-                    best.flag = 0;
-                    best.uk = uk;
-                    best.ul = ul;
-                    best.us = us;
-                    best.e = e;
-                }
-            });
-        }
+        if (key < best.key)
+            set_best(best, key, crid, local + sl, sl, sr, nm == 0 ? 60u : 20u, is_rev * 16, uk, ul, us, e);
+    } else if (del_room) {
+        deletion_candidates<S>(ix.pacw, q, qn, bstart, qlen, budget, prune_nm, ord, crid, local, best, uk, ul, us,
+                               e, t);
     }
 }
 
@@ -352,10 +384,11 @@ __device__ void eval_locus(const DevIndex& ix, const ReadView& rd, int64_t b0, i
                            int budget, int clip_cap, uint32_t ord_row, Best& best, uint64_t uk, uint64_t ul,
                            int us, int e, Tally& t) {
     if constexpr (S) t.loci++;
+    const ContigHint hint = contig_hint(ix, b0);
     for (int adj = -adj_cap; adj <= adj_cap; ++adj) {
         const uint64_t bn = best.key >> ORD_SHIFT;
         eval_adj<S>(ix, rd, b0, is_rev, adj, budget, clip_cap, ord_row, best, uk, ul, us, e,
-                    bn < (1u << 20) ? static_cast<int>(bn) : (1 << 20), t);
+                    bn < (1u << 20) ? static_cast<int>(bn) : (1 << 20), hint, t);
     }
 }
 
@@ -663,6 +696,7 @@ struct Locus {
     uint64_t uk, ul;
     uint32_t ord_row;
     int32_t us, e, rev;
+    ContigHint hint;
 };
 
 constexpr int S2_WARPS = 8;   // warps per block of the stage-2 kernel
@@ -695,12 +729,15 @@ __device__ __forceinline__ uint64_t warp_min64(uint64_t v) {
 // cannot win.  Such endpoints are skipped without touching the index.
 template <bool S>
 __device__ __forceinline__ bool predicted_duplicate(const DevIndex& ix, const ReadView& rd, int e,
-                                                    const DevParams& P, const uint64_t* memo, int n_check,
-                                                    Tally& t) {
+                                                    const DevParams& P, int64_t first_tag, const uint64_t* memo,
+                                                    int n_check, Tally& t) {
     const int qlen = rd.qlen;
     const int64_t L = static_cast<int64_t>(ix.l_pac);
-    for (int m = 0; m < n_check; ++m) {
-        const int64_t tag = static_cast<int64_t>(memo[m]);
+    // the best hit's locus first (valid tags are >= -2^40; -1 marks none),
+    // then the first memo entries
+    for (int m = first_tag == -1 ? 0 : -1; m < n_check; ++m) {
+        if (m >= 0 && static_cast<int64_t>(memo[m]) == first_tag) continue;
+        const int64_t tag = m < 0 ? first_tag : static_cast<int64_t>(memo[m]);
         const int64_t b0 = tag >> 1;
         const int rev = static_cast<int>(tag & 1);
         // text position (in T) of the window's right end
@@ -767,6 +804,7 @@ __global__ void __launch_bounds__(S2_WARPS * 32, MINB) seed_stage2_kernel(DevInd
         Best win;  // valid when improved
         win.crid = -1;
         bool improved = false;
+        int64_t best_tag = -1;  // locus of the best hit found in this stage (b0*2+strand)
         const bool can_predict = ix.summary && ix.kmer3_k > 0 && ix.kmer3_k <= P.seed_len;
         int width = first_wave;
         for (int j0 = h.resume[r]; j0 < n_end; j0 += width, width = 32) {
@@ -774,8 +812,8 @@ __global__ void __launch_bounds__(S2_WARPS * 32, MINB) seed_stage2_kernel(DevInd
             const int e = P.seed_len - 1 + j * P.seed_stride;
             Seed sd{0, 0, -1, false};
             if (lane < width && j < n_end) {
-                const bool dup = can_predict && predicted_duplicate<S>(ix, rd, e, P, s_memo,
-                                                                       n_memo < 8 ? n_memo : 8, t);
+                const bool dup = can_predict && predicted_duplicate<S>(ix, rd, e, P, best_tag, s_memo,
+                                                                       n_memo < 4 ? n_memo : 4, t);
                 if constexpr (S) t.skipped += dup;
                 if (!dup) sd = search_endpoint<S>(ix, rd, e, P, t);
             }
@@ -831,6 +869,7 @@ __global__ void __launch_bounds__(S2_WARPS * 32, MINB) seed_stage2_kernel(DevInd
                     L.us = o_s;
                     L.e = o_e;
                     L.rev = rev;
+                    L.hint = contig_hint(ix, b0);
                     s_loci[rank] = L;
                     if constexpr (S) t.loci++;
                 }
@@ -841,13 +880,16 @@ __global__ void __launch_bounds__(S2_WARPS * 32, MINB) seed_stage2_kernel(DevInd
                 Best lb;
                 lb.key = ~0ull;
                 lb.crid = -1;
+                int64_t lb_tag = -1;
                 const uint64_t bn = best_key >> ORD_SHIFT;
                 const int prune = bn < (1u << 20) ? static_cast<int>(bn) : (1 << 20);
                 for (int it = lane; it < U * A; it += 32) {
                     const int u = it / A, a = it - u * A;
                     const Locus L = s_loci[u];
+                    const uint64_t before = lb.key;
                     eval_adj<S>(ix, rd, L.b0, L.rev, a - cl.adj_cap, cl.budget, cl.clip_cap, L.ord_row, lb, L.uk,
-                                L.ul, L.us, L.e, prune, t);
+                                L.ul, L.us, L.e, prune, L.hint, t);
+                    if (lb.key != before) lb_tag = L.b0 * 2 + L.rev;
                 }
                 const uint64_t wmin = warp_min64(lb.key);
                 if (wmin < best_key) {
@@ -864,6 +906,7 @@ __global__ void __launch_bounds__(S2_WARPS * 32, MINB) seed_stage2_kernel(DevInd
                     win.ul = __shfl_sync(FULL, lb.ul, wl);
                     win.us = __shfl_sync(FULL, lb.us, wl);
                     win.e = __shfl_sync(FULL, lb.e, wl);
+                    best_tag = __shfl_sync(FULL, lb_tag, wl);
                     improved = true;
                 }
                 __syncwarp();
