@@ -278,8 +278,9 @@ int ma_ctx_set_profiling(ma_ctx* ctx, int flags);
  * rescue, and stage 1 alone (equal to seed/extend for seed_kernel 0). */
 int ma_ctx_kernel_ms(const ma_ctx* ctx, float* out4);
 /* Tallies of the last counting call: 32-B Occ lines, k-mer entries, SA
- * entries, 32-B pac sectors, backward steps, endpoints searched, loci
- * evaluated, read words read, endpoints skipped as predicted duplicates. */
+ * entries, distinct 32-B pac sectors per evaluated locus, backward steps,
+ * endpoints searched, loci evaluated, read words read, endpoints skipped as
+ * predicted duplicates. */
 int ma_ctx_traffic(const ma_ctx* ctx, uint64_t* out9);
 /* Random aligned `line_bytes` (32 or 64) gathers over a buffer of
  * buffer_bytes: achieved GB/s (the random-gather roofline). */

@@ -74,6 +74,13 @@ struct ma_ctx {
     uint64_t traffic[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     bool rescue_ran = false;
     DevBuf tally;
+    // two-slot pipeline of ma_map_batch: H2D of chunk k+1 on copy_stream
+    // while chunk k computes on `stream`
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t h2d_done[2] = {nullptr, nullptr}, slot_free[2] = {nullptr, nullptr};
+    struct Slot {
+        DevBuf bases, lens, out[12];
+    } slot[2];
     ma_tuning tuning{1, 1, 0, 1, 2, 32};
     int sm_count = 0;
     DevBuf seed_scratch;
@@ -156,12 +163,12 @@ DevParams to_dev(const ma_params* p) {
 // Enqueues pack -> seed/extend -> rescue for device-resident inputs.
 void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const uint32_t* d_lens, uint32_t n1,
                  int paired, uint32_t max_len, int bs_r1, int bs_r2, const ma_params* p, const DevOut& out,
-                 cudaStream_t st) {
+                 cudaStream_t st, bool reset_err = true) {
     const int64_t n_seq = paired ? 2 * static_cast<int64_t>(n1) : n1;
     const int words = static_cast<int>((max_len + 31) / 32);
     ctx->packed.ensure(static_cast<size_t>(n_seq) * 4 * words * 8);
     ctx->err_flag.ensure(sizeof(int));
-    ck(cudaMemsetAsync(ctx->err_flag.p, 0, sizeof(int), st), "memset");
+    if (reset_err) ck(cudaMemsetAsync(ctx->err_flag.p, 0, sizeof(int), st), "memset");
     int launches = 0;
     const bool timed = ctx->profiling & 1;
     unsigned long long* d_tally = nullptr;
@@ -266,6 +273,16 @@ void ma_ctx_destroy(ma_ctx* ctx) {
         if (e) cudaEventDestroy(e);
     ctx->tally.release();
     ctx->seed_scratch.release();
+    for (auto& sl : ctx->slot) {
+        sl.bases.release();
+        sl.lens.release();
+        for (DevBuf& b : sl.out) b.release();
+    }
+    for (int i = 0; i < 2; ++i) {
+        if (ctx->h2d_done[i]) cudaEventDestroy(ctx->h2d_done[i]);
+        if (ctx->slot_free[i]) cudaEventDestroy(ctx->slot_free[i]);
+    }
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     for (DevBuf* b : {&ctx->bases, &ctx->lens, &ctx->packed, &ctx->err_flag, &ctx->o_rid, &ctx->o_pos, &ctx->o_mapq,
                       &ctx->o_flag, &ctx->o_sl, &ctx->o_sr, &ctx->o_nm, &ctx->d_uk, &ctx->d_ul, &ctx->d_us,
                       &ctx->d_e, &ctx->d_score})
@@ -386,43 +403,68 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
             fail(MA_ERR_ARG, "null output array");
         use_device(ctx);
         cudaStream_t st = ctx->stream;
-        const size_t nb = static_cast<size_t>(n_seq) * max_len;
-        ctx->bases.ensure(nb);
-        ctx->lens.ensure(n_seq * 4);
-        for (DevBuf* b : {&ctx->o_rid, &ctx->o_pos, &ctx->o_mapq, &ctx->o_flag, &ctx->o_sl, &ctx->o_sr, &ctx->o_nm,
-                          &ctx->d_us, &ctx->d_e, &ctx->d_score})
-            b->ensure(n_seq * 4);
-        ctx->d_uk.ensure(n_seq * 8);
-        ctx->d_ul.ensure(n_seq * 8);
-        ck(cudaMemcpyAsync(ctx->bases.p, bases, nb, cudaMemcpyHostToDevice, st), "H2D bases");
-        ck(cudaMemcpyAsync(ctx->lens.p, lens, n_seq * 4, cudaMemcpyHostToDevice, st), "H2D lens");
-        DevOut o{ctx->o_rid.as<int32_t>(), ctx->o_pos.as<uint32_t>(), ctx->o_mapq.as<uint32_t>(),
-                 ctx->o_flag.as<int32_t>(), ctx->o_sl.as<uint32_t>(), ctx->o_sr.as<uint32_t>(),
-                 ctx->o_nm.as<uint32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr};
-        const bool want_dbg = dbg && (dbg->uk || dbg->ul || dbg->us || dbg->e || dbg->score);
-        if (want_dbg) {
-            o.uk = ctx->d_uk.as<uint64_t>();
-            o.ul = ctx->d_ul.as<uint64_t>();
-            o.us = ctx->d_us.as<int32_t>();
-            o.e = ctx->d_e.as<int32_t>();
-            o.score = ctx->d_score.as<int32_t>();
+        if (!ctx->copy_stream) {
+            ck(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+            for (int i = 0; i < 2; ++i) {
+                ck(cudaEventCreateWithFlags(&ctx->h2d_done[i], cudaEventDisableTiming), "cudaEventCreate");
+                ck(cudaEventCreateWithFlags(&ctx->slot_free[i], cudaEventDisableTiming), "cudaEventCreate");
+            }
         }
-        enqueue_map(ctx, idx, ctx->bases.as<uint8_t>(), ctx->lens.as<uint32_t>(), n1, paired, max_len, bs_r1, bs_r2,
-                    p, o, st);
-        const size_t n4 = n_seq * 4;
-        ck(cudaMemcpyAsync(out->rid, o.rid, n4, cudaMemcpyDeviceToHost, st), "D2H");
-        ck(cudaMemcpyAsync(out->pos, o.pos, n4, cudaMemcpyDeviceToHost, st), "D2H");
-        ck(cudaMemcpyAsync(out->mapq, o.mapq, n4, cudaMemcpyDeviceToHost, st), "D2H");
-        ck(cudaMemcpyAsync(out->flag, o.flag, n4, cudaMemcpyDeviceToHost, st), "D2H");
-        ck(cudaMemcpyAsync(out->sl, o.sl, n4, cudaMemcpyDeviceToHost, st), "D2H");
-        ck(cudaMemcpyAsync(out->sr, o.sr, n4, cudaMemcpyDeviceToHost, st), "D2H");
-        ck(cudaMemcpyAsync(out->nm, o.nm, n4, cudaMemcpyDeviceToHost, st), "D2H");
-        if (want_dbg) {
-            if (dbg->uk) ck(cudaMemcpyAsync(dbg->uk, o.uk, n_seq * 8, cudaMemcpyDeviceToHost, st), "D2H");
-            if (dbg->ul) ck(cudaMemcpyAsync(dbg->ul, o.ul, n_seq * 8, cudaMemcpyDeviceToHost, st), "D2H");
-            if (dbg->us) ck(cudaMemcpyAsync(dbg->us, o.us, n4, cudaMemcpyDeviceToHost, st), "D2H");
-            if (dbg->e) ck(cudaMemcpyAsync(dbg->e, o.e, n4, cudaMemcpyDeviceToHost, st), "D2H");
-            if (dbg->score) ck(cudaMemcpyAsync(dbg->score, o.score, n4, cudaMemcpyDeviceToHost, st), "D2H");
+        const bool want_dbg = dbg && (dbg->uk || dbg->ul || dbg->us || dbg->e || dbg->score);
+        // Pipeline over chunks of pairs (pairs never split: rescue reads both
+        // mates).  Chunk k's R1 rows and R2 rows are copied into one slot as
+        // a batch of its own while chunk k-1 computes; results are copied
+        // back into the caller's arrays at the pairs' positions.
+        const uint32_t chunk = std::max<uint32_t>(131072u, (n1 + 7) / 8);
+        const int mates = paired ? 2 : 1;
+        void* host_out[12] = {out->rid, out->pos, out->mapq, out->flag, out->sl, out->sr, out->nm,
+                              want_dbg ? dbg->uk : nullptr, want_dbg ? dbg->ul : nullptr,
+                              want_dbg ? dbg->us : nullptr, want_dbg ? dbg->e : nullptr,
+                              want_dbg ? dbg->score : nullptr};
+        const size_t width[12] = {4, 4, 4, 4, 4, 4, 4, 8, 8, 4, 4, 4};
+        int k = 0;
+        for (uint32_t a = 0; a < n1; a += chunk, ++k) {
+            const uint32_t c = std::min(chunk, n1 - a);
+            const int64_t cs = static_cast<int64_t>(c) * mates;
+            ma_ctx::Slot& sl = ctx->slot[k & 1];
+            sl.bases.ensure(static_cast<size_t>(cs) * max_len);
+            sl.lens.ensure(cs * 4);
+            for (int f = 0; f < 12; ++f) sl.out[f].ensure(cs * width[f]);
+            // copy: wait until the slot's previous chunk has been read back
+            ck(cudaStreamWaitEvent(ctx->copy_stream, ctx->slot_free[k & 1], 0), "cudaStreamWaitEvent");
+            for (int m = 0; m < mates; ++m) {
+                const size_t row0 = static_cast<size_t>(m) * n1 + a;
+                ck(cudaMemcpyAsync(sl.bases.as<uint8_t>() + static_cast<size_t>(m) * c * max_len,
+                                   bases + row0 * max_len, static_cast<size_t>(c) * max_len, cudaMemcpyHostToDevice,
+                                   ctx->copy_stream), "H2D bases");
+                ck(cudaMemcpyAsync(sl.lens.as<uint32_t>() + static_cast<size_t>(m) * c, lens + row0, c * 4,
+                                   cudaMemcpyHostToDevice, ctx->copy_stream), "H2D lens");
+            }
+            ck(cudaEventRecord(ctx->h2d_done[k & 1], ctx->copy_stream), "cudaEventRecord");
+            // compute the chunk, then read it back on the compute stream
+            ck(cudaStreamWaitEvent(st, ctx->h2d_done[k & 1], 0), "cudaStreamWaitEvent");
+            DevOut o{sl.out[0].as<int32_t>(), sl.out[1].as<uint32_t>(), sl.out[2].as<uint32_t>(),
+                     sl.out[3].as<int32_t>(), sl.out[4].as<uint32_t>(), sl.out[5].as<uint32_t>(),
+                     sl.out[6].as<uint32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr};
+            if (want_dbg) {
+                o.uk = sl.out[7].as<uint64_t>();
+                o.ul = sl.out[8].as<uint64_t>();
+                o.us = sl.out[9].as<int32_t>();
+                o.e = sl.out[10].as<int32_t>();
+                o.score = sl.out[11].as<int32_t>();
+            }
+            enqueue_map(ctx, idx, sl.bases.as<uint8_t>(), sl.lens.as<uint32_t>(), c, paired, max_len, bs_r1, bs_r2,
+                        p, o, st, k == 0);
+            for (int f = 0; f < 12; ++f) {
+                if (!host_out[f]) continue;
+                for (int m = 0; m < mates; ++m) {
+                    const size_t row0 = static_cast<size_t>(m) * n1 + a;
+                    ck(cudaMemcpyAsync(static_cast<char*>(host_out[f]) + row0 * width[f],
+                                       sl.out[f].as<char>() + static_cast<size_t>(m) * c * width[f], c * width[f],
+                                       cudaMemcpyDeviceToHost, st), "D2H");
+                }
+            }
+            ck(cudaEventRecord(ctx->slot_free[k & 1], st), "cudaEventRecord");
         }
         check_err_flag(ctx, st);
     });

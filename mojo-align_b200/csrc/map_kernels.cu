@@ -226,6 +226,16 @@ __device__ __forceinline__ void deletion_scan(const uint64_t* __restrict__ pacw,
 // One shift adj of one locus (b0, strand): the body of the reference's adj
 // loop, linear_gpu_fm.mojo:1528-1826.  Folds the candidate (full compare,
 // or the deletion probe's offsets) into `best` by its (nm, ordinal) key.
+// Tally of one evaluated locus: the distinct 32-B pac sectors its shifts
+// read, the text [b0 - adj_cap, b0 + adj_cap + qlen] at 4 bases a byte.
+__device__ __forceinline__ void tally_locus(Tally& t, int64_t b0, int adj_cap, int qlen) {
+    t.loci++;
+    int64_t lo = b0 - adj_cap;
+    if (lo < 0) lo = 0;
+    const int64_t hi = b0 + adj_cap + qlen;
+    if (hi >= lo) t.pac_sectors += static_cast<uint32_t>(((hi >> 2) >> 5) - ((lo >> 2) >> 5) + 1);
+}
+
 // Contig of a locus, looked up once for all of its shifts.
 struct ContigHint {
     int64_t crid, coff, clen;
@@ -342,11 +352,6 @@ __device__ void eval_adj(const DevIndex& ix, const ReadView& rd, int64_t b0, int
     const int64_t sr0 = local + qlen > clen ? local + qlen - clen : 0;
     if (!(sl0 + sr0 < qlen && sl0 <= clip_cap && sr0 <= clip_cap)) return;
     const uint32_t ord = (ord_row + static_cast<uint32_t>(adj + 12)) * KIND_SPAN;
-    if constexpr (S) {
-        // text bytes of the window [bstart, bstart + qlen], 4 bases a byte
-        const int64_t lo = (bstart < 0 ? 0 : bstart) >> 2, hi = (bstart + qlen) >> 2;
-        t.pac_sectors += static_cast<uint32_t>((hi >> 5) - (lo >> 5) + 1);
-    }
     const bool del_probe = adj == 0 && is_rev == 0;
     const bool del_room = del_probe && prune_nm > 1 && bstart + qlen + 1 <= coff + clen;
     // Exact pruning.  sl0, sr0 and every soft clip are at most clip_cap, so
@@ -383,7 +388,7 @@ template <bool S>
 __device__ void eval_locus(const DevIndex& ix, const ReadView& rd, int64_t b0, int is_rev, int adj_cap,
                            int budget, int clip_cap, uint32_t ord_row, Best& best, uint64_t uk, uint64_t ul,
                            int us, int e, Tally& t) {
-    if constexpr (S) t.loci++;
+    if constexpr (S) tally_locus(t, b0, adj_cap, rd.qlen);
     const ContigHint hint = contig_hint(ix, b0);
     for (int adj = -adj_cap; adj <= adj_cap; ++adj) {
         const uint64_t bn = best.key >> ORD_SHIFT;
@@ -871,7 +876,7 @@ __global__ void __launch_bounds__(S2_WARPS * 32, MINB) seed_stage2_kernel(DevInd
                     L.rev = rev;
                     L.hint = contig_hint(ix, b0);
                     s_loci[rank] = L;
-                    if constexpr (S) t.loci++;
+                    if constexpr (S) tally_locus(t, b0, cl.adj_cap, qlen);
                 }
                 n_memo += __popc(kb);
                 if (n_memo > MEMO2) n_memo = MEMO2;

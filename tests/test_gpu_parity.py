@@ -217,3 +217,27 @@ def test_toy_fixture_shape(ctx, tmp_path):
     for p in (FmParams(), FmParams(seed_len=19), FmParams(seed_len=8, max_occ=4096)):
         compare(prefix, ctx, bases, lens, 1, True, 32, p, k=0, k3=0)
         compare(prefix, ctx, bases, lens, 1, True, 32, p, k=4, k3=8)
+
+
+def test_host_batch_pipeline_matches_device_batch(ctx, small_ref):
+    """ma_map_batch pipelines large batches in chunks of pairs over two
+    streams; its outputs must equal one device-resident launch."""
+    torch = pytest.importorskip("torch")
+    from mojoalign_b200 import MapResult, map_batch_device
+
+    fa, prefix = small_ref
+    gi = gpu_index(ctx, prefix, 12, 12)
+    rb = sim(fa, 300_000, True, seed=31, sub_rate=0.01)
+    host = map_batch(ctx, gi, rb.bases, rb.lens, rb.n1, True, 150, "C2T", "G2A", BENCH_PARAMS, debug=True)
+    dev = torch.device("cuda:0")
+    d_bases = torch.from_numpy(rb.bases.reshape(-1)).to(dev)
+    d_lens = torch.from_numpy(rb.lens.view(np.int32)).to(dev)
+    out = {f: torch.empty(rb.n_seq, dtype=torch.int64 if f in ("uk", "ul") else torch.int32, device=dev)
+           for f in FIELDS}
+    map_batch_device(ctx, gi, d_bases.data_ptr(), d_lens.data_ptr(), rb.n1, True, 150,
+                     {f: out[f].data_ptr() for f in MapResult.FIELDS}, "C2T", "G2A", BENCH_PARAMS,
+                     d_debug={f: out[f].data_ptr() for f in MapResult.DEBUG},
+                     stream=torch.cuda.current_stream(dev).cuda_stream)
+    torch.cuda.synchronize()
+    for f in FIELDS:
+        assert np.array_equal(out[f].cpu().numpy(), getattr(host, f).view(out[f].cpu().numpy().dtype)), f
