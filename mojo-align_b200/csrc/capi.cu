@@ -317,6 +317,32 @@ void ma_index_options_default(ma_index_options* o) {
     o->hbm_budget_bytes = 0;
 }
 
+int ma_index_probe(const char* prefix, int kmer_k, int kmer3_k, ma_index_info* out) {
+    if (!prefix || !out) {
+        t_err = "null argument";
+        return MA_ERR_ARG;
+    }
+    return guarded(nullptr, [&] {
+        if (kmer_k < 0 || kmer_k > 14 || kmer3_k < 0 || kmer3_k > 20) fail(MA_ERR_ARG, "bad k-mer table sizes");
+        BwaIndexHost h = load_bwa_index(prefix);
+        ma_index_info I{};
+        I.seq_len = h.seq_len;
+        I.l_pac = h.l_pac;
+        I.primary = h.primary;
+        for (int c = 0; c < 5; ++c) I.L2[c] = h.L2[c];
+        I.sa_intv = h.sa_intv;
+        I.n_sa = h.n_sa;
+        I.n_contigs = static_cast<int64_t>(h.contigs.size());
+        uint64_t p0 = h.seq_len;
+        for (uint64_t v : h.sa) p0 = v < p0 ? v : p0;
+        I.sa_reject_below = p0;
+        I.kmer_k = kmer_k;
+        I.kmer3_k = kmer3_k;
+        I.device_bytes = device_index_bytes(h, kmer_k, kmer3_k) + device_index_staging_bytes(h, kmer3_k);
+        *out = I;
+    });
+}
+
 int ma_index_open(ma_ctx* ctx, const char* prefix, const ma_index_options* opt, ma_index** out) {
     if (!ctx || !prefix || !out) return MA_ERR_ARG;
     *out = nullptr;
@@ -423,6 +449,7 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
                               want_dbg ? dbg->score : nullptr};
         const size_t width[12] = {4, 4, 4, 4, 4, 4, 4, 8, 8, 4, 4, 4};
         int k = 0;
+        float acc_ms[4] = {0, 0, 0, 0};
         for (uint32_t a = 0; a < n1; a += chunk, ++k) {
             const uint32_t c = std::min(chunk, n1 - a);
             const int64_t cs = static_cast<int64_t>(c) * mates;
@@ -455,6 +482,16 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
             }
             enqueue_map(ctx, idx, sl.bases.as<uint8_t>(), sl.lens.as<uint32_t>(), c, paired, max_len, bs_r1, bs_r2,
                         p, o, st, k == 0);
+            if (ctx->profiling & 1) {
+                // profiling runs give up the overlap to time every chunk
+                ck(cudaStreamSynchronize(st), "chunk");
+                float ms[4] = {0, 0, 0, 0};
+                for (int i = 0; i < 3; ++i) ck(cudaEventElapsedTime(&ms[i], ctx->ev[i], ctx->ev[i + 1]), "elapsed");
+                if (!ctx->rescue_ran) ms[2] = 0;
+                ms[3] = ms[1];
+                if (ctx->tuning.seed_kernel == 1) ck(cudaEventElapsedTime(&ms[3], ctx->ev[1], ctx->ev[4]), "elapsed");
+                for (int i = 0; i < 4; ++i) acc_ms[i] += ms[i];
+            }
             for (int f = 0; f < 12; ++f) {
                 if (!host_out[f]) continue;
                 for (int m = 0; m < mates; ++m) {
@@ -467,6 +504,8 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
             ck(cudaEventRecord(ctx->slot_free[k & 1], st), "cudaEventRecord");
         }
         check_err_flag(ctx, st);
+        if (ctx->profiling & 1)
+            for (int i = 0; i < 4; ++i) ctx->kernel_ms[i] = acc_ms[i];
     });
 }
 

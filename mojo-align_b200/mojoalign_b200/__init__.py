@@ -4,8 +4,8 @@ The compute path is libmojoalign_b200.so (CUDA, sm_100a), loaded through
 ctypes by `_lib`; importing this package fails when the library is missing.
 """
 from ._lib import MojoAlignError
-from .mapper import GpuContext, GpuIndex, MapResult, build_index, map_batch, map_batch_device
+from .mapper import GpuContext, GpuIndex, MapResult, build_index, map_batch, map_batch_device, probe_index
 from .params import BENCH_PARAMS, FmParams
 
 __all__ = ["MojoAlignError", "GpuContext", "GpuIndex", "MapResult", "build_index", "map_batch",
-           "map_batch_device", "FmParams", "BENCH_PARAMS"]
+           "map_batch_device", "probe_index", "FmParams", "BENCH_PARAMS"]

@@ -131,6 +131,7 @@ SIGNATURES = [
     ("ma_index_options_default", None, [C.POINTER(ma_index_options)]),
     ("ma_index_open", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(ma_index_options), C.POINTER(C.c_void_p)]),
     ("ma_index_close", None, [C.c_void_p]),
+    ("ma_index_probe", C.c_int, [C.c_char_p, C.c_int, C.c_int, C.POINTER(ma_index_info)]),
     ("ma_index_get_info", C.c_int, [C.c_void_p, C.POINTER(ma_index_info)]),
     ("ma_index_contig", C.c_int,
      [C.c_void_p, C.c_int64, C.POINTER(C.c_char_p), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),

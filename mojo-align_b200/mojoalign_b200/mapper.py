@@ -209,10 +209,17 @@ def map_batch_device(ctx: GpuContext, index: GpuIndex, d_bases: int, d_lens: int
     check(rc, ctx.handle)
 
 
+def probe_index(prefix, kmer_k: int = 12, kmer3_k: int = 0) -> ma_index_info:
+    """Validates a bwa index on the host (no GPU) and reports its HBM need."""
+    info = ma_index_info()
+    check(lib.ma_index_probe(fspath(prefix), kmer_k, kmer3_k, C.byref(info)))
+    return info
+
+
 def build_index(fasta, out_prefix, bwameth_c2t: bool = True, sa_intv: int = 32, device: int = -1) -> None:
     """Writes a bwa-0.7 FM-index (optionally of the bwa-meth c2t text)."""
     check(lib.ma_index_build(fspath(fasta), fspath(out_prefix), int(bwameth_c2t), sa_intv, device))
 
 
-__all__ = ["GpuContext", "GpuIndex", "MapResult", "map_batch", "map_batch_device", "build_index", "bs_mode",
-           "_lib"]
+__all__ = ["GpuContext", "GpuIndex", "MapResult", "map_batch", "map_batch_device", "build_index", "probe_index",
+           "bs_mode", "_lib"]
