@@ -53,6 +53,15 @@ def parse_args():
     ap.add_argument("--workdir", default=os.environ.get("MOJOALIGN_BENCH_DIR", tempfile.gettempdir()))
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the oracle timing (profiling runs)")
+    ap.add_argument("--no-forms", action="store_true", help="skip the plain / batched / served comparison")
+    ap.add_argument("--forms-reads", type=int, default=4_000_000, help="uneven-length reads of the comparison")
+    ap.add_argument("--forms-ref-batches", type=int, default=64, help="16384-read batches timed in the "
+                    "reference-loop form")
+    ap.add_argument("--serve-pool", type=int, default=2_000_000, help="reads per simulated sample")
+    ap.add_argument("--serve-burst", type=int, default=160, help="requests of the saturation burst")
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="Poisson phase duration")
+    ap.add_argument("--serve-group", type=int, default=262144, help="reads (pairs) per launch group")
+    ap.add_argument("--serve-budget-gb", type=int, default=8, help="serving HBM budget")
     ap.add_argument("--tuning", default="", help="fixed kernel choice 'seed_kernel,stage1_endpoints,"
                     "stage2_blocks_per_sm,reg_level,stage1_max_rows,stage2_first_wave' instead of the autotuner")
     return ap.parse_args()
@@ -383,11 +392,215 @@ def run_ours(args, rank, world, local):
             g = np.concatenate([g[:n], g[args.pairs:args.pairs + n]])
             bad += int((g != o[f]).sum())
         line["parity_sample"] = {"reads": 2 * n, "mismatched_fields": bad}
+    if rank == 0 and world == 1 and not args.no_forms:
+        best = tuple(tune.tuning[f] for f in ("seed_kernel", "stage1_endpoints", "stage2_blocks_per_sm", "reg_level",
+                                             "stage1_max_rows", "stage2_first_wave"))
+        del d_bases, d_lens, d_out
+        torch.cuda.empty_cache()
+        line["forms"] = run_forms(args, ctx, gi, params, fa, local, best)
     if rank == 0:
         print(json.dumps(line), flush=True)
     gi.close()
     ctx.close()
     dist.close()
+
+
+UNEVEN_MODEL = dict(len_fixed=0, len_lognorm_median=120.0, len_lognorm_sigma=0.35, len_min=36, len_max=300,
+                    non_directional=0.5)
+UNEVEN_MAX = 300
+
+
+def serving_samples():
+    """Eight simulated samples: CpG retention 0.4-0.9 and three length
+    profiles (fixed 150; lognormal median 120 in 36-300; lognormal median 90,
+    sigma 0.5, in 36-250), mixed directional / non-directional."""
+    out = []
+    for k in range(8):
+        prof = k % 3
+        m = dict(cpg_retain=0.4 + 0.5 * k / 7, non_directional=0.25 * (k % 2))
+        if prof == 0:
+            m.update(len_fixed=150)
+            ml = 150
+        elif prof == 1:
+            m.update(len_fixed=0, len_lognorm_median=120.0, len_lognorm_sigma=0.35, len_min=36, len_max=300)
+            ml = 300
+        else:
+            m.update(len_fixed=0, len_lognorm_median=90.0, len_lognorm_sigma=0.5, len_min=36, len_max=250)
+            ml = 250
+        out.append((m, ml))
+    return out
+
+
+def log_uniform_sizes(rng, n, lo, hi):
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), n)).astype(np.int64)
+
+
+def run_forms(args, ctx, gi, params, fa, local, best_tuning):
+    """Plain single-launch vs batched vs served on uneven-length reads.
+
+    - plain_1launch: the reference's launch shape (one thread per read over
+      every right endpoint, seed_kernel 0), one launch over all reads, inputs
+      resident in HBM (device time);
+    - plain_reference_batches: the same kernel through ma_map_batch in the
+      reference's fixed 16384-read batches, one synchronous call per batch
+      (host time, copies included);
+    - batched: the autotuned two-stage persistent kernel (work queue), one
+      call over all reads, inputs resident (device time);
+    - served: the request loop (ma_serve_*), host buffers, copies included:
+      saturation throughput over a burst of requests from 8 samples
+      (log-uniform 1k-2M reads), then p50/p99/p99.9 request latency under
+      Poisson arrivals at half that throughput.
+    Every form's outputs for the uneven batch are compared with plain's.
+    """
+    import torch
+    from mojoalign_b200 import MapResult, map_batch, map_batch_device, synth
+    from mojoalign_b200.serve import Server, percentiles
+
+    n = args.forms_reads
+    dev = f"cuda:{local}"
+    pinned = torch.empty((n, UNEVEN_MAX), dtype=torch.uint8, pin_memory=True)
+    rb = synth.simulate_reads(fa, synth.ReadModel(**UNEVEN_MODEL), n, False, UNEVEN_MAX, seed=101,
+                              bases_out=pinned.numpy())
+    bases_np, lens_np = pinned.numpy(), rb.lens
+    d_bases = pinned.to(dev).reshape(-1)
+    d_lens = torch.from_numpy(lens_np.view(np.int32)).to(dev)
+    stream = torch.cuda.current_stream()
+    forms = {"workload": f"{n} single-end reads, lengths lognormal (median 120, sigma 0.35) clipped to 36-300, "
+                         f"half non-directional, on the {args.genome_mb} Mbp index",
+             "mean_len": round(float(lens_np.mean()), 1)}
+
+    def device_form(tuning, reps=3):
+        ctx.set_tuning(*tuning)
+        d_out = {f: torch.empty(n, dtype=torch.int32, device=dev) for f in MapResult.FIELDS}
+        ptrs = {f: t.data_ptr() for f, t in d_out.items()}
+
+        def go():
+            map_batch_device(ctx, gi, d_bases.data_ptr(), d_lens.data_ptr(), n, False, UNEVEN_MAX, ptrs, "C2T", "",
+                             params, stream=stream.cuda_stream)
+        go()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            go()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        return n / (ms / 1000.0), {f: t.cpu().numpy().view(np.uint32) for f, t in d_out.items()}
+
+    plain_tuning = (0, 1, 0, 1, 16, 32)
+    plain_rate, plain_out = device_form(plain_tuning)
+    batched_rate, batched_out = device_form(best_tuning)
+    same = all(np.array_equal(plain_out[f], batched_out[f]) for f in MapResult.FIELDS)
+    forms["plain_1launch"] = {"reads_per_s": round(plain_rate, 1), "tuning": "seed_kernel 0 (thread per read)",
+                              "timing": "device, inputs resident"}
+    forms["batched"] = {"reads_per_s": round(batched_rate, 1), "tuning": dict(zip(
+        ["seed_kernel", "stage1_endpoints", "stage2_blocks_per_sm", "reg_level", "stage1_max_rows",
+         "stage2_first_wave"], best_tuning)), "timing": "device, inputs resident", "equals_plain": same}
+
+    # the reference's loop: 16384-read synchronous batches of the same kernel
+    ctx.set_tuning(*plain_tuning)
+    res = MapResult.empty(n, debug=False)
+    nb = min(n, args.forms_ref_batches * 16384)
+    t = time.perf_counter()
+    for a in range(0, nb, 16384):
+        c = min(16384, nb - a)
+        sub = MapResult(*[getattr(res, f)[a:a + c] for f in MapResult.FIELDS])
+        map_batch(ctx, gi, bases_np[a:a + c], lens_np[a:a + c], c, False, UNEVEN_MAX, "C2T", "", params, out=sub)
+    ref_rate = nb / (time.perf_counter() - t)
+    forms["plain_reference_batches"] = {"reads_per_s": round(ref_rate, 1), "reads": nb, "batch": 16384,
+                                        "timing": "host, pinned host buffers, copies included",
+                                        "equals_plain": all(np.array_equal(getattr(res, f)[:nb].view(np.uint32), plain_out[f][:nb])
+                                                            for f in MapResult.FIELDS)}
+    ctx.set_tuning(*best_tuning)
+
+    # ---- served ----
+    rng = np.random.default_rng(7)
+    budget = args.serve_budget_gb << 30
+    with Server(ctx, gi, hbm_budget_bytes=budget, max_group_pairs=args.serve_group, max_inflight=3) as srv:
+        # the uneven batch itself as a request stream: equality with plain
+        sizes = log_uniform_sizes(rng, 4096, 1000, 2_000_000)
+        cuts, a = [], 0
+        for sz in sizes:
+            if a >= n:
+                break
+            cuts.append((a, int(min(sz, n - a))))
+            a += cuts[-1][1]
+        tickets = [srv.submit(bases_np[a:a + c], lens_np[a:a + c], c, False, UNEVEN_MAX, "C2T", "", params)
+                   for a, c in cuts]
+        srv.drain()
+        served_same = all(np.array_equal(getattr(t_.result, f).view(np.uint32), plain_out[f][a:a + c])
+                          for t_, (a, c) in zip(tickets, cuts) for f in MapResult.FIELDS)
+        del tickets
+
+        # 8 samples, each a pool of reads; requests are slices of a pool
+        pools = []
+        for k, (m, ml) in enumerate(serving_samples()):
+            pb = torch.empty((args.serve_pool, ml), dtype=torch.uint8, pin_memory=True)
+            r = synth.simulate_reads(fa, synth.ReadModel(**m), args.serve_pool, False, ml, seed=200 + k,
+                                     bases_out=pb.numpy())
+            pools.append((pb, pb.numpy(), r.lens, ml))
+
+        def request(k, size):
+            _, b, l, ml = pools[k]
+            size = int(min(size, args.serve_pool))
+            a = int(rng.integers(0, args.serve_pool - size + 1))
+            return b[a:a + size], l[a:a + size], size, ml
+
+        def burst(count):
+            reqs = [request(int(rng.integers(0, 8)), s) for s in log_uniform_sizes(rng, count, 1000, 2_000_000)]
+            t0 = time.perf_counter()
+            for b, l, c, ml in reqs:
+                srv.submit(b, l, c, False, ml, "C2T", "", params)
+            srv.drain()
+            return sum(r[2] for r in reqs) / (time.perf_counter() - t0)
+
+        burst(16)  # warm-up
+        g0 = srv.stats()
+        sat = burst(args.serve_burst)
+        g1 = srv.stats()
+        # Poisson arrivals at half the saturation rate
+        mean_size = (2_000_000 - 1000) / np.log(2_000_000 / 1000)
+        lam = 0.5 * sat / mean_size
+        _, _, before = srv.latencies()
+        n0 = before.size
+        t0 = time.perf_counter()
+        t_next = t0
+        sent = 0
+        while t_next - t0 < args.serve_seconds:
+            now = time.perf_counter()
+            if now < t_next:
+                time.sleep(t_next - now)
+            b, l, c, ml = request(int(rng.integers(0, 8)), log_uniform_sizes(rng, 1, 1000, 2_000_000)[0])
+            srv.submit(b, l, c, False, ml, "C2T", "", params)
+            sent += c
+            t_next += rng.exponential(1.0 / lam)
+        srv.drain()
+        wall = time.perf_counter() - t0
+        _, reads, ms = srv.latencies()
+        ms, reads = ms[n0:], reads[n0:]
+        st = srv.stats()
+    small = ms[reads <= 10_000]
+    forms["served"] = {
+        "reads_per_s": round(sat, 1), "timing": "host, submit to last completion, copies included",
+        "burst_requests": args.serve_burst, "groups_in_burst": g1["groups_issued"] - g0["groups_issued"],
+        "equals_plain": bool(served_same),
+        "poisson": {"offered_reads_per_s": round(0.5 * sat, 1), "achieved_reads_per_s": round(sent / wall, 1),
+                    "seconds": round(wall, 1), "requests": int(ms.size),
+                    "latency_ms": {k: (round(v, 2) if v is not None else None)
+                                   for k, v in percentiles(ms).items()},
+                    "latency_ms_requests_le_10k_reads": {k: (round(v, 2) if v is not None else None)
+                                                         for k, v in percentiles(small).items()}},
+        "options": {"hbm_budget_bytes": budget, "max_group_pairs": args.serve_group, "max_inflight": 3},
+        "stats": {k: st[k] for k in ("groups_issued", "parts_issued", "max_requests_in_group",
+                                     "max_groups_in_flight", "peak_bytes", "admission_waits")},
+        "samples": "8 (CpG retention 0.4-0.9; fixed 150 / lognormal 120 / lognormal 90 length profiles), "
+                   f"pools of {args.serve_pool} reads, request sizes log-uniform 1k-2M reads"}
+    forms["served_over_plain_1launch"] = round(sat / plain_rate, 3)
+    forms["served_over_plain_reference_batches"] = round(sat / ref_rate, 3)
+    forms["batched_over_plain_1launch"] = round(batched_rate / plain_rate, 3)
+    del d_bases, d_lens, pools
+    return forms
 
 
 def _cpu_model() -> str:

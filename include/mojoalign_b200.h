@@ -271,6 +271,87 @@ typedef struct ma_tuning {
 int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t);
 int ma_ctx_get_tuning(const ma_ctx* ctx, ma_tuning* t);
 
+/* ---- served form: a request loop over a resident index ----------------
+ *
+ * No counterpart in the reference, whose map_fastq_fm_gpu maps one FASTQ
+ * stream in fixed 16384-pair batches (linear_gpu_fm.mojo:2074, 2438-3094).
+ * A server keeps one resident index and maps requests (read batches of any
+ * size, from any number of samples) submitted from any host thread:
+ *   - admission: the server reserves hbm_budget_bytes of device memory
+ *     once and carves every launch group's buffers out of it; a group is
+ *     issued only when its buffers fit in what is free, so the work in
+ *     flight never exceeds the budget;
+ *   - continuous batching: one launch group takes the pending work of
+ *     several requests (in arrival order, up to max_group_pairs pairs;
+ *     requests with the same `paired` and parameters merge; lengths and
+ *     bisulfite modes may differ) and a large request is split over
+ *     several groups, so requests that arrive while others are on the GPU
+ *     join the next group as memory frees;
+ *   - overlap: up to max_inflight groups are in flight on their own
+ *     streams, so one group's copies and kernels overlap another's.
+ * Every read's outputs are those ma_map_batch gives for it alone.  The
+ * caller's host buffers (reads and ma_hits arrays) must stay valid and
+ * unmodified until the request completes.  Requests complete in any
+ * order; latency is measured from submit to completion on the host clock.
+ */
+typedef struct ma_server ma_server;
+
+/* MA_SERVE_SCHEDULER_TEST: no device work at all; each launch group's
+ * "mapping" is a host function of the packed reads (rid = read length,
+ * pos = FNV-1a hash of the converted read, nm = the mate's hash, mapq =
+ * seed_len, flag = 128 for second mates, sl/sr = 0).  It is not an
+ * aligner: it exercises admission, grouping and result scatter without a
+ * GPU. */
+#define MA_SERVE_SCHEDULER_TEST 1
+
+typedef struct ma_serve_options {
+    uint64_t hbm_budget_bytes; /* 0 = min(free HBM / 4, 16 GiB)             */
+    uint32_t max_group_pairs;  /* pairs (or SE reads) per launch group,
+                                  default 262144                            */
+    uint32_t max_inflight;     /* launch groups in flight, default 3        */
+    uint32_t flags;            /* MA_SERVE_* bits                           */
+} ma_serve_options;
+
+typedef struct ma_serve_stats {
+    uint64_t requests_submitted, requests_completed, requests_failed;
+    uint64_t reads_completed;   /* each mate counts as one read             */
+    uint64_t groups_issued, parts_issued; /* parts: request pieces in groups */
+    uint64_t max_requests_in_group;
+    uint64_t max_groups_in_flight;
+    uint64_t budget_bytes, peak_bytes; /* reserved budget, peak in use     */
+    uint64_t admission_waits;   /* times a group waited for memory         */
+} ma_serve_stats;
+
+void ma_serve_options_default(ma_serve_options* o);
+/* ctx supplies the device and the kernel tuning (copied); idx must stay open
+ * until the server is destroyed.  With MA_SERVE_SCHEDULER_TEST, ctx and idx
+ * may be NULL. */
+int ma_serve_create(ma_ctx* ctx, const ma_index* idx,
+                    const ma_serve_options* opt, ma_server** out);
+/* Queues a request (the ma_map_batch arguments, host buffers) and returns
+ * at once with its id.  Fails with MA_ERR_ARG on bad arguments and
+ * MA_ERR_NOMEM when one pair of the request cannot fit the budget. */
+int ma_serve_submit(ma_server* s, const uint8_t* bases, const uint32_t* lens,
+                    uint32_t n1, int paired, uint32_t max_len, int bs_r1,
+                    int bs_r2, const ma_params* p, const ma_hits* out,
+                    uint64_t* request_id);
+/* *done = 1 once the request has completed; returns its status then. */
+int ma_serve_poll(ma_server* s, uint64_t request_id, int* done);
+/* Waits for one request (timeout_ms < 0: no limit); MA_ERR_TIMEOUT when
+ * the time runs out first, else the request's status. */
+int ma_serve_wait(ma_server* s, uint64_t request_id, int timeout_ms);
+/* Waits until every submitted request has completed. */
+int ma_serve_drain(ma_server* s, int timeout_ms);
+int ma_serve_get_stats(ma_server* s, ma_serve_stats* out);
+/* Completed requests in completion order: ids, reads and latency (ms).
+ * Copies min(cap, count) entries; *count gets the total. */
+int ma_serve_latencies(ma_server* s, uint64_t* ids, uint64_t* reads,
+                       double* ms, uint64_t cap, uint64_t* count);
+/* Message of the last failure on the server (or of a failed request). */
+const char* ma_serve_last_error(const ma_server* s);
+/* Drains, stops the worker threads and frees the reserved memory. */
+void ma_serve_destroy(ma_server* s);
+
 /* ---- measurement (no reference counterpart; the reference only prints
  * perf_counter stage timers, linear_gpu_fm.mojo:2270-2273,3317-3340) ---- */
 

@@ -105,6 +105,13 @@ const DevIndex* index_device_view(const ma_index* idx, int* device) {
     if (device) *device = idx->ctx->device;
     return &idx->dix;
 }
+
+// Device ordinal, SM count and kernel tuning of a context.
+void ctx_launch_config(const ma_ctx* ctx, int* device, int* sm_count, ma_tuning* tuning) {
+    *device = ctx->device;
+    *sm_count = ctx->sm_count;
+    *tuning = ctx->tuning;
+}
 }  // namespace ma
 
 namespace {

@@ -77,6 +77,17 @@ struct DevReads {
     int64_t n_seq;
 };
 
+// One request's piece of a merged batch (pack_parts_kernel).
+struct PackPart {
+    uint64_t src;      // byte offset of the piece's first row in the staged bases
+    int64_t row0;      // index of that row among all staged rows of the batch
+    uint32_t c;        // pairs (or single reads) in the piece
+    uint32_t max_len;  // row stride of the piece's staged rows
+    int32_t bs_r1, bs_r2;
+    uint32_t dst;      // batch pair offset of the piece's first pair
+    uint32_t pad;
+};
+
 struct DevOut {
     int32_t* rid;
     uint32_t* pos;

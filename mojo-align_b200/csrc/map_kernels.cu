@@ -499,22 +499,11 @@ __device__ __forceinline__ Seed search_endpoint(const DevIndex& ix, const ReadVi
     return res;
 }
 
-__global__ void __launch_bounds__(256) pack_reads_kernel(const uint8_t* __restrict__ bases,
-                                                         const uint32_t* __restrict__ lens, int64_t n_seq,
-                                                         int64_t n1, int max_len, int words, int bs_r1,
-                                                         int bs_r2, uint64_t* __restrict__ packed,
-                                                         int* __restrict__ err) {
-    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    const int64_t r = t / words;
-    const int w = static_cast<int>(t - r * words);
-    if (r >= n_seq) return;
-    int len = static_cast<int>(lens[r]);
-    if (len > max_len) {
-        atomicExch(err, 1);
-        len = max_len;
-    }
-    const int mode = r < n1 ? bs_r1 : bs_r2;
-    const uint8_t* row = bases + r * static_cast<int64_t>(max_len);
+// Word w of packed read row `row` (len bases, conversion `mode`): forward
+// codes, reverse-complement codes and the two non-ACGT masks, each at
+// `words` stride from `out`.
+__device__ __forceinline__ void pack_word(const uint8_t* __restrict__ row, int len, int mode, int w, int words,
+                                          uint64_t* __restrict__ out) {
     uint64_t f = 0, fn = 0, rw = 0, rn = 0;
     for (int i = 0; i < 32; ++i) {
         const int j = 32 * w + i;
@@ -526,11 +515,66 @@ __global__ void __launch_bounds__(256) pack_reads_kernel(const uint8_t* __restri
         if (c2 > 3) rn |= 1ull << (2 * i);
         else rw |= static_cast<uint64_t>(3 - c2) << (2 * i);
     }
-    uint64_t* out = packed + r * 4 * static_cast<int64_t>(words);
     out[w] = f;
     out[words + w] = rw;
     out[2 * words + w] = fn;
     out[3 * words + w] = rn;
+}
+
+// Source row r (stride max_len) lands at batch row dst1 + r for the first
+// n1 rows and dst2 + (r - n1) after them; lens are read at the batch row.  A
+// plain batch uses dst1 = 0, dst2 = n1.
+__global__ void __launch_bounds__(256) pack_reads_kernel(const uint8_t* __restrict__ bases,
+                                                         const uint32_t* __restrict__ lens, int64_t n_seq,
+                                                         int64_t n1, int max_len, int words, int bs_r1,
+                                                         int bs_r2, int64_t dst1, int64_t dst2,
+                                                         uint64_t* __restrict__ packed, int* __restrict__ err) {
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int64_t r = t / words;
+    const int w = static_cast<int>(t - r * words);
+    if (r >= n_seq) return;
+    const int64_t d = r < n1 ? dst1 + r : dst2 + (r - n1);
+    int len = static_cast<int>(lens[d]);
+    if (len > max_len) {
+        atomicExch(err, 1);
+        len = max_len;
+    }
+    pack_word(bases + r * static_cast<int64_t>(max_len), len, r < n1 ? bs_r1 : bs_r2, w, words,
+              packed + d * 4 * static_cast<int64_t>(words));
+}
+
+// A batch merged from several requests.  Part j holds c pairs (or single
+// reads) staged at byte `src` of `bases`: its c first mates, then its c
+// second mates, rows of stride max_len.  Its pair i lands at batch row
+// dst + i and, when paired, n1_batch + dst + i.  Source rows of all parts
+// are numbered consecutively from 0 (part j's first row is row0).
+__global__ void __launch_bounds__(256) pack_parts_kernel(const uint8_t* __restrict__ bases,
+                                                         const uint32_t* __restrict__ lens,
+                                                         const PackPart* __restrict__ parts, int n_parts,
+                                                         int64_t n_rows, int64_t n1_batch, int words,
+                                                         uint64_t* __restrict__ packed, int* __restrict__ err) {
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int64_t r = t / words;
+    const int w = static_cast<int>(t - r * words);
+    if (r >= n_rows) return;
+    int lo = 0, hi = n_parts - 1;  // last part with row0 <= r
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (parts[mid].row0 <= r) lo = mid;
+        else hi = mid - 1;
+    }
+    const PackPart pp = parts[lo];
+    const int64_t local = r - pp.row0;
+    const bool second = local >= pp.c;
+    const int64_t i = second ? local - pp.c : local;
+    const int64_t d = second ? n1_batch + pp.dst + i : pp.dst + i;
+    int len = static_cast<int>(lens[d]);
+    if (len > static_cast<int>(pp.max_len)) {
+        atomicExch(err, 1);
+        len = static_cast<int>(pp.max_len);
+    }
+    pack_word(bases + pp.src + local * static_cast<int64_t>(pp.max_len), len, second ? pp.bs_r2 : pp.bs_r1, w,
+              words, packed + d * 4 * static_cast<int64_t>(words));
 }
 
 // Per-read clamps of linear_gpu_fm.mojo:1204-1216.
@@ -1031,6 +1075,16 @@ int launch_pack(const uint8_t* d_bases, const uint32_t* d_lens, int64_t n_seq, i
                 int bs_r1, int bs_r2, uint64_t* d_packed, int* d_err, cudaStream_t st) {
     const int64_t n = n_seq * words;
     pack_reads_kernel<<<grid_for(n, 256), 256, 0, st>>>(d_bases, d_lens, n_seq, n1, max_len, words, bs_r1, bs_r2,
+                                                        0, n1, d_packed, d_err);
+    return 1;
+}
+
+// Packs the parts of a merged batch (see pack_parts_kernel); d_lens is the
+// batch's length array, already at the batch rows.
+int launch_pack_parts(const uint8_t* d_bases, const uint32_t* d_lens, const PackPart* d_parts, int n_parts,
+                      int64_t n_rows, int64_t n1_batch, int words, uint64_t* d_packed, int* d_err, cudaStream_t st) {
+    const int64_t n = n_rows * words;
+    pack_parts_kernel<<<grid_for(n, 256), 256, 0, st>>>(d_bases, d_lens, d_parts, n_parts, n_rows, n1_batch, words,
                                                         d_packed, d_err);
     return 1;
 }

@@ -120,6 +120,20 @@ class ma_read_model(C.Structure):
     ]
 
 
+class ma_serve_options(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_group_pairs", C.c_uint32), ("max_inflight", C.c_uint32),
+                ("flags", C.c_uint32)]
+
+
+class ma_serve_stats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in (
+        "requests_submitted", "requests_completed", "requests_failed", "reads_completed", "groups_issued",
+        "parts_issued", "max_requests_in_group", "max_groups_in_flight", "budget_bytes", "peak_bytes",
+        "admission_waits")]
+
+
+MA_SERVE_SCHEDULER_TEST = 1
+
 # (name, restype, argtypes) of every exported entry point of the header.
 SIGNATURES = [
     ("ma_params_default", None, [C.POINTER(ma_params)]),
@@ -151,6 +165,19 @@ SIGNATURES = [
     ("ma_ctx_kernel_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     ("ma_ctx_traffic", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     ("ma_bench_gather", C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_uint64, C.POINTER(C.c_double)]),
+    ("ma_serve_options_default", None, [C.POINTER(ma_serve_options)]),
+    ("ma_serve_create", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(ma_serve_options), C.POINTER(C.c_void_p)]),
+    ("ma_serve_submit", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_uint32, C.c_int, C.c_int, C.POINTER(ma_params),
+      C.POINTER(ma_hits), C.POINTER(C.c_uint64)]),
+    ("ma_serve_poll", C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_int)]),
+    ("ma_serve_wait", C.c_int, [C.c_void_p, C.c_uint64, C.c_int]),
+    ("ma_serve_drain", C.c_int, [C.c_void_p, C.c_int]),
+    ("ma_serve_get_stats", C.c_int, [C.c_void_p, C.POINTER(ma_serve_stats)]),
+    ("ma_serve_latencies", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("ma_serve_last_error", C.c_char_p, [C.c_void_p]),
+    ("ma_serve_destroy", None, [C.c_void_p]),
     ("ma_synth_reference", C.c_int, [C.c_char_p, C.c_uint64, C.c_int, C.c_double, C.c_double, C.c_uint64]),
     ("ma_synth_reads", C.c_int,
      [C.c_char_p, C.POINTER(ma_read_model), C.c_uint32, C.c_int, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p,
