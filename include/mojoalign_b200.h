@@ -365,8 +365,9 @@ int ma_ctx_kernel_ms(const ma_ctx* ctx, float* out4);
 /* Tallies of the last counting call: 32-B Occ lines, k-mer entries, SA
  * entries, distinct 32-B pac sectors per evaluated locus, backward steps,
  * endpoints searched, loci evaluated, read words read, endpoints skipped as
- * predicted duplicates. */
-int ma_ctx_traffic(const ma_ctx* ctx, uint64_t* out9);
+ * predicted duplicates, reads handled by stage 2, stage-2 endpoint groups,
+ * shift evaluations. */
+int ma_ctx_traffic(const ma_ctx* ctx, uint64_t* out12);
 /* Random aligned `line_bytes` (32 or 64) gathers over a buffer of
  * buffer_bytes: achieved GB/s (the random-gather roofline). */
 int ma_bench_gather(ma_ctx* ctx, uint64_t buffer_bytes, int line_bytes, uint64_t n_loads, double* gbps);

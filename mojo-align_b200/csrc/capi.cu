@@ -71,7 +71,7 @@ struct ma_ctx {
     int profiling = 0;           // bit 0: per-kernel events, bit 1: traffic tally
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // pack | stage 1 | stage 2 | rescue
     float kernel_ms[4] = {0, 0, 0, 0};  // pack, seed (both stages), rescue, stage 1 alone
-    uint64_t traffic[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    uint64_t traffic[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     bool rescue_ran = false;
     DevBuf tally;
     // two-slot pipeline of ma_map_batch: H2D of chunk k+1 on copy_stream
@@ -180,9 +180,9 @@ void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const
     const bool timed = ctx->profiling & 1;
     unsigned long long* d_tally = nullptr;
     if (ctx->profiling & 2) {
-        ctx->tally.ensure(9 * sizeof(unsigned long long));
+        ctx->tally.ensure(12 * sizeof(unsigned long long));
         d_tally = ctx->tally.as<unsigned long long>();
-        ck(cudaMemsetAsync(d_tally, 0, 9 * sizeof(unsigned long long), st), "memset");
+        ck(cudaMemsetAsync(d_tally, 0, 12 * sizeof(unsigned long long), st), "memset");
     }
     if (timed) ck(cudaEventRecord(ctx->ev[0], st), "event");
     launches += launch_pack(d_bases, d_lens, n_seq, n1, static_cast<int>(max_len), words, bs_r1, bs_r2,
@@ -223,9 +223,9 @@ void check_err_flag(ma_ctx* ctx, cudaStream_t st) {
         if (ctx->tuning.seed_kernel == 1) ck(cudaEventElapsedTime(&ctx->kernel_ms[3], ctx->ev[1], ctx->ev[4]), "elapsed");
     }
     if (ctx->profiling & 2) {
-        unsigned long long t[9];
+        unsigned long long t[12];
         ck(cudaMemcpy(t, ctx->tally.p, sizeof t, cudaMemcpyDeviceToHost), "D2H tally");
-        for (int i = 0; i < 9; ++i) ctx->traffic[i] = t[i];
+        for (int i = 0; i < 12; ++i) ctx->traffic[i] = t[i];
     }
 }
 
@@ -584,9 +584,9 @@ int ma_ctx_kernel_ms(const ma_ctx* ctx, float* out4) {
     return MA_OK;
 }
 
-int ma_ctx_traffic(const ma_ctx* ctx, uint64_t* out9) {
-    if (!ctx || !out9) return MA_ERR_ARG;
-    for (int i = 0; i < 9; ++i) out9[i] = ctx->traffic[i];
+int ma_ctx_traffic(const ma_ctx* ctx, uint64_t* out12) {
+    if (!ctx || !out12) return MA_ERR_ARG;
+    for (int i = 0; i < 12; ++i) out12[i] = ctx->traffic[i];
     return MA_OK;
 }
 

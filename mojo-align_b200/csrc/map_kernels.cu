@@ -92,8 +92,9 @@ __device__ __forceinline__ uint64_t window_bits(const uint64_t* words, int s, in
 // away.
 struct Tally {
     uint32_t occ_lines, kmer_loads, sa_loads, pac_sectors, steps, endpoints, loci, read_words, skipped;
+    uint32_t s2_reads, s2_groups, shifts;  // stage-2 reads, stage-2 endpoint groups, shift evaluations
 };
-constexpr int TALLY_N = 9;
+constexpr int TALLY_N = 12;
 
 // Mismatch bits (even positions) of read word w against the text at
 // bstart + 32*w; N bases always mismatch.
@@ -333,6 +334,7 @@ template <bool S>
 __device__ void eval_adj(const DevIndex& ix, const ReadView& rd, int64_t b0, int is_rev, int adj, int budget,
                          int clip_cap, uint32_t ord_row, Best& best, uint64_t uk, uint64_t ul, int us, int e,
                          int prune_nm, const ContigHint& hint, Tally& t) {
+    if constexpr (S) t.shifts++;
     const int qlen = rd.qlen;
     const uint64_t* q = is_rev ? rd.rc : rd.fwd;
     const uint64_t* qn = is_rev ? rd.nr : rd.nf;
@@ -357,7 +359,13 @@ __device__ void eval_adj(const DevIndex& ix, const ReadView& rd, int64_t b0, int
     // Exact pruning.  sl0, sr0 and every soft clip are at most clip_cap, so
     // the full compare and any clipped recount both span read positions
     // [clip_cap, qlen - clip_cap); their mismatches bound nm from below.
-    const int core = count_mm<S>(ix.pacw, q, qn, bstart, clip_cap, qlen - clip_cap, budget + 1, t);
+    if (!del_probe) {
+        // a shift without deletion probe only matters with a core below
+        // both the budget and the best so far: count no further
+        const int cap = prune_nm < budget + 1 ? prune_nm : budget + 1;
+        if (count_mm<S>(ix.pacw, q, qn, bstart, clip_cap, qlen - clip_cap, cap, t) >= cap) return;
+    }
+    const int core = del_probe ? count_mm<S>(ix.pacw, q, qn, bstart, clip_cap, qlen - clip_cap, budget + 1, t) : 0;
     if (core > budget) {
         // neither compare is accepted: only the deletion probe remains
         if (del_room)
@@ -395,6 +403,55 @@ __device__ void eval_locus(const DevIndex& ix, const ReadView& rd, int64_t b0, i
         eval_adj<S>(ix, rd, b0, is_rev, adj, budget, clip_cap, ord_row, best, uk, ul, us, e,
                     bn < (1u << 20) ? static_cast<int>(bn) : (1 << 20), hint, t);
     }
+}
+
+// Exact early stop for a best hit with nm == 1.  Every later candidate
+// comes after the best in the reference's order, so only an nm == 0
+// candidate could replace it; deletion-probe candidates have nm >= 1, so it
+// would be a full or clipped compare with no mismatch over the read's core
+// [clip_cap, qlen - clip_cap) (soft and contig-edge clips are at most
+// clip_cap each).  The best hit, a full or clipped compare aligning the read
+// at text position bstart, has at most one mismatch p in the core, which
+// splits the core into at most two segments matching the text at bstart
+// exactly.  An nm == 0 candidate at any other text position (either strand)
+// would hold each segment a second time, so if one segment's text is unique
+// in the dual-strand text (its length reaches the shortest unique length of
+// the text ending at its last base, from the summary), no nm == 0 candidate
+// exists.  A candidate at bstart itself on the same strand is the same
+// compare and has nm == 1.  An N in the core mismatches every candidate, so
+// then no nm == 0 candidate exists either.
+template <bool S>
+__device__ bool exact_hit_impossible(const DevIndex& ix, const ReadView& rd, int64_t bstart, int rev, int clip_cap,
+                                     Tally& t) {
+    const int qlen = rd.qlen;
+    const int c0 = clip_cap, c1 = qlen - clip_cap;
+    if (!ix.summary || c1 <= c0 || bstart + c0 < 0 || bstart + c1 > static_cast<int64_t>(ix.l_pac)) return false;
+    const uint64_t* q = rev ? rd.rc : rd.fwd;
+    const uint64_t* qn = rev ? rd.nr : rd.nf;
+    int p = -1;
+    for (int w = c0 >> 5; w <= (c1 - 1) >> 5; ++w) {
+        const uint64_t rm = range_mask(w, c0, c1);
+        if (qn[w] & rm) return true;
+        uint64_t m = mm_word<S>(ix.pacw, q, qn, bstart, w, t) & rm;
+        while (m) {
+            if (p >= 0) return false;
+            p = 32 * w + (__ffsll(static_cast<long long>(m)) - 1) / 2;
+            m &= m - 1;
+        }
+    }
+    const int u0 = c0, v0 = p < 0 ? c1 : p, u1 = p + 1, v1 = c1;
+    for (int k = 0; k < (p < 0 ? 1 : 2); ++k) {
+        const int u = k ? u1 : u0, v = k ? v1 : v0;
+        if (v <= u) continue;
+        const int mul = __ldg(ix.summary + bstart + v - 1) & 0xFF;
+        if (mul != 255 && mul <= v - u) return true;
+    }
+    return false;
+}
+
+// Whether a best key is a full or clipped compare (not a deletion offset).
+__device__ __forceinline__ bool full_compare_key(uint64_t key) {
+    return (static_cast<uint32_t>(key & ((1ull << ORD_SHIFT) - 1)) % KIND_SPAN) == 0;
 }
 
 struct Seed {
@@ -651,7 +708,8 @@ template <bool S>
 __device__ __forceinline__ void flush_tally(const Tally& t, unsigned long long* tally_out) {
     if constexpr (S) {
         const uint32_t v[TALLY_N] = {t.occ_lines, t.kmer_loads, t.sa_loads, t.pac_sectors, t.steps,
-                                     t.endpoints, t.loci, t.read_words, t.skipped};
+                                     t.endpoints, t.loci, t.read_words, t.skipped, t.s2_reads, t.s2_groups,
+                                     t.shifts};
         for (int i = 0; i < TALLY_N; ++i)
             if (v[i]) atomicAdd(tally_out + i, static_cast<unsigned long long>(v[i]));
     }
@@ -717,7 +775,12 @@ __global__ void __launch_bounds__(128, MINB) seed_stage1_kernel(DevIndex ix, Dev
 done:
     write_hit(out, r, best, qlen);
     {
-        const bool pend = h.pending && (best.key >> ORD_SHIFT) != 0 && n_end > resume;
+        bool pend = h.pending && (best.key >> ORD_SHIFT) != 0 && n_end > resume;
+        if (pend && (best.key >> ORD_SHIFT) == 1 && full_compare_key(best.key)) {
+            const int64_t bstart = static_cast<int64_t>(__ldg(ix.coff + best.crid)) + best.pos - best.sl;
+            if (exact_hit_impossible<S>(ix, rd, bstart, (best.flag & 16) ? 1 : 0, clamps_for(P, qlen).clip_cap, t))
+                pend = false;
+        }
         if (pend) {
             h.key[r] = best.key;
             h.resume[r] = static_cast<uint16_t>(resume);
@@ -833,6 +896,7 @@ __global__ void __launch_bounds__(S2_WARPS * 32, MINB) seed_stage2_kernel(DevInd
         qi = __shfl_sync(FULL, qi, 0);
         if (qi >= n_pending) break;
         const int64_t r = h.pending[qi];
+        if constexpr (S) t.s2_reads += lane == 0;
         const int words = R.words;
         const uint64_t* g = R.packed + r * 4 * static_cast<int64_t>(words);
         for (int i = lane; i < 4 * words; i += 32) s_words[i] = g[i];
@@ -850,6 +914,7 @@ __global__ void __launch_bounds__(S2_WARPS * 32, MINB) seed_stage2_kernel(DevInd
         const int A = 2 * cl.adj_cap + 1;
         const int n_end = endpoint_count(P, qlen);
         uint64_t best_key = h.key[r];
+        uint64_t tested_key = best_key;  // stage 1 ran the early-stop test on its best
         Best win;  // valid when improved
         win.crid = -1;
         bool improved = false;
@@ -857,6 +922,7 @@ __global__ void __launch_bounds__(S2_WARPS * 32, MINB) seed_stage2_kernel(DevInd
         const bool can_predict = ix.summary && ix.kmer3_k > 0 && ix.kmer3_k <= P.seed_len;
         int width = first_wave;
         for (int j0 = h.resume[r]; j0 < n_end; j0 += width, width = 32) {
+            if constexpr (S) t.s2_groups += lane == 0;
             const int j = j0 + lane;
             const int e = P.seed_len - 1 + j * P.seed_stride;
             Seed sd{0, 0, -1, false};
@@ -961,6 +1027,16 @@ __global__ void __launch_bounds__(S2_WARPS * 32, MINB) seed_stage2_kernel(DevInd
                 __syncwarp();
             }
             if ((best_key >> ORD_SHIFT) == 0) break;
+            if ((best_key >> ORD_SHIFT) == 1 && best_key != tested_key && full_compare_key(best_key)) {
+                tested_key = best_key;
+                // every lane runs the same test on the same data
+                const int32_t crid = improved ? win.crid : out.rid[r];
+                const int64_t pos = improved ? win.pos : out.pos[r];
+                const int sl = improved ? win.sl : static_cast<int>(out.sl[r]);
+                const int rev = ((improved ? win.flag : out.flag[r]) & 16) ? 1 : 0;
+                const int64_t bstart = static_cast<int64_t>(__ldg(ix.coff + crid)) + pos - sl;
+                if (exact_hit_impossible<S>(ix, rd, bstart, rev, cl.clip_cap, t)) break;
+            }
         }
         if (improved && lane == 0) write_hit(out, r, win, qlen);
         __syncwarp();

@@ -65,7 +65,7 @@ class GpuContext:
         return list(v)
 
     def traffic(self) -> list[int]:
-        v = (C.c_uint64 * 9)()
+        v = (C.c_uint64 * 12)()
         check(lib.ma_ctx_traffic(self.handle, v), self.handle)
         return list(v)
 
