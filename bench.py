@@ -63,7 +63,8 @@ def parse_args():
     ap.add_argument("--serve-group", type=int, default=262144, help="reads (pairs) per launch group")
     ap.add_argument("--serve-budget-gb", type=int, default=8, help="serving HBM budget")
     ap.add_argument("--tuning", default="", help="fixed kernel choice 'seed_kernel,stage1_endpoints,"
-                    "stage2_blocks_per_sm,reg_level,stage1_max_rows,stage2_first_wave' instead of the autotuner")
+                    "stage2_blocks_per_sm,reg_level,stage1_max_rows,stage2_first_wave[,wave_endpoints,"
+                    "wave_loci_per_read,wave_max_rounds]' instead of the autotuner")
     return ap.parse_args()
 
 
@@ -264,6 +265,7 @@ def run_ours(args, rank, world, local):
         from mojoalign_b200.autotune import FIELDS, TuneResult
 
         fixed = [int(x) for x in args.tuning.split(",")]
+        fixed += [1, 1, 0, 1, 2, 32, 32, 4, 0][len(fixed):]
         ctx.set_tuning(*fixed)
         tune = TuneResult(dict(zip(FIELDS, fixed)), float("nan"), [])
         ns = 0
@@ -395,8 +397,9 @@ def run_ours(args, rank, world, local):
             bad += int((g != o[f]).sum())
         line["parity_sample"] = {"reads": 2 * n, "mismatched_fields": bad}
     if rank == 0 and world == 1 and not args.no_forms:
-        best = tuple(tune.tuning[f] for f in ("seed_kernel", "stage1_endpoints", "stage2_blocks_per_sm", "reg_level",
-                                             "stage1_max_rows", "stage2_first_wave"))
+        from mojoalign_b200.autotune import FIELDS as TFIELDS
+
+        best = tuple(tune.tuning[f] for f in TFIELDS if f in tune.tuning)
         del d_bases, d_lens, d_out
         torch.cuda.empty_cache()
         line["forms"] = run_forms(args, ctx, gi, params, fa, local, best)
@@ -490,16 +493,17 @@ def run_forms(args, ctx, gi, params, fa, local, best_tuning):
         ms = e0.elapsed_time(e1) / reps
         return n / (ms / 1000.0), {f: t.cpu().numpy().view(np.uint32) for f, t in d_out.items()}
 
-    plain_tuning = (0, 1, 0, 1, 16, 32)
+    plain_tuning = (0, 1, 0, 1, 16, 32, 32, 4, 0)
     plain_rate, plain_out = device_form(plain_tuning)
     batched_rate, batched_out = device_form(best_tuning)
     same = all(np.array_equal(plain_out[f], batched_out[f]) for f in MapResult.FIELDS)
     forms["mapped_frac"] = round(float((plain_out["rid"].view(np.int32) >= 0).mean()), 4)
     forms["plain_1launch"] = {"reads_per_s": round(plain_rate, 1), "tuning": "seed_kernel 0 (thread per read)",
                               "timing": "device, inputs resident"}
-    forms["batched"] = {"reads_per_s": round(batched_rate, 1), "tuning": dict(zip(
-        ["seed_kernel", "stage1_endpoints", "stage2_blocks_per_sm", "reg_level", "stage1_max_rows",
-         "stage2_first_wave"], best_tuning)), "timing": "device, inputs resident", "equals_plain": same}
+    from mojoalign_b200.autotune import FIELDS as TFIELDS
+
+    forms["batched"] = {"reads_per_s": round(batched_rate, 1), "tuning": dict(zip(TFIELDS, best_tuning)),
+                        "timing": "device, inputs resident", "equals_plain": same}
 
     # the reference's loop: 16384-read synchronous batches of the same kernel
     ctx.set_tuning(*plain_tuning)

@@ -246,8 +246,15 @@ int ma_last_launch_count(const ma_ctx* ctx);
  *                         1: two stages (default): one thread per read over
  *                         the first stage1_endpoints endpoints, then one
  *                         warp per remaining read in a persistent kernel
- *                         fed by a work queue.
- *   stage1_endpoints      endpoints stage 1 covers (default 1).
+ *                         fed by a work queue;
+ *                         2: wavefront: rounds of batch-wide passes (one
+ *                         thread per read and endpoint, then one per
+ *                         candidate locus and shift), stage1_endpoints
+ *                         endpoints in the first round and wave_endpoints in
+ *                         each later one; reads left over go to the stage-2
+ *                         warps.
+ *   stage1_endpoints      endpoints stage 1 (or the first round) covers
+ *                         (default 1).
  *   stage2_blocks_per_sm  persistent blocks per SM for stage 2 (0 = the
  *                         occupancy maximum).
  *   reg_level             register budget of the seed kernels: 0 = the
@@ -259,6 +266,15 @@ int ma_last_launch_count(const ma_ctx* ctx);
  *   stage2_first_wave     right endpoints stage 2 searches in its first
  *                         group for a read (1..32, default 32); later groups
  *                         take 32.
+ *   wave_endpoints        right endpoints per read in each wavefront round
+ *                         after the first (1..256, default 32).
+ *   wave_loci_per_read    wavefront locus list capacity per read of the
+ *                         batch (1..64, default 4; at least 1024 entries);
+ *                         reads whose loci do not fit a round are finished
+ *                         by the stage-2 warps.
+ *   wave_max_rounds       wavefront rounds before the reads still active
+ *                         go to the stage-2 warps (0 = as many as the
+ *                         longest read needs, default).
  */
 typedef struct ma_tuning {
     int32_t seed_kernel;
@@ -267,6 +283,9 @@ typedef struct ma_tuning {
     int32_t reg_level;
     int32_t stage1_max_rows;
     int32_t stage2_first_wave;
+    int32_t wave_endpoints;
+    int32_t wave_loci_per_read;
+    int32_t wave_max_rounds;
 } ma_tuning;
 int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t);
 int ma_ctx_get_tuning(const ma_ctx* ctx, ma_tuning* t);

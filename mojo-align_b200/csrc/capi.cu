@@ -19,6 +19,10 @@ int launch_seed_extend(const DevIndex& ix, const DevReads& R, const DevParams& P
                        unsigned long long* d_tally, int level, cudaStream_t st);
 double run_gather_bench(uint64_t buffer_bytes, int line_bytes, uint64_t n_loads, int sm_count, cudaStream_t st);
 size_t two_stage_scratch_bytes(int64_t n_seq);
+size_t wavefront_scratch_bytes(int64_t n_seq, int loci_per_read);
+int launch_seed_wavefront(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int max_len,
+                          const ma_tuning& t, int stage2_blocks, void* scratch, int sm_count, int* d_err,
+                          unsigned long long* d_tally, cudaStream_t st);
 int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
                           int stage1_endpoints, int stage1_max_rows, int stage2_blocks, int level,
                           int first_wave, void* scratch, unsigned long long* d_tally, cudaEvent_t mid,
@@ -81,7 +85,7 @@ struct ma_ctx {
     struct Slot {
         DevBuf bases, lens, out[12];
     } slot[2];
-    ma_tuning tuning{1, 1, 0, 1, 2, 32};
+    ma_tuning tuning{1, 1, 0, 1, 2, 32, 32, 4, 0};
     int sm_count = 0;
     DevBuf seed_scratch;
     DevBuf bases, lens, packed, err_flag;
@@ -193,6 +197,13 @@ void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const
     const int level = ctx->tuning.reg_level;
     if (ctx->tuning.seed_kernel == 0) {
         launches += launch_seed_extend(idx->dix, R, P, out, d_tally, level, st);
+    } else if (ctx->tuning.seed_kernel == 2) {
+        ctx->seed_scratch.ensure(wavefront_scratch_bytes(n_seq, ctx->tuning.wave_loci_per_read));
+        const int bps = ctx->tuning.stage2_blocks_per_sm > 0 ? ctx->tuning.stage2_blocks_per_sm
+                                                             : stage2_blocks_per_sm(level, d_tally != nullptr);
+        launches += launch_seed_wavefront(idx->dix, R, P, out, static_cast<int>(max_len), ctx->tuning,
+                                          bps * ctx->sm_count, ctx->seed_scratch.p, ctx->sm_count,
+                                          ctx->err_flag.as<int>(), d_tally, st);
     } else {
         ctx->seed_scratch.ensure(two_stage_scratch_bytes(n_seq));
         const int bps = ctx->tuning.stage2_blocks_per_sm > 0 ? ctx->tuning.stage2_blocks_per_sm
@@ -561,13 +572,17 @@ int ma_ctx_set_profiling(ma_ctx* ctx, int flags) {
 int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t) {
     if (!ctx || !t) return MA_ERR_ARG;
     return guarded(ctx, [&] {
-        if (t->seed_kernel < 0 || t->seed_kernel > 1) fail(MA_ERR_ARG, "seed_kernel must be 0 or 1");
+        if (t->seed_kernel < 0 || t->seed_kernel > 2) fail(MA_ERR_ARG, "seed_kernel must be 0, 1 or 2");
         if (t->stage1_endpoints < 1) fail(MA_ERR_ARG, "stage1_endpoints must be >= 1");
         if (t->stage2_blocks_per_sm < 0 || t->stage2_blocks_per_sm > 64) fail(MA_ERR_ARG, "bad stage2_blocks_per_sm");
         if (t->reg_level < 0 || t->reg_level > 2) fail(MA_ERR_ARG, "reg_level must be 0, 1 or 2");
         if (t->stage1_max_rows < 1 || t->stage1_max_rows > 16) fail(MA_ERR_ARG, "stage1_max_rows must be in 1..16");
         if (t->stage2_first_wave < 1 || t->stage2_first_wave > 32)
             fail(MA_ERR_ARG, "stage2_first_wave must be in 1..32");
+        if (t->wave_endpoints < 1 || t->wave_endpoints > 256) fail(MA_ERR_ARG, "wave_endpoints must be in 1..256");
+        if (t->wave_loci_per_read < 1 || t->wave_loci_per_read > 64)
+            fail(MA_ERR_ARG, "wave_loci_per_read must be in 1..64");
+        if (t->wave_max_rounds < 0) fail(MA_ERR_ARG, "wave_max_rounds must be >= 0");
         ctx->tuning = *t;
     });
 }

@@ -40,6 +40,10 @@ int launch_pack_parts(const uint8_t* d_bases, const uint32_t* d_lens, const Pack
 int launch_seed_extend(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
                        unsigned long long* d_tally, int level, cudaStream_t st);
 size_t two_stage_scratch_bytes(int64_t n_seq);
+size_t wavefront_scratch_bytes(int64_t n_seq, int loci_per_read);
+int launch_seed_wavefront(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int max_len,
+                          const ma_tuning& t, int stage2_blocks, void* scratch, int sm_count, int* d_err,
+                          unsigned long long* d_tally, cudaStream_t st);
 int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
                           int stage1_endpoints, int stage1_max_rows, int stage2_blocks, int level,
                           int first_wave, void* scratch, unsigned long long* d_tally, cudaEvent_t mid,
@@ -110,7 +114,9 @@ uint64_t rnd(uint64_t n) { return OffsetArena::round_up(n); }
 
 // Lays out a group of n1 pairs with `stage_bytes` of staged rows over
 // `n_parts` parts.
-GroupLayout layout_for(uint32_t n1, bool paired, int words, uint64_t stage_bytes, size_t n_parts, bool two_stage) {
+GroupLayout layout_for(uint32_t n1, bool paired, int words, uint64_t stage_bytes, size_t n_parts,
+                       const ma_tuning& t) {
+    const int seed_kernel = t.seed_kernel;
     const uint64_t n_seq = paired ? 2ull * n1 : n1;
     GroupLayout L;
     uint64_t o = 0;
@@ -129,7 +135,8 @@ GroupLayout layout_for(uint32_t n1, bool paired, int words, uint64_t stage_bytes
     L.err = o;
     o += OffsetArena::kAlign;
     L.scratch = o;
-    if (two_stage) o += rnd(two_stage_scratch_bytes(static_cast<int64_t>(n_seq)));
+    if (seed_kernel == 1) o += rnd(two_stage_scratch_bytes(static_cast<int64_t>(n_seq)));
+    if (seed_kernel == 2) o += rnd(wavefront_scratch_bytes(static_cast<int64_t>(n_seq), t.wave_loci_per_read));
     L.total = o;
     return L;
 }
@@ -147,7 +154,7 @@ struct HostSlot {
 struct ma_server {
     bool test_mode = false;
     int device = 0, sm_count = 0;
-    ma_tuning tuning{1, 1, 0, 1, 2, 32};
+    ma_tuning tuning{1, 1, 0, 1, 2, 32, 32, 4, 0};
     const DevIndex* dix = nullptr;
     ma_serve_options opt{};
     char* base = nullptr;  // reserved device range (host memory in test mode)
@@ -172,7 +179,7 @@ struct ma_server {
     std::vector<double> lat_ms;
     std::thread issuer, completer;
 
-    bool two_stage() const { return tuning.seed_kernel == 1; }
+    int seed_kernel() const { return tuning.seed_kernel; }
 };
 
 namespace {
@@ -207,7 +214,7 @@ std::unique_ptr<Group> plan_group(ma_server* s, uint32_t cap) {
         if (g->n1 == cap) break;
     }
     g->words = words;
-    g->L = layout_for(g->n1, g->paired, words, stage, g->parts.size(), s->two_stage());
+    g->L = layout_for(g->n1, g->paired, words, stage, g->parts.size(), s->tuning);
     return g;
 }
 
@@ -340,10 +347,13 @@ void issue_group(ma_server* s, Group& g) {
              reinterpret_cast<uint32_t*>(dev + g.L.out[6]), nullptr, nullptr, nullptr, nullptr, nullptr};
     const DevParams P = dev_params(g.p);
     const ma_tuning& t = s->tuning;
-    if (s->two_stage()) {
-        const int bps = t.stage2_blocks_per_sm > 0 ? t.stage2_blocks_per_sm : stage2_blocks_per_sm(t.reg_level, false);
+    const int bps = t.stage2_blocks_per_sm > 0 ? t.stage2_blocks_per_sm : stage2_blocks_per_sm(t.reg_level, false);
+    if (s->seed_kernel() == 1) {
         launch_seed_two_stage(*s->dix, R, P, o, t.stage1_endpoints, t.stage1_max_rows, bps * s->sm_count, t.reg_level,
                               t.stage2_first_wave, dev + g.L.scratch, nullptr, nullptr, st);
+    } else if (s->seed_kernel() == 2) {
+        launch_seed_wavefront(*s->dix, R, P, o, 32 * g.words, t, bps * s->sm_count, dev + g.L.scratch, s->sm_count,
+                              d_err, nullptr, st);
     } else {
         launch_seed_extend(*s->dix, R, P, o, nullptr, t.reg_level, st);
     }
@@ -663,7 +673,7 @@ int ma_serve_submit(ma_server* s, const uint8_t* bases, const uint32_t* lens, ui
         for (uint64_t i = 0; i < n_seq; ++i)
             if (lens[i] > max_len) fail(MA_ERR_ARG, "read " + std::to_string(i) + " longer than max_len");
         const GroupLayout one = layout_for(1, paired != 0, words_for(max_len), rnd(static_cast<uint64_t>(mates) * max_len),
-                                           1, s->two_stage());
+                                           1, s->tuning);
         if (one.total > s->arena.capacity())
             fail(MA_ERR_NOMEM, "one pair needs " + std::to_string(one.total) + " bytes, over the serving budget");
         auto rq = std::make_shared<Request>();

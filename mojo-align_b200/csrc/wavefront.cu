@@ -1,0 +1,482 @@
+// wavefront.cu - seed_kernel 2: the seed/extend search as rounds of
+// data-parallel passes over the whole batch (fm_seed_extend_kernel,
+// fq2bam-meth/src/linear_gpu_fm.mojo:1156-1837, with the candidate order
+// and exactness argument of seed_core.cuh).
+//
+// Round k covers right endpoints [resume, resume + width) of every read
+// still active (width w0 in round 0, w after it):
+//   search   one thread per (read, endpoint): duplicate prediction, backward
+//            search, SA rows -> candidate loci appended to a batch-wide
+//            locus list (one atomic per warp);
+//   eval     one thread per (locus, shift): the shift's candidates (full
+//            compare, soft-clip retry, deletion probe) and an atomicMin of
+//            the best key per read, packed with the locus' list index;
+//   finalize one thread per active read: the new best (its fields are
+//            recomputed from the winning locus and shift), the nm == 0 stop,
+//            the exact nm == 1 early stop, the next round's active list.
+// Every candidate of a round comes after the best of the rounds before it
+// in the reference's order, so pruning against that best and taking the
+// minimum key over the round gives the reference's hit.  A read whose loci
+// do not fit the list is left out of its round (its memo and best roll
+// back) and finished by the stage-2 warp kernel from that round's first
+// endpoint, as are reads still active after the last round.
+#include <cuda_runtime.h>
+
+#include "ma_device.cuh"
+#include "seed_core.cuh"
+
+namespace ma {
+
+int launch_stage2_pending(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
+                          uint64_t* key, uint64_t* memo, uint8_t* memo_n, uint16_t* resume, uint32_t* pending,
+                          uint32_t* counters, int blocks, int level, int first_wave, unsigned long long* tally,
+                          cudaStream_t st);
+
+namespace {
+
+// counters[]
+constexpr int C_ACTIVE = 0;    // reads active in the current round
+constexpr int C_NEXT = 1;      // reads appended to the next round's list
+constexpr int C_LOCI = 2;      // loci appended in the current round
+constexpr int C_ROUNDS = 3;    // read-rounds processed (tally)
+constexpr int C_HANDOFF = 8;   // [8] reads for stage 2, [9] its work cursor
+constexpr int N_COUNTERS = 16;
+
+constexpr uint64_t LIDX_MASK = (1ull << 27) - 1;  // round keys: nm << 54 | ordinal << 27 | locus index
+constexpr uint64_t MAX_LOCI = LIDX_MASK;          // list capacity limit (indices fit 27 bits)
+
+// One candidate locus of a round.
+struct WLocus {
+    int64_t b0;
+    uint64_t uk, ul;
+    uint32_t read, ord_row;
+    int32_t us, e, crid, rev;
+};
+
+struct Wave {
+    uint32_t* counters;
+    uint64_t* best_key;   // nm << 27 | ordinal of the best so far, ~0 = none
+    uint64_t* round_key;  // this round's minimum, packed with the locus index
+    uint64_t* memo;       // [n][MEMO1] loci evaluated (b0 * 2 + strand)
+    uint8_t* memo_n;      // memo entries valid at the start of the round
+    uint32_t* memo_next;  // memo entries claimed during the round
+    uint16_t* resume;     // first right endpoint of the read's next round
+    uint8_t* overflow;    // the read's loci did not fit the list this round
+    int64_t* best_tag;    // locus of the best hit, -1 = none
+    uint32_t* active[2];  // ping-pong lists of active reads
+    uint32_t* pending;    // reads handed to stage 2
+    WLocus* loci;
+    uint64_t locus_cap;
+};
+
+size_t align256(size_t b) { return (b + 255) & ~static_cast<size_t>(255); }
+
+// Carves the scratch; returns the bytes used (layout only when p != null).
+size_t wave_layout(char* p, int64_t n_seq, uint64_t locus_cap, Wave* w) {
+    const size_t n = static_cast<size_t>(n_seq);
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        char* q = p ? p + o : nullptr;
+        o += align256(bytes);
+        return q;
+    };
+    Wave v{};
+    v.counters = reinterpret_cast<uint32_t*>(take(N_COUNTERS * 4));
+    v.best_key = reinterpret_cast<uint64_t*>(take(n * 8));
+    v.round_key = reinterpret_cast<uint64_t*>(take(n * 8));
+    v.memo = reinterpret_cast<uint64_t*>(take(n * 8 * MEMO1));
+    v.memo_n = reinterpret_cast<uint8_t*>(take(n));
+    v.memo_next = reinterpret_cast<uint32_t*>(take(n * 4));
+    v.resume = reinterpret_cast<uint16_t*>(take(n * 2));
+    v.overflow = reinterpret_cast<uint8_t*>(take(n));
+    v.best_tag = reinterpret_cast<int64_t*>(take(n * 8));
+    v.active[0] = reinterpret_cast<uint32_t*>(take(n * 4));
+    v.active[1] = reinterpret_cast<uint32_t*>(take(n * 4));
+    v.pending = reinterpret_cast<uint32_t*>(take(n * 4));
+    v.loci = reinterpret_cast<WLocus*>(take(locus_cap * sizeof(WLocus)));
+    v.locus_cap = locus_cap;
+    if (w) *w = v;
+    return o;
+}
+
+uint64_t locus_capacity(int64_t n_seq, int per_read) {
+    uint64_t c = static_cast<uint64_t>(per_read) * static_cast<uint64_t>(n_seq);
+    if (c < 1024) c = 1024;
+    return c < MAX_LOCI ? c : MAX_LOCI;
+}
+
+__global__ void __launch_bounds__(256) wf_init_kernel(Wave w, DevOut out, const uint32_t* __restrict__ lens,
+                                                      int64_t n_seq) {
+    const int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (r == 0) {
+        for (int i = 0; i < N_COUNTERS; ++i) w.counters[i] = 0;
+        w.counters[C_ACTIVE] = static_cast<uint32_t>(n_seq);
+    }
+    if (r >= n_seq) return;
+    w.best_key[r] = ~0ull;
+    w.round_key[r] = ~0ull;
+    w.memo_n[r] = 0;
+    w.memo_next[r] = 0;
+    w.resume[r] = 0;
+    w.overflow[r] = 0;
+    w.best_tag[r] = -1;
+    w.active[0][r] = static_cast<uint32_t>(r);
+    Best none;
+    none.key = ~0ull;
+    none.crid = -1;
+    none.uk = none.ul = 0;
+    none.us = none.e = -1;
+    write_hit(out, r, none, static_cast<int>(lens[r]));
+}
+
+// Moves the next round's active count into place (one thread).
+__global__ void wf_round_begin_kernel(Wave w) {
+    w.counters[C_ACTIVE] = w.counters[C_NEXT];
+    w.counters[C_NEXT] = 0;
+    w.counters[C_LOCI] = 0;
+}
+
+// Whether an SA row of a found seed gives a locus not evaluated before.
+__device__ __forceinline__ bool fresh_locus(const DevIndex& ix, const Wave& w, int64_t r, int n_memo, uint64_t sa_pos,
+                                            int us, int e, int qlen, int64_t& b0, int& rev) {
+    if (!locus_of_row(ix, sa_pos, us, e, qlen, b0, rev)) return false;
+    const uint64_t tag = static_cast<uint64_t>(b0 * 2 + rev);
+    for (int m = 0; m < n_memo; ++m)
+        if (w.memo[r * MEMO1 + m] == tag) return false;
+    return true;
+}
+
+// Search: one thread per (active read, endpoint of the round).  The loop
+// is warp-uniform (whole warps step together) for the warp-wide append.
+template <bool S>
+__global__ void __launch_bounds__(256) wf_search_kernel(DevIndex ix, DevReads R, DevParams P, Wave w,
+                                                        const uint32_t* __restrict__ act, int width,
+                                                        unsigned long long* __restrict__ tally_out) {
+    Tally t{};
+    const uint64_t n_items = static_cast<uint64_t>(w.counters[C_ACTIVE]) * static_cast<uint64_t>(width);
+    const int lane = threadIdx.x & 31;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const bool can_predict = ix.summary && ix.kmer3_k > 0 && ix.kmer3_k <= P.seed_len;
+    for (uint64_t base = (blockIdx.x * static_cast<uint64_t>(blockDim.x)) + (threadIdx.x & ~31u); base < n_items;
+         base += stride) {
+        const uint64_t item = base + lane;
+        Seed sd{0, 0, -1, false};
+        int64_t r = 0;
+        int ei = 0, e = 0, qlen = 0, n_memo = 0;
+        ReadView rd{};
+        if (item < n_items) {
+            const uint64_t a = item < (1ull << 32) ? static_cast<uint32_t>(item) / static_cast<uint32_t>(width)
+                                                   : item / static_cast<uint64_t>(width);
+            const int j = static_cast<int>(item - a * static_cast<uint64_t>(width));
+            r = act[a];
+            rd = read_view(R, r);
+            qlen = rd.qlen;
+            ei = static_cast<int>(w.resume[r]) + j;
+            if (ei < endpoint_count(P, qlen)) {
+                e = P.seed_len - 1 + ei * P.seed_stride;
+                n_memo = w.memo_n[r];
+                const bool dup = can_predict && predicted_duplicate<S>(ix, rd, e, P, w.best_tag[r],
+                                                                       w.memo + r * MEMO1, n_memo < 4 ? n_memo : 4, t);
+                if constexpr (S) t.skipped += dup;
+                if (!dup) sd = search_endpoint<S>(ix, rd, e, P, t);
+            }
+        }
+        // count pass: loci not in the memo
+        uint32_t n_keep = 0;
+        if (sd.found) {
+            for (uint64_t hi = sd.k; hi <= sd.l; ++hi) {
+                const uint64_t sa_pos = __ldg(ix.sa + hi);
+                if constexpr (S) t.sa_loads++;
+                int64_t b0;
+                int rev;
+                n_keep += fresh_locus(ix, w, r, n_memo, sa_pos, sd.s, e, qlen, b0, rev);
+            }
+        }
+        uint32_t incl = n_keep;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const uint32_t warp_total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        uint32_t wbase = 0;
+        if (lane == 31 && warp_total) wbase = atomicAdd(&w.counters[C_LOCI], warp_total);
+        wbase = __shfl_sync(0xFFFFFFFFu, wbase, 31);
+        if (n_keep) {
+            uint64_t slot = static_cast<uint64_t>(wbase) + (incl - n_keep);
+            for (uint64_t hi = sd.k; hi <= sd.l; ++hi) {
+                int64_t b0;
+                int rev;
+                if (!fresh_locus(ix, w, r, n_memo, __ldg(ix.sa + hi), sd.s, e, qlen, b0, rev)) continue;
+                if (slot >= w.locus_cap) {
+                    w.overflow[r] = 1;
+                    break;
+                }
+                WLocus L;
+                L.b0 = b0;
+                L.uk = sd.k;
+                L.ul = sd.l;
+                L.read = static_cast<uint32_t>(r);
+                L.ord_row = (static_cast<uint32_t>(ei) * 16 + static_cast<uint32_t>(hi - sd.k)) * ADJ_SPAN;
+                L.us = sd.s;
+                L.e = e;
+                L.crid = static_cast<int32_t>(contig_hint(ix, b0).crid);
+                L.rev = rev;
+                w.loci[slot++] = L;
+                if constexpr (S) tally_locus(t, b0, clamps_for(P, qlen).adj_cap, qlen);
+                const uint32_t m = atomicAdd(&w.memo_next[r], 1u);
+                if (m < static_cast<uint32_t>(MEMO1)) w.memo[r * MEMO1 + m] = static_cast<uint64_t>(b0 * 2 + rev);
+            }
+        }
+    }
+    flush_tally<S>(t, tally_out);
+}
+
+// Eval: one thread per locus filters its shifts (live_shifts); the shifts
+// left in the warp are spread over its lanes.  Candidates are pruned
+// against the read's best from earlier rounds; the round's minimum key per
+// read is an atomicMin of (nm << 54 | ordinal << 27 | locus index).  The
+// loop over loci is warp-uniform for the redistribution.
+constexpr int EVAL_THREADS = 256;
+
+template <bool S>
+__global__ void __launch_bounds__(EVAL_THREADS) wf_eval_kernel(DevIndex ix, DevReads R, DevParams P, Wave w,
+                                                               unsigned long long* __restrict__ tally_out) {
+    __shared__ WLocus s_loci[EVAL_THREADS];
+    constexpr unsigned FULL = 0xFFFFFFFFu;
+    Tally t{};
+    uint64_t n_loci = w.counters[C_LOCI];
+    if (n_loci > w.locus_cap) n_loci = w.locus_cap;
+    const int adj_cap = clamps_for(P, 1 << 20).adj_cap;  // read-independent
+    const int lane = threadIdx.x & 31;
+    WLocus* wl = s_loci + (threadIdx.x & ~31u);
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n_loci; base += stride) {
+        const uint32_t li = base + lane;
+        uint32_t live = 0;
+        if (li < n_loci) {
+            const WLocus L = w.loci[li];
+            wl[lane] = L;
+            const int64_t r = L.read;
+            if (!w.overflow[r]) {
+                const ReadView rd = read_view(R, r);
+                const Clamps cl = clamps_for(P, rd.qlen);
+                const uint64_t bn = w.best_key[r] >> ORD_SHIFT;
+                const int prune = bn < (1u << 20) ? static_cast<int>(bn) : (1 << 20);
+                live = live_shifts<S>(ix, rd, L.b0, L.rev, adj_cap, cl.budget, cl.clip_cap, prune, t);
+            }
+        }
+        __syncwarp();
+        const int n_live = __popc(live);
+        int incl = n_live;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(FULL, incl, 31);
+        for (int c = 0; c < total; c += 32) {
+            const int idx = c + lane;
+            int owner = 0;  // first lane whose inclusive count exceeds idx
+            for (int step = 16; step >= 1; step >>= 1) {
+                const int v = __shfl_sync(FULL, incl, owner + step - 1);
+                if (v <= idx) owner += step;
+            }
+            const int own = owner < 32 ? owner : 31;
+            const uint32_t o_live = __shfl_sync(FULL, live, own);
+            const int o_first = __shfl_sync(FULL, incl - n_live, own);
+            if (idx < total) {
+                const int adj = static_cast<int>(__fns(o_live, 0, idx - o_first + 1)) - adj_cap;
+                const WLocus L = wl[own];
+                const int64_t r = L.read;
+                const ReadView rd = read_view(R, r);
+                const Clamps cl = clamps_for(P, rd.qlen);
+                const uint64_t bn = w.best_key[r] >> ORD_SHIFT;
+                const int prune = bn < (1u << 20) ? static_cast<int>(bn) : (1 << 20);
+                ContigHint hint{L.crid, 0, 0};
+                if (L.crid >= 0) {
+                    hint.coff = static_cast<int64_t>(__ldg(ix.coff + L.crid));
+                    hint.clen = static_cast<int64_t>(__ldg(ix.clen + L.crid));
+                }
+                Best lb;
+                lb.key = ~0ull;
+                lb.crid = -1;
+                eval_adj<S>(ix, rd, L.b0, L.rev, adj, cl.budget, cl.clip_cap, L.ord_row, lb, L.uk, L.ul, L.us, L.e,
+                            prune, hint, t);
+                if (lb.key != ~0ull) {
+                    const uint64_t nm = lb.key >> ORD_SHIFT;
+                    const uint64_t ord = lb.key & ((1ull << ORD_SHIFT) - 1);
+                    atomicMin(reinterpret_cast<unsigned long long*>(w.round_key + r),
+                              static_cast<unsigned long long>((nm << 54) | (ord << 27) | (base + own)));
+                }
+            }
+        }
+        __syncwarp();
+    }
+    flush_tally<S>(t, tally_out);
+}
+
+// Finalize: one thread per active read (warp-uniform loop for the list
+// appends).  last_round: reads with endpoints left go to stage 2.
+template <bool S>
+__global__ void __launch_bounds__(256) wf_finalize_kernel(DevIndex ix, DevReads R, DevParams P, DevOut out, Wave w,
+                                                          const uint32_t* __restrict__ act,
+                                                          uint32_t* __restrict__ next, int width, int last_round,
+                                                          int* __restrict__ err,
+                                                          unsigned long long* __restrict__ tally_out) {
+    Tally t{};
+    const uint32_t n_act = w.counters[C_ACTIVE];
+    const int lane = threadIdx.x & 31;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    if constexpr (S) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&w.counters[C_ROUNDS], n_act);
+    }
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n_act; base += stride) {
+        const uint32_t a = base + lane;
+        bool to_next = false, to_stage2 = false;
+        int64_t r = 0;
+        if (a < n_act) {
+            r = act[a];
+            const ReadView rd = read_view(R, r);
+            const int qlen = rd.qlen;
+            const Clamps cl = clamps_for(P, qlen);
+            const int n_end = endpoint_count(P, qlen);
+            if (w.overflow[r]) {
+                // left out of this round: roll back and let stage 2 redo it
+                w.overflow[r] = 0;
+                w.memo_next[r] = w.memo_n[r];
+                to_stage2 = true;
+            } else {
+                const uint32_t mn = w.memo_next[r];
+                w.memo_n[r] = static_cast<uint8_t>(mn < static_cast<uint32_t>(MEMO1) ? mn : MEMO1);
+                const uint64_t rk = w.round_key[r];
+                const uint64_t old = w.best_key[r];
+                bool stop = false;
+                if (rk != ~0ull && (rk >> 27) < old) {
+                    // the new best: recompute its fields from the winning locus and shift
+                    const WLocus L = w.loci[rk & LIDX_MASK];
+                    const uint32_t ord = static_cast<uint32_t>((rk >> 27) & ((1ull << ORD_SHIFT) - 1));
+                    const int adj = static_cast<int>(ord / KIND_SPAN) - static_cast<int>(L.ord_row) - 12;
+                    const uint64_t bn = old >> ORD_SHIFT;
+                    const int prune = bn < (1u << 20) ? static_cast<int>(bn) : (1 << 20);
+                    ContigHint hint{L.crid, 0, 0};
+                    if (L.crid >= 0) {
+                        hint.coff = static_cast<int64_t>(__ldg(ix.coff + L.crid));
+                        hint.clen = static_cast<int64_t>(__ldg(ix.clen + L.crid));
+                    }
+                    Best lb;
+                    lb.key = ~0ull;
+                    lb.crid = -1;
+                    eval_adj<S>(ix, rd, L.b0, L.rev, adj, cl.budget, cl.clip_cap, L.ord_row, lb, L.uk, L.ul, L.us,
+                                L.e, prune, hint, t);
+                    if (lb.key != (rk >> 27)) {
+                        atomicExch(err, 3);  // the recomputed candidate must be the round's minimum
+                    } else {
+                        write_hit(out, r, lb, qlen);
+                        w.best_key[r] = lb.key;
+                        w.best_tag[r] = L.b0 * 2 + L.rev;
+                        const uint64_t nm = lb.key >> ORD_SHIFT;
+                        if (nm == 0) {
+                            stop = true;
+                        } else if (nm <= 2 && full_compare_key(lb.key)) {
+                            const int64_t bstart = static_cast<int64_t>(__ldg(ix.coff + lb.crid)) + lb.pos - lb.sl;
+                            stop = better_hit_impossible<S>(ix, rd, bstart, (lb.flag & 16) ? 1 : 0, cl.clip_cap,
+                                                            static_cast<int>(nm), t);
+                        }
+                    }
+                }
+                w.round_key[r] = ~0ull;
+                const int nxt = static_cast<int>(w.resume[r]) + width;
+                if (!stop && nxt < n_end) {
+                    w.resume[r] = static_cast<uint16_t>(nxt);
+                    if (last_round) to_stage2 = true;
+                    else to_next = true;
+                }
+            }
+        }
+        const unsigned bn = __ballot_sync(0xFFFFFFFFu, to_next);
+        if (bn) {
+            uint32_t b = 0;
+            if (lane == 0) b = atomicAdd(&w.counters[C_NEXT], static_cast<uint32_t>(__popc(bn)));
+            b = __shfl_sync(0xFFFFFFFFu, b, 0);
+            if (to_next) next[b + __popc(bn & ((1u << lane) - 1))] = static_cast<uint32_t>(r);
+        }
+        const unsigned bs = __ballot_sync(0xFFFFFFFFu, to_stage2);
+        if (bs) {
+            uint32_t b = 0;
+            if (lane == 0) b = atomicAdd(&w.counters[C_HANDOFF], static_cast<uint32_t>(__popc(bs)));
+            b = __shfl_sync(0xFFFFFFFFu, b, 0);
+            if (to_stage2) w.pending[b + __popc(bs & ((1u << lane) - 1))] = static_cast<uint32_t>(r);
+        }
+    }
+    flush_tally<S>(t, tally_out);
+}
+
+int endpoint_count_host(const DevParams& P, int qlen) {
+    return qlen >= P.seed_len ? (qlen - P.seed_len) / P.seed_stride + 1 : 0;
+}
+
+template <typename K>
+int grid_blocks(K kernel, int sm_count) {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, 256, 0);
+    if (nb < 1) nb = 1;
+    return nb * sm_count;
+}
+
+template <bool S>
+int launch_rounds(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, const Wave& w,
+                  int max_len, int w0, int wn, int max_rounds, int sm_count, int* d_err, unsigned long long* tally,
+                  cudaStream_t st) {
+    const int n_end_max = endpoint_count_host(P, max_len);
+    int rounds = 1;
+    if (n_end_max > w0) rounds += (n_end_max - w0 + wn - 1) / wn;
+    if (max_rounds > 0 && rounds > max_rounds) rounds = max_rounds;
+    static const int g_search = grid_blocks(wf_search_kernel<S>, sm_count);
+    static const int g_eval = grid_blocks(wf_eval_kernel<S>, sm_count);  // EVAL_THREADS = 256
+    static const int g_fin = grid_blocks(wf_finalize_kernel<S>, sm_count);
+    const unsigned init_blocks = static_cast<unsigned>((R.n_seq + 255) / 256);
+    wf_init_kernel<<<init_blocks ? init_blocks : 1, 256, 0, st>>>(w, out, R.lens, R.n_seq);
+    int launches = 1;
+    for (int k = 0; k < rounds; ++k) {
+        const int width = k == 0 ? w0 : wn;
+        const uint32_t* act = w.active[k & 1];
+        uint32_t* nxt = w.active[(k + 1) & 1];
+        if (k > 0) {
+            wf_round_begin_kernel<<<1, 1, 0, st>>>(w);
+            ++launches;
+        }
+        wf_search_kernel<S><<<g_search, 256, 0, st>>>(ix, R, P, w, act, width, tally);
+        wf_eval_kernel<S><<<g_eval, 256, 0, st>>>(ix, R, P, w, tally);
+        wf_finalize_kernel<S><<<g_fin, 256, 0, st>>>(ix, R, P, out, w, act, nxt, width, k == rounds - 1, d_err,
+                                                     tally);
+        launches += 3;
+    }
+    return launches;
+}
+
+}  // namespace
+
+size_t wavefront_scratch_bytes(int64_t n_seq, int loci_per_read) {
+    return wave_layout(nullptr, n_seq, locus_capacity(n_seq, loci_per_read), nullptr);
+}
+
+// The wavefront form; `scratch` holds wavefront_scratch_bytes(n_seq,
+// t.wave_loci_per_read) bytes, d_err is the batch's error word.  Returns
+// the number of kernel launches.
+int launch_seed_wavefront(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int max_len,
+                          const ma_tuning& t, int stage2_blocks, void* scratch, int sm_count, int* d_err,
+                          unsigned long long* d_tally, cudaStream_t st) {
+    Wave w;
+    wave_layout(static_cast<char*>(scratch), R.n_seq, locus_capacity(R.n_seq, t.wave_loci_per_read), &w);
+    const int w0 = t.stage1_endpoints > 0 ? t.stage1_endpoints : 1;
+    const int wn = t.wave_endpoints > 0 ? t.wave_endpoints : 1;
+    int launches = d_tally ? launch_rounds<true>(ix, R, P, out, w, max_len, w0, wn, t.wave_max_rounds, sm_count,
+                                                 d_err, d_tally, st)
+                           : launch_rounds<false>(ix, R, P, out, w, max_len, w0, wn, t.wave_max_rounds, sm_count,
+                                                  d_err, nullptr, st);
+    // reads that overflowed the locus list or outlived the rounds
+    launches += launch_stage2_pending(ix, R, P, out, w.best_key, w.memo, w.memo_n, w.resume, w.pending,
+                                      w.counters + C_HANDOFF, stage2_blocks, t.reg_level, 32, d_tally, st);
+    return launches;
+}
+
+}  // namespace ma

@@ -1,7 +1,8 @@
 """Autotuner for the result-neutral execution choices of the seed kernels.
 
-Sweeps the kernel form (one thread per read, or two stages), the number of
-right endpoints stage 1 covers, the seed kernels' register budget and the
+Sweeps the kernel form (one thread per read, two stages, or wavefront
+rounds), the number of right endpoints stage 1 (or the first round)
+covers, the round width, the seed kernels' register budget and the
 persistent stage-2 grid, on a sample batch.  Every candidate must produce
 identical outputs (checked here); the fastest by device time wins.
 
@@ -18,19 +19,25 @@ from .mapper import GpuContext, GpuIndex, MapResult, map_batch
 from .params import FmParams
 
 DEFAULT_CANDIDATES = [
-    (0, 1, 0, 1, 16, 32),
-    (1, 1, 0, 2, 16, 32),
-    (1, 1, 0, 2, 2, 32),
-    (1, 1, 0, 2, 1, 32),
-    (1, 1, 0, 2, 1, 1),
-    (1, 1, 0, 2, 1, 4),
-    (1, 1, 0, 2, 1, 8),
-    (1, 1, 0, 1, 1, 1),
-    (1, 1, 0, 1, 1, 4),
-    (1, 2, 0, 2, 2, 4),
+    (0, 1, 0, 1, 16, 32, 32),
+    (1, 1, 0, 2, 2, 32, 32),
+    (1, 1, 0, 2, 1, 32, 32),
+    (1, 1, 0, 2, 1, 1, 32),
+    (1, 1, 0, 2, 1, 4, 32),
+    (1, 1, 0, 1, 1, 1, 32),
+    (1, 2, 0, 2, 2, 4, 32),
+    (2, 1, 0, 1, 1, 1, 32),
+    (2, 1, 0, 2, 1, 1, 32),
+    (2, 1, 0, 1, 1, 1, 16),
+    (2, 1, 0, 1, 1, 1, 64),
+    (2, 2, 0, 1, 1, 1, 32),
+    (2, 1, 0, 0, 1, 1, 32),
 ]
 FIELDS = ("seed_kernel", "stage1_endpoints", "stage2_blocks_per_sm", "reg_level", "stage1_max_rows",
-          "stage2_first_wave")
+          "stage2_first_wave", "wave_endpoints", "wave_loci_per_read", "wave_max_rounds")
+
+
+DEFAULTS = (1, 1, 0, 1, 2, 32, 32, 4, 0)
 
 
 @dataclass
@@ -69,5 +76,6 @@ def autotune(ctx: GpuContext, index: GpuIndex, bases: np.ndarray, lens: np.ndarr
         ctx.set_profiling(0)
     best_ms, best = min(timings)
     ctx.set_tuning(*best)
+    best = tuple(best) + tuple(DEFAULTS[len(best):])
     return TuneResult(dict(zip(FIELDS, best)), best_ms,
                       [{"tuning": dict(zip(FIELDS, c)), "seed_ms": round(t, 3)} for t, c in timings])
