@@ -79,9 +79,10 @@ struct ma_ctx {
     bool rescue_ran = false;
     DevBuf tally;
     // two-slot pipeline of ma_map_batch: H2D of chunk k+1 on copy_stream
-    // while chunk k computes on `stream`
-    cudaStream_t copy_stream = nullptr;
+    // and D2H of chunk k-1 on d2h_stream while chunk k computes on `stream`
+    cudaStream_t copy_stream = nullptr, d2h_stream = nullptr;
     cudaEvent_t h2d_done[2] = {nullptr, nullptr}, slot_free[2] = {nullptr, nullptr};
+    cudaEvent_t comp_done[2] = {nullptr, nullptr};
     struct Slot {
         DevBuf bases, lens, out[12];
     } slot[2];
@@ -299,8 +300,10 @@ void ma_ctx_destroy(ma_ctx* ctx) {
     for (int i = 0; i < 2; ++i) {
         if (ctx->h2d_done[i]) cudaEventDestroy(ctx->h2d_done[i]);
         if (ctx->slot_free[i]) cudaEventDestroy(ctx->slot_free[i]);
+        if (ctx->comp_done[i]) cudaEventDestroy(ctx->comp_done[i]);
     }
     if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+    if (ctx->d2h_stream) cudaStreamDestroy(ctx->d2h_stream);
     for (DevBuf* b : {&ctx->bases, &ctx->lens, &ctx->packed, &ctx->err_flag, &ctx->o_rid, &ctx->o_pos, &ctx->o_mapq,
                       &ctx->o_flag, &ctx->o_sl, &ctx->o_sr, &ctx->o_nm, &ctx->d_uk, &ctx->d_ul, &ctx->d_us,
                       &ctx->d_e, &ctx->d_score})
@@ -449,17 +452,20 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
         cudaStream_t st = ctx->stream;
         if (!ctx->copy_stream) {
             ck(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+            ck(cudaStreamCreateWithFlags(&ctx->d2h_stream, cudaStreamNonBlocking), "cudaStreamCreate");
             for (int i = 0; i < 2; ++i) {
                 ck(cudaEventCreateWithFlags(&ctx->h2d_done[i], cudaEventDisableTiming), "cudaEventCreate");
                 ck(cudaEventCreateWithFlags(&ctx->slot_free[i], cudaEventDisableTiming), "cudaEventCreate");
+                ck(cudaEventCreateWithFlags(&ctx->comp_done[i], cudaEventDisableTiming), "cudaEventCreate");
             }
         }
         const bool want_dbg = dbg && (dbg->uk || dbg->ul || dbg->us || dbg->e || dbg->score);
         // Pipeline over chunks of pairs (pairs never split: rescue reads both
         // mates).  Chunk k's R1 rows and R2 rows are copied into one slot as
-        // a batch of its own while chunk k-1 computes; results are copied
-        // back into the caller's arrays at the pairs' positions.
-        const uint32_t chunk = std::max<uint32_t>(131072u, (n1 + 7) / 8);
+        // a batch of its own while chunk k-1 computes, and chunk k-1's results
+        // go back into the caller's arrays (at the pairs' positions) while
+        // chunk k computes: three streams, two slots.
+        const uint32_t chunk = std::max<uint32_t>(131072u, (n1 + 15) / 16);
         const int mates = paired ? 2 : 1;
         void* host_out[12] = {out->rid, out->pos, out->mapq, out->flag, out->sl, out->sr, out->nm,
                               want_dbg ? dbg->uk : nullptr, want_dbg ? dbg->ul : nullptr,
@@ -510,17 +516,21 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
                 if (ctx->tuning.seed_kernel == 1) ck(cudaEventElapsedTime(&ms[3], ctx->ev[1], ctx->ev[4]), "elapsed");
                 for (int i = 0; i < 4; ++i) acc_ms[i] += ms[i];
             }
+            ck(cudaEventRecord(ctx->comp_done[k & 1], st), "cudaEventRecord");
+            ck(cudaStreamWaitEvent(ctx->d2h_stream, ctx->comp_done[k & 1], 0), "cudaStreamWaitEvent");
             for (int f = 0; f < 12; ++f) {
                 if (!host_out[f]) continue;
                 for (int m = 0; m < mates; ++m) {
                     const size_t row0 = static_cast<size_t>(m) * n1 + a;
                     ck(cudaMemcpyAsync(static_cast<char*>(host_out[f]) + row0 * width[f],
                                        sl.out[f].as<char>() + static_cast<size_t>(m) * c * width[f], c * width[f],
-                                       cudaMemcpyDeviceToHost, st), "D2H");
+                                       cudaMemcpyDeviceToHost, ctx->d2h_stream), "D2H");
                 }
             }
-            ck(cudaEventRecord(ctx->slot_free[k & 1], st), "cudaEventRecord");
+            ck(cudaEventRecord(ctx->slot_free[k & 1], ctx->d2h_stream), "cudaEventRecord");
         }
+        // the error word after the last copies back
+        ck(cudaStreamWaitEvent(st, ctx->slot_free[(k - 1) & 1], 0), "cudaStreamWaitEvent");
         check_err_flag(ctx, st);
         if (ctx->profiling & 1)
             for (int i = 0; i < 4; ++i) ctx->kernel_ms[i] = acc_ms[i];

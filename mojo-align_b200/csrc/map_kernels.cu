@@ -64,6 +64,138 @@ __global__ void __launch_bounds__(256) pack_reads_kernel(const uint8_t* __restri
               packed + d * 4 * static_cast<int64_t>(words));
 }
 
+// Four bases at base[x .. x+3] (reversed: base[x+3] first) from 4-byte
+// aligned loads; base must be 4-byte aligned.
+__device__ __forceinline__ uint32_t load4(const uint8_t* base, int x, bool reversed) {
+    const uint32_t* a = reinterpret_cast<const uint32_t*>(base + (x & ~3));
+    const uint32_t o = static_cast<uint32_t>(x & 3) * 0x1111u;
+    return __byte_perm(a[0], a[1], (reversed ? 0x0123u : 0x3210u) + o);
+}
+
+// 2-bit codes (bits 0,2,4,6) and N flags (bits 0,2,4,6) of four ASCII bases
+// after conversion `mode` (linear_fastq.mojo:37-46): A/a 0, C/c 1, G/g 2,
+// T/t 3 (C -> T under C2T, G -> A under G2A), anything else N (code 0).
+// Bits 1-2 of the ASCII letters give the codes, ((b >> 1) ^ (b >> 2)) & 3;
+// a byte is a base exactly when its upper-case form equals the letter of
+// its code (a byte permute of "ACGT" by the codes).
+__device__ __forceinline__ void codes4(uint32_t v, int mode, uint32_t& codes, uint32_t& nflags) {
+    const uint32_t u = v & 0xDFDFDFDFu;
+    uint32_t c = ((v >> 1) ^ (v >> 2)) & 0x03030303u;
+    const uint32_t sel = (c & 0x3u) | ((c >> 4) & 0x30u) | ((c >> 8) & 0x300u) | ((c >> 12) & 0x3000u);
+    const uint32_t x = u ^ __byte_perm(0x54474341u, 0u, sel);
+    const uint32_t nz = (((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x) & 0x80808080u;  // high bit: byte not a base
+    if (mode == MA_BS_C2T) c |= (c & ~(c >> 1) & 0x01010101u) << 1;
+    if (mode == MA_BS_G2A) c &= ~(((c >> 1) & ~c & 0x01010101u) << 1);
+    const uint32_t nb = nz >> 7;
+    c &= ~(nb * 3u);
+    codes = (c & 0x3u) | ((c >> 6) & 0xCu) | ((c >> 12) & 0x30u) | ((c >> 18) & 0xC0u);
+    nflags = (nb & 0x1u) | ((nb >> 6) & 0x4u) | ((nb >> 12) & 0x10u) | ((nb >> 18) & 0x40u);
+}
+
+// Order of the 32 two-bit fields of a word reversed.
+__device__ __forceinline__ uint64_t reverse_fields(uint64_t x) {
+    const uint64_t y = __brevll(x);
+    return ((y >> 1) & kEven) | ((y & kEven) << 1);
+}
+
+// One packed read from a staged row (`row` = its offset in the 4-byte
+// aligned `base`): forward words from the bytes 4 bases at a time, then the
+// reverse-complement words from the forward ones (fields reversed, shifted
+// by 32 * ceil(len / 32) - len bases, complemented).  Reads may touch up to
+// 7 bytes after the row's last base.
+__device__ __forceinline__ void pack_row_staged(const uint8_t* base, int row, int len, int mode, int words,
+                                                uint64_t* __restrict__ out) {
+    const int wr = (len + 31) >> 5;     // words holding bases
+    const int sh = 2 * (32 * wr - len);  // bits the reversed stream is shifted by
+    uint64_t r_prev = 0, rn_prev = 0;    // reversed word j - 1
+    for (int k = wr - 1; k >= 0; --k) {  // j = wr - 1 - k ascending
+        uint64_t f = 0, fn = 0;
+        for (int g = 0; g < 8; ++g) {
+            if (32 * k + 4 * g >= len) break;
+            uint32_t c, n;
+            codes4(load4(base, row + 32 * k + 4 * g, false), mode, c, n);
+            f |= static_cast<uint64_t>(c) << (8 * g);
+            fn |= static_cast<uint64_t>(n) << (8 * g);
+        }
+        const int nv = len - 32 * k;
+        const uint64_t keep = nv >= 32 ? ~0ull : ((1ull << (2 * nv)) - 1);
+        f &= keep;
+        fn &= keep;
+        out[k] = f;
+        out[2 * words + k] = fn;
+        const uint64_t r = reverse_fields(f), rn = reverse_fields(fn);
+        const int j = wr - 1 - k;
+        if (j > 0) {
+            // reverse-complement word j - 1 from reversed words j - 1 and j
+            const uint64_t sr = sh ? ((r_prev >> sh) | (r << (64 - sh))) : r_prev;
+            const uint64_t sn = sh ? ((rn_prev >> sh) | (rn << (64 - sh))) : rn_prev;
+            out[words + j - 1] = (sr ^ ~0ull) & ~(sn * 3ull);
+            out[3 * words + j - 1] = sn;
+        }
+        r_prev = r;
+        rn_prev = rn;
+    }
+    if (wr > 0) {
+        const int nv = len - 32 * (wr - 1);
+        const uint64_t keep = nv >= 32 ? ~0ull : ((1ull << (2 * nv)) - 1);
+        const uint64_t sr = r_prev >> sh, sn = rn_prev >> sh;
+        out[words + wr - 1] = (sr ^ ~0ull) & ~(sn * 3ull) & keep;
+        out[3 * words + wr - 1] = sn & keep;
+    }
+    for (int w = wr; w < words; ++w) {
+        out[w] = 0;
+        out[words + w] = 0;
+        out[2 * words + w] = 0;
+        out[3 * words + w] = 0;
+    }
+}
+
+// Staged form of pack_reads_kernel: a block copies the bytes of its rows
+// (one contiguous range of the row-major input) into shared memory with
+// 16-byte loads, then packs one row per thread from there.
+// rows_per_block * max_len must fit PACK_STAGE bytes.
+constexpr int PACK_THREADS = 256;
+constexpr int PACK_STAGE = 40960;
+constexpr int PACK_SLACK = 16;  // before and after the staged bytes
+
+__global__ void __launch_bounds__(PACK_THREADS) pack_rows_kernel(const uint8_t* __restrict__ bases,
+                                                                const uint32_t* __restrict__ lens, int64_t n_seq,
+                                                                int64_t n1, int max_len, int words,
+                                                                int rows_per_block, int bs_r1, int bs_r2,
+                                                                int64_t dst1, int64_t dst2,
+                                                                uint64_t* __restrict__ packed,
+                                                                int* __restrict__ err) {
+    __shared__ __align__(16) uint8_t s_rows[PACK_SLACK + PACK_STAGE + 16 + PACK_SLACK];
+    const int64_t r0 = static_cast<int64_t>(blockIdx.x) * rows_per_block;
+    if (r0 >= n_seq) return;
+    const int nr = static_cast<int>(n_seq - r0 < rows_per_block ? n_seq - r0 : rows_per_block);
+    const uint8_t* g = bases + r0 * static_cast<int64_t>(max_len);
+    const int bytes = nr * max_len;
+    // s_rows[PACK_SLACK + off + j] = g[j]; off lines up the 16-byte
+    // boundaries of g with those of s_rows
+    const int off = static_cast<int>(reinterpret_cast<uintptr_t>(g) & 15);
+    const int head = off ? (16 - off < bytes ? 16 - off : bytes) : 0;
+    const int n16 = (bytes - head) >> 4;
+    uint8_t* st = s_rows + PACK_SLACK + off;
+    for (int j = threadIdx.x; j < head; j += blockDim.x) st[j] = g[j];
+    const uint4* g16 = reinterpret_cast<const uint4*>(g + head);
+    uint4* s16 = reinterpret_cast<uint4*>(st + head);
+    for (int k = threadIdx.x; k < n16; k += blockDim.x) s16[k] = __ldg(g16 + k);
+    for (int j = head + 16 * n16 + threadIdx.x; j < bytes; j += blockDim.x) st[j] = g[j];
+    __syncthreads();
+    for (int lr = threadIdx.x; lr < nr; lr += blockDim.x) {
+        const int64_t r = r0 + lr;
+        const int64_t d = r < n1 ? dst1 + r : dst2 + (r - n1);
+        int len = static_cast<int>(lens[d]);
+        if (len > max_len) {
+            atomicExch(err, 1);
+            len = max_len;
+        }
+        pack_row_staged(s_rows, PACK_SLACK + off + lr * max_len, len, r < n1 ? bs_r1 : bs_r2, words,
+                        packed + d * 4 * static_cast<int64_t>(words));
+    }
+}
+
 // A batch merged from several requests.  Part j holds c pairs (or single
 // reads) staged at byte `src` of `bases`: its c first mates, then its c
 // second mates, rows of stride max_len.  Its pair i lands at batch row
@@ -506,9 +638,16 @@ unsigned grid_for(int64_t n, int block) {
 // Host launchers (stream-ordered).  Returns the number of kernels launched.
 int launch_pack(const uint8_t* d_bases, const uint32_t* d_lens, int64_t n_seq, int64_t n1, int max_len, int words,
                 int bs_r1, int bs_r2, uint64_t* d_packed, int* d_err, cudaStream_t st) {
-    const int64_t n = n_seq * words;
-    pack_reads_kernel<<<grid_for(n, 256), 256, 0, st>>>(d_bases, d_lens, n_seq, n1, max_len, words, bs_r1, bs_r2,
-                                                        0, n1, d_packed, d_err);
+    int rows = PACK_STAGE / max_len;
+    if (rows > PACK_THREADS) rows = PACK_THREADS;
+    if (rows >= 1) {
+        pack_rows_kernel<<<grid_for(n_seq, rows), PACK_THREADS, 0, st>>>(d_bases, d_lens, n_seq, n1, max_len, words,
+                                                                        rows, bs_r1, bs_r2, 0, n1, d_packed, d_err);
+    } else {  // rows longer than the stage
+        const int64_t n = n_seq * words;
+        pack_reads_kernel<<<grid_for(n, 256), 256, 0, st>>>(d_bases, d_lens, n_seq, n1, max_len, words, bs_r1,
+                                                            bs_r2, 0, n1, d_packed, d_err);
+    }
     return 1;
 }
 
