@@ -64,7 +64,7 @@ def parse_args():
     ap.add_argument("--serve-budget-gb", type=int, default=8, help="serving HBM budget")
     ap.add_argument("--tuning", default="", help="fixed kernel choice 'seed_kernel,stage1_endpoints,"
                     "stage2_blocks_per_sm,reg_level,stage1_max_rows,stage2_first_wave[,wave_endpoints,"
-                    "wave_loci_per_read,wave_max_rounds]' instead of the autotuner")
+                    "wave_loci_per_read,wave_max_rounds,wave_growth]' instead of the autotuner")
     return ap.parse_args()
 
 
@@ -265,12 +265,29 @@ def run_ours(args, rank, world, local):
         from mojoalign_b200.autotune import FIELDS, TuneResult
 
         fixed = [int(x) for x in args.tuning.split(",")]
-        fixed += [1, 1, 0, 1, 2, 32, 32, 4, 0][len(fixed):]
+        fixed += [1, 1, 0, 1, 2, 32, 32, 4, 0, 0][len(fixed):]
         ctx.set_tuning(*fixed)
         tune = TuneResult(dict(zip(FIELDS, fixed)), float("nan"), [])
         ns = 0
     else:
-        tune = autotune(ctx, gi, tb, tl, ns, True, READ_LEN, "C2T", "G2A", params)
+        # the sample as one device-resident call, like the timed steps
+        dev = f"cuda:{local}"
+        d_tb = torch.from_numpy(tb).to(dev).reshape(-1)
+        d_tl = torch.from_numpy(tl.view(np.int32)).to(dev)
+        t_out = {f: torch.empty(2 * ns, dtype=torch.int32, device=dev) for f in MapResult.FIELDS}
+        t_dbg = {f: torch.empty(2 * ns, dtype=torch.int64 if f in ("uk", "ul") else torch.int32, device=dev)
+                 for f in MapResult.DEBUG}
+
+        def run_sample():
+            map_batch_device(ctx, gi, d_tb.data_ptr(), d_tl.data_ptr(), ns, True, READ_LEN,
+                             {f: x.data_ptr() for f, x in t_out.items()}, "C2T", "G2A", params,
+                             d_debug={f: x.data_ptr() for f, x in t_dbg.items()},
+                             stream=torch.cuda.current_stream().cuda_stream)
+            outs = {f: x.cpu().numpy() for f, x in list(t_out.items()) + list(t_dbg.items())}
+            return outs, ctx.kernel_ms()[1]
+
+        tune = autotune(ctx, gi, tb, tl, ns, True, READ_LEN, "C2T", "G2A", params, run=run_sample)
+        del d_tb, d_tl, t_out, t_dbg
     del tb, tl
 
     # ---- device-resident inputs and outputs ----
@@ -493,7 +510,7 @@ def run_forms(args, ctx, gi, params, fa, local, best_tuning):
         ms = e0.elapsed_time(e1) / reps
         return n / (ms / 1000.0), {f: t.cpu().numpy().view(np.uint32) for f, t in d_out.items()}
 
-    plain_tuning = (0, 1, 0, 1, 16, 32, 32, 4, 0)
+    plain_tuning = (0, 1, 0, 1, 16, 32, 32, 4, 0, 0)
     plain_rate, plain_out = device_form(plain_tuning)
     batched_rate, batched_out = device_form(best_tuning)
     same = all(np.array_equal(plain_out[f], batched_out[f]) for f in MapResult.FIELDS)

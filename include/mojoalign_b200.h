@@ -275,6 +275,11 @@ int ma_last_launch_count(const ma_ctx* ctx);
  *   wave_max_rounds       wavefront rounds before the reads still active
  *                         go to the stage-2 warps (0 = as many as the
  *                         longest read needs, default).
+ *   wave_growth           1: each wavefront round after the second covers
+ *                         twice the endpoints of the one before (fewer,
+ *                         fuller rounds for the reads that stay active
+ *                         longest); 0: every later round covers
+ *                         wave_endpoints (default).
  */
 typedef struct ma_tuning {
     int32_t seed_kernel;
@@ -286,6 +291,7 @@ typedef struct ma_tuning {
     int32_t wave_endpoints;
     int32_t wave_loci_per_read;
     int32_t wave_max_rounds;
+    int32_t wave_growth;
 } ma_tuning;
 int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t);
 int ma_ctx_get_tuning(const ma_ctx* ctx, ma_tuning* t);

@@ -86,7 +86,7 @@ struct ma_ctx {
     struct Slot {
         DevBuf bases, lens, out[12];
     } slot[2];
-    ma_tuning tuning{1, 1, 0, 1, 2, 32, 32, 4, 0};
+    ma_tuning tuning{1, 1, 0, 1, 2, 32, 32, 4, 0, 0};
     int sm_count = 0;
     DevBuf seed_scratch;
     DevBuf bases, lens, packed, err_flag;
@@ -593,6 +593,7 @@ int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t) {
         if (t->wave_loci_per_read < 1 || t->wave_loci_per_read > 64)
             fail(MA_ERR_ARG, "wave_loci_per_read must be in 1..64");
         if (t->wave_max_rounds < 0) fail(MA_ERR_ARG, "wave_max_rounds must be >= 0");
+        if (t->wave_growth < 0 || t->wave_growth > 1) fail(MA_ERR_ARG, "wave_growth must be 0 or 1");
         ctx->tuning = *t;
     });
 }

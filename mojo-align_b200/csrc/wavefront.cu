@@ -45,6 +45,8 @@ constexpr int N_COUNTERS = 16;
 constexpr uint64_t LIDX_MASK = (1ull << 27) - 1;  // round keys: nm << 54 | ordinal << 27 | locus index
 constexpr uint64_t MAX_LOCI = LIDX_MASK;          // list capacity limit (indices fit 27 bits)
 
+constexpr uint32_t DEAD_LOCUS = 0xFFFFFFFFu;  // WLocus.read of a slot without a locus
+
 // One candidate locus of a round.
 struct WLocus {
     int64_t b0;
@@ -181,18 +183,10 @@ __global__ void __launch_bounds__(256) wf_search_kernel(DevIndex ix, DevReads R,
                 if (!dup) sd = search_endpoint<S>(ix, rd, e, P, t);
             }
         }
-        // count pass: loci not in the memo
-        uint32_t n_keep = 0;
-        if (sd.found) {
-            for (uint64_t hi = sd.k; hi <= sd.l; ++hi) {
-                const uint64_t sa_pos = __ldg(ix.sa + hi);
-                if constexpr (S) t.sa_loads++;
-                int64_t b0;
-                int rev;
-                n_keep += fresh_locus(ix, w, r, n_memo, sa_pos, sd.s, e, qlen, b0, rev);
-            }
-        }
-        uint32_t incl = n_keep;
+        // every SA row takes a list slot (one atomic per warp); rows that
+        // give no new locus leave their slot dead
+        const uint32_t n_rows = sd.found ? static_cast<uint32_t>(sd.l - sd.k + 1) : 0u;
+        uint32_t incl = n_rows;
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
             if (lane >= o) incl += v;
@@ -201,17 +195,23 @@ __global__ void __launch_bounds__(256) wf_search_kernel(DevIndex ix, DevReads R,
         uint32_t wbase = 0;
         if (lane == 31 && warp_total) wbase = atomicAdd(&w.counters[C_LOCI], warp_total);
         wbase = __shfl_sync(0xFFFFFFFFu, wbase, 31);
-        if (n_keep) {
-            uint64_t slot = static_cast<uint64_t>(wbase) + (incl - n_keep);
-            for (uint64_t hi = sd.k; hi <= sd.l; ++hi) {
-                int64_t b0;
-                int rev;
-                if (!fresh_locus(ix, w, r, n_memo, __ldg(ix.sa + hi), sd.s, e, qlen, b0, rev)) continue;
+        if (n_rows) {
+            uint64_t slot = static_cast<uint64_t>(wbase) + (incl - n_rows);
+            for (uint64_t hi = sd.k; hi <= sd.l; ++hi, ++slot) {
                 if (slot >= w.locus_cap) {
                     w.overflow[r] = 1;
                     break;
                 }
+                const uint64_t sa_pos = __ldg(ix.sa + hi);
+                if constexpr (S) t.sa_loads++;
                 WLocus L;
+                int64_t b0;
+                int rev;
+                if (!fresh_locus(ix, w, r, n_memo, sa_pos, sd.s, e, qlen, b0, rev)) {
+                    L.read = DEAD_LOCUS;
+                    w.loci[slot] = L;
+                    continue;
+                }
                 L.b0 = b0;
                 L.uk = sd.k;
                 L.ul = sd.l;
@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(256) wf_search_kernel(DevIndex ix, DevReads R,
                 L.e = e;
                 L.crid = static_cast<int32_t>(contig_hint(ix, b0).crid);
                 L.rev = rev;
-                w.loci[slot++] = L;
+                w.loci[slot] = L;
                 if constexpr (S) tally_locus(t, b0, clamps_for(P, qlen).adj_cap, qlen);
                 const uint32_t m = atomicAdd(&w.memo_next[r], 1u);
                 if (m < static_cast<uint32_t>(MEMO1)) w.memo[r * MEMO1 + m] = static_cast<uint64_t>(b0 * 2 + rev);
@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(EVAL_THREADS) wf_eval_kernel(DevIndex ix, DevR
             const WLocus L = w.loci[li];
             wl[lane] = L;
             const int64_t r = L.read;
-            if (!w.overflow[r]) {
+            if (L.read != DEAD_LOCUS && !w.overflow[r]) {
                 const ReadView rd = read_view(R, r);
                 const Clamps cl = clamps_for(P, rd.qlen);
                 const uint64_t bn = w.best_key[r] >> ORD_SHIFT;
@@ -424,11 +424,18 @@ int grid_blocks(K kernel, int sm_count) {
 
 template <bool S>
 int launch_rounds(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, const Wave& w,
-                  int max_len, int w0, int wn, int max_rounds, int sm_count, int* d_err, unsigned long long* tally,
-                  cudaStream_t st) {
+                  int max_len, int w0, int wn, int max_rounds, int growth, int sm_count, int* d_err,
+                  unsigned long long* tally, cudaStream_t st) {
     const int n_end_max = endpoint_count_host(P, max_len);
-    int rounds = 1;
-    if (n_end_max > w0) rounds += (n_end_max - w0 + wn - 1) / wn;
+    // round widths: w0, then wn (doubling from the third round with growth)
+    int widths[1100];
+    int rounds = 0, covered = 0;
+    for (int width = w0; covered < n_end_max || rounds == 0; ++rounds) {
+        widths[rounds] = width;
+        covered += width;
+        if (rounds == 0) width = wn;
+        else if (growth && width < 4096) width *= 2;
+    }
     if (max_rounds > 0 && rounds > max_rounds) rounds = max_rounds;
     static const int g_search = grid_blocks(wf_search_kernel<S>, sm_count);
     static const int g_eval = grid_blocks(wf_eval_kernel<S>, sm_count);  // EVAL_THREADS = 256
@@ -437,7 +444,7 @@ int launch_rounds(const DevIndex& ix, const DevReads& R, const DevParams& P, con
     wf_init_kernel<<<init_blocks ? init_blocks : 1, 256, 0, st>>>(w, out, R.lens, R.n_seq);
     int launches = 1;
     for (int k = 0; k < rounds; ++k) {
-        const int width = k == 0 ? w0 : wn;
+        const int width = widths[k];
         const uint32_t* act = w.active[k & 1];
         uint32_t* nxt = w.active[(k + 1) & 1];
         if (k > 0) {
@@ -469,10 +476,10 @@ int launch_seed_wavefront(const DevIndex& ix, const DevReads& R, const DevParams
     wave_layout(static_cast<char*>(scratch), R.n_seq, locus_capacity(R.n_seq, t.wave_loci_per_read), &w);
     const int w0 = t.stage1_endpoints > 0 ? t.stage1_endpoints : 1;
     const int wn = t.wave_endpoints > 0 ? t.wave_endpoints : 1;
-    int launches = d_tally ? launch_rounds<true>(ix, R, P, out, w, max_len, w0, wn, t.wave_max_rounds, sm_count,
-                                                 d_err, d_tally, st)
-                           : launch_rounds<false>(ix, R, P, out, w, max_len, w0, wn, t.wave_max_rounds, sm_count,
-                                                  d_err, nullptr, st);
+    int launches = d_tally ? launch_rounds<true>(ix, R, P, out, w, max_len, w0, wn, t.wave_max_rounds,
+                                                 t.wave_growth, sm_count, d_err, d_tally, st)
+                           : launch_rounds<false>(ix, R, P, out, w, max_len, w0, wn, t.wave_max_rounds,
+                                                  t.wave_growth, sm_count, d_err, nullptr, st);
     // reads that overflowed the locus list or outlived the rounds
     launches += launch_stage2_pending(ix, R, P, out, w.best_key, w.memo, w.memo_n, w.resume, w.pending,
                                       w.counters + C_HANDOFF, stage2_blocks, t.reg_level, 32, d_tally, st);

@@ -101,7 +101,8 @@ class ma_index_options(C.Structure):
 class ma_tuning(C.Structure):
     _fields_ = [("seed_kernel", C.c_int32), ("stage1_endpoints", C.c_int32), ("stage2_blocks_per_sm", C.c_int32),
                 ("reg_level", C.c_int32), ("stage1_max_rows", C.c_int32), ("stage2_first_wave", C.c_int32),
-                ("wave_endpoints", C.c_int32), ("wave_loci_per_read", C.c_int32), ("wave_max_rounds", C.c_int32)]
+                ("wave_endpoints", C.c_int32), ("wave_loci_per_read", C.c_int32), ("wave_max_rounds", C.c_int32),
+                ("wave_growth", C.c_int32)]
 
 
 class ma_read_model(C.Structure):

@@ -20,24 +20,21 @@ from .params import FmParams
 
 DEFAULT_CANDIDATES = [
     (0, 1, 0, 1, 16, 32, 32),
-    (1, 1, 0, 2, 2, 32, 32),
-    (1, 1, 0, 2, 1, 32, 32),
     (1, 1, 0, 2, 1, 1, 32),
-    (1, 1, 0, 2, 1, 4, 32),
     (1, 1, 0, 1, 1, 1, 32),
-    (1, 2, 0, 2, 2, 4, 32),
-    (2, 1, 0, 1, 1, 1, 32),
-    (2, 1, 0, 2, 1, 1, 32),
     (2, 1, 0, 1, 1, 1, 16),
-    (2, 1, 0, 1, 1, 1, 64),
-    (2, 2, 0, 1, 1, 1, 32),
-    (2, 1, 0, 0, 1, 1, 32),
+    (2, 1, 0, 1, 1, 1, 32),
+    (2, 1, 0, 2, 1, 1, 16),
+    (2, 1, 0, 1, 1, 1, 8, 4, 0, 1),
+    (2, 1, 0, 1, 1, 1, 16, 4, 0, 1),
+    (2, 1, 0, 1, 1, 1, 32, 4, 0, 1),
+    (2, 2, 0, 1, 1, 1, 16, 4, 0, 1),
 ]
 FIELDS = ("seed_kernel", "stage1_endpoints", "stage2_blocks_per_sm", "reg_level", "stage1_max_rows",
-          "stage2_first_wave", "wave_endpoints", "wave_loci_per_read", "wave_max_rounds")
+          "stage2_first_wave", "wave_endpoints", "wave_loci_per_read", "wave_max_rounds", "wave_growth")
 
 
-DEFAULTS = (1, 1, 0, 1, 2, 32, 32, 4, 0)
+DEFAULTS = (1, 1, 0, 1, 2, 32, 32, 4, 0, 0)
 
 
 @dataclass
@@ -49,29 +46,34 @@ class TuneResult:
 
 def autotune(ctx: GpuContext, index: GpuIndex, bases: np.ndarray, lens: np.ndarray, n1: int, paired: bool,
              max_len: int, bs_r1="C2T", bs_r2="G2A", params: FmParams | None = None, candidates=None,
-             reps: int = 2) -> TuneResult:
+             reps: int = 2, run=None) -> TuneResult:
+    """`run()`, when given, maps the sample once with the context's current
+    tuning and returns (outputs as a dict of arrays, seed/extend ms); by
+    default the sample goes through map_batch from host memory."""
     params = params or FmParams()
     candidates = candidates or DEFAULT_CANDIDATES
     n_seq = n1 * (2 if paired else 1)
     ref = None
     timings = []
+
+    def host_run():
+        res = MapResult.empty(n_seq, debug=True)
+        map_batch(ctx, index, bases, lens, n1, paired, max_len, bs_r1, bs_r2, params, out=res)
+        return {f: getattr(res, f) for f in MapResult.FIELDS + MapResult.DEBUG}, ctx.kernel_ms()[1]
+
+    run = run or host_run
     ctx.set_profiling(1)
     try:
         for cand in candidates:
             ctx.set_tuning(*cand)
-            res = MapResult.empty(n_seq, debug=True)
-            map_batch(ctx, index, bases, lens, n1, paired, max_len, bs_r1, bs_r2, params, out=res)
+            out, _ = run()
             if ref is None:
-                ref = res
+                ref = out
             else:
-                for f in MapResult.FIELDS + MapResult.DEBUG:
-                    if not np.array_equal(getattr(res, f), getattr(ref, f)):
+                for f in ref:
+                    if not np.array_equal(out[f], ref[f]):
                         raise AssertionError(f"tuning {cand} changed output {f}; the kernels are not result-neutral")
-            ms = []
-            for _ in range(reps):
-                map_batch(ctx, index, bases, lens, n1, paired, max_len, bs_r1, bs_r2, params, out=res)
-                ms.append(ctx.kernel_ms()[1])
-            timings.append((min(ms), cand))
+            timings.append((min(run()[1] for _ in range(reps)), cand))
     finally:
         ctx.set_profiling(0)
     best_ms, best = min(timings)

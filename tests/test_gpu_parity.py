@@ -40,9 +40,11 @@ def gpu_index(ctx, prefix, k, k3=0):
 # stage2_blocks_per_sm, reg_level, stage1_max_rows, stage2_first_wave, wave_endpoints, wave_loci_per_read,
 # wave_max_rounds): one thread per read; two stages with the first 1, 2 or 3 right endpoints in stage 1, at
 # each register budget; wavefront rounds of several widths, with a locus list too small for the batch (reads
-# overflow to the stage-2 warps) and with the rounds cut short (the rest finished by stage 2).
+# overflow to the stage-2 warps), with the rounds cut short (the rest finished by stage 2) and with doubling
+# round widths.
 TUNINGS = [(0, 1, 0, 0, 16, 32), (1, 1, 0, 1, 2, 32), (1, 3, 1, 2, 1, 1), (1, 2, 0, 0, 16, 4), (1, 1, 0, 2, 1, 7),
-           (2, 1, 0, 1, 2, 32, 32, 4, 0), (2, 2, 0, 2, 1, 1, 5, 1, 0), (2, 1, 0, 0, 2, 32, 3, 4, 2)]
+           (2, 1, 0, 1, 2, 32, 32, 4, 0), (2, 2, 0, 2, 1, 1, 5, 1, 0), (2, 1, 0, 0, 2, 32, 3, 4, 2),
+           (2, 1, 0, 1, 1, 1, 4, 2, 0, 1)]
 
 
 def compare(prefix, ctx, bases, lens, n1, paired, max_len, params, k=12, bs=(1, 2), tunings=TUNINGS, k3=12):
