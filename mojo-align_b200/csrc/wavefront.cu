@@ -45,7 +45,8 @@ constexpr int N_COUNTERS = 16;
 constexpr uint64_t LIDX_MASK = (1ull << 27) - 1;  // round keys: nm << 54 | ordinal << 27 | locus index
 constexpr uint64_t MAX_LOCI = LIDX_MASK;          // list capacity limit (indices fit 27 bits)
 
-constexpr uint32_t DEAD_LOCUS = 0xFFFFFFFFu;  // WLocus.read of a slot without a locus
+constexpr uint32_t DEAD_LOCUS = 0xFFFFFFFFu;
+constexpr int PREDICT_MEMO = 4;  // memo loci a duplicate prediction checks besides the best  // WLocus.read of a slot without a locus
 
 // One candidate locus of a round.
 struct WLocus {
@@ -177,8 +178,12 @@ __global__ void __launch_bounds__(256) wf_search_kernel(DevIndex ix, DevReads R,
             if (ei < endpoint_count(P, qlen)) {
                 e = P.seed_len - 1 + ei * P.seed_stride;
                 n_memo = w.memo_n[r];
-                const bool dup = can_predict && predicted_duplicate<S>(ix, rd, e, P, w.best_tag[r],
-                                                                       w.memo + r * MEMO1, n_memo < 4 ? n_memo : 4, t);
+                // a read with no hit yet gains little from predicting its
+                // rejected loci again: only reads with a best try the memo
+                const int64_t best_tag = w.best_tag[r];
+                const bool dup = can_predict && best_tag != -1 &&
+                                 predicted_duplicate<S>(ix, rd, e, P, best_tag, w.memo + r * MEMO1,
+                                                        n_memo < PREDICT_MEMO ? n_memo : PREDICT_MEMO, t);
                 if constexpr (S) t.skipped += dup;
                 if (!dup) sd = search_endpoint<S>(ix, rd, e, P, t);
             }
