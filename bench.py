@@ -37,6 +37,15 @@ for p in (ROOT, ROOT / "mojo-align_b200"):
 import numpy as np  # noqa: E402
 
 METRIC = "reads/s seed+extend"
+# DRAM bytes / algorithmic bytes of the wavefront seed kernels, from one ncu
+# capture of the 50 Mbp / 2M-read case (profiles/seed_wavefront_50mbp_1Mpairs.md)
+TRAFFIC_OVER_ALG = 1.73
+SEED_KERNELS = {
+    0: "seed/extend: seed_stage1_kernel over every endpoint (one thread per read)",
+    1: "seed/extend: seed_stage1_kernel + seed_stage2_kernel (thread per read, then warp per read)",
+    2: "seed/extend: wavefront rounds (wf_search_kernel + wf_eval_kernel + wf_finalize_kernel per round, "
+       "seed_stage2_kernel for reads left over)",
+}
 READ_LEN = 150
 
 
@@ -358,10 +367,14 @@ def run_ours(args, rank, world, local):
     seed_avg_ms = statistics.mean(seed_ms)
     achieved = alg_bytes / (seed_avg_ms / 1000.0) / 1e9
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
-            "frac": round(achieved / peaks.get("hbm_gbs"), 4), "traffic": None,
+            "frac": round(achieved / peaks.get("hbm_gbs"), 4),
+            "traffic": int(alg_bytes * TRAFFIC_OVER_ALG) if tune.tuning.get("seed_kernel") == 2 else None,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the seed kernels of one call "
+                              "on the 50 Mbp / 2M-read case, as a ratio to the algorithmic bytes "
+                              f"({TRAFFIC_OVER_ALG}), applied to this call's algorithmic bytes",
             "peak_source": "fallback" if peaks.get("_fallback") else "measured (MEASURED_PEAKS.json hbm_gbs)",
-            "kernel": "seed/extend (seed_stage1_kernel + seed_stage2_kernel)", "kernel_ms": round(seed_avg_ms, 3),
-            "stage1_ms": round(statistics.mean(stage1_ms), 3),
+            "kernel": SEED_KERNELS.get(tune.tuning.get("seed_kernel", 1), "seed/extend"),
+            "kernel_ms": round(seed_avg_ms, 3), "stage1_ms": round(statistics.mean(stage1_ms), 3),
             "pack_ms": round(statistics.mean(x[0] for x in other_ms), 3),
             "rescue_ms": round(statistics.mean(x[1] for x in other_ms), 3),
             "alg_bytes_per_launch": int(alg_bytes),
