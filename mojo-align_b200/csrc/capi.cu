@@ -464,8 +464,13 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
         // mates).  Chunk k's R1 rows and R2 rows are copied into one slot as
         // a batch of its own while chunk k-1 computes, and chunk k-1's results
         // go back into the caller's arrays (at the pairs' positions) while
-        // chunk k computes: three streams, two slots.
-        const uint32_t chunk = std::max<uint32_t>(131072u, (n1 + 15) / 16);
+        // chunk k computes: three streams, two slots.  Chunks grow by half
+        // from a small first one (the pipeline fills quickly, while the
+        // large later chunks keep the kernels' per-call overhead small);
+        // copies run faster than the kernels, so each copy still hides
+        // behind the previous chunk's kernels.
+        const uint32_t first = std::min<uint32_t>(n1, std::max<uint32_t>(65536u, n1 / 64));
+        const uint32_t cap = std::max<uint32_t>(first, std::max<uint32_t>(131072u, n1 / 4));
         const int mates = paired ? 2 : 1;
         void* host_out[12] = {out->rid, out->pos, out->mapq, out->flag, out->sl, out->sr, out->nm,
                               want_dbg ? dbg->uk : nullptr, want_dbg ? dbg->ul : nullptr,
@@ -474,13 +479,18 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
         const size_t width[12] = {4, 4, 4, 4, 4, 4, 4, 8, 8, 4, 4, 4};
         int k = 0;
         float acc_ms[4] = {0, 0, 0, 0};
-        for (uint32_t a = 0; a < n1; a += chunk, ++k) {
-            const uint32_t c = std::min(chunk, n1 - a);
-            const int64_t cs = static_cast<int64_t>(c) * mates;
-            ma_ctx::Slot& sl = ctx->slot[k & 1];
+        // both slots sized for the largest chunk before any copy starts
+        // (growing a buffer later would free memory still in use)
+        for (auto& sl : ctx->slot) {
+            const int64_t cs = static_cast<int64_t>(std::min(cap, n1)) * mates;
             sl.bases.ensure(static_cast<size_t>(cs) * max_len);
             sl.lens.ensure(cs * 4);
             for (int f = 0; f < 12; ++f) sl.out[f].ensure(cs * width[f]);
+        }
+        uint32_t chunk = first;
+        for (uint32_t a = 0, c = 0; a < n1; a += c, ++k, chunk = std::min<uint32_t>(cap, chunk + chunk / 2)) {
+            c = std::min(chunk, n1 - a);
+            ma_ctx::Slot& sl = ctx->slot[k & 1];
             // copy: wait until the slot's previous chunk has been read back
             ck(cudaStreamWaitEvent(ctx->copy_stream, ctx->slot_free[k & 1], 0), "cudaStreamWaitEvent");
             for (int m = 0; m < mates; ++m) {
