@@ -413,7 +413,7 @@ __device__ void eval_adj(const DevIndex& ix, const ReadView& rd, int64_t b0, int
 }
 
 // Shifts of one locus that can fold a candidate into a best of nm prune_nm
-// (bit adj + adj_cap set), from the first two 16-base halves of the core
+// (bit adj + adj_cap set), from the first three 16-base halves of the core
 // [clip_cap, qlen - clip_cap) alone.  A shift's full and clipped compares
 // have at least as many mismatches as any part of the core, so a shift
 // whose partial core count reaches min(prune_nm, budget + 1) has no
@@ -433,50 +433,58 @@ __device__ uint32_t live_shifts(const DevIndex& ix, const ReadView& rd, int64_t 
     const uint64_t* q = is_rev ? rd.rc : rd.fwd;
     const uint64_t* qn = is_rev ? rd.nr : rd.nf;
     const int h0 = c0 >> 4;
-    const int h1 = ((c1 - 1) >> 4) < h0 + 1 ? ((c1 - 1) >> 4) : h0 + 1;
+    const int hl = (c1 - 1) >> 4;  // last half holding core bases
+    const int nh = hl - h0 + 1 < 3 ? hl - h0 + 1 : 3;
     // loci whose filter window leaves the text are left to eval_adj
-    if (b0 - adj_cap + 16 * h0 < 0 || b0 + adj_cap + 1 + 16 * (h1 + 1) > static_cast<int64_t>(ix.l_pac)) return all;
-    // the text of every shift's two halves lies in five 16-base words from
-    // wlo: shift i starts s0 + i bases into them
+    if (b0 - adj_cap + 16 * h0 < 0 || b0 + adj_cap + 1 + 16 * (h0 + nh) > static_cast<int64_t>(ix.l_pac)) return all;
+    // the text of every shift's halves lies in six 16-base words from wlo:
+    // shift i starts s0 + i bases into them
     const uint32_t* p32 = reinterpret_cast<const uint32_t*>(ix.pacw);
     const int64_t p0 = b0 - adj_cap + 16 * h0 + 32 * PAC_PAD;
     const uint64_t wlo = static_cast<uint64_t>(p0) >> 4;
     const int s0 = static_cast<int>(p0 & 15);
     const uint32_t w0 = __ldg(p32 + wlo), w1 = __ldg(p32 + wlo + 1), w2 = __ldg(p32 + wlo + 2);
-    const uint32_t w3 = __ldg(p32 + wlo + 3), w4 = __ldg(p32 + wlo + 4);
+    const uint32_t w3 = __ldg(p32 + wlo + 3), w4 = __ldg(p32 + wlo + 4), w5 = __ldg(p32 + wlo + 5);
     const uint32_t* q32 = reinterpret_cast<const uint32_t*>(q);
     const uint32_t* n32 = reinterpret_cast<const uint32_t*>(qn);
     const uint32_t qa = q32[h0], na = n32[h0], ma = range_mask16(h0, c0, c1);
-    const uint32_t qb = h1 > h0 ? q32[h1] : 0u, nb = h1 > h0 ? n32[h1] : 0u;
-    const uint32_t mb = h1 > h0 ? range_mask16(h1, c0, c1) : 0u;
-    // mismatch bits of both halves for the shift starting `off` bases in
-    auto halves = [&](int off, uint32_t& xa, uint32_t& xb) {
+    const uint32_t qb = nh > 1 ? q32[h0 + 1] : 0u, nb = nh > 1 ? n32[h0 + 1] : 0u;
+    const uint32_t mb = nh > 1 ? range_mask16(h0 + 1, c0, c1) : 0u;
+    const uint32_t qc = nh > 2 ? q32[h0 + 2] : 0u, nc = nh > 2 ? n32[h0 + 2] : 0u;
+    const uint32_t mc = nh > 2 ? range_mask16(h0 + 2, c0, c1) : 0u;
+    // mismatch bits of the three halves for the shift starting `off` bases in
+    auto halves = [&](int off, uint32_t& xa, uint32_t& xb, uint32_t& xc) {
         const int k = off >> 4;
         const uint32_t sh = static_cast<uint32_t>(off & 15) * 2;
         const uint32_t a = k == 0 ? w0 : (k == 1 ? w1 : w2);
         const uint32_t b = k == 0 ? w1 : (k == 1 ? w2 : w3);
         const uint32_t c = k == 0 ? w2 : (k == 1 ? w3 : w4);
+        const uint32_t d = k == 0 ? w3 : (k == 1 ? w4 : w5);
         const uint32_t ta = qa ^ __funnelshift_r(a, b, sh), tb = qb ^ __funnelshift_r(b, c, sh);
+        const uint32_t tc = qc ^ __funnelshift_r(c, d, sh);
         xa = (((ta | (ta >> 1)) & 0x55555555u) | na) & ma;
         xb = (((tb | (tb >> 1)) & 0x55555555u) | nb) & mb;
+        xc = (((tc | (tc >> 1)) & 0x55555555u) | nc) & mc;
     };
-    if constexpr (S) t.read_words += 5;
-    uint32_t live = 0, z0a = 0, z0b = 0, z1a = 0, z1b = 0;  // shift 0 and +1 bits
+    if constexpr (S) t.read_words += 6;
+    uint32_t live = 0, z0a = 0, z0b = 0, z0c = 0, z1a = 0, z1b = 0, z1c = 0;  // shift 0 and +1 bits
     for (int i = 0; i < A; ++i) {
-        uint32_t xa, xb;
-        halves(s0 + i, xa, xb);
-        if (__popc(xa) + __popc(xb) < cap) live |= 1u << i;
+        uint32_t xa, xb, xc;
+        halves(s0 + i, xa, xb, xc);
+        if (__popc(xa) + __popc(xb) + __popc(xc) < cap) live |= 1u << i;
         if (i == adj_cap) {
             z0a = xa;
             z0b = xb;
+            z0c = xc;
         } else if (i == adj_cap + 1) {
             z1a = xa;
             z1b = xb;
+            z1c = xc;
         }
     }
     if (!is_rev && !((live >> adj_cap) & 1u)) {
-        if (adj_cap == 0) halves(s0 + 1, z1a, z1b);
-        if (1 + __popc(z0a & z1a) + __popc(z0b & z1b) < cap) live |= 1u << adj_cap;
+        if (adj_cap == 0) halves(s0 + 1, z1a, z1b, z1c);
+        if (1 + __popc(z0a & z1a) + __popc(z0b & z1b) + __popc(z0c & z1c) < cap) live |= 1u << adj_cap;
     }
     return live;
 }
