@@ -200,37 +200,54 @@ __global__ void __launch_bounds__(256) wf_search_kernel(DevIndex ix, DevReads R,
         uint32_t wbase = 0;
         if (lane == 31 && warp_total) wbase = atomicAdd(&w.counters[C_LOCI], warp_total);
         wbase = __shfl_sync(0xFFFFFFFFu, wbase, 31);
-        if (n_rows) {
-            uint64_t slot = static_cast<uint64_t>(wbase) + (incl - n_rows);
-            for (uint64_t hi = sd.k; hi <= sd.l; ++hi, ++slot) {
-                if (slot >= w.locus_cap) {
-                    w.overflow[r] = 1;
-                    break;
-                }
-                const uint64_t sa_pos = __ldg(ix.sa + hi);
-                if constexpr (S) t.sa_loads++;
-                WLocus L;
-                int64_t b0;
-                int rev;
-                if (!fresh_locus(ix, w, r, n_memo, sa_pos, sd.s, e, qlen, b0, rev)) {
-                    L.read = DEAD_LOCUS;
-                    w.loci[slot] = L;
-                    continue;
-                }
-                L.b0 = b0;
-                L.uk = sd.k;
-                L.ul = sd.l;
-                L.read = static_cast<uint32_t>(r);
-                L.ord_row = (static_cast<uint32_t>(ei) * 16 + static_cast<uint32_t>(hi - sd.k)) * ADJ_SPAN;
-                L.us = sd.s;
-                L.e = e;
-                L.crid = static_cast<int32_t>(contig_hint(ix, b0).crid);
-                L.rev = rev;
-                w.loci[slot] = L;
-                if constexpr (S) tally_locus(t, b0, clamps_for(P, qlen).adj_cap, qlen);
-                const uint32_t m = atomicAdd(&w.memo_next[r], 1u);
-                if (m < static_cast<uint32_t>(MEMO1)) w.memo[r * MEMO1 + m] = static_cast<uint64_t>(b0 * 2 + rev);
+        // the warp's rows, 32 at a time, one per lane (seeds have 1..16 rows)
+        for (uint32_t c0 = 0; c0 < warp_total; c0 += 32) {
+            const uint32_t idx = c0 + lane;
+            int owner = 0;  // first lane whose inclusive row count exceeds idx
+            for (int step = 16; step >= 1; step >>= 1) {
+                const uint32_t v = __shfl_sync(0xFFFFFFFFu, incl, owner + step - 1);
+                if (v <= idx) owner += step;
             }
+            const int own = owner < 32 ? owner : 31;
+            const uint64_t o_k = __shfl_sync(0xFFFFFFFFu, sd.k, own);
+            const uint64_t o_l = __shfl_sync(0xFFFFFFFFu, sd.l, own);
+            const int o_s = __shfl_sync(0xFFFFFFFFu, sd.s, own);
+            const int o_e = __shfl_sync(0xFFFFFFFFu, e, own);
+            const int o_ei = __shfl_sync(0xFFFFFFFFu, ei, own);
+            const int o_qlen = __shfl_sync(0xFFFFFFFFu, qlen, own);
+            const int o_memo = __shfl_sync(0xFFFFFFFFu, n_memo, own);
+            const int64_t o_r = __shfl_sync(0xFFFFFFFFu, r, own);
+            const uint32_t o_first = __shfl_sync(0xFFFFFFFFu, incl - n_rows, own);
+            if (idx >= warp_total) continue;
+            const uint64_t hi = o_k + (idx - o_first);
+            const uint64_t slot = static_cast<uint64_t>(wbase) + idx;
+            if (slot >= w.locus_cap) {
+                w.overflow[o_r] = 1;
+                continue;
+            }
+            const uint64_t sa_pos = __ldg(ix.sa + hi);
+            if constexpr (S) t.sa_loads++;
+            WLocus L;
+            int64_t b0;
+            int rev;
+            if (!fresh_locus(ix, w, o_r, o_memo, sa_pos, o_s, o_e, o_qlen, b0, rev)) {
+                L.read = DEAD_LOCUS;
+                w.loci[slot] = L;
+                continue;
+            }
+            L.b0 = b0;
+            L.uk = o_k;
+            L.ul = o_l;
+            L.read = static_cast<uint32_t>(o_r);
+            L.ord_row = (static_cast<uint32_t>(o_ei) * 16 + static_cast<uint32_t>(hi - o_k)) * ADJ_SPAN;
+            L.us = o_s;
+            L.e = o_e;
+            L.crid = static_cast<int32_t>(contig_hint(ix, b0).crid);
+            L.rev = rev;
+            w.loci[slot] = L;
+            if constexpr (S) tally_locus(t, b0, clamps_for(P, o_qlen).adj_cap, o_qlen);
+            const uint32_t m = atomicAdd(&w.memo_next[o_r], 1u);
+            if (m < static_cast<uint32_t>(MEMO1)) w.memo[o_r * MEMO1 + m] = static_cast<uint64_t>(b0 * 2 + rev);
         }
     }
     flush_tally<S>(t, tally_out);
