@@ -259,7 +259,10 @@ int ma_last_launch_count(const ma_ctx* ctx);
  *                         occupancy maximum).
  *   reg_level             register budget of the seed kernels: 0 = the
  *                         compiler's choice, 1 = 80 registers (default),
- *                         2 = 64 registers.
+ *                         2 = 64 registers (stage kernels); for the
+ *                         wavefront's search / eval kernels 0 = the
+ *                         compiler's choice, 1 = 5 / 4 blocks of 256
+ *                         threads per SM, 2 = 6 / 5.
  *   stage1_max_rows       stage 1 hands a read to stage 2 as soon as one of
  *                         its seeds has more SA rows than this (1..16,
  *                         default 2; 16 = never).

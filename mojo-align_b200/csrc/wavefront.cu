@@ -151,8 +151,8 @@ __device__ __forceinline__ bool fresh_locus(const DevIndex& ix, const Wave& w, i
 
 // Search: one thread per (active read, endpoint of the round).  The loop
 // is warp-uniform (whole warps step together) for the warp-wide append.
-template <bool S>
-__global__ void __launch_bounds__(256) wf_search_kernel(DevIndex ix, DevReads R, DevParams P, Wave w,
+template <bool S, int MINB>
+__global__ void __launch_bounds__(256, MINB) wf_search_kernel(DevIndex ix, DevReads R, DevParams P, Wave w,
                                                         const uint32_t* __restrict__ act, int width,
                                                         unsigned long long* __restrict__ tally_out) {
     Tally t{};
@@ -260,8 +260,8 @@ __global__ void __launch_bounds__(256) wf_search_kernel(DevIndex ix, DevReads R,
 // loop over loci is warp-uniform for the redistribution.
 constexpr int EVAL_THREADS = 256;
 
-template <bool S>
-__global__ void __launch_bounds__(EVAL_THREADS) wf_eval_kernel(DevIndex ix, DevReads R, DevParams P, Wave w,
+template <bool S, int MINB>
+__global__ void __launch_bounds__(EVAL_THREADS, MINB) wf_eval_kernel(DevIndex ix, DevReads R, DevParams P, Wave w,
                                                                unsigned long long* __restrict__ tally_out) {
     __shared__ WLocus s_loci[EVAL_THREADS];
     constexpr unsigned FULL = 0xFFFFFFFFu;
@@ -444,7 +444,9 @@ int grid_blocks(K kernel, int sm_count) {
     return nb * sm_count;
 }
 
-template <bool S>
+// Register budget of the search / eval kernels (result-neutral): blocks of
+// 256 threads asked per SM (1 = the compiler's choice).
+template <bool S, int MS, int ME>
 int launch_rounds(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, const Wave& w,
                   int max_len, int w0, int wn, int max_rounds, int growth, int sm_count, int* d_err,
                   unsigned long long* tally, cudaStream_t st) {
@@ -459,8 +461,8 @@ int launch_rounds(const DevIndex& ix, const DevReads& R, const DevParams& P, con
         else if (growth && width < 4096) width *= 2;
     }
     if (max_rounds > 0 && rounds > max_rounds) rounds = max_rounds;
-    static const int g_search = grid_blocks(wf_search_kernel<S>, sm_count);
-    static const int g_eval = grid_blocks(wf_eval_kernel<S>, sm_count);  // EVAL_THREADS = 256
+    static const int g_search = grid_blocks(wf_search_kernel<S, MS>, sm_count);
+    static const int g_eval = grid_blocks(wf_eval_kernel<S, ME>, sm_count);  // EVAL_THREADS = 256
     static const int g_fin = grid_blocks(wf_finalize_kernel<S>, sm_count);
     const unsigned init_blocks = static_cast<unsigned>((R.n_seq + 255) / 256);
     wf_init_kernel<<<init_blocks ? init_blocks : 1, 256, 0, st>>>(w, out, R.lens, R.n_seq);
@@ -473,8 +475,8 @@ int launch_rounds(const DevIndex& ix, const DevReads& R, const DevParams& P, con
             wf_round_begin_kernel<<<1, 1, 0, st>>>(w);
             ++launches;
         }
-        wf_search_kernel<S><<<g_search, 256, 0, st>>>(ix, R, P, w, act, width, tally);
-        wf_eval_kernel<S><<<g_eval, 256, 0, st>>>(ix, R, P, w, tally);
+        wf_search_kernel<S, MS><<<g_search, 256, 0, st>>>(ix, R, P, w, act, width, tally);
+        wf_eval_kernel<S, ME><<<g_eval, 256, 0, st>>>(ix, R, P, w, tally);
         wf_finalize_kernel<S><<<g_fin, 256, 0, st>>>(ix, R, P, out, w, act, nxt, width, k == rounds - 1, d_err,
                                                      tally);
         launches += 3;
@@ -498,10 +500,16 @@ int launch_seed_wavefront(const DevIndex& ix, const DevReads& R, const DevParams
     wave_layout(static_cast<char*>(scratch), R.n_seq, locus_capacity(R.n_seq, t.wave_loci_per_read), &w);
     const int w0 = t.stage1_endpoints > 0 ? t.stage1_endpoints : 1;
     const int wn = t.wave_endpoints > 0 ? t.wave_endpoints : 1;
-    int launches = d_tally ? launch_rounds<true>(ix, R, P, out, w, max_len, w0, wn, t.wave_max_rounds,
-                                                 t.wave_growth, sm_count, d_err, d_tally, st)
-                           : launch_rounds<false>(ix, R, P, out, w, max_len, w0, wn, t.wave_max_rounds,
-                                                  t.wave_growth, sm_count, d_err, nullptr, st);
+    int launches = 0;
+    const int mr = t.wave_max_rounds, gr = t.wave_growth;
+    if (d_tally)
+        launches = launch_rounds<true, 1, 1>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, d_tally, st);
+    else if (t.reg_level == 1)
+        launches = launch_rounds<false, 5, 4>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, nullptr, st);
+    else if (t.reg_level == 2)
+        launches = launch_rounds<false, 6, 5>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, nullptr, st);
+    else
+        launches = launch_rounds<false, 1, 1>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, nullptr, st);
     // reads that overflowed the locus list or outlived the rounds
     launches += launch_stage2_pending(ix, R, P, out, w.best_key, w.memo, w.memo_n, w.resume, w.pending,
                                       w.counters + C_HANDOFF, stage2_blocks, t.reg_level, 32, d_tally, st);

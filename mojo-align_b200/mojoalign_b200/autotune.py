@@ -21,14 +21,14 @@ from .params import FmParams
 DEFAULT_CANDIDATES = [
     (0, 1, 0, 1, 16, 32, 32),
     (1, 1, 0, 2, 1, 1, 32),
-    (1, 1, 0, 1, 1, 1, 32),
-    (2, 1, 0, 1, 1, 1, 16),
-    (2, 1, 0, 1, 1, 1, 32),
-    (2, 1, 0, 2, 1, 1, 16),
+    (2, 1, 0, 0, 1, 1, 8, 4, 0, 1),
     (2, 1, 0, 1, 1, 1, 8, 4, 0, 1),
-    (2, 1, 0, 1, 1, 1, 16, 4, 0, 1),
-    (2, 1, 0, 1, 1, 1, 32, 4, 0, 1),
-    (2, 2, 0, 1, 1, 1, 16, 4, 0, 1),
+    (2, 1, 0, 2, 1, 1, 8, 4, 0, 1),
+    (2, 1, 0, 0, 1, 1, 16, 4, 0, 0),
+    (2, 1, 0, 1, 1, 1, 16, 4, 0, 0),
+    (2, 1, 0, 0, 1, 1, 4, 4, 0, 1),
+    (2, 1, 0, 1, 1, 1, 4, 4, 0, 1),
+    (2, 2, 0, 1, 1, 1, 8, 4, 0, 1),
 ]
 FIELDS = ("seed_kernel", "stage1_endpoints", "stage2_blocks_per_sm", "reg_level", "stage1_max_rows",
           "stage2_first_wave", "wave_endpoints", "wave_loci_per_read", "wave_max_rounds", "wave_growth")
