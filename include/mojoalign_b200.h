@@ -299,6 +299,29 @@ typedef struct ma_tuning {
 int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t);
 int ma_ctx_get_tuning(const ma_ctx* ctx, ma_tuning* t);
 
+/*
+ * Chunking of ma_map_batch's copy / compute pipeline (result-neutral; no
+ * reference counterpart: _fm_fire_batch runs fixed 16384-pair batches two
+ * deep, linear_gpu_fm.mojo:2438-3094).  Chunk k+1 is copied in and chunk k-1
+ * copied out while chunk k computes.
+ *   first_chunk_pairs  pairs of the first chunk (0 = max(65536, n1 / 64))
+ *   growth_percent     each chunk is this much larger than the one before
+ *                      (default 50)
+ *   max_chunk_pairs    chunk size cap (0 = min(655360, max(131072, n1 / 4)))
+ *   compute_streams    1: chunks compute in turn on the context's stream;
+ *                      2 (default): consecutive chunks compute on two
+ *                      streams with their own work buffers, so one chunk's
+ *                      last kernels overlap the next one's first.
+ */
+typedef struct ma_pipeline {
+    uint32_t first_chunk_pairs;
+    uint32_t growth_percent;
+    uint32_t max_chunk_pairs;
+    uint32_t compute_streams;
+} ma_pipeline;
+int ma_ctx_set_pipeline(ma_ctx* ctx, const ma_pipeline* p);
+int ma_ctx_get_pipeline(const ma_ctx* ctx, ma_pipeline* p);
+
 /* ---- served form: a request loop over a resident index ----------------
  *
  * No counterpart in the reference, whose map_fastq_fm_gpu maps one FASTQ

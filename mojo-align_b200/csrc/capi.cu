@@ -81,11 +81,17 @@ struct ma_ctx {
     // two-slot pipeline of ma_map_batch: H2D of chunk k+1 on copy_stream
     // and D2H of chunk k-1 on d2h_stream while chunk k computes on `stream`
     cudaStream_t copy_stream = nullptr, d2h_stream = nullptr;
-    cudaEvent_t h2d_done[2] = {nullptr, nullptr}, slot_free[2] = {nullptr, nullptr};
-    cudaEvent_t comp_done[2] = {nullptr, nullptr};
+    static constexpr int NSLOT = 3;  // chunks whose host copies are in flight
+    cudaEvent_t h2d_done[NSLOT] = {}, slot_free[NSLOT] = {}, comp_done[NSLOT] = {};
     struct Slot {
         DevBuf bases, lens, out[12];
-    } slot[2];
+    } slot[NSLOT];
+    struct Lane {  // a second compute stream with its own work buffers
+        DevBuf packed, seed_scratch;
+        cudaStream_t stream = nullptr;
+    } lane[2];
+    cudaEvent_t err_reset = nullptr;
+    ma_pipeline pipeline{0, 50, 0, 2};
     ma_tuning tuning{1, 1, 0, 1, 2, 32, 32, 4, 0, 0};
     int sm_count = 0;
     DevBuf seed_scratch;
@@ -172,13 +178,17 @@ DevParams to_dev(const ma_params* p) {
     return d;
 }
 
-// Enqueues pack -> seed/extend -> rescue for device-resident inputs.
+// Enqueues pack -> seed/extend -> rescue for device-resident inputs, with
+// `packed` and `seed_scratch` as work buffers (the context's own by
+// default).
 void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const uint32_t* d_lens, uint32_t n1,
                  int paired, uint32_t max_len, int bs_r1, int bs_r2, const ma_params* p, const DevOut& out,
-                 cudaStream_t st, bool reset_err = true) {
+                 cudaStream_t st, bool reset_err = true, DevBuf* packed = nullptr, DevBuf* seed_scratch = nullptr) {
+    if (!packed) packed = &ctx->packed;
+    if (!seed_scratch) seed_scratch = &ctx->seed_scratch;
     const int64_t n_seq = paired ? 2 * static_cast<int64_t>(n1) : n1;
     const int words = static_cast<int>((max_len + 31) / 32);
-    ctx->packed.ensure(static_cast<size_t>(n_seq) * 4 * words * 8);
+    packed->ensure(static_cast<size_t>(n_seq) * 4 * words * 8);
     ctx->err_flag.ensure(sizeof(int));
     if (reset_err) ck(cudaMemsetAsync(ctx->err_flag.p, 0, sizeof(int), st), "memset");
     int launches = 0;
@@ -191,27 +201,27 @@ void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const
     }
     if (timed) ck(cudaEventRecord(ctx->ev[0], st), "event");
     launches += launch_pack(d_bases, d_lens, n_seq, n1, static_cast<int>(max_len), words, bs_r1, bs_r2,
-                            ctx->packed.as<uint64_t>(), ctx->err_flag.as<int>(), st);
+                            packed->as<uint64_t>(), ctx->err_flag.as<int>(), st);
     if (timed) ck(cudaEventRecord(ctx->ev[1], st), "event");
-    DevReads R{ctx->packed.as<uint64_t>(), d_lens, words, n_seq};
+    DevReads R{packed->as<uint64_t>(), d_lens, words, n_seq};
     DevParams P = to_dev(p);
     const int level = ctx->tuning.reg_level;
     if (ctx->tuning.seed_kernel == 0) {
         launches += launch_seed_extend(idx->dix, R, P, out, d_tally, level, st);
     } else if (ctx->tuning.seed_kernel == 2) {
-        ctx->seed_scratch.ensure(wavefront_scratch_bytes(n_seq, ctx->tuning.wave_loci_per_read));
+        seed_scratch->ensure(wavefront_scratch_bytes(n_seq, ctx->tuning.wave_loci_per_read));
         const int bps = ctx->tuning.stage2_blocks_per_sm > 0 ? ctx->tuning.stage2_blocks_per_sm
                                                              : stage2_blocks_per_sm(level, d_tally != nullptr);
         launches += launch_seed_wavefront(idx->dix, R, P, out, static_cast<int>(max_len), ctx->tuning,
-                                          bps * ctx->sm_count, ctx->seed_scratch.p, ctx->sm_count,
+                                          bps * ctx->sm_count, seed_scratch->p, ctx->sm_count,
                                           ctx->err_flag.as<int>(), d_tally, st);
     } else {
-        ctx->seed_scratch.ensure(two_stage_scratch_bytes(n_seq));
+        seed_scratch->ensure(two_stage_scratch_bytes(n_seq));
         const int bps = ctx->tuning.stage2_blocks_per_sm > 0 ? ctx->tuning.stage2_blocks_per_sm
                                                              : stage2_blocks_per_sm(level, d_tally != nullptr);
         launches += launch_seed_two_stage(idx->dix, R, P, out, ctx->tuning.stage1_endpoints,
                                           ctx->tuning.stage1_max_rows, bps * ctx->sm_count, level,
-                                          ctx->tuning.stage2_first_wave, ctx->seed_scratch.p, d_tally,
+                                          ctx->tuning.stage2_first_wave, seed_scratch->p, d_tally,
                                           timed ? ctx->ev[4] : nullptr, st);
     }
     if (timed) ck(cudaEventRecord(ctx->ev[2], st), "event");
@@ -297,7 +307,13 @@ void ma_ctx_destroy(ma_ctx* ctx) {
         sl.lens.release();
         for (DevBuf& b : sl.out) b.release();
     }
-    for (int i = 0; i < 2; ++i) {
+    for (auto& ln : ctx->lane) {
+        ln.packed.release();
+        ln.seed_scratch.release();
+        if (ln.stream) cudaStreamDestroy(ln.stream);
+    }
+    if (ctx->err_reset) cudaEventDestroy(ctx->err_reset);
+    for (int i = 0; i < ma_ctx::NSLOT; ++i) {
         if (ctx->h2d_done[i]) cudaEventDestroy(ctx->h2d_done[i]);
         if (ctx->slot_free[i]) cudaEventDestroy(ctx->slot_free[i]);
         if (ctx->comp_done[i]) cudaEventDestroy(ctx->comp_done[i]);
@@ -453,24 +469,30 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
         if (!ctx->copy_stream) {
             ck(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
             ck(cudaStreamCreateWithFlags(&ctx->d2h_stream, cudaStreamNonBlocking), "cudaStreamCreate");
-            for (int i = 0; i < 2; ++i) {
+            for (int i = 0; i < ma_ctx::NSLOT; ++i) {
                 ck(cudaEventCreateWithFlags(&ctx->h2d_done[i], cudaEventDisableTiming), "cudaEventCreate");
                 ck(cudaEventCreateWithFlags(&ctx->slot_free[i], cudaEventDisableTiming), "cudaEventCreate");
                 ck(cudaEventCreateWithFlags(&ctx->comp_done[i], cudaEventDisableTiming), "cudaEventCreate");
             }
+            for (auto& ln : ctx->lane)
+                ck(cudaStreamCreateWithFlags(&ln.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+            ck(cudaEventCreateWithFlags(&ctx->err_reset, cudaEventDisableTiming), "cudaEventCreate");
         }
         const bool want_dbg = dbg && (dbg->uk || dbg->ul || dbg->us || dbg->e || dbg->score);
         // Pipeline over chunks of pairs (pairs never split: rescue reads both
         // mates).  Chunk k's R1 rows and R2 rows are copied into one slot as
         // a batch of its own while chunk k-1 computes, and chunk k-1's results
         // go back into the caller's arrays (at the pairs' positions) while
-        // chunk k computes: three streams, two slots.  Chunks grow by half
-        // from a small first one (the pipeline fills quickly, while the
-        // large later chunks keep the kernels' per-call overhead small);
-        // copies run faster than the kernels, so each copy still hides
-        // behind the previous chunk's kernels.
-        const uint32_t first = std::min<uint32_t>(n1, std::max<uint32_t>(65536u, n1 / 64));
-        const uint32_t cap = std::max<uint32_t>(first, std::max<uint32_t>(131072u, n1 / 4));
+        // chunk k computes: three slots, three or four streams (ma_pipeline).
+        // Chunks grow from a small first one (the pipeline fills quickly,
+        // while large later chunks keep the kernels' per-call overhead
+        // small).
+        const ma_pipeline& pl = ctx->pipeline;
+        const uint32_t first = std::min<uint32_t>(
+            n1, pl.first_chunk_pairs ? pl.first_chunk_pairs : std::max<uint32_t>(65536u, n1 / 64));
+        const uint32_t cap = std::max<uint32_t>(
+            first, pl.max_chunk_pairs ? pl.max_chunk_pairs : std::min<uint32_t>(655360u, std::max<uint32_t>(131072u, n1 / 4)));
+        const bool two = pl.compute_streams == 2;
         const int mates = paired ? 2 : 1;
         void* host_out[12] = {out->rid, out->pos, out->mapq, out->flag, out->sl, out->sr, out->nm,
                               want_dbg ? dbg->uk : nullptr, want_dbg ? dbg->ul : nullptr,
@@ -487,12 +509,26 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
             sl.lens.ensure(cs * 4);
             for (int f = 0; f < 12; ++f) sl.out[f].ensure(cs * width[f]);
         }
+        // one error word for the call, cleared before any chunk computes
+        ctx->err_flag.ensure(sizeof(int));
+        ck(cudaMemsetAsync(ctx->err_flag.p, 0, sizeof(int), st), "memset");
+        if (two) {
+            ck(cudaEventRecord(ctx->err_reset, st), "cudaEventRecord");
+            for (auto& ln : ctx->lane) ck(cudaStreamWaitEvent(ln.stream, ctx->err_reset, 0), "cudaStreamWaitEvent");
+        }
         uint32_t chunk = first;
-        for (uint32_t a = 0, c = 0; a < n1; a += c, ++k, chunk = std::min<uint32_t>(cap, chunk + chunk / 2)) {
+        auto grow = [&](uint32_t x) {
+            const uint64_t g = static_cast<uint64_t>(x) + static_cast<uint64_t>(x) * pl.growth_percent / 100;
+            return static_cast<uint32_t>(std::min<uint64_t>(cap, std::max<uint64_t>(g, 1)));
+        };
+        for (uint32_t a = 0, c = 0; a < n1; a += c, ++k, chunk = grow(chunk)) {
             c = std::min(chunk, n1 - a);
-            ma_ctx::Slot& sl = ctx->slot[k & 1];
+            const int si = k % ma_ctx::NSLOT;
+            ma_ctx::Slot& sl = ctx->slot[si];
+            ma_ctx::Lane& ln = ctx->lane[k & 1];
+            cudaStream_t cst = two ? ln.stream : st;
             // copy: wait until the slot's previous chunk has been read back
-            ck(cudaStreamWaitEvent(ctx->copy_stream, ctx->slot_free[k & 1], 0), "cudaStreamWaitEvent");
+            ck(cudaStreamWaitEvent(ctx->copy_stream, ctx->slot_free[si], 0), "cudaStreamWaitEvent");
             for (int m = 0; m < mates; ++m) {
                 const size_t row0 = static_cast<size_t>(m) * n1 + a;
                 ck(cudaMemcpyAsync(sl.bases.as<uint8_t>() + static_cast<size_t>(m) * c * max_len,
@@ -501,9 +537,9 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
                 ck(cudaMemcpyAsync(sl.lens.as<uint32_t>() + static_cast<size_t>(m) * c, lens + row0, c * 4,
                                    cudaMemcpyHostToDevice, ctx->copy_stream), "H2D lens");
             }
-            ck(cudaEventRecord(ctx->h2d_done[k & 1], ctx->copy_stream), "cudaEventRecord");
+            ck(cudaEventRecord(ctx->h2d_done[si], ctx->copy_stream), "cudaEventRecord");
             // compute the chunk, then read it back on the compute stream
-            ck(cudaStreamWaitEvent(st, ctx->h2d_done[k & 1], 0), "cudaStreamWaitEvent");
+            ck(cudaStreamWaitEvent(cst, ctx->h2d_done[si], 0), "cudaStreamWaitEvent");
             DevOut o{sl.out[0].as<int32_t>(), sl.out[1].as<uint32_t>(), sl.out[2].as<uint32_t>(),
                      sl.out[3].as<int32_t>(), sl.out[4].as<uint32_t>(), sl.out[5].as<uint32_t>(),
                      sl.out[6].as<uint32_t>(), nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -515,10 +551,10 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
                 o.score = sl.out[11].as<int32_t>();
             }
             enqueue_map(ctx, idx, sl.bases.as<uint8_t>(), sl.lens.as<uint32_t>(), c, paired, max_len, bs_r1, bs_r2,
-                        p, o, st, k == 0);
+                        p, o, cst, false, two ? &ln.packed : nullptr, two ? &ln.seed_scratch : nullptr);
             if (ctx->profiling & 1) {
                 // profiling runs give up the overlap to time every chunk
-                ck(cudaStreamSynchronize(st), "chunk");
+                ck(cudaStreamSynchronize(cst), "chunk");
                 float ms[4] = {0, 0, 0, 0};
                 for (int i = 0; i < 3; ++i) ck(cudaEventElapsedTime(&ms[i], ctx->ev[i], ctx->ev[i + 1]), "elapsed");
                 if (!ctx->rescue_ran) ms[2] = 0;
@@ -526,8 +562,8 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
                 if (ctx->tuning.seed_kernel == 1) ck(cudaEventElapsedTime(&ms[3], ctx->ev[1], ctx->ev[4]), "elapsed");
                 for (int i = 0; i < 4; ++i) acc_ms[i] += ms[i];
             }
-            ck(cudaEventRecord(ctx->comp_done[k & 1], st), "cudaEventRecord");
-            ck(cudaStreamWaitEvent(ctx->d2h_stream, ctx->comp_done[k & 1], 0), "cudaStreamWaitEvent");
+            ck(cudaEventRecord(ctx->comp_done[si], cst), "cudaEventRecord");
+            ck(cudaStreamWaitEvent(ctx->d2h_stream, ctx->comp_done[si], 0), "cudaStreamWaitEvent");
             for (int f = 0; f < 12; ++f) {
                 if (!host_out[f]) continue;
                 for (int m = 0; m < mates; ++m) {
@@ -537,10 +573,10 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
                                        cudaMemcpyDeviceToHost, ctx->d2h_stream), "D2H");
                 }
             }
-            ck(cudaEventRecord(ctx->slot_free[k & 1], ctx->d2h_stream), "cudaEventRecord");
+            ck(cudaEventRecord(ctx->slot_free[si], ctx->d2h_stream), "cudaEventRecord");
         }
         // the error word after the last copies back
-        ck(cudaStreamWaitEvent(st, ctx->slot_free[(k - 1) & 1], 0), "cudaStreamWaitEvent");
+        ck(cudaStreamWaitEvent(st, ctx->slot_free[(k - 1) % ma_ctx::NSLOT], 0), "cudaStreamWaitEvent");
         check_err_flag(ctx, st);
         if (ctx->profiling & 1)
             for (int i = 0; i < 4; ++i) ctx->kernel_ms[i] = acc_ms[i];
@@ -606,6 +642,21 @@ int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t) {
         if (t->wave_growth < 0 || t->wave_growth > 1) fail(MA_ERR_ARG, "wave_growth must be 0 or 1");
         ctx->tuning = *t;
     });
+}
+
+int ma_ctx_set_pipeline(ma_ctx* ctx, const ma_pipeline* p) {
+    if (!ctx || !p) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (p->compute_streams < 1 || p->compute_streams > 2) fail(MA_ERR_ARG, "compute_streams must be 1 or 2");
+        if (p->growth_percent > 1000) fail(MA_ERR_ARG, "growth_percent must be <= 1000");
+        ctx->pipeline = *p;
+    });
+}
+
+int ma_ctx_get_pipeline(const ma_ctx* ctx, ma_pipeline* p) {
+    if (!ctx || !p) return MA_ERR_ARG;
+    *p = ctx->pipeline;
+    return MA_OK;
 }
 
 int ma_ctx_get_tuning(const ma_ctx* ctx, ma_tuning* t) {

@@ -105,6 +105,11 @@ class ma_tuning(C.Structure):
                 ("wave_growth", C.c_int32)]
 
 
+class ma_pipeline(C.Structure):
+    _fields_ = [("first_chunk_pairs", C.c_uint32), ("growth_percent", C.c_uint32), ("max_chunk_pairs", C.c_uint32),
+                ("compute_streams", C.c_uint32)]
+
+
 class ma_read_model(C.Structure):
     _fields_ = [
         ("len_fixed", C.c_uint32),
@@ -164,6 +169,8 @@ SIGNATURES = [
     ("ma_ctx_set_profiling", C.c_int, [C.c_void_p, C.c_int]),
     ("ma_ctx_set_tuning", C.c_int, [C.c_void_p, C.POINTER(ma_tuning)]),
     ("ma_ctx_get_tuning", C.c_int, [C.c_void_p, C.POINTER(ma_tuning)]),
+    ("ma_ctx_set_pipeline", C.c_int, [C.c_void_p, C.POINTER(ma_pipeline)]),
+    ("ma_ctx_get_pipeline", C.c_int, [C.c_void_p, C.POINTER(ma_pipeline)]),
     ("ma_ctx_kernel_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     ("ma_ctx_traffic", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     ("ma_bench_gather", C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_uint64, C.POINTER(C.c_double)]),

@@ -53,6 +53,17 @@ class GpuContext:
                            stage2_first_wave, wave_endpoints, wave_loci_per_read, wave_max_rounds, wave_growth)
         check(lib.ma_ctx_set_tuning(self.handle, C.byref(t)), self.handle)
 
+    def set_pipeline(self, first_chunk_pairs: int = 0, growth_percent: int = 50, max_chunk_pairs: int = 0,
+                     compute_streams: int = 2) -> None:
+        """Chunking of map_batch's copy / compute pipeline (see ma_pipeline)."""
+        p = _lib.ma_pipeline(first_chunk_pairs, growth_percent, max_chunk_pairs, compute_streams)
+        check(lib.ma_ctx_set_pipeline(self.handle, C.byref(p)), self.handle)
+
+    def pipeline(self) -> dict:
+        p = _lib.ma_pipeline()
+        check(lib.ma_ctx_get_pipeline(self.handle, C.byref(p)), self.handle)
+        return {f: getattr(p, f) for f, _ in p._fields_}
+
     def tuning(self) -> dict:
         t = _lib.ma_tuning()
         check(lib.ma_ctx_get_tuning(self.handle, C.byref(t)), self.handle)
