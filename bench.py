@@ -274,7 +274,7 @@ def run_ours(args, rank, world, local):
         from mojoalign_b200.autotune import FIELDS, TuneResult
 
         fixed = [int(x) for x in args.tuning.split(",")]
-        fixed += [1, 1, 0, 1, 2, 32, 32, 4, 0, 0][len(fixed):]
+        fixed += [2, 1, 0, 2, 1, 1, 8, 4, 0, 1][len(fixed):]
         ctx.set_tuning(*fixed)
         tune = TuneResult(dict(zip(FIELDS, fixed)), float("nan"), [])
         ns = 0

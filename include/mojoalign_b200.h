@@ -243,7 +243,7 @@ int ma_last_launch_count(const ma_ctx* ctx);
  * Result-neutral execution choices (every setting gives identical outputs).
  *   seed_kernel           0: one thread per read over all right endpoints
  *                         (the reference's launch shape, L2336-2382);
- *                         1: two stages (default): one thread per read over
+ *                         1: two stages: one thread per read over
  *                         the first stage1_endpoints endpoints, then one
  *                         warp per remaining read in a persistent kernel
  *                         fed by a work queue;
@@ -252,25 +252,25 @@ int ma_last_launch_count(const ma_ctx* ctx);
  *                         candidate locus and shift), stage1_endpoints
  *                         endpoints in the first round and wave_endpoints in
  *                         each later one; reads left over go to the stage-2
- *                         warps.
+ *                         warps (default).
  *   stage1_endpoints      endpoints stage 1 (or the first round) covers
  *                         (default 1).
  *   stage2_blocks_per_sm  persistent blocks per SM for stage 2 (0 = the
  *                         occupancy maximum).
  *   reg_level             register budget of the seed kernels: 0 = the
- *                         compiler's choice, 1 = 80 registers (default),
- *                         2 = 64 registers (stage kernels); for the
- *                         wavefront's search / eval kernels 0 = the
- *                         compiler's choice, 1 = 5 / 4 blocks of 256
- *                         threads per SM, 2 = 6 / 5.
+ *                         compiler's choice, 1 = 80 registers, 2 = 64
+ *                         registers (stage kernels); for the wavefront's
+ *                         search / eval kernels 0 = the compiler's choice,
+ *                         1 = 5 / 4 blocks of 256 threads per SM, 2 = 6 / 5
+ *                         (default 2).
  *   stage1_max_rows       stage 1 hands a read to stage 2 as soon as one of
  *                         its seeds has more SA rows than this (1..16,
- *                         default 2; 16 = never).
+ *                         default 1; 16 = never).
  *   stage2_first_wave     right endpoints stage 2 searches in its first
- *                         group for a read (1..32, default 32); later groups
+ *                         group for a read (1..32, default 1); later groups
  *                         take 32.
  *   wave_endpoints        right endpoints per read in each wavefront round
- *                         after the first (1..256, default 32).
+ *                         after the first (1..256, default 8).
  *   wave_loci_per_read    wavefront locus list capacity per read of the
  *                         batch (1..64, default 4; at least 1024 entries);
  *                         reads whose loci do not fit a round are finished
@@ -281,8 +281,8 @@ int ma_last_launch_count(const ma_ctx* ctx);
  *   wave_growth           1: each wavefront round after the second covers
  *                         twice the endpoints of the one before (fewer,
  *                         fuller rounds for the reads that stay active
- *                         longest); 0: every later round covers
- *                         wave_endpoints (default).
+ *                         longest; default); 0: every later round covers
+ *                         wave_endpoints.
  */
 typedef struct ma_tuning {
     int32_t seed_kernel;

@@ -92,7 +92,7 @@ struct ma_ctx {
     } lane[2];
     cudaEvent_t err_reset = nullptr;
     ma_pipeline pipeline{0, 50, 0, 2};
-    ma_tuning tuning{1, 1, 0, 1, 2, 32, 32, 4, 0, 0};
+    ma_tuning tuning{2, 1, 0, 2, 1, 1, 8, 4, 0, 1};
     int sm_count = 0;
     DevBuf seed_scratch;
     DevBuf bases, lens, packed, err_flag;

@@ -154,7 +154,7 @@ struct HostSlot {
 struct ma_server {
     bool test_mode = false;
     int device = 0, sm_count = 0;
-    ma_tuning tuning{1, 1, 0, 1, 2, 32, 32, 4, 0, 0};
+    ma_tuning tuning{2, 1, 0, 2, 1, 1, 8, 4, 0, 1};
     const DevIndex* dix = nullptr;
     ma_serve_options opt{};
     char* base = nullptr;  // reserved device range (host memory in test mode)

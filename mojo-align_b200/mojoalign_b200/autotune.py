@@ -34,7 +34,7 @@ FIELDS = ("seed_kernel", "stage1_endpoints", "stage2_blocks_per_sm", "reg_level"
           "stage2_first_wave", "wave_endpoints", "wave_loci_per_read", "wave_max_rounds", "wave_growth")
 
 
-DEFAULTS = (1, 1, 0, 1, 2, 32, 32, 4, 0, 0)
+DEFAULTS = (2, 1, 0, 2, 1, 1, 8, 4, 0, 1)
 
 
 @dataclass

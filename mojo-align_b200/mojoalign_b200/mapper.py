@@ -44,10 +44,10 @@ class GpuContext:
     def last_launch_count(self) -> int:
         return lib.ma_last_launch_count(self.handle)
 
-    def set_tuning(self, seed_kernel: int = 1, stage1_endpoints: int = 1, stage2_blocks_per_sm: int = 0,
-                   reg_level: int = 1, stage1_max_rows: int = 2, stage2_first_wave: int = 32,
-                   wave_endpoints: int = 32, wave_loci_per_read: int = 4, wave_max_rounds: int = 0,
-                   wave_growth: int = 0) -> None:
+    def set_tuning(self, seed_kernel: int = 2, stage1_endpoints: int = 1, stage2_blocks_per_sm: int = 0,
+                   reg_level: int = 2, stage1_max_rows: int = 1, stage2_first_wave: int = 1,
+                   wave_endpoints: int = 8, wave_loci_per_read: int = 4, wave_max_rounds: int = 0,
+                   wave_growth: int = 1) -> None:
         """Result-neutral kernel choices (see ma_tuning in the C header)."""
         t = _lib.ma_tuning(seed_kernel, stage1_endpoints, stage2_blocks_per_sm, reg_level, stage1_max_rows,
                            stage2_first_wave, wave_endpoints, wave_loci_per_read, wave_max_rounds, wave_growth)

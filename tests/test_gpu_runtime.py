@@ -29,6 +29,7 @@ def test_repeatable_and_launch_count(small_ref):
     fa, prefix = small_ref
     rb = synth.simulate_reads(fa, synth.ReadModel(), 3000, True, 150, seed=41)
     with GpuContext(0) as ctx, GpuIndex(ctx, prefix, kmer_k=12, kmer3_k=12) as gi:
+        ctx.set_tuning(1, 1, 0, 2, 1, 1)  # the two-stage form
         a = map_batch(ctx, gi, rb.bases, rb.lens, rb.n1, True, 150, "C2T", "G2A", BENCH_PARAMS, debug=True)
         assert ctx.last_launch_count() == 4  # pack, stage 1, stage 2, rescue
         b = map_batch(ctx, gi, rb.bases, rb.lens, rb.n1, True, 150, "C2T", "G2A", BENCH_PARAMS, debug=True)
@@ -37,3 +38,22 @@ def test_repeatable_and_launch_count(small_ref):
         se = map_batch(ctx, gi, rb.bases[: rb.n1], rb.lens[: rb.n1], rb.n1, False, 150, "C2T", "", BENCH_PARAMS)
         assert ctx.last_launch_count() == 3  # no rescue for single-end reads
         assert se.rid.size == rb.n1
+
+
+@pytest.mark.parametrize("pipeline", [(1000, 0, 1000, 1), (1000, 50, 2500, 2), (700, 100, 0, 2), (0, 50, 0, 1)])
+def test_pipeline_chunking_is_result_neutral(small_ref, pipeline):
+    """Chunk sizes, growth and compute lanes of map_batch's copy / compute
+    pipeline change no output (pairs are never split across chunks)."""
+    fa, prefix = small_ref
+    rb = synth.simulate_reads(fa, synth.ReadModel(), 9000, True, 150, seed=43)
+    with GpuContext(0) as ctx, GpuIndex(ctx, prefix, kmer_k=12, kmer3_k=12) as gi:
+        ctx.set_tuning(2, 1, 0, 2, 1, 1, 8, 4, 0, 1)
+        ctx.set_pipeline(9000, 0, 9000, 1)  # one chunk
+        a = map_batch(ctx, gi, rb.bases, rb.lens, rb.n1, True, 150, "C2T", "G2A", BENCH_PARAMS, debug=True)
+        ctx.set_pipeline(*pipeline)
+        for _ in range(2):
+            b = map_batch(ctx, gi, rb.bases, rb.lens, rb.n1, True, 150, "C2T", "G2A", BENCH_PARAMS, debug=True)
+            for f in a.FIELDS + a.DEBUG:
+                assert np.array_equal(getattr(a, f), getattr(b, f)), (pipeline, f)
+        with pytest.raises(MojoAlignError):
+            ctx.set_pipeline(0, 50, 0, 3)
