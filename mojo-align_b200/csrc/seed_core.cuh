@@ -533,6 +533,13 @@ __device__ void eval_locus(const DevIndex& ix, const ReadView& rd, int64_t b0, i
 //          best hit's mismatches lie in the other part and so do at least
 //          two segments.  Either way at most one non-unique segment rules
 //          it out.
+//   b = 2, k = 1 (one mismatch outside the core): a full or clipped
+//          candidate with <= 1 core mismatch matches one of the two
+//          segments exactly; for a deletion candidate, if a part coincides
+//          with the best hit's alignment both mismatches lie in the other
+//          part and so does the segment beyond the core mismatch, otherwise
+//          a segment that does not span the split lies shifted.  Two unique
+//          segments rule out both.
 // N bases mismatch every candidate: b of them in the core rule out both
 // kinds (full: nm >= b; deletion: nm_d >= 1 + b).
 template <bool S>
@@ -558,7 +565,7 @@ __device__ bool better_hit_impossible(const DevIndex& ix, const ReadView& rd, in
         }
     }
     if (n_n >= b) return true;
-    if (k > b || (b == 2 && k < 2)) return false;
+    if (k > b || (b == 2 && k < 1)) return false;
     // segments [c0, p0), (p0, p1), (p1, c1) of the k mismatches
     int non_unique = 0;
     for (int i = 0; i <= k; ++i) {
@@ -570,7 +577,8 @@ __device__ bool better_hit_impossible(const DevIndex& ix, const ReadView& rd, in
         }
         non_unique += !uniq;
     }
-    return b == 1 ? non_unique <= k : non_unique <= 1;
+    if (b == 1) return non_unique <= k;
+    return k == 2 ? non_unique <= 1 : non_unique == 0;
 }
 
 // Whether a best key is a full or clipped compare (not a deletion offset).
