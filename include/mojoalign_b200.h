@@ -307,11 +307,11 @@ int ma_ctx_get_tuning(const ma_ctx* ctx, ma_tuning* t);
  *   first_chunk_pairs  pairs of the first chunk (0 = max(65536, n1 / 64))
  *   growth_percent     each chunk is this much larger than the one before
  *                      (default 50)
- *   max_chunk_pairs    chunk size cap (0 = min(655360, max(131072, n1 / 4)))
+ *   max_chunk_pairs    chunk size cap (0 = min(400000, max(131072, n1 / 4)))
  *   compute_streams    1: chunks compute in turn on the context's stream;
- *                      2 (default): consecutive chunks compute on two
- *                      streams with their own work buffers, so one chunk's
- *                      last kernels overlap the next one's first.
+ *                      2 or 3 (default): consecutive chunks compute on that
+ *                      many streams with their own work buffers, so one
+ *                      chunk's last kernels overlap the next one's first.
  */
 typedef struct ma_pipeline {
     uint32_t first_chunk_pairs;

@@ -89,9 +89,9 @@ struct ma_ctx {
     struct Lane {  // a second compute stream with its own work buffers
         DevBuf packed, seed_scratch;
         cudaStream_t stream = nullptr;
-    } lane[2];
+    } lane[3];
     cudaEvent_t err_reset = nullptr;
-    ma_pipeline pipeline{0, 50, 0, 2};
+    ma_pipeline pipeline{0, 50, 0, 3};
     ma_tuning tuning{2, 1, 0, 2, 1, 1, 8, 4, 0, 1};
     int sm_count = 0;
     DevBuf seed_scratch;
@@ -491,8 +491,9 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
         const uint32_t first = std::min<uint32_t>(
             n1, pl.first_chunk_pairs ? pl.first_chunk_pairs : std::max<uint32_t>(65536u, n1 / 64));
         const uint32_t cap = std::max<uint32_t>(
-            first, pl.max_chunk_pairs ? pl.max_chunk_pairs : std::min<uint32_t>(655360u, std::max<uint32_t>(131072u, n1 / 4)));
-        const bool two = pl.compute_streams == 2;
+            first, pl.max_chunk_pairs ? pl.max_chunk_pairs : std::min<uint32_t>(400000u, std::max<uint32_t>(131072u, n1 / 4)));
+        const int lanes = static_cast<int>(pl.compute_streams);
+        const bool two = lanes > 1;
         const int mates = paired ? 2 : 1;
         void* host_out[12] = {out->rid, out->pos, out->mapq, out->flag, out->sl, out->sr, out->nm,
                               want_dbg ? dbg->uk : nullptr, want_dbg ? dbg->ul : nullptr,
@@ -525,7 +526,7 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
             c = std::min(chunk, n1 - a);
             const int si = k % ma_ctx::NSLOT;
             ma_ctx::Slot& sl = ctx->slot[si];
-            ma_ctx::Lane& ln = ctx->lane[k & 1];
+            ma_ctx::Lane& ln = ctx->lane[k % (lanes > 1 ? lanes : 1)];
             cudaStream_t cst = two ? ln.stream : st;
             // copy: wait until the slot's previous chunk has been read back
             ck(cudaStreamWaitEvent(ctx->copy_stream, ctx->slot_free[si], 0), "cudaStreamWaitEvent");
@@ -647,7 +648,7 @@ int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t) {
 int ma_ctx_set_pipeline(ma_ctx* ctx, const ma_pipeline* p) {
     if (!ctx || !p) return MA_ERR_ARG;
     return guarded(ctx, [&] {
-        if (p->compute_streams < 1 || p->compute_streams > 2) fail(MA_ERR_ARG, "compute_streams must be 1 or 2");
+        if (p->compute_streams < 1 || p->compute_streams > 3) fail(MA_ERR_ARG, "compute_streams must be 1..3");
         if (p->growth_percent > 1000) fail(MA_ERR_ARG, "growth_percent must be <= 1000");
         ctx->pipeline = *p;
     });

@@ -54,7 +54,7 @@ class GpuContext:
         check(lib.ma_ctx_set_tuning(self.handle, C.byref(t)), self.handle)
 
     def set_pipeline(self, first_chunk_pairs: int = 0, growth_percent: int = 50, max_chunk_pairs: int = 0,
-                     compute_streams: int = 2) -> None:
+                     compute_streams: int = 3) -> None:
         """Chunking of map_batch's copy / compute pipeline (see ma_pipeline)."""
         p = _lib.ma_pipeline(first_chunk_pairs, growth_percent, max_chunk_pairs, compute_streams)
         check(lib.ma_ctx_set_pipeline(self.handle, C.byref(p)), self.handle)

@@ -40,7 +40,7 @@ def test_repeatable_and_launch_count(small_ref):
         assert se.rid.size == rb.n1
 
 
-@pytest.mark.parametrize("pipeline", [(1000, 0, 1000, 1), (1000, 50, 2500, 2), (700, 100, 0, 2), (0, 50, 0, 1)])
+@pytest.mark.parametrize("pipeline", [(1000, 0, 1000, 1), (1000, 50, 2500, 2), (700, 100, 0, 3), (0, 50, 0, 1)])
 def test_pipeline_chunking_is_result_neutral(small_ref, pipeline):
     """Chunk sizes, growth and compute lanes of map_batch's copy / compute
     pipeline change no output (pairs are never split across chunks)."""
@@ -56,4 +56,4 @@ def test_pipeline_chunking_is_result_neutral(small_ref, pipeline):
             for f in a.FIELDS + a.DEBUG:
                 assert np.array_equal(getattr(a, f), getattr(b, f)), (pipeline, f)
         with pytest.raises(MojoAlignError):
-            ctx.set_pipeline(0, 50, 0, 3)
+            ctx.set_pipeline(0, 50, 0, 4)
