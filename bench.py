@@ -71,6 +71,8 @@ def parse_args():
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="Poisson phase duration")
     ap.add_argument("--serve-group", type=int, default=262144, help="reads (pairs) per launch group")
     ap.add_argument("--serve-budget-gb", type=int, default=8, help="serving HBM budget")
+    ap.add_argument("--bam-pairs", type=int, default=1_000_000, help="read pairs of the BAM-packing batch "
+                    "(0 = skip that stage)")
     ap.add_argument("--tuning", default="", help="fixed kernel choice 'seed_kernel,stage1_endpoints,"
                     "stage2_blocks_per_sm,reg_level,stage1_max_rows,stage2_first_wave[,wave_endpoints,"
                     "wave_loci_per_read,wave_max_rounds,wave_growth]' instead of the autotuner")
@@ -233,6 +235,144 @@ class ClockSampler:
         busy = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
         return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
+
+
+BAM_RG = b"mojo1"
+BAM_NAME_LEN = 20
+
+
+def bam_batch(rb, res, n1: int, seed: int = 7):
+    """The BAM packer's input for the first n1 pairs of the mapped workload:
+    their mapping outputs and a FASTQ arena of 20-byte names, the original
+    bases and phred+33 qualities 2..41, records of equal size back to back
+    (name, bases, qualities per record, the reference arena's order)."""
+    from mojoalign_b200.bam import HIT_FIELDS, BatchArena
+
+    sel = np.concatenate([np.arange(n1), rb.n1 + np.arange(n1)])
+    n_seq = 2 * n1
+    hits = {k: np.ascontiguousarray(getattr(res, k)[sel]).astype(t, copy=False) for k, t in HIT_FIELDS}
+    rec = BAM_NAME_LEN + 2 * READ_LEN
+    data = np.empty((n_seq, rec), np.uint8)
+    idx = np.arange(n_seq)
+    digits = np.array([(idx % n1) // 10 ** k % 10 for k in range(9, -1, -1)], np.uint8).T + 48
+    data[:, :10] = np.frombuffer(b"B200:7:FC:", np.uint8)
+    data[:, 10:20] = digits
+    data[:, BAM_NAME_LEN:BAM_NAME_LEN + READ_LEN] = rb.bases[sel, :READ_LEN]
+    data[:, BAM_NAME_LEN + READ_LEN:] = np.random.default_rng(seed).integers(35, 75, size=(n_seq, READ_LEN),
+                                                                              dtype=np.uint8)
+    base = idx.astype(np.uint64) * rec
+    arena = BatchArena(data.reshape(-1), base, np.full(n_seq, BAM_NAME_LEN, np.uint32),
+                       base + BAM_NAME_LEN, rb.lens[sel].astype(np.uint32),
+                       base + BAM_NAME_LEN + READ_LEN, rb.lens[sel].astype(np.uint32))
+    return hits, arena
+
+
+def device_copy(a, dev):
+    """numpy -> device tensor holding the same bytes (unsigned integer
+    arrays travel as the signed type of their width)."""
+    import torch
+
+    a = np.ascontiguousarray(a)
+    signed = {np.dtype(np.uint64): np.int64, np.dtype(np.uint32): np.int32}
+    if a.dtype in signed:
+        a = a.view(signed[a.dtype])
+    return torch.from_numpy(a).to(dev)
+
+
+def run_bam_stage(args, ctx, rb, res, local, peaks):
+    """BAM record packing of one mapped batch: device-resident throughput,
+    the host API end to end, the oracle on one core, and byte parity."""
+    import torch
+
+    import oracle
+    from mojoalign_b200.bam import META_FIELDS, BamTile, emit_bam_device, emit_bam_from_batch
+
+    n1 = min(args.bam_pairs, rb.n1)
+    hits, arena = bam_batch(rb, res, n1)
+    n_seq = 2 * n1
+    tids = np.arange(16, dtype=np.int32) // 2  # f<name> / r<name> contigs share a tid
+    # parity at full size and the CPU baseline (one core)
+    t = time.perf_counter()
+    want, want_meta, want_mapped = oracle.emit_bam(hits, vars(arena), n1, True, tids, BAM_RG, meta_cap=n_seq,
+                                                   cap=n_seq * 512)
+    cpu_s = time.perf_counter() - t
+    bam_bytes = len(want)
+    dev = torch.device("cuda", local)
+    d_hits = {k: device_copy(v, dev) for k, v in hits.items()}
+    d_arena = {k: device_copy(getattr(arena, k), dev)
+               for k in ("data", "name_off", "name_len", "orig_off", "orig_len", "qual_off", "qual_len")}
+    d_tids = device_copy(tids, dev)
+    d_rg = device_copy(np.frombuffer(BAM_RG, np.uint8), dev)
+    d_bam = torch.empty(bam_bytes + 16, dtype=torch.uint8, device=dev)
+    d_meta = {k: torch.empty(n_seq, dtype=torch.int64 if t_ == np.uint64 else torch.int32, device=dev)
+              for k, t_ in META_FIELDS}
+    d_status = torch.zeros(3, dtype=torch.int64, device=dev)
+    tile = BamTile(meta_cap=n_seq)
+    torch.cuda.synchronize()
+    stream = torch.cuda.Stream(device=dev)  # a handle of 0 would select the context's own stream
+
+    def step():
+        emit_bam_device(ctx, {k: v.data_ptr() for k, v in d_hits.items()}, n1, True,
+                        {k: v.data_ptr() for k, v in d_arena.items()}, int(arena.data.size), d_tids.data_ptr(),
+                        int(tids.size), d_rg.data_ptr(), len(BAM_RG), d_bam.data_ptr(), bam_bytes,
+                        {k: v.data_ptr() for k, v in d_meta.items()}, tile, d_status.data_ptr(),
+                        stream.cuda_stream)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    launches = ctx.last_launch_count()
+    status = d_status.cpu().numpy()
+    same = d_bam[:bam_bytes].cpu().numpy().tobytes() == want and int(status[1]) == want_mapped
+    for k, t_ in META_FIELDS:
+        same = same and np.array_equal(d_meta[k].cpu().numpy().view(t_), want_meta[k])
+    del d_hits, d_arena, d_bam, d_meta
+    # end to end: pinned host buffers in, records and metadata out
+    pin = {k: torch.from_numpy(v.view(np.int32) if v.dtype == np.uint32 else v).pin_memory().numpy().view(v.dtype)
+           for k, v in hits.items()}
+    pin_arena = type(arena)(*[None if v is None else torch.from_numpy(
+        v.view({8: np.int64, 4: np.int32, 1: np.uint8}[v.itemsize])).pin_memory().numpy().view(v.dtype)
+        for v in (arena.data, arena.name_off, arena.name_len, arena.orig_off, arena.orig_len, arena.qual_off,
+                  arena.qual_len)])
+    out = torch.empty(bam_bytes, dtype=torch.uint8, pin_memory=True).numpy()
+    host_tile = BamTile(meta_cap=n_seq, meta={k: torch.empty(n_seq, dtype=torch.int64 if t_ == np.uint64 else
+                                                             torch.int32, pin_memory=True).numpy().view(t_)
+                                              for k, t_ in META_FIELDS})
+    emit_bam_from_batch(ctx, pin, n1, True, pin_arena, tids, BAM_RG, host_tile, bam_bytes, out=out)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        host_tile.n_reads = 0
+        emit_bam_from_batch(ctx, pin, n1, True, pin_arena, tids, BAM_RG, host_tile, bam_bytes, out=out)
+    e2e_s = (time.perf_counter() - t) / args.steps
+    same = same and out.tobytes() == want
+    in_bytes = int(arena.name_len.sum()) + int(arena.orig_len.sum()) + int(arena.qual_len.sum())
+    alg = n_seq * (28 + 36 + 44) + in_bytes + bam_bytes
+    achieved = alg / (ms / 1000.0) / 1e9
+    return {
+        "metric": "records/s BAM pack", "value": round(n_seq / (ms / 1000.0), 1), "unit": "records/s",
+        "ms_per_batch": round(ms, 3),
+        "config": {"workload": f"BAM records of the first {n1} pairs of the mapped workload (PE 2x{READ_LEN}, "
+                               f"{BAM_NAME_LEN}-byte names, qualities, RG {BAM_RG.decode()})",
+                   "records": n_seq, "bam_bytes": bam_bytes, "mapped_records": want_mapped},
+        "e2e": {"value": round(n_seq / e2e_s, 1), "unit": "records/s",
+                "h2d_bytes_per_step": int(arena.data.size + n_seq * (28 + 36)),
+                "d2h_bytes_per_step": int(bam_bytes + n_seq * 44)},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                     "frac": round(achieved / peaks.get("hbm_gbs"), 4), "traffic": None,
+                     "alg_bytes_per_launch": alg,
+                     "kernel": "bam_layout_kernel + record-size scan + bam_records_kernel (one emit call)"},
+        "gpu_launches": launches * args.steps,
+        "cpu_baseline": {"value": round(n_seq / cpu_s, 1), "unit": "records/s", "cores": 1, "kind": "port",
+                         "sample": f"the whole batch ({n_seq} records), {cpu_s:.2f} s"},
+        "parity": {"records": n_seq, "bytes_and_metadata_identical": bool(same)},
+    }
 
 
 def measured_peaks() -> dict:
@@ -426,6 +566,8 @@ def run_ours(args, rank, world, local):
             g = np.concatenate([g[:n], g[args.pairs:args.pairs + n]])
             bad += int((g != o[f]).sum())
         line["parity_sample"] = {"reads": 2 * n, "mismatched_fields": bad}
+    if rank == 0 and world == 1 and args.bam_pairs > 0:
+        line["stages"] = {"bam_pack": run_bam_stage(args, ctx, rb, res, local, peaks)}
     if rank == 0 and world == 1 and not args.no_forms:
         from mojoalign_b200.autotune import FIELDS as TFIELDS
 

@@ -403,6 +403,97 @@ const char* ma_serve_last_error(const ma_server* s);
 /* Drains, stops the worker threads and frees the reserved memory. */
 void ma_serve_destroy(ma_server* s);
 
+/* ---- BAM records of a mapped batch ---------------------------------- */
+
+/*
+ * The FASTQ arena of a batch (FastqArena, fq2bam-meth/src/linear_fastq.mojo:
+ * 75-95, as fq_export_ptrs L518-544 hands it to the BAM packer): one byte
+ * array and, per record [n_seq] (R1 rows then R2 rows), the byte offset and
+ * length of the read name (the qname span), of the original (unconverted)
+ * bases and of the qualities.  qual_off == NULL: no qualities.
+ */
+typedef struct ma_fastq_arena {
+    const uint8_t* data;
+    uint64_t data_bytes;
+    const uint64_t* name_off;
+    const uint32_t* name_len;
+    const uint64_t* orig_off;
+    const uint32_t* orig_len;
+    const uint64_t* qual_off;
+    const uint32_t* qual_len;
+} ma_fastq_arena;
+
+/*
+ * Sort / duplicate-marking metadata of a tile (h_coord .. h_pair,
+ * linear_gpu_fm.mojo:2133-2139), arrays of meta_cap entries indexed by the
+ * record's position in the tile.
+ *   coord  _coord_key (L389-395): tid << 32 | pos, unplaced records
+ *          0xffffffff << 32 | tile index
+ *   dhi, dlo  duplicate key: _pack_end (L398-405) of the 5' ends, pair-wise
+ *          ordered; unplaced: ~0 and the tile index
+ *   rec    chunk << 32 | byte offset of the record in its chunk
+ *   len    record bytes including the block_size word
+ *   score  mapq << 8 | (255 - clamp(NM)), summed over a pair
+ *   pair   pair id, unique across tiles
+ */
+typedef struct ma_bam_meta {
+    uint64_t* coord;
+    uint64_t* dhi;
+    uint64_t* dlo;
+    uint64_t* rec;
+    uint32_t* len;
+    uint32_t* score;
+    uint32_t* pair;
+} ma_bam_meta;
+
+/* Tile state carried from batch to batch: the n_reads / n_mapped / n_total /
+ * tile_chunks / meta_cap arguments of _emit_bam_from_batch. */
+typedef struct ma_bam_tile {
+    uint64_t n_reads;  /* records already in the tile (in/out)            */
+    uint64_t n_mapped; /* mapped records so far (in/out)                  */
+    uint64_t n_total;  /* records of tiles flushed before this one        */
+    uint64_t meta_cap; /* entries of the metadata arrays                  */
+    uint32_t chunk;    /* index of this batch's BAM chunk in the tile     */
+} ma_bam_tile;
+
+/*
+ * Packs the BAM records of one mapped batch.  Replaces _emit_bam_from_batch
+ * (linear_gpu_fm.mojo:669-984) and _pack_bam_aln (L497-666): single-end
+ * records get flags 1|64, pairs 1|64 and 1|128 with the mate fields, proper
+ * pair flag and TLEN; SEQ is the original bases (reverse-complemented on the
+ * reverse strand), QUAL phred-33 (0xff without qualities of the read's
+ * length), tags RG:Z:<rg> and NM:C.  Records are written to `bam` in R1,R2
+ * order exactly as the reference's serial loop writes them; metadata goes to
+ * entries [n_reads, n_reads + n_seq) and the tile's n_reads / n_mapped
+ * advance.  Host buffers, synchronous.
+ *   hits        the batch's mapping outputs (host arrays [n_seq])
+ *   rid_to_tid  [n_tid] contig index -> SAM tid (_rid_to_tid_table L423-435)
+ *   rg, rg_n    read-group id bytes
+ * Errors (nothing is written, the tile is unchanged):
+ *   MA_ERR_ARG  "FM sort cap exceeded" (n_reads + n_seq > meta_cap),
+ *               "BAM batch buffer overflow" (records exceed bam_cap), or an
+ *               arena span outside the arena.
+ */
+int ma_emit_bam_batch(ma_ctx* ctx, const ma_hits* hits, uint32_t n1, int paired,
+                      const ma_fastq_arena* arena, const int32_t* rid_to_tid, int32_t n_tid,
+                      const uint8_t* rg, uint32_t rg_n, uint8_t* bam, uint64_t bam_cap,
+                      uint64_t* bam_bytes, const ma_bam_meta* meta, ma_bam_tile* tile);
+
+/*
+ * Same on device buffers, asynchronous on `stream` (NULL = the context's
+ * stream); the metadata arrays are the tile's, on the device.  d_status
+ * (device, 3 x u64) receives the batch's record bytes, its mapped records
+ * and the number of records whose arena spans fall outside data_bytes
+ * (written with zero bytes in their place; a caller treats the batch as
+ * failed).  Records and `rec` are written only when d_status[0] <= bam_cap.
+ * The tile is read, not advanced: the caller adds n_seq and d_status[1].
+ */
+int ma_emit_bam_batch_device(ma_ctx* ctx, const ma_hits* d_hits, uint32_t n1, int paired,
+                             const ma_fastq_arena* d_arena, const int32_t* d_rid_to_tid, int32_t n_tid,
+                             const uint8_t* d_rg, uint32_t rg_n, uint8_t* d_bam, uint64_t bam_cap,
+                             const ma_bam_meta* d_meta, const ma_bam_tile* tile, uint64_t* d_status,
+                             void* stream);
+
 /* ---- measurement (no reference counterpart; the reference only prints
  * perf_counter stage timers, linear_gpu_fm.mojo:2270-2273,3317-3340) ---- */
 

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <string>
 
+#include "bam_pack.h"
 #include "ma_device.cuh"
 #include "ma_internal.h"
 
@@ -98,6 +99,9 @@ struct ma_ctx {
     DevBuf bases, lens, packed, err_flag;
     DevBuf o_rid, o_pos, o_mapq, o_flag, o_sl, o_sr, o_nm;
     DevBuf d_uk, d_ul, d_us, d_e, d_score;
+    // BAM packing: inputs of the host-buffer form, records, metadata,
+    // layout scratch and status
+    DevBuf bam_in, bam_arena, bam_out, bam_meta, bam_scratch, bam_status;
 };
 
 struct ma_index {
@@ -322,7 +326,8 @@ void ma_ctx_destroy(ma_ctx* ctx) {
     if (ctx->d2h_stream) cudaStreamDestroy(ctx->d2h_stream);
     for (DevBuf* b : {&ctx->bases, &ctx->lens, &ctx->packed, &ctx->err_flag, &ctx->o_rid, &ctx->o_pos, &ctx->o_mapq,
                       &ctx->o_flag, &ctx->o_sl, &ctx->o_sr, &ctx->o_nm, &ctx->d_uk, &ctx->d_ul, &ctx->d_us,
-                      &ctx->d_e, &ctx->d_score})
+                      &ctx->d_e, &ctx->d_score, &ctx->bam_in, &ctx->bam_arena, &ctx->bam_out, &ctx->bam_meta,
+                      &ctx->bam_scratch, &ctx->bam_status})
         b->release();
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -611,6 +616,203 @@ int ma_map_batch_device(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases
         }
         enqueue_map(ctx, idx, d_bases, d_lens, n1, paired, max_len, bs_r1, bs_r2, p, o, st);
         check_err_flag(ctx, st);
+    });
+}
+
+namespace {
+
+// Checks shared by both BAM entry points; returns the record count.
+uint64_t bam_records_checked(const ma_hits* hits, uint32_t n1, int paired, const ma_fastq_arena* arena,
+                             const int32_t* rid_to_tid, int32_t n_tid, const uint8_t* rg, uint32_t rg_n,
+                             const void* bam, uint64_t bam_cap, const ma_bam_meta* meta, const ma_bam_tile* tile) {
+    if (!hits || !arena || !meta || !tile) fail(MA_ERR_ARG, "null argument");
+    const uint64_t n_rec = paired ? 2ull * n1 : n1;
+    if (n_rec == 0) return 0;
+    if (!hits->rid || !hits->pos || !hits->mapq || !hits->flag || !hits->sl || !hits->sr || !hits->nm)
+        fail(MA_ERR_ARG, "null mapping output");
+    if (!arena->name_off || !arena->name_len || !arena->orig_off || !arena->orig_len ||
+        (arena->qual_off && !arena->qual_len) || (arena->data_bytes && !arena->data))
+        fail(MA_ERR_ARG, "null arena array");
+    if (!meta->coord || !meta->dhi || !meta->dlo || !meta->rec || !meta->len || !meta->score || !meta->pair)
+        fail(MA_ERR_ARG, "null metadata array");
+    if (n_tid < 0 || (n_tid && !rid_to_tid) || (rg_n && !rg) || (bam_cap && !bam))
+        fail(MA_ERR_ARG, "null argument");
+    // _emit_bam_from_batch raises when a record would land at or past
+    // meta_cap (L772-775, L875-878)
+    if (tile->n_reads + n_rec > tile->meta_cap) fail(MA_ERR_ARG, "FM sort cap exceeded");
+    return n_rec;
+}
+
+ma::BamDev bam_view(const ma_hits& h, uint32_t n1, int paired, const ma_fastq_arena& a, const int32_t* rid_to_tid,
+                    int32_t n_tid, const uint8_t* rg, uint32_t rg_n, uint8_t* bam, uint64_t cap, const ma_bam_meta& m,
+                    const ma_bam_tile& t, uint64_t meta_origin, unsigned long long* status) {
+    ma::BamDev b{};
+    b.rid = h.rid;
+    b.pos = h.pos;
+    b.mapq = h.mapq;
+    b.flag = h.flag;
+    b.sl = h.sl;
+    b.sr = h.sr;
+    b.nm = h.nm;
+    b.arena = a.data;
+    b.arena_bytes = a.data_bytes;
+    b.name_off = a.name_off;
+    b.orig_off = a.orig_off;
+    b.qual_off = a.qual_off;
+    b.name_len = a.name_len;
+    b.orig_len = a.orig_len;
+    b.qual_len = a.qual_len;
+    b.rid_to_tid = rid_to_tid;
+    b.n_tid = n_tid;
+    b.rg = rg;
+    b.rg_n = rg_n;
+    b.n1 = n1;
+    b.paired = paired ? 1 : 0;
+    b.n_reads = t.n_reads;
+    b.n_total = t.n_total;
+    b.meta_origin = meta_origin;
+    b.chunk = t.chunk;
+    b.bam = bam;
+    b.cap = cap;
+    b.coord = m.coord;
+    b.dhi = m.dhi;
+    b.dlo = m.dlo;
+    b.rec = m.rec;
+    b.len = m.len;
+    b.score = m.score;
+    b.pair = m.pair;
+    b.status = status;
+    return b;
+}
+
+}  // namespace
+
+int ma_emit_bam_batch(ma_ctx* ctx, const ma_hits* hits, uint32_t n1, int paired, const ma_fastq_arena* arena,
+                      const int32_t* rid_to_tid, int32_t n_tid, const uint8_t* rg, uint32_t rg_n, uint8_t* bam,
+                      uint64_t bam_cap, uint64_t* bam_bytes, const ma_bam_meta* meta, ma_bam_tile* tile) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (!bam_bytes) fail(MA_ERR_ARG, "null argument");
+        *bam_bytes = 0;
+        ctx->last_launches = 0;
+        const uint64_t n_rec =
+            bam_records_checked(hits, n1, paired, arena, rid_to_tid, n_tid, rg, rg_n, bam, bam_cap, meta, tile);
+        if (n_rec == 0) return;
+        const bool quals = arena->qual_off != nullptr;
+        for (uint64_t i = 0; i < n_rec; ++i) {
+            const bool bad = arena->name_off[i] + arena->name_len[i] > arena->data_bytes ||
+                             arena->orig_off[i] + arena->orig_len[i] > arena->data_bytes ||
+                             (quals && arena->qual_off[i] + arena->qual_len[i] > arena->data_bytes);
+            if (bad) fail(MA_ERR_ARG, "arena span of record " + std::to_string(i) + " lies outside the arena");
+        }
+        use_device(ctx);
+        cudaStream_t st = ctx->stream;
+        // inputs: 7 hit arrays, 3 offset and 3 length arrays, the tid table
+        // and the RG id, packed into one buffer at 256-byte boundaries
+        auto al = [](uint64_t n) { return (n + 255) & ~uint64_t(255); };
+        const uint64_t hb = al(n_rec * 4), ob = al(n_rec * 8);
+        const uint64_t in_bytes = 7 * hb + 3 * ob + (quals ? 3 : 2) * hb + al(uint64_t(n_tid) * 4) + al(rg_n);
+        ctx->bam_in.ensure(in_bytes);
+        ctx->bam_arena.ensure(arena->data_bytes);
+        uint8_t* d = ctx->bam_in.as<uint8_t>();
+        auto put = [&](const void* src, uint64_t bytes, uint64_t slot) -> void* {
+            void* dst = d;
+            if (bytes) ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st), "H2D bam input");
+            d += slot;
+            return dst;
+        };
+        ma_hits dh;
+        dh.rid = static_cast<int32_t*>(put(hits->rid, n_rec * 4, hb));
+        dh.pos = static_cast<uint32_t*>(put(hits->pos, n_rec * 4, hb));
+        dh.mapq = static_cast<uint32_t*>(put(hits->mapq, n_rec * 4, hb));
+        dh.flag = static_cast<int32_t*>(put(hits->flag, n_rec * 4, hb));
+        dh.sl = static_cast<uint32_t*>(put(hits->sl, n_rec * 4, hb));
+        dh.sr = static_cast<uint32_t*>(put(hits->sr, n_rec * 4, hb));
+        dh.nm = static_cast<uint32_t*>(put(hits->nm, n_rec * 4, hb));
+        ma_fastq_arena da{};
+        da.data = ctx->bam_arena.as<uint8_t>();
+        da.data_bytes = arena->data_bytes;
+        if (arena->data_bytes)
+            ck(cudaMemcpyAsync(ctx->bam_arena.p, arena->data, arena->data_bytes, cudaMemcpyHostToDevice, st),
+               "H2D arena");
+        da.name_off = static_cast<const uint64_t*>(put(arena->name_off, n_rec * 8, ob));
+        da.orig_off = static_cast<const uint64_t*>(put(arena->orig_off, n_rec * 8, ob));
+        da.name_len = static_cast<const uint32_t*>(put(arena->name_len, n_rec * 4, hb));
+        da.orig_len = static_cast<const uint32_t*>(put(arena->orig_len, n_rec * 4, hb));
+        if (quals) {
+            da.qual_off = static_cast<const uint64_t*>(put(arena->qual_off, n_rec * 8, ob));
+            da.qual_len = static_cast<const uint32_t*>(put(arena->qual_len, n_rec * 4, hb));
+        }
+        const int32_t* d_tids = static_cast<const int32_t*>(put(rid_to_tid, uint64_t(n_tid) * 4, al(uint64_t(n_tid) * 4)));
+        const uint8_t* d_rg = static_cast<const uint8_t*>(put(rg, rg_n, al(rg_n)));
+        // batch-local metadata, copied into the tile arrays at n_reads
+        const uint64_t mb8 = al(n_rec * 8), mb4 = al(n_rec * 4);
+        ctx->bam_meta.ensure(4 * mb8 + 3 * mb4);
+        uint8_t* m = ctx->bam_meta.as<uint8_t>();
+        ma_bam_meta dm{reinterpret_cast<uint64_t*>(m), reinterpret_cast<uint64_t*>(m + mb8),
+                       reinterpret_cast<uint64_t*>(m + 2 * mb8), reinterpret_cast<uint64_t*>(m + 3 * mb8),
+                       reinterpret_cast<uint32_t*>(m + 4 * mb8), reinterpret_cast<uint32_t*>(m + 4 * mb8 + mb4),
+                       reinterpret_cast<uint32_t*>(m + 4 * mb8 + 2 * mb4)};
+        ctx->bam_status.ensure(4 * sizeof(unsigned long long));
+        unsigned long long* d_status = ctx->bam_status.as<unsigned long long>();
+        ck(cudaMemsetAsync(d_status, 0, 3 * sizeof(unsigned long long), st), "memset");
+        const size_t scratch = bam_scratch_bytes(n_rec);
+        ctx->bam_scratch.ensure(scratch);
+        ma::BamDev b = bam_view(dh, n1, paired, da, d_tids, n_tid, d_rg, rg_n, nullptr, 0, dm, *tile, tile->n_reads,
+                                d_status);
+        int launches = enqueue_bam_layout(b, ctx->bam_scratch.p, scratch, st);
+        uint64_t total = 0;
+        ck(cudaMemcpyAsync(&total, bam_total_in_scratch(ctx->bam_scratch.p, n_rec), 8, cudaMemcpyDeviceToHost, st),
+           "D2H bam size");
+        ck(cudaStreamSynchronize(st), "bam layout");
+        if (total > bam_cap) fail(MA_ERR_ARG, "BAM batch buffer overflow");
+        ctx->bam_out.ensure(total);
+        b.bam = ctx->bam_out.as<uint8_t>();
+        b.cap = total;
+        launches += enqueue_bam_records(b, ctx->bam_scratch.p, ctx->sm_count, st);
+        unsigned long long status[3] = {0, 0, 0};
+        ck(cudaMemcpyAsync(status, d_status, sizeof(status), cudaMemcpyDeviceToHost, st), "D2H bam status");
+        ck(cudaMemcpyAsync(bam, b.bam, total, cudaMemcpyDeviceToHost, st), "D2H bam records");
+        const uint64_t t0 = tile->n_reads;
+        ck(cudaMemcpyAsync(meta->coord + t0, dm.coord, n_rec * 8, cudaMemcpyDeviceToHost, st), "D2H meta");
+        ck(cudaMemcpyAsync(meta->dhi + t0, dm.dhi, n_rec * 8, cudaMemcpyDeviceToHost, st), "D2H meta");
+        ck(cudaMemcpyAsync(meta->dlo + t0, dm.dlo, n_rec * 8, cudaMemcpyDeviceToHost, st), "D2H meta");
+        ck(cudaMemcpyAsync(meta->rec + t0, dm.rec, n_rec * 8, cudaMemcpyDeviceToHost, st), "D2H meta");
+        ck(cudaMemcpyAsync(meta->len + t0, dm.len, n_rec * 4, cudaMemcpyDeviceToHost, st), "D2H meta");
+        ck(cudaMemcpyAsync(meta->score + t0, dm.score, n_rec * 4, cudaMemcpyDeviceToHost, st), "D2H meta");
+        ck(cudaMemcpyAsync(meta->pair + t0, dm.pair, n_rec * 4, cudaMemcpyDeviceToHost, st), "D2H meta");
+        ck(cudaStreamSynchronize(st), "bam records");
+        if (status[0] != total || status[2] != 0) fail(MA_ERR_INTERNAL, "BAM record pass disagrees with its layout");
+        ctx->last_launches = launches;
+        *bam_bytes = total;
+        tile->n_reads += n_rec;
+        tile->n_mapped += status[1];
+    });
+}
+
+int ma_emit_bam_batch_device(ma_ctx* ctx, const ma_hits* d_hits, uint32_t n1, int paired,
+                             const ma_fastq_arena* d_arena, const int32_t* d_rid_to_tid, int32_t n_tid,
+                             const uint8_t* d_rg, uint32_t rg_n, uint8_t* d_bam, uint64_t bam_cap,
+                             const ma_bam_meta* d_meta, const ma_bam_tile* tile, uint64_t* d_status, void* stream) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->last_launches = 0;
+        if (!d_status) fail(MA_ERR_ARG, "null argument");
+        const uint64_t n_rec = bam_records_checked(d_hits, n1, paired, d_arena, d_rid_to_tid, n_tid, d_rg, rg_n,
+                                                   d_bam, bam_cap, d_meta, tile);
+        use_device(ctx);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+        unsigned long long* status = reinterpret_cast<unsigned long long*>(d_status);
+        ck(cudaMemsetAsync(status, 0, 3 * sizeof(unsigned long long), st), "memset");
+        if (n_rec == 0) return;
+        const size_t scratch = bam_scratch_bytes(n_rec);
+        ctx->bam_scratch.ensure(scratch);
+        ma::BamDev b = bam_view(*d_hits, n1, paired, *d_arena, d_rid_to_tid, n_tid, d_rg, rg_n, d_bam, bam_cap,
+                                *d_meta, *tile, 0, status);
+        int launches = enqueue_bam_layout(b, ctx->bam_scratch.p, scratch, st);
+        launches += enqueue_bam_records(b, ctx->bam_scratch.p, ctx->sm_count, st);
+        ck(cudaGetLastError(), "bam kernels");
+        ctx->last_launches = launches;
     });
 }
 

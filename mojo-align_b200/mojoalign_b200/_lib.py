@@ -141,6 +141,21 @@ class ma_serve_stats(C.Structure):
 
 MA_SERVE_SCHEDULER_TEST = 1
 
+
+class ma_fastq_arena(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("data_bytes", C.c_uint64), ("name_off", C.c_void_p), ("name_len", C.c_void_p),
+                ("orig_off", C.c_void_p), ("orig_len", C.c_void_p), ("qual_off", C.c_void_p),
+                ("qual_len", C.c_void_p)]
+
+
+class ma_bam_meta(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("coord", "dhi", "dlo", "rec", "len", "score", "pair")]
+
+
+class ma_bam_tile(C.Structure):
+    _fields_ = [("n_reads", C.c_uint64), ("n_mapped", C.c_uint64), ("n_total", C.c_uint64), ("meta_cap", C.c_uint64),
+                ("chunk", C.c_uint32)]
+
 # (name, restype, argtypes) of every exported entry point of the header.
 SIGNATURES = [
     ("ma_params_default", None, [C.POINTER(ma_params)]),
@@ -187,6 +202,14 @@ SIGNATURES = [
      [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
     ("ma_serve_last_error", C.c_char_p, [C.c_void_p]),
     ("ma_serve_destroy", None, [C.c_void_p]),
+    ("ma_emit_bam_batch", C.c_int,
+     [C.c_void_p, C.POINTER(ma_hits), C.c_uint32, C.c_int, C.POINTER(ma_fastq_arena), C.c_void_p, C.c_int32,
+      C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(ma_bam_meta),
+      C.POINTER(ma_bam_tile)]),
+    ("ma_emit_bam_batch_device", C.c_int,
+     [C.c_void_p, C.POINTER(ma_hits), C.c_uint32, C.c_int, C.POINTER(ma_fastq_arena), C.c_void_p, C.c_int32,
+      C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.POINTER(ma_bam_meta), C.POINTER(ma_bam_tile),
+      C.c_void_p, C.c_void_p]),
     ("ma_synth_reference", C.c_int, [C.c_char_p, C.c_uint64, C.c_int, C.c_double, C.c_double, C.c_uint64]),
     ("ma_synth_reads", C.c_int,
      [C.c_char_p, C.POINTER(ma_read_model), C.c_uint32, C.c_int, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p,

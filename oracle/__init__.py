@@ -19,8 +19,8 @@ LIB = HERE / "liboracle_fm.so"
 
 
 def build() -> Path:
-    src = HERE / "oracle_fm.c"
-    if not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
+    newest = max((HERE / f).stat().st_mtime for f in ("oracle_fm.c", "oracle_bam.c", "Makefile"))
+    if not LIB.exists() or LIB.stat().st_mtime < newest:
         subprocess.run(["make", "-s", "-C", str(HERE), "liboracle_fm.so"], check=True)
     return LIB
 
@@ -31,6 +31,22 @@ class Counters(C.Structure):
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class BamIn(C.Structure):
+    _fields_ = [("n1", C.c_uint32), ("paired", C.c_int32)] + \
+        [(n, C.c_void_p) for n in ("rid", "pos", "mapq", "flag", "sl", "sr", "nm", "arena", "name_off", "orig_off",
+                                   "qual_off", "name_len", "orig_len", "qual_len", "rid_to_tid")] + \
+        [("n_tid_map", C.c_int32), ("rg", C.c_void_p), ("rg_n", C.c_uint32), ("n_reads", C.c_uint64),
+         ("n_total", C.c_uint64), ("meta_cap", C.c_uint64), ("chunk", C.c_uint32)]
+
+
+BAM_META_FIELDS = (("coord", np.uint64), ("dhi", np.uint64), ("dlo", np.uint64), ("rec", np.uint64),
+                   ("len", np.uint32), ("score", np.uint32), ("pair", np.uint32))
+
+
+class BamMeta(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n, _ in BAM_META_FIELDS]
 
 
 def _load():
@@ -61,6 +77,11 @@ def _load():
                             vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, C.POINTER(Counters), C.c_int]
     lib.orc_map.restype = C.c_int
     lib.orc_max_threads.restype = C.c_int
+    lib.orc_emit_bam.argtypes = [C.POINTER(BamIn), vp, C.c_uint64, C.POINTER(BamMeta), C.POINTER(C.c_uint64)]
+    lib.orc_emit_bam.restype = C.c_int64
+    lib.orc_pack_aln.argtypes = [vp, C.c_uint64, C.c_char_p] + [C.c_int64] * 7 + [C.c_char_p, C.c_int64, C.c_char_p] + \
+        [C.c_int64] * 5 + [C.c_char_p, C.c_int64]
+    lib.orc_pack_aln.restype = C.c_int64
     return lib
 
 
@@ -148,6 +169,64 @@ class OracleIndex:
         if counters:
             out["counters"] = ct.as_dict()
         return out
+
+
+HIT_FIELDS = (("rid", np.int32), ("pos", np.uint32), ("mapq", np.uint32), ("flag", np.int32),
+              ("sl", np.uint32), ("sr", np.uint32), ("nm", np.uint32))
+
+
+def emit_bam(hits, arena, n1: int, paired: bool, rid_to_tid, rg: bytes, *, n_reads: int = 0,
+             n_total: int = 0, meta_cap: int | None = None, chunk: int = 0, cap: int | None = None):
+    """orc_emit_bam: _emit_bam_from_batch (linear_gpu_fm.mojo:669-984) on one batch.
+
+    hits: mapping outputs by field name, [n_seq] (R1 rows then R2 rows).
+    arena: dict with "data" (uint8) and "name_off"/"orig_off"/"qual_off"
+    (uint64, qual_off may be None) and "name_len"/"orig_len"/"qual_len"
+    (uint32), [n_seq].  Returns (bam bytes, metadata arrays of the batch's
+    records, mapped count); raises on overflow like the reference.
+    """
+    n_seq = n1 * (2 if paired else 1)
+    h = {k: np.ascontiguousarray(hits[k], dtype=t) for k, t in HIT_FIELDS}
+    data = np.ascontiguousarray(arena["data"], dtype=np.uint8)
+    offs = {k: (None if arena.get(k) is None else np.ascontiguousarray(arena[k], dtype=np.uint64))
+            for k in ("name_off", "orig_off", "qual_off")}
+    lens = {k: (None if arena.get(k) is None else np.ascontiguousarray(arena[k], dtype=np.uint32))
+            for k in ("name_len", "orig_len", "qual_len")}
+    tids = np.ascontiguousarray(rid_to_tid, dtype=np.int32)
+    rgb = np.frombuffer(bytes(rg) + b"\0", dtype=np.uint8)
+    if meta_cap is None:
+        meta_cap = n_reads + n_seq + 1
+    if cap is None:
+        cap = sum(int(x) for x in (n_seq * 64, lens["name_len"].sum(dtype=np.uint64),
+                                   2 * lens["orig_len"].sum(dtype=np.uint64), n_seq * len(rg)))
+    bam = np.zeros(max(cap, 1), np.uint8)
+    meta = {k: np.zeros(meta_cap, t) for k, t in BAM_META_FIELDS}
+    bi = BamIn(n1=n1, paired=int(paired), **{k: _p(v) for k, v in h.items()}, arena=_p(data),
+               **{k: _p(v) for k, v in offs.items()}, **{k: _p(v) for k, v in lens.items()},
+               rid_to_tid=_p(tids), n_tid_map=len(tids), rg=_p(rgb), rg_n=len(rg), n_reads=n_reads,
+               n_total=n_total, meta_cap=meta_cap, chunk=chunk)
+    bm = BamMeta(**{k: _p(v) for k, v in meta.items()})
+    mapped = C.c_uint64(0)
+    n = lib.orc_emit_bam(C.byref(bi), _p(bam), cap, C.byref(bm), C.byref(mapped))
+    if n == -1:
+        raise RuntimeError("BAM batch buffer overflow")
+    if n == -2:
+        raise RuntimeError("FM sort cap exceeded")
+    return bam[:n].tobytes(), {k: v[n_reads:n_reads + n_seq].copy() for k, v in meta.items()}, mapped.value
+
+
+def pack_aln(name: bytes, flag: int, tid: int, pos0: int, mapq: int, sl: int, sr: int, seq: bytes, qual,
+             ntid: int, npos: int, tlen: int, nm: int, rg: bytes) -> bytes:
+    """orc_pack_aln: one record of _pack_bam_aln (linear_gpu_fm.mojo:497-666).
+    qual None = no qualities; sl/sr are in read orientation (swapped on the
+    reverse strand inside)."""
+    cap = 64 + len(name) + 2 * len(seq) + len(rg) + 16
+    buf = np.zeros(cap, np.uint8)
+    n = lib.orc_pack_aln(_p(buf), cap, name, len(name), flag, tid, pos0, mapq, sl, sr, seq, len(seq),
+                         qual, len(qual) if qual is not None else 0, ntid, npos, tlen, nm, rg, len(rg))
+    if n < 0:
+        raise RuntimeError("BAM batch buffer overflow")
+    return buf[:n].tobytes()
 
 
 def pack_bases(ascii_bytes) -> np.ndarray:

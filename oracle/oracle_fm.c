@@ -30,6 +30,7 @@
  * and pack vectors, convert_fastq vectors, the FM round-trip property and
  * the toy fixture; see tests/), not against reference outputs.
  */
+#define _POSIX_C_SOURCE 200809L /* strdup */
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
