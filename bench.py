@@ -73,6 +73,8 @@ def parse_args():
     ap.add_argument("--serve-budget-gb", type=int, default=8, help="serving HBM budget")
     ap.add_argument("--bam-pairs", type=int, default=1_000_000, help="read pairs of the BAM-packing batch "
                     "(0 = skip that stage)")
+    ap.add_argument("--sort-batches", type=int, default=4, help="BAM batches (of --bam-pairs pairs) in the "
+                    "tile of the sort / duplicate-marking / gather stage (0 = skip)")
     ap.add_argument("--tuning", default="", help="fixed kernel choice 'seed_kernel,stage1_endpoints,"
                     "stage2_blocks_per_sm,reg_level,stage1_max_rows,stage2_first_wave[,wave_endpoints,"
                     "wave_loci_per_read,wave_max_rounds,wave_growth]' instead of the autotuner")
@@ -241,25 +243,26 @@ BAM_RG = b"mojo1"
 BAM_NAME_LEN = 20
 
 
-def bam_batch(rb, res, n1: int, seed: int = 7):
-    """The BAM packer's input for the first n1 pairs of the mapped workload:
-    their mapping outputs and a FASTQ arena of 20-byte names, the original
-    bases and phred+33 qualities 2..41, records of equal size back to back
-    (name, bases, qualities per record, the reference arena's order)."""
+def bam_batch(rb, res, n1: int, first: int = 0, seed: int = 7):
+    """The BAM packer's input for pairs [first, first + n1) of the mapped
+    workload: their mapping outputs and a FASTQ arena of 20-byte names, the
+    original bases and phred+33 qualities 2..41, records of equal size back
+    to back (name, bases, qualities per record, the reference arena's
+    order)."""
     from mojoalign_b200.bam import HIT_FIELDS, BatchArena
 
-    sel = np.concatenate([np.arange(n1), rb.n1 + np.arange(n1)])
+    sel = np.concatenate([first + np.arange(n1), rb.n1 + first + np.arange(n1)])
     n_seq = 2 * n1
     hits = {k: np.ascontiguousarray(getattr(res, k)[sel]).astype(t, copy=False) for k, t in HIT_FIELDS}
     rec = BAM_NAME_LEN + 2 * READ_LEN
     data = np.empty((n_seq, rec), np.uint8)
     idx = np.arange(n_seq)
-    digits = np.array([(idx % n1) // 10 ** k % 10 for k in range(9, -1, -1)], np.uint8).T + 48
+    digits = np.array([(first + idx % n1) // 10 ** k % 10 for k in range(9, -1, -1)], np.uint8).T + 48
     data[:, :10] = np.frombuffer(b"B200:7:FC:", np.uint8)
     data[:, 10:20] = digits
     data[:, BAM_NAME_LEN:BAM_NAME_LEN + READ_LEN] = rb.bases[sel, :READ_LEN]
-    data[:, BAM_NAME_LEN + READ_LEN:] = np.random.default_rng(seed).integers(35, 75, size=(n_seq, READ_LEN),
-                                                                              dtype=np.uint8)
+    data[:, BAM_NAME_LEN + READ_LEN:] = np.random.default_rng(seed + first).integers(35, 75, size=(n_seq, READ_LEN),
+                                                                                      dtype=np.uint8)
     base = idx.astype(np.uint64) * rec
     arena = BatchArena(data.reshape(-1), base, np.full(n_seq, BAM_NAME_LEN, np.uint32),
                        base + BAM_NAME_LEN, rb.lens[sel].astype(np.uint32),
@@ -276,6 +279,8 @@ def device_copy(a, dev):
     signed = {np.dtype(np.uint64): np.int64, np.dtype(np.uint32): np.int32}
     if a.dtype in signed:
         a = a.view(signed[a.dtype])
+    if not a.flags.writeable:
+        a = a.copy()
     return torch.from_numpy(a).to(dev)
 
 
@@ -372,6 +377,148 @@ def run_bam_stage(args, ctx, rb, res, local, peaks):
         "cpu_baseline": {"value": round(n_seq / cpu_s, 1), "unit": "records/s", "cores": 1, "kind": "port",
                          "sample": f"the whole batch ({n_seq} records), {cpu_s:.2f} s"},
         "parity": {"records": n_seq, "bytes_and_metadata_identical": bool(same)},
+    }
+
+
+def run_sort_stage(args, ctx, rb, res, local, peaks):
+    """Coordinate sort + duplicate marking + sorted gather of one BAM tile
+    made of --sort-batches emitted batches: device-resident throughput, the
+    host API end to end, the oracle on one core, and parity."""
+    import torch
+
+    import oracle
+    from mojoalign_b200 import _lib
+    from mojoalign_b200.bam import META_FIELDS, BamTile, emit_bam_device
+
+    bp = min(args.bam_pairs, rb.n1 // max(1, args.sort_batches))
+    nb = args.sort_batches
+    n = 2 * bp * nb
+    dev = torch.device("cuda", local)
+    tids = np.arange(16, dtype=np.int32) // 2
+    d_tids = device_copy(tids, dev)
+    d_rg = device_copy(np.frombuffer(BAM_RG, np.uint8), dev)
+    d_meta = {k: torch.empty(n, dtype=torch.int64 if t_ == np.uint64 else torch.int32, device=dev)
+              for k, t_ in META_FIELDS}
+    d_status = torch.zeros(3, dtype=torch.int64, device=dev)
+    tile = BamTile(meta_cap=n, meta={"unused": None})
+    chunks, chunk_len = [], []
+    rec_cap = 4 + 32 + BAM_NAME_LEN + 1 + 12 + (READ_LEN + 1) // 2 + READ_LEN + 8 + len(BAM_RG)
+    for c in range(nb):
+        hits, arena = bam_batch(rb, res, bp, first=c * bp)
+        d_hits = {k: device_copy(v, dev) for k, v in hits.items()}
+        d_arena = {k: device_copy(getattr(arena, k), dev)
+                   for k in ("data", "name_off", "name_len", "orig_off", "orig_len", "qual_off", "qual_len")}
+        d_chunk = torch.empty(2 * bp * rec_cap, dtype=torch.uint8, device=dev)
+        tile.n_reads, tile.chunk = 2 * bp * c, c
+        torch.cuda.synchronize()
+        emit_bam_device(ctx, {k: v.data_ptr() for k, v in d_hits.items()}, bp, True,
+                        {k: v.data_ptr() for k, v in d_arena.items()}, int(arena.data.size), d_tids.data_ptr(),
+                        int(tids.size), d_rg.data_ptr(), len(BAM_RG), d_chunk.data_ptr(), d_chunk.numel(),
+                        {k: v.data_ptr() for k, v in d_meta.items()}, tile, d_status.data_ptr())
+        torch.cuda.synchronize()
+        st = d_status.cpu().numpy()
+        assert st[0] <= d_chunk.numel() and st[2] == 0
+        chunks.append(d_chunk)
+        chunk_len.append(int(st[0]))
+        del d_hits, d_arena
+    meta = {k: d_meta[k].cpu().numpy().view(t_) for k, t_ in META_FIELDS}
+    d_chunk_ptrs = device_copy(np.array([c.data_ptr() for c in chunks], np.uint64), dev)
+    d_chunk_len = device_copy(np.array(chunk_len, np.uint64), dev)
+    total = int(sum(chunk_len))
+    d_out = {k: torch.empty(n, dtype=torch.int32, device=dev) for k in ("is_dup", "perm")}
+    d_marked = torch.zeros(1, dtype=torch.int64, device=dev)
+    d_sorted = torch.empty(total, dtype=torch.uint8, device=dev)
+    d_gstat = torch.zeros(2, dtype=torch.int64, device=dev)
+    torch.cuda.synchronize()
+    stream = torch.cuda.Stream(device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+
+    def step(timed=False):
+        if timed:
+            ev[0].record(stream)
+        _lib.check(_lib.lib.ma_sort_markdup_device(
+            ctx.handle, n, d_meta["coord"].data_ptr(), d_meta["dhi"].data_ptr(), d_meta["dlo"].data_ptr(),
+            d_meta["score"].data_ptr(), d_meta["pair"].data_ptr(), d_out["is_dup"].data_ptr(),
+            d_out["perm"].data_ptr(), 1, None, d_marked.data_ptr(), stream.cuda_stream), ctx.handle)
+        sort_launches = ctx.last_launch_count()
+        if timed:
+            ev[1].record(stream)
+        _lib.check(_lib.lib.ma_gather_sorted_bam_device(
+            ctx.handle, n, d_out["perm"].data_ptr(), d_meta["rec"].data_ptr(), d_meta["len"].data_ptr(),
+            d_out["is_dup"].data_ptr(), 1, d_chunk_ptrs.data_ptr(), d_chunk_len.data_ptr(), nb,
+            d_sorted.data_ptr(), total, d_gstat.data_ptr(), stream.cuda_stream), ctx.handle)
+        if timed:
+            ev[2].record(stream)
+        return sort_launches + ctx.last_launch_count()
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    sort_ms, gather_ms = [], []
+    launches = 0
+    for _ in range(args.steps):
+        launches += step(timed=True)
+        stream.synchronize()
+        sort_ms.append(ev[0].elapsed_time(ev[1]))
+        gather_ms.append(ev[1].elapsed_time(ev[2]))
+    g_is_dup = d_out["is_dup"].cpu().numpy().view(np.uint32)
+    g_perm = d_out["perm"].cpu().numpy().view(np.uint32)
+    g_sorted = d_sorted.cpu().numpy()
+    gst = d_gstat.cpu().numpy()
+    host_chunks = [c[:l].cpu().numpy() for c, l in zip(chunks, chunk_len)]
+    del chunks, d_sorted
+    # the oracle (one core) on the same tile: CPU baseline and parity
+    t = time.perf_counter()
+    w_dup, w_perm, _, w_marked = oracle.sort_markdup(meta["coord"], meta["dhi"], meta["dlo"], meta["score"],
+                                                     meta["pair"], dup_perm=False)
+    w_sorted = oracle.gather_sorted(host_chunks, w_perm, meta["rec"], meta["len"], w_dup)
+    cpu_s = time.perf_counter() - t
+    same = (np.array_equal(g_perm, w_perm) and np.array_equal(g_is_dup, w_dup) and int(gst[0]) == total
+            and g_sorted.tobytes() == w_sorted and int(d_marked.item()) == w_marked)
+    del w_sorted
+    # end to end through the host API: pinned metadata and chunks in, perm /
+    # flags / sorted stream out
+    from mojoalign_b200.bam import gather_sorted, sort_markdup
+
+    pin_meta = {k: torch.from_numpy(v.view(np.int64 if v.dtype == np.uint64 else np.int32)).pin_memory().numpy()
+                .view(v.dtype) for k, v in meta.items()}
+    pin_chunks = [torch.from_numpy(c).pin_memory().numpy() for c in host_chunks]
+    host_tile = BamTile(meta_cap=n, n_reads=n, meta=pin_meta)
+    pin_out = torch.empty(total, dtype=torch.uint8, pin_memory=True).numpy()
+    res_ = sort_markdup(ctx, host_tile)
+    gather_sorted(ctx, pin_chunks, host_tile, res_, out=pin_out)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        res_ = sort_markdup(ctx, host_tile)
+        out = gather_sorted(ctx, pin_chunks, host_tile, res_, out=pin_out)
+    e2e_s = (time.perf_counter() - t) / args.steps
+    same = same and np.array_equal(res_.perm, w_perm) and len(out) == total
+    ms = statistics.mean(sort_ms) + statistics.mean(gather_ms)
+    sort_alg = n * (3 * 8 + 2 * 4 + 2 * 4)
+    gather_alg = 2 * total + n * (4 + 8 + 4 + 4)
+    s_ach = sort_alg / (statistics.mean(sort_ms) / 1000.0) / 1e9
+    g_ach = gather_alg / (statistics.mean(gather_ms) / 1000.0) / 1e9
+    return {
+        "metric": "records/s sort+markdup+gather", "value": round(n / (ms / 1000.0), 1), "unit": "records/s",
+        "ms_per_tile": round(ms, 3), "sort_markdup_ms": round(statistics.mean(sort_ms), 3),
+        "gather_ms": round(statistics.mean(gather_ms), 3),
+        "config": {"workload": f"one BAM tile of {nb} emitted batches x {bp} PE 2x{READ_LEN} pairs of the mapped "
+                               f"workload", "records": n, "bam_bytes": total, "duplicates_marked": int(w_marked)},
+        "e2e": {"value": round(n / e2e_s, 1), "unit": "records/s",
+                "h2d_bytes_per_step": int(n * 32 + total + n * 24), "d2h_bytes_per_step": int(n * 8 + total)},
+        "roofline": {"bound": "hbm", "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                     "sort_markdup": {"achieved": round(s_ach, 1), "frac": round(s_ach / peaks.get("hbm_gbs"), 4),
+                                      "alg_bytes_per_launch": sort_alg,
+                                      "alg": "read coord/dhi/dlo (8 B each) + score/pair (4 B each), write perm "
+                                             "and is_dup (4 B each)"},
+                     "gather": {"achieved": round(g_ach, 1), "frac": round(g_ach / peaks.get("hbm_gbs"), 4),
+                                "alg_bytes_per_launch": gather_alg,
+                                "alg": "read and write every record byte once + perm/rec/len/is_dup per record"},
+                     "traffic": None},
+        "gpu_launches": launches,
+        "cpu_baseline": {"value": round(n / cpu_s, 1), "unit": "records/s", "cores": 1, "kind": "port",
+                         "sample": f"the whole tile ({n} records), {cpu_s:.2f} s"},
+        "parity": {"records": n, "perm_flags_and_stream_identical": bool(same)},
     }
 
 
@@ -568,6 +715,9 @@ def run_ours(args, rank, world, local):
         line["parity_sample"] = {"reads": 2 * n, "mismatched_fields": bad}
     if rank == 0 and world == 1 and args.bam_pairs > 0:
         line["stages"] = {"bam_pack": run_bam_stage(args, ctx, rb, res, local, peaks)}
+        if args.sort_batches > 0:
+            torch.cuda.empty_cache()
+            line["stages"]["sort_markdup_gather"] = run_sort_stage(args, ctx, rb, res, local, peaks)
     if rank == 0 and world == 1 and not args.no_forms:
         from mojoalign_b200.autotune import FIELDS as TFIELDS
 

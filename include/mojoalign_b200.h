@@ -494,6 +494,62 @@ int ma_emit_bam_batch_device(ma_ctx* ctx, const ma_hits* d_hits, uint32_t n1, in
                              const ma_bam_meta* d_meta, const ma_bam_tile* tile, uint64_t* d_status,
                              void* stream);
 
+/* ---- coordinate sort, duplicate marking, sorted record gather -------- */
+
+/*
+ * Sorts a tile of n records (n < 2^32) by coordinate and marks duplicates.
+ * Replaces gpu_sort_markdup (fq2bam-meth/src/linear_gpu_sort.mojo:24-560),
+ * whose results do not depend on its tile size (METHYLGRAPHER_FM_SORT_TILE):
+ *   perm      record indices in coordinate order: stable by coord, ties in
+ *             record order (L469-525)
+ *   is_dup    1 for a duplicate, in record order.  Records are grouped by
+ *             equal (dhi, dlo); in each group except the unplaced one
+ *             (dhi == ~0) the pair with the highest score, then the lowest
+ *             pair id, is kept and every record of another pair is marked
+ *             (L409-466).  All 0 when do_markdup == 0.
+ *   dup_perm  (optional) record indices in (dhi, dlo, index) order; the
+ *             identity when do_markdup == 0
+ *   n_marked  (optional) number of records marked
+ * Inputs are the ma_bam_meta arrays of the tile.  Host buffers, synchronous.
+ */
+int ma_sort_markdup(ma_ctx* ctx, uint64_t n, const uint64_t* coord, const uint64_t* dhi,
+                    const uint64_t* dlo, const uint32_t* score, const uint32_t* pair,
+                    uint32_t* is_dup, uint32_t* perm, int do_markdup, uint32_t* dup_perm,
+                    uint64_t* n_marked);
+
+/* Same on device buffers, asynchronous on `stream` (NULL = the context's
+ * stream); d_marked (device u64, optional) receives the marked count. */
+int ma_sort_markdup_device(ma_ctx* ctx, uint64_t n, const uint64_t* d_coord,
+                           const uint64_t* d_dhi, const uint64_t* d_dlo, const uint32_t* d_score,
+                           const uint32_t* d_pair, uint32_t* d_is_dup, uint32_t* d_perm,
+                           int do_markdup, uint32_t* d_dup_perm, uint64_t* d_marked, void* stream);
+
+/*
+ * The tile's records in perm order as one uncompressed BAM record stream,
+ * flag 0x400 set on records with is_dup != 0 when apply_dup.  Replaces the
+ * record gather of _gather_perm_to_writer (linear_gpu_fm.mojo:177-225; the
+ * flag edit is _or_dup_flag, L408-420).  rec[i] = chunk << 32 | offset
+ * locates record i in chunks[chunk] (chunk_len bytes each); len[i] is its
+ * size.  Host buffers, synchronous.  MA_ERR_ARG when the stream exceeds
+ * out_cap or a record lies outside its chunk.
+ */
+int ma_gather_sorted_bam(ma_ctx* ctx, uint64_t n, const uint32_t* perm, const uint64_t* rec,
+                         const uint32_t* len, const uint32_t* is_dup, int apply_dup,
+                         const uint8_t* const* chunks, const uint64_t* chunk_len, uint32_t n_chunks,
+                         uint8_t* out, uint64_t out_cap, uint64_t* out_bytes);
+
+/* Same on device buffers (d_chunks: a device array of device chunk
+ * pointers), asynchronous.  d_status (device, 2 x u64) receives the stream's
+ * size and the number of records whose index, chunk or span is out of range
+ * (written as zero bytes).  Records are written only when d_status[0] <=
+ * out_cap. */
+int ma_gather_sorted_bam_device(ma_ctx* ctx, uint64_t n, const uint32_t* d_perm,
+                                const uint64_t* d_rec, const uint32_t* d_len,
+                                const uint32_t* d_is_dup, int apply_dup,
+                                const uint8_t* const* d_chunks, const uint64_t* d_chunk_len,
+                                uint32_t n_chunks, uint8_t* d_out, uint64_t out_cap,
+                                uint64_t* d_status, void* stream);
+
 /* ---- measurement (no reference counterpart; the reference only prints
  * perf_counter stage timers, linear_gpu_fm.mojo:2270-2273,3317-3340) ---- */
 

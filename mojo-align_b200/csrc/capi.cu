@@ -10,6 +10,7 @@
 #include <string>
 
 #include "bam_pack.h"
+#include "sort_markdup.h"
 #include "ma_device.cuh"
 #include "ma_internal.h"
 
@@ -102,6 +103,8 @@ struct ma_ctx {
     // BAM packing: inputs of the host-buffer form, records, metadata,
     // layout scratch and status
     DevBuf bam_in, bam_arena, bam_out, bam_meta, bam_scratch, bam_status;
+    // sort / markdup / gather of a tile
+    DevBuf sort_in, sort_out, sort_scratch, gather_in, gather_chunks, gather_out, gather_scratch;
 };
 
 struct ma_index {
@@ -327,7 +330,8 @@ void ma_ctx_destroy(ma_ctx* ctx) {
     for (DevBuf* b : {&ctx->bases, &ctx->lens, &ctx->packed, &ctx->err_flag, &ctx->o_rid, &ctx->o_pos, &ctx->o_mapq,
                       &ctx->o_flag, &ctx->o_sl, &ctx->o_sr, &ctx->o_nm, &ctx->d_uk, &ctx->d_ul, &ctx->d_us,
                       &ctx->d_e, &ctx->d_score, &ctx->bam_in, &ctx->bam_arena, &ctx->bam_out, &ctx->bam_meta,
-                      &ctx->bam_scratch, &ctx->bam_status})
+                      &ctx->bam_scratch, &ctx->bam_status, &ctx->sort_in, &ctx->sort_out, &ctx->sort_scratch,
+                      &ctx->gather_in, &ctx->gather_chunks, &ctx->gather_out, &ctx->gather_scratch})
         b->release();
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -812,6 +816,196 @@ int ma_emit_bam_batch_device(ma_ctx* ctx, const ma_hits* d_hits, uint32_t n1, in
         int launches = enqueue_bam_layout(b, ctx->bam_scratch.p, scratch, st);
         launches += enqueue_bam_records(b, ctx->bam_scratch.p, ctx->sm_count, st);
         ck(cudaGetLastError(), "bam kernels");
+        ctx->last_launches = launches;
+    });
+}
+
+namespace {
+void check_tile_size(uint64_t n) {
+    if (n >= (uint64_t(1) << 32)) fail(MA_ERR_ARG, "a tile holds fewer than 2^32 records");
+}
+}  // namespace
+
+int ma_sort_markdup(ma_ctx* ctx, uint64_t n, const uint64_t* coord, const uint64_t* dhi, const uint64_t* dlo,
+                    const uint32_t* score, const uint32_t* pair, uint32_t* is_dup, uint32_t* perm, int do_markdup,
+                    uint32_t* dup_perm, uint64_t* n_marked) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->last_launches = 0;
+        if (n_marked) *n_marked = 0;
+        if (n == 0) return;
+        check_tile_size(n);
+        if (!coord || !is_dup || !perm || (do_markdup && (!dhi || !dlo || !score || !pair)))
+            fail(MA_ERR_ARG, "null argument");
+        use_device(ctx);
+        cudaStream_t st = ctx->stream;
+        const uint64_t b8 = (n * 8 + 255) & ~uint64_t(255), b4 = (n * 4 + 255) & ~uint64_t(255);
+        ctx->sort_in.ensure(3 * b8 + 2 * b4);
+        ctx->sort_out.ensure(3 * b4 + 256);
+        uint8_t* in = ctx->sort_in.as<uint8_t>();
+        uint8_t* out = ctx->sort_out.as<uint8_t>();
+        SortDev s{};
+        s.n = n;
+        s.coord = reinterpret_cast<const uint64_t*>(in);
+        s.dhi = reinterpret_cast<const uint64_t*>(in + b8);
+        s.dlo = reinterpret_cast<const uint64_t*>(in + 2 * b8);
+        s.score = reinterpret_cast<const uint32_t*>(in + 3 * b8);
+        s.pair = reinterpret_cast<const uint32_t*>(in + 3 * b8 + b4);
+        s.is_dup = reinterpret_cast<uint32_t*>(out);
+        s.perm = reinterpret_cast<uint32_t*>(out + b4);
+        s.dup_perm = dup_perm ? reinterpret_cast<uint32_t*>(out + 2 * b4) : nullptr;
+        s.do_markdup = do_markdup ? 1 : 0;
+        s.marked = reinterpret_cast<unsigned long long*>(out + 3 * b4);
+        ck(cudaMemcpyAsync(in, coord, n * 8, cudaMemcpyHostToDevice, st), "H2D sort keys");
+        if (do_markdup) {
+            ck(cudaMemcpyAsync(in + b8, dhi, n * 8, cudaMemcpyHostToDevice, st), "H2D sort keys");
+            ck(cudaMemcpyAsync(in + 2 * b8, dlo, n * 8, cudaMemcpyHostToDevice, st), "H2D sort keys");
+            ck(cudaMemcpyAsync(in + 3 * b8, score, n * 4, cudaMemcpyHostToDevice, st), "H2D sort keys");
+            ck(cudaMemcpyAsync(in + 3 * b8 + b4, pair, n * 4, cudaMemcpyHostToDevice, st), "H2D sort keys");
+        }
+        const size_t scratch = sort_scratch_bytes(n);
+        ctx->sort_scratch.ensure(scratch);
+        const int launches = enqueue_sort_markdup(s, ctx->sort_scratch.p, scratch, st);
+        unsigned long long marked = 0;
+        ck(cudaMemcpyAsync(is_dup, s.is_dup, n * 4, cudaMemcpyDeviceToHost, st), "D2H is_dup");
+        ck(cudaMemcpyAsync(perm, s.perm, n * 4, cudaMemcpyDeviceToHost, st), "D2H perm");
+        if (dup_perm) ck(cudaMemcpyAsync(dup_perm, s.dup_perm, n * 4, cudaMemcpyDeviceToHost, st), "D2H dup_perm");
+        ck(cudaMemcpyAsync(&marked, s.marked, 8, cudaMemcpyDeviceToHost, st), "D2H marked");
+        ck(cudaStreamSynchronize(st), "sort/markdup");
+        if (n_marked) *n_marked = marked;
+        ctx->last_launches = launches;
+    });
+}
+
+int ma_sort_markdup_device(ma_ctx* ctx, uint64_t n, const uint64_t* d_coord, const uint64_t* d_dhi,
+                           const uint64_t* d_dlo, const uint32_t* d_score, const uint32_t* d_pair, uint32_t* d_is_dup,
+                           uint32_t* d_perm, int do_markdup, uint32_t* d_dup_perm, uint64_t* d_marked, void* stream) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->last_launches = 0;
+        use_device(ctx);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+        if (d_marked) ck(cudaMemsetAsync(d_marked, 0, 8, st), "memset");
+        if (n == 0) return;
+        check_tile_size(n);
+        if (!d_coord || !d_is_dup || !d_perm || (do_markdup && (!d_dhi || !d_dlo || !d_score || !d_pair)))
+            fail(MA_ERR_ARG, "null argument");
+        SortDev s{n, d_coord, d_dhi, d_dlo, d_score, d_pair, d_is_dup, d_perm, d_dup_perm, do_markdup ? 1 : 0,
+                  reinterpret_cast<unsigned long long*>(d_marked)};
+        const size_t scratch = sort_scratch_bytes(n);
+        ctx->sort_scratch.ensure(scratch);
+        ctx->last_launches = enqueue_sort_markdup(s, ctx->sort_scratch.p, scratch, st);
+    });
+}
+
+int ma_gather_sorted_bam(ma_ctx* ctx, uint64_t n, const uint32_t* perm, const uint64_t* rec, const uint32_t* len,
+                         const uint32_t* is_dup, int apply_dup, const uint8_t* const* chunks,
+                         const uint64_t* chunk_len, uint32_t n_chunks, uint8_t* out, uint64_t out_cap,
+                         uint64_t* out_bytes) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->last_launches = 0;
+        if (!out_bytes) fail(MA_ERR_ARG, "null argument");
+        *out_bytes = 0;
+        if (n == 0) return;
+        check_tile_size(n);
+        if (!perm || !rec || !len || (apply_dup && !is_dup) || (n_chunks && (!chunks || !chunk_len)) ||
+            (out_cap && !out))
+            fail(MA_ERR_ARG, "null argument");
+        use_device(ctx);
+        cudaStream_t st = ctx->stream;
+        // the chunks back to back in one device buffer
+        std::vector<uint64_t> base(n_chunks + 1, 0);
+        for (uint32_t c = 0; c < n_chunks; ++c) base[c + 1] = base[c] + ((chunk_len[c] + 15) & ~uint64_t(15));
+        ctx->gather_chunks.ensure(base[n_chunks] + (n_chunks + 1) * 16);
+        uint8_t* dch = ctx->gather_chunks.as<uint8_t>();
+        std::vector<const uint8_t*> ptrs(n_chunks);
+        for (uint32_t c = 0; c < n_chunks; ++c) {
+            if (chunk_len[c] && !chunks[c]) fail(MA_ERR_ARG, "null chunk");
+            if (chunk_len[c])
+                ck(cudaMemcpyAsync(dch + base[c], chunks[c], chunk_len[c], cudaMemcpyHostToDevice, st), "H2D chunk");
+            ptrs[c] = dch + base[c];
+        }
+        const uint64_t b8 = (n * 8 + 255) & ~uint64_t(255), b4 = (n * 4 + 255) & ~uint64_t(255);
+        const uint64_t tb = ((n_chunks + 1) * 8 + 255) & ~uint64_t(255);
+        ctx->gather_in.ensure(b8 + 3 * b4 + 2 * tb + 256);
+        uint8_t* in = ctx->gather_in.as<uint8_t>();
+        GatherDev g{};
+        g.n = n;
+        g.rec = reinterpret_cast<const uint64_t*>(in);
+        g.perm = reinterpret_cast<const uint32_t*>(in + b8);
+        g.len = reinterpret_cast<const uint32_t*>(in + b8 + b4);
+        g.is_dup = apply_dup ? reinterpret_cast<const uint32_t*>(in + b8 + 2 * b4) : nullptr;
+        g.apply_dup = apply_dup ? 1 : 0;
+        g.chunks = reinterpret_cast<const uint8_t* const*>(in + b8 + 3 * b4);
+        g.chunk_len = reinterpret_cast<const uint64_t*>(in + b8 + 3 * b4 + tb);
+        g.n_chunks = n_chunks;
+        g.status = reinterpret_cast<unsigned long long*>(in + b8 + 3 * b4 + 2 * tb);
+        ck(cudaMemcpyAsync(in, rec, n * 8, cudaMemcpyHostToDevice, st), "H2D rec");
+        ck(cudaMemcpyAsync(in + b8, perm, n * 4, cudaMemcpyHostToDevice, st), "H2D perm");
+        ck(cudaMemcpyAsync(in + b8 + b4, len, n * 4, cudaMemcpyHostToDevice, st), "H2D len");
+        if (apply_dup) ck(cudaMemcpyAsync(in + b8 + 2 * b4, is_dup, n * 4, cudaMemcpyHostToDevice, st), "H2D is_dup");
+        if (n_chunks) {
+            ck(cudaMemcpyAsync(in + b8 + 3 * b4, ptrs.data(), n_chunks * 8, cudaMemcpyHostToDevice, st), "H2D chunks");
+            ck(cudaMemcpyAsync(in + b8 + 3 * b4 + tb, chunk_len, n_chunks * 8, cudaMemcpyHostToDevice, st),
+               "H2D chunk sizes");
+        }
+        ck(cudaMemsetAsync(g.status, 0, 16, st), "memset");
+        const size_t scratch = gather_scratch_bytes(n);
+        ctx->gather_scratch.ensure(scratch);
+        int launches = enqueue_gather_layout(g, ctx->gather_scratch.p, scratch, st);
+        uint64_t total = 0;
+        unsigned long long status[2] = {0, 0};
+        ck(cudaMemcpyAsync(&total, gather_total_in_scratch(ctx->gather_scratch.p, n), 8, cudaMemcpyDeviceToHost, st),
+           "D2H size");
+        ck(cudaMemcpyAsync(status, g.status, 16, cudaMemcpyDeviceToHost, st), "D2H status");
+        ck(cudaStreamSynchronize(st), "gather layout");
+        if (status[1]) fail(MA_ERR_ARG, std::to_string(status[1]) + " records lie outside their chunks");
+        if (total > out_cap) fail(MA_ERR_ARG, "BAM record stream larger than the output buffer");
+        ctx->gather_out.ensure(total);
+        g.out = ctx->gather_out.as<uint8_t>();
+        g.cap = total;
+        launches += enqueue_gather_records(g, ctx->gather_scratch.p, ctx->sm_count, st);
+        ck(cudaMemcpyAsync(out, g.out, total, cudaMemcpyDeviceToHost, st), "D2H records");
+        ck(cudaStreamSynchronize(st), "gather records");
+        ctx->last_launches = launches;
+        *out_bytes = total;
+    });
+}
+
+int ma_gather_sorted_bam_device(ma_ctx* ctx, uint64_t n, const uint32_t* d_perm, const uint64_t* d_rec,
+                                const uint32_t* d_len, const uint32_t* d_is_dup, int apply_dup,
+                                const uint8_t* const* d_chunks, const uint64_t* d_chunk_len, uint32_t n_chunks,
+                                uint8_t* d_out, uint64_t out_cap, uint64_t* d_status, void* stream) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->last_launches = 0;
+        if (!d_status) fail(MA_ERR_ARG, "null argument");
+        use_device(ctx);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+        ck(cudaMemsetAsync(d_status, 0, 16, st), "memset");
+        if (n == 0) return;
+        check_tile_size(n);
+        if (!d_perm || !d_rec || !d_len || (apply_dup && !d_is_dup) || (n_chunks && (!d_chunks || !d_chunk_len)) ||
+            (out_cap && !d_out))
+            fail(MA_ERR_ARG, "null argument");
+        GatherDev g{};
+        g.n = n;
+        g.perm = d_perm;
+        g.rec = d_rec;
+        g.len = d_len;
+        g.is_dup = apply_dup ? d_is_dup : nullptr;
+        g.apply_dup = apply_dup ? 1 : 0;
+        g.chunks = d_chunks;
+        g.chunk_len = d_chunk_len;
+        g.n_chunks = n_chunks;
+        g.out = d_out;
+        g.cap = out_cap;
+        g.status = reinterpret_cast<unsigned long long*>(d_status);
+        const size_t scratch = gather_scratch_bytes(n);
+        ctx->gather_scratch.ensure(scratch);
+        int launches = enqueue_gather_layout(g, ctx->gather_scratch.p, scratch, st);
+        launches += enqueue_gather_records(g, ctx->gather_scratch.p, ctx->sm_count, st);
         ctx->last_launches = launches;
     });
 }

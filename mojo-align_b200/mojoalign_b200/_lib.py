@@ -210,6 +210,16 @@ SIGNATURES = [
      [C.c_void_p, C.POINTER(ma_hits), C.c_uint32, C.c_int, C.POINTER(ma_fastq_arena), C.c_void_p, C.c_int32,
       C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.POINTER(ma_bam_meta), C.POINTER(ma_bam_tile),
       C.c_void_p, C.c_void_p]),
+    ("ma_sort_markdup", C.c_int,
+     [C.c_void_p, C.c_uint64] + [C.c_void_p] * 7 + [C.c_int, C.c_void_p, C.POINTER(C.c_uint64)]),
+    ("ma_sort_markdup_device", C.c_int,
+     [C.c_void_p, C.c_uint64] + [C.c_void_p] * 7 + [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("ma_gather_sorted_bam", C.c_int,
+     [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+      C.c_uint32, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("ma_gather_sorted_bam_device", C.c_int,
+     [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+      C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     ("ma_synth_reference", C.c_int, [C.c_char_p, C.c_uint64, C.c_int, C.c_double, C.c_double, C.c_uint64]),
     ("ma_synth_reads", C.c_int,
      [C.c_char_p, C.POINTER(ma_read_model), C.c_uint32, C.c_int, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p,

@@ -15,6 +15,11 @@ contract of fq2bam-meth/src/linear_gpu_fm.mojo:
                    buffer overflow").
 - `rid_to_tid_table`  contig index -> SAM tid over canonical contig names
                    (_rid_to_tid_table, L423-435).
+- `sort_markdup`   gpu_sort_markdup (linear_gpu_sort.mojo:24-560) on a tile's
+                   metadata: coordinate permutation, duplicate flags and the
+                   duplicate-key order.
+- `gather_sorted`  the record gather of _gather_perm_to_writer (L177-225):
+                   the tile's records in coordinate order, duplicates flagged.
 """
 from __future__ import annotations
 
@@ -153,3 +158,48 @@ def canonical_rid_to_tid(contig_names) -> np.ndarray:
 
 
 rid_to_tid_table = canonical_rid_to_tid
+
+
+@dataclass
+class SortResult:
+    is_dup: np.ndarray
+    perm: np.ndarray
+    dup_perm: np.ndarray | None
+    n_marked: int
+
+
+def sort_markdup(ctx, tile: BamTile, do_markdup: bool = True, dup_perm: bool = False) -> SortResult:
+    """Sorts the tile's first n_reads records (host arrays in, host out)."""
+    n = tile.n_reads
+    m = {k: np.ascontiguousarray(tile.meta[k][:n]) for k in ("coord", "dhi", "dlo", "score", "pair")}
+    is_dup = np.empty(n, np.uint32)
+    perm = np.empty(n, np.uint32)
+    dp = np.empty(n, np.uint32) if dup_perm else None
+    marked = C.c_uint64(0)
+    rc = lib.ma_sort_markdup(ctx.handle, n, ptr(m["coord"]), ptr(m["dhi"]), ptr(m["dlo"]), ptr(m["score"]),
+                             ptr(m["pair"]), ptr(is_dup), ptr(perm), int(do_markdup), ptr(dp), C.byref(marked))
+    check(rc, ctx.handle)
+    return SortResult(is_dup, perm, dp, marked.value)
+
+
+def gather_sorted(ctx, chunks, tile: BamTile, res: SortResult, apply_dup: bool = True,
+                  out: np.ndarray | None = None) -> np.ndarray:
+    """The tile's records in res.perm order; chunks are the BAM chunks the
+    tile's `rec` entries point into (chunk index = position in the list).
+    Returns a view of `out` (allocated when missing or too small)."""
+    n = tile.n_reads
+    bufs = [np.ascontiguousarray(np.frombuffer(c, np.uint8) if not isinstance(c, np.ndarray) else c, dtype=np.uint8)
+            for c in chunks]
+    ptrs = (C.c_void_p * max(1, len(bufs)))(*[ptr(b) for b in bufs])
+    lens = np.array([b.size for b in bufs] or [0], np.uint64)
+    rec = np.ascontiguousarray(tile.meta["rec"][:n])
+    length = np.ascontiguousarray(tile.meta["len"][:n])
+    cap = int(length.sum(dtype=np.uint64))
+    if out is None or out.size < cap:
+        out = np.empty(max(cap, 1), np.uint8)
+    got = C.c_uint64(0)
+    rc = lib.ma_gather_sorted_bam(ctx.handle, n, ptr(res.perm), ptr(rec), ptr(length), ptr(res.is_dup),
+                                  int(apply_dup), C.cast(ptrs, C.c_void_p), ptr(lens), len(bufs), ptr(out), cap,
+                                  C.byref(got))
+    check(rc, ctx.handle)
+    return out[: got.value]

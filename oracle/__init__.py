@@ -19,7 +19,7 @@ LIB = HERE / "liboracle_fm.so"
 
 
 def build() -> Path:
-    newest = max((HERE / f).stat().st_mtime for f in ("oracle_fm.c", "oracle_bam.c", "Makefile"))
+    newest = max((HERE / f).stat().st_mtime for f in ("oracle_fm.c", "oracle_bam.c", "oracle_sort.c", "Makefile"))
     if not LIB.exists() or LIB.stat().st_mtime < newest:
         subprocess.run(["make", "-s", "-C", str(HERE), "liboracle_fm.so"], check=True)
     return LIB
@@ -82,6 +82,10 @@ def _load():
     lib.orc_pack_aln.argtypes = [vp, C.c_uint64, C.c_char_p] + [C.c_int64] * 7 + [C.c_char_p, C.c_int64, C.c_char_p] + \
         [C.c_int64] * 5 + [C.c_char_p, C.c_int64]
     lib.orc_pack_aln.restype = C.c_int64
+    lib.orc_sort_markdup.argtypes = [C.c_uint64, C.c_uint64] + [vp] * 7 + [C.c_int, vp]
+    lib.orc_sort_markdup.restype = C.c_int64
+    lib.orc_gather_sorted.argtypes = [C.c_uint64] + [vp] * 5 + [C.c_int, vp, C.c_uint64]
+    lib.orc_gather_sorted.restype = C.c_int64
     return lib
 
 
@@ -227,6 +231,40 @@ def pack_aln(name: bytes, flag: int, tid: int, pos0: int, mapq: int, sl: int, sr
     if n < 0:
         raise RuntimeError("BAM batch buffer overflow")
     return buf[:n].tobytes()
+
+
+def sort_markdup(coord, dhi, dlo, score, pair, do_markdup: bool = True, tile: int = 0, dup_perm: bool = True):
+    """orc_sort_markdup: gpu_sort_markdup (linear_gpu_sort.mojo:24-560).
+    Returns (is_dup, perm, dup_perm or None, marked)."""
+    coord, dhi, dlo = (np.ascontiguousarray(a, dtype=np.uint64) for a in (coord, dhi, dlo))
+    score, pair = (np.ascontiguousarray(a, dtype=np.uint32) for a in (score, pair))
+    n = coord.size
+    is_dup = np.zeros(n, np.uint32)
+    perm = np.zeros(n, np.uint32)
+    dp = np.zeros(n, np.uint32) if dup_perm else None
+    m = lib.orc_sort_markdup(n, tile, _p(coord), _p(dhi), _p(dlo), _p(score), _p(pair), _p(is_dup), _p(perm),
+                             int(do_markdup), _p(dp))
+    if m < 0:
+        raise MemoryError("orc_sort_markdup")
+    return is_dup, perm, dp, int(m)
+
+
+def gather_sorted(chunks, perm, rec, length, is_dup, apply_dup: bool = True) -> bytes:
+    """orc_gather_sorted: _gather_perm_to_writer (linear_gpu_fm.mojo:177-225)
+    as one byte stream.  chunks: list of bytes-like BAM chunks."""
+    bufs = [np.frombuffer(bytes(c), np.uint8) for c in chunks]
+    ptrs = (C.c_void_p * max(1, len(bufs)))(*[b.ctypes.data for b in bufs])
+    perm = np.ascontiguousarray(perm, dtype=np.uint32)
+    rec = np.ascontiguousarray(rec, dtype=np.uint64)
+    length = np.ascontiguousarray(length, dtype=np.uint32)
+    is_dup = np.ascontiguousarray(is_dup, dtype=np.uint32)
+    cap = int(length.sum(dtype=np.uint64))
+    out = np.zeros(max(cap, 1), np.uint8)
+    k = lib.orc_gather_sorted(perm.size, C.cast(ptrs, C.c_void_p), _p(perm), _p(rec), _p(length), _p(is_dup),
+                              int(apply_dup), _p(out), cap)
+    if k < 0:
+        raise RuntimeError("BAM record larger than batch buffer")
+    return out[:k].tobytes()
 
 
 def pack_bases(ascii_bytes) -> np.ndarray:

@@ -164,7 +164,7 @@ int orc_index_load(const char *prefix, orc_index **out) {
         snprintf(path, sizeof path, "%s.ann", prefix);
         FILE *f = fopen(path, "r");
         if (!f) {
-            snprintf(g_err, sizeof g_err, "FmIndex missing %s", path);
+            snprintf(g_err, sizeof g_err, "FmIndex missing %.400s", path);
             goto fail;
         }
         char line[8192];

@@ -116,3 +116,29 @@ def read_records(buf: bytes) -> list[dict]:
         off += 4 + block
     assert off == len(buf)
     return out
+
+
+def random_tile_meta(seed: int, n: int, *, dup_rate: float = 0.3, unplaced: float = 0.05):
+    """Sort/markdup inputs shaped like a tile's metadata: pairs share their
+    duplicate key, score and pair id; a fraction of pairs repeat another
+    pair's key (duplicates), some records are unplaced (dhi = ~0)."""
+    rng = np.random.default_rng(seed)
+    n_pairs = (n + 1) // 2
+    tid = rng.integers(0, 4, size=n_pairs).astype(np.uint64)
+    p5 = rng.integers(0, 1 << 20, size=n_pairs).astype(np.uint64)
+    src = np.arange(n_pairs)
+    dups = rng.random(n_pairs) < dup_rate
+    src[dups] = rng.integers(0, n_pairs, size=int(dups.sum()))
+    dhi = ((tid[src] + 1) << 48) | (p5[src] + (1 << 30))
+    dlo = ((tid[src] + 1) << 48) | (np.uint64(1) << 47) | (p5[src] + (1 << 30) + 300)
+    score = rng.integers(0, 4, size=n_pairs).astype(np.uint32) << 8
+    pair = np.arange(n_pairs, dtype=np.uint32) + np.uint32(rng.integers(0, 1000))
+    un = rng.random(n_pairs) < unplaced
+    dhi[un] = ~np.uint64(0)
+    rec = np.repeat(np.arange(n_pairs), 2)[:n]
+    coord = (tid[rec] << 32) | (p5[rec] + np.uint64(rng.integers(0, 400, size=n)))
+    idx = np.arange(n, dtype=np.uint64)
+    coord[un[rec]] = (np.uint64(0xFFFFFFFF) << 32) | idx[un[rec]]
+    dlo_r = dlo[rec].copy()
+    dlo_r[un[rec]] = (2 * (idx[un[rec]] // 2))
+    return {"coord": coord, "dhi": dhi[rec], "dlo": dlo_r, "score": score[rec], "pair": pair[rec]}
