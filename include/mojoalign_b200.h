@@ -403,6 +403,53 @@ const char* ma_serve_last_error(const ma_server* s);
 /* Drains, stops the worker threads and frees the reserved memory. */
 void ma_serve_destroy(ma_server* s);
 
+/* ---- FASTQ records on the device ------------------------------------ */
+
+/* Per-record spans of a parsed FASTQ buffer, arrays of max_records entries:
+ * the read name (qname span), the bases and the qualities, as byte offsets
+ * (plus `base`) into the buffer.  These are the name / orig / qual columns
+ * of ma_fastq_arena with the buffer as the arena. */
+typedef struct ma_fastq_records {
+    uint64_t* name_off;
+    uint32_t* name_len;
+    uint64_t* seq_off;
+    uint32_t* seq_len;
+    uint64_t* qual_off;
+    uint32_t* qual_len;
+} ma_fastq_records;
+
+/*
+ * Splits uncompressed FASTQ bytes into records.  Replaces the record split of
+ * fq_read_batch (fq2bam-meth/src/linear_fastq.mojo:437-451) with _store_rec
+ * (L365-417), _pipe_line (L233-280: lines end at '\n', one trailing '\r'
+ * dropped; at the end of the stream an unterminated rest is a line when it is
+ * not empty after that strip) and _qname_span (L308-325: leading '@' dropped,
+ * name cut at the first ' ' or '/').  Takes at most max_records records.
+ * at_eof == 0: the buffer continues in a later one, so only records whose
+ * four lines all end in '\n' are taken.  out3 (host) receives the records
+ * taken, the bytes they span (where the next buffer must start) and the
+ * longest SEQ.  n_bytes < 2^32.  A record cut short at the end of the stream
+ * fails with MA_ERR_FORMAT and the reference's message ("truncated FASTQ
+ * (missing SEQ)" / "(missing +)" / "(missing QUAL)").  Host buffers.
+ */
+int ma_fastq_parse(ma_ctx* ctx, const uint8_t* buf, uint64_t n_bytes, int at_eof,
+                   uint32_t max_records, uint64_t base, const ma_fastq_records* out,
+                   uint64_t* out3);
+
+/* Same on a device buffer with device outputs; returns when the counts are
+ * known (the split needs two small device-to-host reads). */
+int ma_fastq_parse_device(ma_ctx* ctx, const uint8_t* d_buf, uint64_t n_bytes, int at_eof,
+                          uint32_t max_records, uint64_t base, const ma_fastq_records* d_out,
+                          uint64_t* out3, void* stream);
+
+/* The mapper's input rows from parsed records: [n_seq][max_len] bytes, each
+ * SEQ span followed by 'N' up to max_len, and the lengths (fq_pack_bases,
+ * linear_fastq.mojo:454-492; the bases stay unconverted: the mapping call's
+ * bisulfite modes convert them).  d_lens may be NULL.  Asynchronous. */
+int ma_fastq_rows_device(ma_ctx* ctx, const uint8_t* d_arena, const uint64_t* d_seq_off,
+                         const uint32_t* d_seq_len, uint32_t n_seq, uint32_t max_len,
+                         uint8_t* d_rows, uint32_t* d_lens, void* stream);
+
 /* ---- BAM records of a mapped batch ---------------------------------- */
 
 /*

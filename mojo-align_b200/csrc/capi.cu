@@ -10,6 +10,7 @@
 #include <string>
 
 #include "bam_pack.h"
+#include "fastq_parse.h"
 #include "sort_markdup.h"
 #include "ma_device.cuh"
 #include "ma_internal.h"
@@ -105,6 +106,8 @@ struct ma_ctx {
     DevBuf bam_in, bam_arena, bam_out, bam_meta, bam_scratch, bam_status;
     // sort / markdup / gather of a tile
     DevBuf sort_in, sort_out, sort_scratch, gather_in, gather_chunks, gather_out, gather_scratch;
+    // FASTQ split
+    DevBuf fq_in, fq_out, fq_scratch, fq_newlines;
 };
 
 struct ma_index {
@@ -331,7 +334,8 @@ void ma_ctx_destroy(ma_ctx* ctx) {
                       &ctx->o_flag, &ctx->o_sl, &ctx->o_sr, &ctx->o_nm, &ctx->d_uk, &ctx->d_ul, &ctx->d_us,
                       &ctx->d_e, &ctx->d_score, &ctx->bam_in, &ctx->bam_arena, &ctx->bam_out, &ctx->bam_meta,
                       &ctx->bam_scratch, &ctx->bam_status, &ctx->sort_in, &ctx->sort_out, &ctx->sort_scratch,
-                      &ctx->gather_in, &ctx->gather_chunks, &ctx->gather_out, &ctx->gather_scratch})
+                      &ctx->gather_in, &ctx->gather_chunks, &ctx->gather_out, &ctx->gather_scratch, &ctx->fq_in,
+                      &ctx->fq_out, &ctx->fq_scratch, &ctx->fq_newlines})
         b->release();
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -1007,6 +1011,106 @@ int ma_gather_sorted_bam_device(ma_ctx* ctx, uint64_t n, const uint32_t* d_perm,
         int launches = enqueue_gather_layout(g, ctx->gather_scratch.p, scratch, st);
         launches += enqueue_gather_records(g, ctx->gather_scratch.p, ctx->sm_count, st);
         ctx->last_launches = launches;
+    });
+}
+
+namespace {
+void* fq_newline_buffer(void* user, size_t bytes) {
+    DevBuf* b = static_cast<DevBuf*>(user);
+    b->ensure(bytes);
+    return b->p;
+}
+
+const char* fastq_error(unsigned long long code) {
+    return code == 1 ? "truncated FASTQ (missing SEQ)"
+                     : code == 2 ? "truncated FASTQ (missing +)" : "truncated FASTQ (missing QUAL)";
+}
+
+// Parses on the device; outputs in d_out.  Returns the status of
+// fastq_parse_enqueue.
+void parse_on_device(ma_ctx* ctx, const uint8_t* d_buf, uint64_t n, int at_eof, uint32_t max_records, uint64_t base,
+                     const ma_fastq_records& d_out, cudaStream_t st, unsigned long long* status) {
+    if (n >= (uint64_t(1) << 32)) fail(MA_ERR_ARG, "a FASTQ buffer holds fewer than 2^32 bytes");
+    const size_t scratch = fastq_scratch_bytes(n);
+    ctx->fq_scratch.ensure(scratch);
+    FastqRecordsDev o{d_out.name_off, d_out.name_len, d_out.seq_off, d_out.seq_len, d_out.qual_off, d_out.qual_len};
+    ctx->last_launches = fastq_parse_enqueue(d_buf, n, at_eof, max_records, base, o, ctx->fq_scratch.p, scratch,
+                                             fq_newline_buffer, &ctx->fq_newlines, st, status);
+    if (status[3]) fail(MA_ERR_FORMAT, fastq_error(status[3]));
+}
+
+void check_records(const ma_fastq_records* o) {
+    if (!o || !o->name_off || !o->name_len || !o->seq_off || !o->seq_len || !o->qual_off || !o->qual_len)
+        fail(MA_ERR_ARG, "null record array");
+}
+}  // namespace
+
+int ma_fastq_parse(ma_ctx* ctx, const uint8_t* buf, uint64_t n_bytes, int at_eof, uint32_t max_records, uint64_t base,
+                   const ma_fastq_records* out, uint64_t* out3) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->last_launches = 0;
+        if (!out3 || (n_bytes && !buf)) fail(MA_ERR_ARG, "null argument");
+        check_records(out);
+        out3[0] = out3[1] = out3[2] = 0;
+        use_device(ctx);
+        cudaStream_t st = ctx->stream;
+        ctx->fq_in.ensure(n_bytes + 16);
+        if (n_bytes) ck(cudaMemcpyAsync(ctx->fq_in.p, buf, n_bytes, cudaMemcpyHostToDevice, st), "H2D FASTQ");
+        const uint64_t m = max_records;
+        const uint64_t b8 = (m * 8 + 255) & ~uint64_t(255), b4 = (m * 4 + 255) & ~uint64_t(255);
+        ctx->fq_out.ensure(3 * (b8 + b4) + 256);
+        uint8_t* o = ctx->fq_out.as<uint8_t>();
+        ma_fastq_records d{reinterpret_cast<uint64_t*>(o), reinterpret_cast<uint32_t*>(o + b8),
+                           reinterpret_cast<uint64_t*>(o + b8 + b4), reinterpret_cast<uint32_t*>(o + 2 * b8 + b4),
+                           reinterpret_cast<uint64_t*>(o + 2 * b8 + 2 * b4),
+                           reinterpret_cast<uint32_t*>(o + 3 * b8 + 2 * b4)};
+        unsigned long long status[6] = {0, 0, 0, 0, 0, 0};
+        parse_on_device(ctx, ctx->fq_in.as<uint8_t>(), n_bytes, at_eof, max_records, base, d, st, status);
+        const uint64_t r = status[1];
+        if (r) {
+            ck(cudaMemcpyAsync(out->name_off, d.name_off, r * 8, cudaMemcpyDeviceToHost, st), "D2H records");
+            ck(cudaMemcpyAsync(out->name_len, d.name_len, r * 4, cudaMemcpyDeviceToHost, st), "D2H records");
+            ck(cudaMemcpyAsync(out->seq_off, d.seq_off, r * 8, cudaMemcpyDeviceToHost, st), "D2H records");
+            ck(cudaMemcpyAsync(out->seq_len, d.seq_len, r * 4, cudaMemcpyDeviceToHost, st), "D2H records");
+            ck(cudaMemcpyAsync(out->qual_off, d.qual_off, r * 8, cudaMemcpyDeviceToHost, st), "D2H records");
+            ck(cudaMemcpyAsync(out->qual_len, d.qual_len, r * 4, cudaMemcpyDeviceToHost, st), "D2H records");
+            ck(cudaStreamSynchronize(st), "D2H records");
+        }
+        out3[0] = r;
+        out3[1] = status[2];
+        out3[2] = status[5];
+    });
+}
+
+int ma_fastq_parse_device(ma_ctx* ctx, const uint8_t* d_buf, uint64_t n_bytes, int at_eof, uint32_t max_records,
+                          uint64_t base, const ma_fastq_records* d_out, uint64_t* out3, void* stream) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->last_launches = 0;
+        if (!out3 || (n_bytes && !d_buf)) fail(MA_ERR_ARG, "null argument");
+        check_records(d_out);
+        out3[0] = out3[1] = out3[2] = 0;
+        use_device(ctx);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+        unsigned long long status[6] = {0, 0, 0, 0, 0, 0};
+        parse_on_device(ctx, d_buf, n_bytes, at_eof, max_records, base, *d_out, st, status);
+        out3[0] = status[1];
+        out3[1] = status[2];
+        out3[2] = status[5];
+    });
+}
+
+int ma_fastq_rows_device(ma_ctx* ctx, const uint8_t* d_arena, const uint64_t* d_seq_off, const uint32_t* d_seq_len,
+                         uint32_t n_seq, uint32_t max_len, uint8_t* d_rows, uint32_t* d_lens, void* stream) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->last_launches = 0;
+        if (n_seq == 0) return;
+        if (!d_arena || !d_seq_off || !d_seq_len || !d_rows) fail(MA_ERR_ARG, "null argument");
+        use_device(ctx);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+        ctx->last_launches = fastq_rows_enqueue(d_arena, d_seq_off, d_seq_len, n_seq, max_len, d_rows, d_lens, st);
     });
 }
 

@@ -148,6 +148,10 @@ class ma_fastq_arena(C.Structure):
                 ("qual_len", C.c_void_p)]
 
 
+class ma_fastq_records(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("name_off", "name_len", "seq_off", "seq_len", "qual_off", "qual_len")]
+
+
 class ma_bam_meta(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("coord", "dhi", "dlo", "rec", "len", "score", "pair")]
 
@@ -220,6 +224,14 @@ SIGNATURES = [
     ("ma_gather_sorted_bam_device", C.c_int,
      [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
       C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
+    ("ma_fastq_parse", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_uint32, C.c_uint64, C.POINTER(ma_fastq_records),
+      C.POINTER(C.c_uint64)]),
+    ("ma_fastq_parse_device", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_uint32, C.c_uint64, C.POINTER(ma_fastq_records),
+      C.POINTER(C.c_uint64), C.c_void_p]),
+    ("ma_fastq_rows_device", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("ma_synth_reference", C.c_int, [C.c_char_p, C.c_uint64, C.c_int, C.c_double, C.c_double, C.c_uint64]),
     ("ma_synth_reads", C.c_int,
      [C.c_char_p, C.POINTER(ma_read_model), C.c_uint32, C.c_int, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p,

@@ -75,10 +75,20 @@ class _Pipe:
         self.convert = mode
 
     def line(self):
+        """_pipe_line: a line ends at '\\n' and loses one trailing '\\r'; an
+        unterminated rest at the end of the stream is a line when it is not
+        empty after that strip."""
         ln = self.fh.readline()
         if not ln:
             return None
-        return ln.rstrip(b"\r\n")
+        terminated = ln.endswith(b"\n")
+        if terminated:
+            ln = ln[:-1]
+        if ln.endswith(b"\r"):
+            ln = ln[:-1]
+        if not terminated and not ln:
+            return None
+        return ln
 
     def record(self):
         h = self.line()

@@ -19,7 +19,7 @@ LIB = HERE / "liboracle_fm.so"
 
 
 def build() -> Path:
-    newest = max((HERE / f).stat().st_mtime for f in ("oracle_fm.c", "oracle_bam.c", "oracle_sort.c", "Makefile"))
+    newest = max((HERE / f).stat().st_mtime for f in ("oracle_fm.c", "oracle_bam.c", "oracle_sort.c", "oracle_fastq.c", "Makefile"))
     if not LIB.exists() or LIB.stat().st_mtime < newest:
         subprocess.run(["make", "-s", "-C", str(HERE), "liboracle_fm.so"], check=True)
     return LIB
@@ -86,6 +86,9 @@ def _load():
     lib.orc_sort_markdup.restype = C.c_int64
     lib.orc_gather_sorted.argtypes = [C.c_uint64] + [vp] * 5 + [C.c_int, vp, C.c_uint64]
     lib.orc_gather_sorted.restype = C.c_int64
+    lib.orc_fastq_parse.argtypes = [vp, C.c_uint64, C.c_int, C.c_uint64, C.c_uint64] + [vp] * 6 + \
+        [C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]
+    lib.orc_fastq_parse.restype = C.c_int64
     return lib
 
 
@@ -265,6 +268,30 @@ def gather_sorted(chunks, perm, rec, length, is_dup, apply_dup: bool = True) -> 
     if k < 0:
         raise RuntimeError("BAM record larger than batch buffer")
     return out[:k].tobytes()
+
+
+FASTQ_ERRORS = {-1: "truncated FASTQ (missing SEQ)", -2: "truncated FASTQ (missing +)",
+                -3: "truncated FASTQ (missing QUAL)"}
+
+
+def fastq_parse(buf, at_eof: bool = True, max_records: int | None = None, base: int = 0) -> dict:
+    """orc_fastq_parse: the record split of fq_read_batch / _store_rec /
+    _pipe_line / _qname_span (linear_fastq.mojo:233-451) over one buffer.
+    Returns name/seq/qual offsets and lengths, `n`, `consumed`, `max_len`;
+    raises RuntimeError with the reference's message on a truncated record."""
+    b = np.frombuffer(bytes(buf), np.uint8)
+    cap = b.size // 4 + 2 if max_records is None else max_records
+    out = {k: np.zeros(cap, np.uint64 if k.endswith("off") else np.uint32)
+           for k in ("name_off", "name_len", "seq_off", "seq_len", "qual_off", "qual_len")}
+    consumed, ml = C.c_uint64(0), C.c_uint32(0)
+    n = lib.orc_fastq_parse(_p(b) if b.size else None, b.size, int(at_eof), cap, base,
+                            *[_p(out[k]) for k in ("name_off", "name_len", "seq_off", "seq_len", "qual_off",
+                                                   "qual_len")], C.byref(consumed), C.byref(ml))
+    if n < 0:
+        raise RuntimeError(FASTQ_ERRORS[n])
+    res = {k: v[:n].copy() for k, v in out.items()}
+    res.update(n=int(n), consumed=consumed.value, max_len=ml.value)
+    return res
 
 
 def pack_bases(ascii_bytes) -> np.ndarray:
