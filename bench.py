@@ -75,6 +75,8 @@ def parse_args():
                     "(0 = skip that stage)")
     ap.add_argument("--sort-batches", type=int, default=4, help="BAM batches (of --bam-pairs pairs) in the "
                     "tile of the sort / duplicate-marking / gather stage (0 = skip)")
+    ap.add_argument("--fastq-pairs", type=int, default=2_000_000, help="read pairs of the FASTQ-split stage "
+                    "(its R1 file; 0 = skip)")
     ap.add_argument("--tuning", default="", help="fixed kernel choice 'seed_kernel,stage1_endpoints,"
                     "stage2_blocks_per_sm,reg_level,stage1_max_rows,stage2_first_wave[,wave_endpoints,"
                     "wave_loci_per_read,wave_max_rounds,wave_growth]' instead of the autotuner")
@@ -377,6 +379,111 @@ def run_bam_stage(args, ctx, rb, res, local, peaks):
         "cpu_baseline": {"value": round(n_seq / cpu_s, 1), "unit": "records/s", "cores": 1, "kind": "port",
                          "sample": f"the whole batch ({n_seq} records), {cpu_s:.2f} s"},
         "parity": {"records": n_seq, "bytes_and_metadata_identical": bool(same)},
+    }
+
+
+def fastq_text(rb, n: int, mate: int = 1, seed: int = 11) -> bytes:
+    """FASTQ text of n reads of the workload (mate 1: the R1 rows): Illumina-
+    style headers with a comment, the original bases, '+' and phred+33
+    qualities, LF line ends."""
+    rows = rb.bases[(mate - 1) * rb.n1:(mate - 1) * rb.n1 + n, :READ_LEN]
+    comment = b" %d:N:0:ACGTACGT\n" % mate
+    c = len(comment)
+    rec = np.empty((n, 21 + c + 2 * READ_LEN + 4), np.uint8)
+    rec[:, :11] = np.frombuffer(b"@B200:7:FC:", np.uint8)
+    idx = np.arange(n)
+    rec[:, 11:21] = np.array([idx // 10 ** k % 10 for k in range(9, -1, -1)], np.uint8).T + 48
+    rec[:, 21:21 + c] = np.frombuffer(comment, np.uint8)
+    q = 21 + c + READ_LEN
+    rec[:, 21 + c:q] = rows
+    rec[:, q:q + 3] = np.frombuffer(b"\n+\n", np.uint8)
+    rec[:, q + 3:q + 3 + READ_LEN] = np.random.default_rng(seed).integers(35, 75, size=(n, READ_LEN), dtype=np.uint8)
+    rec[:, -1] = 10
+    return rec.tobytes()
+
+
+def run_fastq_stage(args, ctx, rb, local, peaks):
+    """Record split + mapper rows of one FASTQ buffer on the device, the
+    host-bytes path end to end, and the oracle's split on one core."""
+    import ctypes as C
+
+    import torch
+
+    import oracle
+    from mojoalign_b200 import _lib
+
+    n = min(args.fastq_pairs, rb.n1)
+    text = fastq_text(rb, n)
+    nb = len(text)
+    dev = torch.device("cuda", local)
+    keys = ("name_off", "name_len", "seq_off", "seq_len", "qual_off", "qual_len")
+    d_out = {k: torch.empty(n, dtype=torch.int64 if k.endswith("off") else torch.int32, device=dev) for k in keys}
+    rec = _lib.ma_fastq_records(*[d_out[k].data_ptr() for k in keys])
+    pin = torch.from_numpy(np.frombuffer(text, np.uint8).copy()).pin_memory()
+    d_buf = pin.to(dev)
+    d_rows = torch.empty(n * READ_LEN, dtype=torch.uint8, device=dev)
+    d_lens = torch.empty(n, dtype=torch.int32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    o3 = (C.c_uint64 * 3)()
+
+    def device_step():
+        _lib.check(_lib.lib.ma_fastq_parse_device(ctx.handle, d_buf.data_ptr(), nb, 1, n, 0, C.byref(rec), o3,
+                                                  stream.cuda_stream), ctx.handle)
+        launches = ctx.last_launch_count()
+        _lib.check(_lib.lib.ma_fastq_rows_device(ctx.handle, d_buf.data_ptr(), d_out["seq_off"].data_ptr(),
+                                                 d_out["seq_len"].data_ptr(), n, int(o3[2]), d_rows.data_ptr(),
+                                                 d_lens.data_ptr(), stream.cuda_stream), ctx.handle)
+        return launches + ctx.last_launch_count()
+
+    torch.cuda.synchronize()
+    for _ in range(max(args.warmup, 3)):
+        device_step()
+    stream.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    ev0.record(stream)
+    for _ in range(args.steps):
+        launches += device_step()
+    ev1.record(stream)
+    stream.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+
+    def e2e_step():
+        d_buf.copy_(pin, non_blocking=True)  # host bytes -> HBM on torch's stream
+        torch.cuda.current_stream().synchronize()
+        return device_step()
+
+    e2e_step()
+    stream.synchronize()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    stream.synchronize()
+    e2e_s = (time.perf_counter() - t) / args.steps
+    got = {k: d_out[k].cpu().numpy().view(np.uint64 if k.endswith("off") else np.uint32) for k in keys}
+    rows = d_rows.cpu().numpy().reshape(n, READ_LEN)
+    t = time.perf_counter()
+    want = oracle.fastq_parse(text, max_records=n)
+    cpu_s = time.perf_counter() - t
+    same = int(o3[0]) == want["n"] == n and all(np.array_equal(got[k], want[k]) for k in keys)
+    same = same and np.array_equal(rows, rb.bases[:n, :READ_LEN])
+    alg = nb + n * (3 * 8 + 3 * 4) + n * (READ_LEN + 4)
+    achieved = alg / (ms / 1000.0) / 1e9
+    return {
+        "metric": "records/s FASTQ split + mapper rows", "value": round(n / (ms / 1000.0), 1), "unit": "records/s",
+        "ms_per_buffer": round(ms, 3), "gb_per_s_of_fastq": round(nb / (ms / 1000.0) / 1e9, 1),
+        "config": {"workload": f"R1 FASTQ text of {n} reads of the workload ({READ_LEN} bp, 40-byte headers, LF)",
+                   "records": n, "fastq_bytes": nb},
+        "e2e": {"value": round(n / e2e_s, 1), "unit": "records/s", "h2d_bytes_per_step": nb,
+                "d2h_bytes_per_step": 48},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                     "frac": round(achieved / peaks.get("hbm_gbs"), 4), "traffic": None,
+                     "alg_bytes_per_launch": alg,
+                     "alg": "FASTQ bytes read once + 36 B of spans and the row + length written per record"},
+        "gpu_launches": launches,
+        "cpu_baseline": {"value": round(n / cpu_s, 1), "unit": "records/s", "cores": 1, "kind": "port",
+                         "sample": f"the whole buffer ({n} records, {nb} bytes), {cpu_s:.2f} s"},
+        "parity": {"records": n, "spans_and_rows_identical": bool(same)},
     }
 
 
@@ -718,6 +825,9 @@ def run_ours(args, rank, world, local):
         if args.sort_batches > 0:
             torch.cuda.empty_cache()
             line["stages"]["sort_markdup_gather"] = run_sort_stage(args, ctx, rb, res, local, peaks)
+    if rank == 0 and world == 1 and args.fastq_pairs > 0:
+        torch.cuda.empty_cache()
+        line.setdefault("stages", {})["fastq_split"] = run_fastq_stage(args, ctx, rb, local, peaks)
     if rank == 0 and world == 1 and not args.no_forms:
         from mojoalign_b200.autotune import FIELDS as TFIELDS
 

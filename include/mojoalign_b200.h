@@ -597,6 +597,35 @@ int ma_gather_sorted_bam_device(ma_ctx* ctx, uint64_t n, const uint32_t* d_perm,
                                 uint32_t n_chunks, uint8_t* d_out, uint64_t out_cap,
                                 uint64_t* d_status, void* stream);
 
+/* ---- BGZF ------------------------------------------------------------ */
+
+/*
+ * Compresses an uncompressed BAM stream (header + records) into BGZF.
+ * Replaces the BGZF layer of the reference's BAM writer
+ * (fq2bam-meth/python/bam_emit.py: _BgzfWriter L101-186, _bgzf_block
+ * L77-98): the stream is cut every 65280 bytes; each piece becomes a gzip
+ * member (FEXTRA "BC" subfield with BSIZE, raw deflate, CRC-32, ISIZE) and,
+ * with append_eof, the 28-byte EOF member closes the file.  level 0 stores
+ * the pieces with the framing zlib produces for one compress + finish call,
+ * so the file is byte-identical to the reference's at that level; levels
+ * 1..9 use this library's LZ77 + dynamic-Huffman coder (the deflate data
+ * differ from zlib's, the members decompress to the same bytes, and the
+ * framing, block boundaries, CRCs and sizes are the reference's).  Host
+ * buffers, synchronous; out_bytes receives the file size.  MA_ERR_ARG when
+ * out_cap is smaller (ma_bgzf_bound gives a safe size).
+ */
+int ma_bgzf_compress(ma_ctx* ctx, const uint8_t* in, uint64_t n, int level, int append_eof,
+                     uint8_t* out, uint64_t out_cap, uint64_t* out_bytes);
+
+/* Same on device buffers; returns when the size is known (synchronous on
+ * `stream`, NULL = the context's stream). */
+int ma_bgzf_compress_device(ma_ctx* ctx, const uint8_t* d_in, uint64_t n, int level,
+                            int append_eof, uint8_t* d_out, uint64_t out_cap,
+                            uint64_t* out_bytes, void* stream);
+
+/* An output size large enough for n input bytes (EOF member included). */
+uint64_t ma_bgzf_bound(uint64_t n);
+
 /* ---- measurement (no reference counterpart; the reference only prints
  * perf_counter stage timers, linear_gpu_fm.mojo:2270-2273,3317-3340) ---- */
 

@@ -10,6 +10,7 @@
 #include <string>
 
 #include "bam_pack.h"
+#include "bgzf.h"
 #include "fastq_parse.h"
 #include "sort_markdup.h"
 #include "ma_device.cuh"
@@ -108,6 +109,8 @@ struct ma_ctx {
     DevBuf sort_in, sort_out, sort_scratch, gather_in, gather_chunks, gather_out, gather_scratch;
     // FASTQ split
     DevBuf fq_in, fq_out, fq_scratch, fq_newlines;
+    // BGZF
+    DevBuf bgzf_in, bgzf_out, bgzf_scratch;
 };
 
 struct ma_index {
@@ -335,7 +338,8 @@ void ma_ctx_destroy(ma_ctx* ctx) {
                       &ctx->d_e, &ctx->d_score, &ctx->bam_in, &ctx->bam_arena, &ctx->bam_out, &ctx->bam_meta,
                       &ctx->bam_scratch, &ctx->bam_status, &ctx->sort_in, &ctx->sort_out, &ctx->sort_scratch,
                       &ctx->gather_in, &ctx->gather_chunks, &ctx->gather_out, &ctx->gather_scratch, &ctx->fq_in,
-                      &ctx->fq_out, &ctx->fq_scratch, &ctx->fq_newlines})
+                      &ctx->fq_out, &ctx->fq_scratch, &ctx->fq_newlines, &ctx->bgzf_in, &ctx->bgzf_out,
+                      &ctx->bgzf_scratch})
         b->release();
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -1111,6 +1115,60 @@ int ma_fastq_rows_device(ma_ctx* ctx, const uint8_t* d_arena, const uint64_t* d_
         use_device(ctx);
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
         ctx->last_launches = fastq_rows_enqueue(d_arena, d_seq_off, d_seq_len, n_seq, max_len, d_rows, d_lens, st);
+    });
+}
+
+uint64_t ma_bgzf_bound(uint64_t n) { return bgzf_bound(n); }
+
+namespace {
+uint64_t bgzf_on_device(ma_ctx* ctx, const uint8_t* d_in, uint64_t n, int level, int append_eof, uint8_t* d_out,
+                        uint64_t out_cap, cudaStream_t st) {
+    if (level < 0 || level > 9) fail(MA_ERR_ARG, "BGZF level must be in 0..9");
+    const size_t scratch = bgzf_scratch_bytes(n, ctx->sm_count);
+    ctx->bgzf_scratch.ensure(scratch);
+    uint64_t need = 0;
+    int launches = 0;
+    const uint64_t got = bgzf_compress(d_in, n, level, d_out, out_cap, append_eof, ctx->bgzf_scratch.p, scratch,
+                                       ctx->sm_count, st, &need, &launches, nullptr);
+    ctx->last_launches = launches;
+    if (!got && need) fail(MA_ERR_ARG, "BGZF output larger than the output buffer (" + std::to_string(need) + " bytes)");
+    return got;
+}
+}  // namespace
+
+int ma_bgzf_compress(ma_ctx* ctx, const uint8_t* in, uint64_t n, int level, int append_eof, uint8_t* out,
+                     uint64_t out_cap, uint64_t* out_bytes) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->last_launches = 0;
+        if (!out_bytes || (n && !in) || (out_cap && !out)) fail(MA_ERR_ARG, "null argument");
+        *out_bytes = 0;
+        use_device(ctx);
+        cudaStream_t st = ctx->stream;
+        ctx->bgzf_in.ensure(n + 16);
+        if (n) ck(cudaMemcpyAsync(ctx->bgzf_in.p, in, n, cudaMemcpyHostToDevice, st), "H2D BGZF input");
+        const uint64_t bound = bgzf_bound(n);
+        ctx->bgzf_out.ensure(bound);
+        const uint64_t got = bgzf_on_device(ctx, ctx->bgzf_in.as<uint8_t>(), n, level, append_eof,
+                                            ctx->bgzf_out.as<uint8_t>(), bound, st);
+        if (got > out_cap) fail(MA_ERR_ARG, "BGZF output larger than the output buffer (" + std::to_string(got) +
+                                                " bytes)");
+        if (got) ck(cudaMemcpyAsync(out, ctx->bgzf_out.p, got, cudaMemcpyDeviceToHost, st), "D2H BGZF");
+        ck(cudaStreamSynchronize(st), "D2H BGZF");
+        *out_bytes = got;
+    });
+}
+
+int ma_bgzf_compress_device(ma_ctx* ctx, const uint8_t* d_in, uint64_t n, int level, int append_eof, uint8_t* d_out,
+                            uint64_t out_cap, uint64_t* out_bytes, void* stream) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->last_launches = 0;
+        if (!out_bytes || (n && !d_in) || (out_cap && !d_out)) fail(MA_ERR_ARG, "null argument");
+        *out_bytes = 0;
+        use_device(ctx);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+        *out_bytes = bgzf_on_device(ctx, d_in, n, level, append_eof, d_out, out_cap, st);
     });
 }
 
