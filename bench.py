@@ -77,6 +77,8 @@ def parse_args():
                     "tile of the sort / duplicate-marking / gather stage (0 = skip)")
     ap.add_argument("--fastq-pairs", type=int, default=2_000_000, help="read pairs of the FASTQ-split stage "
                     "(its R1 file; 0 = skip)")
+    ap.add_argument("--bgzf-level", type=int, default=1, help="BGZF level of the compression stage "
+                    "(the reference's default, METHYLGRAPHER_BAM_LEVEL=1; -1 = skip)")
     ap.add_argument("--tuning", default="", help="fixed kernel choice 'seed_kernel,stage1_endpoints,"
                     "stage2_blocks_per_sm,reg_level,stage1_max_rows,stage2_first_wave[,wave_endpoints,"
                     "wave_loci_per_read,wave_max_rounds,wave_growth]' instead of the autotuner")
@@ -487,6 +489,104 @@ def run_fastq_stage(args, ctx, rb, local, peaks):
     }
 
 
+def run_bgzf_stage(args, ctx, stream_bytes, local, peaks):
+    """BGZF of the sorted record stream: device throughput, the host API end
+    to end, the oracle's zlib writer on the host cores, the size against
+    zlib at the same level, and the round trip."""
+    import concurrent.futures as cf
+    import ctypes as C
+    import zlib
+
+    import torch
+
+    from mojoalign_b200 import _lib
+    from oracle import bgzf_ref
+
+    data = np.ascontiguousarray(stream_bytes)
+    n = int(data.size)
+    level = args.bgzf_level
+    dev = torch.device("cuda", local)
+    d_in = torch.from_numpy(data).to(dev)
+    cap = int(_lib.lib.ma_bgzf_bound(n))
+    d_out = torch.empty(cap, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    got = C.c_uint64(0)
+
+    def device_step():
+        _lib.check(_lib.lib.ma_bgzf_compress_device(ctx.handle, d_in.data_ptr(), n, level, 1, d_out.data_ptr(), cap,
+                                                    C.byref(got), stream.cuda_stream), ctx.handle)
+        return ctx.last_launch_count()
+
+    torch.cuda.synchronize()
+    for _ in range(max(args.warmup, 3)):
+        device_step()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    ev0.record(stream)
+    for _ in range(args.steps):
+        launches += device_step()
+    ev1.record(stream)
+    stream.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    out = d_out[:got.value].cpu().numpy().tobytes()
+    # round trip and framing of every member
+    ms_ = bgzf_ref.members(out)
+    ok = out[ms_[-1]["off"]:] == bgzf_ref.EOF_MEMBER and len(ms_) - 1 == (n + bgzf_ref.BLOCK - 1) // bgzf_ref.BLOCK
+    mv = memoryview(data)
+    for i, m in enumerate(ms_[:-1]):
+        piece = mv[i * bgzf_ref.BLOCK:(i + 1) * bgzf_ref.BLOCK]
+        ok = ok and m["isize"] == len(piece) and m["crc"] == (zlib.crc32(piece) & 0xFFFFFFFF)
+        ok = ok and m["fixed"] == (31, 139, 8, 4, 0, 0, 255, 6, 66, 67, 2)
+        if i % 16 == 0:
+            ok = ok and bgzf_ref.inflate(m["payload"]) == bytes(piece)
+    # end to end: pinned host stream in, BGZF bytes out
+    pin_in = torch.from_numpy(data).pin_memory().numpy()
+    pin_out = torch.empty(cap, dtype=torch.uint8, pin_memory=True).numpy()
+
+    def host_step():
+        _lib.check(_lib.lib.ma_bgzf_compress(ctx.handle, pin_in.ctypes.data, n, level, 1, pin_out.ctypes.data, cap,
+                                             C.byref(got)), ctx.handle)
+
+    host_step()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        host_step()
+    e2e_s = (time.perf_counter() - t) / args.steps
+    ok = ok and pin_out[:got.value].tobytes() == out
+    # the oracle (the reference's zlib writer) on all host cores over a sample
+    sample = bytes(mv[:min(n, 256 * bgzf_ref.BLOCK)])
+    cores = os.cpu_count() or 1
+    pieces = [sample[i:i + bgzf_ref.BLOCK] for i in range(0, len(sample), bgzf_ref.BLOCK)]
+    t = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=cores) as ex:
+        zparts = list(ex.map(lambda c: bgzf_ref.member(c, level), pieces))
+    cpu_s = time.perf_counter() - t
+    zsize = sum(len(z) for z in zparts)
+    gsize = sum(m["size"] for m in ms_[:len(pieces)])
+    return {
+        "metric": "GB/s BGZF (uncompressed bytes)", "value": round(n / (ms / 1000.0) / 1e9, 2), "unit": "GB/s",
+        "ms_per_stream": round(ms, 3),
+        "config": {"workload": "the sorted, duplicate-marked record stream of the sort stage", "bytes": n,
+                   "level": level, "bgzf_bytes": len(out),
+                   "ratio": round(n / len(out), 3),
+                   "size_vs_zlib_same_level": round(gsize / zsize, 4)},
+        "e2e": {"value": round(n / e2e_s / 1e9, 2), "unit": "GB/s", "h2d_bytes_per_step": n,
+                "d2h_bytes_per_step": len(out)},
+        "roofline": {"bound": "hbm", "achieved": round((n + len(out)) / (ms / 1000.0) / 1e9, 1),
+                     "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                     "frac": round((n + len(out)) / (ms / 1000.0) / 1e9 / peaks.get("hbm_gbs"), 4),
+                     "traffic": None, "alg_bytes_per_launch": n + len(out),
+                     "alg": "input read once + members written once; the coder is bound by shared-memory "
+                            "matching, not HBM"},
+        "gpu_launches": launches,
+        "cpu_baseline": {"value": round(len(sample) / cpu_s / 1e9, 3), "unit": "GB/s", "cores": cores,
+                         "kind": "port", "sample": f"first {len(pieces)} pieces ({len(sample)} bytes) through the "
+                                                   f"reference writer's zlib member code, {cores} threads, "
+                                                   f"{cpu_s:.2f} s"},
+        "parity": {"members": len(ms_) - 1, "framing_crc_isize_and_round_trip": bool(ok)},
+    }
+
+
 def run_sort_stage(args, ctx, rb, res, local, peaks):
     """Coordinate sort + duplicate marking + sorted gather of one BAM tile
     made of --sort-batches emitted batches: device-resident throughput, the
@@ -600,6 +700,7 @@ def run_sort_stage(args, ctx, rb, res, local, peaks):
         out = gather_sorted(ctx, pin_chunks, host_tile, res_, out=pin_out)
     e2e_s = (time.perf_counter() - t) / args.steps
     same = same and np.array_equal(res_.perm, w_perm) and len(out) == total
+    args._sorted_stream = g_sorted
     ms = statistics.mean(sort_ms) + statistics.mean(gather_ms)
     sort_alg = n * (3 * 8 + 2 * 4 + 2 * 4)
     gather_alg = 2 * total + n * (4 + 8 + 4 + 4)
@@ -825,6 +926,10 @@ def run_ours(args, rank, world, local):
         if args.sort_batches > 0:
             torch.cuda.empty_cache()
             line["stages"]["sort_markdup_gather"] = run_sort_stage(args, ctx, rb, res, local, peaks)
+            if args.bgzf_level >= 0 and getattr(args, "_sorted_stream", None) is not None:
+                torch.cuda.empty_cache()
+                line["stages"]["bgzf"] = run_bgzf_stage(args, ctx, args._sorted_stream, local, peaks)
+                del args._sorted_stream
     if rank == 0 and world == 1 and args.fastq_pairs > 0:
         torch.cuda.empty_cache()
         line.setdefault("stages", {})["fastq_split"] = run_fastq_stage(args, ctx, rb, local, peaks)

@@ -42,16 +42,17 @@
 namespace ma {
 namespace {
 
-constexpr int THREADS = 1024;
-constexpr int SUB = 32;                        // bytes per parse thread
+constexpr int THREADS = 512;                   // two CTAs per SM
+constexpr int SUB = 32;                        // bytes per parse sub-block
 constexpr int NSUB = (BGZF_BLOCK + SUB - 1) / SUB;  // 2040
-constexpr int WBITS = 15;
-constexpr uint32_t WSIZE = 1u << WBITS;        // deflate window
+constexpr int SUBS_PER_THREAD = (NSUB + THREADS - 1) / THREADS;  // 4
+constexpr int WBITS = 13;
+constexpr uint32_t WSIZE = 1u << WBITS;        // match window (deflate allows up to 32 KB)
 constexpr uint32_t WMASK = WSIZE - 1;
 constexpr int HBITS = 12;
 constexpr int HSIZE = 1 << HBITS;
 constexpr uint16_t NONE = 0xffff;              // no previous position
-constexpr int CRC_SEG = 64;
+constexpr int CRC_SEG = 128;
 constexpr uint32_t CRC_POLY = 0xedb88320u;     // CRC-32, reflected
 constexpr int NLL = 286, NDIST = 30, NCL = 19;
 
@@ -219,15 +220,15 @@ __device__ void huff_codes(const uint8_t* len, int n, uint16_t* code, int lane) 
     __syncwarp();
 }
 
-// Everything one CTA keeps for the piece it compresses.
+// Everything one CTA keeps for the piece it compresses (under half of an
+// SM's shared memory, so two pieces are in flight per SM).
 struct Smem {
-    uint8_t data[BGZF_BLOCK + 64];
     union {
-        uint16_t prev[WSIZE];     // LZ77 links, a ring over the window
-        uint32_t out[WSIZE / 2];  // then: the deflate bits
+        uint8_t data[BGZF_BLOCK + 64];
+        uint32_t out[(BGZF_BLOCK + 64) / 4];  // deflate bits, once the tokens hold the data
     } u;
+    uint16_t prev[WSIZE];  // LZ77 links, a ring over the window
     uint32_t head[HSIZE];  // per hash: last position + 1 of earlier phases
-    uint32_t best[THREADS];
     uint32_t crc_seg[THREADS];
     uint32_t crc_tab[256];
     uint32_t freq_ll[NLL + 2], freq_d[NDIST + 2], freq_cl[NCL + 1];
@@ -242,6 +243,26 @@ struct Smem {
     uint32_t nl_nd[2];
     typename cub::BlockScan<uint32_t, THREADS>::TempStorage scan;
 };
+
+// Four bytes of the piece starting at byte i (two aligned shared loads).
+__device__ __forceinline__ uint32_t load4(const uint32_t* w, uint32_t i) {
+    return __funnelshift_r(w[i >> 2], w[(i >> 2) + 1], 8 * (i & 3));
+}
+
+// Length of the common prefix of the piece at q and at p, at most lim
+// (reads may run into the 64 padding bytes; the result is clamped).
+__device__ __forceinline__ uint32_t match_len(const uint32_t* w, uint32_t q, uint32_t p, uint32_t lim) {
+    uint32_t L = 0;
+    while (L < lim) {
+        const uint32_t x = load4(w, q + L) ^ load4(w, p + L);
+        if (x) {
+            L += (__ffs(x) - 1) >> 3;
+            break;
+        }
+        L += 4;
+    }
+    return L < lim ? L : lim;
+}
 
 __device__ __forceinline__ uint32_t hash3(const uint8_t* d) {
     const uint32_t v = (static_cast<uint32_t>(d[0]) << 16) | (static_cast<uint32_t>(d[1]) << 8) | d[2];
@@ -269,10 +290,20 @@ struct BitOut {
     }
 };
 
-// Sequential writer into the header words (one thread).
+// Sequential writer into the (zeroed) header words (one thread).
 __device__ __forceinline__ void hdr_put(uint32_t* hdr, uint32_t& pos, uint32_t v, uint32_t nbits) {
-    for (uint32_t i = 0; i < nbits; ++i, ++pos)
-        if ((v >> i) & 1u) hdr[pos >> 5] |= 1u << (pos & 31);
+    const uint64_t x = static_cast<uint64_t>(v) << (pos & 31);
+    hdr[pos >> 5] |= static_cast<uint32_t>(x);
+    if ((pos & 31) + nbits > 32) hdr[(pos >> 5) + 1] |= static_cast<uint32_t>(x >> 32);
+    pos += nbits;
+}
+
+// One atomic per distinct symbol of the warp's active lanes.
+__device__ __forceinline__ void warp_count(uint32_t* freq, uint32_t sym, bool on) {
+    const uint32_t act = __ballot_sync(0xffffffffu, on);
+    if (!on) return;
+    const uint32_t same = __match_any_sync(act, sym);
+    if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(&freq[sym], static_cast<uint32_t>(__popc(same)));
 }
 
 __device__ __forceinline__ void token_bits(const Smem& S, uint32_t tokv, uint32_t& bits) {
@@ -286,17 +317,18 @@ __device__ __forceinline__ void token_bits(const Smem& S, uint32_t tokv, uint32_
     }
 }
 
-// CRC-32 of the piece from the 64-byte segment remainders (one warp): lane
-// l folds segments [32 l, 32 l + 32), lane 0 folds the lanes, and the
+// CRC-32 of the piece from the segment remainders (one warp): each lane
+// folds its run of segments, lane 0 folds the lanes, and the
 // standard initial and final inversion contribute F x^(8n) + F.
 __device__ void crc_combine(Smem& S, uint32_t n, int lane) {
     const uint32_t x64 = S.x_seg, x2048 = S.x_lane;
     uint32_t c = 0, len = 0;
-    for (int k = 0; k < 32; ++k) {
-        const uint32_t s0 = (lane * 32 + k) * CRC_SEG;
+    constexpr int PER_LANE = THREADS / 32;
+    for (int k = 0; k < PER_LANE; ++k) {
+        const uint32_t s0 = (lane * PER_LANE + k) * CRC_SEG;
         if (s0 >= n) break;
         const uint32_t sl = s0 + CRC_SEG <= n ? CRC_SEG : n - s0;
-        c = gf2_mul(c, sl == CRC_SEG ? x64 : gf2_xpow(8ull * sl)) ^ S.crc_seg[lane * 32 + k];
+        c = gf2_mul(c, sl == CRC_SEG ? x64 : gf2_xpow(8ull * sl)) ^ S.crc_seg[lane * PER_LANE + k];
         len += sl;
     }
     S.lane_crc[lane] = c;
@@ -306,7 +338,7 @@ __device__ void crc_combine(Smem& S, uint32_t n, int lane) {
         uint32_t r = 0;
         for (int l = 0; l < 32; ++l) {
             const uint32_t ll = S.lane_len[l];
-            if (ll) r = gf2_mul(r, ll == 32 * CRC_SEG ? x2048 : gf2_xpow(8ull * ll)) ^ S.lane_crc[l];
+            if (ll) r = gf2_mul(r, ll == (THREADS / 32) * CRC_SEG ? x2048 : gf2_xpow(8ull * ll)) ^ S.lane_crc[l];
         }
         S.crc = r ^ gf2_mul(0xffffffffu, gf2_xpow(8ull * n)) ^ 0xffffffffu;
     }
@@ -327,9 +359,9 @@ __device__ void write_frame(uint8_t* slot, uint32_t payload, uint32_t crc, uint3
     }
 }
 
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __launch_bounds__(THREADS, 2)
     bgzf_kernel(const uint8_t* in, uint64_t n_total, uint32_t n_blocks, int level, int chain, uint8_t* slots,
-                uint32_t* sizes, uint32_t* tok_all) {
+                uint32_t* sizes, uint32_t* tok_all, uint32_t* best_all) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     Smem& S = *reinterpret_cast<Smem*>(smem_raw);
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -340,15 +372,23 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     if (t == 0) {
         S.x_seg = gf2_xpow(8ull * CRC_SEG);
-        S.x_lane = gf2_xpow(8ull * 32 * CRC_SEG);
+        S.x_lane = gf2_xpow(8ull * (THREADS / 32) * CRC_SEG);
     }
     uint32_t* tok = tok_all + static_cast<size_t>(blockIdx.x) * BGZF_BLOCK;
+    uint32_t* best = best_all + static_cast<size_t>(blockIdx.x) * BGZF_BLOCK;
     for (uint32_t b = blockIdx.x; b < n_blocks; b += gridDim.x) {
         const uint64_t base = static_cast<uint64_t>(b) * BGZF_BLOCK;
         const uint32_t n = static_cast<uint32_t>(n_total - base < BGZF_BLOCK ? n_total - base : BGZF_BLOCK);
         uint8_t* slot = slots + static_cast<size_t>(b) * 65536;
         __syncthreads();  // the previous piece is done with shared memory
-        for (uint32_t i = t; i < n + 64; i += THREADS) S.data[i] = i < n ? in[base + i] : 0;
+        if ((reinterpret_cast<uintptr_t>(in + base) & 15) == 0) {
+            const uint4* src = reinterpret_cast<const uint4*>(in + base);
+            uint4* dst = reinterpret_cast<uint4*>(S.u.data);
+            for (uint32_t i = t; i < n / 16; i += THREADS) dst[i] = src[i];
+            for (uint32_t i = (n & ~15u) + t; i < n + 64; i += THREADS) S.u.data[i] = i < n ? in[base + i] : 0;
+        } else {
+            for (uint32_t i = t; i < n + 64; i += THREADS) S.u.data[i] = i < n ? in[base + i] : 0;
+        }
         for (int i = t; i < HSIZE; i += THREADS) S.head[i] = 0;
         for (int i = t; i < NLL + 2; i += THREADS) S.freq_ll[i] = 0;
         if (t < NDIST + 2) S.freq_d[t] = 0;
@@ -359,7 +399,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         {
             const uint32_t s0 = t * CRC_SEG, s1 = s0 + CRC_SEG < n ? s0 + CRC_SEG : n;
             uint32_t c = 0;
-            for (uint32_t i = s0; i < s1; ++i) c = (c >> 8) ^ S.crc_tab[(c ^ S.data[i]) & 255u];
+            for (uint32_t i = s0; i < s1; ++i) c = (c >> 8) ^ S.crc_tab[(c ^ S.u.data[i]) & 255u];
             S.crc_seg[t] = c;
         }
         __syncthreads();
@@ -370,7 +410,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             const uint32_t two = n > 32767;
             const uint32_t payload = n + (two ? 10 : 5);
             uint8_t* pl = slot + 18;
-            for (uint32_t i = t; i < n; i += THREADS) pl[5 + i] = S.data[i];
+            for (uint32_t i = t; i < n; i += THREADS) pl[5 + i] = S.u.data[i];
             if (t == 0) {
                 pl[0] = two ? 0 : 1;
                 pl[1] = n & 255;
@@ -391,7 +431,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         for (uint32_t k = 0; k < n_phase; ++k) {
             const uint32_t p = k * THREADS + t;
             const bool valid = p + 3 <= n;
-            const uint32_t h = valid ? hash3(S.data + p) : 0;
+            const uint32_t h = valid ? hash3(S.u.data + p) : 0;
             const uint32_t same = __match_any_sync(0xffffffffu, valid ? h : (0x80000000u | t));
             const uint32_t lower = same & ((1u << lane) - 1);
             uint32_t prev_p = NONE;
@@ -403,7 +443,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                     prev_p = hv ? hv - 1 : NONE;
                 }
             }
-            if (p < n) S.u.prev[p & WMASK] = static_cast<uint16_t>(prev_p);
+            if (p < n) S.prev[p & WMASK] = static_cast<uint16_t>(prev_p);
             __syncthreads();
             uint32_t bm = 0;
             if (valid) {
@@ -412,53 +452,60 @@ __global__ void __launch_bounds__(THREADS, 1)
                 if (lim >= 3) {
                     uint32_t q = prev_p, best_len = 2, best_d = 0;
                     for (int c = 0; c < chain && q != NONE && q < p && p - q <= WSIZE; ++c) {
-                        uint32_t L = 0;
-                        while (L < lim && S.data[q + L] == S.data[p + L]) ++L;
+                        // a candidate can only win if it also matches the
+                        // byte just past the current best
+                        const bool may = best_len >= lim || S.u.data[q + best_len] == S.u.data[p + best_len];
+                        const uint32_t L = may ? match_len(S.u.out, q, p, lim) : 0;
                         if (L > best_len) {
                             best_len = L;
                             best_d = p - q;
                             if (L == lim) break;
                         }
-                        const uint32_t nq = S.u.prev[q & WMASK];
+                        const uint32_t nq = S.prev[q & WMASK];
                         if (nq == NONE || nq >= q) break;
                         q = nq;
                     }
                     if (best_len >= 3) bm = (best_len << 16) | best_d;
                 }
             }
-            S.best[t] = bm;
+            if (p < n) best[p] = bm;
             if (valid) atomicMax(&S.head[h], p + 1);
             __syncthreads();
-            if (warp == 0) {
-                // greedy parse of sub-block s from its own start
-                const uint32_t s = k * (THREADS / SUB) + lane;
-                const uint32_t s0 = s * SUB;
-                if (s0 < n) {
-                    const uint32_t e = s0 + SUB < n ? s0 + SUB : n;
-                    uint32_t q = s0, cnt = 0;
-                    while (q < e) {
-                        const uint32_t m = S.best[q - k * THREADS];
-                        uint32_t tokv;
-                        if (m) {
-                            uint32_t sym, eb, ev;
-                            length_code(m >> 16, sym, eb, ev);
-                            atomicAdd(&S.freq_ll[sym], 1u);
-                            dist_code(m & 0xffff, sym, eb, ev);
-                            atomicAdd(&S.freq_d[sym], 1u);
-                            tokv = m;
-                            q += m >> 16;
-                        } else {
-                            tokv = S.data[q];
-                            atomicAdd(&S.freq_ll[tokv], 1u);
-                            ++q;
-                        }
-                        tok[s0 + cnt++] = tokv;
-                    }
-                    S.sub_cnt[s] = static_cast<uint8_t>(cnt);
-                }
-            }
-            __syncthreads();
         }
+        // ---- greedy parse: thread t takes sub-blocks SUBS_PER_THREAD t ..,
+        // each from its own start; lanes step together so symbol counts are
+        // aggregated per warp ----
+        {
+            uint32_t s = SUBS_PER_THREAD * t;
+            for (int j = 0; j < SUBS_PER_THREAD; ++j, ++s) {
+                const uint32_t s0 = s * SUB;
+                const bool mine = s0 < n;
+                const uint32_t e = mine ? (s0 + SUB < n ? s0 + SUB : n) : 0;
+                uint32_t q = s0, cnt = 0;
+                for (int step = 0; step < SUB; ++step) {
+                    const bool on = mine && q < e;
+                    uint32_t mv = 0, lit = 0;
+                    if (on) {
+                        mv = best[q];
+                        lit = S.u.data[q];
+                    }
+                    const bool is_match = on && mv != 0;
+                    uint32_t sym = lit, eb, ev, dsym = 0;
+                    if (is_match) {
+                        length_code(mv >> 16, sym, eb, ev);
+                        dist_code(mv & 0xffff, dsym, eb, ev);
+                    }
+                    warp_count(S.freq_ll, sym, on);
+                    warp_count(S.freq_d, dsym, is_match);
+                    if (on) {
+                        tok[s0 + cnt++] = is_match ? mv : lit;
+                        q += is_match ? (mv >> 16) : 1;
+                    }
+                }
+                if (mine) S.sub_cnt[s] = static_cast<uint8_t>(cnt);
+            }
+        }
+        __syncthreads();
         // ---- Huffman codes (warp 0) while warp 1 finishes the CRC ----
         if (warp == 1) crc_combine(S, n, lane);
         if (warp == 0) {
@@ -558,8 +605,18 @@ __global__ void __launch_bounds__(THREADS, 1)
         // ---- bit count per thread (sub-blocks 2t, 2t+1), offsets by scan ----
         const uint32_t n_sub = (n + SUB - 1) / SUB;
         uint32_t bits = 0;
-        for (uint32_t s = 2 * t; s < 2 * t + 2 && s < n_sub; ++s)
-            for (uint32_t i = 0, c = S.sub_cnt[s]; i < c; ++i) token_bits(S, tok[s * SUB + i], bits);
+        const uint32_t s_first = SUBS_PER_THREAD * t, s_last = s_first + SUBS_PER_THREAD;
+        for (uint32_t s = s_first; s < s_last && s < n_sub; ++s) {
+            const uint4* tv = reinterpret_cast<const uint4*>(tok + s * SUB);
+            const uint32_t c = S.sub_cnt[s];
+            for (uint32_t i = 0; i < c; i += 4) {
+                const uint4 v = tv[i >> 2];
+                token_bits(S, v.x, bits);
+                if (i + 1 < c) token_bits(S, v.y, bits);
+                if (i + 2 < c) token_bits(S, v.z, bits);
+                if (i + 3 < c) token_bits(S, v.w, bits);
+            }
+        }
         uint32_t off, sum;
         cub::BlockScan<uint32_t, THREADS>(S.scan).ExclusiveSum(bits, off, sum);
         const uint32_t total = S.hdr_bits + sum + S.len_ll[256];
@@ -567,23 +624,31 @@ __global__ void __launch_bounds__(THREADS, 1)
         const uint32_t stored_bytes = n + (n > 32767 ? 10 : 5);
         const bool use_dyn = dyn_bytes < stored_bytes;
         if (use_dyn) {
-            for (int i = t; i < static_cast<int>(WSIZE / 2); i += THREADS) S.u.out[i] = 0;
+            for (int i = t; i < static_cast<int>((BGZF_BLOCK + 64) / 4); i += THREADS) S.u.out[i] = 0;
             __syncthreads();
             for (uint32_t i = t; i < (S.hdr_bits + 31) / 32; i += THREADS) atomicOr(&S.u.out[i], S.hdr[i]);
             BitOut bo(S.u.out, S.hdr_bits + off);
-            for (uint32_t s = 2 * t; s < 2 * t + 2 && s < n_sub; ++s) {
-                for (uint32_t i = 0, c = S.sub_cnt[s]; i < c; ++i) {
-                    const uint32_t tv = tok[s * SUB + i];
-                    if ((tv >> 16) == 0) {
-                        bo.put(S.code_ll[tv], S.len_ll[tv]);
-                    } else {
-                        uint32_t sym, eb, ev;
-                        length_code(tv >> 16, sym, eb, ev);
-                        bo.put(S.code_ll[sym], S.len_ll[sym]);
-                        if (eb) bo.put(ev, eb);
-                        dist_code(tv & 0xffff, sym, eb, ev);
-                        bo.put(S.code_d[sym], S.len_d[sym]);
-                        if (eb) bo.put(ev, eb);
+            for (uint32_t s = s_first; s < s_last && s < n_sub; ++s) {
+                const uint4* tv4 = reinterpret_cast<const uint4*>(tok + s * SUB);
+                const uint32_t c = S.sub_cnt[s];
+                for (uint32_t i = 0; i < c; i += 4) {
+                    const uint4 v = tv4[i >> 2];
+                    const uint32_t four[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        if (i + k >= c) break;
+                        const uint32_t tv = four[k];
+                        if ((tv >> 16) == 0) {
+                            bo.put(S.code_ll[tv], S.len_ll[tv]);
+                        } else {
+                            uint32_t sym, eb, ev;
+                            length_code(tv >> 16, sym, eb, ev);
+                            bo.put(S.code_ll[sym], S.len_ll[sym]);
+                            if (eb) bo.put(ev, eb);
+                            dist_code(tv & 0xffff, sym, eb, ev);
+                            bo.put(S.code_d[sym], S.len_d[sym]);
+                            if (eb) bo.put(ev, eb);
+                        }
                     }
                 }
             }
@@ -601,7 +666,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         } else {
             const uint32_t two = n > 32767;
             uint8_t* pl = slot + 18;
-            for (uint32_t i = t; i < n; i += THREADS) pl[5 + i] = S.data[i];
+            for (uint32_t i = t; i < n; i += THREADS) pl[5 + i] = S.u.data[i];
             if (t == 0) {
                 pl[0] = two ? 0 : 1;
                 pl[1] = n & 255;
@@ -648,13 +713,22 @@ uint64_t bgzf_bound(uint64_t n_bytes) {
     return nb * (BGZF_MEMBER_MAX) + BGZF_EOF_BYTES;
 }
 
+namespace {
+// CTAs of the compression kernel: two per SM.
+uint64_t bgzf_grid(uint64_t nb, int sm_count) {
+    const uint64_t g = 2ull * static_cast<uint64_t>(sm_count > 0 ? sm_count : 148);
+    return nb < g ? nb : g;
+}
+}  // namespace
+
 size_t bgzf_scratch_bytes(uint64_t n_bytes, int sm_count) {
     const uint64_t nb = (n_bytes + BGZF_BLOCK - 1) / BGZF_BLOCK;
     size_t t = 0;
     cub::DeviceScan::InclusiveSum(nullptr, t, static_cast<const uint32_t*>(nullptr), static_cast<uint64_t*>(nullptr),
                                   static_cast<int64_t>(nb ? nb : 1));
-    const size_t grid = static_cast<size_t>(sm_count > 0 ? sm_count : 148);
-    return align256(grid * BGZF_BLOCK * 4) + align256(nb * 65536) + align256(nb * 4) + align256(nb * 8) +
+    const size_t grid = bgzf_grid(nb ? nb : 1, sm_count);
+    // tokens and matches per CTA, member slots, sizes, ends, scan temp
+    return 2 * align256(grid * BGZF_BLOCK * 4) + align256(nb * 65536) + align256(nb * 4) + align256(nb * 8) +
            align256(t) + 256;
 }
 
@@ -662,10 +736,13 @@ uint64_t bgzf_compress(const uint8_t* in, uint64_t n, int level, uint8_t* out, u
                        void* scratch, size_t scratch_bytes, int sm_count, cudaStream_t st, uint64_t* need,
                        int* launches, float* kernel_ms) {
     const uint64_t nb = (n + BGZF_BLOCK - 1) / BGZF_BLOCK;
-    const int grid = static_cast<int>(nb < static_cast<uint64_t>(sm_count) ? nb : sm_count);
+    const uint64_t gmax = bgzf_grid(nb ? nb : 1, sm_count);
+    const int grid = static_cast<int>(nb < gmax ? nb : gmax);
     uint8_t* s = static_cast<uint8_t*>(scratch);
     uint32_t* tok = reinterpret_cast<uint32_t*>(s);
-    s += align256(static_cast<size_t>(sm_count) * BGZF_BLOCK * 4);
+    s += align256(gmax * BGZF_BLOCK * 4);
+    uint32_t* best = reinterpret_cast<uint32_t*>(s);
+    s += align256(gmax * BGZF_BLOCK * 4);
     uint8_t* slots = s;
     s += align256(nb * 65536);
     uint32_t* sizes = reinterpret_cast<uint32_t*>(s);
@@ -689,7 +766,7 @@ uint64_t bgzf_compress(const uint8_t* in, uint64_t n, int level, uint8_t* out, u
             check_launch(cudaEventRecord(e0, st), "event");
         }
         bgzf_kernel<<<grid, THREADS, smem, st>>>(in, n, static_cast<uint32_t>(nb), level, chain_for(level), slots,
-                                                 sizes, tok);
+                                                 sizes, tok, best);
         check_launch(cudaGetLastError(), "bgzf_kernel");
         if (kernel_ms) check_launch(cudaEventRecord(e1, st), "event");
         check_launch(cub::DeviceScan::InclusiveSum(temp, tb, static_cast<const uint32_t*>(sizes), ends,
