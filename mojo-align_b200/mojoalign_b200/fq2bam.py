@@ -1,0 +1,285 @@
+"""FASTQ to coordinate-sorted, duplicate-marked BAM with every stage on the GPU.
+
+The .bam destination of map_fastq_fm_gpu (fq2bam-meth/src/linear_gpu_fm.mojo:
+1028-3341 with emit_bam, L2084): the reference parses FASTQ on the host
+(linear_fastq.mojo), maps each batch on the GPU, copies the outputs back,
+packs BAM records on the host (_emit_bam_from_batch), sorts and marks
+duplicates (gpu_sort_markdup, with host round trips), gathers the records in
+coordinate order and compresses them with zlib threads (bam_emit.BamWriter).
+Here the uncompressed FASTQ bytes are copied to the device once and nothing
+but the finished BGZF file comes back:
+
+    host: read / gunzip FASTQ  ->  HBM: split records (ma_fastq_parse_device)
+      -> mapper rows (ma_fastq_rows_device) -> map (ma_map_batch_device)
+      -> BAM records + tile metadata (ma_emit_bam_batch_device; the FASTQ
+         bytes of the batch are the arena) ... for every batch, then
+      -> sort + markdup (ma_sort_markdup_device)
+      -> header + sorted records (ma_gather_sorted_bam_device)
+      -> BGZF (ma_bgzf_compress_device)  ->  host: write the file.
+
+The file is the reference's: same header (BamWriter.__init__, bam_emit.py:
+312-356, with the canonical @SQ list of _open_bam_writer,
+linear_gpu_fm.mojo:91-125), same records in the same order and flags, BGZF
+pieces cut at the same 65280-byte boundaries.  At METHYLGRAPHER_BAM_LEVEL=0 the
+bytes are identical; at levels 1..9 the deflate data come from this library's
+coder and the members inflate to the same bytes.  The result does not depend
+on the batch size.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import gzip
+import os
+import struct
+
+import numpy as np
+
+from ._lib import check, lib, ma_bam_meta, ma_bam_tile, ma_fastq_arena, ma_fastq_records, ma_hits
+from .bam import META_FIELDS, canonical_rid_to_tid
+from .linear_fm import canonical_contig, fm_prefix_from_ref, select_device
+from .mapper import GpuContext, GpuIndex, MapResult, bs_mode
+from .params import FmParams
+
+SORT_CAP_ENV = ("METHYLGRAPHER_FM_SORT_CAP", 67108864)
+MAX_LEN_CAP = 1024
+REC_KEYS = ("name_off", "name_len", "seq_off", "seq_len", "qual_off", "qual_len")
+
+
+def _env(env, name, default):
+    v = env.get(name, "")
+    return v if v else default
+
+
+def bam_header(contigs, env=None) -> bytes:
+    """The uncompressed BAM header BamWriter writes (bam_emit.py:312-356) for
+    the canonical @SQ list of _open_bam_writer (linear_gpu_fm.mojo:91-125)."""
+    env = os.environ if env is None else env
+    names, lens, seen = [], [], set()
+    for c in contigs:
+        canon = canonical_contig(c.name)
+        if canon not in seen:
+            seen.add(canon)
+            names.append(canon)
+            lens.append(int(c.length))
+    rg = _env(env, "METHYLGRAPHER_RG_ID", "mojo1")
+    sm = _env(env, "METHYLGRAPHER_RG_SM", "sample")
+    lb = _env(env, "METHYLGRAPHER_RG_LB", "lib1")
+    pl = _env(env, "METHYLGRAPHER_RG_PL", "ILLUMINA")
+    lines = ["@HD\tVN:1.6\tSO:coordinate"]
+    lines += [f"@SQ\tSN:{n}\tLN:{ln}" for n, ln in zip(names, lens)]
+    lines.append(f"@RG\tID:{rg}\tSM:{sm}\tLB:{lb}\tPL:{pl}\tPU:{rg}")
+    lines.append("@PG\tID:MojoFq2bamMeth\tPN:MojoFq2bamMeth\tVN:0.1.0-mojo-fm")
+    text = ("\n".join(lines) + "\n").encode("ascii")
+    blob = bytearray(b"BAM\x01") + struct.pack("<i", len(text)) + text + struct.pack("<i", len(names))
+    for n, ln in zip(names, lens):
+        nb = n.encode("ascii") + b"\x00"
+        blob += struct.pack("<i", len(nb)) + nb + struct.pack("<i", ln)
+    return bytes(blob)
+
+
+class _Feed:
+    """Uncompressed bytes of one FASTQ file, in chunks (gzip by suffix, like
+    _looks_gz, linear_fastq.mojo:49-51)."""
+
+    def __init__(self, path: str, chunk: int):
+        low = path.lower()
+        self.fh = gzip.open(path, "rb") if (low.endswith(".gz") or low.endswith(".gzip")) else open(path, "rb")
+        self.buf = b""
+        self.eof = False
+        self.chunk = chunk
+
+    def fill(self):
+        while not self.eof and len(self.buf) < self.chunk:
+            b = self.fh.read(self.chunk - len(self.buf))
+            if not b:
+                self.eof = True
+                break
+            self.buf += b
+
+    def close(self):
+        self.fh.close()
+
+
+class _Grow:
+    """A device array that keeps its contents when it grows."""
+
+    def __init__(self, torch, dtype, dev):
+        self.torch, self.dtype, self.dev = torch, dtype, dev
+        self.t = torch.empty(0, dtype=dtype, device=dev)
+
+    def ensure(self, n):
+        if self.t.numel() >= n:
+            return self.t
+        new = self.torch.empty(max(n, 2 * self.t.numel()), dtype=self.dtype, device=self.dev)
+        if self.t.numel():
+            new[: self.t.numel()] = self.t
+        self.t = new
+        return new
+
+
+def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", bs_r1: str = "",
+                     bs_r2: str = "", params: FmParams | None = None, environ=None, kmer_k: int = 12,
+                     kmer3_k: int | None = None, ctx: GpuContext | None = None, index: GpuIndex | None = None,
+                     batch_pairs: int = 1 << 20, chunk_bytes: int = 256 << 20, level: int | None = None) -> int:
+    """FASTQ -> sorted, duplicate-marked BGZF BAM; returns the mapped records."""
+    import torch
+
+    env = os.environ if environ is None else environ
+    params = params or FmParams.from_env(env)
+    level = int(_env(env, "METHYLGRAPHER_BAM_LEVEL", "1")) if level is None else level
+    md_raw = _env(env, "METHYLGRAPHER_LINEAR_MARKDUP", "1").lower()
+    do_markdup = md_raw not in ("0", "false", "no", "off")
+    meta_cap = int(_env(env, SORT_CAP_ENV[0], str(SORT_CAP_ENV[1])))
+    own_ctx = ctx is None
+    ctx = ctx or GpuContext(select_device(device))
+    own_index = index is None
+    if index is None:
+        k3 = min(params.seed_len, 18) if kmer3_k is None else kmer3_k
+        index = GpuIndex(ctx, fm_prefix_from_ref(ref_fa), kmer_k=min(kmer_k, params.seed_len), kmer3_k=k3)
+    paired = len(str(fq2)) > 0
+    dev = torch.device("cuda", ctx.device)
+    stream = torch.cuda.Stream(device=dev)
+    sh = stream.cuda_stream
+    rg = _env(env, "METHYLGRAPHER_RG_ID", "mojo1").encode("ascii")
+    d_rg = torch.tensor(list(rg) or [0], dtype=torch.uint8, device=dev)
+    tids = canonical_rid_to_tid([c.name for c in index.contigs])
+    d_tids = torch.from_numpy(tids).to(dev)
+    header = bam_header(index.contigs, env)
+    p = params.to_c()
+    feeds = [_Feed(str(fq1), chunk_bytes)] + ([_Feed(str(fq2), chunk_bytes)] if paired else [])
+    meta = {k: _Grow(torch, torch.int64 if t == np.uint64 else torch.int32, dev) for k, t in META_FIELDS}
+    chunks, chunk_len = [], []
+    n_reads = n_mapped = 0
+    status = torch.zeros(3, dtype=torch.int64, device=dev)
+    o3 = (C.c_uint64 * 3)()
+    guard = torch.cuda.stream(stream)
+    guard.__enter__()
+    try:
+        while True:
+            for f in feeds:
+                f.fill()
+            if not feeds[0].buf:
+                break
+            # both mates' bytes in one device buffer: the batch's arena
+            sizes = [len(f.buf) for f in feeds]
+            d_buf = torch.empty(sum(sizes) + 16, dtype=torch.uint8, device=dev)
+            host = torch.frombuffer(bytearray(b"".join(f.buf for f in feeds)), dtype=torch.uint8)
+            d_buf[: host.numel()].copy_(host)
+            recs, rcs, counts = [], [], []
+            for m, f in enumerate(feeds):
+                base = sum(sizes[:m])
+                r = {k: torch.empty(batch_pairs, dtype=torch.int64 if k.endswith("off") else torch.int32,
+                                    device=dev) for k in REC_KEYS}
+                rc = ma_fastq_records(*[r[k].data_ptr() for k in REC_KEYS])
+                check(lib.ma_fastq_parse_device(ctx.handle, d_buf.data_ptr() + base, sizes[m], int(f.eof),
+                                                batch_pairs, base, C.byref(rc), o3, sh), ctx.handle)
+                recs.append(r)
+                rcs.append(rc)
+                counts.append((int(o3[0]), int(o3[1]), int(o3[2])))
+            n1 = counts[0][0]
+            if paired:
+                if counts[1][0] < n1:
+                    if feeds[1].eof:
+                        raise RuntimeError("paired FASTQ length mismatch (R2 ended early)")
+                    n1 = counts[1][0]  # R2's chunk ended first: take the pairs both hold
+            if n1 == 0:
+                if all(f.eof for f in feeds[:1]):
+                    break
+                raise RuntimeError("FASTQ record larger than the read chunk")
+            # bytes to drop from each feed: the span of its first n1 records
+            for m, f in enumerate(feeds):
+                used = counts[m][1]
+                if counts[m][0] != n1:
+                    check(lib.ma_fastq_parse_device(ctx.handle, d_buf.data_ptr() + sum(sizes[:m]), sizes[m],
+                                                    int(f.eof), n1, sum(sizes[:m]), C.byref(rcs[m]), o3, sh),
+                          ctx.handle)
+                    used = int(o3[1])
+                f.buf = f.buf[used:]
+            max_len = max(max(c[2] for c in counts), params.seed_len)
+            if max_len > MAX_LEN_CAP:
+                raise RuntimeError("read longer than FM base cap (1024)")
+            n_seq = n1 * (2 if paired else 1)
+            if n_reads + n_seq > meta_cap:
+                raise RuntimeError("FM sort cap exceeded; set METHYLGRAPHER_FM_SORT_CAP")
+            # mapper rows, R1 rows then R2 rows
+            rows = torch.empty(n_seq * max_len, dtype=torch.uint8, device=dev)
+            lens = torch.empty(n_seq, dtype=torch.int32, device=dev)
+            for m, r in enumerate(recs):
+                check(lib.ma_fastq_rows_device(ctx.handle, d_buf.data_ptr(), r["seq_off"].data_ptr(),
+                                               r["seq_len"].data_ptr(), n1, max_len,
+                                               rows.data_ptr() + m * n1 * max_len, lens.data_ptr() + m * n1 * 4,
+                                               sh), ctx.handle)
+            out = {f: torch.empty(n_seq, dtype=torch.int32, device=dev) for f in MapResult.FIELDS}
+            hits = ma_hits(*[out[f].data_ptr() for f in MapResult.FIELDS])
+            check(lib.ma_map_batch_device(ctx.handle, index.handle, rows.data_ptr(), lens.data_ptr(), n1,
+                                          int(paired), max_len, bs_mode(bs_r1), bs_mode(bs_r2), C.byref(p),
+                                          C.byref(hits), None, sh), ctx.handle)
+            # arena columns of the batch: R1 records then R2 records
+            cols = {k: torch.cat([r[k][:n1] for r in recs]) for k in REC_KEYS}
+            arena = ma_fastq_arena(d_buf.data_ptr(), int(sum(sizes)), cols["name_off"].data_ptr(),
+                                   cols["name_len"].data_ptr(), cols["seq_off"].data_ptr(),
+                                   cols["seq_len"].data_ptr(), cols["qual_off"].data_ptr(),
+                                   cols["qual_len"].data_ptr())
+            dm = {k: meta[k].ensure(n_reads + n_seq) for k, _ in META_FIELDS}
+            dmeta = ma_bam_meta(*[dm[k].data_ptr() for k, _ in META_FIELDS])
+            seq_total = int(cols["seq_len"].sum().item())
+            name_total = int(cols["name_len"].sum().item())
+            cap = n_seq * (64 + len(rg)) + name_total + 2 * seq_total
+            d_chunk = torch.empty(cap, dtype=torch.uint8, device=dev)
+            tile = ma_bam_tile(n_reads, n_mapped, 0, meta_cap, len(chunks))
+            check(lib.ma_emit_bam_batch_device(ctx.handle, C.byref(hits), n1, int(paired), C.byref(arena),
+                                               d_tids.data_ptr(), int(tids.size), d_rg.data_ptr(), len(rg),
+                                               d_chunk.data_ptr(), cap, C.byref(dmeta), C.byref(tile),
+                                               status.data_ptr(), sh), ctx.handle)
+            stream.synchronize()
+            st = status.cpu().numpy()
+            if st[2] or st[0] > cap:
+                raise RuntimeError("BAM batch buffer overflow")
+            chunks.append(d_chunk)
+            chunk_len.append(int(st[0]))
+            n_reads += n_seq
+            n_mapped += int(st[1])
+            del d_buf, rows, out, cols
+        # ---- sort, mark, gather, compress ----
+        total_records = int(sum(chunk_len))
+        d_stream = torch.empty(len(header) + total_records + 16, dtype=torch.uint8, device=dev)
+        d_stream[: len(header)].copy_(torch.frombuffer(bytearray(header), dtype=torch.uint8))
+        if n_reads:
+            perm = torch.empty(n_reads, dtype=torch.int32, device=dev)
+            is_dup = torch.empty(n_reads, dtype=torch.int32, device=dev)
+            mt = {k: meta[k].t for k, _ in META_FIELDS}
+            check(lib.ma_sort_markdup_device(ctx.handle, n_reads, mt["coord"].data_ptr(), mt["dhi"].data_ptr(),
+                                             mt["dlo"].data_ptr(), mt["score"].data_ptr(), mt["pair"].data_ptr(),
+                                             is_dup.data_ptr(), perm.data_ptr(), int(do_markdup), None, None, sh),
+                  ctx.handle)
+            d_ptrs = torch.tensor([c.data_ptr() for c in chunks], dtype=torch.int64, device=dev)
+            d_lens = torch.tensor(chunk_len, dtype=torch.int64, device=dev)
+            gst = torch.zeros(2, dtype=torch.int64, device=dev)
+            check(lib.ma_gather_sorted_bam_device(ctx.handle, n_reads, perm.data_ptr(), mt["rec"].data_ptr(),
+                                                  mt["len"].data_ptr(), is_dup.data_ptr(), int(do_markdup),
+                                                  d_ptrs.data_ptr(), d_lens.data_ptr(), len(chunks),
+                                                  d_stream.data_ptr() + len(header), total_records,
+                                                  gst.data_ptr(), sh), ctx.handle)
+            stream.synchronize()
+            g = gst.cpu().numpy()
+            if g[1] or int(g[0]) != total_records:
+                raise RuntimeError("sorted record stream does not match the tile")
+            del chunks
+        n_stream = len(header) + total_records
+        cap = int(lib.ma_bgzf_bound(n_stream))
+        d_out = torch.empty(cap, dtype=torch.uint8, device=dev)
+        got = C.c_uint64(0)
+        check(lib.ma_bgzf_compress_device(ctx.handle, d_stream.data_ptr(), n_stream, level, 1, d_out.data_ptr(), cap,
+                                          C.byref(got), sh), ctx.handle)
+        with open(out_bam, "wb") as fh:
+            fh.write(d_out[: got.value].cpu().numpy().tobytes())
+    finally:
+        stream.synchronize()
+        guard.__exit__(None, None, None)
+        for f in feeds:
+            f.close()
+        if own_index:
+            index.close()
+        if own_ctx:
+            ctx.close()
+    return n_mapped

@@ -13,8 +13,9 @@ follows fq2bam-meth/src/linear_gpu_fm.mojo:1028-3341 on its SAM path:
   _sam_with_rg_fm (L80-81) and the header of _write_sam_header_fm (L40-76);
 - the return value is the number of mapped records.
 
-BAM output (the reference's .bam path: GPU sort, markdup, BGZF) is not part
-of this library; a .bam destination raises.
+A .bam destination takes the reference's BAM path on the GPU end to end
+(mojoalign_b200.fq2bam.map_fastq_to_bam): record packing, coordinate sort,
+duplicate marking and BGZF.
 """
 from __future__ import annotations
 
@@ -164,8 +165,11 @@ def map_fastq_fm_gpu(ref_fa, fq1, out_sam, device: str = "auto", fq2: str = "", 
                      params: FmParams | None = None, environ=None, kmer_k: int = 12, kmer3_k: int | None = None,
                      ctx: GpuContext | None = None, index: GpuIndex | None = None) -> int:
     env = os.environ if environ is None else environ
-    if str(out_sam).lower().endswith(".bam"):
-        raise NotImplementedError("BAM output (GPU sort / markdup / BGZF) is outside this library; write SAM")
+    if str(out_sam).lower().endswith(".bam"):  # _path_is_bam, linear_gpu_fm.mojo:84-88
+        from .fq2bam import map_fastq_to_bam
+
+        return map_fastq_to_bam(ref_fa, fq1, out_sam, device, fq2, bs_r1, bs_r2, params, env, kmer_k, kmer3_k,
+                                ctx, index)
     params = params or FmParams.from_env(env)
     batch = env_int(READ_BATCH_ENV[0], READ_BATCH_ENV[1], env)
     own_ctx = ctx is None

@@ -13,7 +13,9 @@ below 2^29 (the BAM binning range; BamWriter rejects larger bins), qualities
 stored-strand orientation, since _pack_bam_aln swaps them itself on the
 reverse strand (L531-534).  The fixture stores the clips as _pack_bam_aln
 receives them.  Also records the reference's own unit vectors
-(tests/test_bam_emit.py:15-17).
+(tests/test_bam_emit.py:15-17) and the uncompressed header BamWriter writes
+for a two-contig reference with the default read group (BamWriter.__init__,
+L312-356, as _open_bam_writer calls it, linear_gpu_fm.mojo:91-125).
 """
 from __future__ import annotations
 
@@ -98,7 +100,10 @@ def main(root: Path) -> None:
                     [(0, 1), (0, 0), (16383, 16385), (100, 200), (1 << 17, (1 << 17) + 5), (0, 1 << 20),
                      (5, (1 << 23) + 1), (1 << 26, (1 << 26) + 1), (0, 1 << 29)]],
     }
-    OUT.write_text(json.dumps({"rg": RG, "unit": unit, "records": recs}, indent=0) + "\n")
+    header = b"".join(w._bgzf.parts[:header_parts])
+    OUT.write_text(json.dumps({"rg": RG, "unit": unit, "header": {"sq_names": ["chr1", "chr2"], "sq_lens": [1000, 2000],
+                                                               "blob": header.hex()},
+                               "records": recs}, indent=0) + "\n")
     print(f"wrote {OUT} ({len(recs)} records)")
 
 

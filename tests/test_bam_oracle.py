@@ -119,3 +119,14 @@ def test_failure_modes():
     oracle.emit_bam(_hits(rows), _arena(recs), 2, True, RID_TO_TID, b"r", n_reads=0, meta_cap=4)
     with pytest.raises(RuntimeError, match="BAM batch buffer overflow"):
         oracle.emit_bam(_hits(rows), _arena(recs), 4, False, RID_TO_TID, b"r", cap=100)
+
+
+def test_header_matches_reference_writer():
+    from mojoalign_b200.fq2bam import bam_header
+    from mojoalign_b200.mapper import Contig
+
+    g = _golden()["header"]
+    # bwa-meth contigs: f<name> / r<name> pairs collapse to one @SQ each
+    contigs = [Contig("r" + n, 0, ln) for n, ln in zip(g["sq_names"], g["sq_lens"])]
+    contigs += [Contig("f" + n, 0, ln) for n, ln in zip(g["sq_names"], g["sq_lens"])]
+    assert bam_header(contigs, {}).hex() == g["blob"]
