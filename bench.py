@@ -79,6 +79,8 @@ def parse_args():
                     "(its R1 file; 0 = skip)")
     ap.add_argument("--bgzf-level", type=int, default=1, help="BGZF level of the compression stage "
                     "(the reference's default, METHYLGRAPHER_BAM_LEVEL=1; -1 = skip)")
+    ap.add_argument("--fq2bam-pairs", type=int, default=2_000_000, help="read pairs of the FASTQ -> sorted BAM "
+                    "stage (0 = skip)")
     ap.add_argument("--tuning", default="", help="fixed kernel choice 'seed_kernel,stage1_endpoints,"
                     "stage2_blocks_per_sm,reg_level,stage1_max_rows,stage2_first_wave[,wave_endpoints,"
                     "wave_loci_per_read,wave_max_rounds,wave_growth]' instead of the autotuner")
@@ -587,6 +589,70 @@ def run_bgzf_stage(args, ctx, stream_bytes, local, peaks):
     }
 
 
+def run_fq2bam_stage(args, ctx, gi, rb, local, params):
+    """FASTQ files of the workload -> sorted, duplicate-marked BAM file through
+    map_fastq_to_bam (every stage on the GPU, files read and written on the
+    host), against the same path restated on the CPU from the oracle on a
+    sample (its mapping step dominates)."""
+    import gzip
+    import shutil
+    import sys as _sys
+
+    from mojoalign_b200.fq2bam import bam_header, map_fastq_to_bam
+
+    n = min(args.fq2bam_pairs, rb.n1)
+    d = Path(tempfile.mkdtemp(prefix="fq2bam_", dir=args.workdir))
+    try:
+        r1, r2 = d / "r1.fq", d / "r2.fq"
+        r1.write_bytes(fastq_text(rb, n, 1))
+        r2.write_bytes(fastq_text(rb, n, 2))
+        out = d / "out.bam"
+        fq_bytes = r1.stat().st_size + r2.stat().st_size
+        map_fastq_to_bam(None, r1, out, fq2=r2, bs_r1="C2T", bs_r2="G2A", params=params, environ={}, ctx=ctx,
+                         index=gi, level=args.bgzf_level if args.bgzf_level >= 0 else 1)
+        times = []
+        for _ in range(max(1, min(args.steps, 3))):
+            t = time.perf_counter()
+            mapped = map_fastq_to_bam(None, r1, out, fq2=r2, bs_r1="C2T", bs_r2="G2A", params=params, environ={},
+                                      ctx=ctx, index=gi, level=args.bgzf_level if args.bgzf_level >= 0 else 1)
+            times.append(time.perf_counter() - t)
+        wall = statistics.median(times)
+        bam_size = out.stat().st_size
+        # parity on a sample: the first pairs through both paths at level 0
+        ns = 20_000
+        s1, s2 = d / "s1.fq", d / "s2.fq"
+        s1.write_bytes(fastq_text(rb, ns, 1))
+        s2.write_bytes(fastq_text(rb, ns, 2))
+        so = d / "s.bam"
+        map_fastq_to_bam(None, s1, so, fq2=s2, bs_r1="C2T", bs_r2="G2A", params=params, environ={}, ctx=ctx,
+                         index=gi, level=0)
+        _sys.path.insert(0, str(ROOT / "tests"))
+        import fq2bam_oracle
+
+        t = time.perf_counter()
+        want = fq2bam_oracle.fq2bam(args._prefix, s1, s2, params.as_list(), 1, 2, bam_header(gi.contigs, {}),
+                                    b"mojo1", 0)
+        cpu_s = time.perf_counter() - t
+        same = so.read_bytes() == want
+        records = 2 * n
+        return {
+            "metric": "reads/s FASTQ -> sorted, duplicate-marked BAM", "value": round(records / wall, 1),
+            "unit": "reads/s", "s_per_run": round(wall, 3),
+            "config": {"workload": f"{n} PE 2x{READ_LEN} pairs of the workload as two FASTQ files "
+                                   f"({fq_bytes} bytes) -> one BAM file", "bam_bytes": bam_size,
+                       "bgzf_level": args.bgzf_level if args.bgzf_level >= 0 else 1, "mapped_records": mapped},
+            "e2e": {"value": round(records / wall, 1), "unit": "reads/s", "h2d_bytes_per_step": fq_bytes,
+                    "d2h_bytes_per_step": bam_size,
+                    "timing": "host wall clock of the whole call: file reads, every GPU stage, the file write"},
+            "cpu_baseline": {"value": round(2 * ns / cpu_s, 1), "unit": "reads/s", "cores": os.cpu_count(),
+                             "kind": "port", "sample": f"the first {ns} pairs through the oracle pipeline "
+                                                       f"(mapping on all cores), {cpu_s:.2f} s"},
+            "parity": {"reads": 2 * ns, "bam_file_identical_at_level0": bool(same)},
+        }
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
 def run_sort_stage(args, ctx, rb, res, local, peaks):
     """Coordinate sort + duplicate marking + sorted gather of one BAM tile
     made of --sort-batches emitted batches: device-resident throughput, the
@@ -930,6 +996,10 @@ def run_ours(args, rank, world, local):
                 torch.cuda.empty_cache()
                 line["stages"]["bgzf"] = run_bgzf_stage(args, ctx, args._sorted_stream, local, peaks)
                 del args._sorted_stream
+    if rank == 0 and world == 1 and args.fq2bam_pairs > 0:
+        torch.cuda.empty_cache()
+        args._prefix = prefix
+        line.setdefault("stages", {})["fq2bam"] = run_fq2bam_stage(args, ctx, gi, rb, local, params)
     if rank == 0 and world == 1 and args.fastq_pairs > 0:
         torch.cuda.empty_cache()
         line.setdefault("stages", {})["fastq_split"] = run_fastq_stage(args, ctx, rb, local, peaks)
