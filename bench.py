@@ -610,11 +610,12 @@ def run_fq2bam_stage(args, ctx, gi, rb, local, params):
         fq_bytes = r1.stat().st_size + r2.stat().st_size
         map_fastq_to_bam(None, r1, out, fq2=r2, bs_r1="C2T", bs_r2="G2A", params=params, environ={}, ctx=ctx,
                          index=gi, level=args.bgzf_level if args.bgzf_level >= 0 else 1)
-        times = []
+        times, phases = [], {}
         for _ in range(max(1, min(args.steps, 3))):
             t = time.perf_counter()
             mapped = map_fastq_to_bam(None, r1, out, fq2=r2, bs_r1="C2T", bs_r2="G2A", params=params, environ={},
-                                      ctx=ctx, index=gi, level=args.bgzf_level if args.bgzf_level >= 0 else 1)
+                                      ctx=ctx, index=gi, level=args.bgzf_level if args.bgzf_level >= 0 else 1,
+                                      stats=phases)
             times.append(time.perf_counter() - t)
         wall = statistics.median(times)
         bam_size = out.stat().st_size

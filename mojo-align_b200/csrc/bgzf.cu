@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(THREADS, 2)
         if (t < NCL + 1) S.freq_cl[t] = 0;
         for (int i = t; i < 112; i += THREADS) S.hdr[i] = 0;
         __syncthreads();
-        // CRC remainders of 64-byte segments (register starting at 0)
+        // CRC remainders of 128-byte segments (register starting at 0)
         {
             const uint32_t s0 = t * CRC_SEG, s1 = s0 + CRC_SEG < n ? s0 + CRC_SEG : n;
             uint32_t c = 0;
@@ -602,7 +602,7 @@ __global__ void __launch_bounds__(THREADS, 2)
             }
         }
         __syncthreads();
-        // ---- bit count per thread (sub-blocks 2t, 2t+1), offsets by scan ----
+        // ---- bit count per thread (its sub-blocks), offsets by scan ----
         const uint32_t n_sub = (n + SUB - 1) / SUB;
         uint32_t bits = 0;
         const uint32_t s_first = SUBS_PER_THREAD * t, s_last = s_first + SUBS_PER_THREAD;

@@ -31,6 +31,7 @@ import ctypes as C
 import gzip
 import os
 import struct
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -78,23 +79,31 @@ def bam_header(contigs, env=None) -> bytes:
 
 
 class _Feed:
-    """Uncompressed bytes of one FASTQ file, in chunks (gzip by suffix, like
-    _looks_gz, linear_fastq.mojo:49-51)."""
+    """Uncompressed bytes of one FASTQ file in a pinned host buffer (gzip by
+    suffix, like _looks_gz, linear_fastq.mojo:49-51): fill() tops the buffer
+    up to its capacity, consume(n) drops the first n bytes."""
 
-    def __init__(self, path: str, chunk: int):
+    def __init__(self, path: str, chunk: int, torch):
         low = path.lower()
         self.fh = gzip.open(path, "rb") if (low.endswith(".gz") or low.endswith(".gzip")) else open(path, "rb")
-        self.buf = b""
+        self.pin = torch.empty(chunk, dtype=torch.uint8, pin_memory=True).numpy()
+        self.len = 0
         self.eof = False
-        self.chunk = chunk
 
     def fill(self):
-        while not self.eof and len(self.buf) < self.chunk:
-            b = self.fh.read(self.chunk - len(self.buf))
-            if not b:
+        mv = memoryview(self.pin)
+        while not self.eof and self.len < self.pin.size:
+            k = self.fh.readinto(mv[self.len:])
+            if not k:
                 self.eof = True
                 break
-            self.buf += b
+            self.len += k
+
+    def consume(self, n: int):
+        rest = self.len - n
+        if rest > 0 and n > 0:
+            self.pin[:rest] = self.pin[n:self.len].copy()
+        self.len = max(rest, 0)
 
     def close(self):
         self.fh.close()
@@ -120,9 +129,17 @@ class _Grow:
 def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", bs_r1: str = "",
                      bs_r2: str = "", params: FmParams | None = None, environ=None, kmer_k: int = 12,
                      kmer3_k: int | None = None, ctx: GpuContext | None = None, index: GpuIndex | None = None,
-                     batch_pairs: int = 1 << 20, chunk_bytes: int = 256 << 20, level: int | None = None) -> int:
-    """FASTQ -> sorted, duplicate-marked BGZF BAM; returns the mapped records."""
+                     batch_pairs: int = 1 << 20, chunk_bytes: int = 512 << 20, level: int | None = None,
+                     stats: dict | None = None) -> int:
+    """FASTQ -> sorted, duplicate-marked BGZF BAM; returns the mapped records.
+    `stats`, when given, receives seconds spent per phase (waiting for FASTQ
+    bytes, the per-batch device work, sort + gather, BGZF, writing)."""
+    import time
+
     import torch
+
+    tm = {"read_wait": 0.0, "batches": 0.0, "sort_gather": 0.0, "bgzf": 0.0, "write": 0.0}
+    t_start = time.perf_counter()
 
     env = os.environ if environ is None else environ
     params = params or FmParams.from_env(env)
@@ -146,7 +163,9 @@ def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", 
     d_tids = torch.from_numpy(tids).to(dev)
     header = bam_header(index.contigs, env)
     p = params.to_c()
-    feeds = [_Feed(str(fq1), chunk_bytes)] + ([_Feed(str(fq2), chunk_bytes)] if paired else [])
+    feeds = [_Feed(str(fq1), chunk_bytes, torch)] + ([_Feed(str(fq2), chunk_bytes, torch)] if paired else [])
+    pool = ThreadPoolExecutor(max_workers=1)  # reads the next chunk while the GPU maps this one
+    pending = None
     meta = {k: _Grow(torch, torch.int64 if t == np.uint64 else torch.int32, dev) for k, t in META_FIELDS}
     chunks, chunk_len = [], []
     n_reads = n_mapped = 0
@@ -155,16 +174,24 @@ def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", 
     guard = torch.cuda.stream(stream)
     guard.__enter__()
     try:
+        for f in feeds:
+            f.fill()
         while True:
-            for f in feeds:
-                f.fill()
-            if not feeds[0].buf:
+            t0 = time.perf_counter()
+            if pending is not None:
+                pending.result()
+                pending = None
+            tm["read_wait"] += time.perf_counter() - t0
+            t0 = time.perf_counter()
+            if not feeds[0].len:
                 break
             # both mates' bytes in one device buffer: the batch's arena
-            sizes = [len(f.buf) for f in feeds]
+            sizes = [f.len for f in feeds]
             d_buf = torch.empty(sum(sizes) + 16, dtype=torch.uint8, device=dev)
-            host = torch.frombuffer(bytearray(b"".join(f.buf for f in feeds)), dtype=torch.uint8)
-            d_buf[: host.numel()].copy_(host)
+            off = 0
+            for f in feeds:
+                d_buf[off:off + f.len].copy_(torch.from_numpy(f.pin[: f.len]), non_blocking=True)
+                off += f.len
             recs, rcs, counts = [], [], []
             for m, f in enumerate(feeds):
                 base = sum(sizes[:m])
@@ -186,15 +213,25 @@ def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", 
                 if all(f.eof for f in feeds[:1]):
                     break
                 raise RuntimeError("FASTQ record larger than the read chunk")
-            # bytes to drop from each feed: the span of its first n1 records
+            # bytes to drop from each feed: the span of its first n1 records;
+            # the host buffers are free once the copies above are done
+            used = []
             for m, f in enumerate(feeds):
-                used = counts[m][1]
+                u = counts[m][1]
                 if counts[m][0] != n1:
                     check(lib.ma_fastq_parse_device(ctx.handle, d_buf.data_ptr() + sum(sizes[:m]), sizes[m],
                                                     int(f.eof), n1, sum(sizes[:m]), C.byref(rcs[m]), o3, sh),
                           ctx.handle)
-                    used = int(o3[1])
-                f.buf = f.buf[used:]
+                    u = int(o3[1])
+                used.append(u)
+            stream.synchronize()
+
+            def refill(used=used):
+                for f, u in zip(feeds, used):
+                    f.consume(u)
+                    f.fill()
+
+            pending = pool.submit(refill)
             max_len = max(max(c[2] for c in counts), params.seed_len)
             if max_len > MAX_LEN_CAP:
                 raise RuntimeError("read longer than FM base cap (1024)")
@@ -240,7 +277,9 @@ def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", 
             n_reads += n_seq
             n_mapped += int(st[1])
             del d_buf, rows, out, cols
+            tm["batches"] += time.perf_counter() - t0
         # ---- sort, mark, gather, compress ----
+        t0 = time.perf_counter()
         total_records = int(sum(chunk_len))
         d_stream = torch.empty(len(header) + total_records + 16, dtype=torch.uint8, device=dev)
         d_stream[: len(header)].copy_(torch.frombuffer(bytearray(header), dtype=torch.uint8))
@@ -265,15 +304,28 @@ def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", 
             if g[1] or int(g[0]) != total_records:
                 raise RuntimeError("sorted record stream does not match the tile")
             del chunks
+        tm["sort_gather"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
         n_stream = len(header) + total_records
         cap = int(lib.ma_bgzf_bound(n_stream))
         d_out = torch.empty(cap, dtype=torch.uint8, device=dev)
         got = C.c_uint64(0)
         check(lib.ma_bgzf_compress_device(ctx.handle, d_stream.data_ptr(), n_stream, level, 1, d_out.data_ptr(), cap,
                                           C.byref(got), sh), ctx.handle)
+        tm["bgzf"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        host_out = torch.empty(got.value, dtype=torch.uint8, pin_memory=True)
+        host_out.copy_(d_out[: got.value])
         with open(out_bam, "wb") as fh:
-            fh.write(d_out[: got.value].cpu().numpy().tobytes())
+            fh.write(memoryview(host_out.numpy()))
+        tm["write"] = time.perf_counter() - t0
+        tm["total"] = time.perf_counter() - t_start
+        if stats is not None:
+            stats.update({k: round(v, 4) for k, v in tm.items()})
     finally:
+        if pending is not None:
+            pending.exception()
+        pool.shutdown(wait=True)
         stream.synchronize()
         guard.__exit__(None, None, None)
         for f in feeds:
