@@ -638,7 +638,7 @@ def run_fq2bam_stage(args, ctx, gi, rb, local, params):
         records = 2 * n
         return {
             "metric": "reads/s FASTQ -> sorted, duplicate-marked BAM", "value": round(records / wall, 1),
-            "unit": "reads/s", "s_per_run": round(wall, 3),
+            "unit": "reads/s", "s_per_run": round(wall, 3), "phases_s": phases,
             "config": {"workload": f"{n} PE 2x{READ_LEN} pairs of the workload as two FASTQ files "
                                    f"({fq_bytes} bytes) -> one BAM file", "bam_bytes": bam_size,
                        "bgzf_level": args.bgzf_level if args.bgzf_level >= 0 else 1, "mapped_records": mapped},
