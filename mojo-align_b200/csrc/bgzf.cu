@@ -123,65 +123,97 @@ __constant__ uint8_t CL_ORDER[NCL] = {16, 17, 18, 0, 8, 7, 9, 6, 10, 5, 11, 4, 1
 
 // Scratch of the Huffman builder (one warp).
 struct HuffScratch {
-    uint32_t weight[2 * NLL];
-    uint16_t parent[2 * NLL];
-    uint16_t sorted[NLL];  // symbols by ascending (count, symbol)
-    uint8_t depth[2 * NLL];
-    uint16_t bl_count[16 + 8];
+    uint32_t a[NLL];         // sorted weights -> in-place tree -> depths
+    uint16_t sorted[NLL];    // symbols by ascending (count, symbol)
+    uint32_t bl_count[16 + 8];
+    uint32_t next_code[16];
 };
 
+constexpr int RANK_SLOTS = (NLL + 31) / 32;  // symbols per lane in the rank pass
+
+__device__ __forceinline__ uint32_t A_len(uint32_t depth, int maxbits) {
+    return depth > static_cast<uint32_t>(maxbits) ? maxbits : depth;
+}
+
 // Code lengths <= maxbits for counts freq[0, n) (at least two nonzero).
-// Called by a whole warp; lane 0 does the sequential parts.
+// Called by a whole warp.  The symbols are ranked by (count, symbol) with
+// every lane holding its symbols in registers while the counts stream past;
+// the optimal lengths come from the in-place algorithm of Moffat and
+// Katajainen (1995) on the sorted counts (lane 0): the counts array becomes
+// the tree (parent indices), then internal depths, then leaf depths; lengths
+// above maxbits are pulled up and the Kraft sum restored by splitting
+// shorter codes, and the lengths are dealt out again with the heaviest
+// symbols taking the shortest.
 __device__ void huff_lengths(const uint32_t* freq, int n, int maxbits, uint8_t* len, HuffScratch& hs, int lane) {
-    // rank every used symbol by (count, symbol)
+    uint32_t f[RANK_SLOTS], r[RANK_SLOTS];
     int used = 0;
-    for (int i = lane; i < n; i += 32) len[i] = 0;
-    for (int base = 0; base < n; base += 32) {
-        const int i = base + lane;
-        const bool u = i < n && freq[i] != 0;
-        used += __popc(__ballot_sync(0xffffffffu, u));
+#pragma unroll
+    for (int k = 0; k < RANK_SLOTS; ++k) {
+        const int i = lane + 32 * k;
+        f[k] = i < n ? freq[i] : 0;
+        r[k] = 0;
+        used += __popc(__ballot_sync(0xffffffffu, f[k] != 0));
+        if (i < n) len[i] = 0;
     }
-    for (int i = lane; i < n; i += 32) {
-        const uint32_t f = freq[i];
-        if (!f) continue;
-        int r = 0;
-        for (int j = 0; j < n; ++j) {
-            const uint32_t g = freq[j];
-            r += g && (g < f || (g == f && j < i));
-        }
-        hs.sorted[r] = static_cast<uint16_t>(i);
+    for (int j = 0; j < n; ++j) {
+        const uint32_t g = freq[j];
+        if (!g) continue;
+#pragma unroll
+        for (int k = 0; k < RANK_SLOTS; ++k) r[k] += g < f[k] || (g == f[k] && j < lane + 32 * k);
     }
+#pragma unroll
+    for (int k = 0; k < RANK_SLOTS; ++k)
+        if (f[k]) hs.sorted[r[k]] = static_cast<uint16_t>(lane + 32 * k);
+    if (lane < 16 + 8) hs.bl_count[lane] = 0;
+    __syncwarp();
+    const int m = used;
+    for (int k = lane; k < m; k += 32) hs.a[k] = freq[hs.sorted[k]];
     __syncwarp();
     if (lane == 0) {
-        const int m = used;
-        for (int k = 0; k < m; ++k) hs.weight[k] = freq[hs.sorted[k]];
-        // two-queue merge: leaves 0..m-1 in order, internal nodes m.. in
-        // creation order (their weights never decrease)
-        int ia = 0, ib = m, next = m;
-        for (int step = 0; step < m - 1; ++step) {
-            int pick[2];
-            for (int t = 0; t < 2; ++t) {
-                const bool leaf = ia < m && (ib >= next || hs.weight[ia] <= hs.weight[ib]);
-                pick[t] = leaf ? ia++ : ib++;
+        uint32_t* A = hs.a;
+        // tree: A[t] = weight of internal node t; a consumed node's slot
+        // takes its parent's index
+        A[0] += A[1];
+        int root = 0, leaf = 2;
+        for (int next = 1; next < m - 1; ++next) {
+            if (leaf >= m || A[root] < A[leaf]) {
+                A[next] = A[root];
+                A[root++] = next;
+            } else {
+                A[next] = A[leaf++];
             }
-            hs.weight[next] = hs.weight[pick[0]] + hs.weight[pick[1]];
-            hs.parent[pick[0]] = hs.parent[pick[1]] = static_cast<uint16_t>(next);
-            ++next;
+            if (leaf >= m || (root < next && A[root] < A[leaf])) {
+                A[next] += A[root];
+                A[root++] = next;
+            } else {
+                A[next] += A[leaf++];
+            }
         }
-        const int root = next - 1;
-        hs.depth[root] = 0;
-        for (int v = root - 1; v >= 0; --v) hs.depth[v] = hs.depth[hs.parent[v]] + 1;
-        // lengths per level, limited to maxbits: every code deeper than
-        // maxbits moves up to maxbits; then while the Kraft sum exceeds one,
-        // a code at maxbits goes away and a shorter code splits into two
-        // one level down, which lowers the sum by exactly 2^-maxbits
-        for (int b = 0; b <= maxbits; ++b) hs.bl_count[b] = 0;
-        for (int k = 0; k < m; ++k) {
-            const int d = hs.depth[k] > maxbits ? maxbits : hs.depth[k];
-            ++hs.bl_count[d];
+        // internal depths
+        A[m - 2] = 0;
+        for (int t = m - 3; t >= 0; --t) A[t] = A[A[t]] + 1;
+        // leaf depths, heaviest leaf (index m - 1) first
+        int avail = 1, nused = 0, depth = 0, rt = m - 2, nx = m - 1;
+        while (avail > 0) {
+            while (rt >= 0 && static_cast<int>(A[rt]) == depth) {
+                ++nused;
+                --rt;
+            }
+            while (avail > nused) {
+                A[nx--] = depth;
+                --avail;
+            }
+            avail = 2 * nused;
+            ++depth;
+            nused = 0;
         }
+    }
+    __syncwarp();
+    for (int k = lane; k < m; k += 32) atomicAdd(&hs.bl_count[A_len(hs.a[k], maxbits)], 1u);
+    __syncwarp();
+    if (lane == 0) {
         uint32_t kraft = 0;
-        for (int b = 1; b <= maxbits; ++b) kraft += static_cast<uint32_t>(hs.bl_count[b]) << (maxbits - b);
+        for (int b = 1; b <= maxbits; ++b) kraft += hs.bl_count[b] << (maxbits - b);
         while (kraft > (1u << maxbits)) {
             --hs.bl_count[maxbits];
             for (int b = maxbits - 1; b > 0; --b) {
@@ -193,31 +225,49 @@ __device__ void huff_lengths(const uint32_t* freq, int n, int maxbits, uint8_t* 
             }
             --kraft;
         }
-        // most frequent symbols get the shortest codes
-        int k = m - 1;
-        for (int b = 1; b <= maxbits; ++b)
-            for (int c = 0; c < hs.bl_count[b]; ++c) len[hs.sorted[k--]] = static_cast<uint8_t>(b);
+    }
+    __syncwarp();
+    // the rank-th heaviest symbol takes the rank-th shortest length
+    for (int k = lane; k < m; k += 32) {
+        const uint32_t rank = m - 1 - k;
+        uint32_t cum = 0;
+        int b = 1;
+        for (; b < maxbits; ++b) {
+            cum += hs.bl_count[b];
+            if (rank < cum) break;
+        }
+        len[hs.sorted[k]] = static_cast<uint8_t>(b);
     }
     __syncwarp();
 }
 
-// Canonical codes, bit-reversed for LSB-first output (RFC 1951 3.2.2).
-__device__ void huff_codes(const uint8_t* len, int n, uint16_t* code, int lane) {
+// Canonical codes, bit-reversed for LSB-first output (RFC 1951 3.2.2):
+// symbol i of length l gets next_code[l] plus the number of earlier
+// symbols of length l, counted 32 symbols at a time with __match_any_sync.
+__device__ void huff_codes(const uint8_t* len, int n, uint16_t* code, HuffScratch& hs, int lane) {
+    if (lane < 16) hs.bl_count[lane] = 0;
+    __syncwarp();
+    for (int i = lane; i < n; i += 32)
+        if (len[i]) atomicAdd(&hs.bl_count[len[i]], 1u);
+    __syncwarp();
     if (lane == 0) {
-        uint16_t count[16] = {0}, next[16];
-        for (int i = 0; i < n; ++i) ++count[len[i]];
-        count[0] = 0;
         uint32_t c = 0;
         for (int b = 1; b < 16; ++b) {
-            c = (c + count[b - 1]) << 1;
-            next[b] = static_cast<uint16_t>(c);
-        }
-        for (int i = 0; i < n; ++i) {
-            const int l = len[i];
-            code[i] = l ? static_cast<uint16_t>(__brev(next[l]++) >> (32 - l)) : 0;
+            c = (c + (b > 1 ? hs.bl_count[b - 1] : 0)) << 1;
+            hs.next_code[b] = c;
         }
     }
     __syncwarp();
+    for (int base = 0; base < n; base += 32) {
+        const int i = base + lane;
+        const uint32_t l = i < n ? len[i] : 0;
+        const uint32_t peers = __match_any_sync(0xffffffffu, l);
+        const uint32_t c = (l ? hs.next_code[l] : 0) + __popc(peers & ((1u << lane) - 1));
+        if (i < n) code[i] = l ? static_cast<uint16_t>(__brev(c) >> (32 - l)) : 0;
+        __syncwarp();
+        if (l && lane == 31 - __clz(peers)) hs.next_code[l] += __popc(peers);
+        __syncwarp();
+    }
 }
 
 // Everything one CTA keeps for the piece it compresses (under half of an
@@ -526,8 +576,8 @@ __global__ void __launch_bounds__(THREADS, 2)
             __syncwarp();
             huff_lengths(S.freq_ll, NLL, 15, S.len_ll, S.hs, lane);
             huff_lengths(S.freq_d, NDIST, 15, S.len_d, S.hs, lane);
-            huff_codes(S.len_ll, NLL, S.code_ll, lane);
-            huff_codes(S.len_d, NDIST, S.code_d, lane);
+            huff_codes(S.len_ll, NLL, S.code_ll, S.hs, lane);
+            huff_codes(S.len_d, NDIST, S.code_d, S.hs, lane);
             if (lane == 0) {
                 int nl = NLL, nd = NDIST;
                 while (nl > 257 && !S.len_ll[nl - 1]) --nl;
@@ -579,7 +629,7 @@ __global__ void __launch_bounds__(THREADS, 2)
             }
             __syncwarp();
             huff_lengths(S.freq_cl, NCL, 7, S.len_cl, S.hs, lane);
-            huff_codes(S.len_cl, NCL, S.code_cl, lane);
+            huff_codes(S.len_cl, NCL, S.code_cl, S.hs, lane);
             if (lane == 0) {
                 const uint32_t nl = S.nl_nd[0], nd = S.nl_nd[1];
                 int hclen = NCL;
