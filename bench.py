@@ -318,7 +318,7 @@ def run_bam_stage(args, ctx, rb, res, local, peaks):
     d_meta = {k: torch.empty(n_seq, dtype=torch.int64 if t_ == np.uint64 else torch.int32, device=dev)
               for k, t_ in META_FIELDS}
     d_status = torch.zeros(3, dtype=torch.int64, device=dev)
-    tile = BamTile(meta_cap=n_seq)
+    tile = BamTile(meta_cap=n_seq, host_meta=False)
     torch.cuda.synchronize()
     stream = torch.cuda.Stream(device=dev)  # a handle of 0 would select the context's own stream
 
@@ -674,7 +674,7 @@ def run_sort_stage(args, ctx, rb, res, local, peaks):
     d_meta = {k: torch.empty(n, dtype=torch.int64 if t_ == np.uint64 else torch.int32, device=dev)
               for k, t_ in META_FIELDS}
     d_status = torch.zeros(3, dtype=torch.int64, device=dev)
-    tile = BamTile(meta_cap=n, meta={"unused": None})
+    tile = BamTile(meta_cap=n, host_meta=False)
     chunks, chunk_len = [], []
     rec_cap = 4 + 32 + BAM_NAME_LEN + 1 + 12 + (READ_LEN + 1) // 2 + READ_LEN + 8 + len(BAM_RG)
     for c in range(nb):

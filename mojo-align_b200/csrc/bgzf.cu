@@ -16,16 +16,18 @@
 //     earlier phases through a head table, inside its warp through
 //     __match_any_sync) in a 32 KB ring of 16-bit links, and follows up to
 //     `chain` links for its longest match (deflate's 32 KB window, 258
-//     bytes at most).  Each warp-wide 32-byte sub-block is parsed greedily
-//     by one thread from its own start, matches cut at the sub-block's end,
-//     so the parse needs no cross-thread order.
+//     bytes at most).  Each 32-byte sub-block (one warp's positions of a
+//     phase) is parsed greedily from its own start right after it is matched,
+//     the warp walking it together with shuffles; matches are cut at the
+//     sub-block's end, so the parse needs no cross-warp order.
 //   * Huffman: dynamic codes (literal/length, distance, code-length
 //     alphabets) built per piece: symbols ranked by (count, symbol) over a
 //     warp, Huffman merge with two queues, lengths limited to 15 (7) bits by
 //     moving codes down one level at a time until the Kraft sum fits,
 //     canonical codes (RFC 1951 3.2.2).
-//   * Bits: every parse thread knows its bit count; a block scan gives its
-//     offset and the thread ORs its codes into a shared-memory word buffer.
+//   * Bits: every thread counts the bits of its sub-blocks' tokens; a block
+//     scan gives its offset and the thread ORs its codes into a shared-memory
+//     word buffer.
 //     A piece whose dynamic coding is not smaller than storing it is stored.
 //
 // Level 0 writes stored blocks exactly as zlib does for one compress +
@@ -46,6 +48,7 @@ constexpr int THREADS = 512;                   // two CTAs per SM
 constexpr int SUB = 32;                        // bytes per parse sub-block
 constexpr int NSUB = (BGZF_BLOCK + SUB - 1) / SUB;  // 2040
 constexpr int SUBS_PER_THREAD = (NSUB + THREADS - 1) / THREADS;  // 4
+static_assert(SUB == 32, "a parse sub-block is one warp's positions");
 constexpr int WBITS = 13;
 constexpr uint32_t WSIZE = 1u << WBITS;        // match window (deflate allows up to 32 KB)
 constexpr uint32_t WMASK = WSIZE - 1;
@@ -411,7 +414,7 @@ __device__ void write_frame(uint8_t* slot, uint32_t payload, uint32_t crc, uint3
 
 __global__ void __launch_bounds__(THREADS, 2)
     bgzf_kernel(const uint8_t* in, uint64_t n_total, uint32_t n_blocks, int level, int chain, uint8_t* slots,
-                uint32_t* sizes, uint32_t* tok_all, uint32_t* best_all) {
+                uint32_t* sizes, uint32_t* tok_all) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     Smem& S = *reinterpret_cast<Smem*>(smem_raw);
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -425,7 +428,6 @@ __global__ void __launch_bounds__(THREADS, 2)
         S.x_lane = gf2_xpow(8ull * (THREADS / 32) * CRC_SEG);
     }
     uint32_t* tok = tok_all + static_cast<size_t>(blockIdx.x) * BGZF_BLOCK;
-    uint32_t* best = best_all + static_cast<size_t>(blockIdx.x) * BGZF_BLOCK;
     for (uint32_t b = blockIdx.x; b < n_blocks; b += gridDim.x) {
         const uint64_t base = static_cast<uint64_t>(b) * BGZF_BLOCK;
         const uint32_t n = static_cast<uint32_t>(n_total - base < BGZF_BLOCK ? n_total - base : BGZF_BLOCK);
@@ -518,44 +520,37 @@ __global__ void __launch_bounds__(THREADS, 2)
                     if (best_len >= 3) bm = (best_len << 16) | best_d;
                 }
             }
-            if (p < n) best[p] = bm;
             if (valid) atomicMax(&S.head[h], p + 1);
+            // greedy parse of this warp's 32-byte sub-block, which the warp's
+            // lanes just matched: the walk position is warp-uniform, so the
+            // lane at that position hands over its match by shuffle; token j
+            // ends up in lane j
+            const uint32_t s0 = k * THREADS + 32 * warp;
+            if (s0 < n) {
+                const uint32_t e = n - s0 < SUB ? n - s0 : SUB;
+                const uint32_t lit = p < n ? S.u.data[p] : 0;
+                uint32_t q = 0, cnt = 0, mine = 0;
+                while (q < e) {
+                    const uint32_t m = __shfl_sync(0xffffffffu, bm, q);
+                    const uint32_t tv = m ? m : __shfl_sync(0xffffffffu, lit, q);
+                    if (lane == cnt) mine = tv;
+                    ++cnt;
+                    q += m ? (m >> 16) : 1;
+                }
+                const bool on = lane < cnt;
+                const bool is_match = on && (mine >> 16) != 0;
+                uint32_t sym = mine, eb, ev, dsym = 0;
+                if (is_match) {
+                    length_code(mine >> 16, sym, eb, ev);
+                    dist_code(mine & 0xffff, dsym, eb, ev);
+                }
+                warp_count(S.freq_ll, sym, on);
+                warp_count(S.freq_d, dsym, is_match);
+                if (on) tok[s0 + lane] = mine;
+                if (lane == 0) S.sub_cnt[s0 / SUB] = static_cast<uint8_t>(cnt);
+            }
             __syncthreads();
         }
-        // ---- greedy parse: thread t takes sub-blocks SUBS_PER_THREAD t ..,
-        // each from its own start; lanes step together so symbol counts are
-        // aggregated per warp ----
-        {
-            uint32_t s = SUBS_PER_THREAD * t;
-            for (int j = 0; j < SUBS_PER_THREAD; ++j, ++s) {
-                const uint32_t s0 = s * SUB;
-                const bool mine = s0 < n;
-                const uint32_t e = mine ? (s0 + SUB < n ? s0 + SUB : n) : 0;
-                uint32_t q = s0, cnt = 0;
-                for (int step = 0; step < SUB; ++step) {
-                    const bool on = mine && q < e;
-                    uint32_t mv = 0, lit = 0;
-                    if (on) {
-                        mv = best[q];
-                        lit = S.u.data[q];
-                    }
-                    const bool is_match = on && mv != 0;
-                    uint32_t sym = lit, eb, ev, dsym = 0;
-                    if (is_match) {
-                        length_code(mv >> 16, sym, eb, ev);
-                        dist_code(mv & 0xffff, dsym, eb, ev);
-                    }
-                    warp_count(S.freq_ll, sym, on);
-                    warp_count(S.freq_d, dsym, is_match);
-                    if (on) {
-                        tok[s0 + cnt++] = is_match ? mv : lit;
-                        q += is_match ? (mv >> 16) : 1;
-                    }
-                }
-                if (mine) S.sub_cnt[s] = static_cast<uint8_t>(cnt);
-            }
-        }
-        __syncthreads();
         // ---- Huffman codes (warp 0) while warp 1 finishes the CRC ----
         if (warp == 1) crc_combine(S, n, lane);
         if (warp == 0) {
@@ -777,8 +772,8 @@ size_t bgzf_scratch_bytes(uint64_t n_bytes, int sm_count) {
     cub::DeviceScan::InclusiveSum(nullptr, t, static_cast<const uint32_t*>(nullptr), static_cast<uint64_t*>(nullptr),
                                   static_cast<int64_t>(nb ? nb : 1));
     const size_t grid = bgzf_grid(nb ? nb : 1, sm_count);
-    // tokens and matches per CTA, member slots, sizes, ends, scan temp
-    return 2 * align256(grid * BGZF_BLOCK * 4) + align256(nb * 65536) + align256(nb * 4) + align256(nb * 8) +
+    // tokens per CTA, member slots, sizes, ends, scan temp
+    return align256(grid * BGZF_BLOCK * 4) + align256(nb * 65536) + align256(nb * 4) + align256(nb * 8) +
            align256(t) + 256;
 }
 
@@ -790,8 +785,6 @@ uint64_t bgzf_compress(const uint8_t* in, uint64_t n, int level, uint8_t* out, u
     const int grid = static_cast<int>(nb < gmax ? nb : gmax);
     uint8_t* s = static_cast<uint8_t*>(scratch);
     uint32_t* tok = reinterpret_cast<uint32_t*>(s);
-    s += align256(gmax * BGZF_BLOCK * 4);
-    uint32_t* best = reinterpret_cast<uint32_t*>(s);
     s += align256(gmax * BGZF_BLOCK * 4);
     uint8_t* slots = s;
     s += align256(nb * 65536);
@@ -816,7 +809,7 @@ uint64_t bgzf_compress(const uint8_t* in, uint64_t n, int level, uint8_t* out, u
             check_launch(cudaEventRecord(e0, st), "event");
         }
         bgzf_kernel<<<grid, THREADS, smem, st>>>(in, n, static_cast<uint32_t>(nb), level, chain_for(level), slots,
-                                                 sizes, tok, best);
+                                                 sizes, tok);
         check_launch(cudaGetLastError(), "bgzf_kernel");
         if (kernel_ms) check_launch(cudaEventRecord(e1, st), "event");
         check_launch(cub::DeviceScan::InclusiveSum(temp, tb, static_cast<const uint32_t*>(sizes), ends,

@@ -84,16 +84,18 @@ class BatchArena:
 
 @dataclass
 class BamTile:
-    """Tile state of the FM BAM path: metadata arrays and counters."""
+    """Tile state of the FM BAM path: counters and, unless the metadata lives
+    elsewhere (host_meta=False: the device forms), the host metadata arrays."""
     meta_cap: int
     n_reads: int = 0
     n_mapped: int = 0
     n_total: int = 0
     chunk: int = 0
     meta: dict = field(default_factory=dict)
+    host_meta: bool = True
 
     def __post_init__(self):
-        if not self.meta:
+        if not self.meta and self.host_meta:
             self.meta = {k: np.zeros(self.meta_cap, t) for k, t in META_FIELDS}
 
     def to_c(self) -> ma_bam_tile:

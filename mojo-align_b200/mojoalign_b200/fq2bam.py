@@ -27,6 +27,7 @@ on the batch size.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import gzip
 import os
@@ -171,8 +172,8 @@ def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", 
     n_reads = n_mapped = 0
     status = torch.zeros(3, dtype=torch.int64, device=dev)
     o3 = (C.c_uint64 * 3)()
-    guard = torch.cuda.stream(stream)
-    guard.__enter__()
+    scope = contextlib.ExitStack()
+    scope.enter_context(torch.cuda.stream(stream))  # torch work shares the pipeline's stream
     try:
         for f in feeds:
             f.fill()
@@ -327,7 +328,7 @@ def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", 
             pending.exception()
         pool.shutdown(wait=True)
         stream.synchronize()
-        guard.__exit__(None, None, None)
+        scope.close()
         for f in feeds:
             f.close()
         if own_index:
