@@ -273,8 +273,9 @@ __device__ void huff_codes(const uint8_t* len, int n, uint16_t* code, HuffScratc
     }
 }
 
-// Everything one CTA keeps for the piece it compresses (under half of an
-// SM's shared memory, so two pieces are in flight per SM).
+// Everything one CTA keeps for its two pieces in flight (the one being
+// matched and the one being coded); under half of an SM's shared memory, so
+// two CTAs run per SM.
 struct Smem {
     union {
         uint8_t data[BGZF_BLOCK + 64];
@@ -284,18 +285,20 @@ struct Smem {
     uint32_t head[HSIZE];  // per hash: last position + 1 of earlier phases
     uint32_t crc_seg[THREADS];
     uint32_t crc_tab[256];
-    uint32_t freq_ll[NLL + 2], freq_d[NDIST + 2], freq_cl[NCL + 1];
+    uint32_t freq_ll[2][NLL + 2], freq_d[2][NDIST + 2], freq_cl[NCL + 1];  // [piece & 1]
     uint16_t code_ll[NLL + 2], code_d[NDIST + 2], code_cl[NCL + 1];
     uint8_t len_ll[NLL + 2], len_d[NDIST + 2], len_cl[NCL + 1];
-    uint8_t sub_cnt[NSUB];
+    uint8_t sub_cnt[2][NSUB];
     uint8_t lens_all[NLL + NDIST];
     uint16_t rle[NLL + NDIST];  // code-length symbol | extra value << 5
     uint32_t hdr[112];          // header bits
     HuffScratch hs;
-    uint32_t hdr_bits, n_rle, crc, x_seg, x_lane, lane_len[32], lane_crc[32];
+    uint32_t hdr_bits, n_rle, crc[2], x_seg, x_lane, lane_len[32], lane_crc[32];
     uint32_t nl_nd[2];
     typename cub::BlockScan<uint32_t, THREADS>::TempStorage scan;
 };
+// two CTAs per SM: 228 KB of shared memory, 1 KB of it reserved per CTA
+static_assert(2 * (sizeof(Smem) + 1024) <= 228 * 1024, "two CTAs per SM");
 
 // Four bytes of the piece starting at byte i (two aligned shared loads).
 __device__ __forceinline__ uint32_t load4(const uint32_t* w, uint32_t i) {
@@ -373,7 +376,7 @@ __device__ __forceinline__ void token_bits(const Smem& S, uint32_t tokv, uint32_
 // CRC-32 of the piece from the segment remainders (one warp): each lane
 // folds its run of segments, lane 0 folds the lanes, and the
 // standard initial and final inversion contribute F x^(8n) + F.
-__device__ void crc_combine(Smem& S, uint32_t n, int lane) {
+__device__ void crc_combine(Smem& S, uint32_t n, int lane, int buf) {
     const uint32_t x64 = S.x_seg, x2048 = S.x_lane;
     uint32_t c = 0, len = 0;
     constexpr int PER_LANE = THREADS / 32;
@@ -393,7 +396,7 @@ __device__ void crc_combine(Smem& S, uint32_t n, int lane) {
             const uint32_t ll = S.lane_len[l];
             if (ll) r = gf2_mul(r, ll == (THREADS / 32) * CRC_SEG ? x2048 : gf2_xpow(8ull * ll)) ^ S.lane_crc[l];
         }
-        S.crc = r ^ gf2_mul(0xffffffffu, gf2_xpow(8ull * n)) ^ 0xffffffffu;
+        S.crc[buf] = r ^ gf2_mul(0xffffffffu, gf2_xpow(8ull * n)) ^ 0xffffffffu;
     }
 }
 
@@ -412,6 +415,310 @@ __device__ void write_frame(uint8_t* slot, uint32_t payload, uint32_t crc, uint3
     }
 }
 
+// ---- the stages of one piece ----
+
+// Piece bytes into shared memory (64 zero bytes after them), its CRC
+// segment remainders, and a cleared head table and symbol counts.
+__device__ void load_piece(Smem& S, const uint8_t* src, uint32_t n, int buf, int t) {
+    if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+        const uint4* s4 = reinterpret_cast<const uint4*>(src);
+        uint4* d4 = reinterpret_cast<uint4*>(S.u.data);
+        for (uint32_t i = t; i < n / 16; i += THREADS) d4[i] = s4[i];
+        for (uint32_t i = (n & ~15u) + t; i < n + 64; i += THREADS) S.u.data[i] = i < n ? src[i] : 0;
+    } else {
+        for (uint32_t i = t; i < n + 64; i += THREADS) S.u.data[i] = i < n ? src[i] : 0;
+    }
+    for (int i = t; i < HSIZE; i += THREADS) S.head[i] = 0;
+    for (int i = t; i < NLL + 2; i += THREADS) S.freq_ll[buf][i] = 0;
+    if (t < NDIST + 2) S.freq_d[buf][t] = 0;
+    __syncthreads();
+    const uint32_t s0 = t * CRC_SEG, s1 = s0 + CRC_SEG < n ? s0 + CRC_SEG : n;
+    uint32_t c = 0;
+    for (uint32_t i = s0; i < s1; ++i) c = (c >> 8) ^ S.crc_tab[(c ^ S.u.data[i]) & 255u];
+    S.crc_seg[t] = c;
+}
+
+constexpr int MATCH_WARPS = THREADS / 32 - 1;  // warp 0 builds codes meanwhile
+constexpr uint32_t PHASE = MATCH_WARPS * 32;   // positions per matching phase
+
+// Barrier of the matching warps only (warps 1..15); warp 0 never takes it.
+__device__ __forceinline__ void match_barrier() { asm volatile("bar.sync 1, %0;" ::"n"(PHASE) : "memory"); }
+
+// LZ77 + greedy parse of the piece in shared memory by warps 1..15:
+// phases of PHASE positions (one thread each); tokens to `tok`, symbol
+// counts to freq[buf], token counts per 32-byte sub-block to sub_cnt[buf].
+__device__ void match_piece(Smem& S, uint32_t n, int chain, uint32_t* tok, int buf, int wt, int lane, int mw) {
+    const uint32_t n_phase = (n + PHASE - 1) / PHASE;
+    for (uint32_t k = 0; k < n_phase; ++k) {
+        const uint32_t p = k * PHASE + wt;
+        const bool valid = p + 3 <= n;
+        const uint32_t h = valid ? hash3(S.u.data + p) : 0;
+        const uint32_t same = __match_any_sync(0xffffffffu, valid ? h : (0x80000000u | wt));
+        const uint32_t lower = same & ((1u << lane) - 1);
+        uint32_t prev_p = NONE;
+        if (valid) {
+            if (lower) {
+                prev_p = p - (lane - (31 - __clz(lower)));
+            } else {
+                const uint32_t hv = S.head[h];
+                prev_p = hv ? hv - 1 : NONE;
+            }
+        }
+        if (p < n) S.prev[p & WMASK] = static_cast<uint16_t>(prev_p);
+        match_barrier();
+        uint32_t bm = 0;
+        if (valid) {
+            const uint32_t sub_end = (p & ~static_cast<uint32_t>(SUB - 1)) + SUB;
+            const uint32_t lim = (sub_end < n ? sub_end : n) - p;
+            if (lim >= 3) {
+                uint32_t q = prev_p, best_len = 2, best_d = 0;
+                for (int c = 0; c < chain && q != NONE && q < p && p - q <= WSIZE; ++c) {
+                    // a candidate can only win if it also matches the byte
+                    // just past the current best
+                    const bool may = best_len >= lim || S.u.data[q + best_len] == S.u.data[p + best_len];
+                    const uint32_t L = may ? match_len(S.u.out, q, p, lim) : 0;
+                    if (L > best_len) {
+                        best_len = L;
+                        best_d = p - q;
+                        if (L == lim) break;
+                    }
+                    const uint32_t nq = S.prev[q & WMASK];
+                    if (nq == NONE || nq >= q) break;
+                    q = nq;
+                }
+                if (best_len >= 3) bm = (best_len << 16) | best_d;
+            }
+        }
+        if (valid) atomicMax(&S.head[h], p + 1);
+        // greedy parse of this warp's 32-byte sub-block, which its lanes just
+        // matched: the walk position is warp-uniform, the lane at that
+        // position hands over its match by shuffle; token i ends up in lane i
+        const uint32_t s0 = k * PHASE + 32 * mw;
+        if (s0 < n) {
+            const uint32_t e = n - s0 < SUB ? n - s0 : SUB;
+            const uint32_t lit = p < n ? S.u.data[p] : 0;
+            uint32_t q = 0, cnt = 0, mine = 0;
+            while (q < e) {
+                const uint32_t m = __shfl_sync(0xffffffffu, bm, q);
+                const uint32_t tv = m ? m : __shfl_sync(0xffffffffu, lit, q);
+                if (lane == cnt) mine = tv;
+                ++cnt;
+                q += m ? (m >> 16) : 1;
+            }
+            const bool on = lane < cnt;
+            const bool is_match = on && (mine >> 16) != 0;
+            uint32_t sym = mine, eb, ev, dsym = 0;
+            if (is_match) {
+                length_code(mine >> 16, sym, eb, ev);
+                dist_code(mine & 0xffff, dsym, eb, ev);
+            }
+            warp_count(S.freq_ll[buf], sym, on);
+            warp_count(S.freq_d[buf], dsym, is_match);
+            if (on) tok[s0 + lane] = mine;
+            if (lane == 0) S.sub_cnt[buf][s0 / SUB] = static_cast<uint8_t>(cnt);
+        }
+        match_barrier();
+    }
+}
+
+// Dynamic Huffman codes of a matched piece from freq[buf], and the block
+// header bits (warp 0).
+__device__ void build_codes(Smem& S, int buf, int lane) {
+    uint32_t* freq_ll = S.freq_ll[buf];
+    uint32_t* freq_d = S.freq_d[buf];
+    for (int i = lane; i < 112; i += 32) S.hdr[i] = 0;
+    if (lane < NCL + 1) S.freq_cl[lane] = 0;
+    if (lane == 0) {
+        freq_ll[256] += 1;  // end of block
+        // at least two codes in each alphabet
+        int used = 0;
+        for (int i = 0; i < NLL; ++i) used += freq_ll[i] != 0;
+        if (used < 2) freq_ll[freq_ll[0] ? 1 : 0] = 1;
+        used = 0;
+        for (int i = 0; i < NDIST; ++i) used += freq_d[i] != 0;
+        for (int i = 0; used < 2; ++i)
+            if (!freq_d[i]) {
+                freq_d[i] = 1;
+                ++used;
+            }
+    }
+    __syncwarp();
+    huff_lengths(freq_ll, NLL, 15, S.len_ll, S.hs, lane);
+    huff_lengths(freq_d, NDIST, 15, S.len_d, S.hs, lane);
+    huff_codes(S.len_ll, NLL, S.code_ll, S.hs, lane);
+    huff_codes(S.len_d, NDIST, S.code_d, S.hs, lane);
+    if (lane == 0) {
+        int nl = NLL, nd = NDIST;
+        while (nl > 257 && !S.len_ll[nl - 1]) --nl;
+        while (nd > 1 && !S.len_d[nd - 1]) --nd;
+        for (int i = 0; i < nl; ++i) S.lens_all[i] = S.len_ll[i];
+        for (int i = 0; i < nd; ++i) S.lens_all[nl + i] = S.len_d[i];
+        // run-length code the lengths: 16 = repeat the previous length
+        // 3..6 times, 17 / 18 = 3..10 / 11..138 zeros
+        const int tot = nl + nd;
+        uint32_t nr = 0;
+        for (int i = 0; i < tot;) {
+            const uint32_t v = S.lens_all[i];
+            int run = 1;
+            while (i + run < tot && S.lens_all[i + run] == v) ++run;
+            i += run;
+            if (v == 0) {
+                while (run >= 11) {
+                    const int k = run < 138 ? run : 138;
+                    S.rle[nr++] = static_cast<uint16_t>(18 | (k - 11) << 5);
+                    run -= k;
+                }
+                if (run >= 3) {
+                    S.rle[nr++] = static_cast<uint16_t>(17 | (run - 3) << 5);
+                    run = 0;
+                }
+                while (run-- > 0) S.rle[nr++] = 0;
+            } else {
+                S.rle[nr++] = static_cast<uint16_t>(v);
+                --run;
+                while (run >= 3) {
+                    const int k = run < 6 ? run : 6;
+                    S.rle[nr++] = static_cast<uint16_t>(16 | (k - 3) << 5);
+                    run -= k;
+                }
+                while (run-- > 0) S.rle[nr++] = static_cast<uint16_t>(v);
+            }
+        }
+        S.n_rle = nr;
+        for (uint32_t i = 0; i < nr; ++i) ++S.freq_cl[S.rle[i] & 31];
+        int used = 0;
+        for (int i = 0; i < NCL; ++i) used += S.freq_cl[i] != 0;
+        for (int i = 0; used < 2; ++i)
+            if (!S.freq_cl[i]) {
+                S.freq_cl[i] = 1;
+                ++used;
+            }
+        S.nl_nd[0] = nl;
+        S.nl_nd[1] = nd;
+    }
+    __syncwarp();
+    huff_lengths(S.freq_cl, NCL, 7, S.len_cl, S.hs, lane);
+    huff_codes(S.len_cl, NCL, S.code_cl, S.hs, lane);
+    if (lane == 0) {
+        const uint32_t nl = S.nl_nd[0], nd = S.nl_nd[1];
+        int hclen = NCL;
+        while (hclen > 4 && !S.len_cl[CL_ORDER[hclen - 1]]) --hclen;
+        uint32_t pos = 0;
+        hdr_put(S.hdr, pos, 1, 1);  // BFINAL
+        hdr_put(S.hdr, pos, 2, 2);  // BTYPE = dynamic
+        hdr_put(S.hdr, pos, nl - 257, 5);
+        hdr_put(S.hdr, pos, nd - 1, 5);
+        hdr_put(S.hdr, pos, hclen - 4, 4);
+        for (int i = 0; i < hclen; ++i) hdr_put(S.hdr, pos, S.len_cl[CL_ORDER[i]], 3);
+        for (uint32_t i = 0; i < S.n_rle; ++i) {
+            const uint32_t r = S.rle[i], sym = r & 31, ex = r >> 5;
+            hdr_put(S.hdr, pos, S.code_cl[sym], S.len_cl[sym]);
+            if (sym == 16) hdr_put(S.hdr, pos, ex, 2);
+            else if (sym == 17) hdr_put(S.hdr, pos, ex, 3);
+            else if (sym == 18) hdr_put(S.hdr, pos, ex, 7);
+        }
+        S.hdr_bits = pos;
+    }
+    __syncwarp();
+}
+
+// Stored deflate blocks of a piece with zlib's framing for one compress +
+// finish call, read from `src`.
+__device__ void write_stored(uint8_t* slot, const uint8_t* src, uint32_t n, uint32_t crc, uint32_t* size, int t) {
+    const uint32_t two = n > 32767;
+    const uint32_t payload = n + (two ? 10 : 5);
+    uint8_t* pl = slot + 18;
+    for (uint32_t i = t; i < n; i += THREADS) pl[5 + i] = src[i];
+    if (t == 0) {
+        pl[0] = two ? 0 : 1;
+        pl[1] = n & 255;
+        pl[2] = n >> 8;
+        pl[3] = ~n & 255;
+        pl[4] = (~n >> 8) & 255;
+        if (two) {
+            const uint8_t e[5] = {1, 0, 0, 255, 255};
+            for (int k = 0; k < 5; ++k) pl[5 + n + k] = e[k];
+        }
+        *size = 26 + payload;
+    }
+    write_frame(slot, payload, crc, n, t);
+}
+
+// Bits of a coded piece (all threads): per-thread bit counts of its
+// sub-blocks, a block scan, the codes ORed into the shared word buffer
+// (which reuses the piece bytes), the member to its slot; stored instead
+// when that is not larger.  `src` is the piece in global memory.
+__device__ void emit_piece(Smem& S, const uint32_t* tok, const uint8_t* src, uint32_t n, int buf, uint8_t* slot,
+                           uint32_t* size, int t) {
+    const uint32_t n_sub = (n + SUB - 1) / SUB;
+    const uint8_t* sub_cnt = S.sub_cnt[buf];
+    uint32_t bits = 0;
+    const uint32_t s_first = SUBS_PER_THREAD * t, s_last = s_first + SUBS_PER_THREAD;
+    for (uint32_t s = s_first; s < s_last && s < n_sub; ++s) {
+        const uint4* tv = reinterpret_cast<const uint4*>(tok + s * SUB);
+        const uint32_t c = sub_cnt[s];
+        for (uint32_t i = 0; i < c; i += 4) {
+            const uint4 v = tv[i >> 2];
+            token_bits(S, v.x, bits);
+            if (i + 1 < c) token_bits(S, v.y, bits);
+            if (i + 2 < c) token_bits(S, v.z, bits);
+            if (i + 3 < c) token_bits(S, v.w, bits);
+        }
+    }
+    uint32_t off, sum;
+    cub::BlockScan<uint32_t, THREADS>(S.scan).ExclusiveSum(bits, off, sum);
+    const uint32_t total = S.hdr_bits + sum + S.len_ll[256];
+    const uint32_t dyn_bytes = (total + 7) / 8;
+    const uint32_t stored_bytes = n + (n > 32767 ? 10 : 5);
+    if (dyn_bytes >= stored_bytes) {
+        write_stored(slot, src, n, S.crc[buf], size, t);
+        return;
+    }
+    for (int i = t; i < static_cast<int>((BGZF_BLOCK + 64) / 4); i += THREADS) S.u.out[i] = 0;
+    __syncthreads();
+    for (uint32_t i = t; i < (S.hdr_bits + 31) / 32; i += THREADS) atomicOr(&S.u.out[i], S.hdr[i]);
+    BitOut bo(S.u.out, S.hdr_bits + off);
+    for (uint32_t s = s_first; s < s_last && s < n_sub; ++s) {
+        const uint4* tv4 = reinterpret_cast<const uint4*>(tok + s * SUB);
+        const uint32_t c = sub_cnt[s];
+        for (uint32_t i = 0; i < c; i += 4) {
+            const uint4 v = tv4[i >> 2];
+            const uint32_t four[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (i + k >= c) break;
+                const uint32_t tv = four[k];
+                if ((tv >> 16) == 0) {
+                    bo.put(S.code_ll[tv], S.len_ll[tv]);
+                } else {
+                    uint32_t sym, eb, ev;
+                    length_code(tv >> 16, sym, eb, ev);
+                    bo.put(S.code_ll[sym], S.len_ll[sym]);
+                    if (eb) bo.put(ev, eb);
+                    dist_code(tv & 0xffff, sym, eb, ev);
+                    bo.put(S.code_d[sym], S.len_d[sym]);
+                    if (eb) bo.put(ev, eb);
+                }
+            }
+        }
+    }
+    bo.flush();
+    if (t == 0) {
+        BitOut eob(S.u.out, S.hdr_bits + sum);
+        eob.put(S.code_ll[256], S.len_ll[256]);
+        eob.flush();
+    }
+    __syncthreads();
+    const uint8_t* ob = reinterpret_cast<const uint8_t*>(S.u.out);
+    for (uint32_t i = t; i < dyn_bytes; i += THREADS) slot[18 + i] = ob[i];
+    write_frame(slot, dyn_bytes, S.crc[buf], n, t);
+    if (t == 0) *size = 26 + dyn_bytes;
+}
+
+// One CTA walks its pieces b = blockIdx.x + j gridDim.x.  At levels 1..9 it
+// runs a two-stage pipeline: while warps 1..15 match piece j, warp 0 builds
+// the codes of piece j-1 (and folds piece j's CRC); then all warps emit
+// piece j-1.  Tokens and symbol counts are double-buffered by piece parity.
 __global__ void __launch_bounds__(THREADS, 2)
     bgzf_kernel(const uint8_t* in, uint64_t n_total, uint32_t n_blocks, int level, int chain, uint8_t* slots,
                 uint32_t* sizes, uint32_t* tok_all) {
@@ -427,305 +734,43 @@ __global__ void __launch_bounds__(THREADS, 2)
         S.x_seg = gf2_xpow(8ull * CRC_SEG);
         S.x_lane = gf2_xpow(8ull * (THREADS / 32) * CRC_SEG);
     }
-    uint32_t* tok = tok_all + static_cast<size_t>(blockIdx.x) * BGZF_BLOCK;
-    for (uint32_t b = blockIdx.x; b < n_blocks; b += gridDim.x) {
+    auto piece_len = [&](uint32_t b) {
         const uint64_t base = static_cast<uint64_t>(b) * BGZF_BLOCK;
-        const uint32_t n = static_cast<uint32_t>(n_total - base < BGZF_BLOCK ? n_total - base : BGZF_BLOCK);
-        uint8_t* slot = slots + static_cast<size_t>(b) * 65536;
-        __syncthreads();  // the previous piece is done with shared memory
-        if ((reinterpret_cast<uintptr_t>(in + base) & 15) == 0) {
-            const uint4* src = reinterpret_cast<const uint4*>(in + base);
-            uint4* dst = reinterpret_cast<uint4*>(S.u.data);
-            for (uint32_t i = t; i < n / 16; i += THREADS) dst[i] = src[i];
-            for (uint32_t i = (n & ~15u) + t; i < n + 64; i += THREADS) S.u.data[i] = i < n ? in[base + i] : 0;
-        } else {
-            for (uint32_t i = t; i < n + 64; i += THREADS) S.u.data[i] = i < n ? in[base + i] : 0;
+        return static_cast<uint32_t>(n_total - base < BGZF_BLOCK ? n_total - base : BGZF_BLOCK);
+    };
+    if (level == 0) {
+        for (uint32_t b = blockIdx.x; b < n_blocks; b += gridDim.x) {
+            const uint32_t n = piece_len(b);
+            const uint8_t* src = in + static_cast<uint64_t>(b) * BGZF_BLOCK;
+            __syncthreads();
+            load_piece(S, src, n, 0, t);
+            __syncthreads();
+            if (warp == 0) crc_combine(S, n, lane, 0);
+            __syncthreads();
+            write_stored(slots + static_cast<size_t>(b) * 65536, src, n, S.crc[0], sizes + b, t);
         }
-        for (int i = t; i < HSIZE; i += THREADS) S.head[i] = 0;
-        for (int i = t; i < NLL + 2; i += THREADS) S.freq_ll[i] = 0;
-        if (t < NDIST + 2) S.freq_d[t] = 0;
-        if (t < NCL + 1) S.freq_cl[t] = 0;
-        for (int i = t; i < 112; i += THREADS) S.hdr[i] = 0;
+        return;
+    }
+    const uint32_t count = blockIdx.x < n_blocks ? (n_blocks - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    uint32_t* tok2 = tok_all + static_cast<size_t>(blockIdx.x) * 2 * BGZF_BLOCK;
+    for (uint32_t j = 0; j <= count; ++j) {
+        const bool cur = j < count, prv = j > 0;
+        const uint32_t b = blockIdx.x + j * gridDim.x, bp = b - gridDim.x;
+        const int buf = j & 1, pbuf = buf ^ 1;
+        __syncthreads();  // the previous emission is done with shared memory
+        const uint32_t n = cur ? piece_len(b) : 0;
+        if (cur) load_piece(S, in + static_cast<uint64_t>(b) * BGZF_BLOCK, n, buf, t);
         __syncthreads();
-        // CRC remainders of 128-byte segments (register starting at 0)
-        {
-            const uint32_t s0 = t * CRC_SEG, s1 = s0 + CRC_SEG < n ? s0 + CRC_SEG : n;
-            uint32_t c = 0;
-            for (uint32_t i = s0; i < s1; ++i) c = (c >> 8) ^ S.crc_tab[(c ^ S.u.data[i]) & 255u];
-            S.crc_seg[t] = c;
-        }
-        __syncthreads();
-        if (level == 0) {
-            // stored blocks, zlib's framing for one compress + finish call
-            if (warp == 1) crc_combine(S, n, lane);
-            __syncthreads();
-            const uint32_t two = n > 32767;
-            const uint32_t payload = n + (two ? 10 : 5);
-            uint8_t* pl = slot + 18;
-            for (uint32_t i = t; i < n; i += THREADS) pl[5 + i] = S.u.data[i];
-            if (t == 0) {
-                pl[0] = two ? 0 : 1;
-                pl[1] = n & 255;
-                pl[2] = n >> 8;
-                pl[3] = ~n & 255;
-                pl[4] = (~n >> 8) & 255;
-                if (two) {
-                    const uint8_t e[5] = {1, 0, 0, 255, 255};
-                    for (int k = 0; k < 5; ++k) pl[5 + n + k] = e[k];
-                }
-                sizes[b] = 26 + payload;
-            }
-            write_frame(slot, payload, S.crc, n, t);
-            continue;
-        }
-        // ---- LZ77 over phases of THREADS positions ----
-        const uint32_t n_phase = (n + THREADS - 1) / THREADS;
-        for (uint32_t k = 0; k < n_phase; ++k) {
-            const uint32_t p = k * THREADS + t;
-            const bool valid = p + 3 <= n;
-            const uint32_t h = valid ? hash3(S.u.data + p) : 0;
-            const uint32_t same = __match_any_sync(0xffffffffu, valid ? h : (0x80000000u | t));
-            const uint32_t lower = same & ((1u << lane) - 1);
-            uint32_t prev_p = NONE;
-            if (valid) {
-                if (lower) {
-                    prev_p = p - (lane - (31 - __clz(lower)));
-                } else {
-                    const uint32_t hv = S.head[h];
-                    prev_p = hv ? hv - 1 : NONE;
-                }
-            }
-            if (p < n) S.prev[p & WMASK] = static_cast<uint16_t>(prev_p);
-            __syncthreads();
-            uint32_t bm = 0;
-            if (valid) {
-                const uint32_t sub_end = (p & ~static_cast<uint32_t>(SUB - 1)) + SUB;
-                const uint32_t lim = (sub_end < n ? sub_end : n) - p;
-                if (lim >= 3) {
-                    uint32_t q = prev_p, best_len = 2, best_d = 0;
-                    for (int c = 0; c < chain && q != NONE && q < p && p - q <= WSIZE; ++c) {
-                        // a candidate can only win if it also matches the
-                        // byte just past the current best
-                        const bool may = best_len >= lim || S.u.data[q + best_len] == S.u.data[p + best_len];
-                        const uint32_t L = may ? match_len(S.u.out, q, p, lim) : 0;
-                        if (L > best_len) {
-                            best_len = L;
-                            best_d = p - q;
-                            if (L == lim) break;
-                        }
-                        const uint32_t nq = S.prev[q & WMASK];
-                        if (nq == NONE || nq >= q) break;
-                        q = nq;
-                    }
-                    if (best_len >= 3) bm = (best_len << 16) | best_d;
-                }
-            }
-            if (valid) atomicMax(&S.head[h], p + 1);
-            // greedy parse of this warp's 32-byte sub-block, which the warp's
-            // lanes just matched: the walk position is warp-uniform, so the
-            // lane at that position hands over its match by shuffle; token j
-            // ends up in lane j
-            const uint32_t s0 = k * THREADS + 32 * warp;
-            if (s0 < n) {
-                const uint32_t e = n - s0 < SUB ? n - s0 : SUB;
-                const uint32_t lit = p < n ? S.u.data[p] : 0;
-                uint32_t q = 0, cnt = 0, mine = 0;
-                while (q < e) {
-                    const uint32_t m = __shfl_sync(0xffffffffu, bm, q);
-                    const uint32_t tv = m ? m : __shfl_sync(0xffffffffu, lit, q);
-                    if (lane == cnt) mine = tv;
-                    ++cnt;
-                    q += m ? (m >> 16) : 1;
-                }
-                const bool on = lane < cnt;
-                const bool is_match = on && (mine >> 16) != 0;
-                uint32_t sym = mine, eb, ev, dsym = 0;
-                if (is_match) {
-                    length_code(mine >> 16, sym, eb, ev);
-                    dist_code(mine & 0xffff, dsym, eb, ev);
-                }
-                warp_count(S.freq_ll, sym, on);
-                warp_count(S.freq_d, dsym, is_match);
-                if (on) tok[s0 + lane] = mine;
-                if (lane == 0) S.sub_cnt[s0 / SUB] = static_cast<uint8_t>(cnt);
-            }
-            __syncthreads();
-        }
-        // ---- Huffman codes (warp 0) while warp 1 finishes the CRC ----
-        if (warp == 1) crc_combine(S, n, lane);
         if (warp == 0) {
-            if (lane == 0) {
-                S.freq_ll[256] += 1;  // end of block
-                // at least two codes in each alphabet
-                int used = 0;
-                for (int i = 0; i < NLL; ++i) used += S.freq_ll[i] != 0;
-                if (used < 2) S.freq_ll[S.freq_ll[0] ? 1 : 0] = 1;
-                used = 0;
-                for (int i = 0; i < NDIST; ++i) used += S.freq_d[i] != 0;
-                for (int i = 0; used < 2; ++i)
-                    if (!S.freq_d[i]) {
-                        S.freq_d[i] = 1;
-                        ++used;
-                    }
-            }
-            __syncwarp();
-            huff_lengths(S.freq_ll, NLL, 15, S.len_ll, S.hs, lane);
-            huff_lengths(S.freq_d, NDIST, 15, S.len_d, S.hs, lane);
-            huff_codes(S.len_ll, NLL, S.code_ll, S.hs, lane);
-            huff_codes(S.len_d, NDIST, S.code_d, S.hs, lane);
-            if (lane == 0) {
-                int nl = NLL, nd = NDIST;
-                while (nl > 257 && !S.len_ll[nl - 1]) --nl;
-                while (nd > 1 && !S.len_d[nd - 1]) --nd;
-                for (int i = 0; i < nl; ++i) S.lens_all[i] = S.len_ll[i];
-                for (int i = 0; i < nd; ++i) S.lens_all[nl + i] = S.len_d[i];
-                // run-length code the lengths: 16 = repeat the previous
-                // length 3..6 times, 17 / 18 = 3..10 / 11..138 zeros
-                const int tot = nl + nd;
-                uint32_t nr = 0;
-                for (int i = 0; i < tot;) {
-                    const uint32_t v = S.lens_all[i];
-                    int run = 1;
-                    while (i + run < tot && S.lens_all[i + run] == v) ++run;
-                    i += run;
-                    if (v == 0) {
-                        while (run >= 11) {
-                            const int k = run < 138 ? run : 138;
-                            S.rle[nr++] = static_cast<uint16_t>(18 | (k - 11) << 5);
-                            run -= k;
-                        }
-                        if (run >= 3) {
-                            S.rle[nr++] = static_cast<uint16_t>(17 | (run - 3) << 5);
-                            run = 0;
-                        }
-                        while (run-- > 0) S.rle[nr++] = 0;
-                    } else {
-                        S.rle[nr++] = static_cast<uint16_t>(v);
-                        --run;
-                        while (run >= 3) {
-                            const int k = run < 6 ? run : 6;
-                            S.rle[nr++] = static_cast<uint16_t>(16 | (k - 3) << 5);
-                            run -= k;
-                        }
-                        while (run-- > 0) S.rle[nr++] = static_cast<uint16_t>(v);
-                    }
-                }
-                S.n_rle = nr;
-                for (uint32_t i = 0; i < nr; ++i) ++S.freq_cl[S.rle[i] & 31];
-                int used = 0;
-                for (int i = 0; i < NCL; ++i) used += S.freq_cl[i] != 0;
-                for (int i = 0; used < 2; ++i)
-                    if (!S.freq_cl[i]) {
-                        S.freq_cl[i] = 1;
-                        ++used;
-                    }
-                S.nl_nd[0] = nl;
-                S.nl_nd[1] = nd;
-            }
-            __syncwarp();
-            huff_lengths(S.freq_cl, NCL, 7, S.len_cl, S.hs, lane);
-            huff_codes(S.len_cl, NCL, S.code_cl, S.hs, lane);
-            if (lane == 0) {
-                const uint32_t nl = S.nl_nd[0], nd = S.nl_nd[1];
-                int hclen = NCL;
-                while (hclen > 4 && !S.len_cl[CL_ORDER[hclen - 1]]) --hclen;
-                uint32_t pos = 0;
-                hdr_put(S.hdr, pos, 1, 1);  // BFINAL
-                hdr_put(S.hdr, pos, 2, 2);  // BTYPE = dynamic
-                hdr_put(S.hdr, pos, nl - 257, 5);
-                hdr_put(S.hdr, pos, nd - 1, 5);
-                hdr_put(S.hdr, pos, hclen - 4, 4);
-                for (int i = 0; i < hclen; ++i) hdr_put(S.hdr, pos, S.len_cl[CL_ORDER[i]], 3);
-                for (uint32_t i = 0; i < S.n_rle; ++i) {
-                    const uint32_t r = S.rle[i], sym = r & 31, ex = r >> 5;
-                    hdr_put(S.hdr, pos, S.code_cl[sym], S.len_cl[sym]);
-                    if (sym == 16) hdr_put(S.hdr, pos, ex, 2);
-                    else if (sym == 17) hdr_put(S.hdr, pos, ex, 3);
-                    else if (sym == 18) hdr_put(S.hdr, pos, ex, 7);
-                }
-                S.hdr_bits = pos;
-            }
+            if (cur) crc_combine(S, n, lane, buf);
+            if (prv) build_codes(S, pbuf, lane);
+        } else if (cur) {
+            match_piece(S, n, chain, tok2 + buf * BGZF_BLOCK, buf, t - 32, lane, warp - 1);
         }
         __syncthreads();
-        // ---- bit count per thread (its sub-blocks), offsets by scan ----
-        const uint32_t n_sub = (n + SUB - 1) / SUB;
-        uint32_t bits = 0;
-        const uint32_t s_first = SUBS_PER_THREAD * t, s_last = s_first + SUBS_PER_THREAD;
-        for (uint32_t s = s_first; s < s_last && s < n_sub; ++s) {
-            const uint4* tv = reinterpret_cast<const uint4*>(tok + s * SUB);
-            const uint32_t c = S.sub_cnt[s];
-            for (uint32_t i = 0; i < c; i += 4) {
-                const uint4 v = tv[i >> 2];
-                token_bits(S, v.x, bits);
-                if (i + 1 < c) token_bits(S, v.y, bits);
-                if (i + 2 < c) token_bits(S, v.z, bits);
-                if (i + 3 < c) token_bits(S, v.w, bits);
-            }
-        }
-        uint32_t off, sum;
-        cub::BlockScan<uint32_t, THREADS>(S.scan).ExclusiveSum(bits, off, sum);
-        const uint32_t total = S.hdr_bits + sum + S.len_ll[256];
-        const uint32_t dyn_bytes = (total + 7) / 8;
-        const uint32_t stored_bytes = n + (n > 32767 ? 10 : 5);
-        const bool use_dyn = dyn_bytes < stored_bytes;
-        if (use_dyn) {
-            for (int i = t; i < static_cast<int>((BGZF_BLOCK + 64) / 4); i += THREADS) S.u.out[i] = 0;
-            __syncthreads();
-            for (uint32_t i = t; i < (S.hdr_bits + 31) / 32; i += THREADS) atomicOr(&S.u.out[i], S.hdr[i]);
-            BitOut bo(S.u.out, S.hdr_bits + off);
-            for (uint32_t s = s_first; s < s_last && s < n_sub; ++s) {
-                const uint4* tv4 = reinterpret_cast<const uint4*>(tok + s * SUB);
-                const uint32_t c = S.sub_cnt[s];
-                for (uint32_t i = 0; i < c; i += 4) {
-                    const uint4 v = tv4[i >> 2];
-                    const uint32_t four[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        if (i + k >= c) break;
-                        const uint32_t tv = four[k];
-                        if ((tv >> 16) == 0) {
-                            bo.put(S.code_ll[tv], S.len_ll[tv]);
-                        } else {
-                            uint32_t sym, eb, ev;
-                            length_code(tv >> 16, sym, eb, ev);
-                            bo.put(S.code_ll[sym], S.len_ll[sym]);
-                            if (eb) bo.put(ev, eb);
-                            dist_code(tv & 0xffff, sym, eb, ev);
-                            bo.put(S.code_d[sym], S.len_d[sym]);
-                            if (eb) bo.put(ev, eb);
-                        }
-                    }
-                }
-            }
-            bo.flush();
-            if (t == 0) {
-                BitOut eob(S.u.out, S.hdr_bits + sum);
-                eob.put(S.code_ll[256], S.len_ll[256]);
-                eob.flush();
-            }
-            __syncthreads();
-            const uint8_t* ob = reinterpret_cast<const uint8_t*>(S.u.out);
-            for (uint32_t i = t; i < dyn_bytes; i += THREADS) slot[18 + i] = ob[i];
-            write_frame(slot, dyn_bytes, S.crc, n, t);
-            if (t == 0) sizes[b] = 26 + dyn_bytes;
-        } else {
-            const uint32_t two = n > 32767;
-            uint8_t* pl = slot + 18;
-            for (uint32_t i = t; i < n; i += THREADS) pl[5 + i] = S.u.data[i];
-            if (t == 0) {
-                pl[0] = two ? 0 : 1;
-                pl[1] = n & 255;
-                pl[2] = n >> 8;
-                pl[3] = ~n & 255;
-                pl[4] = (~n >> 8) & 255;
-                if (two) {
-                    const uint8_t e[5] = {1, 0, 0, 255, 255};
-                    for (int k = 0; k < 5; ++k) pl[5 + n + k] = e[k];
-                }
-                sizes[b] = 26 + stored_bytes;
-            }
-            write_frame(slot, stored_bytes, S.crc, n, t);
-        }
+        if (prv)
+            emit_piece(S, tok2 + pbuf * BGZF_BLOCK, in + static_cast<uint64_t>(bp) * BGZF_BLOCK, piece_len(bp), pbuf,
+                       slots + static_cast<size_t>(bp) * 65536, sizes + bp, t);
     }
 }
 
@@ -772,8 +817,8 @@ size_t bgzf_scratch_bytes(uint64_t n_bytes, int sm_count) {
     cub::DeviceScan::InclusiveSum(nullptr, t, static_cast<const uint32_t*>(nullptr), static_cast<uint64_t*>(nullptr),
                                   static_cast<int64_t>(nb ? nb : 1));
     const size_t grid = bgzf_grid(nb ? nb : 1, sm_count);
-    // tokens per CTA, member slots, sizes, ends, scan temp
-    return align256(grid * BGZF_BLOCK * 4) + align256(nb * 65536) + align256(nb * 4) + align256(nb * 8) +
+    // tokens (two pieces) per CTA, member slots, sizes, ends, scan temp
+    return align256(grid * 2 * BGZF_BLOCK * 4) + align256(nb * 65536) + align256(nb * 4) + align256(nb * 8) +
            align256(t) + 256;
 }
 
@@ -785,7 +830,7 @@ uint64_t bgzf_compress(const uint8_t* in, uint64_t n, int level, uint8_t* out, u
     const int grid = static_cast<int>(nb < gmax ? nb : gmax);
     uint8_t* s = static_cast<uint8_t*>(scratch);
     uint32_t* tok = reinterpret_cast<uint32_t*>(s);
-    s += align256(gmax * BGZF_BLOCK * 4);
+    s += align256(gmax * 2 * BGZF_BLOCK * 4);
     uint8_t* slots = s;
     s += align256(nb * 65536);
     uint32_t* sizes = reinterpret_cast<uint32_t*>(s);
