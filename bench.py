@@ -81,6 +81,8 @@ def parse_args():
                     "(the reference's default, METHYLGRAPHER_BAM_LEVEL=1; -1 = skip)")
     ap.add_argument("--fq2bam-pairs", type=int, default=2_000_000, help="read pairs of the FASTQ -> sorted BAM "
                     "stage (0 = skip)")
+    ap.add_argument("--fq2sam-pairs", type=int, default=2_000_000, help="read pairs of the FASTQ -> SAM stage "
+                    "(0 = skip)")
     ap.add_argument("--tuning", default="", help="fixed kernel choice 'seed_kernel,stage1_endpoints,"
                     "stage2_blocks_per_sm,reg_level,stage1_max_rows,stage2_first_wave[,wave_endpoints,"
                     "wave_loci_per_read,wave_max_rounds,wave_growth]' instead of the autotuner")
@@ -654,6 +656,85 @@ def run_fq2bam_stage(args, ctx, gi, rb, local, params):
         shutil.rmtree(d, ignore_errors=True)
 
 
+def run_fq2sam_stage(args, ctx, gi, rb, local, params, peaks):
+    """FASTQ files of the workload -> SAM text through map_fastq_to_sam (split,
+    mapping and SAM lines on the GPU; files read and the text written on the
+    host), the SAM emitter's device time inside it, and the same path
+    restated on the CPU from the oracle on a sample (mapping dominates)."""
+    import shutil
+    import sys as _sys
+
+    from mojoalign_b200.fq2sam import map_fastq_to_sam
+    from mojoalign_b200.linear_fm import sam_header
+
+    n = min(args.fq2sam_pairs, rb.n1)
+    d = Path(tempfile.mkdtemp(prefix="fq2sam_", dir=args.workdir))
+    try:
+        r1, r2 = d / "r1.fq", d / "r2.fq"
+        r1.write_bytes(fastq_text(rb, n, 1))
+        r2.write_bytes(fastq_text(rb, n, 2))
+        out = d / "out.sam"
+        fq_bytes = r1.stat().st_size + r2.stat().st_size
+        kw = dict(fq2=r2, bs_r1="C2T", bs_r2="G2A", params=params, environ={}, ctx=ctx, index=gi)
+        map_fastq_to_sam(None, r1, out, **kw)
+        times, phases = [], {}
+        for _ in range(max(1, min(args.steps, 3))):
+            ph = {}
+            t = time.perf_counter()
+            mapped = map_fastq_to_sam(None, r1, out, stats=ph, **kw)
+            times.append(time.perf_counter() - t)
+            if not phases or ph["emit_kernel_s"] < phases["emit_kernel_s"]:
+                phases = ph
+        wall = statistics.median(times)
+        sam_size = out.stat().st_size
+        # the emitter: algorithmic bytes = arena spans read once, 24 B of hit
+        # fields and 36 B of span columns per line, the text written once
+        emit_s = phases["emit_kernel_s"]
+        lines = phases["emit_lines"]
+        alg = phases["emit_arena_bytes"] + 60 * lines + phases["emit_text_bytes"]
+        achieved = alg / emit_s / 1e9
+        # parity + CPU baseline on a sample of the same reads
+        ns = 20_000
+        t1, t2 = fastq_text(rb, ns, 1), fastq_text(rb, ns, 2)
+        s1, s2 = d / "s1.fq", d / "s2.fq"
+        s1.write_bytes(t1)
+        s2.write_bytes(t2)
+        so = d / "s.sam"
+        map_fastq_to_sam(None, s1, so, fq2=s2, bs_r1="C2T", bs_r2="G2A", params=params, environ={}, ctx=ctx,
+                         index=gi)
+        _sys.path.insert(0, str(ROOT / "tests"))
+        import fq2sam_oracle
+
+        t = time.perf_counter()
+        want, _ = fq2sam_oracle.fq2sam(args._prefix, None, None, params.as_list(), 1, 2,
+                                       [c.name for c in gi.contigs], b"mojo1", texts=(t1, t2))
+        cpu_s = time.perf_counter() - t
+        same = so.read_bytes() == sam_header(gi.contigs, {}).encode() + want
+        records = 2 * n
+        return {
+            "metric": "reads/s FASTQ -> SAM", "value": round(records / wall, 1), "unit": "reads/s",
+            "s_per_run": round(wall, 3), "phases_s": phases,
+            "config": {"workload": f"{n} PE 2x{READ_LEN} pairs of the workload as two FASTQ files "
+                                   f"({fq_bytes} bytes) -> one SAM file", "sam_bytes": sam_size,
+                       "mapped_records": mapped},
+            "e2e": {"value": round(records / wall, 1), "unit": "reads/s", "h2d_bytes_per_step": fq_bytes,
+                    "d2h_bytes_per_step": sam_size,
+                    "timing": "host wall clock of the whole call: file reads, every GPU stage, the file write"},
+            "emitter": {"lines_per_s": round(lines / emit_s, 1), "ms": round(emit_s * 1e3, 3),
+                        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"),
+                                     "unit": "GB/s", "frac": round(achieved / peaks.get("hbm_gbs"), 4),
+                                     "traffic": None, "alg_bytes": alg,
+                                     "alg": "name + SEQ + QUAL spans read once, 60 B of hit and span fields per "
+                                            "line, the text written once"}},
+            "cpu_baseline": {"value": round(2 * ns / cpu_s, 1), "unit": "reads/s", "cores": os.cpu_count(),
+                             "kind": "port", "sample": f"the first {ns} pairs through the oracle pipeline "
+                                                       f"(mapping on all cores), {cpu_s:.2f} s"},
+            "parity": {"reads": 2 * ns, "sam_file_identical": bool(same)},
+        }
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
 def run_sort_stage(args, ctx, rb, res, local, peaks):
     """Coordinate sort + duplicate marking + sorted gather of one BAM tile
     made of --sort-batches emitted batches: device-resident throughput, the
@@ -1001,6 +1082,10 @@ def run_ours(args, rank, world, local):
         torch.cuda.empty_cache()
         args._prefix = prefix
         line.setdefault("stages", {})["fq2bam"] = run_fq2bam_stage(args, ctx, gi, rb, local, params)
+    if rank == 0 and world == 1 and args.fq2sam_pairs > 0:
+        torch.cuda.empty_cache()
+        args._prefix = prefix
+        line.setdefault("stages", {})["fq2sam"] = run_fq2sam_stage(args, ctx, gi, rb, local, params, peaks)
     if rank == 0 and world == 1 and args.fastq_pairs > 0:
         torch.cuda.empty_cache()
         line.setdefault("stages", {})["fastq_split"] = run_fastq_stage(args, ctx, rb, local, peaks)

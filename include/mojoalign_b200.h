@@ -442,6 +442,24 @@ int ma_fastq_parse_device(ma_ctx* ctx, const uint8_t* d_buf, uint64_t n_bytes, i
                           uint32_t max_records, uint64_t base, const ma_fastq_records* d_out,
                           uint64_t* out3, void* stream);
 
+/* Which reader's rules a FASTQ split follows: the BAM path's
+ * (fq_read_batch above) or the SAM path's, fastq_batch.FastqPairReader
+ * (fq2bam-meth/python/fastq_batch.py:230-317 with _qname L18-28): every
+ * trailing '\r' dropped from a line, four lines per record whatever they
+ * hold, a non-empty unterminated rest is a line, and at the end of the stream
+ * a record cut short reads its missing lines as empty (no error). */
+#define MA_FASTQ_RULES_STREAM 0
+#define MA_FASTQ_RULES_PAIR_READER 1
+
+/* ma_fastq_parse / ma_fastq_parse_device under `rules` (those two are
+ * MA_FASTQ_RULES_STREAM). */
+int ma_fastq_parse_rules(ma_ctx* ctx, const uint8_t* buf, uint64_t n_bytes, int at_eof,
+                         uint32_t max_records, uint64_t base, int rules,
+                         const ma_fastq_records* out, uint64_t* out3);
+int ma_fastq_parse_rules_device(ma_ctx* ctx, const uint8_t* d_buf, uint64_t n_bytes, int at_eof,
+                                uint32_t max_records, uint64_t base, int rules,
+                                const ma_fastq_records* d_out, uint64_t* out3, void* stream);
+
 /* The mapper's input rows from parsed records: [n_seq][max_len] bytes, each
  * SEQ span followed by 'N' up to max_len, and the lengths (fq_pack_bases,
  * linear_fastq.mojo:454-492; the bases stay unconverted: the mapping call's
@@ -596,6 +614,64 @@ int ma_gather_sorted_bam_device(ma_ctx* ctx, uint64_t n, const uint32_t* d_perm,
                                 const uint8_t* const* d_chunks, const uint64_t* d_chunk_len,
                                 uint32_t n_chunks, uint8_t* d_out, uint64_t out_cap,
                                 uint64_t* d_status, void* stream);
+
+/* ---- SAM records of a mapped batch ---------------------------------- */
+
+/* Per rid, the canonical contig name the SAM text carries (_canonical_contig,
+ * fq2bam-meth/src/linear_gpu_locate.mojo:156-162: bwa-meth's leading f / r
+ * dropped) as a span of `names`, and a canonical id that is equal for two
+ * rids exactly when their canonical names are equal. */
+typedef struct ma_sam_contigs {
+    const uint8_t* names;
+    uint64_t names_bytes;
+    const uint64_t* name_off;
+    const uint32_t* name_len;
+    const uint32_t* canon;
+    uint32_t n;
+} ma_sam_contigs;
+
+/*
+ * The SAM text lines of one mapped batch: for each read (single-end) or pair
+ * (R1 line, then R2 line), in batch order.  Replaces the SAM loop of
+ * map_fastq_fm_gpu (fq2bam-meth/src/linear_gpu_fm.mojo:2787-2836) with
+ * _hit_from_fm (L987-1025), pair_hits and hit_to_sam_line
+ * (fq2bam-meth/src/linear_extend.mojo:263-320) and the RG tag of
+ * _sam_with_rg_fm (L80-81):
+ *   - unmapped (rid < 0, or no base left between the clips): FLAG 4, RNAME
+ *     "*", POS 0, MAPQ 0, CIGAR "*"; otherwise the hit's flag, RNAME the
+ *     canonical name, POS pos + 1, CIGAR [slS]mM[srS];
+ *   - SEQ the original bases (arena orig span), reverse-complemented on
+ *     flag 16 (byte-wise, any byte but A/C/G/T becomes N); QUAL the record's
+ *     qualities as they are (an empty span gives an empty field);
+ *   - pairs: flags 1|64 / 1|128; both placed on the same canonical contig:
+ *     flag 2, RNEXT "=", PNEXT the mate's POS, TLEN |POS2 - POS1| + len(SEQ2)
+ *     (negated on R2); otherwise flag 8 on the mate of an unplaced record and
+ *     RNEXT / PNEXT of a placed mate (a canonical name "*" counts as
+ *     unplaced);
+ *   - names: each byte >= 0x80 is written as U+FFFD (EF BF BD), the ASCII
+ *     decode with replacement of the reference's reader; SEQ and QUAL must be
+ *     valid UTF-8 (the reference decodes them strictly).
+ * Hits and arena columns hold R1 rows then R2 rows; the arena's qual_off
+ * must be set.  mapped receives the records whose RNAME is not "*".  Host
+ * buffers, synchronous.  Errors: MA_ERR_ARG "SAM batch buffer overflow"
+ * (sam_cap too small; sam_bytes still receives the size), "FASTQ SEQ/QUAL is
+ * not valid UTF-8", "hit rid outside the contig table", or an arena span
+ * outside the arena.
+ */
+int ma_emit_sam_batch(ma_ctx* ctx, const ma_hits* hits, uint32_t n1, int paired,
+                      const ma_fastq_arena* arena, const ma_sam_contigs* contigs,
+                      const uint8_t* rg, uint32_t rg_n, uint8_t* sam, uint64_t sam_cap,
+                      uint64_t* sam_bytes, uint64_t* mapped);
+
+/* Same on device buffers (hits, arena columns, contig table, rg, output),
+ * asynchronous on `stream`.  d_status (device, 3 x u64): [0] the batch's
+ * text size, [1] mapped records, [2] error bits (1 text larger than sam_cap,
+ * 2 SEQ/QUAL not valid UTF-8, 4 rid outside the contig table, 8 an arena span
+ * outside the arena).  Text is written only when [2] == 0. */
+int ma_emit_sam_batch_device(ma_ctx* ctx, const ma_hits* d_hits, uint32_t n1, int paired,
+                             const ma_fastq_arena* d_arena, const ma_sam_contigs* d_contigs,
+                             const uint8_t* d_rg, uint32_t rg_n, uint8_t* d_sam, uint64_t sam_cap,
+                             uint64_t* d_status, void* stream);
 
 /* ---- BGZF ------------------------------------------------------------ */
 

@@ -12,6 +12,7 @@
 #include "bam_pack.h"
 #include "bgzf.h"
 #include "fastq_parse.h"
+#include "sam_emit.h"
 #include "sort_markdup.h"
 #include "ma_device.cuh"
 #include "ma_internal.h"
@@ -111,6 +112,8 @@ struct ma_ctx {
     DevBuf fq_in, fq_out, fq_scratch, fq_newlines;
     // BGZF
     DevBuf bgzf_in, bgzf_out, bgzf_scratch;
+    // SAM text of a batch
+    DevBuf sam_in, sam_arena, sam_out, sam_scratch, sam_status;
 };
 
 struct ma_index {
@@ -1033,12 +1036,13 @@ const char* fastq_error(unsigned long long code) {
 // Parses on the device; outputs in d_out.  Returns the status of
 // fastq_parse_enqueue.
 void parse_on_device(ma_ctx* ctx, const uint8_t* d_buf, uint64_t n, int at_eof, uint32_t max_records, uint64_t base,
-                     const ma_fastq_records& d_out, cudaStream_t st, unsigned long long* status) {
+                     int rules, const ma_fastq_records& d_out, cudaStream_t st, unsigned long long* status) {
     if (n >= (uint64_t(1) << 32)) fail(MA_ERR_ARG, "a FASTQ buffer holds fewer than 2^32 bytes");
+    if (rules != MA_FASTQ_RULES_STREAM && rules != MA_FASTQ_RULES_PAIR_READER) fail(MA_ERR_ARG, "unknown FASTQ rules");
     const size_t scratch = fastq_scratch_bytes(n);
     ctx->fq_scratch.ensure(scratch);
     FastqRecordsDev o{d_out.name_off, d_out.name_len, d_out.seq_off, d_out.seq_len, d_out.qual_off, d_out.qual_len};
-    ctx->last_launches = fastq_parse_enqueue(d_buf, n, at_eof, max_records, base, o, ctx->fq_scratch.p, scratch,
+    ctx->last_launches = fastq_parse_enqueue(d_buf, n, at_eof, max_records, base, rules, o, ctx->fq_scratch.p, scratch,
                                              fq_newline_buffer, &ctx->fq_newlines, st, status);
     if (status[3]) fail(MA_ERR_FORMAT, fastq_error(status[3]));
 }
@@ -1049,8 +1053,8 @@ void check_records(const ma_fastq_records* o) {
 }
 }  // namespace
 
-int ma_fastq_parse(ma_ctx* ctx, const uint8_t* buf, uint64_t n_bytes, int at_eof, uint32_t max_records, uint64_t base,
-                   const ma_fastq_records* out, uint64_t* out3) {
+int ma_fastq_parse_rules(ma_ctx* ctx, const uint8_t* buf, uint64_t n_bytes, int at_eof, uint32_t max_records,
+                         uint64_t base, int rules, const ma_fastq_records* out, uint64_t* out3) {
     if (!ctx) return MA_ERR_ARG;
     return guarded(ctx, [&] {
         ctx->last_launches = 0;
@@ -1070,7 +1074,7 @@ int ma_fastq_parse(ma_ctx* ctx, const uint8_t* buf, uint64_t n_bytes, int at_eof
                            reinterpret_cast<uint64_t*>(o + 2 * b8 + 2 * b4),
                            reinterpret_cast<uint32_t*>(o + 3 * b8 + 2 * b4)};
         unsigned long long status[6] = {0, 0, 0, 0, 0, 0};
-        parse_on_device(ctx, ctx->fq_in.as<uint8_t>(), n_bytes, at_eof, max_records, base, d, st, status);
+        parse_on_device(ctx, ctx->fq_in.as<uint8_t>(), n_bytes, at_eof, max_records, base, rules, d, st, status);
         const uint64_t r = status[1];
         if (r) {
             ck(cudaMemcpyAsync(out->name_off, d.name_off, r * 8, cudaMemcpyDeviceToHost, st), "D2H records");
@@ -1087,8 +1091,9 @@ int ma_fastq_parse(ma_ctx* ctx, const uint8_t* buf, uint64_t n_bytes, int at_eof
     });
 }
 
-int ma_fastq_parse_device(ma_ctx* ctx, const uint8_t* d_buf, uint64_t n_bytes, int at_eof, uint32_t max_records,
-                          uint64_t base, const ma_fastq_records* d_out, uint64_t* out3, void* stream) {
+int ma_fastq_parse_rules_device(ma_ctx* ctx, const uint8_t* d_buf, uint64_t n_bytes, int at_eof,
+                                uint32_t max_records, uint64_t base, int rules, const ma_fastq_records* d_out,
+                                uint64_t* out3, void* stream) {
     if (!ctx) return MA_ERR_ARG;
     return guarded(ctx, [&] {
         ctx->last_launches = 0;
@@ -1098,11 +1103,22 @@ int ma_fastq_parse_device(ma_ctx* ctx, const uint8_t* d_buf, uint64_t n_bytes, i
         use_device(ctx);
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
         unsigned long long status[6] = {0, 0, 0, 0, 0, 0};
-        parse_on_device(ctx, d_buf, n_bytes, at_eof, max_records, base, *d_out, st, status);
+        parse_on_device(ctx, d_buf, n_bytes, at_eof, max_records, base, rules, *d_out, st, status);
         out3[0] = status[1];
         out3[1] = status[2];
         out3[2] = status[5];
     });
+}
+
+int ma_fastq_parse(ma_ctx* ctx, const uint8_t* buf, uint64_t n_bytes, int at_eof, uint32_t max_records, uint64_t base,
+                   const ma_fastq_records* out, uint64_t* out3) {
+    return ma_fastq_parse_rules(ctx, buf, n_bytes, at_eof, max_records, base, MA_FASTQ_RULES_STREAM, out, out3);
+}
+
+int ma_fastq_parse_device(ma_ctx* ctx, const uint8_t* d_buf, uint64_t n_bytes, int at_eof, uint32_t max_records,
+                          uint64_t base, const ma_fastq_records* d_out, uint64_t* out3, void* stream) {
+    return ma_fastq_parse_rules_device(ctx, d_buf, n_bytes, at_eof, max_records, base, MA_FASTQ_RULES_STREAM, d_out,
+                                       out3, stream);
 }
 
 int ma_fastq_rows_device(ma_ctx* ctx, const uint8_t* d_arena, const uint64_t* d_seq_off, const uint32_t* d_seq_len,
@@ -1115,6 +1131,169 @@ int ma_fastq_rows_device(ma_ctx* ctx, const uint8_t* d_arena, const uint64_t* d_
         use_device(ctx);
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
         ctx->last_launches = fastq_rows_enqueue(d_arena, d_seq_off, d_seq_len, n_seq, max_len, d_rows, d_lens, st);
+    });
+}
+
+namespace {
+uint64_t sam_lines_checked(const ma_hits* h, uint32_t n1, int paired, const ma_fastq_arena* a,
+                           const ma_sam_contigs* c, const uint8_t* rg, uint32_t rg_n, const uint8_t* out,
+                           uint64_t cap) {
+    const uint64_t n_seq = static_cast<uint64_t>(n1) * (paired ? 2 : 1);
+    if (!h || !a || !c) fail(MA_ERR_ARG, "null argument");
+    if (n_seq == 0) return 0;
+    if (!h->rid || !h->pos || !h->mapq || !h->flag || !h->sl || !h->sr) fail(MA_ERR_ARG, "null hit array");
+    if (!a->name_off || !a->name_len || !a->orig_off || !a->orig_len || !a->qual_off || !a->qual_len ||
+        (a->data_bytes && !a->data))
+        fail(MA_ERR_ARG, "null arena array (SAM needs qualities)");
+    if (c->n && (!c->name_off || !c->name_len || !c->canon || (c->names_bytes && !c->names)))
+        fail(MA_ERR_ARG, "null contig table array");
+    if ((rg_n && !rg) || (cap && !out)) fail(MA_ERR_ARG, "null argument");
+    return n_seq;
+}
+
+SamDev sam_view(const ma_hits& h, uint32_t n1, int paired, const ma_fastq_arena& a, const ma_sam_contigs& c,
+                const uint8_t* rg, uint32_t rg_n, uint8_t* out, uint64_t cap, unsigned long long* status) {
+    SamDev d{};
+    d.rid = h.rid;
+    d.pos = h.pos;
+    d.mapq = h.mapq;
+    d.flag = h.flag;
+    d.sl = h.sl;
+    d.sr = h.sr;
+    d.arena = a.data;
+    d.arena_bytes = a.data_bytes;
+    d.name_off = a.name_off;
+    d.name_len = a.name_len;
+    d.seq_off = a.orig_off;
+    d.seq_len = a.orig_len;
+    d.qual_off = a.qual_off;
+    d.qual_len = a.qual_len;
+    d.names = c.names;
+    d.names_bytes = c.names_bytes;
+    d.cname_off = c.name_off;
+    d.cname_len = c.name_len;
+    d.canon = c.canon;
+    d.n_contigs = c.n;
+    d.rg = rg;
+    d.rg_n = rg_n;
+    d.n1 = n1;
+    d.paired = paired ? 1 : 0;
+    d.sam = out;
+    d.cap = cap;
+    d.status = status;
+    return d;
+}
+
+const char* sam_error(unsigned long long bits) {
+    if (bits & 4) return "hit rid outside the contig table";
+    if (bits & 8) return "arena or contig-name span outside its buffer";
+    if (bits & 2) return "FASTQ SEQ/QUAL is not valid UTF-8";
+    return "SAM batch buffer overflow";
+}
+}  // namespace
+
+int ma_emit_sam_batch(ma_ctx* ctx, const ma_hits* hits, uint32_t n1, int paired, const ma_fastq_arena* arena,
+                      const ma_sam_contigs* contigs, const uint8_t* rg, uint32_t rg_n, uint8_t* sam,
+                      uint64_t sam_cap, uint64_t* sam_bytes, uint64_t* mapped) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->last_launches = 0;
+        if (!sam_bytes || !mapped) fail(MA_ERR_ARG, "null argument");
+        *sam_bytes = 0;
+        *mapped = 0;
+        const uint64_t n_seq = sam_lines_checked(hits, n1, paired, arena, contigs, rg, rg_n, sam, sam_cap);
+        if (n_seq == 0) return;
+        for (uint64_t i = 0; i < n_seq; ++i) {
+            const uint64_t n = arena->data_bytes;
+            const bool bad = arena->name_off[i] > n || arena->name_len[i] > n - arena->name_off[i] ||
+                             arena->orig_off[i] > n || arena->orig_len[i] > n - arena->orig_off[i] ||
+                             arena->qual_off[i] > n || arena->qual_len[i] > n - arena->qual_off[i];
+            if (bad) fail(MA_ERR_ARG, "arena span of record " + std::to_string(i) + " lies outside the arena");
+        }
+        for (uint32_t i = 0; i < contigs->n; ++i)
+            if (contigs->name_off[i] > contigs->names_bytes ||
+                contigs->name_len[i] > contigs->names_bytes - contigs->name_off[i])
+                fail(MA_ERR_ARG, "contig name span outside the name buffer");
+        use_device(ctx);
+        cudaStream_t st = ctx->stream;
+        auto al = [](uint64_t n) { return (n + 255) & ~uint64_t(255); };
+        const uint64_t hb = al(n_seq * 4), ob = al(n_seq * 8), cb4 = al(uint64_t(contigs->n) * 4),
+                       cb8 = al(uint64_t(contigs->n) * 8);
+        const uint64_t in_bytes = 6 * hb + 3 * ob + 3 * hb + cb8 + 2 * cb4 + al(contigs->names_bytes) + al(rg_n);
+        ctx->sam_in.ensure(in_bytes);
+        ctx->sam_arena.ensure(arena->data_bytes);
+        uint8_t* d = ctx->sam_in.as<uint8_t>();
+        auto put = [&](const void* src, uint64_t bytes, uint64_t slot) -> void* {
+            void* dst = d;
+            if (bytes) ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st), "H2D sam input");
+            d += slot;
+            return dst;
+        };
+        ma_hits dh{};
+        dh.rid = static_cast<int32_t*>(put(hits->rid, n_seq * 4, hb));
+        dh.pos = static_cast<uint32_t*>(put(hits->pos, n_seq * 4, hb));
+        dh.mapq = static_cast<uint32_t*>(put(hits->mapq, n_seq * 4, hb));
+        dh.flag = static_cast<int32_t*>(put(hits->flag, n_seq * 4, hb));
+        dh.sl = static_cast<uint32_t*>(put(hits->sl, n_seq * 4, hb));
+        dh.sr = static_cast<uint32_t*>(put(hits->sr, n_seq * 4, hb));
+        ma_fastq_arena da{};
+        da.data = ctx->sam_arena.as<uint8_t>();
+        da.data_bytes = arena->data_bytes;
+        if (arena->data_bytes)
+            ck(cudaMemcpyAsync(ctx->sam_arena.p, arena->data, arena->data_bytes, cudaMemcpyHostToDevice, st),
+               "H2D arena");
+        da.name_off = static_cast<const uint64_t*>(put(arena->name_off, n_seq * 8, ob));
+        da.orig_off = static_cast<const uint64_t*>(put(arena->orig_off, n_seq * 8, ob));
+        da.qual_off = static_cast<const uint64_t*>(put(arena->qual_off, n_seq * 8, ob));
+        da.name_len = static_cast<const uint32_t*>(put(arena->name_len, n_seq * 4, hb));
+        da.orig_len = static_cast<const uint32_t*>(put(arena->orig_len, n_seq * 4, hb));
+        da.qual_len = static_cast<const uint32_t*>(put(arena->qual_len, n_seq * 4, hb));
+        ma_sam_contigs dc{};
+        dc.n = contigs->n;
+        dc.names_bytes = contigs->names_bytes;
+        dc.name_off = static_cast<const uint64_t*>(put(contigs->name_off, uint64_t(contigs->n) * 8, cb8));
+        dc.name_len = static_cast<const uint32_t*>(put(contigs->name_len, uint64_t(contigs->n) * 4, cb4));
+        dc.canon = static_cast<const uint32_t*>(put(contigs->canon, uint64_t(contigs->n) * 4, cb4));
+        dc.names = static_cast<const uint8_t*>(put(contigs->names, contigs->names_bytes, al(contigs->names_bytes)));
+        const uint8_t* d_rg = static_cast<const uint8_t*>(put(rg, rg_n, al(rg_n)));
+        ctx->sam_status.ensure(4 * sizeof(unsigned long long));
+        unsigned long long* d_status = ctx->sam_status.as<unsigned long long>();
+        ck(cudaMemsetAsync(d_status, 0, 3 * sizeof(unsigned long long), st), "memset");
+        ctx->sam_out.ensure(sam_cap ? sam_cap : 1);
+        const size_t scratch = sam_scratch_bytes(n_seq);
+        ctx->sam_scratch.ensure(scratch);
+        SamDev v = sam_view(dh, n1, paired, da, dc, d_rg, rg_n, ctx->sam_out.as<uint8_t>(), sam_cap, d_status);
+        ctx->last_launches = enqueue_sam(v, ctx->sam_scratch.p, scratch, ctx->sm_count, st);
+        unsigned long long status[3] = {0, 0, 0};
+        ck(cudaMemcpyAsync(status, d_status, sizeof(status), cudaMemcpyDeviceToHost, st), "D2H sam status");
+        ck(cudaStreamSynchronize(st), "sam");
+        *sam_bytes = status[0];
+        if (status[2]) fail(MA_ERR_ARG, sam_error(status[2]));
+        if (status[0]) {
+            ck(cudaMemcpyAsync(sam, ctx->sam_out.p, status[0], cudaMemcpyDeviceToHost, st), "D2H sam");
+            ck(cudaStreamSynchronize(st), "D2H sam");
+        }
+        *mapped = status[1];
+    });
+}
+
+int ma_emit_sam_batch_device(ma_ctx* ctx, const ma_hits* d_hits, uint32_t n1, int paired,
+                             const ma_fastq_arena* d_arena, const ma_sam_contigs* d_contigs, const uint8_t* d_rg,
+                             uint32_t rg_n, uint8_t* d_sam, uint64_t sam_cap, uint64_t* d_status, void* stream) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->last_launches = 0;
+        if (!d_status) fail(MA_ERR_ARG, "null argument");
+        const uint64_t n_seq = sam_lines_checked(d_hits, n1, paired, d_arena, d_contigs, d_rg, rg_n, d_sam, sam_cap);
+        use_device(ctx);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+        unsigned long long* status = reinterpret_cast<unsigned long long*>(d_status);
+        ck(cudaMemsetAsync(status, 0, 3 * sizeof(unsigned long long), st), "memset");
+        if (n_seq == 0) return;
+        const size_t scratch = sam_scratch_bytes(n_seq);
+        ctx->sam_scratch.ensure(scratch);
+        SamDev v = sam_view(*d_hits, n1, paired, *d_arena, *d_contigs, d_rg, rg_n, d_sam, sam_cap, status);
+        ctx->last_launches = enqueue_sam(v, ctx->sam_scratch.p, scratch, ctx->sm_count, st);
     });
 }
 

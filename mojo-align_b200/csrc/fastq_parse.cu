@@ -1,9 +1,15 @@
 // fastq_parse.cu - FASTQ record split on the device.
 //
-// Replaces the host record split of the FM path's FASTQ reader
-// (fq2bam-meth/src/linear_fastq.mojo: _pipe_line L233-280, _qname_span
-// L308-325, _store_rec L365-417, fq_read_batch L437-451) and the row
-// packing fq_pack_bases (L454-492).  The reference walks the decompressed
+// Replaces the host record split of the FM path's two FASTQ readers and
+// the row packing fq_pack_bases (fq2bam-meth/src/linear_fastq.mojo:454-492):
+//   rules 0, the BAM path's reader (linear_fastq.mojo: _pipe_line L233-280,
+//     _qname_span L308-325, _store_rec L365-417, fq_read_batch L437-451):
+//     one trailing '\r' dropped per line, a record cut short is an error;
+//   rules 1, the SAM path's reader (fq2bam-meth/python/fastq_batch.py:
+//     _qname L18-28, FastqPairReader._one / read_batch L250-317): every
+//     trailing '\r' dropped, four lines per record whatever they hold, and
+//     at the end of the stream a record cut short reads its missing lines
+//     as empty.  The reference walks the decompressed
 // bytes one record at a time on one host thread and copies name, original
 // bases, converted bases and qualities into an arena; here the uncompressed
 // bytes are copied to HBM once and become the arena themselves:
@@ -14,8 +20,8 @@
 //      consumed and the truncation error, exactly as the reference's line
 //      reader sees the stream;
 //   3. fq_records_kernel: one thread per record, name span (leading '@'
-//      dropped, cut at ' ' or '/'), SEQ and QUAL spans with one trailing
-//      '\r' dropped, the longest SEQ;
+//      dropped, cut at ' ' or '/'), SEQ and QUAL spans without their
+//      trailing '\r' (one, or all), the longest SEQ;
 //   4. fq_rows_kernel: one warp per read builds the padded row the mapper
 //      takes ('N' fill).  The C->T / G->A conversion is applied by the
 //      mapper's pack kernel, so the rows hold the original bases.
@@ -89,24 +95,30 @@ __global__ void nl_write_kernel(const uint8_t* buf, uint64_t n, uint64_t n_seg, 
 
 // st[0] lines, [1] records, [2] bytes consumed, [3] error (0, or 1/2/3 for a
 // record missing its SEQ / + / QUAL line), [4] newlines, [5] max SEQ length
-__global__ void fq_lines_kernel(const uint8_t* buf, uint64_t n, int at_eof, uint64_t max_records, const uint32_t* nl,
-                                const uint32_t* seg_base, const uint32_t* counts, uint64_t n_seg,
+__global__ void fq_lines_kernel(const uint8_t* buf, uint64_t n, int at_eof, uint64_t max_records, int rules,
+                                const uint32_t* nl, const uint32_t* seg_base, const uint32_t* counts, uint64_t n_seg,
                                 unsigned long long* st) {
     const uint64_t n_nl = n_seg ? static_cast<uint64_t>(seg_base[n_seg - 1]) + counts[n_seg - 1] : 0;
     const uint64_t rest = n_nl ? static_cast<uint64_t>(nl[n_nl - 1]) + 1 : 0;
     uint64_t lines = n_nl;
-    if (at_eof && rest < n) {  // an unterminated last line counts when not empty after the '\r' strip
-        uint64_t e = n;
-        if (buf[e - 1] == 13) --e;
-        if (e > rest) ++lines;
+    if (at_eof && rest < n) {
+        if (rules == 1) {
+            ++lines;  // readline() returns any non-empty rest
+        } else {      // the rest counts when not empty after the '\r' strip
+            uint64_t e = n;
+            if (buf[e - 1] == 13) --e;
+            if (e > rest) ++lines;
+        }
     }
-    const uint64_t whole = lines / 4;
+    // rules 1 at the end of the stream: a header line starts a record, its
+    // missing lines read as empty
+    const uint64_t whole = (rules == 1 && at_eof) ? (lines + 3) / 4 : lines / 4;
     const uint64_t recs = whole < max_records ? whole : max_records;
     st[0] = lines;
     st[1] = recs;
     // the reference reads one record past the complete ones only while it
     // still wants records
-    st[3] = (at_eof && max_records > whole && (lines & 3)) ? (lines & 3) : 0;
+    st[3] = (rules == 0 && at_eof && max_records > whole && (lines & 3)) ? (lines & 3) : 0;
     uint64_t consumed = 0;
     if (recs) {
         const uint64_t last = 4 * recs - 1;  // index of the last QUAL line
@@ -117,18 +129,28 @@ __global__ void fq_lines_kernel(const uint8_t* buf, uint64_t n, int at_eof, uint
     st[5] = 0;
 }
 
-__global__ void fq_records_kernel(const uint8_t* buf, uint64_t n, uint64_t base, const uint32_t* nl, uint64_t n_nl,
-                                  const unsigned long long* st, FastqRecordsDev out, unsigned long long* max_len) {
+__global__ void fq_records_kernel(const uint8_t* buf, uint64_t n, uint64_t base, int rules, const uint32_t* nl,
+                                  uint64_t n_nl, const unsigned long long* st, FastqRecordsDev out,
+                                  unsigned long long* max_len) {
     const uint64_t r = static_cast<uint64_t>(blockIdx.x) * THREADS + threadIdx.x;
     uint32_t seq_len = 0;
     if (r < st[1]) {
+        const uint64_t lines = st[0];
         uint64_t s[4], e[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const uint64_t li = 4 * r + k;
+            if (li >= lines) {  // past the end of the stream (rules 1): empty
+                s[k] = e[k] = n;
+                continue;
+            }
             s[k] = li ? static_cast<uint64_t>(nl[li - 1]) + 1 : 0;
             e[k] = li < n_nl ? nl[li] : n;
-            if (e[k] > s[k] && buf[e[k] - 1] == 13) --e[k];
+            if (rules == 1) {
+                while (e[k] > s[k] && buf[e[k] - 1] == 13) --e[k];
+            } else if (e[k] > s[k] && buf[e[k] - 1] == 13) {
+                --e[k];
+            }
         }
         uint64_t ns = s[0], ne = e[0];
         if (ne > ns && buf[ns] == 64) ++ns;
@@ -174,7 +196,7 @@ size_t fastq_scratch_bytes(uint64_t n_bytes) {
     return 2 * align256(n_seg * 4) + 256 + align256(t);
 }
 
-int fastq_parse_enqueue(const uint8_t* buf, uint64_t n, int at_eof, uint64_t max_records, uint64_t base,
+int fastq_parse_enqueue(const uint8_t* buf, uint64_t n, int at_eof, uint64_t max_records, uint64_t base, int rules,
                         const FastqRecordsDev& out, void* scratch, size_t scratch_bytes,
                         void* (*newline_buffer)(void* user, size_t bytes), void* user, cudaStream_t st,
                         unsigned long long* h_status) {
@@ -205,7 +227,7 @@ int fastq_parse_enqueue(const uint8_t* buf, uint64_t n, int at_eof, uint64_t max
         check_launch(cudaGetLastError(), "nl_write_kernel");
         ++launches;
     }
-    fq_lines_kernel<<<1, 1, 0, st>>>(buf, n, at_eof, max_records, nl, seg_base, counts, n_seg, status);
+    fq_lines_kernel<<<1, 1, 0, st>>>(buf, n, at_eof, max_records, rules, nl, seg_base, counts, n_seg, status);
     check_launch(cudaGetLastError(), "fq_lines_kernel");
     ++launches;
     unsigned long long head[6];
@@ -214,7 +236,7 @@ int fastq_parse_enqueue(const uint8_t* buf, uint64_t n, int at_eof, uint64_t max
     const uint64_t recs = head[1];
     if (recs) {
         const unsigned g = static_cast<unsigned>((recs + THREADS - 1) / THREADS);
-        fq_records_kernel<<<g, THREADS, 0, st>>>(buf, n, base, nl, head[4], status, out, status + 5);
+        fq_records_kernel<<<g, THREADS, 0, st>>>(buf, n, base, rules, nl, head[4], status, out, status + 5);
         check_launch(cudaGetLastError(), "fq_records_kernel");
         ++launches;
         check_launch(cudaMemcpyAsync(head + 5, status + 5, 8, cudaMemcpyDeviceToHost, st), "D2H max_len");

@@ -21,12 +21,13 @@ struct FastqRecordsDev {
 
 size_t fastq_scratch_bytes(uint64_t n_bytes);
 
-// Splits buf[0, n) into records (synchronous on st).  newline_buffer(user,
+// Splits buf[0, n) into records (synchronous on st) under `rules`: 0 the
+// BAM path's reader (linear_fastq.mojo), 1 the SAM path's (fastq_batch.py).  newline_buffer(user,
 // bytes) supplies the device array of newline positions once their count is
 // known.  h_status: [0] lines, [1] records, [2] bytes consumed, [3] error (0,
 // or 1/2/3: a record missing its SEQ / + / QUAL line), [4] newlines, [5] the
 // longest SEQ.  Returns the number of kernels launched.
-int fastq_parse_enqueue(const uint8_t* buf, uint64_t n, int at_eof, uint64_t max_records, uint64_t base,
+int fastq_parse_enqueue(const uint8_t* buf, uint64_t n, int at_eof, uint64_t max_records, uint64_t base, int rules,
                         const FastqRecordsDev& out, void* scratch, size_t scratch_bytes,
                         void* (*newline_buffer)(void* user, size_t bytes), void* user, cudaStream_t st,
                         unsigned long long* h_status);

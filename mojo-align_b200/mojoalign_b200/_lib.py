@@ -152,6 +152,15 @@ class ma_fastq_records(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("name_off", "name_len", "seq_off", "seq_len", "qual_off", "qual_len")]
 
 
+class ma_sam_contigs(C.Structure):
+    _fields_ = [("names", C.c_void_p), ("names_bytes", C.c_uint64), ("name_off", C.c_void_p), ("name_len", C.c_void_p),
+                ("canon", C.c_void_p), ("n", C.c_uint32)]
+
+
+MA_FASTQ_RULES_STREAM = 0
+MA_FASTQ_RULES_PAIR_READER = 1
+
+
 class ma_bam_meta(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("coord", "dhi", "dlo", "rec", "len", "score", "pair")]
 
@@ -230,6 +239,18 @@ SIGNATURES = [
     ("ma_fastq_parse_device", C.c_int,
      [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_uint32, C.c_uint64, C.POINTER(ma_fastq_records),
       C.POINTER(C.c_uint64), C.c_void_p]),
+    ("ma_fastq_parse_rules", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_uint32, C.c_uint64, C.c_int, C.POINTER(ma_fastq_records),
+      C.POINTER(C.c_uint64)]),
+    ("ma_fastq_parse_rules_device", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_uint32, C.c_uint64, C.c_int, C.POINTER(ma_fastq_records),
+      C.POINTER(C.c_uint64), C.c_void_p]),
+    ("ma_emit_sam_batch", C.c_int,
+     [C.c_void_p, C.POINTER(ma_hits), C.c_uint32, C.c_int, C.POINTER(ma_fastq_arena), C.POINTER(ma_sam_contigs),
+      C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("ma_emit_sam_batch_device", C.c_int,
+     [C.c_void_p, C.POINTER(ma_hits), C.c_uint32, C.c_int, C.POINTER(ma_fastq_arena), C.POINTER(ma_sam_contigs),
+      C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     ("ma_fastq_rows_device", C.c_int,
      [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("ma_bgzf_compress", C.c_int,

@@ -36,6 +36,7 @@ from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
+from . import pinned
 from ._lib import check, lib, ma_bam_meta, ma_bam_tile, ma_fastq_arena, ma_fastq_records, ma_hits
 from .bam import META_FIELDS, canonical_rid_to_tid
 from .linear_fm import canonical_contig, fm_prefix_from_ref, select_device
@@ -87,7 +88,8 @@ class _Feed:
     def __init__(self, path: str, chunk: int, torch):
         low = path.lower()
         self.fh = gzip.open(path, "rb") if (low.endswith(".gz") or low.endswith(".gzip")) else open(path, "rb")
-        self.pin = torch.empty(chunk, dtype=torch.uint8, pin_memory=True).numpy()
+        self._buf = pinned.take(chunk)
+        self.pin = self._buf[:chunk].numpy()
         self.len = 0
         self.eof = False
 
@@ -108,6 +110,8 @@ class _Feed:
 
     def close(self):
         self.fh.close()
+        pinned.give(self._buf)
+        self._buf = None
 
 
 class _Grow:
@@ -315,10 +319,13 @@ def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", 
                                           C.byref(got), sh), ctx.handle)
         tm["bgzf"] = time.perf_counter() - t0
         t0 = time.perf_counter()
-        host_out = torch.empty(got.value, dtype=torch.uint8, pin_memory=True)
-        host_out.copy_(d_out[: got.value])
-        with open(out_bam, "wb") as fh:
-            fh.write(memoryview(host_out.numpy()))
+        host_out = pinned.take(got.value)
+        try:
+            host_out[: got.value].copy_(d_out[: got.value])
+            with open(out_bam, "wb") as fh:
+                fh.write(memoryview(host_out.numpy())[: got.value])
+        finally:
+            pinned.give(host_out)
         tm["write"] = time.perf_counter() - t0
         tm["total"] = time.perf_counter() - t_start
         if stats is not None:

@@ -5,13 +5,19 @@ follows fq2bam-meth/src/linear_gpu_fm.mojo:1028-3341 on its SAM path:
 
 - the index prefix is resolved like fm_prefix_from_ref
   (fq2bam-meth/src/linear_fm_index.mojo:350-358);
-- FASTQ batches of METHYLGRAPHER_LINEAR_READ_BATCH pairs are mapped on the
-  GPU (conversion by bs_r1 / bs_r2 on the device);
-- records are written as the reference writes them: _hit_from_fm
-  (linear_gpu_fm.mojo:987-1025), pair_hits and hit_to_sam_line
-  (fq2bam-meth/src/linear_extend.mojo:263-320), the RG tag of
-  _sam_with_rg_fm (L80-81) and the header of _write_sam_header_fm (L40-76);
+- FASTQ is split on the device under the rules of the SAM path's reader
+  (fastq_batch.FastqPairReader), mapped on the GPU (conversion by bs_r1 /
+  bs_r2 on the device), and the SAM lines are built on the device
+  (mojoalign_b200.fq2sam.map_fastq_to_sam, ma_emit_sam_batch_device) as the
+  reference writes them: _hit_from_fm (linear_gpu_fm.mojo:987-1025),
+  pair_hits and hit_to_sam_line (fq2bam-meth/src/linear_extend.mojo:263-320),
+  the RG tag of _sam_with_rg_fm (L80-81), after the header of
+  _write_sam_header_fm (L40-76);
 - the return value is the number of mapped records.
+
+The per-record functions below (hit_from_fm, pair_hits, hit_to_sam_line,
+reverse_complement) restate the reference's record rules for Python callers;
+the drop-in's own SAM text comes from the device.
 
 A .bam destination takes the reference's BAM path on the GPU end to end
 (mojoalign_b200.fq2bam.map_fastq_to_bam): record packing, coordinate sort,
@@ -23,11 +29,10 @@ import os
 from dataclasses import dataclass, replace
 from pathlib import Path
 
-from .fastq import FastqPairStream, pack_bases
-from .mapper import GpuContext, GpuIndex, map_batch
-from .params import READ_BATCH_ENV, FmParams, env_int
+from .mapper import GpuContext, GpuIndex
+from .params import FmParams
 
-_RC = bytes.maketrans(b"ACGT", b"TGCA")
+_RC_BYTES = bytes(ord({"A": "T", "T": "A", "C": "G", "G": "C"}.get(chr(c), "N")) for c in range(256))
 
 
 def canonical_contig(name: str) -> str:
@@ -39,14 +44,9 @@ def canonical_contig(name: str) -> str:
 
 def reverse_complement(seq: str) -> str:
     """utility.reverse_complement (methylgrapher/src/utility.mojo:28-49):
-    A<->T, C<->G, any other byte (lower case included) -> N."""
-    b = seq.encode("ascii", "replace")
-    out = bytearray(b.translate(_RC)[::-1])
-    src = b[::-1]
-    for i, ch in enumerate(src):
-        if ch not in b"ACGT":
-            out[i] = ord("N")
-    return out.decode("ascii")
+    byte-wise over the UTF-8 bytes, A<->T, C<->G, any other byte (lower case
+    included) -> N."""
+    return bytes(_RC_BYTES[c] for c in reversed(seq.encode("utf-8"))).decode("ascii")
 
 
 @dataclass
@@ -67,9 +67,9 @@ class LinearHit:
 
 def hit_from_fm(contig_names, name: str, align_seq: str, original_seq: str, rid: int, start0: int, mapq: int,
                 flag: int, soft_l: int, soft_r: int) -> LinearHit:
-    """_hit_from_fm, linear_gpu_fm.mojo:987-1025."""
-    qlen = len(align_seq)
-    emit = original_seq if original_seq else align_seq
+    """_hit_from_fm, linear_gpu_fm.mojo:987-1025 (lengths in bytes)."""
+    qlen = len(align_seq.encode("utf-8"))
+    emit = original_seq if original_seq.encode("utf-8") else align_seq
     if rid < 0:
         return LinearHit(name, 4, "*", 0, 0, "*", emit, "*")
     m = qlen - soft_l - soft_r
@@ -91,7 +91,7 @@ def pair_hits(h1: LinearHit, h2: LinearHit) -> tuple[LinearHit, LinearHit]:
         a.rnext = b.rnext = "="
         a.pnext = b.pos
         b.pnext = a.pos
-        tlen = abs(b.pos - a.pos) + len(b.seq)
+        tlen = abs(b.pos - a.pos) + len(b.seq.encode("utf-8"))
         a.tlen = tlen
         b.tlen = -tlen
     else:
@@ -170,53 +170,6 @@ def map_fastq_fm_gpu(ref_fa, fq1, out_sam, device: str = "auto", fq2: str = "", 
 
         return map_fastq_to_bam(ref_fa, fq1, out_sam, device, fq2, bs_r1, bs_r2, params, env, kmer_k, kmer3_k,
                                 ctx, index)
-    params = params or FmParams.from_env(env)
-    batch = env_int(READ_BATCH_ENV[0], READ_BATCH_ENV[1], env)
-    own_ctx = ctx is None
-    ctx = ctx or GpuContext(select_device(device))
-    own_index = index is None
-    if index is None:
-        k3 = min(params.seed_len, 18) if kmer3_k is None else kmer3_k
-        index = GpuIndex(ctx, fm_prefix_from_ref(ref_fa), kmer_k=min(kmer_k, params.seed_len), kmer3_k=k3)
-    paired = len(str(fq2)) > 0
-    names = [c.name for c in index.contigs]
-    rg = _env_str("METHYLGRAPHER_RG_ID", "mojo1", env)
-    n_mapped = 0
-    try:
-        with open(out_sam, "w") as fh, FastqPairStream(str(fq1), str(fq2), "", "") as stream:
-            fh.write(sam_header(index.contigs, env))
-            while True:
-                a = stream.read_batch(batch)
-                if a.n1 == 0:
-                    break
-                max_len = max(a.max_len, params.seed_len)
-                if max_len > 1024:
-                    raise RuntimeError("read longer than FM base cap (1024)")
-                bases, lens = pack_bases(a, paired, max_len, converted=False)
-                r = map_batch(ctx, index, bases, lens, a.n1, paired, max_len, bs_r1, bs_r2, params)
-                out = []
-                for i in range(a.n1):
-                    h1 = hit_from_fm(names, a.name1[i].decode(), a.seq1[i].decode(), a.orig1[i].decode(),
-                                     int(r.rid[i]), int(r.pos[i]), int(r.mapq[i]), int(r.flag[i]), int(r.sl[i]),
-                                     int(r.sr[i]))
-                    h1.qual = a.qual1[i].decode()
-                    if not paired:
-                        n_mapped += h1.contig != "*"
-                        out.append(hit_to_sam_line(h1) + "\tRG:Z:" + rg)
-                        continue
-                    j = a.n1 + i
-                    h2 = hit_from_fm(names, a.name2[i].decode(), a.seq2[i].decode(), a.orig2[i].decode(),
-                                     int(r.rid[j]), int(r.pos[j]), int(r.mapq[j]), int(r.flag[j]), int(r.sl[j]),
-                                     int(r.sr[j]))
-                    h2.qual = a.qual2[i].decode()
-                    p1, p2 = pair_hits(h1, h2)
-                    n_mapped += (p1.contig != "*") + (p2.contig != "*")
-                    out.append(hit_to_sam_line(p1) + "\tRG:Z:" + rg)
-                    out.append(hit_to_sam_line(p2) + "\tRG:Z:" + rg)
-                fh.write("\n".join(out) + "\n")
-    finally:
-        if own_index:
-            index.close()
-        if own_ctx:
-            ctx.close()
-    return n_mapped
+    from .fq2sam import map_fastq_to_sam
+
+    return map_fastq_to_sam(ref_fa, fq1, out_sam, device, fq2, bs_r1, bs_r2, params, env, kmer_k, kmer3_k, ctx, index)

@@ -89,6 +89,11 @@ def _load():
     lib.orc_fastq_parse.argtypes = [vp, C.c_uint64, C.c_int, C.c_uint64, C.c_uint64] + [vp] * 6 + \
         [C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]
     lib.orc_fastq_parse.restype = C.c_int64
+    lib.orc_fastq_parse_pr.argtypes = lib.orc_fastq_parse.argtypes
+    lib.orc_fastq_parse_pr.restype = C.c_int64
+    lib.orc_emit_sam.argtypes = [vp] * 6 + [C.c_uint64, C.c_int] + [vp] * 7 + [vp] * 4 + \
+        [C.c_uint32, C.c_char_p, C.c_uint32, vp, C.c_uint64, C.POINTER(C.c_uint64)]
+    lib.orc_emit_sam.restype = C.c_int64
     return lib
 
 
@@ -311,3 +316,69 @@ def convert(seq: bytes, mode: int) -> bytes:
 
 def max_threads() -> int:
     return lib.orc_max_threads()
+
+
+REC_KEYS = ("name_off", "name_len", "seq_off", "seq_len", "qual_off", "qual_len")
+
+
+def fastq_parse_pr(buf, at_eof: bool = True, max_records: int | None = None, base: int = 0) -> dict:
+    """orc_fastq_parse_pr: the record split of FastqPairReader (fq2bam-meth/
+    python/fastq_batch.py:18-317), the reader of the SAM path, over one
+    buffer.  Same result keys as fastq_parse; never raises."""
+    b = np.frombuffer(bytes(buf), np.uint8)
+    cap = b.size // 4 + 2 if max_records is None else max_records
+    out = {k: np.zeros(max(cap, 1), np.uint64 if k.endswith("off") else np.uint32) for k in REC_KEYS}
+    consumed, ml = C.c_uint64(0), C.c_uint32(0)
+    n = lib.orc_fastq_parse_pr(_p(b) if b.size else None, b.size, int(at_eof), cap, base,
+                               *[_p(out[k]) for k in REC_KEYS], C.byref(consumed), C.byref(ml))
+    res = {k: v[:n].copy() for k, v in out.items()}
+    res.update(n=int(n), consumed=consumed.value, max_len=ml.value)
+    return res
+
+
+def sam_contigs(contig_names) -> dict:
+    """Per rid: the canonical name (_canonical_contig, linear_gpu_locate.mojo:
+    156-162, a leading f/r dropped from names of two or more bytes) and a
+    canonical id, equal exactly when the canonical names are equal."""
+    blob, off, ln, canon, ids = bytearray(), [], [], [], {}
+    for name in contig_names:
+        nb = name.encode() if isinstance(name, str) else bytes(name)
+        c = nb[1:] if len(nb) >= 2 and nb[:1] in (b"f", b"r") else nb
+        off.append(len(blob))
+        ln.append(len(c))
+        blob += c
+        canon.append(ids.setdefault(c, len(ids)))
+    return {"names": np.frombuffer(bytes(blob) or b"\0", np.uint8).copy(), "off": np.array(off, np.uint64),
+            "len": np.array(ln, np.uint32), "canon": np.array(canon, np.uint32)}
+
+
+SAM_ERRORS = {-1: "SAM batch buffer overflow", -2: "FASTQ SEQ/QUAL is not valid UTF-8",
+              -3: "hit rid outside the contig table"}
+
+
+def emit_sam(hits: dict, n1: int, paired: bool, arena: dict, contig_names, rg: bytes, cap: int | None = None):
+    """orc_emit_sam: the SAM lines of one mapped batch (_hit_from_fm, pair_hits,
+    hit_to_sam_line, _sam_with_rg_fm).  `hits`: rid/pos/mapq/flag/sl/sr rows
+    (R1 then R2); `arena`: data + the REC_KEYS columns in the same order.
+    Returns (text bytes, mapped records); raises RuntimeError on the errors of
+    SAM_ERRORS."""
+    t = sam_contigs(contig_names)
+    h = {k: np.ascontiguousarray(hits[k], dt) for k, dt in
+         (("rid", np.int32), ("pos", np.uint32), ("mapq", np.uint32), ("flag", np.int32), ("sl", np.uint32),
+          ("sr", np.uint32))}
+    a = {k: np.ascontiguousarray(arena[k], np.uint64 if k.endswith("off") else np.uint32) for k in REC_KEYS}
+    data = np.ascontiguousarray(np.frombuffer(bytes(arena["data"]), np.uint8) if not isinstance(arena["data"], np.ndarray)
+                                else arena["data"], np.uint8)
+    if cap is None:
+        n_seq = n1 * (2 if paired else 1)
+        cap = n_seq * (160 + len(rg)) + 3 * int(a["name_len"][:n_seq].sum()) + int(a["seq_len"][:n_seq].sum()) + \
+            int(a["qual_len"][:n_seq].sum()) + 2 * n_seq * int(t["len"].max(initial=1))
+    out = np.zeros(max(cap, 1), np.uint8)
+    mapped = C.c_uint64(0)
+    k = lib.orc_emit_sam(*[_p(h[x]) for x in ("rid", "pos", "mapq", "flag", "sl", "sr")], n1, int(paired),
+                         _p(data) if data.size else None, *[_p(a[x]) for x in REC_KEYS], _p(t["names"]), _p(t["off"]),
+                         _p(t["len"]), _p(t["canon"]), int(t["canon"].size), rg, len(rg), _p(out), cap,
+                         C.byref(mapped))
+    if k < 0:
+        raise RuntimeError(SAM_ERRORS[int(k)])
+    return out[:k].tobytes(), int(mapped.value)

@@ -10,6 +10,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
+import fq2sam_oracle
 import oracle
 from mojoalign_b200 import FmParams, synth
 from mojoalign_b200.linear_fm import hit_from_fm, hit_to_sam_line, map_fastq_fm_gpu, pair_hits, sam_header
@@ -95,3 +96,68 @@ def test_map_fastq_fm_gpu_matches_oracle_records(small_ref, tmp_path, paired, mo
     bad = [i for i, (a, b) in enumerate(zip(body, exp)) if a != b]
     assert not bad, f"{len(bad)} records differ; first:\n{body[bad[0]]}\n{exp[bad[0]]}"
     assert n_mapped == exp_mapped and 0 < n_mapped <= len(exp)
+
+
+def messy_fastq(rows, names, mate, seed):
+    """FASTQ text with mixed line ends (LF, CRLF, CR CR LF), names with
+    comments and bytes >= 0x80, and a last record cut after its SEQ line."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i, (nm, s) in enumerate(zip(names, rows)):
+        eol = [b"\n", b"\r\n", b"\r\r\n"][int(rng.integers(0, 3))]
+        q = bytes(33 + (k * 7 + len(s)) % 41 for k in range(len(s)))
+        head = b"@" + nm.encode() + (b"\xe9" if i % 97 == 5 else b"") + b"/%d x" % mate
+        out.append(head + eol + s.encode() + eol + b"+" + eol + q + eol)
+    out.append(b"@cut/%d\n" % mate + rows[0][:30].encode() + b"\n")
+    return b"".join(out)
+
+
+@pytest.mark.parametrize("paired", [True, False])
+def test_sam_path_on_messy_fastq_in_small_chunks(small_ref, tmp_path, paired):
+    from mojoalign_b200 import GpuContext, GpuIndex
+    from mojoalign_b200.fq2sam import map_fastq_to_sam
+
+    fa, prefix = small_ref
+    n1 = 1800
+    rows = reads(fa, n1, paired, seed=21 + paired)
+    names = [f"m{i}" for i in range(n1)]
+    t1 = messy_fastq(rows[:n1], names, 1, 5)
+    t2 = messy_fastq(rows[n1:], names, 2, 6) if paired else None
+    fq1, fq2 = tmp_path / "m1.fq", tmp_path / "m2.fq"
+    fq1.write_bytes(t1)
+    if paired:
+        fq2.write_bytes(t2)
+    params = FmParams.from_env({})
+    ctx = GpuContext(0)
+    gi = GpuIndex(ctx, prefix, kmer_k=12)
+    try:
+        out = tmp_path / "m.sam"
+        stats = {}
+        n_mapped = map_fastq_to_sam(fa, fq1, out, "auto", str(fq2) if paired else "", "C2T", "G2A", params, {},
+                                    ctx=ctx, index=gi, batch_pairs=700, chunk_bytes=64 << 10, stats=stats)
+        want, want_mapped = fq2sam_oracle.fq2sam(prefix, None, None, params.as_list(), 1, 2,
+                                                 [c.name for c in gi.contigs], b"mojo1", texts=(t1, t2))
+        hdr = sam_header(gi.contigs, {}).encode()
+    finally:
+        gi.close()
+        ctx.close()
+    got = out.read_bytes()
+    assert got[:len(hdr)] == hdr
+    body = got[len(hdr):]
+    if body != want:
+        a, b = body.split(b"\n"), want.split(b"\n")
+        bad = [i for i, (x, y) in enumerate(zip(a, b)) if x != y]
+        raise AssertionError(f"{len(a)} vs {len(b)} lines, {len(bad)} differ; first:\n{a[bad[0]] if bad else ''}\n"
+                             f"{b[bad[0]] if bad else ''}")
+    assert n_mapped == want_mapped
+    assert b"\xef\xbf\xbd" in body  # a name byte >= 0x80 became U+FFFD
+
+
+def test_sam_path_r2_ending_early_fails(small_ref, tmp_path):
+    fa, _ = small_ref
+    rows = reads(fa, 50, True, seed=3)
+    names = [f"e{i}" for i in range(50)]
+    (tmp_path / "a1.fq").write_bytes(messy_fastq(rows[:50], names, 1, 1))
+    (tmp_path / "a2.fq").write_bytes(messy_fastq(rows[50:90], names[:40], 2, 2))
+    with pytest.raises(RuntimeError, match="R2 ended early"):
+        map_fastq_fm_gpu(fa, tmp_path / "a1.fq", tmp_path / "a.sam", "auto", str(tmp_path / "a2.fq"), "C2T", "G2A")
