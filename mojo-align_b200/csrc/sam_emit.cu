@@ -6,18 +6,18 @@
 // (fq2bam-meth/src/linear_extend.mojo:263-294), formats each line with
 // hit_to_sam_line (L297-320) + the RG tag (_sam_with_rg_fm, L80-81) and
 // writes it.  Here the lines of a whole batch are built in HBM in three
-// passes over one warp per line:
-//   1. sam_layout_kernel: each line's byte length (the hit and its mate are
-//      both resolved, so pair fields are known), names' bytes >= 0x80
-//      counted (each becomes U+FFFD), SEQ / QUAL checked for strict UTF-8,
-//      mapped records and error bits gathered per block;
+// passes:
+//   1. sam_layout_kernel (one thread per pair): both hits and the pair
+//      fields, each line's byte length and a compact record of its fields,
+//      names' bytes >= 0x80 counted (each becomes U+FFFD), SEQ / QUAL
+//      checked for strict UTF-8, mapped records and error bits;
 //   2. a device scan of the lengths (line end offsets);
-//   3. sam_write_kernel: the line assembled in a per-warp shared-memory
-//      stage at its destination's 16-byte phase (lanes copy the name, the
+//   3. sam_write_kernel (one warp per line): the line assembled in a
+//      shared-memory stage at its destination's 16-byte phase (lanes copy the name, the
 //      contig names, SEQ reverse-complemented on flag 16, QUAL and the RG
 //      tag from aligned word loads; lane 0 writes the integer fields), then
-//      stored with 16-byte stores; lines longer than the stage and names
-//      that widen are built in place.
+//      stored with 16-byte stores; lines longer than the stage are built in
+//      place.
 #include <cub/device/device_scan.cuh>
 
 #include <string>
@@ -32,7 +32,7 @@ constexpr int THREADS = 256;
 constexpr int WARPS = THREADS / 32;
 constexpr unsigned FULL = 0xffffffffu;
 constexpr uint32_t STAGE = 2048;  // bytes of a warp's line stage in shared memory
-constexpr int SPAN_UNROLL = 4;    // words a lane loads per round of a span copy
+constexpr int SPAN_UNROLL = 2;    // words a lane loads per round of a span copy
 
 enum : unsigned { E_OVER = 1, E_UTF8 = 2, E_RID = 4, E_SPAN = 8 };
 enum : uint8_t { K_NAME = 0, K_STAR = 1, K_EQ = 2 };
@@ -132,27 +132,21 @@ __device__ void pair_up(Hit& a, Hit& b, uint32_t len2) {
     }
 }
 
-// The hit of line L after pairing, and its read index.
-__device__ Hit line_hit(const SamDev& d, uint64_t L, uint64_t& r, unsigned& err) {
-    if (!d.paired) {
-        r = L;
-        return hit_of(d, L, err);
-    }
-    const uint64_t p = L >> 1;
-    Hit a = hit_of(d, p, err);
-    Hit b = hit_of(d, p + d.n1, err);
-    pair_up(a, b, d.seq_len[p + d.n1]);
-    r = p + (L & 1) * d.n1;
-    return (L & 1) ? b : a;
-}
-
+// Decimal digits of u: comparisons against powers of ten below 2^32, a
+// division loop above.
 __device__ __forceinline__ uint32_t ndig(uint64_t u) {
-    uint32_t k = 1;
-    while (u >= 10) {
-        u /= 10;
-        ++k;
+    if (u >> 32) {
+        uint32_t k = 10;
+        u /= 10000000000ull;
+        while (u) {
+            u /= 10;
+            ++k;
+        }
+        return k;
     }
-    return k;
+    const uint32_t v = static_cast<uint32_t>(u);
+    return 1 + (v >= 10u) + (v >= 100u) + (v >= 1000u) + (v >= 10000u) + (v >= 100000u) + (v >= 1000000u) +
+           (v >= 10000000u) + (v >= 100000000u) + (v >= 1000000000u);
 }
 
 __device__ __forceinline__ uint64_t mag(int64_t v) {
@@ -214,44 +208,47 @@ __device__ __forceinline__ bool spans_ok(const SamDev& d, uint64_t r) {
            span_ok(d.qual_off[r], d.qual_len[r], d.arena_bytes);
 }
 
-__device__ __forceinline__ uint32_t warp_sum(uint32_t v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-    return v;
-}
+// What the write pass needs of a line, resolved once by the layout pass.
+struct LineRec {
+    int64_t flag, pos1, pnext, tlen;
+    uint64_t contig_off, rnext_off;
+    uint32_t mapq, sl, sr, m;
+    uint32_t contig_len, rnext_len;
+    uint8_t contig_kind, rnext_kind, mapped, widen;
+    uint32_t pad;
+};
+static_assert(sizeof(LineRec) == 80, "line record layout");
 
-// Calls f(j, byte) for every byte j of src[0, n): the lanes split the
-// aligned 4-byte words that cover the span, 512 bytes per round with the
-// round's loads issued together.  (A word is read whole; its bytes outside
-// the span lie in the same aligned word as a byte inside it.)
-template <typename F>
-__device__ __forceinline__ void for_span_bytes(const uint8_t* src, uint32_t n, int lane, F&& f) {
-    if (!n) return;
-    const uintptr_t a = reinterpret_cast<uintptr_t>(src);
-    const uint32_t* w0 = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
-    const uint32_t lead = static_cast<uint32_t>(a & 3);
-    const uint32_t nw = (lead + n + 3) >> 2;
-    for (uint32_t base = 0; base < nw; base += 32 * SPAN_UNROLL) {
-        uint32_t v[SPAN_UNROLL];
+// Bytes >= 0x80 in p[0, n), from the aligned 16-byte blocks that cover the
+// span (their bytes outside the span lie in the same block as one inside).
+__device__ __forceinline__ uint32_t count_high(const uint8_t* p, uint32_t n) {
+    if (!n) return 0;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p), e = a + n;
+    uint32_t c = 0;
+    for (uintptr_t q = a & ~uintptr_t(15); q < e; q += 16) {
+        const uint4 v = *reinterpret_cast<const uint4*>(q);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-        for (int t = 0; t < SPAN_UNROLL; ++t) {
-            const uint32_t i = base + 32 * t + lane;
-            v[t] = i < nw ? w0[i] : 0u;
-        }
+        for (int k = 0; k < 4; ++k) {
+            uint32_t m = w[k] & 0x80808080u;
+            if (m) {
 #pragma unroll
-        for (int t = 0; t < SPAN_UNROLL; ++t) {
-            const uint32_t i = base + 32 * t + lane;
-            if (i < nw) {
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int64_t j = static_cast<int64_t>(4 * i + k) - lead;
-                    if (j >= 0 && j < n) f(static_cast<uint32_t>(j), static_cast<uint8_t>(v[t] >> (8 * k)));
+                for (int b = 0; b < 4; ++b) {
+                    const uintptr_t x = q + 4 * k + b;
+                    if (x < a || x >= e) m &= ~(0x80u << (8 * b));
                 }
+                c += __popc(m);
             }
         }
     }
+    return c;
 }
 
-__global__ void __launch_bounds__(THREADS) sam_layout_kernel(SamDev d, uint64_t n_lines, uint32_t* line_len) {
+// One thread per pair (one per read single-end): both hits, the pairing,
+// each line's length and record; the SEQ / QUAL UTF-8 check; mapped records
+// and error bits gathered per block.
+__global__ void __launch_bounds__(THREADS) sam_layout_kernel(SamDev d, uint64_t n_units, uint32_t* line_len,
+                                                             LineRec* recs) {
     __shared__ unsigned long long blk_mapped;
     __shared__ unsigned blk_err;
     if (threadIdx.x == 0) {
@@ -259,42 +256,62 @@ __global__ void __launch_bounds__(THREADS) sam_layout_kernel(SamDev d, uint64_t 
         blk_err = 0;
     }
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const uint64_t w0 = (static_cast<uint64_t>(blockIdx.x) * THREADS + threadIdx.x) >> 5;
-    const uint64_t nw = static_cast<uint64_t>(gridDim.x) * WARPS;
     unsigned err = 0;
     uint32_t mapped = 0;
-    for (uint64_t L = w0; L < n_lines; L += nw) {
-        uint64_t r;
-        const Hit h = line_hit(d, L, r, err);
-        if (!spans_ok(d, r)) {
-            err |= E_SPAN;
-            if (lane == 0) line_len[L] = 0;
-            continue;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * THREADS;
+    for (uint64_t u = static_cast<uint64_t>(blockIdx.x) * THREADS + threadIdx.x; u < n_units; u += stride) {
+        Hit hs[2];
+        hs[0] = hit_of(d, u, err);
+        const int k = d.paired ? 2 : 1;
+        if (d.paired) {
+            hs[1] = hit_of(d, u + d.n1, err);
+            pair_up(hs[0], hs[1], d.seq_len[u + d.n1]);
         }
-        const uint8_t* nm = d.arena + d.name_off[r];
-        const uint8_t* sq = d.arena + d.seq_off[r];
-        const uint8_t* ql = d.arena + d.qual_off[r];
-        const uint32_t n_nm = d.name_len[r], n_sq = d.seq_len[r], n_ql = d.qual_len[r];
-        uint32_t high = 0, any = 0;
-        for_span_bytes(nm, n_nm, lane, [&](uint32_t, uint8_t c) { high += c >> 7; });
-        for_span_bytes(sq, n_sq, lane, [&](uint32_t, uint8_t c) { any |= c >> 7; });
-        for_span_bytes(ql, n_ql, lane, [&](uint32_t, uint8_t c) { any |= c >> 7; });
-        high = warp_sum(high);
-        if (__any_sync(FULL, any)) {  // rare: validate on one lane
-            bool ok = true;
-            if (lane == 0) ok = utf8_ok(sq, n_sq) && utf8_ok(ql, n_ql);
-            if (!__shfl_sync(FULL, ok, 0)) err |= E_UTF8;
-        }
-        const uint64_t len = head_len(h, n_nm + 2ull * high) + n_sq + 1 + n_ql + 6 + d.rg_n + 1;
-        if (len > 0xffffffffull) err |= E_OVER;
-        if (lane == 0) {
+        for (int m = 0; m < k; ++m) {
+            const Hit& h = hs[m];
+            const uint64_t r = u + static_cast<uint64_t>(m) * d.n1;
+            const uint64_t L = d.paired ? 2 * u + m : u;
+            if (!spans_ok(d, r)) {
+                err |= E_SPAN;
+                line_len[L] = 0;
+                continue;
+            }
+            const uint8_t* sq = d.arena + d.seq_off[r];
+            const uint8_t* ql = d.arena + d.qual_off[r];
+            const uint32_t n_nm = d.name_len[r], n_sq = d.seq_len[r], n_ql = d.qual_len[r];
+            const uint32_t high = count_high(d.arena + d.name_off[r], n_nm);
+            if ((count_high(sq, n_sq) || count_high(ql, n_ql)) && !(utf8_ok(sq, n_sq) && utf8_ok(ql, n_ql)))
+                err |= E_UTF8;
+            const uint64_t len = head_len(h, n_nm + 2ull * high) + n_sq + 1 + n_ql + 6 + d.rg_n + 1;
+            if (len > 0xffffffffull) err |= E_OVER;
             line_len[L] = static_cast<uint32_t>(len);
             mapped += !h.star;
+            LineRec rc;
+            rc.flag = h.flag;
+            rc.pos1 = h.pos1;
+            rc.pnext = h.pnext;
+            rc.tlen = h.tlen;
+            rc.contig_off = h.contig_off;
+            rc.rnext_off = h.rnext_off;
+            rc.mapq = static_cast<uint32_t>(h.mapq);
+            rc.sl = static_cast<uint32_t>(h.sl);
+            rc.sr = static_cast<uint32_t>(h.sr);
+            rc.m = static_cast<uint32_t>(h.mapped ? h.m : 0);
+            rc.contig_len = h.contig_len;
+            rc.rnext_len = h.rnext_len;
+            rc.contig_kind = h.contig_kind;
+            rc.rnext_kind = h.rnext_kind;
+            rc.mapped = h.mapped;
+            rc.widen = high != 0;
+            rc.pad = 0;
+            recs[L] = rc;
         }
     }
-    for (int o = 16; o > 0; o >>= 1) err |= __shfl_xor_sync(FULL, err, o);
-    if (lane == 0) {
+    for (int o = 16; o > 0; o >>= 1) {
+        err |= __shfl_xor_sync(FULL, err, o);
+        mapped += __shfl_xor_sync(FULL, mapped, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
         if (mapped) atomicAdd(&blk_mapped, static_cast<unsigned long long>(mapped));
         if (err) atomicOr(&blk_err, err);
     }
@@ -305,16 +322,74 @@ __global__ void __launch_bounds__(THREADS) sam_layout_kernel(SamDev d, uint64_t 
     }
 }
 
-__device__ __forceinline__ uint32_t put_int(uint8_t* o, int64_t v) {
-    const uint32_t k = sdig(v);
+// The aligned 4-byte words covering a span, up to 32 * SPAN_UNROLL of them
+// loaded at once (one round of loads for spans up to ~0.5 KB).
+struct SpanWords {
+    uint32_t v[SPAN_UNROLL];
+    uint32_t lead, nw;
+};
+
+__device__ __forceinline__ bool span_fits(const uint8_t* src, uint32_t n) {
+    return ((reinterpret_cast<uintptr_t>(src) & 3) + n + 3) / 4 <= 32u * SPAN_UNROLL;
+}
+
+__device__ __forceinline__ void span_load(SpanWords& s, const uint8_t* src, uint32_t n, int lane) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+    const uint32_t* w0 = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+    s.lead = static_cast<uint32_t>(a & 3);
+    s.nw = n ? (s.lead + n + 3) >> 2 : 0;
+#pragma unroll
+    for (int t = 0; t < SPAN_UNROLL; ++t) {
+        const uint32_t i = 32 * t + lane;
+        s.v[t] = i < s.nw ? w0[i] : 0u;
+    }
+}
+
+template <typename F>
+__device__ __forceinline__ void span_scatter(const SpanWords& s, uint32_t n, int lane, F&& f) {
+#pragma unroll
+    for (int t = 0; t < SPAN_UNROLL; ++t) {
+        const uint32_t i = 32 * t + lane;
+        if (i < s.nw) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const uint32_t j = 4 * i + k - s.lead;  // wraps below the span's start
+                if (j < n) f(j, static_cast<uint8_t>(s.v[t] >> (8 * k)));
+            }
+        }
+    }
+}
+
+// Calls f(j, byte) for every byte j of src[0, n), any length, 512 bytes per
+// round.
+template <typename F>
+__device__ __forceinline__ void for_span_bytes(const uint8_t* src, uint32_t n, int lane, F&& f) {
+    for (uint32_t b = 0; b < n;) {
+        const uint8_t* p = src + b;
+        const uint32_t lead = static_cast<uint32_t>(reinterpret_cast<uintptr_t>(p) & 3);
+        const uint32_t take = min(n - b, 32u * SPAN_UNROLL * 4 - lead);
+        SpanWords s;
+        span_load(s, p, take, lane);
+        span_scatter(s, take, lane, [&](uint32_t j, uint8_t c) { f(b + j, c); });
+        b += take;
+    }
+}
+
+// The decimal text of v at o (k = sdig(v) bytes); 32-bit divisions while
+// the value fits.
+__device__ __forceinline__ void put_int(uint8_t* o, int64_t v, uint32_t k) {
     uint64_t u = mag(v);
     uint32_t j = k;
-    do {
+    while (u >> 32) {
         o[--j] = static_cast<uint8_t>('0' + u % 10);
         u /= 10;
-    } while (u);
+    }
+    uint32_t x = static_cast<uint32_t>(u);
+    do {
+        o[--j] = static_cast<uint8_t>('0' + x % 10);
+        x /= 10;
+    } while (x);
     if (v < 0) o[0] = '-';
-    return k;
 }
 
 // Lanes copy a contig field: a name span, "*" or "=".
@@ -327,16 +402,25 @@ __device__ __forceinline__ void put_field(uint8_t* o, const SamDev& d, uint8_t k
     }
 }
 
+__device__ __forceinline__ uint8_t complement(uint8_t c) {
+    return c == 'A' ? 'T' : c == 'T' ? 'A' : c == 'C' ? 'G' : c == 'G' ? 'C' : 'N';
+}
+
 // One line at o (shared-memory stage or the output itself) by the warp.
-// widen: the name holds bytes >= 0x80, each written as U+FFFD.
-__device__ void build_line(uint8_t* o, const SamDev& d, const Hit& h, uint64_t r, bool widen, int lane) {
-    const uint8_t* nm = d.arena + d.name_off[r];
-    const uint32_t n_nm = d.name_len[r];
-    uint64_t w = 0;
-    if (!widen) {
-        for_span_bytes(nm, n_nm, lane, [&](uint32_t j, uint8_t c) { o[j] = c; });
-        w = n_nm;
-    } else {
+// The name, SEQ and QUAL words are loaded before the integer fields are
+// formatted, so the loads overlap that work.
+__device__ void build_line(uint8_t* o, const SamDev& d, const LineRec& h, const uint8_t* nm, uint32_t n_nm,
+                           const uint8_t* sq, uint32_t n_sq, const uint8_t* ql, uint32_t n_ql, int lane) {
+    const bool pre = !h.widen && span_fits(nm, n_nm) && span_fits(sq, n_sq) && span_fits(ql, n_ql);
+    SpanWords wn, ws, wq;
+    if (pre) {
+        span_load(wn, nm, n_nm, lane);
+        span_load(ws, sq, n_sq, lane);
+        span_load(wq, ql, n_ql, lane);
+    }
+    uint64_t w = n_nm;
+    if (h.widen) {  // each byte >= 0x80 of the name becomes U+FFFD
+        w = 0;
         for (uint32_t b = 0; b < n_nm; b += 32) {
             const uint32_t i = b + lane;
             const uint8_t c = i < n_nm ? nm[i] : 0;
@@ -357,62 +441,81 @@ __device__ void build_line(uint8_t* o, const SamDev& d, const Hit& h, uint64_t r
             w += __shfl_sync(FULL, incl, 31);
         }
     }
-    // FLAG, RNAME, POS, MAPQ, CIGAR, RNEXT, PNEXT, TLEN
-    const uint64_t w_contig = w + 2 + sdig(h.flag);
-    const uint64_t w_rnext = w_contig + h.contig_len + 4 + sdig(h.pos1) + sdig(h.mapq) + cigar_len(h);
-    const uint64_t w_seq = w_rnext + h.rnext_len + 3 + sdig(h.pnext) + sdig(h.tlen);
+    // FLAG, RNAME, POS, MAPQ, CIGAR, RNEXT, PNEXT, TLEN: every lane knows the
+    // layout
+    const uint32_t d_flag = sdig(h.flag), d_pos = sdig(h.pos1), d_mapq = ndig(h.mapq);
+    const uint32_t d_sl = h.sl > 0 ? ndig(h.sl) + 1 : 0, d_m = h.mapped ? ndig(h.m) : 0;
+    const uint32_t d_sr = h.sr > 0 ? ndig(h.sr) + 1 : 0, d_pn = sdig(h.pnext), d_tl = sdig(h.tlen);
+    const uint32_t cig = h.mapped ? d_sl + d_m + 1 + d_sr : 1;
+    const uint64_t w_contig = w + 2 + d_flag;
+    const uint64_t p_tab3 = w_contig + h.contig_len, p_pos = p_tab3 + 1, p_mapq = p_pos + d_pos + 1;
+    const uint64_t p_cig = p_mapq + d_mapq + 1;
+    const uint64_t w_rnext = p_cig + cig + 1;
+    const uint64_t p_tab7 = w_rnext + h.rnext_len, p_pnext = p_tab7 + 1, p_tlen = p_pnext + d_pn + 1;
+    const uint64_t w_seq = p_tlen + d_tl + 1;
+    // each of lanes 0-7 picks one number, lanes 3-5 and 8-16 one separator;
+    // the picks are selects, the writes one code path for all lanes
+    int64_t v = 0;
+    uint64_t vp = 0, cp = 0;
+    uint32_t vn = 0;
+    uint8_t ch = '\t';
+    bool vb = lane < 8, cb = lane >= 8 && lane <= 16;
     if (lane == 0) {
-        uint64_t k = w;
-        o[k++] = '\t';
-        k += put_int(o + k, h.flag);
-        o[k] = '\t';
-        k = w_contig + h.contig_len;
-        o[k++] = '\t';
-        k += put_int(o + k, h.pos1);
-        o[k++] = '\t';
-        k += put_int(o + k, h.mapq);
-        o[k++] = '\t';
-        if (!h.mapped) {
-            o[k++] = '*';
-        } else {
-            if (h.sl > 0) {
-                k += put_int(o + k, h.sl);
-                o[k++] = 'S';
-            }
-            k += put_int(o + k, h.m);
-            o[k++] = 'M';
-            if (h.sr > 0) {
-                k += put_int(o + k, h.sr);
-                o[k++] = 'S';
-            }
-        }
-        o[k] = '\t';
-        k = w_rnext + h.rnext_len;
-        o[k++] = '\t';
-        k += put_int(o + k, h.pnext);
-        o[k++] = '\t';
-        k += put_int(o + k, h.tlen);
-        o[k] = '\t';
+        v = h.flag, vp = w + 1, vn = d_flag;
+    } else if (lane == 1) {
+        v = h.pos1, vp = p_pos, vn = d_pos;
+    } else if (lane == 2) {
+        v = h.mapq, vp = p_mapq, vn = d_mapq;
+    } else if (lane == 3) {
+        vb = cb = h.mapped && h.sl > 0;
+        v = h.sl, vp = p_cig, vn = d_sl - 1, cp = p_cig + d_sl - 1, ch = 'S';
+    } else if (lane == 4) {
+        vb = h.mapped;
+        cb = true;
+        v = h.m, vp = p_cig + d_sl, vn = d_m;
+        cp = h.mapped ? p_cig + d_sl + d_m : p_cig;
+        ch = h.mapped ? 'M' : '*';
+    } else if (lane == 5) {
+        vb = cb = h.mapped && h.sr > 0;
+        v = h.sr, vp = p_cig + d_sl + d_m + 1, vn = d_sr - 1, cp = p_cig + d_sl + d_m + d_sr, ch = 'S';
+    } else if (lane == 6) {
+        v = h.pnext, vp = p_pnext, vn = d_pn;
+    } else if (lane == 7) {
+        v = h.tlen, vp = p_tlen, vn = d_tl;
+    } else {  // the nine tabs
+        cp = lane == 8    ? w
+             : lane == 9  ? w_contig - 1
+             : lane == 10 ? p_tab3
+             : lane == 11 ? p_mapq - 1
+             : lane == 12 ? p_cig - 1
+             : lane == 13 ? w_rnext - 1
+             : lane == 14 ? p_tab7
+             : lane == 15 ? p_tlen - 1
+                          : w_seq - 1;
     }
+    if (vb) put_int(o + vp, v, vn);
+    if (cb) o[cp] = ch;
     put_field(o + w_contig, d, h.contig_kind, h.contig_off, h.contig_len, lane);
     put_field(o + w_rnext, d, h.rnext_kind, h.rnext_off, h.rnext_len, lane);
-    // SEQ (reverse complement on flag 16: A<->T, C<->G, anything else N)
-    const uint8_t* sq = d.arena + d.seq_off[r];
-    const uint32_t n_sq = d.seq_len[r];
     uint8_t* os = o + w_seq;
-    if (h.mapped && (h.flag & 16)) {
-        for_span_bytes(sq, n_sq, lane, [&](uint32_t j, uint8_t c) {
-            os[n_sq - 1 - j] = c == 'A' ? 'T' : c == 'T' ? 'A' : c == 'C' ? 'G' : c == 'G' ? 'C' : 'N';
-        });
-    } else {
-        for_span_bytes(sq, n_sq, lane, [&](uint32_t j, uint8_t c) { os[j] = c; });
-    }
-    // QUAL, then "\tRG:Z:" + id + "\n"
-    const uint8_t* ql = d.arena + d.qual_off[r];
-    const uint32_t n_ql = d.qual_len[r];
     uint8_t* oq = os + n_sq + 1;
+    const bool rc = h.mapped && (h.flag & 16);
+    auto seq_f = [&](uint32_t j, uint8_t c) { os[j] = c; };
+    auto seq_r = [&](uint32_t j, uint8_t c) { os[n_sq - 1 - j] = complement(c); };
+    auto qual_f = [&](uint32_t j, uint8_t c) { oq[j] = c; };
+    if (pre) {
+        span_scatter(wn, n_nm, lane, [&](uint32_t j, uint8_t c) { o[j] = c; });
+        if (rc) span_scatter(ws, n_sq, lane, seq_r);
+        else span_scatter(ws, n_sq, lane, seq_f);
+        span_scatter(wq, n_ql, lane, qual_f);
+    } else {
+        if (!h.widen) for_span_bytes(nm, n_nm, lane, [&](uint32_t j, uint8_t c) { o[j] = c; });
+        if (rc) for_span_bytes(sq, n_sq, lane, seq_r);
+        else for_span_bytes(sq, n_sq, lane, seq_f);
+        for_span_bytes(ql, n_ql, lane, qual_f);
+    }
+    // SEQ <tab> QUAL, then "\tRG:Z:" + id + "\n"
     if (lane == 0) os[n_sq] = '\t';
-    for_span_bytes(ql, n_ql, lane, [&](uint32_t j, uint8_t c) { oq[j] = c; });
     uint8_t* ot = oq + n_ql;
     const uint32_t n_tail = 7 + d.rg_n;
     for (uint32_t j = lane; j < n_tail; j += 32) {
@@ -424,7 +527,11 @@ __device__ void build_line(uint8_t* o, const SamDev& d, const Hit& h, uint64_t r
     }
 }
 
-__global__ void __launch_bounds__(THREADS) sam_write_kernel(SamDev d, uint64_t n_lines, const uint64_t* ends) {
+// One warp per line: the line in the warp's shared-memory stage at its
+// destination's 16-byte phase, then 16-byte stores (byte stores at the
+// ragged ends); lines longer than the stage are built in place.
+__global__ void __launch_bounds__(THREADS) sam_write_kernel(SamDev d, uint64_t n_lines, const uint64_t* ends,
+                                                            const LineRec* recs) {
     __shared__ __align__(16) uint8_t stage[WARPS][STAGE];
     const uint64_t total = ends[n_lines - 1];
     const bool over = total > d.cap;
@@ -440,25 +547,22 @@ __global__ void __launch_bounds__(THREADS) sam_write_kernel(SamDev d, uint64_t n
     const uint64_t w0 = (static_cast<uint64_t>(blockIdx.x) * THREADS + threadIdx.x) >> 5;
     const uint64_t nw = static_cast<uint64_t>(gridDim.x) * WARPS;
     for (uint64_t L = w0; L < n_lines; L += nw) {
-        uint64_t r;
-        unsigned err = 0;
-        const Hit h = line_hit(d, L, r, err);
+        const LineRec h = recs[L];
+        const uint64_t r = d.paired ? (L >> 1) + (L & 1) * d.n1 : L;
         const uint64_t start = L ? ends[L - 1] : 0, len = ends[L] - start;
-        // the name's width follows from the line's length: wider than the
-        // name when it holds bytes >= 0x80
-        const uint64_t rest = head_len(h, 0) + d.seq_len[r] + 1 + d.qual_len[r] + 7 + d.rg_n;
-        const bool widen = len - rest != d.name_len[r];
+        const uint8_t* nm = d.arena + d.name_off[r];
+        const uint8_t* sq = d.arena + d.seq_off[r];
+        const uint8_t* ql = d.arena + d.qual_off[r];
+        const uint32_t n_nm = d.name_len[r], n_sq = d.seq_len[r], n_ql = d.qual_len[r];
         const uintptr_t gs = reinterpret_cast<uintptr_t>(d.sam) + start, ge = gs + len;
         const uint32_t ph = static_cast<uint32_t>(gs & 15);
-        if (widen || ph + len > STAGE) {  // long lines and widened names: straight to the output
-            build_line(d.sam + start, d, h, r, widen, lane);
+        if (ph + len > STAGE) {
+            build_line(d.sam + start, d, h, nm, n_nm, sq, n_sq, ql, n_ql, lane);
             continue;
         }
-        build_line(sb + ph, d, h, r, false, lane);
+        build_line(sb + ph, d, h, nm, n_nm, sq, n_sq, ql, n_ql, lane);
         __syncwarp();
-        // the stage out in 16-byte stores (sb[0] is the aligned address
-        // gs - ph), byte stores at the ragged ends
-        const uintptr_t a0 = gs - ph;
+        const uintptr_t a0 = gs - ph;  // sb[0] stands for this aligned address
         for (uintptr_t c = a0 + 16 * lane; c < ge; c += 512) {
             const uint32_t so = static_cast<uint32_t>(c - a0);
             if (c >= gs && c + 16 <= ge) {
@@ -480,7 +584,7 @@ size_t sam_scratch_bytes(uint64_t n_lines) {
     size_t t = 0;
     cub::DeviceScan::InclusiveSum(nullptr, t, static_cast<const uint32_t*>(nullptr), static_cast<uint64_t*>(nullptr),
                                   static_cast<int64_t>(n_lines ? n_lines : 1));
-    return align256(n_lines * 4) + align256(n_lines * 8) + align256(t);
+    return align256(n_lines * 4) + align256(n_lines * 8) + align256(n_lines * sizeof(LineRec)) + align256(t);
 }
 
 int enqueue_sam(const SamDev& d, void* scratch, size_t scratch_bytes, int sm_count, cudaStream_t st) {
@@ -488,18 +592,23 @@ int enqueue_sam(const SamDev& d, void* scratch, size_t scratch_bytes, int sm_cou
     if (!n_lines) return 0;
     uint8_t* s = static_cast<uint8_t*>(scratch);
     uint32_t* line_len = reinterpret_cast<uint32_t*>(s);
-    uint64_t* ends = reinterpret_cast<uint64_t*>(s + align256(n_lines * 4));
-    void* temp = s + align256(n_lines * 4) + align256(n_lines * 8);
-    size_t tb = scratch_bytes - align256(n_lines * 4) - align256(n_lines * 8);
-    const uint64_t want = (n_lines + WARPS - 1) / WARPS;
-    const uint64_t cap_blocks = static_cast<uint64_t>(sm_count > 0 ? sm_count : 148) * 16;
-    const unsigned g = static_cast<unsigned>(want < cap_blocks ? want : cap_blocks);
-    sam_layout_kernel<<<g, THREADS, 0, st>>>(d, n_lines, line_len);
+    s += align256(n_lines * 4);
+    uint64_t* ends = reinterpret_cast<uint64_t*>(s);
+    s += align256(n_lines * 8);
+    LineRec* recs = reinterpret_cast<LineRec*>(s);
+    s += align256(n_lines * sizeof(LineRec));
+    void* temp = s;
+    size_t tb = scratch_bytes - static_cast<size_t>(s - static_cast<uint8_t*>(scratch));
+    const uint64_t sms = static_cast<uint64_t>(sm_count > 0 ? sm_count : 148);
+    const uint64_t n_units = d.n1;  // pairs, or reads single-end
+    const uint64_t g1w = (n_units + THREADS - 1) / THREADS, g1c = sms * 8;
+    sam_layout_kernel<<<static_cast<unsigned>(g1w < g1c ? g1w : g1c), THREADS, 0, st>>>(d, n_units, line_len, recs);
     check_launch(cudaGetLastError(), "sam_layout_kernel");
     check_launch(cub::DeviceScan::InclusiveSum(temp, tb, static_cast<const uint32_t*>(line_len), ends,
                                                static_cast<int64_t>(n_lines), st),
                  "sam scan");
-    sam_write_kernel<<<g, THREADS, 0, st>>>(d, n_lines, ends);
+    const uint64_t g2w = (n_lines + WARPS - 1) / WARPS, g2c = sms * 16;
+    sam_write_kernel<<<static_cast<unsigned>(g2w < g2c ? g2w : g2c), THREADS, 0, st>>>(d, n_lines, ends, recs);
     check_launch(cudaGetLastError(), "sam_write_kernel");
     return 4;
 }
