@@ -29,7 +29,6 @@ from __future__ import annotations
 
 import contextlib
 import ctypes as C
-import gzip
 import os
 import struct
 from concurrent.futures import ThreadPoolExecutor
@@ -37,6 +36,7 @@ from concurrent.futures import ThreadPoolExecutor
 import numpy as np
 
 from . import pinned
+from .fqio import open_fastq
 from ._lib import check, lib, ma_bam_meta, ma_bam_tile, ma_fastq_arena, ma_fastq_records, ma_hits
 from .bam import META_FIELDS, canonical_rid_to_tid
 from .linear_fm import canonical_contig, fm_prefix_from_ref, select_device
@@ -82,12 +82,12 @@ def bam_header(contigs, env=None) -> bytes:
 
 class _Feed:
     """Uncompressed bytes of one FASTQ file in a pinned host buffer (gzip by
-    suffix, like _looks_gz, linear_fastq.mojo:49-51): fill() tops the buffer
-    up to its capacity, consume(n) drops the first n bytes."""
+    suffix, like _looks_gz, linear_fastq.mojo:49-51; BGZF files inflated on
+    a thread pool): fill() tops the buffer up to its capacity, consume(n)
+    drops the first n bytes."""
 
     def __init__(self, path: str, chunk: int, torch):
-        low = path.lower()
-        self.fh = gzip.open(path, "rb") if (low.endswith(".gz") or low.endswith(".gzip")) else open(path, "rb")
+        self.fh = open_fastq(path)
         self._buf = pinned.take(chunk)
         self.pin = self._buf[:chunk].numpy()
         self.len = 0

@@ -1,0 +1,185 @@
+"""Opening FASTQ files for the device pipelines.
+
+The reference reads `.gz` / `.gzip` files through `pigz -dc` (or Python's
+gzip module when pigz is absent: fq2bam-meth/python/fastq_batch.py:31-46,
+linear_fastq.mojo _looks_gz L49-51) and anything else as plain bytes.  The
+same bytes come out of open_fastq().  A gzip file made of BGZF members (the
+blocked gzip of bgzip / htslib: every member carries a "BC" extra field
+with its size) is inflated on a thread pool, many members at once; any other
+gzip file is read by the gzip module, one member after another.
+"""
+from __future__ import annotations
+
+import gzip
+import os
+import struct
+import zlib
+from collections import deque
+from concurrent.futures import ThreadPoolExecutor
+
+_MAGIC = b"\x1f\x8b\x08"
+JOB_BYTES = 1 << 20  # compressed bytes per inflate job
+
+
+def _bgzf_size(head: bytes) -> int:
+    """Total size of the BGZF member whose first bytes are `head` (at least
+    18 bytes), or 0 when it is not a BGZF member."""
+    if len(head) < 18 or head[:3] != _MAGIC or not (head[3] & 4):
+        return 0
+    xlen = struct.unpack_from("<H", head, 10)[0]
+    if len(head) < 12 + xlen:
+        return 0
+    i = 12
+    while i + 4 <= 12 + xlen:
+        slen = struct.unpack_from("<H", head, i + 2)[0]
+        if head[i:i + 2] == b"BC" and slen == 2:
+            return struct.unpack_from("<H", head, i + 4)[0] + 1
+        i += 4 + slen
+    return 0
+
+
+def _inflate_members(blob: bytes, sizes: list) -> bytes:
+    """The members of `blob` (consecutive BGZF members of the given sizes)
+    inflated and checked (CRC-32, ISIZE), concatenated."""
+    out = []
+    pos = 0
+    for n in sizes:
+        m = memoryview(blob)[pos:pos + n]
+        xlen = struct.unpack_from("<H", m, 10)[0]
+        crc, isize = struct.unpack_from("<II", m, n - 8)
+        # one inflate call into a buffer of the stored size (the GIL is
+        # released for the whole member)
+        data = zlib.decompress(m[12 + xlen:n - 8], -15, max(isize, 1))
+        if len(data) != isize or zlib.crc32(data) != crc:
+            raise gzip.BadGzipFile("BGZF member fails its CRC-32 / size check")
+        out.append(data)
+        pos += n
+    return b"".join(out)
+
+
+class BgzfReader:
+    """A binary file object over a BGZF file: its members are inflated by a
+    thread pool in batches of about `batch_bytes` compressed bytes, in order.
+    A member that is not BGZF (a plain gzip member appended to the file)
+    switches the rest of the file to the gzip module."""
+
+    def __init__(self, path: str, threads: int | None = None, batch_bytes: int = 16 << 20):
+        self._fh = open(path, "rb")
+        self._threads = max(1, threads or (os.cpu_count() or 1))
+        self._pool = ThreadPoolExecutor(max_workers=self._threads)
+        self._batch = batch_bytes
+        self._jobs: deque = deque()
+        self._raw = b""  # compressed bytes read but not yet split into members
+        self._done = False  # no more compressed bytes to schedule
+        self._tail = None  # gzip.GzipFile over a non-BGZF remainder
+        self._cur = memoryview(b"")
+
+    def _read_batch(self) -> None:
+        """Reads about batch_bytes of whole members and schedules them."""
+        if len(self._raw) < self._batch:
+            self._raw += self._fh.read(self._batch - len(self._raw))
+        sizes, pos = [], 0
+        while True:
+            n = _bgzf_size(self._raw[pos:pos + 18 + 256])
+            if n == 0 or pos + n > len(self._raw):
+                break
+            sizes.append(n)
+            pos += n
+        if sizes:
+            blob, self._raw = self._raw[:pos], self._raw[pos:]
+            # jobs of about JOB_BYTES compressed bytes, so that all threads work
+            first_byte = first_member = off = 0
+            for i, n in enumerate(sizes):
+                off += n
+                if off - first_byte >= JOB_BYTES or i == len(sizes) - 1:
+                    self._jobs.append(self._pool.submit(_inflate_members, blob[first_byte:off],
+                                                        sizes[first_member:i + 1]))
+                    first_byte, first_member = off, i + 1
+            return
+        # no whole BGZF member at the front
+        more = self._fh.read(1)
+        if more:  # a member that is not BGZF: read on to the end of the file
+            self._raw += more
+            self._batch *= 2
+            return
+        self._done = True
+        rest = self._raw.lstrip(b"\0")  # gzip allows zero padding after a member
+        self._raw = b""
+        if not rest:
+            return
+        if rest[:2] != _MAGIC[:2]:
+            raise gzip.BadGzipFile("Not a gzipped file (%r)" % rest[:2])
+        if _bgzf_size(rest[:18 + 256]) and len(rest) < _bgzf_size(rest[:18 + 256]):
+            raise EOFError("Compressed file ended before the end-of-stream marker was reached")
+        import io
+
+        # a plain gzip member (or zero padding between members) from here on
+        self._tail = gzip.GzipFile(fileobj=io.BytesIO(rest))
+
+    def _fill_jobs(self) -> None:
+        while not self._done and len(self._jobs) < 4 * self._threads:
+            self._read_batch()
+
+    def readinto(self, b) -> int:
+        mv = memoryview(b).cast("B")
+        got = 0
+        while got < len(mv):
+            if len(self._cur):
+                k = min(len(self._cur), len(mv) - got)
+                mv[got:got + k] = self._cur[:k]
+                self._cur = self._cur[k:]
+                got += k
+                continue
+            self._fill_jobs()
+            if self._jobs:
+                self._cur = memoryview(self._jobs.popleft().result())
+                continue
+            if self._tail is not None:
+                k = self._tail.readinto(mv[got:])
+                if k:
+                    got += k
+                    continue
+            break
+        return got
+
+    def read(self, n: int = -1) -> bytes:
+        if n is None or n < 0:
+            parts = []
+            while True:
+                chunk = bytearray(1 << 20)
+                k = self.readinto(chunk)
+                if not k:
+                    return b"".join(parts)
+                parts.append(bytes(chunk[:k]))
+        buf = bytearray(n)
+        return bytes(buf[:self.readinto(buf)])
+
+    def close(self) -> None:
+        for j in self._jobs:
+            j.cancel()
+        self._pool.shutdown(wait=True)
+        self._fh.close()
+        if self._tail is not None:
+            self._tail.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def is_bgzf(path: str) -> bool:
+    with open(path, "rb") as fh:
+        return _bgzf_size(fh.read(18 + 256)) > 0
+
+
+def open_fastq(path: str, threads: int | None = None):
+    """A binary file object with the uncompressed FASTQ bytes of `path`
+    (gzip by the .gz / .gzip suffix, like the reference)."""
+    low = str(path).lower()
+    if low.endswith(".gz") or low.endswith(".gzip"):
+        if is_bgzf(path):
+            return BgzfReader(str(path), threads)
+        return gzip.open(path, "rb")
+    return open(path, "rb")
