@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(THREADS) sam_layout_kernel(SamDev d, uint64_t 
 }
 
 // The aligned 4-byte words covering a span, up to 32 * SPAN_UNROLL of them
-// loaded at once (one round of loads for spans up to ~0.5 KB).
+// (256 bytes) loaded at once: one round of loads for a span that fits.
 struct SpanWords {
     uint32_t v[SPAN_UNROLL];
     uint32_t lead, nw;
@@ -360,8 +360,8 @@ __device__ __forceinline__ void span_scatter(const SpanWords& s, uint32_t n, int
     }
 }
 
-// Calls f(j, byte) for every byte j of src[0, n), any length, 512 bytes per
-// round.
+// Calls f(j, byte) for every byte j of src[0, n), any length, 32 *
+// SPAN_UNROLL words per round.
 template <typename F>
 __device__ __forceinline__ void for_span_bytes(const uint8_t* src, uint32_t n, int lane, F&& f) {
     for (uint32_t b = 0; b < n;) {
