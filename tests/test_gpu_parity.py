@@ -246,3 +246,31 @@ def test_host_batch_pipeline_matches_device_batch(ctx, small_ref):
     torch.cuda.synchronize()
     for f in FIELDS:
         assert np.array_equal(out[f].cpu().numpy(), getattr(host, f).view(out[f].cpu().numpy().dtype)), f
+
+
+@pytest.fixture(scope="module")
+def config0_ref(tmp_path_factory):
+    """The reference's CPU-runnable case: synthetic 4 Mbp, GC 0.41, CpG ~1%, seed 0."""
+    from pathlib import Path
+
+    from mojoalign_b200 import build_index
+
+    d = tmp_path_factory.mktemp("config0")
+    fa = d / "ref.fa"
+    synth.write_reference(fa, 4_000_000, n_contigs=1, gc=0.41, cpg=0.01, seed=0)
+    prefix = Path(str(fa) + ".bwameth.c2t")
+    build_index(fa, prefix, bwameth_c2t=True, sa_intv=32, device=-1)
+    return fa, prefix
+
+
+def test_config0_in_full(ctx, config0_ref):
+    """100 k single-end 150 bp reads from both strands (conversion 0.99, CpG
+    retention 0.75, 0.5% substitutions, 5% random reads, seed 1), seeds of
+    19 bp with at most 500 occurrences: every output, the SA intervals and
+    scores included, equal to the oracle's, in the reference's launch shape
+    and in the wavefront form."""
+    fa, prefix = config0_ref
+    rb = sim(fa, 100_000, False)
+    g = compare(prefix, ctx, rb.bases, rb.lens, rb.n1, False, 150, BENCH_PARAMS, bs=(1, 0),
+                tunings=[TUNINGS[0], TUNINGS[5]])
+    assert 0.9 < (g.rid >= 0).mean() < 0.97  # the 5% random reads stay unmapped
