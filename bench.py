@@ -187,8 +187,9 @@ def sample_pairs(rb, n):
     return b, l
 
 
-def time_oracle(prefix, rb, params, target_s, probe_pairs=20000):
-    """Times the oracle on a bounded sample sized to about target_s seconds."""
+def time_oracle(prefix, rb, params, target_s, probe_pairs=20000, min_pairs=500_000):
+    """Times the oracle on a bounded sample sized to about target_s seconds,
+    at least min_pairs pairs (the parity sample: 1 M reads or more)."""
     import oracle
 
     ix = oracle.OracleIndex(prefix)
@@ -196,7 +197,7 @@ def time_oracle(prefix, rb, params, target_s, probe_pairs=20000):
     t = time.perf_counter()
     ix.map(b, l, probe_pairs, True, READ_LEN, 1, 2, params.as_list())
     rate = 2 * probe_pairs / (time.perf_counter() - t)
-    n = int(min(rb.n1, max(probe_pairs, rate * target_s / 2)))
+    n = int(min(rb.n1, max(probe_pairs, min_pairs, rate * target_s / 2)))
     b, l = sample_pairs(rb, n)
     t = time.perf_counter()
     out = ix.map(b, l, n, True, READ_LEN, 1, 2, params.as_list())
