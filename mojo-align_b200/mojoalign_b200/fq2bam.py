@@ -36,7 +36,7 @@ from concurrent.futures import ThreadPoolExecutor
 import numpy as np
 
 from . import pinned
-from .fqio import open_fastq
+from .fqio import ParallelWriter, open_fastq
 from ._lib import check, lib, ma_bam_meta, ma_bam_tile, ma_fastq_arena, ma_fastq_records, ma_hits
 from .bam import META_FIELDS, canonical_rid_to_tid
 from .linear_fm import canonical_contig, fm_prefix_from_ref, select_device
@@ -322,8 +322,8 @@ def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", 
         host_out = pinned.take(got.value)
         try:
             host_out[: got.value].copy_(d_out[: got.value])
-            with open(out_bam, "wb") as fh:
-                fh.write(memoryview(host_out.numpy())[: got.value])
+            with ParallelWriter(out_bam) as fw:
+                fw.write(memoryview(host_out.numpy())[: got.value])
         finally:
             pinned.give(host_out)
         tm["write"] = time.perf_counter() - t0

@@ -28,6 +28,7 @@ from concurrent.futures import ThreadPoolExecutor
 from . import pinned
 from ._lib import MA_FASTQ_RULES_PAIR_READER, check, lib, ma_fastq_arena, ma_fastq_records, ma_hits
 from .fq2bam import MAX_LEN_CAP, REC_KEYS, _Feed
+from .fqio import ParallelWriter
 from .linear_fm import _env_str, fm_prefix_from_ref, sam_header, select_device
 from .mapper import GpuContext, GpuIndex, MapResult, bs_mode
 from .params import FmParams
@@ -79,7 +80,7 @@ def map_fastq_to_sam(ref_fa, fq1, out_sam, device: str = "auto", fq2: str = "", 
     o3 = (C.c_uint64 * 3)()
     scope = contextlib.ExitStack()
     scope.enter_context(torch.cuda.stream(stream))
-    fh = open(out_sam, "wb")
+    fh = ParallelWriter(out_sam)
     try:
         fh.write(sam_header(index.contigs, env).encode())
         for f in feeds:

@@ -1,4 +1,4 @@
-"""Opening FASTQ files for the device pipelines.
+"""File input and output of the device pipelines.
 
 The reference reads `.gz` / `.gzip` files through `pigz -dc` (or Python's
 gzip module when pigz is absent: fq2bam-meth/python/fastq_batch.py:31-46,
@@ -183,3 +183,52 @@ def open_fastq(path: str, threads: int | None = None):
             return BgzfReader(str(path), threads)
         return gzip.open(path, "rb")
     return open(path, "rb")
+
+
+WRITE_THREADS = 4  # the page-cache copy of one writer thread tops out well below the disk's
+
+
+class ParallelWriter:
+    """Writes byte buffers at increasing offsets of one file, each buffer
+    split over a few threads (os.pwrite), so that the copy into the page
+    cache is not bound by one core.  Buffers are written in call order;
+    write() returns once the buffer is on its way to the file (the data may
+    be reused after it returns)."""
+
+    def __init__(self, path, threads: int = WRITE_THREADS, min_split: int = 8 << 20):
+        self.fd = os.open(str(path), os.O_WRONLY | os.O_CREAT | os.O_TRUNC, 0o644)
+        self.off = 0
+        self.threads = max(1, threads)
+        self.min_split = min_split
+        self._pool = ThreadPoolExecutor(max_workers=self.threads) if self.threads > 1 else None
+
+    def _put(self, mv, off: int) -> None:
+        done = 0
+        while done < len(mv):
+            done += os.pwrite(self.fd, mv[done:], off + done)
+
+    def write(self, data) -> int:
+        mv = memoryview(data).cast("B")
+        n = len(mv)
+        if self._pool is None or n < self.min_split:
+            self._put(mv, self.off)
+        else:
+            step = (n + self.threads - 1) // self.threads
+            futs = [self._pool.submit(self._put, mv[i:i + step], self.off + i) for i in range(0, n, step)]
+            for f in futs:
+                f.result()
+        self.off += n
+        return n
+
+    def close(self) -> None:
+        if self._pool is not None:
+            self._pool.shutdown(wait=True)
+        if self.fd >= 0:
+            os.close(self.fd)
+            self.fd = -1
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -98,3 +98,20 @@ def test_large_bgzf_file_many_batches(tmp_path):
     with BgzfReader(str(p), threads=4, batch_bytes=1 << 20) as f:
         got = _read_all(f, 3 << 20)
     assert zlib.crc32(got) == zlib.crc32(text) and got == text
+
+
+@pytest.mark.parametrize("threads,min_split", [(1, 1), (4, 1), (3, 1 << 20), (8, 7)])
+def test_parallel_writer(tmp_path, threads, min_split):
+    from mojoalign_b200.fqio import ParallelWriter
+
+    rng = np.random.default_rng(threads)
+    parts = [rng.integers(0, 256, size=n, dtype=np.uint8).tobytes() for n in (0, 1, 5, 4 << 20, 3, 1_000_001)]
+    p = tmp_path / "out.bin"
+    with ParallelWriter(p, threads=threads, min_split=min_split) as w:
+        for b in parts:
+            assert w.write(b) == len(b)
+            assert w.write(memoryview(np.frombuffer(b, np.uint8))) == len(b)
+    assert p.read_bytes() == b"".join(b + b for b in parts)
+    with ParallelWriter(p, threads=threads) as w:  # truncates
+        w.write(b"xy")
+    assert p.read_bytes() == b"xy"
