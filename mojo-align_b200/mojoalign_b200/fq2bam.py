@@ -37,7 +37,8 @@ import numpy as np
 
 from . import pinned
 from .fqio import ParallelWriter, open_fastq
-from ._lib import check, lib, ma_bam_meta, ma_bam_tile, ma_fastq_arena, ma_fastq_records, ma_hits
+from ._lib import (MA_FASTQ_RULES_STREAM, check, lib, ma_bam_meta, ma_bam_tile, ma_fastq_arena, ma_fastq_records,
+                   ma_hits)
 from .bam import META_FIELDS, canonical_rid_to_tid
 from .linear_fm import canonical_contig, fm_prefix_from_ref, select_device
 from .mapper import GpuContext, GpuIndex, MapResult, bs_mode
@@ -131,6 +132,132 @@ class _Grow:
         return new
 
 
+class MappedChunk:
+    """One chunk of the FASTQ files in HBM, split into records and mapped:
+    the bytes of both mates (the arena), the record columns (R1 records then
+    R2 records) and the mapping outputs."""
+
+    def __init__(self, d_buf, n_bytes, n1, n_seq, max_len, cols, out):
+        self.d_buf, self.n_bytes, self.n1, self.n_seq, self.max_len = d_buf, n_bytes, n1, n_seq, max_len
+        self.cols, self.out = cols, out
+        self.hits = ma_hits(*[out[f].data_ptr() for f in MapResult.FIELDS])
+        self.arena = ma_fastq_arena(d_buf.data_ptr(), n_bytes, cols["name_off"].data_ptr(),
+                                    cols["name_len"].data_ptr(), cols["seq_off"].data_ptr(),
+                                    cols["seq_len"].data_ptr(), cols["qual_off"].data_ptr(),
+                                    cols["qual_len"].data_ptr())
+
+
+def mapped_chunks(ctx, index, params, fq1, fq2, bs_r1, bs_r2, rules, batch_pairs, chunk_bytes, stream, tm,
+                  before_map=None):
+    """Yields MappedChunk for consecutive pieces of the FASTQ file(s): the
+    uncompressed bytes go to HBM once (the next piece is read on a host
+    thread meanwhile), records are split under `rules` (MA_FASTQ_RULES_*),
+    at most batch_pairs per piece, and mapped on `stream`.  Pairs follow the
+    reference's readers: R2 running out first is "paired FASTQ length
+    mismatch (R2 ended early)", extra R2 records are ignored.
+    before_map(n_seq), when given, runs before a piece is mapped (it may
+    raise).  tm["read_wait"] accumulates the seconds spent waiting for
+    bytes."""
+    import time
+
+    import torch
+
+    paired = len(str(fq2)) > 0
+    dev = torch.device("cuda", ctx.device)
+    sh = stream.cuda_stream
+    p = params.to_c()
+    feeds = [_Feed(str(fq1), chunk_bytes, torch)] + ([_Feed(str(fq2), chunk_bytes, torch)] if paired else [])
+    pool = ThreadPoolExecutor(max_workers=1)  # reads the next piece while the GPU maps this one
+    pending = None
+    o3 = (C.c_uint64 * 3)()
+    try:
+        for f in feeds:
+            f.fill()
+        while True:
+            t0 = time.perf_counter()
+            if pending is not None:
+                pending.result()
+                pending = None
+            tm["read_wait"] += time.perf_counter() - t0
+            if not feeds[0].len:
+                return
+            # both mates' bytes in one device buffer: the piece's arena
+            sizes = [f.len for f in feeds]
+            d_buf = torch.empty(sum(sizes) + 16, dtype=torch.uint8, device=dev)
+            off = 0
+            for f in feeds:
+                d_buf[off:off + f.len].copy_(torch.from_numpy(f.pin[: f.len]), non_blocking=True)
+                off += f.len
+            recs, rcs, counts = [], [], []
+            for m, f in enumerate(feeds):
+                base = sum(sizes[:m])
+                r = {k: torch.empty(batch_pairs, dtype=torch.int64 if k.endswith("off") else torch.int32,
+                                    device=dev) for k in REC_KEYS}
+                rc = ma_fastq_records(*[r[k].data_ptr() for k in REC_KEYS])
+                check(lib.ma_fastq_parse_rules_device(ctx.handle, d_buf.data_ptr() + base, sizes[m], int(f.eof),
+                                                      batch_pairs, base, rules, C.byref(rc), o3, sh), ctx.handle)
+                recs.append(r)
+                rcs.append(rc)
+                counts.append((int(o3[0]), int(o3[1]), int(o3[2])))
+            n1 = counts[0][0]
+            if paired and counts[1][0] < n1:
+                if feeds[1].eof:
+                    raise RuntimeError("paired FASTQ length mismatch (R2 ended early)")
+                n1 = counts[1][0]  # R2's piece ended first: take the pairs both hold
+            if n1 == 0:
+                if feeds[0].eof:
+                    return
+                raise RuntimeError("FASTQ record larger than the read chunk")
+            # bytes to drop from each feed: the span of its first n1 records;
+            # the host buffers are free once the copies above are done
+            used = []
+            for m, f in enumerate(feeds):
+                u = counts[m][1]
+                if counts[m][0] != n1:
+                    check(lib.ma_fastq_parse_rules_device(ctx.handle, d_buf.data_ptr() + sum(sizes[:m]), sizes[m],
+                                                          int(f.eof), n1, sum(sizes[:m]), rules, C.byref(rcs[m]),
+                                                          o3, sh), ctx.handle)
+                    u = int(o3[1])
+                used.append(u)
+            stream.synchronize()
+
+            def refill(used=used):
+                for f, u in zip(feeds, used):
+                    f.consume(u)
+                    f.fill()
+
+            pending = pool.submit(refill)
+            max_len = max(max(c[2] for c in counts), params.seed_len)
+            if max_len > MAX_LEN_CAP:
+                raise RuntimeError("read longer than FM base cap (1024)")
+            n_seq = n1 * (2 if paired else 1)
+            if before_map is not None:
+                before_map(n_seq)
+            # mapper rows, R1 rows then R2 rows
+            rows = torch.empty(n_seq * max_len, dtype=torch.uint8, device=dev)
+            lens = torch.empty(n_seq, dtype=torch.int32, device=dev)
+            for m, r in enumerate(recs):
+                check(lib.ma_fastq_rows_device(ctx.handle, d_buf.data_ptr(), r["seq_off"].data_ptr(),
+                                               r["seq_len"].data_ptr(), n1, max_len,
+                                               rows.data_ptr() + m * n1 * max_len, lens.data_ptr() + m * n1 * 4,
+                                               sh), ctx.handle)
+            out = {f: torch.empty(n_seq, dtype=torch.int32, device=dev) for f in MapResult.FIELDS}
+            chunk = MappedChunk(d_buf, int(sum(sizes)), n1, n_seq, max_len,
+                                {k: torch.cat([r[k][:n1] for r in recs]) for k in REC_KEYS}, out)
+            check(lib.ma_map_batch_device(ctx.handle, index.handle, rows.data_ptr(), lens.data_ptr(), n1,
+                                          int(paired), max_len, bs_mode(bs_r1), bs_mode(bs_r2), C.byref(p),
+                                          C.byref(chunk.hits), None, sh), ctx.handle)
+            del recs, rcs
+            yield chunk
+            del chunk, d_buf, rows, lens, out
+    finally:
+        if pending is not None:
+            pending.exception()
+        pool.shutdown(wait=True)
+        for f in feeds:
+            f.close()
+
+
 def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", bs_r1: str = "",
                      bs_r2: str = "", params: FmParams | None = None, environ=None, kmer_k: int = 12,
                      kmer3_k: int | None = None, ctx: GpuContext | None = None, index: GpuIndex | None = None,
@@ -167,109 +294,31 @@ def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", 
     tids = canonical_rid_to_tid([c.name for c in index.contigs])
     d_tids = torch.from_numpy(tids).to(dev)
     header = bam_header(index.contigs, env)
-    p = params.to_c()
-    feeds = [_Feed(str(fq1), chunk_bytes, torch)] + ([_Feed(str(fq2), chunk_bytes, torch)] if paired else [])
-    pool = ThreadPoolExecutor(max_workers=1)  # reads the next chunk while the GPU maps this one
-    pending = None
     meta = {k: _Grow(torch, torch.int64 if t == np.uint64 else torch.int32, dev) for k, t in META_FIELDS}
     chunks, chunk_len = [], []
     n_reads = n_mapped = 0
     status = torch.zeros(3, dtype=torch.int64, device=dev)
-    o3 = (C.c_uint64 * 3)()
     scope = contextlib.ExitStack()
     scope.enter_context(torch.cuda.stream(stream))  # torch work shares the pipeline's stream
+
+    def cap_check(n_seq):
+        if n_reads + n_seq > meta_cap:
+            raise RuntimeError("FM sort cap exceeded; set METHYLGRAPHER_FM_SORT_CAP")
+
+    pieces = mapped_chunks(ctx, index, params, fq1, fq2, bs_r1, bs_r2, MA_FASTQ_RULES_STREAM, batch_pairs,
+                           chunk_bytes, stream, tm, cap_check)
     try:
-        for f in feeds:
-            f.fill()
-        while True:
-            t0 = time.perf_counter()
-            if pending is not None:
-                pending.result()
-                pending = None
-            tm["read_wait"] += time.perf_counter() - t0
-            t0 = time.perf_counter()
-            if not feeds[0].len:
-                break
-            # both mates' bytes in one device buffer: the batch's arena
-            sizes = [f.len for f in feeds]
-            d_buf = torch.empty(sum(sizes) + 16, dtype=torch.uint8, device=dev)
-            off = 0
-            for f in feeds:
-                d_buf[off:off + f.len].copy_(torch.from_numpy(f.pin[: f.len]), non_blocking=True)
-                off += f.len
-            recs, rcs, counts = [], [], []
-            for m, f in enumerate(feeds):
-                base = sum(sizes[:m])
-                r = {k: torch.empty(batch_pairs, dtype=torch.int64 if k.endswith("off") else torch.int32,
-                                    device=dev) for k in REC_KEYS}
-                rc = ma_fastq_records(*[r[k].data_ptr() for k in REC_KEYS])
-                check(lib.ma_fastq_parse_device(ctx.handle, d_buf.data_ptr() + base, sizes[m], int(f.eof),
-                                                batch_pairs, base, C.byref(rc), o3, sh), ctx.handle)
-                recs.append(r)
-                rcs.append(rc)
-                counts.append((int(o3[0]), int(o3[1]), int(o3[2])))
-            n1 = counts[0][0]
-            if paired:
-                if counts[1][0] < n1:
-                    if feeds[1].eof:
-                        raise RuntimeError("paired FASTQ length mismatch (R2 ended early)")
-                    n1 = counts[1][0]  # R2's chunk ended first: take the pairs both hold
-            if n1 == 0:
-                if all(f.eof for f in feeds[:1]):
-                    break
-                raise RuntimeError("FASTQ record larger than the read chunk")
-            # bytes to drop from each feed: the span of its first n1 records;
-            # the host buffers are free once the copies above are done
-            used = []
-            for m, f in enumerate(feeds):
-                u = counts[m][1]
-                if counts[m][0] != n1:
-                    check(lib.ma_fastq_parse_device(ctx.handle, d_buf.data_ptr() + sum(sizes[:m]), sizes[m],
-                                                    int(f.eof), n1, sum(sizes[:m]), C.byref(rcs[m]), o3, sh),
-                          ctx.handle)
-                    u = int(o3[1])
-                used.append(u)
-            stream.synchronize()
-
-            def refill(used=used):
-                for f, u in zip(feeds, used):
-                    f.consume(u)
-                    f.fill()
-
-            pending = pool.submit(refill)
-            max_len = max(max(c[2] for c in counts), params.seed_len)
-            if max_len > MAX_LEN_CAP:
-                raise RuntimeError("read longer than FM base cap (1024)")
-            n_seq = n1 * (2 if paired else 1)
-            if n_reads + n_seq > meta_cap:
-                raise RuntimeError("FM sort cap exceeded; set METHYLGRAPHER_FM_SORT_CAP")
-            # mapper rows, R1 rows then R2 rows
-            rows = torch.empty(n_seq * max_len, dtype=torch.uint8, device=dev)
-            lens = torch.empty(n_seq, dtype=torch.int32, device=dev)
-            for m, r in enumerate(recs):
-                check(lib.ma_fastq_rows_device(ctx.handle, d_buf.data_ptr(), r["seq_off"].data_ptr(),
-                                               r["seq_len"].data_ptr(), n1, max_len,
-                                               rows.data_ptr() + m * n1 * max_len, lens.data_ptr() + m * n1 * 4,
-                                               sh), ctx.handle)
-            out = {f: torch.empty(n_seq, dtype=torch.int32, device=dev) for f in MapResult.FIELDS}
-            hits = ma_hits(*[out[f].data_ptr() for f in MapResult.FIELDS])
-            check(lib.ma_map_batch_device(ctx.handle, index.handle, rows.data_ptr(), lens.data_ptr(), n1,
-                                          int(paired), max_len, bs_mode(bs_r1), bs_mode(bs_r2), C.byref(p),
-                                          C.byref(hits), None, sh), ctx.handle)
-            # arena columns of the batch: R1 records then R2 records
-            cols = {k: torch.cat([r[k][:n1] for r in recs]) for k in REC_KEYS}
-            arena = ma_fastq_arena(d_buf.data_ptr(), int(sum(sizes)), cols["name_off"].data_ptr(),
-                                   cols["name_len"].data_ptr(), cols["seq_off"].data_ptr(),
-                                   cols["seq_len"].data_ptr(), cols["qual_off"].data_ptr(),
-                                   cols["qual_len"].data_ptr())
+        t_loop = time.perf_counter()
+        for ch in pieces:
+            n_seq = ch.n_seq
             dm = {k: meta[k].ensure(n_reads + n_seq) for k, _ in META_FIELDS}
             dmeta = ma_bam_meta(*[dm[k].data_ptr() for k, _ in META_FIELDS])
-            seq_total = int(cols["seq_len"].sum().item())
-            name_total = int(cols["name_len"].sum().item())
+            seq_total = int(ch.cols["seq_len"].sum().item())
+            name_total = int(ch.cols["name_len"].sum().item())
             cap = n_seq * (64 + len(rg)) + name_total + 2 * seq_total
             d_chunk = torch.empty(cap, dtype=torch.uint8, device=dev)
             tile = ma_bam_tile(n_reads, n_mapped, 0, meta_cap, len(chunks))
-            check(lib.ma_emit_bam_batch_device(ctx.handle, C.byref(hits), n1, int(paired), C.byref(arena),
+            check(lib.ma_emit_bam_batch_device(ctx.handle, C.byref(ch.hits), ch.n1, int(paired), C.byref(ch.arena),
                                                d_tids.data_ptr(), int(tids.size), d_rg.data_ptr(), len(rg),
                                                d_chunk.data_ptr(), cap, C.byref(dmeta), C.byref(tile),
                                                status.data_ptr(), sh), ctx.handle)
@@ -281,8 +330,8 @@ def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", 
             chunk_len.append(int(st[0]))
             n_reads += n_seq
             n_mapped += int(st[1])
-            del d_buf, rows, out, cols
-            tm["batches"] += time.perf_counter() - t0
+            del ch
+        tm["batches"] = time.perf_counter() - t_loop - tm["read_wait"]
         # ---- sort, mark, gather, compress ----
         t0 = time.perf_counter()
         total_records = int(sum(chunk_len))
@@ -331,13 +380,9 @@ def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", 
         if stats is not None:
             stats.update({k: round(v, 4) for k, v in tm.items()})
     finally:
-        if pending is not None:
-            pending.exception()
-        pool.shutdown(wait=True)
+        pieces.close()
         stream.synchronize()
         scope.close()
-        for f in feeds:
-            f.close()
         if own_index:
             index.close()
         if own_ctx:

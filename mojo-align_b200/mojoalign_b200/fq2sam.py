@@ -26,11 +26,11 @@ import os
 from concurrent.futures import ThreadPoolExecutor
 
 from . import pinned
-from ._lib import MA_FASTQ_RULES_PAIR_READER, check, lib, ma_fastq_arena, ma_fastq_records, ma_hits
-from .fq2bam import MAX_LEN_CAP, REC_KEYS, _Feed
+from ._lib import MA_FASTQ_RULES_PAIR_READER, check, lib
+from .fq2bam import mapped_chunks
 from .fqio import ParallelWriter
 from .linear_fm import _env_str, fm_prefix_from_ref, sam_header, select_device
-from .mapper import GpuContext, GpuIndex, MapResult, bs_mode
+from .mapper import GpuContext, GpuIndex
 from .params import FmParams
 from .sam import LINE_FIXED, SamContigs, sam_error
 
@@ -67,107 +67,32 @@ def map_fastq_to_sam(ref_fa, fq1, out_sam, device: str = "auto", fq2: str = "", 
     d_rg = torch.tensor(list(rg) or [0], dtype=torch.uint8, device=dev)
     contigs = SamContigs.from_names([c.name for c in index.contigs])
     d_contigs = contigs.to_device(torch, dev)
-    p = params.to_c()
-    feeds = [_Feed(str(fq1), chunk_bytes, torch)] + ([_Feed(str(fq2), chunk_bytes, torch)] if paired else [])
-    reader = ThreadPoolExecutor(max_workers=1)  # reads the next chunk while the GPU maps this one
     writer = ThreadPoolExecutor(max_workers=1)  # writes chunk k while chunk k+1 maps
-    pending = None
     host_out = [None, None]  # pinned text buffers, alternating between chunks
     writes = [None, None]
     n_mapped = 0
     k_chunk = 0
     status = torch.zeros(3, dtype=torch.int64, device=dev)
-    o3 = (C.c_uint64 * 3)()
     scope = contextlib.ExitStack()
     scope.enter_context(torch.cuda.stream(stream))
     fh = ParallelWriter(out_sam)
+    pieces = mapped_chunks(ctx, index, params, fq1, fq2, bs_r1, bs_r2, MA_FASTQ_RULES_PAIR_READER, batch_pairs,
+                           chunk_bytes, stream, tm)
     try:
         fh.write(sam_header(index.contigs, env).encode())
-        for f in feeds:
-            f.fill()
-        while True:
-            t0 = time.perf_counter()
-            if pending is not None:
-                pending.result()
-                pending = None
-            tm["read_wait"] += time.perf_counter() - t0
-            t0 = time.perf_counter()
-            if not feeds[0].len:
-                break
-            sizes = [f.len for f in feeds]
-            d_buf = torch.empty(sum(sizes) + 16, dtype=torch.uint8, device=dev)
-            off = 0
-            for f in feeds:
-                d_buf[off:off + f.len].copy_(torch.from_numpy(f.pin[: f.len]), non_blocking=True)
-                off += f.len
-            recs, rcs, counts = [], [], []
-            for m, f in enumerate(feeds):
-                base = sum(sizes[:m])
-                r = {k: torch.empty(batch_pairs, dtype=torch.int64 if k.endswith("off") else torch.int32,
-                                    device=dev) for k in REC_KEYS}
-                rc = ma_fastq_records(*[r[k].data_ptr() for k in REC_KEYS])
-                check(lib.ma_fastq_parse_rules_device(ctx.handle, d_buf.data_ptr() + base, sizes[m], int(f.eof),
-                                                      batch_pairs, base, MA_FASTQ_RULES_PAIR_READER, C.byref(rc), o3,
-                                                      sh), ctx.handle)
-                recs.append(r)
-                rcs.append(rc)
-                counts.append((int(o3[0]), int(o3[1]), int(o3[2])))
-            n1 = counts[0][0]
-            if paired and counts[1][0] < n1:
-                if feeds[1].eof:  # FastqPairReader.read_batch, fastq_batch.py:296-298
-                    raise RuntimeError("paired FASTQ length mismatch (R2 ended early)")
-                n1 = counts[1][0]  # R2's chunk ended first: take the pairs both hold
-            if n1 == 0:
-                if feeds[0].eof:
-                    break
-                raise RuntimeError("FASTQ record larger than the read chunk")
-            used = []
-            for m, f in enumerate(feeds):
-                u = counts[m][1]
-                if counts[m][0] != n1:
-                    check(lib.ma_fastq_parse_rules_device(ctx.handle, d_buf.data_ptr() + sum(sizes[:m]), sizes[m],
-                                                          int(f.eof), n1, sum(sizes[:m]), MA_FASTQ_RULES_PAIR_READER,
-                                                          C.byref(rcs[m]), o3, sh), ctx.handle)
-                    u = int(o3[1])
-                used.append(u)
-            stream.synchronize()
-
-            def refill(used=used):
-                for f, u in zip(feeds, used):
-                    f.consume(u)
-                    f.fill()
-
-            pending = reader.submit(refill)
-            max_len = max(max(c[2] for c in counts), params.seed_len)
-            if max_len > MAX_LEN_CAP:
-                raise RuntimeError("read longer than FM base cap (1024)")
-            n_seq = n1 * (2 if paired else 1)
-            rows = torch.empty(n_seq * max_len, dtype=torch.uint8, device=dev)
-            lens = torch.empty(n_seq, dtype=torch.int32, device=dev)
-            for m, r in enumerate(recs):
-                check(lib.ma_fastq_rows_device(ctx.handle, d_buf.data_ptr(), r["seq_off"].data_ptr(),
-                                               r["seq_len"].data_ptr(), n1, max_len,
-                                               rows.data_ptr() + m * n1 * max_len, lens.data_ptr() + m * n1 * 4,
-                                               sh), ctx.handle)
-            out = {f: torch.empty(n_seq, dtype=torch.int32, device=dev) for f in MapResult.FIELDS}
-            hits = ma_hits(*[out[f].data_ptr() for f in MapResult.FIELDS])
-            check(lib.ma_map_batch_device(ctx.handle, index.handle, rows.data_ptr(), lens.data_ptr(), n1,
-                                          int(paired), max_len, bs_mode(bs_r1), bs_mode(bs_r2), C.byref(p),
-                                          C.byref(hits), None, sh), ctx.handle)
-            cols = {k: torch.cat([r[k][:n1] for r in recs]) for k in REC_KEYS}
-            arena = ma_fastq_arena(d_buf.data_ptr(), int(sum(sizes)), cols["name_off"].data_ptr(),
-                                   cols["name_len"].data_ptr(), cols["seq_off"].data_ptr(),
-                                   cols["seq_len"].data_ptr(), cols["qual_off"].data_ptr(),
-                                   cols["qual_len"].data_ptr())
+        t_loop = time.perf_counter()
+        for ch in pieces:
+            n_seq = ch.n_seq
+            cols = ch.cols
             # the text of the chunk fits in: per line the fixed fields and
             # contig names, three bytes per name byte, SEQ, QUAL
             cap = n_seq * (LINE_FIXED + len(rg) + 2 * contigs.max_name) + 3 * int(
-                cols["name_len"].sum().item()) + sum(sizes)
+                cols["name_len"].sum().item()) + ch.n_bytes
             d_text = torch.empty(cap, dtype=torch.uint8, device=dev)
             if stats is not None:
                 ev = [torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)]
                 ev[0].record(stream)
-            check(lib.ma_emit_sam_batch_device(ctx.handle, C.byref(hits), n1, int(paired), C.byref(arena),
+            check(lib.ma_emit_sam_batch_device(ctx.handle, C.byref(ch.hits), ch.n1, int(paired), C.byref(ch.arena),
                                                C.byref(d_contigs.c), d_rg.data_ptr(), len(rg), d_text.data_ptr(),
                                                cap, status.data_ptr(), sh), ctx.handle)
             if stats is not None:
@@ -196,8 +121,8 @@ def map_fastq_to_sam(ref_fa, fq1, out_sam, device: str = "auto", fq2: str = "", 
             stream.synchronize()
             writes[slot] = writer.submit(fh.write, memoryview(host_out[slot].numpy())[:n_text])
             k_chunk += 1
-            del d_buf, rows, out, cols, d_text
-            tm["batches"] += time.perf_counter() - t0
+            del ch, cols, d_text
+        tm["batches"] = time.perf_counter() - t_loop - tm["read_wait"] - tm["write_wait"]
         t1 = time.perf_counter()
         for w in writes:
             if w is not None:
@@ -207,17 +132,13 @@ def map_fastq_to_sam(ref_fa, fq1, out_sam, device: str = "auto", fq2: str = "", 
         if stats is not None:
             stats.update({k: round(v, 6) if isinstance(v, float) else v for k, v in tm.items()})
     finally:
-        if pending is not None:
-            pending.exception()
-        reader.shutdown(wait=True)
+        pieces.close()
         writer.shutdown(wait=True)
         fh.close()
         for t in host_out:
             pinned.give(t)
         stream.synchronize()
         scope.close()
-        for f in feeds:
-            f.close()
         if own_index:
             index.close()
         if own_ctx:
