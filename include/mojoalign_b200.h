@@ -702,6 +702,33 @@ int ma_bgzf_compress_device(ma_ctx* ctx, const uint8_t* d_in, uint64_t n, int le
 /* An output size large enough for n input bytes (EOF member included). */
 uint64_t ma_bgzf_bound(uint64_t n);
 
+/*
+ * Inflates the members of a BGZF file (compressed FASTQ as bgzip writes it)
+ * on the device, one member per warp: the deflate payload of member m is
+ * in[src_off[m], + src_len[m]) and its isize[m] bytes go to
+ * out[dst_off[m], ...); each member's size and CRC-32 (crc[m]) are checked.
+ * The member table comes from the gzip headers (BSIZE of the "BC" extra
+ * field), parsed on the host.  Replaces the decompression of the
+ * reference's FASTQ readers (`pigz -dc` / the gzip module,
+ * fq2bam-meth/python/fastq_batch.py:31-46, linear_fastq.mojo _looks_gz
+ * L49-51) for BGZF inputs.  status[m]: 0, 1..7 invalid deflate data (ends
+ * early, block type, stored lengths, code lengths, code, distance, more data
+ * than ISIZE), 8 size or 9 CRC-32 mismatch, 10 a span outside its buffer.
+ * Host buffers, synchronous; MA_ERR_FORMAT names the first failing member.
+ */
+int ma_bgzf_inflate(ma_ctx* ctx, const uint8_t* in, uint64_t in_bytes, const uint64_t* src_off,
+                    const uint32_t* src_len, const uint64_t* dst_off, const uint32_t* isize,
+                    const uint32_t* crc, uint32_t n_members, uint8_t* out, uint64_t out_bytes,
+                    uint32_t* status);
+
+/* Same on device buffers, asynchronous on `stream`; d_status receives the
+ * per-member codes. */
+int ma_bgzf_inflate_device(ma_ctx* ctx, const uint8_t* d_in, uint64_t in_bytes,
+                           const uint64_t* d_src_off, const uint32_t* d_src_len,
+                           const uint64_t* d_dst_off, const uint32_t* d_isize,
+                           const uint32_t* d_crc, uint32_t n_members, uint8_t* d_out,
+                           uint64_t out_bytes, uint32_t* d_status, void* stream);
+
 /* ---- measurement (no reference counterpart; the reference only prints
  * perf_counter stage timers, linear_gpu_fm.mojo:2270-2273,3317-3340) ---- */
 

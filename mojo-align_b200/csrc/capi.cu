@@ -10,6 +10,7 @@
 #include <string>
 
 #include "bam_pack.h"
+#include "bgzf_inflate.cuh"
 #include "bgzf.h"
 #include "fastq_parse.h"
 #include "sam_emit.h"
@@ -114,6 +115,8 @@ struct ma_ctx {
     DevBuf bgzf_in, bgzf_out, bgzf_scratch;
     // SAM text of a batch
     DevBuf sam_in, sam_arena, sam_out, sam_scratch, sam_status;
+    // BGZF inflate (host form)
+    DevBuf inf_in, inf_cols, inf_out;
 };
 
 struct ma_index {
@@ -1294,6 +1297,86 @@ int ma_emit_sam_batch_device(ma_ctx* ctx, const ma_hits* d_hits, uint32_t n1, in
         ctx->sam_scratch.ensure(scratch);
         SamDev v = sam_view(*d_hits, n1, paired, *d_arena, *d_contigs, d_rg, rg_n, d_sam, sam_cap, status);
         ctx->last_launches = enqueue_sam(v, ctx->sam_scratch.p, scratch, ctx->sm_count, st);
+    });
+}
+
+namespace {
+const char* inflate_error(uint32_t code) {
+    switch (code) {
+        case 1: return "deflate data end early";
+        case 2: return "invalid block type";
+        case 3: return "invalid stored block lengths";
+        case 4: return "invalid code lengths";
+        case 5: return "invalid code";
+        case 6: return "distance too far back";
+        case 7: return "more data than ISIZE";
+        case bgzf_inflate::S_SIZE: return "inflated size differs from ISIZE";
+        case bgzf_inflate::S_CRC: return "CRC-32 mismatch";
+        default: return "member span outside its buffer";
+    }
+}
+}  // namespace
+
+int ma_bgzf_inflate(ma_ctx* ctx, const uint8_t* in, uint64_t in_bytes, const uint64_t* src_off,
+                    const uint32_t* src_len, const uint64_t* dst_off, const uint32_t* isize, const uint32_t* crc,
+                    uint32_t n_members, uint8_t* out, uint64_t out_bytes, uint32_t* status) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->last_launches = 0;
+        if (n_members == 0) return;
+        if (!in || !src_off || !src_len || !dst_off || !isize || !crc || !status || (out_bytes && !out))
+            fail(MA_ERR_ARG, "null argument");
+        use_device(ctx);
+        cudaStream_t st = ctx->stream;
+        const uint64_t n = n_members, b8 = (n * 8 + 255) & ~uint64_t(255), b4 = (n * 4 + 255) & ~uint64_t(255);
+        ctx->inf_in.ensure(in_bytes ? in_bytes : 1);
+        ctx->inf_cols.ensure(2 * b8 + 4 * b4);
+        ctx->inf_out.ensure(out_bytes ? out_bytes : 1);
+        uint8_t* c = ctx->inf_cols.as<uint8_t>();
+        bgzf_inflate::Job j{};
+        j.in = ctx->inf_in.as<uint8_t>();
+        j.in_bytes = in_bytes;
+        j.src_off = reinterpret_cast<const uint64_t*>(c);
+        j.dst_off = reinterpret_cast<const uint64_t*>(c + b8);
+        j.src_len = reinterpret_cast<const uint32_t*>(c + 2 * b8);
+        j.isize = reinterpret_cast<const uint32_t*>(c + 2 * b8 + b4);
+        j.crc = reinterpret_cast<const uint32_t*>(c + 2 * b8 + 2 * b4);
+        j.status = reinterpret_cast<uint32_t*>(c + 2 * b8 + 3 * b4);
+        j.n = n_members;
+        j.out = ctx->inf_out.as<uint8_t>();
+        j.out_bytes = out_bytes;
+        if (in_bytes) ck(cudaMemcpyAsync(ctx->inf_in.p, in, in_bytes, cudaMemcpyHostToDevice, st), "H2D inflate");
+        ck(cudaMemcpyAsync(c, src_off, n * 8, cudaMemcpyHostToDevice, st), "H2D inflate");
+        ck(cudaMemcpyAsync(c + b8, dst_off, n * 8, cudaMemcpyHostToDevice, st), "H2D inflate");
+        ck(cudaMemcpyAsync(c + 2 * b8, src_len, n * 4, cudaMemcpyHostToDevice, st), "H2D inflate");
+        ck(cudaMemcpyAsync(c + 2 * b8 + b4, isize, n * 4, cudaMemcpyHostToDevice, st), "H2D inflate");
+        ck(cudaMemcpyAsync(c + 2 * b8 + 2 * b4, crc, n * 4, cudaMemcpyHostToDevice, st), "H2D inflate");
+        ctx->last_launches = bgzf_inflate_enqueue(j, ctx->sm_count, st);
+        ck(cudaMemcpyAsync(status, j.status, n * 4, cudaMemcpyDeviceToHost, st), "D2H inflate");
+        if (out_bytes) ck(cudaMemcpyAsync(out, j.out, out_bytes, cudaMemcpyDeviceToHost, st), "D2H inflate");
+        ck(cudaStreamSynchronize(st), "inflate");
+        for (uint64_t m = 0; m < n; ++m)
+            if (status[m])
+                fail(MA_ERR_FORMAT, "BGZF member " + std::to_string(m) + ": " + inflate_error(status[m]));
+    });
+}
+
+int ma_bgzf_inflate_device(ma_ctx* ctx, const uint8_t* d_in, uint64_t in_bytes, const uint64_t* d_src_off,
+                           const uint32_t* d_src_len, const uint64_t* d_dst_off, const uint32_t* d_isize,
+                           const uint32_t* d_crc, uint32_t n_members, uint8_t* d_out, uint64_t out_bytes,
+                           uint32_t* d_status, void* stream) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->last_launches = 0;
+        if (n_members == 0) return;
+        if (!d_in || !d_src_off || !d_src_len || !d_dst_off || !d_isize || !d_crc || !d_status ||
+            (out_bytes && !d_out))
+            fail(MA_ERR_ARG, "null argument");
+        use_device(ctx);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+        bgzf_inflate::Job j{d_in, in_bytes, d_src_off, d_src_len, d_dst_off, d_isize, d_crc, n_members, d_out,
+                            out_bytes, d_status};
+        ctx->last_launches = bgzf_inflate_enqueue(j, ctx->sm_count, st);
     });
 }
 

@@ -259,6 +259,11 @@ SIGNATURES = [
      [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64),
       C.c_void_p]),
     ("ma_bgzf_bound", C.c_uint64, [C.c_uint64]),
+    ("ma_bgzf_inflate", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_uint64] + [C.c_void_p] * 5 + [C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p]),
+    ("ma_bgzf_inflate_device", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_uint64] + [C.c_void_p] * 5 + [C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p,
+                                                                C.c_void_p]),
     ("ma_synth_reference", C.c_int, [C.c_char_p, C.c_uint64, C.c_int, C.c_double, C.c_double, C.c_uint64]),
     ("ma_synth_reads", C.c_int,
      [C.c_char_p, C.POINTER(ma_read_model), C.c_uint32, C.c_int, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p,

@@ -169,6 +169,52 @@ class BgzfReader:
         self.close()
 
 
+def bgzf_members(blob: bytes) -> dict:
+    """The member table of a BGZF file held in memory: per member the offset
+    and length of its deflate payload, the offset of its bytes in the
+    inflated stream, ISIZE and CRC-32 (numpy arrays), and the inflated size.
+    Raises gzip.BadGzipFile when a member is not BGZF or runs past the end."""
+    import numpy as np
+
+    so, sl, do, isz, crc = [], [], [], [], []
+    pos, out = 0, 0
+    while pos < len(blob):
+        n = _bgzf_size(blob[pos:pos + 18 + 256])
+        if n == 0 or pos + n > len(blob) or n < 26:
+            raise gzip.BadGzipFile(f"no whole BGZF member at byte {pos}")
+        xlen = struct.unpack_from("<H", blob, pos + 10)[0]
+        c, s_ = struct.unpack_from("<II", blob, pos + n - 8)
+        so.append(pos + 12 + xlen)
+        sl.append(n - 12 - xlen - 8)
+        do.append(out)
+        isz.append(s_)
+        crc.append(c)
+        out += s_
+        pos += n
+    return {"src_off": np.array(so, np.uint64), "src_len": np.array(sl, np.uint32), "dst_off": np.array(do, np.uint64),
+            "isize": np.array(isz, np.uint32), "crc": np.array(crc, np.uint32), "out_bytes": out}
+
+
+def bgzf_inflate(ctx, blob: bytes) -> bytes:
+    """A BGZF file inflated on the device (ma_bgzf_inflate): the same bytes as
+    the gzip module gives; MojoAlignError names the first bad member."""
+    import ctypes as C
+
+    import numpy as np
+
+    from ._lib import check, lib
+
+    t = bgzf_members(blob)
+    src = np.frombuffer(blob, np.uint8)
+    out = np.empty(max(t["out_bytes"], 1), np.uint8)
+    status = np.zeros(max(t["src_off"].size, 1), np.uint32)
+    p = lambda a: a.ctypes.data  # noqa: E731
+    check(lib.ma_bgzf_inflate(ctx.handle, p(src) if src.size else None, src.size, p(t["src_off"]), p(t["src_len"]),
+                              p(t["dst_off"]), p(t["isize"]), p(t["crc"]), int(t["src_off"].size), p(out),
+                              t["out_bytes"], p(status)), ctx.handle)
+    return out[:t["out_bytes"]].tobytes()
+
+
 def is_bgzf(path: str) -> bool:
     with open(path, "rb") as fh:
         return _bgzf_size(fh.read(18 + 256)) > 0

@@ -182,3 +182,44 @@ int main() {
     assert r.returncode == 0, r.stderr[-2000:]
     ok, bad = map(int, r.stdout.split())
     assert ok > 0 and bad > 0
+
+
+def members_on_host(lib, blob: bytes, table=None):
+    """harness_inflate_members: the kernel's per-member step over a BGZF file."""
+    from mojoalign_b200.fqio import bgzf_members
+
+    t = table or bgzf_members(blob)
+    lib.harness_inflate_members.argtypes = [C.c_char_p, C.c_uint64] + [C.c_void_p] * 5 + \
+        [C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p]
+    out = np.zeros(max(t["out_bytes"], 1), np.uint8)
+    status = np.zeros(max(t["src_off"].size, 1), np.uint32)
+    lib.harness_inflate_members(blob, len(blob), *[t[k].ctypes.data for k in ("src_off", "src_len", "dst_off",
+                                                                               "isize", "crc")],
+                                int(t["src_off"].size), out.ctypes.data, t["out_bytes"], status.ctypes.data)
+    return out[:t["out_bytes"]].tobytes(), status[:t["src_off"].size]
+
+
+def test_member_step_inflates_bgzf_files(lib):
+    import gzip
+
+    from mojoalign_b200.fqio import bgzf_members
+
+    text = random_fastq(12, 3000, crlf=0.2)
+    for level in (0, 1, 5, 9):
+        blob = bgzf_ref.compress(text, level)
+        got, status = members_on_host(lib, blob)
+        assert not status.any() and got == gzip.decompress(blob) == text
+    blob = bgzf_ref.compress(text, 1)
+    t = bgzf_members(blob)
+    assert t["out_bytes"] == len(text) and t["isize"][-1] == 0  # the EOF member
+    # a wrong CRC, a wrong ISIZE, a damaged payload, spans outside the buffers
+    bad = dict(t, crc=t["crc"].copy(), isize=t["isize"].copy(), src_off=t["src_off"].copy())
+    bad["crc"][1] ^= 1
+    bad["isize"][2] -= 1
+    bad["src_off"][3] = len(blob)
+    _, status = members_on_host(lib, blob, bad)
+    assert status[1] == 9 and status[2] == 7 and status[3] == 10 and not status[4:].any()
+    dmg = bytearray(blob)
+    dmg[int(t["src_off"][0]) + 5] ^= 0x55
+    _, status = members_on_host(lib, bytes(dmg), t)
+    assert status[0] != 0 and not status[1:].any()
