@@ -597,7 +597,6 @@ def run_fq2bam_stage(args, ctx, gi, rb, local, params):
     map_fastq_to_bam (every stage on the GPU, files read and written on the
     host), against the same path restated on the CPU from the oracle on a
     sample (its mapping step dominates)."""
-    import gzip
     import shutil
     import sys as _sys
 
