@@ -31,6 +31,24 @@ def test_every_declared_entry_point_is_exported():
     assert names <= bound, f"entry points without a ctypes signature: {sorted(names - bound)}"
 
 
+def declared_arity() -> dict[str, int]:
+    """Parameter count of every prototype in the header."""
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(ma_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
+        args = m.group(2).strip()
+        out[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_ctypes_signatures_match_the_header():
+    arity = declared_arity()
+    assert len(arity) >= 20
+    for name, _, args in _lib.SIGNATURES:
+        if name in arity:
+            assert len(args) == arity[name], f"{name}: {len(args)} ctypes arguments, header declares {arity[name]}"
+
+
 def test_params_default_are_the_reference_defaults():
     p = _lib.ma_params()
     _lib.lib.ma_params_default(p)
