@@ -115,3 +115,21 @@ def test_parallel_writer(tmp_path, threads, min_split):
     with ParallelWriter(p, threads=threads) as w:  # truncates
         w.write(b"xy")
     assert p.read_bytes() == b"xy"
+
+
+def test_bgzf_member_table(text):
+    from mojoalign_b200.fqio import bgzf_members
+
+    blob = bgzf_ref.compress(text, 1)
+    t = bgzf_members(blob)
+    ms = bgzf_ref.members(blob)
+    assert t["src_off"].size == len(ms) and t["out_bytes"] == len(text)
+    for i, m in enumerate(ms):
+        payload = blob[int(t["src_off"][i]):int(t["src_off"][i]) + int(t["src_len"][i])]
+        assert payload == m["payload"] and t["isize"][i] == m["isize"] and t["crc"][i] == m["crc"]
+    assert list(t["dst_off"]) == list(np.concatenate([[0], np.cumsum(t["isize"][:-1].astype(np.uint64))]))
+    with pytest.raises(gzip.BadGzipFile):
+        bgzf_members(blob[:-5])  # the EOF member cut short
+    with pytest.raises(gzip.BadGzipFile):
+        bgzf_members(gzip.compress(text))  # not BGZF
+    assert bgzf_members(b"")["out_bytes"] == 0
