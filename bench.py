@@ -38,8 +38,15 @@ import numpy as np  # noqa: E402
 
 METRIC = "reads/s seed+extend"
 # DRAM bytes / algorithmic bytes of the wavefront seed kernels, from one ncu
-# capture of the 50 Mbp / 2M-read case (profiles/seed_wavefront_50mbp_1Mpairs.md)
+# capture (dram__bytes_read.sum + dram__bytes_write.sum) of the 50 Mbp /
+# 2M-read case, scaled to a call by the ratio to the algorithmic bytes
 TRAFFIC_OVER_ALG = 1.73
+# The workload parameters: the reference defaults with seed_len 19 and
+# max_occ 500 (mojoalign_b200.params.BENCH_PARAMS holds the same values; the
+# reference arm takes them from here so that it loads nothing of the
+# package).
+BENCH_PARAM_VALUES = {"seed_len": 19, "seed_stride": 2, "max_occ": 500, "max_diff": 12, "max_soft": 20,
+                      "max_adj": 8, "rescue_win": 512}
 SEED_KERNELS = {
     0: "seed/extend: seed_stage1_kernel over every endpoint (one thread per read)",
     1: "seed/extend: seed_stage1_kernel + seed_stage2_kernel (thread per read, then warp per read)",
@@ -83,6 +90,9 @@ def parse_args():
                     "stage (0 = skip)")
     ap.add_argument("--fq2sam-pairs", type=int, default=2_000_000, help="read pairs of the FASTQ -> SAM stage "
                     "(0 = skip)")
+    ap.add_argument("--gather-sweep", action="store_true", help="print the measured random-gather roofline "
+                    "(32- and 64-byte lines, 16 MiB to 32 GiB buffers) as one JSON object and exit")
+    ap.add_argument("--prepare-sample", default="", help=argparse.SUPPRESS)
     ap.add_argument("--tuning", default="", help="fixed kernel choice 'seed_kernel,stage1_endpoints,"
                     "stage2_blocks_per_sm,reg_level,stage1_max_rows,stage2_first_wave[,wave_endpoints,"
                     "wave_loci_per_read,wave_max_rounds,wave_growth]' instead of the autotuner")
@@ -878,6 +888,47 @@ def run_sort_stage(args, ctx, rb, res, local, peaks):
     }
 
 
+def workload_config(args) -> dict:
+    """The `config` block: the workload only, the same in both arms."""
+    return {"workload": f"plain single-launch, {args.genome_mb} Mbp synthetic bisulfite reference "
+                        f"(bwa-meth c2t index), {args.pairs} PE 2x{READ_LEN} read pairs per GPU",
+            "form": "plain single-launch", "genome_bp": args.genome_mb * 1_000_000,
+            "reads_per_gpu": 2 * args.pairs, "read_len": READ_LEN, "paired": True,
+            "params": dict(BENCH_PARAM_VALUES),
+            "l2": "inputs larger than L2 (reads and index several GB)"}
+
+
+LINE_HEAD = ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+             "vs_baseline", "dtype", "data", "impl", "parity_failures", "parity_sample", "config", "e2e",
+             "gpu_launches", "cpu_baseline")
+
+
+def ordered_line(line: dict) -> dict:
+    """The JSON line with the contract keys and the parity record first, so
+    that a reader that keeps only the head of the line still sees them."""
+    out = {k: line[k] for k in LINE_HEAD if k in line}
+    out.update(line)
+    return out
+
+
+def parity_failures(obj, path="") -> list:
+    """Every parity check of the line that failed: a sample with mismatched
+    fields, a `parity` record with a false flag, a form not equal to plain."""
+    bad = []
+    if isinstance(obj, dict):
+        for k, v in obj.items():
+            here = f"{path}.{k}" if path else k
+            if k == "mismatched_fields" and isinstance(v, int) and v > 0:
+                bad.append(f"{here}={v}")
+            elif k == "equals_plain" and v is False:
+                bad.append(here)
+            elif path.endswith("parity") and v is False:
+                bad.append(here)
+            else:
+                bad += parity_failures(v, here)
+    return bad
+
+
 def measured_peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -894,6 +945,7 @@ def run_ours(args, rank, world, local):
     from mojoalign_b200 import _lib
 
     params = BENCH_PARAMS
+    assert dict(zip(BENCH_PARAM_VALUES, params.as_list())) == BENCH_PARAM_VALUES
     fa, prefix, prep_s = prepare_reference(args, rank, dist, local)
     n_seq = 2 * args.pairs
     pinned = torch.empty((n_seq, READ_LEN), dtype=torch.uint8, pin_memory=True)
@@ -1028,16 +1080,10 @@ def run_ours(args, rank, world, local):
     line = {"metric": METRIC, "value": round(value, 1), "unit": "reads/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": f"plain single-launch, {args.genome_mb} Mbp synthetic bisulfite reference "
-                                   f"(bwa-meth c2t index), {args.pairs} PE 2x{READ_LEN} read pairs per GPU",
-                       "form": "plain single-launch", "genome_bp": args.genome_mb * 1_000_000,
-                       "reads_per_gpu": n_seq, "read_len": READ_LEN, "paired": True,
-                       "params": dict(zip(["seed_len", "seed_stride", "max_occ", "max_diff", "max_soft", "max_adj",
-                                           "rescue_win"], params.as_list())),
-                       "tuning": tune.tuning, "autotune_sample_reads": 2 * ns,
-                       "kmer_k": args.kmer, "kmer3_k": args.kmer3, "index_hbm_bytes": int(gi.info.device_bytes),
-                       "l2": "inputs larger than L2 (reads and index several GB)",
-                       "mapped_frac": round(mapped, 4)},
+            "config": workload_config(args),
+            "run": {"tuning": tune.tuning, "autotune_sample_reads": 2 * ns, "kmer_k": args.kmer,
+                    "kmer3_k": args.kmer3, "index_hbm_bytes": int(gi.info.device_bytes),
+                    "mapped_frac": round(mapped, 4)},
             "e2e": {"value": round(e2e_value, 1), "unit": "reads/s",
                     "h2d_bytes_per_step": int(n_seq * READ_LEN + n_seq * 4),
                     "d2h_bytes_per_step": int(n_seq * 28)},
@@ -1096,11 +1142,16 @@ def run_ours(args, rank, world, local):
         del d_bases, d_lens, d_out
         torch.cuda.empty_cache()
         line["forms"] = run_forms(args, ctx, gi, params, fa, local, best)
+    bad = parity_failures(line)
+    line["parity_failures"] = bad
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        print(json.dumps(ordered_line(line)), flush=True)
     gi.close()
     ctx.close()
     dist.close()
+    if bad:
+        sys.stderr.write("parity check failed: " + ", ".join(bad) + "\n")
+        sys.exit(3)
 
 
 UNEVEN_MODEL = dict(len_fixed=0, len_lognorm_median=120.0, len_lognorm_sigma=0.35, len_min=36, len_max=300,
@@ -1322,56 +1373,100 @@ def _cpu_model() -> str:
     return "unknown"
 
 
-def run_reference(args, rank, world, local):
-    """The oracle (CPU restatement of the reference kernels) on all host cores."""
-    if rank != 0:
-        return
-    import oracle
-    from mojoalign_b200 import BENCH_PARAMS
+REF_SAMPLE_PAIRS = 1_000_000  # pairs handed to the reference arm (its steps time a part of them)
 
+
+def prepare_sample(args, out: str) -> None:
+    """Data preparation of the reference arm, run in a child process: the
+    synthetic reference and its index (built by this package, on the GPU
+    when there is one), the workload's reads, and the first pairs of the
+    batch saved to `out` (R1 rows, R2 rows, lengths) with the index prefix."""
     class _Solo(Dist):
         def __init__(self):
             super().__init__(1, "gloo")
 
-    dist = _Solo()
-    fa, prefix, _ = prepare_reference(args, 0, dist, local)
+    _, _, local = dist_env()
+    fa, prefix, _ = prepare_reference(args, 0, _Solo(), local)
     rb = simulate(args, fa, 0)
-    params = BENCH_PARAMS
+    n = min(rb.n1, REF_SAMPLE_PAIRS)
+    np.savez(out, r1=rb.bases[:n], r2=rb.bases[rb.n1:rb.n1 + n], l1=rb.lens[:n], l2=rb.lens[rb.n1:rb.n1 + n],
+             prefix=np.array(str(prefix)))
+
+
+def run_reference(args, rank, world, local):
+    """The reference algorithm on the host cores: the oracle (the CPU
+    restatement of the reference kernels; the Mojo reference cannot run
+    here).  The inputs are made by a child process, so this process loads
+    only the oracle's library."""
+    if rank != 0:
+        return
+    with tempfile.TemporaryDirectory(prefix="mojoalign_ref_") as td:
+        sample = Path(td) / "sample.npz"
+        cmd = [sys.executable, str(Path(__file__).resolve()), "--prepare-sample", str(sample),
+               "--genome-mb", str(args.genome_mb), "--pairs", str(args.pairs), "--workdir", args.workdir]
+        subprocess.run(cmd, check=True)
+        z = np.load(sample)
+        r1, r2, l1, l2, prefix = z["r1"], z["r2"], z["l1"], z["l2"], str(z["prefix"])
+    import oracle
+
+    plist = list(BENCH_PARAM_VALUES.values())
     ix = oracle.OracleIndex(prefix)
+
+    def batch(n):
+        return np.concatenate([r1[:n], r2[:n]]), np.concatenate([l1[:n], l2[:n]])
+
     # size one step to about cpu_seconds / (steps + warmup) * 2
-    probe = 10000
-    b, l = sample_pairs(rb, probe)
+    probe = min(10000, len(l1))
+    b, l = batch(probe)
     t = time.perf_counter()
-    ix.map(b, l, probe, True, READ_LEN, 1, 2, params.as_list())
+    ix.map(b, l, probe, True, READ_LEN, 1, 2, plist)
     rate = 2 * probe / (time.perf_counter() - t)
     per_step_s = max(2.0, 60.0 / max(1, args.steps + args.warmup))
-    n = int(min(rb.n1, max(probe, rate * per_step_s / 2)))
-    b, l = sample_pairs(rb, n)
+    n = int(min(len(l1), max(probe, rate * per_step_s / 2)))
+    b, l = batch(n)
     for _ in range(args.warmup):
-        ix.map(b, l, n, True, READ_LEN, 1, 2, params.as_list())
+        ix.map(b, l, n, True, READ_LEN, 1, 2, plist)
     t = time.perf_counter()
     for _ in range(args.steps):
-        ix.map(b, l, n, True, READ_LEN, 1, 2, params.as_list())
+        ix.map(b, l, n, True, READ_LEN, 1, 2, plist)
     dt = (time.perf_counter() - t) / args.steps
     value = 2 * n / dt
     line = {"metric": METRIC, "value": round(value, 1), "unit": "reads/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(dt * 1000, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"plain single-launch, {args.genome_mb} Mbp synthetic bisulfite reference "
-                                   f"(bwa-meth c2t index), {args.pairs} PE 2x{READ_LEN} read pairs per GPU",
-                       "form": "plain single-launch", "genome_bp": args.genome_mb * 1_000_000,
-                       "reads_per_gpu": 2 * args.pairs, "read_len": READ_LEN, "paired": True},
+            "config": workload_config(args),
             "cpu_baseline": {"value": round(value, 1), "unit": "reads/s", "cores": oracle.max_threads(),
                              "kind": "port", "cpu": _cpu_model(),
                              "sample": f"first {n} pairs ({2 * n} reads) of the workload per step"},
             "e2e": {"value": round(value, 1), "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    print(json.dumps(ordered_line(line)), flush=True)
+
+
+def gather_sweep(device: int = 0, sizes_mb=(16, 64, 256, 1024, 4096, 8192, 16384, 32768),
+                 loads: int = 1 << 30) -> dict:
+    """Measured random-gather roofline of this GPU: uniformly random,
+    independent loads of aligned 32- and 64-byte lines over buffers from
+    16 MiB (L2-resident) to 32 GiB (HBM), GB/s per buffer and line size.
+    The seed/extend kernels gather Occ lines, k-mer table entries and SA
+    entries at random: this is their ceiling, far below the copy bandwidth."""
+    from mojoalign_b200 import GpuContext
+
+    ctx = GpuContext(device)
+    try:
+        return {f"{mb}MiB_{lb}B_GBs": round(ctx.gather_gbps(mb << 20, lb, loads), 1)
+                for mb in sizes_mb for lb in (32, 64)}
+    finally:
+        ctx.close()
 
 
 def main():
     args = parse_args()
     rank, world, local = dist_env()
-    if args.impl == "reference":
+    if args.prepare_sample:
+        prepare_sample(args, args.prepare_sample)
+    elif args.gather_sweep:
+        print(json.dumps(gather_sweep(local)), flush=True)
+    elif args.impl == "reference":
         run_reference(args, rank, world, local)
     else:
         run_ours(args, rank, world, local)

@@ -222,13 +222,21 @@ int ma_map_batch_device(ma_ctx* ctx, const ma_index* idx,
  * HBM, or a latency-bound serving loop sharing the GPU with other streams,
  * where cudaMalloc's implicit device synchronisation would stall them.
  * Inputs and outputs stay the caller's device buffers; scratch comes from
- * one fixed file-scope device array (about 11 MiB, held on every GPU that
- * loads the library until exit).  Limits: at most 32768 reads per call
- * (16384 pairs) of at most 256 bases; larger calls fail with MA_ERR_ARG.
- * The first call on a device looks up the array's device address; make it
- * before any stream capture.  Calls share the array: calls whose kernels
- * overlap on the GPU race.  Synchronous on `stream` (a cudaStream_t, NULL
- * = the legacy default stream); errors are reported by ma_last_error(NULL).
+ * one fixed file-scope device array of about 11 MiB.  Limits: at most 32768
+ * reads per call (16384 pairs) of at most 256 bases; larger calls fail with
+ * MA_ERR_ARG.  Set-up: the first call on a device looks up the array's
+ * device address and loads the kernels it runs; under CUDA's default lazy
+ * module loading that is also when the array itself is placed on the
+ * device (with CUDA_MODULE_LOADING=EAGER, when the library loads), so the
+ * set-up can take device memory, as can a kernel's first launch (the driver
+ * sizes its local memory then).  A call with n1 = 0 does the set-up and
+ * launches every kernel of a call over zero reads: make it before a caching
+ * allocator reserves the free HBM, and before any stream capture.  The array then stays on the device until
+ * the process exits.  Calls share the array: calls whose kernels overlap on
+ * the GPU race.  Synchronous: the call waits for `stream` (a cudaStream_t,
+ * NULL = the legacy default stream) to read the device error word back.
+ * The caller's current device is restored on return.  Errors are reported
+ * by ma_last_error(NULL).
  */
 int ma_map_batch_device_noalloc(const ma_index* idx, const uint8_t* d_bases,
                                 const uint32_t* d_lens, uint32_t n1,

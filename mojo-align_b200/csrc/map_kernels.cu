@@ -786,4 +786,24 @@ int launch_rescue(const DevIndex& ix, const DevReads& R, const DevParams& P, con
     return 1;
 }
 
+// Loads (under lazy module loading) the kernels that the no-allocation
+// entry point launches: pack, the two seed stages at register level
+// `level`, and rescue.  Querying a kernel's attributes loads it.
+void load_noalloc_kernels(int level) {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, pack_rows_kernel);
+    cudaFuncGetAttributes(&a, pack_reads_kernel);
+    cudaFuncGetAttributes(&a, mate_rescue_kernel);
+    if (level == 1) {
+        cudaFuncGetAttributes(&a, seed_stage1_kernel<false, SeedKernels<false, 1>::B1>);
+        cudaFuncGetAttributes(&a, seed_stage2_kernel<false, SeedKernels<false, 1>::B2>);
+    } else if (level == 2) {
+        cudaFuncGetAttributes(&a, seed_stage1_kernel<false, SeedKernels<false, 2>::B1>);
+        cudaFuncGetAttributes(&a, seed_stage2_kernel<false, SeedKernels<false, 2>::B2>);
+    } else {
+        cudaFuncGetAttributes(&a, seed_stage1_kernel<false, SeedKernels<false, 0>::B1>);
+        cudaFuncGetAttributes(&a, seed_stage2_kernel<false, SeedKernels<false, 0>::B2>);
+    }
+}
+
 }  // namespace ma

@@ -10,14 +10,23 @@
 // to stage-2 hand-off and the device error flag) from one file-scope
 // __device__ array of fixed size instead of the context's pool.
 //
-// The array is loaded with the library and held on every GPU that loads
-// it until the process exits.  Its device address is looked up once per
-// device (cudaGetSymbolAddress with that device current) by the first call
-// made on that device; make that first call before any stream capture.
-// All calls share the array and it keeps the previous call's contents, so
-// everything that must start at zero is cleared by each call, and calls
-// whose kernels overlap on the GPU (different streams, or host threads
-// without ordering) race on it.
+// The array belongs to this file's module.  Under CUDA's default lazy
+// module loading (CUDA_MODULE_LOADING=LAZY) the module, and with it the
+// array, is loaded on a device the first time this entry point runs there;
+// with CUDA_MODULE_LOADING=EAGER it is loaded with the library.  Either way
+// it stays on every device it was loaded on until the process exits.  The
+// first call on a device is the set-up: with that device current it looks
+// up the array's device address (cudaGetSymbolAddress) and loads the
+// kernels the call runs, both of which can take device memory, as can the
+// first launch of a kernel (the driver sizes its local memory then).  A call
+// with n1 = 0 does the set-up and launches every kernel over zero reads, so a
+// caller can make it before its caching allocator reserves the free HBM;
+// make it before any stream capture too.  Each call is synchronous (it
+// reads the device error word back) and puts the caller's current device
+// back on return.  All calls share the array and it keeps the previous
+// call's contents, so everything that must start at zero is cleared by each
+// call, and calls whose kernels overlap on the GPU (different streams, or
+// host threads without ordering) race on it.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -39,6 +48,7 @@ int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams
 int stage2_blocks_per_sm(int level, bool counting);
 int launch_rescue(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int64_t n_pairs,
                   cudaStream_t st);
+void load_noalloc_kernels(int level);
 }  // namespace ma
 
 using namespace ma;
@@ -64,17 +74,36 @@ void ck(cudaError_t e, const char* what) {
     if (e != cudaSuccess) fail(MA_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-// Device address of the scratch array on `device` (which must be current).
+constexpr int kLevel = 2;  // register budget of the seed kernels this entry point runs
+
+// Set-up on `device` (which must be current), once: the device address of
+// the scratch array and the kernels of the call, loaded now so that later
+// calls load no module.
 void* scratch_on(int device) {
     if (device < 0 || device >= 64) fail(MA_ERR_ARG, "device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_mu);
     if (!g_scratch_addr[device]) {
         void* p = nullptr;
         ck(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(static scratch)");
+        load_noalloc_kernels(kLevel);
+        ck(cudaGetLastError(), "loading the mapping kernels");
         g_scratch_addr[device] = p;
     }
     return g_scratch_addr[device];
 }
+
+// Makes `device` current for the call and puts the caller's device back.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int device) {
+        ck(cudaGetDevice(&prev), "cudaGetDevice");
+        if (prev != device) ck(cudaSetDevice(device), "cudaSetDevice");
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
 
 }  // namespace
 
@@ -96,9 +125,12 @@ extern "C" int ma_map_batch_device_noalloc(const ma_index* idx, const uint8_t* d
             fail(MA_ERR_ARG, std::to_string(n_seq) + " reads exceed the static scratch maximum of " +
                                  std::to_string(kMaxReads) + " reads per call; split the batch");
         if (two_stage_scratch_bytes(n_seq) > kHandoffBytes) fail(MA_ERR_INTERNAL, "hand-off area too small");
-        if (n1 == 0) return MA_OK;
-        ck(cudaSetDevice(device), "cudaSetDevice");
+        DeviceGuard on_device(device);
         char* base = static_cast<char*>(scratch_on(device));
+        // a call with no reads still launches every kernel of a call (each
+        // returns at once), so that the driver sizes their local memory in
+        // the set-up call rather than in a later one
+        const bool setup_only = n1 == 0;
         uint64_t* packed = reinterpret_cast<uint64_t*>(base);
         void* handoff = base + kPackedBytes;
         int* err = reinterpret_cast<int*>(base + kPackedBytes + kHandoffBytes);
@@ -123,10 +155,10 @@ extern "C" int ma_map_batch_device_noalloc(const ma_index* idx, const uint8_t* d
         ck(cudaMemsetAsync(err, 0, sizeof(int), st), "cudaMemsetAsync");
         launch_pack(d_bases, d_lens, n_seq, n1, static_cast<int>(max_len), words, bs_r1, bs_r2, packed, err, st);
         DevReads R{packed, d_lens, words, n_seq};
-        const int level = 2;
+        const int level = kLevel;
         launch_seed_two_stage(*ix, R, P, o, 1, 2, stage2_blocks_per_sm(level, false) * sms, level, 32, handoff,
                               nullptr, nullptr, st);
-        if (paired && p->rescue_win > 0) launch_rescue(*ix, R, P, o, n1, st);
+        if (setup_only || (paired && p->rescue_win > 0)) launch_rescue(*ix, R, P, o, n1, st);
         ck(cudaGetLastError(), "kernel launch");
         int h = 0;
         ck(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H error flag");

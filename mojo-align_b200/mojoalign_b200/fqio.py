@@ -11,6 +11,7 @@ gzip file is read by the gzip module, one member after another.
 from __future__ import annotations
 
 import gzip
+import io
 import os
 import struct
 import zlib
@@ -57,6 +58,27 @@ def _inflate_members(blob: bytes, sizes: list) -> bytes:
     return b"".join(out)
 
 
+class _Prefixed(io.RawIOBase):
+    """A raw binary reader: the bytes `head`, then the rest of file `fh`
+    (which stays open: its owner closes it)."""
+
+    def __init__(self, head: bytes, fh):
+        super().__init__()
+        self._head = memoryview(head)
+        self._fh = fh
+
+    def readable(self) -> bool:
+        return True
+
+    def readinto(self, b) -> int:
+        if len(self._head):
+            k = min(len(b), len(self._head))
+            b[:k] = self._head[:k]
+            self._head = self._head[k:]
+            return k
+        return self._fh.readinto(b)
+
+
 class BgzfReader:
     """A binary file object over a BGZF file: its members are inflated by a
     thread pool in batches of about `batch_bytes` compressed bytes, in order.
@@ -97,24 +119,35 @@ class BgzfReader:
                     first_byte, first_member = off, i + 1
             return
         # no whole BGZF member at the front
-        more = self._fh.read(1)
-        if more:  # a member that is not BGZF: read on to the end of the file
+        n = _bgzf_size(self._raw[:18 + 256])
+        if n and len(self._raw) < n:
+            # a BGZF member cut by the batch boundary: read the rest of it
+            more = self._fh.read(n - len(self._raw))
+            if not more:
+                raise EOFError("Compressed file ended before the end-of-stream marker was reached")
             self._raw += more
-            self._batch *= 2
             return
+        # zero padding (gzip allows it between and after members) is skipped
+        head = self._raw.lstrip(b"\0")
+        while not head:
+            chunk = self._fh.read(1 << 16)
+            if not chunk:
+                self._done = True
+                self._raw = b""
+                return
+            head = chunk.lstrip(b"\0")
+        if len(head) < 18 + 256:
+            head += self._fh.read(18 + 256 - len(head))
+        if _bgzf_size(head[:18 + 256]):
+            self._raw = head  # BGZF members go on after the padding
+            return
+        if head[:2] != _MAGIC[:2]:
+            raise gzip.BadGzipFile("Not a gzipped file (%r)" % head[:2])
+        # a member that is not BGZF: the gzip module reads the rest of the
+        # file from here, straight from the open file
         self._done = True
-        rest = self._raw.lstrip(b"\0")  # gzip allows zero padding after a member
         self._raw = b""
-        if not rest:
-            return
-        if rest[:2] != _MAGIC[:2]:
-            raise gzip.BadGzipFile("Not a gzipped file (%r)" % rest[:2])
-        if _bgzf_size(rest[:18 + 256]) and len(rest) < _bgzf_size(rest[:18 + 256]):
-            raise EOFError("Compressed file ended before the end-of-stream marker was reached")
-        import io
-
-        # a plain gzip member (or zero padding between members) from here on
-        self._tail = gzip.GzipFile(fileobj=io.BytesIO(rest))
+        self._tail = gzip.GzipFile(fileobj=io.BufferedReader(_Prefixed(head, self._fh)))
 
     def _fill_jobs(self) -> None:
         while not self._done and len(self._jobs) < 4 * self._threads:

@@ -1,7 +1,7 @@
 """Regenerates tests/golden/bam_records.json from the reference.
 
 Run from the repository root where the mojo-align source tree is available
-(argument 1, default /root/reference).  The reference's Python BAM writer,
+(its path is the one required argument).  The reference's Python BAM writer,
 fq2bam-meth/python/bam_emit.py (BamWriter.write_batch, L358-475), is
 imported and run on seeded random alignments; its BGZF layer is replaced by
 a byte sink so the raw records can be kept.  The records it packs follow
@@ -108,4 +108,6 @@ def main(root: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <mojo-align source tree>")
+    main(Path(sys.argv[1]))

@@ -1,7 +1,7 @@
 """Regenerates tests/golden/bgzf_vectors.json from the reference.
 
 Run from the repository root where the mojo-align source tree is available
-(argument 1, default /root/reference).  Imports the reference's BAM writer,
+(its path is the one required argument).  Imports the reference's BAM writer,
 fq2bam-meth/python/bam_emit.py, and records what its BGZF layer
 (_bgzf_block L77-98 through _BgzfWriter L101-186) writes for deterministic
 inputs: per level, the SHA-256 and size of the file and of each member, for
@@ -62,4 +62,6 @@ def main(root: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <mojo-align source tree>")
+    main(Path(sys.argv[1]))

@@ -1,7 +1,7 @@
 """Regenerates tests/golden/conversion_vectors.json from the reference.
 
 Run from the repository root in an environment where the mojo-align source
-tree is available (argument 1, default /root/reference).  The reference's
+tree is available (its path is the one required argument).  The reference's
 orchestrator module fq2bam-meth/python/fq2bam_meth.py is plain Python and is
 imported and executed to produce its conversion outputs.  The Mojo FASTQ
 path (fq2bam-meth/src/linear_fastq.mojo) cannot run without the Mojo
@@ -82,4 +82,6 @@ def main(root: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <mojo-align source tree>")
+    main(Path(sys.argv[1]))

@@ -1,7 +1,7 @@
 """Regenerates tests/golden/fastq_pair_reader.json from the reference.
 
 Run from the repository root where the mojo-align source tree is available
-(argument 1, default /root/reference).  The reference's FASTQ reader of the
+(its path is the one required argument).  The reference's FASTQ reader of the
 SAM path, fq2bam-meth/python/fastq_batch.py (FastqPairReader, L230-325, and
 _qname, L18-28), is imported and run over hand-made FASTQ texts: line-ending
 variants, records cut short at the end, blank lines, names with and without
@@ -120,4 +120,6 @@ def main(root: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <mojo-align source tree>")
+    main(Path(sys.argv[1]))

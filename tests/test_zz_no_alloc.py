@@ -6,7 +6,9 @@ holds the free HBM, or a latency-bound loop that cannot absorb cudaMalloc's
 implicit device synchronisation).  It takes its scratch from a fixed
 device array instead of the context's pool.  Its outputs must equal those
 of ma_map_batch_device on the same reads, exactly (integer outputs), on two
-calls in a row, since the array keeps the previous call's contents.
+calls in a row, since the array keeps the previous call's contents, and
+the device's free memory must be the same after each of those calls as
+before it (after the set-up call with no reads).
 
 This file is named to be collected last, so a run that stops at the first
 failure has run every other test before it.
@@ -51,20 +53,32 @@ def test_noalloc_matches_allocating_entry_point(small_ref):
     want = {f: ref[f].cpu().numpy() for f in FIELDS}
 
     p = BENCH_PARAMS.to_c()
-    for call in range(2):
-        out = _device_outputs(torch, n, dev)
+    outs = [_device_outputs(torch, n, dev) for _ in range(2)]
+    args = []
+    for out in outs:
         for t in out.values():
             t.fill_(-7)
-        hits = _lib.ma_hits(*[out[f].data_ptr() for f in MapResult.FIELDS])
-        dbg = _lib.ma_debug(*[out[f].data_ptr() for f in MapResult.DEBUG])
+        args.append((_lib.ma_hits(*[out[f].data_ptr() for f in MapResult.FIELDS]),
+                     _lib.ma_debug(*[out[f].data_ptr() for f in MapResult.DEBUG])))
+    # set-up call (no reads): places the scratch array and loads the kernels
+    _lib.check(_lib.lib.ma_map_batch_device_noalloc(gi.handle, d_bases.data_ptr(), d_lens.data_ptr(), 0, 1, 150,
+                                                    1, 2, C.byref(p), C.byref(args[0][0]), None,
+                                                    stream.cuda_stream))
+    torch.cuda.synchronize()
+    for call, (out, (hits, dbg)) in enumerate(zip(outs, args)):
+        free_before = torch.cuda.mem_get_info(dev)[0]
         rc = _lib.lib.ma_map_batch_device_noalloc(gi.handle, d_bases.data_ptr(), d_lens.data_ptr(), rb.n1, 1, 150,
                                                   1, 2, C.byref(p), C.byref(hits), C.byref(dbg),
                                                   stream.cuda_stream)
         _lib.check(rc)
         torch.cuda.synchronize()
+        # the property the entry point exists for: the device's free memory
+        # is the same after the call as before it
+        assert torch.cuda.mem_get_info(dev)[0] == free_before, f"call {call} changed the free device memory"
         for f in FIELDS:
             got = out[f].cpu().numpy()
             assert np.array_equal(got, want[f]), f"call {call}: field {f} differs from ma_map_batch_device"
+    hits = args[0][0]
 
     # a batch beyond the fixed scratch size is refused with a clear error
     big = 20000  # pairs -> 40000 reads > 32768
