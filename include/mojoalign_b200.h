@@ -766,6 +766,33 @@ int ma_bench_gather(ma_ctx* ctx, uint64_t buffer_bytes, int line_bytes, uint64_t
 int ma_synth_reference(const char* fasta_out, uint64_t total_len,
                        int n_contigs, double gc, double cpg, uint64_t seed);
 
+/* Repeat content of a synthetic reference (ma_synth_reference_model). */
+typedef struct ma_repeat_model {
+    double repeat_frac;   /* share of bases in copies of family elements    */
+    double tandem_frac;   /* share of bases in low-complexity tandem runs    */
+    uint32_t families;    /* element families per length class               */
+    uint32_t short_len;   /* element length of the short class (e.g. 300)    */
+    uint32_t long_len;    /* element length of the long class (e.g. 6000);
+                             long copies are 5' fragments, 1/8..1 of it      */
+    double long_share;    /* share of copied bases from the long class       */
+    double div_min, div_max; /* per-copy divergence, uniform in this range:
+                             substitutions at that rate, 1-bp insertions and
+                             deletions at a twentieth of it each             */
+    uint32_t unit_min, unit_max; /* tandem unit length range (bases)         */
+    uint32_t run_min, run_max;   /* tandem run length range (bases), 2% of
+                             the run's bases substituted                     */
+} ma_repeat_model;
+
+/*
+ * The base model of ma_synth_reference, generated contig by contig on host
+ * threads (the output depends on the seed only), with copies of repeat
+ * family elements (either orientation) and tandem runs interleaved with the
+ * background when rm is not NULL.
+ */
+int ma_synth_reference_model(const char* fasta_out, uint64_t total_len,
+                             int n_contigs, double gc, double cpg,
+                             uint64_t seed, const ma_repeat_model* rm);
+
 typedef struct ma_read_model {
     uint32_t len_fixed;     /* >0: every read this long                       */
     double len_lognorm_median; /* used when len_fixed == 0                    */

@@ -39,6 +39,8 @@ int launch_rescue(const DevIndex& ix, const DevReads& R, const DevParams& P, con
 }  // namespace ma
 
 extern "C" int ma_synth_reference_impl(const char*, uint64_t, int, double, double, uint64_t, char*, size_t);
+extern "C" int ma_synth_reference_model_impl(const char*, uint64_t, int, double, double, uint64_t,
+                                             const ma_repeat_model*, char*, size_t);
 extern "C" int ma_synth_reads_impl(const char*, const ma_read_model*, uint32_t, int, uint32_t, uint64_t, uint8_t*,
                                    uint32_t*, uint64_t*, uint8_t*, char*, size_t);
 
@@ -1512,6 +1514,14 @@ int ma_synth_reference(const char* fasta_out, uint64_t total_len, int n_contigs,
                        uint64_t seed) {
     char err[512] = {0};
     int rc = ma_synth_reference_impl(fasta_out, total_len, n_contigs, gc, cpg, seed, err, sizeof err);
+    if (rc != MA_OK) t_err = err;
+    return rc;
+}
+
+int ma_synth_reference_model(const char* fasta_out, uint64_t total_len, int n_contigs, double gc, double cpg,
+                             uint64_t seed, const ma_repeat_model* rm) {
+    char err[512] = {0};
+    int rc = ma_synth_reference_model_impl(fasta_out, total_len, n_contigs, gc, cpg, seed, rm, err, sizeof err);
     if (rc != MA_OK) t_err = err;
     return rc;
 }

@@ -110,6 +110,23 @@ class ma_pipeline(C.Structure):
                 ("compute_streams", C.c_uint32)]
 
 
+class ma_repeat_model(C.Structure):
+    _fields_ = [
+        ("repeat_frac", C.c_double),
+        ("tandem_frac", C.c_double),
+        ("families", C.c_uint32),
+        ("short_len", C.c_uint32),
+        ("long_len", C.c_uint32),
+        ("long_share", C.c_double),
+        ("div_min", C.c_double),
+        ("div_max", C.c_double),
+        ("unit_min", C.c_uint32),
+        ("unit_max", C.c_uint32),
+        ("run_min", C.c_uint32),
+        ("run_max", C.c_uint32),
+    ]
+
+
 class ma_read_model(C.Structure):
     _fields_ = [
         ("len_fixed", C.c_uint32),
@@ -265,6 +282,8 @@ SIGNATURES = [
      [C.c_void_p, C.c_void_p, C.c_uint64] + [C.c_void_p] * 5 + [C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p,
                                                                 C.c_void_p]),
     ("ma_synth_reference", C.c_int, [C.c_char_p, C.c_uint64, C.c_int, C.c_double, C.c_double, C.c_uint64]),
+    ("ma_synth_reference_model", C.c_int,
+     [C.c_char_p, C.c_uint64, C.c_int, C.c_double, C.c_double, C.c_uint64, C.POINTER(ma_repeat_model)]),
     ("ma_synth_reads", C.c_int,
      [C.c_char_p, C.POINTER(ma_read_model), C.c_uint32, C.c_int, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p,
       C.c_void_p, C.c_void_p]),

@@ -1,17 +1,52 @@
 """Seeded synthetic references and bisulfite reads (benchmarks and tests)."""
 from __future__ import annotations
 
+import ctypes as C
 from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import check, fspath, lib, ma_read_model, ptr
+from ._lib import check, fspath, lib, ma_read_model, ma_repeat_model, ptr
 
 
 def write_reference(path, total_len: int, n_contigs: int = 1, gc: float = 0.41, cpg: float = 0.01,
                     seed: int = 0) -> None:
     """FASTA from a first-order base model (GC fraction gc, CpG rate cpg)."""
     check(lib.ma_synth_reference(fspath(path), total_len, n_contigs, gc, cpg, seed))
+
+
+@dataclass
+class RepeatModel:
+    """Repeat content of a synthetic reference.  The defaults are the
+    repeat-heavy configuration: 45% of the bases in copies of 300 bp and
+    6 kb family elements at 10-20% divergence, 3% in low-complexity tandem
+    runs."""
+    repeat_frac: float = 0.45
+    tandem_frac: float = 0.03
+    families: int = 64
+    short_len: int = 300
+    long_len: int = 6000
+    long_share: float = 0.5
+    div_min: float = 0.10
+    div_max: float = 0.20
+    unit_min: int = 1
+    unit_max: int = 6
+    run_min: int = 20
+    run_max: int = 400
+
+    def to_c(self) -> ma_repeat_model:
+        return ma_repeat_model(self.repeat_frac, self.tandem_frac, self.families, self.short_len, self.long_len,
+                               self.long_share, self.div_min, self.div_max, self.unit_min, self.unit_max,
+                               self.run_min, self.run_max)
+
+
+def write_reference_model(path, total_len: int, n_contigs: int = 1, gc: float = 0.41, cpg: float = 0.01,
+                          seed: int = 0, repeats: RepeatModel | None = None) -> None:
+    """FASTA from the same base model as write_reference, generated contig by
+    contig on host threads, with the repeat model when `repeats` is given."""
+    rm = repeats.to_c() if repeats is not None else None
+    check(lib.ma_synth_reference_model(fspath(path), total_len, n_contigs, gc, cpg, seed,
+                                       None if rm is None else C.byref(rm)))
 
 
 @dataclass

@@ -27,7 +27,8 @@ def build() -> Path:
 
 class Counters(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in
-                ("occ_lines", "lf_lines", "sa_loads", "pac_sectors", "endpoints", "steps", "rows", "extends")]
+                ("occ_lines", "lf_lines", "sa_loads", "pac_sectors", "endpoints", "steps", "rows", "extends",
+                 "capped", "fallback")]
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}

@@ -64,6 +64,8 @@ typedef struct orc_counters {
     uint64_t steps;      /* backward-search steps                            */
     uint64_t rows;       /* SA rows resolved                                 */
     uint64_t extends;    /* (locus, adj) candidates compared                 */
+    uint64_t capped;     /* searches stopped by occ > max_occ (L1378-1379)   */
+    uint64_t fallback;   /* seeds taken from the <= 16-row fallback (L1381-1385) */
 } orc_counters;
 
 static char g_err[512];
@@ -461,11 +463,15 @@ static void seed_extend_one(const orc_index *ix, const uint8_t *codes, const uin
             if (occ_n >= 1 && occ_n <= 16 && mlen >= seed_len) { /* L1374-1377 */
                 last_k = k; last_l = l; last_s = s;
             }
-            if (occ_n > max_occ && mlen >= seed_len) break;      /* L1378-1379 */
+            if (occ_n > max_occ && mlen >= seed_len) {           /* L1378-1379 */
+                if (ct) ct->capped++;
+                break;
+            }
             s -= 1;
         }
         if (!found && last_s >= 0) {                   /* L1381-1385 */
             uk = last_k; ul = last_l; us = last_s; found = 1;
+            if (ct) ct->fallback++;
         }
         if (found) {
             uint64_t hi = uk;
@@ -870,6 +876,8 @@ int orc_map(const orc_index *ix, const uint8_t *bases, const uint32_t *lens, uin
             counters->steps += tc[t].steps;
             counters->rows += tc[t].rows;
             counters->extends += tc[t].extends;
+            counters->capped += tc[t].capped;
+            counters->fallback += tc[t].fallback;
         }
         free(tc);
     }
