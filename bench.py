@@ -90,6 +90,17 @@ def parse_args():
                     "stage (0 = skip)")
     ap.add_argument("--fq2sam-pairs", type=int, default=2_000_000, help="read pairs of the FASTQ -> SAM stage "
                     "(0 = skip)")
+    ap.add_argument("--workload", choices=["chromosome", "genome", "repeats"], default="chromosome",
+                    help="chromosome: 250 Mbp, 10 M pairs 2x150, plain single-launch (and the file stages); "
+                    "genome: 3.1 Gbp, 50 M uneven single-end reads, batched / plain / served forms and the served "
+                    "stream; repeats: 3.1 Gbp with 45%% repeats, 10 M pairs 2x250 at conversion 0.97")
+    ap.add_argument("--genome-mb-large", type=int, default=0, help="reference size of the genome workloads "
+                    "(0 = 3100)")
+    ap.add_argument("--genome-reads", type=int, default=0, help="reads (pairs) of the genome workloads "
+                    "(0 = the workload's)")
+    ap.add_argument("--genome-chunk", type=int, default=25_000_000, help="reads per device call")
+    ap.add_argument("--parity-reads", type=int, default=1_000_000, help="reads checked against the oracle")
+    ap.add_argument("--serve-stream-budget-mb", type=int, default=1536, help="HBM budget of the served stream")
     ap.add_argument("--gather-sweep", action="store_true", help="print the measured random-gather roofline "
                     "(32- and 64-byte lines, 16 MiB to 32 GiB buffers) as one JSON object and exit")
     ap.add_argument("--prepare-sample", default="", help=argparse.SUPPRESS)
@@ -157,11 +168,15 @@ def shard_seed(rank: int) -> int:
     return 1 + rank
 
 
-def prepare_reference(args, rank, dist: Dist, device: int):
-    """Synthetic reference + bwa-meth index, built once per node by rank 0."""
+def prepare_reference(args, rank, dist: Dist, device: int, genome_mb: int | None = None, repeats=None,
+                      tag: str = ""):
+    """Synthetic reference + bwa-meth index, built once per node by rank 0
+    (the index on the GPU).  `repeats` (a synth.RepeatModel) adds the
+    repeat-heavy model."""
     from mojoalign_b200 import build_index, synth
 
-    d = Path(args.workdir) / f"mojoalign_bench_{args.genome_mb}mb"
+    genome_mb = genome_mb or args.genome_mb
+    d = Path(args.workdir) / f"mojoalign_bench_{genome_mb}mb{tag}"
     d.mkdir(parents=True, exist_ok=True)
     fa = d / "ref.fa"
     prefix = Path(str(fa) + ".bwameth.c2t")
@@ -174,8 +189,9 @@ def prepare_reference(args, rank, dist: Dist, device: int):
             device = device if torch.cuda.is_available() else -1
         except ImportError:
             device = -1
-        n_contigs = max(1, args.genome_mb // 50)
-        synth.write_reference(fa, args.genome_mb * 1_000_000, n_contigs=n_contigs, gc=0.41, cpg=0.01, seed=0)
+        n_contigs = max(1, min(24, genome_mb // 50))
+        synth.write_reference_model(fa, genome_mb * 1_000_000, n_contigs=n_contigs, gc=0.41, cpg=0.01, seed=0,
+                                    repeats=repeats)
         build_index(fa, prefix, bwameth_c2t=True, sa_intv=32, device=device)
         done.write_text("ok\n")
     dist.barrier()
@@ -1363,6 +1379,422 @@ def run_forms(args, ctx, gi, params, fa, local, best_tuning):
     return forms
 
 
+GENOME_WORKLOADS = {
+    # configs[2]/[3]: 3.1 Gbp reference, 50 M uneven single-end reads, then
+    # the served stream against the same resident index
+    "genome": dict(genome_mb=3100, repeats=False, n1=50_000_000, paired=False, max_len=UNEVEN_MAX,
+                   model=UNEVEN_MODEL, bs=("C2T", ""),
+                   text="{n1} single-end reads, lengths lognormal (median 120, sigma 0.35) clipped to 36-300, "
+                        "half non-directional, on a {mb} Mbp synthetic bisulfite reference (bwa-meth c2t index)"),
+    # 3.1 Gbp reference with 45% repeats + 3% tandem runs,
+    # 20 M pairs 2x250 at non-CpG conversion 0.97
+    "repeats": dict(genome_mb=3100, repeats=True, n1=10_000_000, paired=True, max_len=250,
+                    model=dict(len_fixed=250, frag_mean=500, frag_sd=60, conv_non_cpg=0.97),
+                    bs=("C2T", "G2A"),
+                    text="{n1} PE 2x250 read pairs (non-CpG conversion 0.97) on a {mb} Mbp synthetic bisulfite "
+                         "reference with 45% repeats (300 bp / 6 kb families, 10-20% divergence) and 3% tandem "
+                         "runs (bwa-meth c2t index)"),
+}
+
+
+def genome_config(args, spec) -> dict:
+    mb = args.genome_mb_large or spec["genome_mb"]
+    n1 = args.genome_reads or spec["n1"]
+    n_seq = n1 * (2 if spec["paired"] else 1)
+    return {"workload": spec["text"].format(n1=n1, mb=mb), "form": "batched (one device call per chunk)",
+            "genome_bp": mb * 1_000_000, "reads_per_gpu": n_seq, "paired": spec["paired"],
+            "max_len": spec["max_len"], "params": dict(BENCH_PARAM_VALUES),
+            "l2": "inputs larger than L2 (reads and index tens of GB)"}
+
+
+def run_genome(args, rank, world, local):
+    """Genome scale: the batched (autotuned) form over the whole read set
+    per step, the plain single-launch form and the served form on the same
+    reads, a served stream of 8 samples, parity against the oracle."""
+    import torch
+    from mojoalign_b200 import BENCH_PARAMS, GpuContext, GpuIndex, MapResult, map_batch, map_batch_device, synth
+    from mojoalign_b200 import _lib
+
+    spec = GENOME_WORKLOADS[args.workload]
+    torch.cuda.set_device(local)
+    dist = Dist(world, "nccl")
+    params = BENCH_PARAMS
+    mb = args.genome_mb_large or spec["genome_mb"]
+    n1 = args.genome_reads or spec["n1"]
+    paired, max_len = spec["paired"], spec["max_len"]
+    n_seq = n1 * (2 if paired else 1)
+    bs1, bs2 = spec["bs"]
+    dev = f"cuda:{local}"
+    timings = {}
+    t = time.time()
+    fa, prefix, timings["reference_and_index"] = prepare_reference(
+        args, rank, dist, local, genome_mb=mb, repeats=synth.RepeatModel() if spec["repeats"] else None,
+        tag="_repeats" if spec["repeats"] else "")
+    t = time.time()
+    pinned = torch.empty((n_seq, max_len), dtype=torch.uint8, pin_memory=True)
+    rb = synth.simulate_reads(fa, synth.ReadModel(**spec["model"]), n1, paired, max_len, seed=shard_seed(rank),
+                              bases_out=pinned.numpy())
+    timings["reads"] = time.time() - t
+    bases_np, lens_np = pinned.numpy(), rb.lens
+    ctx = GpuContext(local)
+    t = time.time()
+    gi = GpuIndex(ctx, prefix, kmer_k=args.kmer, kmer3_k=args.kmer3)
+    timings["index_open"] = time.time() - t
+
+    d_bases = pinned.to(dev).reshape(-1)
+    d_lens = torch.from_numpy(lens_np.view(np.int32)).to(dev)
+    d_out = {f: torch.empty(n_seq, dtype=torch.int32, device=dev) for f in MapResult.FIELDS}
+    stream = torch.cuda.current_stream()
+    # pairs (or reads) per device call: the packed reads and the seed
+    # scratch of one call stay a few GB
+    chunk = max(1, min(n1, args.genome_chunk // (2 if paired else 1)))
+
+    def call(a, c):
+        """One device call over single-end reads [a, a + c)."""
+        offs = {f: x.data_ptr() + 4 * a for f, x in d_out.items()}
+        map_batch_device(ctx, gi, d_bases.data_ptr() + a * max_len, d_lens.data_ptr() + 4 * a, c, False,
+                         max_len, offs, bs1, bs2, params, stream=stream.cuda_stream)
+
+    if paired:
+        # the pairs as one call each chunk: the R1 and R2 rows of a chunk of
+        # pairs are not adjacent in the full batch, so each chunk is staged
+        # as its own batch (R1 rows, then R2 rows)
+        rows = d_bases.view(n_seq, max_len)
+        chunk_rows = torch.empty((2 * chunk, max_len), dtype=torch.uint8, device=dev)
+        chunk_lens = torch.empty(2 * chunk, dtype=torch.int32, device=dev)
+        chunk_out = {f: torch.empty(2 * chunk, dtype=torch.int32, device=dev) for f in MapResult.FIELDS}
+
+        def call(a, c):  # noqa: F811
+            chunk_rows[:c].copy_(rows[a:a + c])
+            chunk_rows[c:2 * c].copy_(rows[n1 + a:n1 + a + c])
+            chunk_lens[:c].copy_(d_lens[a:a + c])
+            chunk_lens[c:2 * c].copy_(d_lens[n1 + a:n1 + a + c])
+            map_batch_device(ctx, gi, chunk_rows.data_ptr(), chunk_lens.data_ptr(), c, True, max_len,
+                             {f: x.data_ptr() for f, x in chunk_out.items()}, bs1, bs2, params,
+                             stream=stream.cuda_stream)
+            for f, x in d_out.items():
+                x[a:a + c].copy_(chunk_out[f][:c])
+                x[n1 + a:n1 + a + c].copy_(chunk_out[f][c:2 * c])
+
+    def step():
+        for a in range(0, n1, chunk):
+            call(a, min(chunk, n1 - a))
+
+    # ---- kernel form picked by the autotuner on a sample ----
+    from mojoalign_b200.autotune import FIELDS as TFIELDS
+    from mojoalign_b200.autotune import TuneResult, autotune
+
+    ns = min(n1, 1_000_000 if paired else 2_000_000)
+    if args.tuning:
+        fixed = [int(x) for x in args.tuning.split(",")]
+        fixed += [2, 1, 0, 2, 1, 1, 8, 4, 0, 1][len(fixed):]
+        ctx.set_tuning(*fixed)
+        tune = TuneResult(dict(zip(TFIELDS, fixed)), float("nan"), [])
+    else:
+        if paired:
+            sb = np.concatenate([bases_np[:ns], bases_np[n1:n1 + ns]])
+            sl = np.concatenate([lens_np[:ns], lens_np[n1:n1 + ns]])
+        else:
+            sb, sl = bases_np[:ns], lens_np[:ns]
+        d_sb = torch.from_numpy(sb).to(dev).reshape(-1)
+        d_sl = torch.from_numpy(sl.view(np.int32)).to(dev)
+        n_s = sl.size
+        s_out = {f: torch.empty(n_s, dtype=torch.int32, device=dev) for f in MapResult.FIELDS}
+        s_dbg = {f: torch.empty(n_s, dtype=torch.int64 if f in ("uk", "ul") else torch.int32, device=dev)
+                 for f in MapResult.DEBUG}
+
+        def run_sample():
+            map_batch_device(ctx, gi, d_sb.data_ptr(), d_sl.data_ptr(), ns, paired, max_len,
+                             {f: x.data_ptr() for f, x in s_out.items()}, bs1, bs2, params,
+                             d_debug={f: x.data_ptr() for f, x in s_dbg.items()}, stream=stream.cuda_stream)
+            outs = {f: x.cpu().numpy() for f, x in list(s_out.items()) + list(s_dbg.items())}
+            return outs, ctx.kernel_ms()[1]
+
+        tune = autotune(ctx, gi, sb, sl, ns, paired, max_len, bs1, bs2, params, run=run_sample)
+        del d_sb, d_sl, s_out, s_dbg, sb, sl
+    best = tuple(tune.tuning[f] for f in TFIELDS if f in tune.tuning)
+
+    # ---- traffic tally: one untimed pass of the counting kernels ----
+    _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 2), ctx.handle)
+    tally = [0] * 12
+    for a in range(0, n1, chunk):
+        call(a, min(chunk, n1 - a))
+        tt = (_lib.C.c_uint64 * 12)()
+        _lib.lib.ma_ctx_traffic(ctx.handle, tt)
+        tally = [x + y for x, y in zip(tally, tt)]
+    _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 1), ctx.handle)
+
+    # ---- timed steps: the batched form over every read ----
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    seed_ms = []
+    kms = (_lib.C.c_float * 4)()
+    launches = 0
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        sm = 0.0
+        for a in range(0, n1, chunk):
+            call(a, min(chunk, n1 - a))
+            _lib.lib.ma_ctx_kernel_ms(ctx.handle, kms)
+            sm += float(kms[1])
+            launches += ctx.last_launch_count()
+        seed_ms.append(sm)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    clk = clocks.stop()
+    dist.barrier()
+    ms_max = dist.max(ms)
+    value = aggregate_reads_per_s(n_seq, world, ms_max)
+    batched_out = {f: x.cpu().numpy() for f, x in d_out.items()}
+
+    # ---- end to end from pinned host buffers (copies inside) ----
+    _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 0), ctx.handle)
+    res = MapResult.empty(n_seq, debug=False)
+    map_batch(ctx, gi, bases_np, lens_np, n1, paired, max_len, bs1, bs2, params, out=res)
+    dist.barrier()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        map_batch(ctx, gi, bases_np, lens_np, n1, paired, max_len, bs1, bs2, params, out=res)
+    e2e_s = dist.max((time.perf_counter() - t) / args.steps)
+    e2e_same = all(np.array_equal(getattr(res, f).view(np.int32), batched_out[f]) for f in MapResult.FIELDS)
+
+    # ---- roofline of the seed kernels ----
+    peaks = measured_peaks()
+    words = (max_len + 31) // 32
+    alg_bytes = 32 * (tally[0] + tally[1] + tally[2] + tally[3]) + n_seq * (4 * words * 8 + 4) + n_seq * 28
+    seed_avg_ms = statistics.mean(seed_ms)
+    achieved = alg_bytes / (seed_avg_ms / 1000.0) / 1e9
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+            "frac": round(achieved / peaks.get("hbm_gbs"), 4), "traffic": None,
+            "peak_source": "fallback" if peaks.get("_fallback") else "measured (MEASURED_PEAKS.json hbm_gbs)",
+            "kernel": SEED_KERNELS.get(tune.tuning.get("seed_kernel", 2), "seed/extend"),
+            "kernel_ms": round(seed_avg_ms, 3), "alg_bytes_per_launch": int(alg_bytes),
+            "tally_per_read": {k: round(v / n_seq, 3) for k, v in zip(
+                ["occ_lines_32B", "kmer_loads", "sa_loads", "pac_sectors_32B", "backward_steps", "endpoints",
+                 "loci_evaluated", "read_words", "endpoints_skipped", "stage2_reads", "stage2_groups",
+                 "shift_evals"], tally)}}
+
+    line = {"metric": METRIC, "value": round(value, 1), "unit": "reads/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": genome_config(args, spec),
+            "run": {"tuning": tune.tuning, "autotune": tune.all_ms, "kmer_k": args.kmer, "kmer3_k": args.kmer3,
+                    "index_hbm_bytes": int(gi.info.device_bytes), "calls_per_step": -(-n1 // chunk),
+                    "mapped_frac": round(float((batched_out["rid"] >= 0).mean()), 4)},
+            "e2e": {"value": round(aggregate_reads_per_s(n_seq, world, e2e_s * 1000.0), 1), "unit": "reads/s",
+                    "h2d_bytes_per_step": int(n_seq * max_len + n_seq * 4), "d2h_bytes_per_step": int(n_seq * 28),
+                    "equals_device": bool(e2e_same)},
+            "gpu_launches": launches, "roofline": roof, "clocks": clk,
+            "setup_s": {k: round(v, 1) for k, v in timings.items()}}
+    if rank == 0:
+        line["gather_roofline"] = {}
+        for lb in (32, 64):
+            g = _lib.C.c_double()
+            _lib.check(_lib.lib.ma_bench_gather(ctx.handle, 8 << 30, lb, 1 << 30, _lib.C.byref(g)), ctx.handle)
+            line["gather_roofline"][f"hbm_{lb}B_GBs"] = round(g.value, 1)
+        line["roofline"]["frac_of_gather32"] = round(achieved / line["gather_roofline"]["hbm_32B_GBs"], 4)
+        line["roofline"]["frac_of_gather64"] = round(achieved / line["gather_roofline"]["hbm_64B_GBs"], 4)
+    if rank == 0 and world == 1 and not args.no_forms and not paired:
+        del d_bases
+        torch.cuda.empty_cache()
+        line["forms"] = genome_forms(args, ctx, gi, params, fa, local, best, bases_np, lens_np, n1, max_len,
+                                     batched_out, value, stream)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        t = time.perf_counter()
+        ix = oracle.OracleIndex(prefix)
+        load_s = time.perf_counter() - t
+        n = min(n1, args.parity_reads // (2 if paired else 1))
+        if paired:
+            b = np.concatenate([bases_np[:n], bases_np[n1:n1 + n]])
+            l_ = np.concatenate([lens_np[:n], lens_np[n1:n1 + n]])
+        else:
+            b, l_ = bases_np[:n], lens_np[:n]
+        t = time.perf_counter()
+        o = ix.map(b, l_, n, paired, max_len, 1, 2 if paired else 0, params.as_list(), counters=True)
+        dt = time.perf_counter() - t
+        bad = 0
+        for f in MapResult.FIELDS:
+            g = batched_out[f]
+            g = np.concatenate([g[:n], g[n1:n1 + n]]) if paired else g[:n]
+            bad += int((g.view(o[f].dtype) != o[f]).sum())
+        nr = n * (2 if paired else 1)
+        ct = o["counters"]
+        line["parity_sample"] = {"reads": nr, "mismatched_fields": bad,
+                                 "oracle_capped_searches": int(ct["capped"]),
+                                 "oracle_fallback_seeds": int(ct["fallback"])}
+        line["cpu_baseline"] = {"value": round(nr / dt, 1), "unit": "reads/s", "cores": oracle.max_threads(),
+                                "kind": "port", "cpu": _cpu_model(),
+                                "sample": f"the parity sample ({nr} reads), {dt:.1f} s, index load {load_s:.1f} s"}
+        # the reference algorithm's bytes (64-B BWT lines per backward
+        # step, LF-walk lines, SA-sample and pac sectors, reads, outputs)
+        ref_bytes = (64 * (ct["occ_lines"] + ct["lf_lines"]) + 8 * ct["sa_loads"] + 32 * ct["pac_sectors"] +
+                     int(((l_.astype(np.int64) + 3) // 4).sum()) + 28 * nr)
+        seed_ref = 64 * (ct["occ_lines"] + ct["lf_lines"]) + 32 * ct["sa_loads"]
+        line["roofline"]["reference_algorithm_bytes_per_read"] = round(ref_bytes / nr, 1)
+        line["roofline"]["reference_seeding_bytes_per_read"] = round(seed_ref / nr, 1)
+        line["roofline"]["reference_algorithm_GBs"] = round(ref_bytes / nr * n_seq / (seed_avg_ms / 1000) / 1e9, 1)
+    bad = parity_failures(line)
+    line["parity_failures"] = bad
+    if rank == 0:
+        print(json.dumps(ordered_line(line)), flush=True)
+    gi.close()
+    ctx.close()
+    dist.close()
+    if bad:
+        sys.stderr.write("parity check failed: " + ", ".join(bad) + "\n")
+        sys.exit(3)
+
+
+def genome_forms(args, ctx, gi, params, fa, local, best, bases_np, lens_np, n, max_len, batched_out, batched_rate,
+                 stream):
+    """Plain single-launch, batched and served forms on the same single-end
+    reads (equal outputs), then the served stream of 8 samples."""
+    import torch
+    from mojoalign_b200 import MapResult, map_batch_device, synth
+    from mojoalign_b200.autotune import FIELDS as TFIELDS
+    from mojoalign_b200.serve import Server, percentiles
+
+    dev = f"cuda:{local}"
+    forms = {}
+    # plain single-launch (the reference's launch shape) on the first reads
+    # of the batch, one call, inputs resident
+    m = min(n, args.forms_reads)
+    d_b = torch.from_numpy(bases_np[:m]).to(dev).reshape(-1)
+    d_l = torch.from_numpy(lens_np[:m].view(np.int32)).to(dev)
+
+    def device_form(tuning, reps=2):
+        ctx.set_tuning(*tuning)
+        d_o = {f: torch.empty(m, dtype=torch.int32, device=dev) for f in MapResult.FIELDS}
+        ptrs = {f: x.data_ptr() for f, x in d_o.items()}
+
+        def go():
+            map_batch_device(ctx, gi, d_b.data_ptr(), d_l.data_ptr(), m, False, max_len, ptrs, "C2T", "", params,
+                             stream=stream.cuda_stream)
+        go()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            go()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return m / (e0.elapsed_time(e1) / reps / 1000.0), {f: x.cpu().numpy() for f, x in d_o.items()}
+
+    plain_rate, plain_out = device_form((0, 1, 0, 1, 16, 32, 32, 4, 0, 0))
+    wave_rate, wave_out = device_form(best)
+    same = all(np.array_equal(plain_out[f], batched_out[f][:m]) and np.array_equal(wave_out[f], plain_out[f])
+               for f in MapResult.FIELDS)
+    forms["reads"] = m
+    forms["plain_1launch"] = {"reads_per_s": round(plain_rate, 1), "tuning": "seed_kernel 0 (thread per read)",
+                              "timing": "device, inputs resident, one call"}
+    forms["wavefront_1call"] = {"reads_per_s": round(wave_rate, 1), "tuning": dict(zip(TFIELDS, best)),
+                                "timing": "device, inputs resident, one call", "equals_plain": bool(same)}
+    ctx.set_tuning(*best)
+    del d_b, d_l
+    torch.cuda.empty_cache()
+
+    # served: the same m reads as requests of log-uniform 1k-2M reads
+    rng = np.random.default_rng(7)
+    sizes = log_uniform_sizes(rng, 1 << 16, 1000, 2_000_000)
+    cuts, a = [], 0
+    for sz in sizes:
+        if a >= m:
+            break
+        cuts.append((a, int(min(sz, m - a))))
+        a += cuts[-1][1]
+    group = args.serve_group
+    with Server(ctx, gi, hbm_budget_bytes=args.serve_budget_gb << 30, max_group_pairs=group, max_inflight=3) as srv:
+        def stream_same():
+            t0 = time.perf_counter()
+            ts = [srv.submit(bases_np[a:a + c], lens_np[a:a + c], c, False, max_len, "C2T", "", params)
+                  for a, c in cuts]
+            srv.drain()
+            return ts, m / (time.perf_counter() - t0)
+
+        stream_same()
+        tickets, served_rate = stream_same()
+        served_same = all(np.array_equal(getattr(t_.result, f).view(np.uint32), plain_out[f][a:a + c].view(np.uint32))
+                          for t_, (a, c) in zip(tickets, cuts) for f in MapResult.FIELDS)
+        del tickets
+    forms["served"] = {"reads_per_s": round(served_rate, 1), "requests": len(cuts),
+                       "timing": "host, submit to last completion, copies included",
+                       "equals_plain": bool(served_same)}
+    forms["batched_all_reads"] = {"reads_per_s": round(batched_rate, 1),
+                                  "timing": "device, inputs resident, the headline step"}
+    forms["served_over_plain_1launch"] = round(served_rate / plain_rate, 3)
+    forms["served_over_wavefront_1call"] = round(served_rate / wave_rate, 3)
+    forms["batched_over_plain_1launch"] = round(batched_rate / plain_rate, 3)
+
+    # served stream: 8 samples, Poisson arrivals at half the burst rate, an
+    # HBM budget that admission has to wait on
+    pools = []
+    for k, (mdl, ml) in enumerate(serving_samples()):
+        pb = torch.empty((args.serve_pool, ml), dtype=torch.uint8, pin_memory=True)
+        r = synth.simulate_reads(fa, synth.ReadModel(**mdl), args.serve_pool, False, ml, seed=200 + k,
+                                 bases_out=pb.numpy())
+        pools.append((pb, pb.numpy(), r.lens, ml))
+
+    def request(k, size):
+        _, b, l, ml = pools[k]
+        size = int(min(size, args.serve_pool))
+        a = int(rng.integers(0, args.serve_pool - size + 1))
+        return b[a:a + size], l[a:a + size], size, ml
+
+    budget = args.serve_stream_budget_mb << 20
+    with Server(ctx, gi, hbm_budget_bytes=budget, max_group_pairs=group, max_inflight=3) as srv:
+        def burst(count):
+            reqs = [request(int(rng.integers(0, 8)), s) for s in log_uniform_sizes(rng, count, 1000, 2_000_000)]
+            t0 = time.perf_counter()
+            for b, l, c, ml in reqs:
+                srv.submit(b, l, c, False, ml, "C2T", "", params)
+            srv.drain()
+            return sum(r[2] for r in reqs) / (time.perf_counter() - t0)
+
+        burst(16)
+        sat = burst(args.serve_burst)
+        mean_size = (2_000_000 - 1000) / np.log(2_000_000 / 1000)
+        lam = 0.5 * sat / mean_size
+        _, _, before = srv.latencies()
+        n0 = before.size
+        t0 = time.perf_counter()
+        t_next = t0
+        sent = 0
+        while t_next - t0 < args.serve_seconds:
+            now = time.perf_counter()
+            if now < t_next:
+                time.sleep(t_next - now)
+            b, l, c, ml = request(int(rng.integers(0, 8)), log_uniform_sizes(rng, 1, 1000, 2_000_000)[0])
+            srv.submit(b, l, c, False, ml, "C2T", "", params)
+            sent += c
+            t_next += rng.exponential(1.0 / lam)
+        srv.drain()
+        wall = time.perf_counter() - t0
+        _, reads, lat = srv.latencies()
+        lat, reads = lat[n0:], reads[n0:]
+        st = srv.stats()
+    forms["serving"] = {
+        "samples": "8 (CpG retention 0.4-0.9; fixed 150 / lognormal 120 / lognormal 90 length profiles), pools of "
+                   f"{args.serve_pool} reads, request sizes log-uniform 1k-2M reads",
+        "burst_reads_per_s": round(sat, 1),
+        "poisson": {"offered_reads_per_s": round(0.5 * sat, 1), "achieved_reads_per_s": round(sent / wall, 1),
+                    "seconds": round(wall, 1), "requests": int(lat.size),
+                    "latency_ms": {k: (round(v, 2) if v is not None else None) for k, v in percentiles(lat).items()}},
+        "options": {"hbm_budget_bytes": budget, "max_group_pairs": group, "max_inflight": 3},
+        "stats": {k: st[k] for k in ("groups_issued", "parts_issued", "max_requests_in_group",
+                                     "max_groups_in_flight", "peak_bytes", "admission_waits")}}
+    del pools
+    return forms
+
+
 def _cpu_model() -> str:
     try:
         for ln in open("/proc/cpuinfo"):
@@ -1379,18 +1811,34 @@ REF_SAMPLE_PAIRS = 1_000_000  # pairs handed to the reference arm (its steps tim
 def prepare_sample(args, out: str) -> None:
     """Data preparation of the reference arm, run in a child process: the
     synthetic reference and its index (built by this package, on the GPU
-    when there is one), the workload's reads, and the first pairs of the
-    batch saved to `out` (R1 rows, R2 rows, lengths) with the index prefix."""
+    when there is one), the workload's reads, and the first reads of the
+    batch saved to `out` (R1 rows, R2 rows when paired, lengths) with the
+    index prefix."""
+    from mojoalign_b200 import synth
+
     class _Solo(Dist):
         def __init__(self):
             super().__init__(1, "gloo")
 
     _, _, local = dist_env()
-    fa, prefix, _ = prepare_reference(args, 0, _Solo(), local)
-    rb = simulate(args, fa, 0)
+    if args.workload == "chromosome":
+        fa, prefix, _ = prepare_reference(args, 0, _Solo(), local)
+        rb = simulate(args, fa, 0)
+        max_len = READ_LEN
+    else:
+        spec = GENOME_WORKLOADS[args.workload]
+        mb = args.genome_mb_large or spec["genome_mb"]
+        fa, prefix, _ = prepare_reference(args, 0, _Solo(), local, genome_mb=mb,
+                                          repeats=synth.RepeatModel() if spec["repeats"] else None,
+                                          tag="_repeats" if spec["repeats"] else "")
+        n1 = min(args.genome_reads or spec["n1"], REF_SAMPLE_PAIRS)
+        max_len = spec["max_len"]
+        rb = synth.simulate_reads(fa, synth.ReadModel(**spec["model"]), n1, spec["paired"], max_len, seed=1)
     n = min(rb.n1, REF_SAMPLE_PAIRS)
-    np.savez(out, r1=rb.bases[:n], r2=rb.bases[rb.n1:rb.n1 + n], l1=rb.lens[:n], l2=rb.lens[rb.n1:rb.n1 + n],
-             prefix=np.array(str(prefix)))
+    r2 = rb.bases[rb.n1:rb.n1 + n] if rb.paired else rb.bases[:0]
+    l2 = rb.lens[rb.n1:rb.n1 + n] if rb.paired else rb.lens[:0]
+    np.savez(out, r1=rb.bases[:n], r2=r2, l1=rb.lens[:n], l2=l2, prefix=np.array(str(prefix)),
+             paired=np.array(rb.paired), max_len=np.array(max_len))
 
 
 def run_reference(args, rank, world, local):
@@ -1403,41 +1851,50 @@ def run_reference(args, rank, world, local):
     with tempfile.TemporaryDirectory(prefix="mojoalign_ref_") as td:
         sample = Path(td) / "sample.npz"
         cmd = [sys.executable, str(Path(__file__).resolve()), "--prepare-sample", str(sample),
-               "--genome-mb", str(args.genome_mb), "--pairs", str(args.pairs), "--workdir", args.workdir]
+               "--genome-mb", str(args.genome_mb), "--pairs", str(args.pairs), "--workdir", args.workdir,
+               "--workload", args.workload, "--genome-mb-large", str(args.genome_mb_large),
+               "--genome-reads", str(args.genome_reads)]
         subprocess.run(cmd, check=True)
         z = np.load(sample)
         r1, r2, l1, l2, prefix = z["r1"], z["r2"], z["l1"], z["l2"], str(z["prefix"])
+        paired, max_len = bool(z["paired"]), int(z["max_len"])
     import oracle
 
     plist = list(BENCH_PARAM_VALUES.values())
     ix = oracle.OracleIndex(prefix)
+    per = 2 if paired else 1
+    bs2 = 2 if paired else 0
 
     def batch(n):
+        if not paired:
+            return r1[:n], l1[:n]
         return np.concatenate([r1[:n], r2[:n]]), np.concatenate([l1[:n], l2[:n]])
 
     # size one step to about cpu_seconds / (steps + warmup) * 2
     probe = min(10000, len(l1))
     b, l = batch(probe)
     t = time.perf_counter()
-    ix.map(b, l, probe, True, READ_LEN, 1, 2, plist)
-    rate = 2 * probe / (time.perf_counter() - t)
+    ix.map(b, l, probe, paired, max_len, 1, bs2, plist)
+    rate = per * probe / (time.perf_counter() - t)
     per_step_s = max(2.0, 60.0 / max(1, args.steps + args.warmup))
-    n = int(min(len(l1), max(probe, rate * per_step_s / 2)))
+    n = int(min(len(l1), max(probe, rate * per_step_s / per)))
     b, l = batch(n)
     for _ in range(args.warmup):
-        ix.map(b, l, n, True, READ_LEN, 1, 2, plist)
+        ix.map(b, l, n, paired, max_len, 1, bs2, plist)
     t = time.perf_counter()
     for _ in range(args.steps):
-        ix.map(b, l, n, True, READ_LEN, 1, 2, plist)
+        ix.map(b, l, n, paired, max_len, 1, bs2, plist)
     dt = (time.perf_counter() - t) / args.steps
-    value = 2 * n / dt
+    value = per * n / dt
+    config = workload_config(args) if args.workload == "chromosome" else genome_config(
+        args, GENOME_WORKLOADS[args.workload])
     line = {"metric": METRIC, "value": round(value, 1), "unit": "reads/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(dt * 1000, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic", "impl": "reference",
-            "config": workload_config(args),
+            "config": config,
             "cpu_baseline": {"value": round(value, 1), "unit": "reads/s", "cores": oracle.max_threads(),
                              "kind": "port", "cpu": _cpu_model(),
-                             "sample": f"first {n} pairs ({2 * n} reads) of the workload per step"},
+                             "sample": f"first {per * n} reads of the workload per step"},
             "e2e": {"value": round(value, 1), "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(ordered_line(line)), flush=True)
 
@@ -1468,8 +1925,10 @@ def main():
         print(json.dumps(gather_sweep(local)), flush=True)
     elif args.impl == "reference":
         run_reference(args, rank, world, local)
-    else:
+    elif args.workload == "chromosome":
         run_ours(args, rank, world, local)
+    else:
+        run_genome(args, rank, world, local)
 
 
 if __name__ == "__main__":

@@ -123,12 +123,22 @@ typedef struct ma_index_info {
  *             bytes (0 = none, 1..20; default 0).  k = seed_len replaces
  *             the first seed_len backward-search steps with one lookup.
  *   hbm_budget_bytes  admission budget (0 = all free HBM).
- * A table is used by a mapping call only when its k <= seed_len.
+ *   wide_rows 1: store SA rows as 40-bit values even when the text is
+ *             short enough for 32-bit rows (automatic from 2^32 - 1 rows).
+ *   occ_super_shift   log2 of the Occ superblock (7..31; 0 = 31): Occ
+ *             lines count symbols from the start of their superblock.
+ *   prep_chunk_rows   SA rows per preparation pass of the k-mer tables and
+ *             the seed summary (0 = 2^30; at least 512).
+ * A table is used by a mapping call only when its k <= seed_len.  Texts of
+ * up to 2^35 - 2 symbols (seq_len) are supported.
  */
 typedef struct ma_index_options {
     int32_t kmer_k;
     int32_t kmer3_k;
     uint64_t hbm_budget_bytes;
+    int32_t wide_rows;
+    int32_t occ_super_shift;
+    uint64_t prep_chunk_rows;
 } ma_index_options;
 void ma_index_options_default(ma_index_options* o);
 
@@ -153,10 +163,21 @@ int ma_hbm_info(ma_ctx* ctx, uint64_t* free_bytes, uint64_t* total_bytes);
  * indexes that, replacing `bwameth.py index` + `bwa index`
  * (fq2bam-meth/scripts/ensure_bwameth_index.sh:23-50).  sa_intv is the SA
  * sampling interval written to .sa (bwa default 32).  device_ordinal >= 0
- * sorts suffixes on that GPU; -1 sorts on the host.
+ * builds the BWT on that GPU (texts up to 2^35 - 2 symbols, e.g. the
+ * 12.4 G-symbol text of a 3.1 Gbp genome); -1 sorts on the host (texts
+ * below 2^32 symbols).
  */
 int ma_index_build(const char* fasta, const char* out_prefix, int bwameth_c2t,
                    int sa_intv, int device_ordinal);
+
+/*
+ * ma_index_build with the GPU construction's batch size: at most
+ * batch_suffixes suffixes are sorted at once (0 = what fits the device);
+ * the files do not depend on it.  No counterpart in the reference.
+ */
+int ma_index_build_batched(const char* fasta, const char* out_prefix,
+                           int bwameth_c2t, int sa_intv, int device_ordinal,
+                           uint64_t batch_suffixes);
 
 /*
  * Loads prefix.{bwt,sa,pac,ann} with the header checks of

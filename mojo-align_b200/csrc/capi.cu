@@ -372,12 +372,38 @@ int ma_index_build(const char* fasta, const char* out_prefix, int bwameth_c2t, i
     return guarded(nullptr, [&] { build_index(fasta, out_prefix, bwameth_c2t != 0, sa_intv, device_ordinal); });
 }
 
+int ma_index_build_batched(const char* fasta, const char* out_prefix, int bwameth_c2t, int sa_intv,
+                           int device_ordinal, uint64_t batch_suffixes) {
+    if (!fasta || !out_prefix) {
+        t_err = "null path";
+        return MA_ERR_ARG;
+    }
+    return guarded(nullptr, [&] {
+        build_index(fasta, out_prefix, bwameth_c2t != 0, sa_intv, device_ordinal, batch_suffixes);
+    });
+}
+
 void ma_index_options_default(ma_index_options* o) {
     if (!o) return;
     o->kmer_k = 12;
     o->kmer3_k = 0;
     o->hbm_budget_bytes = 0;
+    o->wide_rows = 0;
+    o->occ_super_shift = 0;
+    o->prep_chunk_rows = 0;
 }
+
+namespace {
+LayoutOptions layout_of(const ma_index_options& o) {
+    LayoutOptions lo;
+    lo.kmer_k = o.kmer_k;
+    lo.kmer3_k = o.kmer3_k;
+    lo.wide_rows = o.wide_rows != 0;
+    lo.occ_super_shift = o.occ_super_shift ? o.occ_super_shift : OCC_SUPER_SHIFT;
+    lo.prep_chunk_rows = o.prep_chunk_rows;
+    return lo;
+}
+}  // namespace
 
 int ma_index_probe(const char* prefix, int kmer_k, int kmer3_k, ma_index_info* out) {
     if (!prefix || !out) {
@@ -400,7 +426,10 @@ int ma_index_probe(const char* prefix, int kmer_k, int kmer3_k, ma_index_info* o
         I.sa_reject_below = p0;
         I.kmer_k = kmer_k;
         I.kmer3_k = kmer3_k;
-        I.device_bytes = device_index_bytes(h, kmer_k, kmer3_k) + device_index_staging_bytes(h, kmer3_k);
+        LayoutOptions lo;
+        lo.kmer_k = kmer_k;
+        lo.kmer3_k = kmer3_k;
+        I.device_bytes = device_index_bytes(h, lo) + device_index_staging_bytes(h, lo);
         *out = I;
     });
 }
@@ -415,18 +444,19 @@ int ma_index_open(ma_ctx* ctx, const char* prefix, const ma_index_options* opt, 
     int rc = guarded(ctx, [&] {
         use_device(ctx);
         BwaIndexHost h = load_bwa_index(prefix);
-        const uint64_t need = device_index_bytes(h, o.kmer_k, o.kmer3_k);
+        const LayoutOptions lo = layout_of(o);
+        const uint64_t need = device_index_bytes(h, lo);
         size_t f = 0, t = 0;
         ck(cudaMemGetInfo(&f, &t), "cudaMemGetInfo");
         // fail-closed admission like gpu_mem.require_index_capacity: the
         // resident index plus the preparation passes' staging must fit
-        const uint64_t staging = device_index_staging_bytes(h, o.kmer3_k);
+        const uint64_t staging = device_index_staging_bytes(h, lo);
         const uint64_t budget = o.hbm_budget_bytes ? std::min<uint64_t>(o.hbm_budget_bytes, f) : f;
         if (need + staging > budget)
             fail(MA_ERR_NOMEM, "index needs " + std::to_string((need + staging) >> 20) + " MiB of HBM, budget " +
                                    std::to_string(budget >> 20) + " MiB");
         uint64_t p0 = 0;
-        idx->dix = build_device_index(h, o.kmer_k, o.kmer3_k, ctx->stream, idx->bufs, &p0);
+        idx->dix = build_device_index(h, lo, ctx->stream, idx->bufs, &p0);
         idx->ctx = ctx;
         idx->contigs = h.contigs;
         ma_index_info& I = idx->info;

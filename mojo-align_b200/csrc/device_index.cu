@@ -4,16 +4,19 @@
 // on every lookup (linear_gpu_fm.mojo:2034-2069, 1390-1508).  Here the
 // upload is followed by one-time device passes that re-lay the index for
 // random 32-byte gathers:
-//   relayout_occ      bwa 64-B blocks of 128 positions -> 32-B lines of 64
+//   relayout_occ      bwa 64-B blocks of 128 positions -> 32-B lines of 64,
+//                     counts relative to the line's superblock
 //   relayout_pac      MSB-first pac bytes -> LSB-first u64 words, padded
 //   reconstruct_sa    sampled SA -> full SA, one LF chain per sampled row
 //   build_kmer        k-mer -> backward-search interval table
-//   kmer3_rows/bounds 3-letter k-mer tables from one pass over the full SA
+//   kmer3_*           3-letter k-mer tables from passes over the full SA
 //   lcp / summary     capped LCPs of adjacent SA rows -> per-position
 //                     shortest-unique lengths and k-mer counts
-// Every kernel's loops are bounded; a chain that runs past its bound (only
-// possible on an inconsistent index) raises a device error flag instead of
-// spinning.
+// The passes over all SA rows run in chunks of rows (with the few rows of
+// overlap each pass needs), so that their staging stays a few GB whatever
+// the text length.  Every kernel's loops are bounded; a chain that runs
+// past its bound (only possible on an inconsistent index) raises a device
+// error flag instead of spinning.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -42,6 +45,7 @@ __device__ __forceinline__ uint32_t count_sym32(uint32_t w_lsb, int c, int nbase
 }
 
 __global__ void relayout_occ_kernel(const uint32_t* __restrict__ bwa, uint64_t seq_len, uint64_t n_lines,
+                                    const unsigned long long* __restrict__ super, int super_shift,
                                     OccLine* __restrict__ out) {
     uint64_t L = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     if (L >= n_lines) return;
@@ -57,7 +61,8 @@ __global__ void relayout_occ_kernel(const uint32_t* __restrict__ bwa, uint64_t s
         }
     }
     OccLine o;
-    for (int c = 0; c < 4; ++c) o.cnt[c] = static_cast<uint32_t>(cnt[c]);
+    const unsigned long long* sb = super + (((L * 64) >> super_shift) << 2);
+    for (int c = 0; c < 4; ++c) o.cnt[c] = static_cast<uint32_t>(cnt[c] - sb[c]);
     for (int i = 0; i < 4; ++i) {
         uint64_t p0 = L * 64 + 16 * i;  // first position held by word i
         uint32_t w = 0;
@@ -88,13 +93,25 @@ __global__ void relayout_pac_kernel(const uint8_t* __restrict__ pac, uint64_t l_
     out[w] = v;
 }
 
+// Full-SA stores of either layout (index preparation only).  A 40-bit value
+// is written byte by byte, so rows sharing a 16-byte chunk never race.
+__device__ __forceinline__ void sa_put(const DevIndex& ix, uint32_t* sa, uint8_t* sa40, uint64_t row, uint64_t v) {
+    if (!ix.sa_wide) {
+        sa[row] = static_cast<uint32_t>(v);
+        return;
+    }
+    const uint64_t ch = row / 3;
+    uint8_t* p = sa40 + ch * 16 + (row - ch * 3) * 5;
+    for (int i = 0; i < 5; ++i) p[i] = static_cast<uint8_t>(v >> (8 * i));
+}
+
 // One chain per sampled row i (i % intv == 0, i <= seq_len): SA[i] is known
 // (row 0 is the sentinel suffix, SA[0] = seq_len).  LF steps from i visit
 // the rows of text positions SA[i]-1, SA[i]-2, ... until a sampled row or
 // text position 0; every row visited gets its SA value.
 __global__ void reconstruct_sa_kernel(DevIndex ix, const uint64_t* __restrict__ samples, uint64_t n_chains,
-                                      uint64_t intv, uint32_t* __restrict__ sa, uint64_t max_steps,
-                                      int* __restrict__ err) {
+                                      uint64_t intv, uint32_t* __restrict__ sa, uint8_t* __restrict__ sa40,
+                                      uint64_t max_steps, int* __restrict__ err) {
     uint64_t ci = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     if (ci >= n_chains) return;
     uint64_t r = ci * intv;
@@ -103,7 +120,7 @@ __global__ void reconstruct_sa_kernel(DevIndex ix, const uint64_t* __restrict__ 
         atomicExch(err, 1);
         return;
     }
-    sa[r] = static_cast<uint32_t>(s);
+    sa_put(ix, sa, sa40, r, s);
     for (uint64_t step = 0; step < max_steps; ++step) {
         if (s == 0) return;
         if (r == ix.primary) {  // position 0 reached through a bad sample
@@ -119,20 +136,26 @@ __global__ void reconstruct_sa_kernel(DevIndex ix, const uint64_t* __restrict__ 
             return;
         }
         if (r % intv == 0) return;
-        sa[r] = static_cast<uint32_t>(s);
+        sa_put(ix, sa, sa40, r, s);
     }
     atomicExch(err, 4);  // chain longer than any consistent index allows
 }
 
-__global__ void count_unset_kernel(const uint32_t* __restrict__ sa, uint64_t n, unsigned long long* cnt) {
+__global__ void count_unset_kernel(DevIndex ix, uint64_t n, unsigned long long* cnt) {
     uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint64_t unset = ix.sa_wide ? SA40_UNSET : 0xFFFFFFFFull;
     unsigned long long local = 0;
-    for (; i < n; i += stride) local += sa[i] == 0xFFFFFFFFu;
+    for (; i < n; i += stride) local += sa_at(ix, i) == unset;
     if (local) atomicAdd(cnt, local);
 }
 
-__global__ void build_kmer_kernel(DevIndex ix, int K, uint64_t n_kmers, uint2* __restrict__ out) {
+// Packed k-mer table entry of the interval [k, l] (count l - k + 1 >= 1).
+__device__ __forceinline__ uint64_t kmer_entry(uint64_t k, uint64_t count) {
+    return count > KMER_MAX_COUNT ? KMER_UNTABLED : (k | (count << KMER_K_BITS));
+}
+
+__global__ void build_kmer_kernel(DevIndex ix, int K, uint64_t n_kmers, uint64_t* __restrict__ out) {
     uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     if (idx >= n_kmers) return;
     uint64_t k = 0, l = ix.seq_len;
@@ -143,11 +166,11 @@ __global__ void build_kmer_kernel(DevIndex ix, int K, uint64_t n_kmers, uint2* _
         k = ix.L2[c] + ok + 1;
         l = ix.L2[c] + ol;
         if (k > l) {
-            out[idx] = make_uint2(1u, 0u);
+            out[idx] = 0;  // count 0: W does not occur
             return;
         }
     }
-    out[idx] = make_uint2(static_cast<uint32_t>(k), static_cast<uint32_t>(l));
+    out[idx] = kmer_entry(k, l - k + 1);
 }
 
 // 2-bit codes of text T[p, p+K) (T = the pac followed by its reverse
@@ -176,40 +199,53 @@ __device__ uint64_t text_kmer(const DevIndex& ix, uint64_t p, int K) {
     return v;
 }
 
-__global__ void kmer3_rows_kernel(DevIndex ix, int K, uint64_t n_rows, uint64_t* __restrict__ codes) {
+// K-mer codes of SA rows [row0, row0 + n) into codes[0, n).
+__global__ void kmer3_rows_kernel(DevIndex ix, int K, uint64_t row0, uint64_t n, uint64_t* __restrict__ codes) {
     const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-    if (i >= n_rows) return;
-    codes[i] = text_kmer(ix, ix.sa[i], K);
+    if (i >= n) return;
+    codes[i] = text_kmer(ix, sa_at(ix, row0 + i), K);
 }
 
-__global__ void fill_empty_kernel(uint2* __restrict__ t, uint64_t n) {
+__global__ void fill_u64_kernel(uint64_t* __restrict__ t, uint64_t n, uint64_t v) {
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n; i += stride)
-        t[i] = make_uint2(0xFFFFFFFFu, 0u);
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n; i += stride) t[i] = v;
+}
+
+// Base-3 index of a 3-letter k-mer code and the tables it belongs to.
+__device__ __forceinline__ uint32_t kmer3_index(uint64_t c, int K, bool& agt, bool& act) {
+    const uint64_t lo = c & kEven, hi = (c >> 1) & kEven;
+    agt = (lo & ~hi) == 0;  // no C
+    act = (hi & ~lo) == 0;  // no G
+    uint32_t idx = 0;
+    for (int j = K - 1; j >= 0; --j) idx = idx * 3 + static_cast<uint32_t>(__popcll((c >> (2 * j)) & 3));
+    return idx;
 }
 
 // Rows with the same k-mer are contiguous in SA order; the first and last
-// row of each run are the interval (k, l) of that k-mer.
-__global__ void kmer3_bounds_kernel(const uint64_t* __restrict__ codes, uint64_t n_rows, int K,
-                                    uint2* __restrict__ t_agt, uint2* __restrict__ t_act) {
-    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-    if (i >= n_rows) return;
-    const uint64_t c = codes[i];
+// row of each run are the interval (k, l) of that k-mer.  One chunk of rows
+// [a, b): codes[j] is the code of row a - 1 + j (one row of overlap on each
+// side, ~0 outside [0, n_rows)).  pass 0 records the first row of every
+// run starting in the chunk; pass 1 turns the entry of every run ending in
+// the chunk into its packed interval (its first row was recorded by pass 0
+// of this chunk or of an earlier one).
+__global__ void kmer3_bounds_kernel(const uint64_t* __restrict__ codes, uint64_t a, uint64_t n, int K, int pass,
+                                    uint64_t* __restrict__ t_agt, uint64_t* __restrict__ t_act) {
+    const uint64_t j = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (j >= n) return;
+    const uint64_t c = codes[j + 1];
     if (c == ~0ull) return;
-    const bool start = i == 0 || codes[i - 1] != c;
-    const bool end = i + 1 == n_rows || codes[i + 1] != c;
-    if (!start && !end) return;
-    const uint64_t lo = c & kEven, hi = (c >> 1) & kEven;
-    const bool has_c = (lo & ~hi) != 0, has_g = (hi & ~lo) != 0;
-    uint32_t idx = 0;
-    for (int j = K - 1; j >= 0; --j) idx = idx * 3 + static_cast<uint32_t>(__popcll((c >> (2 * j)) & 3));
-    if (!has_c) {
-        if (start) t_agt[idx].x = static_cast<uint32_t>(i);
-        if (end) t_agt[idx].y = static_cast<uint32_t>(i);
-    }
-    if (!has_g) {
-        if (start) t_act[idx].x = static_cast<uint32_t>(i);
-        if (end) t_act[idx].y = static_cast<uint32_t>(i);
+    bool agt, act;
+    if (pass == 0) {
+        if (codes[j] == c) return;
+        const uint32_t idx = kmer3_index(c, K, agt, act);
+        if (agt) t_agt[idx] = a + j;
+        if (act) t_act[idx] = a + j;
+    } else {
+        if (codes[j + 2] == c) return;
+        const uint32_t idx = kmer3_index(c, K, agt, act);
+        const uint64_t row = a + j;
+        if (agt) t_agt[idx] = kmer_entry(t_agt[idx], row - t_agt[idx] + 1);
+        if (act) t_act[idx] = kmer_entry(t_act[idx], row - t_act[idx] + 1);
     }
 }
 
@@ -238,17 +274,19 @@ __device__ uint64_t text_window32(const DevIndex& ix, uint64_t p) {
 
 constexpr int LCP_CAP = 255;
 
-// lcp[i] = min(common prefix of the suffixes of rows i-1 and i, 255).
-__global__ void lcp_kernel(DevIndex ix, uint64_t n_rows, uint8_t* __restrict__ lcp) {
-    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-    if (i >= n_rows) return;
+// lcp[j] = min(common prefix of the suffixes of rows i-1 and i, 255) for
+// rows i = row0 + j, j < n (row 0: 0).
+__global__ void lcp_kernel(DevIndex ix, uint64_t row0, uint64_t n, uint8_t* __restrict__ lcp) {
+    const uint64_t j = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (j >= n) return;
+    const uint64_t i = row0 + j;
     if (i == 0) {
-        lcp[0] = 0;
+        lcp[j] = 0;
         return;
     }
-    const uint64_t n = ix.seq_len;
-    const uint64_t a = ix.sa[i - 1], b = ix.sa[i];
-    uint64_t maxl = n - (a > b ? a : b);  // the shorter suffix
+    const uint64_t len = ix.seq_len;
+    const uint64_t a = sa_at(ix, i - 1), b = sa_at(ix, i);
+    uint64_t maxl = len - (a > b ? a : b);  // the shorter suffix
     if (maxl > LCP_CAP) maxl = LCP_CAP;
     uint64_t l = 0;
     while (l < maxl) {
@@ -260,26 +298,30 @@ __global__ void lcp_kernel(DevIndex ix, uint64_t n_rows, uint8_t* __restrict__ l
         }
         l += 32;
     }
-    lcp[i] = static_cast<uint8_t>(l < maxl ? l : maxl);
+    lcp[j] = static_cast<uint8_t>(l < maxl ? l : maxl);
 }
 
 // Row i holds the suffix starting at y = SA[i]; its shortest unique prefix
 // is 1 + max(lcp[i], lcp[i+1]) and its K-mer occurs as often as the run of
-// adjacent rows with lcp >= K around i.  Stored at x = 2L-1-y.
-__global__ void summary_kernel(DevIndex ix, uint64_t n_rows, int K, const uint8_t* __restrict__ lcp,
+// adjacent rows with lcp >= K around i.  Stored at x = 2L-1-y.  Rows
+// [a, b) of one chunk; lcp[j] holds the LCP of row l0 + j for rows
+// [l0, l1), which covers [a - 255, b + 256) within [0, n_rows).
+__global__ void summary_kernel(DevIndex ix, uint64_t n_rows, int K, uint64_t a, uint64_t b,
+                               const uint8_t* __restrict__ lcp, uint64_t l0, uint64_t l1,
                                uint16_t* __restrict__ summary) {
-    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-    if (i == 0 || i >= n_rows) return;  // row 0 is the sentinel suffix
+    const uint64_t i = a + blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (i == 0 || i >= b) return;  // row 0 is the sentinel suffix
     const uint64_t n = ix.seq_len;
-    const uint64_t y = ix.sa[i];
-    const int l1 = lcp[i], l2 = i + 1 < n_rows ? lcp[i + 1] : 0;
-    const uint64_t m = 1 + static_cast<uint64_t>(l1 > l2 ? l1 : l2);
+    const uint64_t y = sa_at(ix, i);
+    const uint8_t* L = lcp - l0;  // L[r] = LCP of row r, r in [l0, l1)
+    const int l1v = L[i], l2v = i + 1 < n_rows ? L[i + 1] : 0;
+    const uint64_t m = 1 + static_cast<uint64_t>(l1v > l2v ? l1v : l2v);
     const uint32_t mul = (m < LCP_CAP && y + m <= n) ? static_cast<uint32_t>(m) : 255u;
     uint32_t occ = 255;
     if (y + K <= n) {
         occ = 1;
-        for (uint64_t j = i; j >= 1 && lcp[j] >= K && occ < 255; --j) ++occ;
-        for (uint64_t j = i + 1; j < n_rows && lcp[j] >= K && occ < 255; ++j) ++occ;
+        for (uint64_t j = i; j >= 1 && j > l0 && L[j] >= K && occ < 255; --j) ++occ;
+        for (uint64_t j = i + 1; j < n_rows && j < l1 && L[j] >= K && occ < 255; ++j) ++occ;
     }
     summary[n - 1 - y] = static_cast<uint16_t>(mul | (occ << 8));
 }
@@ -301,34 +343,66 @@ uint64_t pow3(int k) {
     return v;
 }
 
-uint64_t device_index_bytes(const BwaIndexHost& h, int kmer_k, int kmer3_k) {
+namespace {
+
+bool wide_rows(const BwaIndexHost& h, const LayoutOptions& lo) {
+    return lo.wide_rows || h.seq_len + 1 >= 0xFFFFFFFFull;
+}
+
+uint64_t n_super(const BwaIndexHost& h, const LayoutOptions& lo) {
+    return ((h.seq_len ? h.seq_len - 1 : 0) >> lo.occ_super_shift) + 1;
+}
+
+uint64_t sa_bytes(const BwaIndexHost& h, const LayoutOptions& lo) {
+    const uint64_t rows = h.seq_len + 1;
+    return wide_rows(h, lo) ? ((rows + 2) / 3) * 16 : rows * 4;
+}
+
+// Rows per preparation pass over the SA.
+uint64_t chunk_rows(const BwaIndexHost& h, const LayoutOptions& lo) {
+    const uint64_t rows = h.seq_len + 1;
+    uint64_t c = lo.prep_chunk_rows ? lo.prep_chunk_rows : (1ull << 30);
+    if (c < 512) c = 512;
+    return c < rows ? c : rows;
+}
+
+constexpr uint64_t LCP_HALO = 256;  // rows of LCP a summary row may look at on each side
+
+}  // namespace
+
+uint64_t device_index_bytes(const BwaIndexHost& h, const LayoutOptions& lo) {
     uint64_t n_lines = (h.seq_len + 63) / 64;
-    uint64_t b = n_lines * sizeof(OccLine);
-    b += (h.seq_len + 1) * 4;
+    uint64_t b = n_lines * sizeof(OccLine) + n_super(h, lo) * 32;
+    b += sa_bytes(h, lo);
     b += ((h.l_pac + 31) / 32 + 2 * PAC_PAD) * 8;
-    if (kmer_k > 0) b += (1ull << (2 * kmer_k)) * 8;
-    if (kmer3_k > 0) b += 2 * pow3(kmer3_k) * 8 + h.seq_len * 2;
+    if (lo.kmer_k > 0) b += (1ull << (2 * lo.kmer_k)) * 8;
+    if (lo.kmer3_k > 0) b += 2 * pow3(lo.kmer3_k) * 8 + h.seq_len * 2;
     b += h.contigs.size() * 12;
     return b;
 }
 
-// Temporary device memory of the preparation passes.
-uint64_t device_index_staging_bytes(const BwaIndexHost& h, int kmer3_k) {
-    uint64_t b = h.bwt.size() * 4 + h.pac.size() + h.sa.size() * 8;
-    if (kmer3_k > 0) b = std::max<uint64_t>(b, (h.seq_len + 1) * 8);
+// Temporary device memory of the preparation passes: the uploaded bwa
+// files, then (after they are freed) one chunk of k-mer codes or LCPs.
+uint64_t device_index_staging_bytes(const BwaIndexHost& h, const LayoutOptions& lo) {
+    uint64_t b = h.bwt.size() * 4 + h.pac.size() + 8 + (h.sa.size() + 1) * 8;
+    if (lo.kmer3_k > 0) b = std::max<uint64_t>(b, (chunk_rows(h, lo) + 2) * 8);
     return b;
 }
 
 // Builds the resident index on the current device; returns its DevIndex and
 // fills `bufs`.  Temporary upload buffers are freed before returning.
-DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, int kmer3_k, cudaStream_t st,
+DevIndex build_device_index(const BwaIndexHost& h, const LayoutOptions& lo, cudaStream_t st,
                             DeviceIndexBuffers& bufs, uint64_t* reject_below) {
-    if (h.seq_len + 1 >= 0xFFFFFFFFull)
-        fail(MA_ERR_UNSUPPORTED, "resident layout stores SA rows as u32; texts of 2^32 symbols or more are not supported yet");
-    if (kmer_k < 0 || kmer_k > 14) fail(MA_ERR_ARG, "kmer_k must be in 0..14");
-    if (kmer3_k < 0 || kmer3_k > 20) fail(MA_ERR_ARG, "kmer3_k must be in 0..20");
+    if (h.seq_len > MAX_SEQ_LEN)
+        fail(MA_ERR_UNSUPPORTED, "resident layout holds texts of at most 2^35 - 2 symbols");
+    if (lo.kmer_k < 0 || lo.kmer_k > 14) fail(MA_ERR_ARG, "kmer_k must be in 0..14");
+    if (lo.kmer3_k < 0 || lo.kmer3_k > 20) fail(MA_ERR_ARG, "kmer3_k must be in 0..20");
+    if (lo.occ_super_shift < 7 || lo.occ_super_shift > 31) fail(MA_ERR_ARG, "occ superblock shift must be in 7..31");
+    const int kmer_k = lo.kmer_k, kmer3_k = lo.kmer3_k;
     const uint64_t n_lines = (h.seq_len + 63) / 64;
     const uint64_t n_pacw = (h.l_pac + 31) / 32 + 2 * PAC_PAD;
+    const uint64_t n_rows = h.seq_len + 1;
+    const bool wide = wide_rows(h, lo);
     DevIndex ix{};
     ix.seq_len = h.seq_len;
     ix.l_pac = h.l_pac;
@@ -337,22 +411,47 @@ DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, int kmer3_k, cuda
     ix.n_contigs = static_cast<int64_t>(h.contigs.size());
     ix.kmer_k = kmer_k;
     ix.kmer3_k = 0;  // set once the tables are built
+    ix.occ_super_shift = lo.occ_super_shift;
+    ix.sa_wide = wide ? 1 : 0;
+
+    // symbols before each superblock, from the bwa block counts (a
+    // superblock starts on a 128-position block boundary)
+    const uint64_t ns = n_super(h, lo);
+    std::vector<unsigned long long> super(ns * 4, 0);
+    for (uint64_t sb = 0; sb < ns; ++sb) {
+        const uint64_t blk = (sb << lo.occ_super_shift) >> 7;
+        for (int c = 0; c < 4; ++c) {
+            const uint64_t w = blk * 16 + 2 * static_cast<uint64_t>(c);
+            if (w + 1 >= h.bwt.size()) fail(MA_ERR_FORMAT, "FmIndex .bwt shorter than seq_len implies");
+            super[sb * 4 + c] = static_cast<uint64_t>(h.bwt[w]) | (static_cast<uint64_t>(h.bwt[w + 1]) << 32);
+        }
+    }
 
     uint32_t* d_bwa = nullptr;
     uint8_t* d_pac = nullptr;
     uint64_t* d_samples = nullptr;
     int* d_err = nullptr;
     unsigned long long* d_cnt = nullptr;
-    auto cleanup = [&]() {
+    uint64_t* d_codes = nullptr;
+    auto free_uploads = [&]() {
         cudaFree(d_bwa);
         cudaFree(d_pac);
         cudaFree(d_samples);
+        d_bwa = nullptr;
+        d_pac = nullptr;
+        d_samples = nullptr;
+    };
+    auto cleanup = [&]() {
+        free_uploads();
         cudaFree(d_err);
         cudaFree(d_cnt);
+        cudaFree(d_codes);
     };
     try {
         check(cudaMalloc(&bufs.occ, n_lines * sizeof(OccLine)), "cudaMalloc occ");
-        check(cudaMalloc(&bufs.sa, (h.seq_len + 1) * 4), "cudaMalloc sa");
+        check(cudaMalloc(&bufs.occ_super, ns * 32), "cudaMalloc occ superblocks");
+        if (wide) check(cudaMalloc(&bufs.sa40, sa_bytes(h, lo)), "cudaMalloc sa");
+        else check(cudaMalloc(&bufs.sa, sa_bytes(h, lo)), "cudaMalloc sa");
         check(cudaMalloc(&bufs.pacw, n_pacw * 8), "cudaMalloc pac");
         check(cudaMalloc(&bufs.coff, (h.contigs.size() + 1) * 8), "cudaMalloc contig_off");
         check(cudaMalloc(&bufs.clen, (h.contigs.size() + 1) * 4), "cudaMalloc contig_len");
@@ -364,6 +463,7 @@ DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, int kmer3_k, cuda
         check(cudaMalloc(&d_cnt, sizeof(unsigned long long)), "cudaMalloc cnt");
         check(cudaMemsetAsync(d_err, 0, sizeof(int), st), "memset");
         check(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), st), "memset");
+        check(cudaMemcpyAsync(bufs.occ_super, super.data(), ns * 32, cudaMemcpyHostToDevice, st), "H2D superblocks");
         check(cudaMemcpyAsync(d_bwa, h.bwt.data(), h.bwt.size() * 4, cudaMemcpyHostToDevice, st), "H2D bwt");
         check(cudaMemsetAsync(d_pac, 0, h.pac.size() + 8, st), "memset");
         check(cudaMemcpyAsync(d_pac, h.pac.data(), h.pac.size(), cudaMemcpyHostToDevice, st), "H2D pac");
@@ -379,22 +479,27 @@ DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, int kmer3_k, cuda
             check(cudaMemcpyAsync(bufs.coff, coff.data(), coff.size() * 8, cudaMemcpyHostToDevice, st), "H2D coff");
             check(cudaMemcpyAsync(bufs.clen, clen.data(), clen.size() * 4, cudaMemcpyHostToDevice, st), "H2D clen");
         }
-        relayout_occ_kernel<<<grid_for(n_lines, 256), 256, 0, st>>>(d_bwa, h.seq_len, n_lines, bufs.occ);
+        relayout_occ_kernel<<<grid_for(n_lines, 256), 256, 0, st>>>(d_bwa, h.seq_len, n_lines, bufs.occ_super,
+                                                                     lo.occ_super_shift, bufs.occ);
         relayout_pac_kernel<<<grid_for(n_pacw, 256), 256, 0, st>>>(d_pac, h.l_pac, n_pacw, bufs.pacw);
         check(cudaGetLastError(), "relayout launch");
         ix.occ = bufs.occ;
+        ix.occ_super = bufs.occ_super;
         ix.pacw = bufs.pacw;
         ix.coff = bufs.coff;
         ix.clen = bufs.clen;
+        ix.sa = bufs.sa;
+        ix.sa40 = bufs.sa40;
         // full SA from the samples
-        check(cudaMemsetAsync(bufs.sa, 0xFF, (h.seq_len + 1) * 4, st), "memset sa");
+        check(cudaMemsetAsync(wide ? static_cast<void*>(bufs.sa40) : static_cast<void*>(bufs.sa), 0xFF,
+                              sa_bytes(h, lo), st), "memset sa");
         const uint64_t intv = static_cast<uint64_t>(h.sa_intv);
         const uint64_t n_chains = h.seq_len / intv + 1;  // rows 0, intv, ..., <= seq_len
         if (h.sa.size() + 1 < n_chains) fail(MA_ERR_FORMAT, "FmIndex .sa holds fewer samples than seq_len implies");
-        reconstruct_sa_kernel<<<grid_for(n_chains, 128), 128, 0, st>>>(ix, d_samples, n_chains, intv, bufs.sa,
-                                                                       1ull << 20, d_err);
+        reconstruct_sa_kernel<<<grid_for(n_chains, 128), 128, 0, st>>>(
+            ix, d_samples, n_chains, intv, bufs.sa, reinterpret_cast<uint8_t*>(bufs.sa40), 1ull << 20, d_err);
         check(cudaGetLastError(), "reconstruct_sa launch");
-        count_unset_kernel<<<1184, 256, 0, st>>>(bufs.sa, h.seq_len + 1, d_cnt);
+        count_unset_kernel<<<1184, 256, 0, st>>>(ix, n_rows, d_cnt);
         int herr = 0;
         unsigned long long hcnt = 0;
         check(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H err");
@@ -402,7 +507,7 @@ DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, int kmer3_k, cuda
         check(cudaStreamSynchronize(st), "index preparation");
         if (herr) fail(MA_ERR_FORMAT, "FmIndex BWT and SA samples are inconsistent (code " + std::to_string(herr) + ")");
         if (hcnt) fail(MA_ERR_FORMAT, "FmIndex SA reconstruction left " + std::to_string(hcnt) + " rows unset");
-        ix.sa = bufs.sa;
+        free_uploads();
         // rejection bound of the reference's sampled walk: the smallest text
         // position whose BWT row is sampled (rows >= intv; row 0 is the
         // sentinel suffix and is never reached by a walk)
@@ -417,26 +522,41 @@ DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, int kmer3_k, cuda
             ix.kmer = bufs.kmer;
         }
         if (kmer3_k > 0) {
-            const uint64_t n3 = pow3(kmer3_k), n_rows = h.seq_len + 1;
+            const uint64_t n3 = pow3(kmer3_k);
+            const uint64_t C = chunk_rows(h, lo);
             check(cudaMalloc(&bufs.kmer3[0], n3 * 8), "cudaMalloc kmer3");
             check(cudaMalloc(&bufs.kmer3[1], n3 * 8), "cudaMalloc kmer3");
             check(cudaMalloc(&bufs.summary, h.seq_len * 2), "cudaMalloc summary");
-            uint64_t* d_codes = nullptr;
-            check(cudaMalloc(&d_codes, n_rows * 8), "cudaMalloc kmer3 staging");
-            fill_empty_kernel<<<4096, 256, 0, st>>>(bufs.kmer3[0], n3);
-            fill_empty_kernel<<<4096, 256, 0, st>>>(bufs.kmer3[1], n3);
-            kmer3_rows_kernel<<<grid_for(n_rows, 256), 256, 0, st>>>(ix, kmer3_k, n_rows, d_codes);
-            kmer3_bounds_kernel<<<grid_for(n_rows, 256), 256, 0, st>>>(d_codes, n_rows, kmer3_k, bufs.kmer3[0],
-                                                                       bufs.kmer3[1]);
-            // the codes buffer (8 B per row) is reused for the u8 LCPs
+            check(cudaMalloc(&d_codes, (C + 2) * 8), "cudaMalloc kmer3 staging");
+            fill_u64_kernel<<<4096, 256, 0, st>>>(bufs.kmer3[0], n3, 0);
+            fill_u64_kernel<<<4096, 256, 0, st>>>(bufs.kmer3[1], n3, 0);
+            // tables: codes of rows [a - 1, b + 1) per chunk
+            for (uint64_t a = 0; a < n_rows; a += C) {
+                const uint64_t b = std::min(n_rows, a + C);
+                const uint64_t r0 = a ? a - 1 : 0, r1 = std::min(n_rows, b + 1);
+                if (!a) fill_u64_kernel<<<1, 32, 0, st>>>(d_codes, 1, ~0ull);
+                if (r1 == b) fill_u64_kernel<<<1, 32, 0, st>>>(d_codes + (b - a + 1), 1, ~0ull);
+                kmer3_rows_kernel<<<grid_for(r1 - r0, 256), 256, 0, st>>>(ix, kmer3_k, r0, r1 - r0,
+                                                                          d_codes + (a ? 0 : 1));
+                for (int pass = 0; pass < 2; ++pass)
+                    kmer3_bounds_kernel<<<grid_for(b - a, 256), 256, 0, st>>>(d_codes, a, b - a, kmer3_k, pass,
+                                                                              bufs.kmer3[0], bufs.kmer3[1]);
+                check(cudaGetLastError(), "kmer3 launch");
+            }
+            // summary: LCPs of rows [a - 256, b + 256) per chunk (the codes
+            // buffer, 8 B per row, holds them as bytes)
             uint8_t* d_lcp = reinterpret_cast<uint8_t*>(d_codes);
-            lcp_kernel<<<grid_for(n_rows, 256), 256, 0, st>>>(ix, n_rows, d_lcp);
-            summary_kernel<<<grid_for(n_rows, 256), 256, 0, st>>>(ix, n_rows, kmer3_k, d_lcp, bufs.summary);
-            cudaError_t le = cudaGetLastError();
-            cudaError_t se = cudaStreamSynchronize(st);
+            for (uint64_t a = 0; a < n_rows; a += C) {
+                const uint64_t b = std::min(n_rows, a + C);
+                const uint64_t l0 = a > LCP_HALO ? a - LCP_HALO : 0, l1 = std::min(n_rows, b + LCP_HALO);
+                lcp_kernel<<<grid_for(l1 - l0, 256), 256, 0, st>>>(ix, l0, l1 - l0, d_lcp);
+                summary_kernel<<<grid_for(b - a, 256), 256, 0, st>>>(ix, n_rows, kmer3_k, a, b, d_lcp, l0, l1,
+                                                                     bufs.summary);
+                check(cudaGetLastError(), "summary launch");
+            }
+            check(cudaStreamSynchronize(st), "kmer3 tables");
             cudaFree(d_codes);
-            check(le, "kmer3 launch");
-            check(se, "kmer3 tables");
+            d_codes = nullptr;
             ix.kmer3[0] = bufs.kmer3[0];
             ix.kmer3[1] = bufs.kmer3[1];
             ix.summary = bufs.summary;
@@ -448,13 +568,15 @@ DevIndex build_device_index(const BwaIndexHost& h, int kmer_k, int kmer3_k, cuda
         throw;
     }
     cleanup();
-    bufs.bytes = device_index_bytes(h, kmer_k, kmer3_k);
+    bufs.bytes = device_index_bytes(h, lo);
     return ix;
 }
 
 void free_device_index(DeviceIndexBuffers& b) {
     cudaFree(b.occ);
+    cudaFree(b.occ_super);
     cudaFree(b.sa);
+    cudaFree(b.sa40);
     cudaFree(b.pacw);
     cudaFree(b.kmer);
     cudaFree(b.kmer3[0]);

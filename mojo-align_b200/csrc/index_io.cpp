@@ -18,6 +18,7 @@
 // (seq_len = 2*l_pac), with the sentinel removed from the stored string at
 // row `primary`.
 #include <algorithm>
+#include <array>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -210,8 +211,25 @@ void write_fasta(const std::string& path, const std::vector<FastaRecord>& recs) 
 
 }  // namespace
 
+namespace {
+
+// Runs f(t, nt) on nt host threads.
+template <typename F>
+void parallel(F f) {
+    const unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nt; ++t) pool.emplace_back(f, t, nt);
+    for (auto& th : pool) th.join();
+}
+
+void put_u64_bytes(std::vector<uint8_t>& out, size_t at, uint64_t v) {
+    for (int b = 0; b < 8; ++b) out[at + b] = static_cast<uint8_t>(v >> (8 * b));
+}
+
+}  // namespace
+
 void build_index(const std::string& fasta, const std::string& out_prefix, bool bwameth_c2t, int sa_intv,
-                 int device) {
+                 int device, uint64_t batch_limit) {
     if (sa_intv <= 0 || (sa_intv & (sa_intv - 1)) != 0) fail(MA_ERR_ARG, "sa_intv must be a power of two");
     std::vector<FastaRecord> recs = read_fasta(fasta);
     if (bwameth_c2t) {
@@ -222,22 +240,49 @@ void build_index(const std::string& fasta, const std::string& out_prefix, bool b
     uint64_t l_pac = 0;
     for (const auto& r : recs) l_pac += r.seq.size();
     if (l_pac == 0) fail(MA_ERR_FORMAT, "FASTA has no bases");
-    if (2 * l_pac + 1 >= 0xFFFFFFFFull)
-        fail(MA_ERR_UNSUPPORTED, "index builder handles texts below 2^32 symbols");
-    std::vector<uint8_t> text(2 * l_pac);
+    const uint64_t n = 2 * l_pac;
+    if (device < 0 && n + 1 >= 0xFFFFFFFFull)
+        fail(MA_ERR_UNSUPPORTED, "the CPU index builder handles texts below 2^32 symbols; give a GPU");
+    if (n > (1ull << 35) - 2) fail(MA_ERR_UNSUPPORTED, "index builder handles texts below 2^35 symbols");
+    // forward text, one code per byte (codes of ambiguous bases drawn in
+    // order from one seeded generator, as before)
+    std::vector<uint8_t> fwd(l_pac);
     std::vector<Contig> contigs;
     std::vector<Hole> holes;
+    std::vector<uint64_t> rec_off;
+    {
+        uint64_t pos = 0;
+        for (const auto& r : recs) {
+            rec_off.push_back(pos);
+            pos += r.seq.size();
+        }
+    }
+    std::vector<uint8_t> any_amb(recs.size(), 0);
+    parallel([&](unsigned t, unsigned nt) {
+        for (size_t ri = t; ri < recs.size(); ri += nt) {
+            const std::string& q = recs[ri].seq;
+            uint8_t* o = fwd.data() + rec_off[ri];
+            uint8_t amb = 0;
+            for (size_t i = 0; i < q.size(); ++i) {
+                const int v = nt4(q[i]);
+                o[i] = static_cast<uint8_t>(v);
+                amb |= v > 3;
+            }
+            any_amb[ri] = amb;
+        }
+    });
     std::mt19937_64 rng(11);
-    uint64_t pos = 0;
-    for (const auto& r : recs) {
+    for (size_t ri = 0; ri < recs.size(); ++ri) {
+        const auto& r = recs[ri];
         Contig c;
         c.name = r.name;
         c.anno = r.anno;
-        c.offset = pos;
+        c.offset = rec_off[ri];
         c.len = static_cast<uint32_t>(r.seq.size());
-        for (size_t i = 0; i < r.seq.size(); ++i) {
-            int v = nt4(r.seq[i]);
-            if (v > 3) {
+        if (any_amb[ri]) {
+            for (size_t i = 0; i < r.seq.size(); ++i) {
+                const uint64_t pos = rec_off[ri] + i;
+                if (fwd[pos] <= 3) continue;
                 if (!holes.empty() && holes.back().offset + holes.back().len == pos &&
                     holes.back().amb == std::toupper(r.seq[i])) {
                     holes.back().len++;
@@ -245,48 +290,69 @@ void build_index(const std::string& fasta, const std::string& out_prefix, bool b
                     holes.push_back(Hole{pos, 1, static_cast<char>(std::toupper(static_cast<unsigned char>(r.seq[i])))});
                     c.n_ambs++;
                 }
-                v = static_cast<int>(rng() & 3);
+                fwd[pos] = static_cast<uint8_t>(rng() & 3);
             }
-            text[pos++] = static_cast<uint8_t>(v);
         }
         contigs.push_back(std::move(c));
     }
-    for (uint64_t i = 0; i < l_pac; ++i) text[2 * l_pac - 1 - i] = static_cast<uint8_t>(3 - text[i]);
-    const uint64_t n = 2 * l_pac;
-
-    // ---- suffix array, BWT ----
-    std::vector<uint32_t> sa = device >= 0 ? suffix_array_gpu(text.data(), n, device)
-                                           : suffix_array_cpu(text.data(), n);
-    if (sa.size() != n + 1 || sa[0] != n) fail(MA_ERR_INTERNAL, "suffix array construction failed");
-    uint64_t primary = 0;
+    std::vector<FastaRecord>().swap(recs);
     uint64_t L2[5] = {0, 0, 0, 0, 0};
-    for (uint64_t i = 0; i < n; ++i) L2[text[i] + 1]++;
-    for (int c = 1; c <= 4; ++c) L2[c] += L2[c - 1];
-    // BWT symbol of every row (4 = the sentinel row), gathered in parallel
-    std::vector<uint8_t> bsym(n + 1);
     {
-        const unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-        std::vector<std::thread> pool;
-        for (unsigned t = 0; t < nt; ++t)
-            pool.emplace_back([&, t] {
-                const uint64_t r0 = (n + 1) * t / nt, r1 = (n + 1) * (t + 1) / nt;
-                for (uint64_t row = r0; row < r1; ++row) bsym[row] = sa[row] ? text[sa[row] - 1] : 4;
-            });
-        for (auto& th : pool) th.join();
+        std::vector<std::array<uint64_t, 4>> part(64, {0, 0, 0, 0});
+        parallel([&](unsigned t, unsigned nt) {
+            const uint64_t a = l_pac * t / nt, b = l_pac * (t + 1) / nt;
+            for (uint64_t i = a; i < b; ++i) part[t][fwd[i]]++;
+        });
+        uint64_t cf[4] = {0, 0, 0, 0};
+        for (auto& pc : part)
+            for (int c = 0; c < 4; ++c) cf[c] += pc[c];
+        // the reverse complement holds each symbol's complement once more
+        for (int c = 0; c < 4; ++c) L2[c + 1] = cf[c] + cf[3 - c];
+        for (int c = 1; c <= 4; ++c) L2[c] += L2[c - 1];
     }
-    // stored BWT: rows 0..n without the sentinel row
-    const uint64_t n_occ = (n + 127) / 128 + 1;
-    std::vector<uint32_t> bwt((n + 15) / 16 + 8 * n_occ, 0);
-    {
+
+    uint64_t primary = 0;
+    std::vector<uint32_t> bwt;
+    std::vector<uint64_t> samples;
+    if (device >= 0) {
+        // T = pac + reverse complement, 32 symbols per word, LSB first
+        const uint64_t n_words = n / 32 + 3;
+        std::vector<uint64_t> tw(n_words, 0);
+        parallel([&](unsigned t, unsigned nt) {
+            const uint64_t w0 = (n / 32 + 1) * t / nt, w1 = (n / 32 + 1) * (t + 1) / nt;
+            for (uint64_t w = w0; w < w1; ++w) {
+                uint64_t v = 0;
+                for (int j = 0; j < 32; ++j) {
+                    const uint64_t i = 32 * w + j;
+                    if (i >= n) break;
+                    const uint64_t c = i < l_pac ? fwd[i] : 3u - fwd[n - 1 - i];
+                    v |= c << (2 * j);
+                }
+                tw[w] = v;
+            }
+        });
+        BwtBuild b = bwt_build_gpu(tw, n, sa_intv, batch_limit, device);
+        primary = b.primary;
+        bwt.swap(b.bwt);
+        samples.swap(b.samples);
+    } else {
+        std::vector<uint8_t> text(n);
+        std::memcpy(text.data(), fwd.data(), l_pac);
+        for (uint64_t i = 0; i < l_pac; ++i) text[n - 1 - i] = static_cast<uint8_t>(3 - fwd[i]);
+        std::vector<uint32_t> sa = suffix_array_cpu(text.data(), n);
+        if (sa.size() != n + 1 || sa[0] != n) fail(MA_ERR_INTERNAL, "suffix array construction failed");
+        // stored BWT: rows 0..n without the sentinel row
+        const uint64_t n_occ = (n + 127) / 128 + 1;
+        bwt.assign((n + 15) / 16 + 8 * n_occ, 0);
         uint64_t cnt[4] = {0, 0, 0, 0};
-        uint64_t k = 0;       // stored position
-        uint64_t wbase = 0;   // word index of current block start
+        uint64_t k = 0;      // stored position
+        uint64_t wbase = 0;  // word index of current block start
         for (uint64_t row = 0; row <= n; ++row) {
-            if (bsym[row] == 4) {
+            if (sa[row] == 0) {
                 primary = row;
                 continue;
             }
-            uint8_t c = bsym[row];
+            const uint8_t c = text[sa[row] - 1];
             if (k % 128 == 0) {
                 wbase = (k / 128) * 16;
                 for (int cc = 0; cc < 4; ++cc) {
@@ -294,8 +360,7 @@ void build_index(const std::string& fasta, const std::string& out_prefix, bool b
                     bwt[wbase + 2 * cc + 1] = static_cast<uint32_t>(cnt[cc] >> 32);
                 }
             }
-            uint64_t wi = wbase + 8 + (k % 128) / 16;
-            bwt[wi] |= static_cast<uint32_t>(c) << ((15 - (k & 15)) << 1);
+            bwt[wbase + 8 + (k % 128) / 16] |= static_cast<uint32_t>(c) << ((15 - (k & 15)) << 1);
             cnt[c]++;
             k++;
         }
@@ -306,33 +371,42 @@ void build_index(const std::string& fasta, const std::string& out_prefix, bool b
             bwt[tb + 2 * cc] = static_cast<uint32_t>(cnt[cc]);
             bwt[tb + 2 * cc + 1] = static_cast<uint32_t>(cnt[cc] >> 32);
         }
+        const uint64_t n_sa = (n + static_cast<uint64_t>(sa_intv)) / static_cast<uint64_t>(sa_intv);
+        samples.resize(n_sa - 1);
+        for (uint64_t i = 1; i < n_sa; ++i) samples[i - 1] = sa[i * static_cast<uint64_t>(sa_intv)];
     }
     if (primary == 0) fail(MA_ERR_INTERNAL, "no primary row");
 
     // ---- write files ----
     {
-        std::vector<uint8_t> out;
-        put64(out, primary);
-        for (int c = 1; c <= 4; ++c) put64(out, L2[c]);
-        size_t h = out.size();
-        out.resize(h + bwt.size() * 4);
-        std::memcpy(out.data() + h, bwt.data(), bwt.size() * 4);
+        std::vector<uint8_t> out(40 + bwt.size() * 4);
+        put_u64_bytes(out, 0, primary);
+        for (int c = 1; c <= 4; ++c) put_u64_bytes(out, 8 * static_cast<size_t>(c), L2[c]);
+        std::memcpy(out.data() + 40, bwt.data(), bwt.size() * 4);
+        std::vector<uint32_t>().swap(bwt);
         write_all(out_prefix + ".bwt", out.data(), out.size());
     }
     {
-        const uint64_t n_sa = (n + static_cast<uint64_t>(sa_intv)) / static_cast<uint64_t>(sa_intv);
-        std::vector<uint8_t> out;
-        out.reserve(56 + 8 * n_sa);
-        put64(out, primary);
-        for (int c = 1; c <= 4; ++c) put64(out, L2[c]);
-        put64(out, static_cast<uint64_t>(sa_intv));
-        put64(out, n);
-        for (uint64_t i = 1; i < n_sa; ++i) put64(out, sa[i * static_cast<uint64_t>(sa_intv)]);
+        std::vector<uint8_t> out(56 + 8 * samples.size());
+        put_u64_bytes(out, 0, primary);
+        for (int c = 1; c <= 4; ++c) put_u64_bytes(out, 8 * static_cast<size_t>(c), L2[c]);
+        put_u64_bytes(out, 40, static_cast<uint64_t>(sa_intv));
+        put_u64_bytes(out, 48, n);
+        std::memcpy(out.data() + 56, samples.data(), samples.size() * 8);  // little-endian host
         write_all(out_prefix + ".sa", out.data(), out.size());
     }
     {
         std::vector<uint8_t> pac((l_pac + 3) / 4, 0);
-        for (uint64_t i = 0; i < l_pac; ++i) pac[i >> 2] |= static_cast<uint8_t>(text[i] << ((~i & 3) << 1));
+        parallel([&](unsigned t, unsigned nt) {
+            const uint64_t nb = (l_pac + 3) / 4;
+            const uint64_t b0 = nb * t / nt, b1 = nb * (t + 1) / nt;
+            for (uint64_t b = b0; b < b1; ++b) {
+                uint8_t v = 0;
+                for (uint64_t i = 4 * b; i < 4 * b + 4 && i < l_pac; ++i)
+                    v |= static_cast<uint8_t>(fwd[i] << ((~i & 3) << 1));
+                pac[b] = v;
+            }
+        });
         if (l_pac % 4 == 0) pac.push_back(0);
         pac.push_back(static_cast<uint8_t>(l_pac % 4));
         write_all(out_prefix + ".pac", pac.data(), pac.size());

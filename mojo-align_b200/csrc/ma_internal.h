@@ -60,10 +60,22 @@ std::vector<FastaRecord> read_fasta(const std::string& path);
 // Suffix array of text[0..n) over {0,1,2,3} with a virtual smallest
 // sentinel at n: returns SA[0..n] (SA[0] == n).  n must be < 2^32 - 1.
 std::vector<uint32_t> suffix_array_cpu(const uint8_t* text, uint64_t n);
-// Same, sorted on GPU `device` (prefix doubling over CUB radix sorts).
-std::vector<uint32_t> suffix_array_gpu(const uint8_t* text, uint64_t n, int device);
+
+// BWT of a text in the bwa .bwt word layout (after the 40-byte header),
+// its primary row and SA samples SA[i * sa_intv], i = 1 .. n_sa - 1.
+struct BwtBuild {
+    uint64_t primary = 0;
+    std::vector<uint32_t> bwt;
+    std::vector<uint64_t> samples;
+};
+// Built on GPU `device` from the text packed 32 symbols per word, least
+// significant first, zero past n, with at least two words after the last
+// symbol's word.  batch_limit caps the suffixes sorted at once (0 = what
+// fits the device).
+BwtBuild bwt_build_gpu(const std::vector<uint64_t>& text_words, uint64_t n, int sa_intv, uint64_t batch_limit,
+                       int device);
 
 void build_index(const std::string& fasta, const std::string& out_prefix, bool bwameth_c2t,
-                 int sa_intv, int device);
+                 int sa_intv, int device, uint64_t batch_limit = 0);
 
 }  // namespace ma

@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(128, MINB) seed_stage1_kernel(DevIndex ix, Dev
                 break;
             }
             for (uint64_t hi = sd.k; hi <= sd.l; ++hi) {
-                const uint64_t sa_pos = __ldg(ix.sa + hi);
+                const uint64_t sa_pos = sa_at(ix, hi);
                 if constexpr (S) t.sa_loads++;
                 int64_t b0;
                 int is_rev;
@@ -422,7 +422,7 @@ __global__ void __launch_bounds__(S2_WARPS * 32, MINB) seed_stage2_kernel(DevInd
                 int rev = 0;
                 bool ok = false;
                 if (valid) {
-                    const uint64_t sa_pos = __ldg(ix.sa + hi);
+                    const uint64_t sa_pos = sa_at(ix, hi);
                     if constexpr (S) t.sa_loads++;
                     ok = locus_of_row(ix, sa_pos, o_s, o_e, qlen, b0, rev);
                     if (ok) tag = static_cast<uint64_t>(b0 * 2 + rev);

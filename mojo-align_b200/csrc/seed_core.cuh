@@ -617,26 +617,26 @@ __device__ __forceinline__ Seed search_endpoint(const DevIndex& ix, const ReadVi
         if (!(has_c && has_g)) {
             uint32_t idx = 0;
             for (int i = 0; i < K3; ++i) idx = idx * 3 + static_cast<uint32_t>(__popcll((win >> (2 * i)) & 3));
-            const uint2 kl = __ldg(ix.kmer3[has_c ? 1 : 0] + idx);
+            const uint64_t kl = __ldg(ix.kmer3[has_c ? 1 : 0] + idx);
             if constexpr (S) t.kmer_loads++;
-            k = kl.x;
-            l = kl.y;
-            have = true;
-            K = K3;
+            if (kmer_interval(kl, k, l)) {
+                have = true;
+                K = K3;
+            }
         }
     }
     if (!have && ix.kmer_k > 0 && ix.kmer_k <= P.seed_len) {
-        K = ix.kmer_k;
-        const int s0 = e - K + 1;
-        if (window_bits(rd.nf, s0, K) != 0) return res;
-        const uint64_t win = window_bits(rd.fwd, s0, K);
+        const int s0 = e - ix.kmer_k + 1;
+        if (window_bits(rd.nf, s0, ix.kmer_k) != 0) return res;
+        const uint64_t win = window_bits(rd.fwd, s0, ix.kmer_k);
         uint32_t idx = 0;
-        for (int i = 0; i < K; ++i) idx = (idx << 2) | static_cast<uint32_t>((win >> (2 * i)) & 3);
-        const uint2 kl = __ldg(ix.kmer + idx);
+        for (int i = 0; i < ix.kmer_k; ++i) idx = (idx << 2) | static_cast<uint32_t>((win >> (2 * i)) & 3);
+        const uint64_t kl = __ldg(ix.kmer + idx);
         if constexpr (S) t.kmer_loads++;
-        k = kl.x;
-        l = kl.y;
-        have = true;
+        if (kmer_interval(kl, k, l)) {  // an untabled entry leaves (k, l) = (0, seq_len)
+            have = true;
+            K = ix.kmer_k;
+        }
     }
     if (have) {
         const int s0 = e - K + 1;

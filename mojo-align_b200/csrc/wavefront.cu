@@ -48,13 +48,20 @@ constexpr uint64_t MAX_LOCI = LIDX_MASK;          // list capacity limit (indice
 constexpr uint32_t DEAD_LOCUS = 0xFFFFFFFFu;
 constexpr int PREDICT_MEMO = 4;  // memo loci a duplicate prediction checks besides the best  // WLocus.read of a slot without a locus
 
-// One candidate locus of a round.
+// One candidate locus of a round (32 bytes: two per 64-B line).
 struct WLocus {
     int64_t b0;
-    uint64_t uk, ul;
+    uint64_t uk;         // first SA row of the seed's interval
     uint32_t read, ord_row;
-    int32_t us, e, crid, rev;
+    int32_t crid_rev;    // contig * 2 + strand (contig -1: -2 | strand)
+    uint16_t us;         // seed start
+    uint16_t e_dl;       // right endpoint (bits 0-10) | (ul - uk) << 11
+    __device__ int crid() const { return crid_rev >> 1; }
+    __device__ int rev() const { return crid_rev & 1; }
+    __device__ int e() const { return e_dl & 0x7FF; }
+    __device__ uint64_t ul() const { return uk + (e_dl >> 11); }
 };
+static_assert(sizeof(WLocus) == 32, "WLocus is 32 bytes");
 
 struct Wave {
     uint32_t* counters;
@@ -225,7 +232,7 @@ __global__ void __launch_bounds__(256, MINB) wf_search_kernel(DevIndex ix, DevRe
                 w.overflow[o_r] = 1;
                 continue;
             }
-            const uint64_t sa_pos = __ldg(ix.sa + hi);
+            const uint64_t sa_pos = sa_at(ix, hi);
             if constexpr (S) t.sa_loads++;
             WLocus L;
             int64_t b0;
@@ -237,13 +244,11 @@ __global__ void __launch_bounds__(256, MINB) wf_search_kernel(DevIndex ix, DevRe
             }
             L.b0 = b0;
             L.uk = o_k;
-            L.ul = o_l;
             L.read = static_cast<uint32_t>(o_r);
             L.ord_row = (static_cast<uint32_t>(o_ei) * 16 + static_cast<uint32_t>(hi - o_k)) * ADJ_SPAN;
-            L.us = o_s;
-            L.e = o_e;
-            L.crid = static_cast<int32_t>(contig_hint(ix, b0).crid);
-            L.rev = rev;
+            L.us = static_cast<uint16_t>(o_s);
+            L.e_dl = static_cast<uint16_t>(o_e | ((o_l - o_k) << 11));
+            L.crid_rev = static_cast<int32_t>(contig_hint(ix, b0).crid) * 2 + rev;
             w.loci[slot] = L;
             if constexpr (S) tally_locus(t, b0, clamps_for(P, o_qlen).adj_cap, o_qlen);
             const uint32_t m = atomicAdd(&w.memo_next[o_r], 1u);
@@ -284,7 +289,7 @@ __global__ void __launch_bounds__(EVAL_THREADS, MINB) wf_eval_kernel(DevIndex ix
                 const Clamps cl = clamps_for(P, rd.qlen);
                 const uint64_t bn = w.best_key[r] >> ORD_SHIFT;
                 const int prune = bn < (1u << 20) ? static_cast<int>(bn) : (1 << 20);
-                live = live_shifts<S>(ix, rd, L.b0, L.rev, adj_cap, cl.budget, cl.clip_cap, prune, t);
+                live = live_shifts<S>(ix, rd, L.b0, L.rev(), adj_cap, cl.budget, cl.clip_cap, prune, t);
             }
         }
         __syncwarp();
@@ -313,16 +318,17 @@ __global__ void __launch_bounds__(EVAL_THREADS, MINB) wf_eval_kernel(DevIndex ix
                 const Clamps cl = clamps_for(P, rd.qlen);
                 const uint64_t bn = w.best_key[r] >> ORD_SHIFT;
                 const int prune = bn < (1u << 20) ? static_cast<int>(bn) : (1 << 20);
-                ContigHint hint{L.crid, 0, 0};
-                if (L.crid >= 0) {
-                    hint.coff = static_cast<int64_t>(__ldg(ix.coff + L.crid));
-                    hint.clen = static_cast<int64_t>(__ldg(ix.clen + L.crid));
+                const int crid = L.crid();
+                ContigHint hint{crid, 0, 0};
+                if (crid >= 0) {
+                    hint.coff = static_cast<int64_t>(__ldg(ix.coff + crid));
+                    hint.clen = static_cast<int64_t>(__ldg(ix.clen + crid));
                 }
                 Best lb;
                 lb.key = ~0ull;
                 lb.crid = -1;
-                eval_adj<S>(ix, rd, L.b0, L.rev, adj, cl.budget, cl.clip_cap, L.ord_row, lb, L.uk, L.ul, L.us, L.e,
-                            prune, hint, t);
+                eval_adj<S>(ix, rd, L.b0, L.rev(), adj, cl.budget, cl.clip_cap, L.ord_row, lb, L.uk, L.ul(), L.us,
+                            L.e(), prune, hint, t);
                 if (lb.key != ~0ull) {
                     const uint64_t nm = lb.key >> ORD_SHIFT;
                     const uint64_t ord = lb.key & ((1ull << ORD_SHIFT) - 1);
@@ -379,22 +385,23 @@ __global__ void __launch_bounds__(256) wf_finalize_kernel(DevIndex ix, DevReads 
                     const int adj = static_cast<int>(ord / KIND_SPAN) - static_cast<int>(L.ord_row) - 12;
                     const uint64_t bn = old >> ORD_SHIFT;
                     const int prune = bn < (1u << 20) ? static_cast<int>(bn) : (1 << 20);
-                    ContigHint hint{L.crid, 0, 0};
-                    if (L.crid >= 0) {
-                        hint.coff = static_cast<int64_t>(__ldg(ix.coff + L.crid));
-                        hint.clen = static_cast<int64_t>(__ldg(ix.clen + L.crid));
+                    const int crid = L.crid();
+                    ContigHint hint{crid, 0, 0};
+                    if (crid >= 0) {
+                        hint.coff = static_cast<int64_t>(__ldg(ix.coff + crid));
+                        hint.clen = static_cast<int64_t>(__ldg(ix.clen + crid));
                     }
                     Best lb;
                     lb.key = ~0ull;
                     lb.crid = -1;
-                    eval_adj<S>(ix, rd, L.b0, L.rev, adj, cl.budget, cl.clip_cap, L.ord_row, lb, L.uk, L.ul, L.us,
-                                L.e, prune, hint, t);
+                    eval_adj<S>(ix, rd, L.b0, L.rev(), adj, cl.budget, cl.clip_cap, L.ord_row, lb, L.uk, L.ul(),
+                                L.us, L.e(), prune, hint, t);
                     if (lb.key != (rk >> 27)) {
                         atomicExch(err, 3);  // the recomputed candidate must be the round's minimum
                     } else {
                         write_hit(out, r, lb, qlen);
                         w.best_key[r] = lb.key;
-                        w.best_tag[r] = L.b0 * 2 + L.rev;
+                        w.best_tag[r] = L.b0 * 2 + L.rev();
                         const uint64_t nm = lb.key >> ORD_SHIFT;
                         if (nm == 0) {
                             stop = true;

@@ -95,7 +95,8 @@ class ma_index_info(C.Structure):
 
 
 class ma_index_options(C.Structure):
-    _fields_ = [("kmer_k", C.c_int32), ("kmer3_k", C.c_int32), ("hbm_budget_bytes", C.c_uint64)]
+    _fields_ = [("kmer_k", C.c_int32), ("kmer3_k", C.c_int32), ("hbm_budget_bytes", C.c_uint64),
+                ("wide_rows", C.c_int32), ("occ_super_shift", C.c_int32), ("prep_chunk_rows", C.c_uint64)]
 
 
 class ma_tuning(C.Structure):
@@ -194,6 +195,7 @@ SIGNATURES = [
     ("ma_last_error", C.c_char_p, [C.c_void_p]),
     ("ma_hbm_info", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("ma_index_build", C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_int]),
+    ("ma_index_build_batched", C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_uint64]),
     ("ma_index_options_default", None, [C.POINTER(ma_index_options)]),
     ("ma_index_open", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(ma_index_options), C.POINTER(C.c_void_p)]),
     ("ma_index_close", None, [C.c_void_p]),

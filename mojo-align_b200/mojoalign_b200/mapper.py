@@ -115,9 +115,15 @@ class Contig:
 class GpuIndex:
     """A bwa 0.7 FM-index made resident in HBM (FmIndex.load + upload)."""
 
-    def __init__(self, ctx: GpuContext, prefix, kmer_k: int = 12, kmer3_k: int = 0, hbm_budget_bytes: int = 0):
+    def __init__(self, ctx: GpuContext, prefix, kmer_k: int = 12, kmer3_k: int = 0, hbm_budget_bytes: int = 0,
+                 wide_rows: bool = False, occ_super_shift: int = 0, prep_chunk_rows: int = 0):
+        """Layout options (result-neutral): wide_rows stores 40-bit SA rows
+        even for short texts, occ_super_shift sets the Occ superblock
+        (log2 positions, 0 = 31), prep_chunk_rows the SA rows per
+        preparation pass (0 = 2^30)."""
         h = C.c_void_p()
-        opt = _lib.ma_index_options(kmer_k, kmer3_k, hbm_budget_bytes)
+        opt = _lib.ma_index_options(kmer_k, kmer3_k, hbm_budget_bytes, int(wide_rows), occ_super_shift,
+                                    prep_chunk_rows)
         check(lib.ma_index_open(ctx.handle, fspath(prefix), C.byref(opt), C.byref(h)), ctx.handle)
         self.handle = h
         self.ctx = ctx
@@ -229,9 +235,16 @@ def probe_index(prefix, kmer_k: int = 12, kmer3_k: int = 0) -> ma_index_info:
     return info
 
 
-def build_index(fasta, out_prefix, bwameth_c2t: bool = True, sa_intv: int = 32, device: int = -1) -> None:
-    """Writes a bwa-0.7 FM-index (optionally of the bwa-meth c2t text)."""
-    check(lib.ma_index_build(fspath(fasta), fspath(out_prefix), int(bwameth_c2t), sa_intv, device))
+def build_index(fasta, out_prefix, bwameth_c2t: bool = True, sa_intv: int = 32, device: int = -1,
+                batch_suffixes: int = 0) -> None:
+    """Writes a bwa-0.7 FM-index (optionally of the bwa-meth c2t text).
+    device >= 0 builds the BWT on that GPU, at most batch_suffixes suffixes
+    sorted at once (0 = what fits); -1 sorts on the host."""
+    if batch_suffixes:
+        check(lib.ma_index_build_batched(fspath(fasta), fspath(out_prefix), int(bwameth_c2t), sa_intv, device,
+                                         batch_suffixes))
+    else:
+        check(lib.ma_index_build(fspath(fasta), fspath(out_prefix), int(bwameth_c2t), sa_intv, device))
 
 
 __all__ = ["GpuContext", "GpuIndex", "MapResult", "map_batch", "map_batch_device", "build_index", "probe_index",
