@@ -329,6 +329,16 @@ int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t);
 int ma_ctx_get_tuning(const ma_ctx* ctx, ma_tuning* t);
 
 /*
+ * enable != 0: ma_map_batch_device replays a CUDA graph of its launch
+ * sequence while its arguments (buffers, sizes, parameters, stream, tuning)
+ * repeat: the first call with new arguments runs as usual, the second
+ * captures the sequence into a graph and launches it, later ones launch the
+ * graph (one host launch per call).  Result-neutral; off while profiling.
+ * No counterpart in the reference.
+ */
+int ma_ctx_set_graphs(ma_ctx* ctx, int enable);
+
+/*
  * Chunking of ma_map_batch's copy / compute pipeline (result-neutral; no
  * reference counterpart: _fm_fire_batch runs fixed 16384-pair batches two
  * deep, linear_gpu_fm.mojo:2438-3094).  Chunk k+1 is copied in and chunk k-1

@@ -119,6 +119,20 @@ struct ma_ctx {
     DevBuf sam_in, sam_arena, sam_out, sam_scratch, sam_status;
     // BGZF inflate (host form)
     DevBuf inf_in, inf_cols, inf_out;
+    // CUDA graphs of the device mapping call (ma_ctx_set_graphs): the launch
+    // sequences of the last few argument sets, each captured when its
+    // arguments come a second time and replayed while they repeat
+    struct GraphEntry {
+        unsigned char key[512] = {};
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        int launches = 0;
+        uint64_t used = 0;
+    };
+    static constexpr size_t MAX_GRAPHS = 8;
+    bool graphs = false;
+    std::vector<GraphEntry> graph_cache;
+    uint64_t graph_clock = 0;
 };
 
 struct ma_index {
@@ -253,6 +267,86 @@ void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const
     ctx->last_launches = launches;
 }
 
+void drop_graphs(ma_ctx* ctx) {
+    for (auto& g : ctx->graph_cache) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+    }
+    ctx->graph_cache.clear();
+}
+
+// enqueue_map through CUDA graphs.  Everything the launch sequence depends
+// on is in the key: the arguments, the stream, the tuning and the work
+// buffers (grow-only, so their addresses change only when they grow).  The
+// first call with a key runs uncaptured (it may allocate); the second
+// captures the sequence and launches the graph; later ones launch it.  The
+// least recently used of MAX_GRAPHS keys is dropped for a new one.
+void enqueue_map_graph(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const uint32_t* d_lens,
+                       uint32_t n1, int paired, uint32_t max_len, int bs_r1, int bs_r2, const ma_params* p,
+                       const DevOut& out, cudaStream_t st) {
+    struct Key {
+        const void* ptrs[20];
+        int64_t vals[24];
+    } key;
+    static_assert(sizeof(Key) <= sizeof(ma_ctx::GraphEntry::key), "graph key");
+    auto make_key = [&]() {
+        std::memset(&key, 0, sizeof key);
+        const void* ptrs[20] = {idx, d_bases, d_lens, out.rid, out.pos, out.mapq, out.flag, out.sl, out.sr, out.nm,
+                                out.uk, out.ul, out.us, out.e, out.score, st, ctx->packed.p, ctx->seed_scratch.p,
+                                ctx->err_flag.p, nullptr};
+        std::memcpy(key.ptrs, ptrs, sizeof ptrs);
+        const int64_t vals[24] = {n1, paired, max_len, bs_r1, bs_r2, p->seed_len, p->seed_stride, p->max_occ,
+                                  p->max_diff, p->max_soft, p->max_adj, p->rescue_win, ctx->tuning.seed_kernel,
+                                  ctx->tuning.stage1_endpoints, ctx->tuning.stage2_blocks_per_sm,
+                                  ctx->tuning.reg_level, ctx->tuning.stage1_max_rows, ctx->tuning.stage2_first_wave,
+                                  ctx->tuning.wave_endpoints, ctx->tuning.wave_loci_per_read,
+                                  ctx->tuning.wave_max_rounds, ctx->tuning.wave_growth, 0, 0};
+        std::memcpy(key.vals, vals, sizeof vals);
+    };
+    make_key();
+    ma_ctx::GraphEntry* e = nullptr;
+    for (auto& g : ctx->graph_cache)
+        if (std::memcmp(g.key, &key, sizeof key) == 0) e = &g;
+    if (e && e->exec) {
+        e->used = ++ctx->graph_clock;
+        ck(cudaGraphLaunch(e->exec, st), "cudaGraphLaunch");
+        ctx->last_launches = e->launches;
+        return;
+    }
+    if (!e) {
+        enqueue_map(ctx, idx, d_bases, d_lens, n1, paired, max_len, bs_r1, bs_r2, p, out, st);
+        make_key();  // the work buffers are sized now
+        if (ctx->graph_cache.size() >= ma_ctx::MAX_GRAPHS) {
+            auto old = std::min_element(ctx->graph_cache.begin(), ctx->graph_cache.end(),
+                                        [](const ma_ctx::GraphEntry& a, const ma_ctx::GraphEntry& b) {
+                                            return a.used < b.used;
+                                        });
+            if (old->exec) cudaGraphExecDestroy(old->exec);
+            if (old->graph) cudaGraphDestroy(old->graph);
+            ctx->graph_cache.erase(old);
+        }
+        ma_ctx::GraphEntry ne;
+        std::memcpy(ne.key, &key, sizeof key);
+        ne.used = ++ctx->graph_clock;
+        ctx->graph_cache.push_back(ne);
+        return;
+    }
+    ck(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    try {
+        enqueue_map(ctx, idx, d_bases, d_lens, n1, paired, max_len, bs_r1, bs_r2, p, out, st);
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(st, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    ck(cudaStreamEndCapture(st, &e->graph), "cudaStreamEndCapture");
+    ck(cudaGraphInstantiate(&e->exec, e->graph, 0), "cudaGraphInstantiate");
+    e->launches = ctx->last_launches;
+    e->used = ++ctx->graph_clock;
+    ck(cudaGraphLaunch(e->exec, st), "cudaGraphLaunch");
+}
+
 void check_err_flag(ma_ctx* ctx, cudaStream_t st) {
     int h = 0;
     ck(cudaMemcpyAsync(&h, ctx->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H err");
@@ -319,6 +413,7 @@ int ma_ctx_create(int device_ordinal, ma_ctx** out) {
 void ma_ctx_destroy(ma_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
+    drop_graphs(ctx);
     for (cudaEvent_t& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     ctx->tally.release();
@@ -664,8 +759,19 @@ int ma_map_batch_device(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases
             o.e = d_dbg->e;
             o.score = d_dbg->score;
         }
-        enqueue_map(ctx, idx, d_bases, d_lens, n1, paired, max_len, bs_r1, bs_r2, p, o, st);
+        if (ctx->graphs && ctx->profiling == 0) enqueue_map_graph(ctx, idx, d_bases, d_lens, n1, paired, max_len,
+                                                                 bs_r1, bs_r2, p, o, st);
+        else enqueue_map(ctx, idx, d_bases, d_lens, n1, paired, max_len, bs_r1, bs_r2, p, o, st);
         check_err_flag(ctx, st);
+    });
+}
+
+int ma_ctx_set_graphs(ma_ctx* ctx, int enable) {
+    if (!ctx) return MA_ERR_ARG;
+    return guarded(ctx, [&] {
+        use_device(ctx);
+        drop_graphs(ctx);
+        ctx->graphs = enable != 0;
     });
 }
 

@@ -677,10 +677,13 @@ struct SeedKernels {
                        const DevOut& out, int first_wave, int, const Handoff& h, unsigned long long* tally) {
         seed_stage2_kernel<S, B2><<<g, S2_WARPS * 32, 0, st>>>(ix, R, P, out, h, first_wave, tally);
     }
-    static int stage2_occupancy() {
-        int nb = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, seed_stage2_kernel<S, B2>, S2_WARPS * 32, 0);
-        return nb > 0 ? nb : 1;
+    static int stage2_occupancy() {  // computed once (calls may be inside a stream capture later)
+        static const int v = [] {
+            int nb = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, seed_stage2_kernel<S, B2>, S2_WARPS * 32, 0);
+            return nb > 0 ? nb : 1;
+        }();
+        return v;
     }
 };
 

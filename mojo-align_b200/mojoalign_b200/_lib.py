@@ -214,6 +214,7 @@ SIGNATURES = [
       C.POINTER(ma_params), C.POINTER(ma_hits), C.POINTER(ma_debug), C.c_void_p]),
     ("ma_last_launch_count", C.c_int, [C.c_void_p]),
     ("ma_ctx_set_profiling", C.c_int, [C.c_void_p, C.c_int]),
+    ("ma_ctx_set_graphs", C.c_int, [C.c_void_p, C.c_int]),
     ("ma_ctx_set_tuning", C.c_int, [C.c_void_p, C.POINTER(ma_tuning)]),
     ("ma_ctx_get_tuning", C.c_int, [C.c_void_p, C.POINTER(ma_tuning)]),
     ("ma_ctx_set_pipeline", C.c_int, [C.c_void_p, C.POINTER(ma_pipeline)]),

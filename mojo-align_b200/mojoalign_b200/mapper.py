@@ -53,6 +53,11 @@ class GpuContext:
                            stage2_first_wave, wave_endpoints, wave_loci_per_read, wave_max_rounds, wave_growth)
         check(lib.ma_ctx_set_tuning(self.handle, C.byref(t)), self.handle)
 
+    def set_graphs(self, enable: bool = True) -> None:
+        """Device mapping calls replay a captured CUDA graph while their
+        arguments repeat (see ma_ctx_set_graphs)."""
+        check(lib.ma_ctx_set_graphs(self.handle, int(enable)), self.handle)
+
     def set_pipeline(self, first_chunk_pairs: int = 0, growth_percent: int = 50, max_chunk_pairs: int = 0,
                      compute_streams: int = 3) -> None:
         """Chunking of map_batch's copy / compute pipeline (see ma_pipeline)."""
