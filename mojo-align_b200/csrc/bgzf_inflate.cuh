@@ -1,7 +1,8 @@
 // bgzf_inflate.cuh - inflating the members of a BGZF file on the device, one
-// warp per member (lane 0 decodes with the warp's tables in shared memory).
-// The per-member step is a host-and-device function, so the host tests run
-// the same code the kernel runs.
+// warp per member (bgzf_inflate.cu: lane 0 decodes tokens, the warp writes
+// their bytes and folds the CRC-32).  The per-member step below is the host
+// form: the same token decoder (inflate.cuh) with the sequential writer, so
+// the host tests run the decoder the kernel runs.
 #pragma once
 
 #include <cstdint>

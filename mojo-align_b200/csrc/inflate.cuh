@@ -1,8 +1,11 @@
 // inflate.cuh - a DEFLATE (RFC 1951) decoder for one raw deflate stream,
-// written for one GPU thread per BGZF member and compiled unchanged as host
-// code.  Every read of the input and every write or back-reference of the
-// output is checked against its buffer; a malformed stream ends with an
-// error status, never with an access outside the buffers.
+// compiled unchanged as host and device code.  The stream is decoded into
+// batches of tokens (literal runs, back-references, stored spans) by one
+// thread; the tokens' bytes are written by a whole warp on the device
+// (bgzf_inflate.cu) or by write_tokens here.  Every read of the input and
+// every write or back-reference of the output is checked against its
+// buffer; a malformed stream ends with an error status, never with an
+// access outside the buffers.
 //
 // Huffman decoding follows the canonical-code construction of RFC 1951
 // section 3.2.2: a 9-bit lookup table for short codes (indexed by the next 9
@@ -162,123 +165,303 @@ MA_HD inline int decode(Bits& b, const Huff& h) {
     return -1;
 }
 
-// Inflates the raw deflate stream in[0, n) into out[0, cap); *out_len
-// receives the bytes written.  t: scratch tables (may live in shared
-// memory).
-MA_HD inline int inflate_raw(const uint8_t* in, uint32_t n, uint8_t* out, uint32_t cap, uint32_t* out_len,
-                             Tables& t) {
-    Bits b{in, n, 0, 0, 0};
-    uint32_t o = 0;
-    *out_len = 0;
-    uint32_t last = 0;
-    do {
-        uint32_t type;
-        if (!b.get(1, last) || !b.get(2, type)) return E_INPUT;
-        if (type == 0) {
-            // stored: skip to the byte boundary, LEN, NLEN, LEN bytes
-            const int drop = b.cnt & 7;
-            b.buf >>= drop;
-            b.cnt -= drop;
-            uint32_t len, nlen;
-            if (!b.get(16, len) || !b.get(16, nlen)) return E_INPUT;
-            if (len != (~nlen & 0xffffu)) return E_STORED;
-            if (len > cap - o) return E_OUTPUT;
-            while (len && b.cnt >= 8) {  // bytes already in the bit buffer
-                out[o++] = static_cast<uint8_t>(b.buf);
-                b.buf >>= 8;
-                b.cnt -= 8;
-                --len;
+// ---- resumable decoding into tokens ----
+// The decoder turns the stream into tokens: a run of literal bytes (kept in
+// a literal buffer), a back-reference (length, distance) or a stored span
+// of the input.  Decoding and writing are separate so that one thread can
+// decode while a warp writes the bytes (bgzf_inflate.cu); write_tokens is
+// the sequential writer.
+constexpr uint32_t TOK_LITERAL = 0;            // dist of a literal run: bytes at lit[src]
+constexpr uint32_t TOK_STORED = 0xFFFFFFFFu;   // dist of a stored span: bytes at in[src]
+
+struct Tok {
+    uint32_t len, dist, src;
+};
+
+// Decoder state between batches of tokens.
+struct Stream {
+    Bits b;
+    uint32_t o;      // bytes of output the tokens so far produce
+    uint32_t cap;    // output buffer size
+    uint32_t last;   // the current (or last) block is the final one
+    int in_block;    // inside a compressed block (tables built)
+    int status;      // Status; OK while decoding
+    int finished;    // the final block has ended
+};
+
+MA_HD inline void stream_init(Stream& s, const uint8_t* in, uint32_t n, uint32_t cap) {
+    s.b = Bits{in, n, 0, 0, 0};
+    s.o = 0;
+    s.cap = cap;
+    s.last = 0;
+    s.in_block = 0;
+    s.status = OK;
+    s.finished = 0;
+}
+
+// Decodes tokens into tok[0, max_tok) (literal bytes into lit[0, max_lit))
+// until either buffer is full, the stream ends or an error sets s.status;
+// returns the number of tokens.  max_tok >= 2, max_lit >= 8.
+MA_HD inline int decode_tokens(Stream& s, Tables& t, Tok* tok, int max_tok, uint8_t* lit, int max_lit) {
+    Bits& b = s.b;
+    int nt = 0, nl = 0;
+    while (s.status == OK && !s.finished) {
+        if (!s.in_block) {
+            if (s.last) {
+                s.finished = 1;
+                break;
             }
-            if (len > b.n - b.pos) return E_INPUT;
-            for (uint32_t i = 0; i < len; ++i) out[o++] = b.in[b.pos + i];
-            b.pos += len;
-            continue;
-        }
-        if (type == 3) return E_BLOCK;
-        int nlit, ndist;
-        if (type == 1) {
-            for (int s = 0; s < 144; ++s) t.lens[s] = 8;
-            for (int s = 144; s < 256; ++s) t.lens[s] = 9;
-            for (int s = 256; s < 280; ++s) t.lens[s] = 7;
-            for (int s = 280; s < NLIT; ++s) t.lens[s] = 8;
-            for (int s = 0; s < NDIST; ++s) t.lens[NLIT + s] = 5;
-            nlit = NLIT;
-            ndist = NDIST;
-            if (build(t.lit, t.lens, nlit, 1) != OK || build(t.dist, t.lens + NLIT, ndist, 1) != OK) return E_CODES;
-        } else {
-            uint32_t hlit, hdist, hclen;
-            if (!b.get(5, hlit) || !b.get(5, hdist) || !b.get(4, hclen)) return E_INPUT;
-            nlit = static_cast<int>(hlit) + 257;
-            ndist = static_cast<int>(hdist) + 1;
-            if (nlit > 286 || ndist > 30) return E_CODES;
-            const uint8_t ORDER[19] = {16, 17, 18, 0, 8, 7, 9, 6, 10, 5, 11, 4, 12, 3, 13, 2, 14, 1, 15};
-            uint8_t cl[19];
-            for (int i = 0; i < 19; ++i) cl[i] = 0;
-            for (uint32_t i = 0; i < hclen + 4; ++i) {
-                uint32_t v;
-                if (!b.get(3, v)) return E_INPUT;
-                cl[ORDER[i]] = static_cast<uint8_t>(v);
+            // room for a stored block's head bytes and span
+            if (nt + 2 > max_tok || nl + 8 > max_lit) break;
+            uint32_t last, type;
+            if (!b.get(1, last) || !b.get(2, type)) {
+                s.status = E_INPUT;
+                break;
             }
-            if (build(t.lit, cl, 19, 0) != OK) return E_CODES;
-            // literal/length then distance code lengths, one run-length sequence
-            int i = 0;
-            while (i < nlit + ndist) {
-                const int sym = decode(b, t.lit);
-                if (sym < 0) return b.cnt == 0 && b.pos >= b.n ? E_INPUT : E_CODES;
-                if (sym < 16) {
-                    t.lens[i++] = static_cast<uint8_t>(sym);
-                    continue;
+            s.last = last;
+            if (type == 0) {
+                // stored: skip to the byte boundary, LEN, NLEN, LEN bytes
+                const int drop = b.cnt & 7;
+                b.buf >>= drop;
+                b.cnt -= drop;
+                uint32_t len, nlen;
+                if (!b.get(16, len) || !b.get(16, nlen)) {
+                    s.status = E_INPUT;
+                    break;
                 }
-                uint32_t rep;
-                uint8_t val = 0;
-                if (sym == 16) {
-                    if (i == 0) return E_CODES;
-                    val = t.lens[i - 1];
-                    if (!b.get(2, rep)) return E_INPUT;
-                    rep += 3;
-                } else if (sym == 17) {
-                    if (!b.get(3, rep)) return E_INPUT;
-                    rep += 3;
-                } else {
-                    if (!b.get(7, rep)) return E_INPUT;
-                    rep += 11;
+                if (len != (~nlen & 0xffffu)) {
+                    s.status = E_STORED;
+                    break;
                 }
-                if (i + static_cast<int>(rep) > nlit + ndist) return E_CODES;
-                while (rep--) t.lens[i++] = val;
-            }
-            if (t.lens[256] == 0) return E_CODES;  // no end-of-block code
-            // distance lengths sit right after the literal/length ones
-            uint8_t dl[NDIST];
-            for (int s = 0; s < ndist; ++s) dl[s] = t.lens[nlit + s];
-            if (build(t.lit, t.lens, nlit, 1) != OK || build(t.dist, dl, ndist, 1) != OK) return E_CODES;
-        }
-        // the block's symbols
-        for (;;) {
-            const int sym = decode(b, t.lit);
-            if (sym < 0) return b.cnt == 0 && b.pos >= b.n ? E_INPUT : E_SYMBOL;
-            if (sym < 256) {
-                if (o >= cap) return E_OUTPUT;
-                out[o++] = static_cast<uint8_t>(sym);
+                if (len > s.cap - s.o) {
+                    s.status = E_OUTPUT;
+                    break;
+                }
+                uint32_t k = 0;  // bytes already in the bit buffer (at most 4 here)
+                while (k < len && b.cnt >= 8) {
+                    lit[nl + static_cast<int>(k)] = static_cast<uint8_t>(b.buf);
+                    b.buf >>= 8;
+                    b.cnt -= 8;
+                    ++k;
+                }
+                if (k) tok[nt++] = Tok{k, TOK_LITERAL, static_cast<uint32_t>(nl)};
+                nl += static_cast<int>(k);
+                const uint32_t rest = len - k;
+                if (rest > b.n - b.pos) {
+                    s.status = E_INPUT;
+                    break;
+                }
+                if (rest) tok[nt++] = Tok{rest, TOK_STORED, b.pos};
+                b.pos += rest;
+                s.o += len;
                 continue;
             }
-            if (sym == 256) break;
+            if (type == 3) {
+                s.status = E_BLOCK;
+                break;
+            }
+            int nlit, ndist;
+            if (type == 1) {
+                for (int v = 0; v < 144; ++v) t.lens[v] = 8;
+                for (int v = 144; v < 256; ++v) t.lens[v] = 9;
+                for (int v = 256; v < 280; ++v) t.lens[v] = 7;
+                for (int v = 280; v < NLIT; ++v) t.lens[v] = 8;
+                for (int v = 0; v < NDIST; ++v) t.lens[NLIT + v] = 5;
+                nlit = NLIT;
+                ndist = NDIST;
+                if (build(t.lit, t.lens, nlit, 1) != OK || build(t.dist, t.lens + NLIT, ndist, 1) != OK) {
+                    s.status = E_CODES;
+                    break;
+                }
+            } else {
+                uint32_t hlit, hdist, hclen;
+                if (!b.get(5, hlit) || !b.get(5, hdist) || !b.get(4, hclen)) {
+                    s.status = E_INPUT;
+                    break;
+                }
+                nlit = static_cast<int>(hlit) + 257;
+                ndist = static_cast<int>(hdist) + 1;
+                if (nlit > 286 || ndist > 30) {
+                    s.status = E_CODES;
+                    break;
+                }
+                const uint8_t ORDER[19] = {16, 17, 18, 0, 8, 7, 9, 6, 10, 5, 11, 4, 12, 3, 13, 2, 14, 1, 15};
+                uint8_t cl[19];
+                for (int i = 0; i < 19; ++i) cl[i] = 0;
+                int st = OK;
+                for (uint32_t i = 0; i < hclen + 4; ++i) {
+                    uint32_t v;
+                    if (!b.get(3, v)) {
+                        st = E_INPUT;
+                        break;
+                    }
+                    cl[ORDER[i]] = static_cast<uint8_t>(v);
+                }
+                if (st == OK && build(t.lit, cl, 19, 0) != OK) st = E_CODES;
+                // literal/length then distance code lengths, one run-length sequence
+                int i = 0;
+                while (st == OK && i < nlit + ndist) {
+                    const int sym = decode(b, t.lit);
+                    if (sym < 0) {
+                        st = b.cnt == 0 && b.pos >= b.n ? E_INPUT : E_CODES;
+                        break;
+                    }
+                    if (sym < 16) {
+                        t.lens[i++] = static_cast<uint8_t>(sym);
+                        continue;
+                    }
+                    uint32_t rep;
+                    uint8_t val = 0;
+                    if (sym == 16) {
+                        if (i == 0) {
+                            st = E_CODES;
+                            break;
+                        }
+                        val = t.lens[i - 1];
+                        if (!b.get(2, rep)) {
+                            st = E_INPUT;
+                            break;
+                        }
+                        rep += 3;
+                    } else if (sym == 17) {
+                        if (!b.get(3, rep)) {
+                            st = E_INPUT;
+                            break;
+                        }
+                        rep += 3;
+                    } else {
+                        if (!b.get(7, rep)) {
+                            st = E_INPUT;
+                            break;
+                        }
+                        rep += 11;
+                    }
+                    if (i + static_cast<int>(rep) > nlit + ndist) {
+                        st = E_CODES;
+                        break;
+                    }
+                    while (rep--) t.lens[i++] = val;
+                }
+                if (st == OK && t.lens[256] == 0) st = E_CODES;  // no end-of-block code
+                if (st == OK) {
+                    // distance lengths sit right after the literal/length ones
+                    uint8_t dl[NDIST];
+                    for (int v = 0; v < ndist; ++v) dl[v] = t.lens[nlit + v];
+                    if (build(t.lit, t.lens, nlit, 1) != OK || build(t.dist, dl, ndist, 1) != OK) st = E_CODES;
+                }
+                if (st != OK) {
+                    s.status = st;
+                    break;
+                }
+            }
+            s.in_block = 1;
+        }
+        // the block's symbols, while there is room for one more token
+        while (nt < max_tok && nl < max_lit) {
+            const int sym = decode(b, t.lit);
+            if (sym < 0) {
+                s.status = b.cnt == 0 && b.pos >= b.n ? E_INPUT : E_SYMBOL;
+                break;
+            }
+            if (sym < 256) {
+                if (s.o >= s.cap) {
+                    s.status = E_OUTPUT;
+                    break;
+                }
+                if (nt > 0 && tok[nt - 1].dist == TOK_LITERAL &&
+                    tok[nt - 1].src + tok[nt - 1].len == static_cast<uint32_t>(nl))
+                    tok[nt - 1].len++;
+                else
+                    tok[nt++] = Tok{1, TOK_LITERAL, static_cast<uint32_t>(nl)};
+                lit[nl++] = static_cast<uint8_t>(sym);
+                s.o++;
+                continue;
+            }
+            if (sym == 256) {
+                s.in_block = 0;
+                break;
+            }
             const int li = sym - 257;
-            if (li >= 29) return E_SYMBOL;
+            if (li >= 29) {
+                s.status = E_SYMBOL;
+                break;
+            }
             uint32_t e = 0;
-            if (len_extra(li) && !b.get(len_extra(li), e)) return E_INPUT;
+            if (len_extra(li) && !b.get(len_extra(li), e)) {
+                s.status = E_INPUT;
+                break;
+            }
             const uint32_t len = len_base(li) + e;
             const int ds = decode(b, t.dist);
-            if (ds < 0) return b.cnt == 0 && b.pos >= b.n ? E_INPUT : E_SYMBOL;
-            if (ds >= 30) return E_SYMBOL;
+            if (ds < 0) {
+                s.status = b.cnt == 0 && b.pos >= b.n ? E_INPUT : E_SYMBOL;
+                break;
+            }
+            if (ds >= 30) {
+                s.status = E_SYMBOL;
+                break;
+            }
             e = 0;
-            if (dist_extra(ds) && !b.get(dist_extra(ds), e)) return E_INPUT;
+            if (dist_extra(ds) && !b.get(dist_extra(ds), e)) {
+                s.status = E_INPUT;
+                break;
+            }
             const uint32_t dist = dist_base(ds) + e;
-            if (dist > o) return E_DIST;
-            if (len > cap - o) return E_OUTPUT;
-            for (uint32_t k = 0; k < len; ++k, ++o) out[o] = out[o - dist];
+            if (dist > s.o) {
+                s.status = E_DIST;
+                break;
+            }
+            if (len > s.cap - s.o) {
+                s.status = E_OUTPUT;
+                break;
+            }
+            tok[nt++] = Tok{len, dist, 0};
+            s.o += len;
         }
-    } while (!last);
-    *out_len = o;
+        if (s.in_block) break;  // a token buffer is full
+    }
+    return nt;
+}
+
+// Writes the bytes of tok[0, ntok) to out from position o0, in order.  A
+// back-reference of distance d copies byte k from o - d + k % d, which is
+// before the token, so its bytes do not depend on one another.
+MA_HD inline void write_tokens(const Tok* tok, int ntok, const uint8_t* lit, const uint8_t* in, uint8_t* out,
+                               uint32_t o0) {
+    uint32_t o = o0;
+    for (int i = 0; i < ntok; ++i) {
+        const Tok& k = tok[i];
+        if (k.dist == TOK_LITERAL) {
+            for (uint32_t j = 0; j < k.len; ++j) out[o + j] = lit[k.src + j];
+        } else if (k.dist == TOK_STORED) {
+            for (uint32_t j = 0; j < k.len; ++j) out[o + j] = in[k.src + j];
+        } else {
+            for (uint32_t j = 0; j < k.len; ++j) out[o + j] = out[o - k.dist + j % k.dist];
+        }
+        o += k.len;
+    }
+}
+
+constexpr int BATCH_TOKENS = 64;   // tokens per decoding batch
+constexpr int BATCH_LITERALS = 256;
+
+// Inflates the raw deflate stream in[0, n) into out[0, cap); *out_len
+// receives the bytes written.  t: scratch tables (may live in shared
+// memory).  The token decoder and the sequential writer, batch by batch.
+MA_HD inline int inflate_raw(const uint8_t* in, uint32_t n, uint8_t* out, uint32_t cap, uint32_t* out_len,
+                             Tables& t) {
+    Stream s;
+    stream_init(s, in, n, cap);
+    Tok tok[BATCH_TOKENS];
+    uint8_t lit[BATCH_LITERALS];
+    *out_len = 0;
+    while (s.status == OK && !s.finished) {
+        const uint32_t o0 = s.o;
+        const int nt = decode_tokens(s, t, tok, BATCH_TOKENS, lit, BATCH_LITERALS);
+        write_tokens(tok, nt, lit, in, out, o0);
+    }
+    if (s.status != OK) return s.status;
+    *out_len = s.o;
     return OK;
 }
 

@@ -29,6 +29,7 @@ from __future__ import annotations
 
 import contextlib
 import ctypes as C
+import gzip
 import os
 import struct
 from concurrent.futures import ThreadPoolExecutor
@@ -115,6 +116,149 @@ class _Feed:
         self._buf = None
 
 
+class _DeviceFeed:
+    """Uncompressed bytes of one BGZF FASTQ file in HBM, inflated on the
+    device: fill() reads whole members (their compressed bytes only cross
+    PCIe) into a pinned buffer, copies them to the device and inflates them
+    behind the bytes left from the last piece (ma_bgzf_inflate_device, one
+    warp per member); consume(n) drops the first n bytes, moving the rest to
+    the front on the device.  Same interface as _Feed, with `dev` in place
+    of `pin`.  A member that is not BGZF (an appended plain gzip member) is
+    inflated on the host and copied in."""
+
+    def __init__(self, path: str, chunk: int, torch, ctx):
+        self.torch, self.ctx = torch, ctx
+        self.fh = open(path, "rb")
+        self.cap = chunk
+        self.dev = torch.empty(chunk + 16, dtype=torch.uint8, device=torch.device("cuda", ctx.device))
+        self.stream = torch.cuda.Stream(device=self.dev.device)
+        # compressed bytes of one fill at most a quarter of the piece (BGZF
+        # members inflate to at most 64 KB; FASTQ compresses 2-4x)
+        self._cbuf = pinned.take(max(chunk // 4, 1 << 20))
+        self.cpin = self._cbuf.numpy()
+        self.craw = b""  # compressed bytes read but not yet inflated
+        self.len = 0
+        self.eof = False
+        self.h2d_bytes = 0
+        self._tail = None  # host reader over a non-BGZF remainder
+
+    def _more(self, need: int) -> bool:
+        """Reads until craw holds `need` bytes; False at the end of the file."""
+        while len(self.craw) < need:
+            more = self.fh.read(max(1 << 20, need - len(self.craw)))
+            if not more:
+                return False
+            self.craw += more
+        return True
+
+    def _members(self):
+        """Whole BGZF members from the file (compressed bytes; as many as fit
+        the pinned buffer and the room left in the device buffer), skipping
+        zero padding between them: their table, compressed and inflated
+        sizes, and why it stopped ("room", "end" of the file, or "other": a
+        member that is not BGZF)."""
+        from .fqio import _bgzf_size
+
+        room = self.cap - self.len
+        so, sl, do, isz, crc = [], [], [], [], []
+        used = out = 0
+        why = "end"
+        while True:
+            self._more(18 + 256)
+            if self.craw[:1] == b"\0":  # gzip allows zero padding between members
+                self.craw = self.craw.lstrip(b"\0")
+                continue
+            if not self.craw:
+                break
+            n = _bgzf_size(self.craw[:18 + 256])
+            if n == 0:
+                why = "other"
+                break
+            if not self._more(n):
+                raise EOFError("Compressed file ended before the end-of-stream marker was reached")
+            isize = struct.unpack_from("<I", self.craw, n - 4)[0]
+            if out + isize > room or used + n > self.cpin.size:
+                why = "room"
+                break
+            xlen = struct.unpack_from("<H", self.craw, 10)[0]
+            self.cpin[used:used + n] = np.frombuffer(self.craw, np.uint8, n)
+            so.append(used + 12 + xlen)
+            sl.append(n - 12 - xlen - 8)
+            do.append(out)
+            isz.append(isize)
+            crc.append(struct.unpack_from("<I", self.craw, n - 8)[0])
+            used += n
+            out += isize
+            self.craw = self.craw[n:]
+        return why, used, out, (so, sl, do, isz, crc)
+
+    def fill(self):
+        torch = self.torch
+        if self._tail is not None:
+            self._fill_host()
+            return
+        why, used, out, table = self._members()
+        if used:
+            so = table[0]
+            with torch.cuda.stream(self.stream):
+                d_in = torch.empty(used, dtype=torch.uint8, device=self.dev.device)
+                d_in.copy_(torch.from_numpy(self.cpin[:used]), non_blocking=True)
+                tab = [torch.from_numpy(np.asarray(v, dt)).to(self.dev.device)
+                       for v, dt in zip(table, (np.uint64, np.uint32, np.uint64, np.uint32, np.uint32))]
+                status = torch.zeros(len(so), dtype=torch.int32, device=self.dev.device)
+                check(lib.ma_bgzf_inflate_device(self.ctx.handle, d_in.data_ptr(), used, *[t.data_ptr() for t in tab],
+                                                 len(so), self.dev.data_ptr() + self.len, self.cap - self.len,
+                                                 status.data_ptr(), self.stream.cuda_stream), self.ctx.handle)
+                bad = torch.nonzero(status).flatten().cpu()
+            self.stream.synchronize()
+            if bad.numel():
+                m = int(bad[0])
+                raise gzip.BadGzipFile(f"BGZF member {m} of a piece fails to inflate (status {int(status[m])})")
+            self.h2d_bytes += used
+            self.len += out
+        if why == "other":
+            # a member that is not BGZF: the gzip module reads the rest
+            import io
+
+            from .fqio import _Prefixed
+
+            self._tail = gzip.GzipFile(fileobj=io.BufferedReader(_Prefixed(self.craw, self.fh)))
+            self.craw = b""
+            self._fill_host()
+            return
+        self.eof = why == "end"
+
+    def _fill_host(self):
+        torch = self.torch
+        room = self.cap - self.len
+        if room <= 0:
+            return
+        data = self._tail.read(room)
+        if not data:
+            self.eof = True
+            return
+        t = torch.from_numpy(np.frombuffer(data, np.uint8).copy())
+        self.dev[self.len:self.len + len(data)].copy_(t)
+        self.h2d_bytes += len(data)
+        self.len += len(data)
+        self.eof = False
+
+    def consume(self, n: int):
+        rest = self.len - n
+        if rest > 0 and n > 0:
+            with self.torch.cuda.stream(self.stream):
+                self.dev[:rest].copy_(self.dev[n:self.len].clone())
+            self.stream.synchronize()
+        self.len = max(rest, 0)
+
+    def close(self):
+        self.fh.close()
+        if self._tail is not None:
+            self._tail.close()
+        pinned.give(self._cbuf)
+        self._cbuf = None
+
+
 class _Grow:
     """A device array that keeps its contents when it grows."""
 
@@ -147,8 +291,20 @@ class MappedChunk:
                                     cols["qual_len"].data_ptr())
 
 
+def _feed(path: str, chunk: int, torch, ctx, device_inflate: bool):
+    """The feed of one FASTQ file: BGZF files (by the gzip suffix and the
+    first member) inflated on the device when device_inflate is set, others
+    through the host reader."""
+    from .fqio import is_bgzf
+
+    low = path.lower()
+    if device_inflate and (low.endswith(".gz") or low.endswith(".gzip")) and is_bgzf(path):
+        return _DeviceFeed(path, chunk, torch, ctx)
+    return _Feed(path, chunk, torch)
+
+
 def mapped_chunks(ctx, index, params, fq1, fq2, bs_r1, bs_r2, rules, batch_pairs, chunk_bytes, stream, tm,
-                  before_map=None):
+                  before_map=None, device_inflate: bool = True):
     """Yields MappedChunk for consecutive pieces of the FASTQ file(s): the
     uncompressed bytes go to HBM once (the next piece is read on a host
     thread meanwhile), records are split under `rules` (MA_FASTQ_RULES_*),
@@ -166,7 +322,9 @@ def mapped_chunks(ctx, index, params, fq1, fq2, bs_r1, bs_r2, rules, batch_pairs
     dev = torch.device("cuda", ctx.device)
     sh = stream.cuda_stream
     p = params.to_c()
-    feeds = [_Feed(str(fq1), chunk_bytes, torch)] + ([_Feed(str(fq2), chunk_bytes, torch)] if paired else [])
+    feeds = [_feed(str(fq1), chunk_bytes, torch, ctx, device_inflate)] + (
+        [_feed(str(fq2), chunk_bytes, torch, ctx, device_inflate)] if paired else [])
+    tm.setdefault("fastq_h2d_bytes", 0)
     pool = ThreadPoolExecutor(max_workers=1)  # reads the next piece while the GPU maps this one
     pending = None
     o3 = (C.c_uint64 * 3)()
@@ -186,7 +344,11 @@ def mapped_chunks(ctx, index, params, fq1, fq2, bs_r1, bs_r2, rules, batch_pairs
             d_buf = torch.empty(sum(sizes) + 16, dtype=torch.uint8, device=dev)
             off = 0
             for f in feeds:
-                d_buf[off:off + f.len].copy_(torch.from_numpy(f.pin[: f.len]), non_blocking=True)
+                if isinstance(f, _DeviceFeed):
+                    d_buf[off:off + f.len].copy_(f.dev[: f.len])
+                else:
+                    d_buf[off:off + f.len].copy_(torch.from_numpy(f.pin[: f.len]), non_blocking=True)
+                    tm["fastq_h2d_bytes"] += f.len
                 off += f.len
             recs, rcs, counts = [], [], []
             for m, f in enumerate(feeds):
@@ -255,6 +417,8 @@ def mapped_chunks(ctx, index, params, fq1, fq2, bs_r1, bs_r2, rules, batch_pairs
             pending.exception()
         pool.shutdown(wait=True)
         for f in feeds:
+            if isinstance(f, _DeviceFeed):
+                tm["fastq_h2d_bytes"] += f.h2d_bytes
             f.close()
 
 
@@ -262,10 +426,12 @@ def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", 
                      bs_r2: str = "", params: FmParams | None = None, environ=None, kmer_k: int = 12,
                      kmer3_k: int | None = None, ctx: GpuContext | None = None, index: GpuIndex | None = None,
                      batch_pairs: int = 1 << 20, chunk_bytes: int = 512 << 20, level: int | None = None,
-                     stats: dict | None = None) -> int:
+                     stats: dict | None = None, device_inflate: bool = True) -> int:
     """FASTQ -> sorted, duplicate-marked BGZF BAM; returns the mapped records.
     `stats`, when given, receives seconds spent per phase (waiting for FASTQ
-    bytes, the per-batch device work, sort + gather, BGZF, writing)."""
+    bytes, the per-batch device work, sort + gather, BGZF, writing) and the
+    FASTQ bytes copied to the device (fastq_h2d_bytes: the compressed bytes
+    of BGZF inputs inflated on the device, device_inflate)."""
     import time
 
     import torch
@@ -306,7 +472,7 @@ def map_fastq_to_bam(ref_fa, fq1, out_bam, device: str = "auto", fq2: str = "", 
             raise RuntimeError("FM sort cap exceeded; set METHYLGRAPHER_FM_SORT_CAP")
 
     pieces = mapped_chunks(ctx, index, params, fq1, fq2, bs_r1, bs_r2, MA_FASTQ_RULES_STREAM, batch_pairs,
-                           chunk_bytes, stream, tm, cap_check)
+                           chunk_bytes, stream, tm, cap_check, device_inflate=device_inflate)
     try:
         t_loop = time.perf_counter()
         for ch in pieces:

@@ -38,12 +38,14 @@ from .sam import LINE_FIXED, SamContigs, sam_error
 def map_fastq_to_sam(ref_fa, fq1, out_sam, device: str = "auto", fq2: str = "", bs_r1: str = "", bs_r2: str = "",
                      params: FmParams | None = None, environ=None, kmer_k: int = 12, kmer3_k: int | None = None,
                      ctx: GpuContext | None = None, index: GpuIndex | None = None, batch_pairs: int = 1 << 20,
-                     chunk_bytes: int = 256 << 20, stats: dict | None = None) -> int:
+                     chunk_bytes: int = 256 << 20, stats: dict | None = None, device_inflate: bool = True) -> int:
     """FASTQ -> SAM; returns the mapped records.  `stats`, when given,
     receives seconds per phase (waiting for FASTQ bytes, device work per
-    chunk, waiting for the writer) and the SAM emitter's device time
-    (CUDA events on the pipeline's stream) with the lines, text bytes and
-    arena bytes (name + SEQ + QUAL) it handled."""
+    chunk, waiting for the writer), the SAM emitter's device time (CUDA
+    events on the pipeline's stream) with the lines, text bytes and arena
+    bytes (name + SEQ + QUAL) it handled, and the FASTQ bytes copied to the
+    device (fastq_h2d_bytes: the compressed bytes of BGZF inputs inflated on
+    the device, device_inflate)."""
     import time
 
     import torch
@@ -77,7 +79,7 @@ def map_fastq_to_sam(ref_fa, fq1, out_sam, device: str = "auto", fq2: str = "", 
     scope.enter_context(torch.cuda.stream(stream))
     fh = ParallelWriter(out_sam)
     pieces = mapped_chunks(ctx, index, params, fq1, fq2, bs_r1, bs_r2, MA_FASTQ_RULES_PAIR_READER, batch_pairs,
-                           chunk_bytes, stream, tm)
+                           chunk_bytes, stream, tm, device_inflate=device_inflate)
     try:
         fh.write(sam_header(index.contigs, env).encode())
         t_loop = time.perf_counter()
