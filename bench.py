@@ -626,6 +626,7 @@ def run_fq2bam_stage(args, ctx, gi, rb, local, params):
     import shutil
     import sys as _sys
 
+    from mojoalign_b200 import _lib
     from mojoalign_b200.fq2bam import bam_header, map_fastq_to_bam
 
     n = min(args.fq2bam_pairs, rb.n1)
@@ -647,6 +648,32 @@ def run_fq2bam_stage(args, ctx, gi, rb, local, params):
             times.append(time.perf_counter() - t)
         wall = statistics.median(times)
         bam_size = out.stat().st_size
+        # the same FASTQ as BGZF files (bgzip's format, level 1): inflated on
+        # the device, only the compressed members cross PCIe
+        gz = []
+        for src in (r1, r2):
+            raw = np.fromfile(src, dtype=np.uint8)
+            cap = int(_lib.lib.ma_bgzf_bound(raw.size))
+            buf = np.empty(cap, np.uint8)
+            size = _lib.C.c_uint64()
+            _lib.check(_lib.lib.ma_bgzf_compress(ctx.handle, raw.ctypes.data, raw.size, 1, 1, buf.ctypes.data, cap,
+                                                 _lib.C.byref(size)), ctx.handle)
+            q = Path(str(src) + ".gz")
+            buf[:size.value].tofile(q)
+            gz.append(q)
+        out_gz = d / "out_gz.bam"
+        lvl = args.bgzf_level if args.bgzf_level >= 0 else 1
+        map_fastq_to_bam(None, gz[0], out_gz, fq2=gz[1], bs_r1="C2T", bs_r2="G2A", params=params, environ={},
+                         ctx=ctx, index=gi, level=lvl)
+        gz_times, gz_phases = [], {}
+        for _ in range(max(1, min(args.steps, 3))):
+            t = time.perf_counter()
+            map_fastq_to_bam(None, gz[0], out_gz, fq2=gz[1], bs_r1="C2T", bs_r2="G2A", params=params, environ={},
+                             ctx=ctx, index=gi, level=lvl, stats=gz_phases)
+            gz_times.append(time.perf_counter() - t)
+        gz_wall = statistics.median(gz_times)
+        gz_bytes = sum(q.stat().st_size for q in gz)
+        gz_same = gzip_content(out_gz) == gzip_content(out)
         # parity on a sample: the first pairs through both paths at level 0
         ns = 20_000
         s1, s2 = d / "s1.fq", d / "s2.fq"
@@ -677,9 +704,21 @@ def run_fq2bam_stage(args, ctx, gi, rb, local, params):
                              "kind": "port", "sample": f"the first {ns} pairs through the oracle pipeline "
                                                        f"(mapping on all cores), {cpu_s:.2f} s"},
             "parity": {"reads": 2 * ns, "bam_file_identical_at_level0": bool(same)},
+            "bgzf_input": {"value": round(records / gz_wall, 1), "unit": "reads/s", "s_per_run": round(gz_wall, 3),
+                           "phases_s": gz_phases, "input_bytes": gz_bytes,
+                           "e2e": {"h2d_bytes_per_step": int(gz_phases.get("fastq_h2d_bytes", gz_bytes)),
+                                   "d2h_bytes_per_step": out_gz.stat().st_size},
+                           "inflate": "BGZF members copied to the device and inflated there (one warp per member)",
+                           "parity": {"bam_content_equals_plain_input": bool(gz_same)}},
         }
     finally:
         shutil.rmtree(d, ignore_errors=True)
+
+
+def gzip_content(path) -> bytes:
+    import gzip
+
+    return gzip.decompress(Path(path).read_bytes())
 
 
 def run_fq2sam_stage(args, ctx, gi, rb, local, params, peaks):
@@ -945,6 +984,60 @@ def parity_failures(obj, path="") -> list:
     return bad
 
 
+def seeding_roofline(tally, wave) -> dict:
+    """The seeding kernels alone (wavefront search: k-mer table, Occ and SA
+    gathers) from the counting pass's tally and the per-round search times."""
+    if not wave or not any(w[0] for w in wave):
+        return {}
+    search_ms = statistics.mean(w[0] for w in wave)
+    seed_bytes = 32 * (tally[0] + tally[1] + tally[2])
+    return {"seeding": {"kernel": "wf_search_kernel (all rounds)", "ms": round(search_ms, 3),
+                        "eval_ms": round(statistics.mean(w[1] for w in wave), 3),
+                        "finalize_ms": round(statistics.mean(w[2] for w in wave), 3),
+                        "alg_bytes": int(seed_bytes),
+                        "alg": "32-B sectors of the Occ lines, k-mer table entries and SA entries the search "
+                               "gathers (this implementation's accesses)",
+                        "achieved_GBs": round(seed_bytes / (search_ms / 1000) / 1e9, 1)}}
+
+
+def add_gather_fractions(line) -> None:
+    """Fractions of the measured random-gather rooflines for the seeding
+    figure (32- and 64-byte lines)."""
+    sd = line["roofline"].get("seeding")
+    g = line.get("gather_roofline") or {}
+    if sd and g:
+        sd["frac_of_gather32"] = round(sd["achieved_GBs"] / g["hbm_32B_GBs"], 4)
+        sd["frac_of_gather64"] = round(sd["achieved_GBs"] / g["hbm_64B_GBs"], 4)
+
+
+def reference_algorithm_bytes(line, ix, bases, lens, n1, paired, max_len, params, n_seq, bs2=2) -> None:
+    """Bytes the reference algorithm moves per read, from the oracle's
+    counters on (up to 100 k pairs of) the given reads: 64-B BWT lines per
+    backward step and per LF-walk step, 8-B SA samples, 32-B pac sectors,
+    packed reads in, 28 B of outputs; and as GB/s over the seed kernels'
+    and the search kernel's times for the whole call."""
+    k = min(n1, 100_000)
+    if paired:
+        b = np.concatenate([bases[:k], bases[n1:n1 + k]])
+        l_ = np.concatenate([lens[:k], lens[n1:n1 + k]])
+    else:
+        b, l_ = bases[:k], lens[:k]
+    ct = ix.map(b, l_, k, paired, max_len, 1, bs2, params.as_list(), counters=True)["counters"]
+    nr = int(l_.size)
+    seed_ref = 64 * (ct["occ_lines"] + ct["lf_lines"]) + 8 * ct["sa_loads"]
+    total = seed_ref + 32 * ct["pac_sectors"] + int(((l_.astype(np.int64) + 3) // 4).sum()) + 28 * nr
+    r = line["roofline"]
+    r["reference_algorithm"] = {
+        "bytes_per_read": round(total / nr, 1), "seeding_bytes_per_read": round(seed_ref / nr, 1),
+        "source": f"oracle counters (orc_counters) on {nr} reads of the workload",
+        "oracle_capped_searches_per_read": round(ct["capped"] / nr, 4),
+        "oracle_fallback_seeds_per_read": round(ct["fallback"] / nr, 4),
+        "GBs_over_seed_kernels": round(total / nr * n_seq / (r["kernel_ms"] / 1000) / 1e9, 1)}
+    if r.get("seeding"):
+        r["reference_algorithm"]["seeding_GBs_over_search_kernel"] = round(
+            seed_ref / nr * n_seq / (r["seeding"]["ms"] / 1000) / 1e9, 1)
+
+
 def measured_peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -1041,12 +1134,14 @@ def run_ours(args, rank, world, local):
     kms = (_lib.C.c_float * 4)()
     torch.cuda.synchronize()
     ev0.record(stream)
+    wave = []
     for _ in range(args.steps):
         step()
         _lib.lib.ma_ctx_kernel_ms(ctx.handle, kms)
         seed_ms.append(float(kms[1]))
         stage1_ms.append(float(kms[3]))
         other_ms.append((float(kms[0]), float(kms[2])))
+        wave.append(ctx.wave_ms())
     ev1.record(stream)
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1) / args.steps
@@ -1094,6 +1189,7 @@ def run_ours(args, rank, world, local):
                 ["occ_lines_32B", "kmer_loads", "sa_loads", "pac_sectors_32B", "backward_steps", "endpoints",
                  "loci_evaluated", "read_words", "endpoints_skipped", "stage2_reads", "stage2_groups",
                  "shift_evals"], tally)}}
+    roof.update(seeding_roofline(tally, wave))
     line = {"metric": METRIC, "value": round(value, 1), "unit": "reads/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
@@ -1118,6 +1214,7 @@ def run_ours(args, rank, world, local):
         _lib.check(_lib.lib.ma_bench_gather(ctx.handle, 64 << 20, 32, 1 << 30, _lib.C.byref(g)), ctx.handle)
         line["gather_roofline"]["l2_32B_GBs"] = round(g.value, 1)
         line["roofline"]["frac_of_gather32"] = round(achieved / line["gather_roofline"]["hbm_32B_GBs"], 4)
+        add_gather_fractions(line)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ix, o, n, rate, dt = time_oracle(prefix, rb, params, args.cpu_seconds)
         import oracle
@@ -1132,6 +1229,7 @@ def run_ours(args, rank, world, local):
             g = np.concatenate([g[:n], g[args.pairs:args.pairs + n]])
             bad += int((g != o[f]).sum())
         line["parity_sample"] = {"reads": 2 * n, "mismatched_fields": bad}
+        reference_algorithm_bytes(line, ix, rb.bases, rb.lens, rb.n1, True, READ_LEN, params, n_seq)
     if rank == 0 and world == 1 and args.bam_pairs > 0:
         line["stages"] = {"bam_pack": run_bam_stage(args, ctx, rb, res, local, peaks)}
         if args.sort_batches > 0:
@@ -1531,16 +1629,18 @@ def run_genome(args, rank, world, local):
 
     # ---- per-kernel times of the seed kernels (events around each kernel
     # group; one profiled step, not the timed one) ----
-    seed_ms = []
+    seed_ms, wave = [], []
     kms = (_lib.C.c_float * 4)()
     for _ in range(2):
-        sm = 0.0
+        sm, wv = 0.0, [0.0, 0.0, 0.0, 0.0]
         for a in range(0, n1, chunk):
             call(a, min(chunk, n1 - a))
             _lib.lib.ma_ctx_kernel_ms(ctx.handle, kms)
             sm += float(kms[1])
+            wv = [x + y for x, y in zip(wv, ctx.wave_ms())]
         seed_ms.append(sm)
-    seed_ms = seed_ms[1:]
+        wave.append(wv)
+    seed_ms, wave = seed_ms[1:], wave[1:]
     _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 0), ctx.handle)
 
     # ---- timed steps: the batched form over every read, each device call
@@ -1596,6 +1696,7 @@ def run_genome(args, rank, world, local):
                 ["occ_lines_32B", "kmer_loads", "sa_loads", "pac_sectors_32B", "backward_steps", "endpoints",
                  "loci_evaluated", "read_words", "endpoints_skipped", "stage2_reads", "stage2_groups",
                  "shift_evals"], tally)}}
+    roof.update(seeding_roofline(tally, wave))
 
     line = {"metric": METRIC, "value": round(value, 1), "unit": "reads/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",
@@ -1618,6 +1719,7 @@ def run_genome(args, rank, world, local):
             line["gather_roofline"][f"hbm_{lb}B_GBs"] = round(g.value, 1)
         line["roofline"]["frac_of_gather32"] = round(achieved / line["gather_roofline"]["hbm_32B_GBs"], 4)
         line["roofline"]["frac_of_gather64"] = round(achieved / line["gather_roofline"]["hbm_64B_GBs"], 4)
+        add_gather_fractions(line)
     if rank == 0 and world == 1 and not args.no_forms and not paired:
         del d_bases
         torch.cuda.empty_cache()
@@ -1636,7 +1738,7 @@ def run_genome(args, rank, world, local):
         else:
             b, l_ = bases_np[:n], lens_np[:n]
         t = time.perf_counter()
-        o = ix.map(b, l_, n, paired, max_len, 1, 2 if paired else 0, params.as_list(), counters=True)
+        o = ix.map(b, l_, n, paired, max_len, 1, 2 if paired else 0, params.as_list())
         dt = time.perf_counter() - t
         bad = 0
         for f in MapResult.FIELDS:
@@ -1644,21 +1746,12 @@ def run_genome(args, rank, world, local):
             g = np.concatenate([g[:n], g[n1:n1 + n]]) if paired else g[:n]
             bad += int((g.view(o[f].dtype) != o[f]).sum())
         nr = n * (2 if paired else 1)
-        ct = o["counters"]
-        line["parity_sample"] = {"reads": nr, "mismatched_fields": bad,
-                                 "oracle_capped_searches": int(ct["capped"]),
-                                 "oracle_fallback_seeds": int(ct["fallback"])}
+        line["parity_sample"] = {"reads": nr, "mismatched_fields": bad}
         line["cpu_baseline"] = {"value": round(nr / dt, 1), "unit": "reads/s", "cores": oracle.max_threads(),
                                 "kind": "port", "cpu": _cpu_model(),
                                 "sample": f"the parity sample ({nr} reads), {dt:.1f} s, index load {load_s:.1f} s"}
-        # the reference algorithm's bytes (64-B BWT lines per backward
-        # step, LF-walk lines, SA-sample and pac sectors, reads, outputs)
-        ref_bytes = (64 * (ct["occ_lines"] + ct["lf_lines"]) + 8 * ct["sa_loads"] + 32 * ct["pac_sectors"] +
-                     int(((l_.astype(np.int64) + 3) // 4).sum()) + 28 * nr)
-        seed_ref = 64 * (ct["occ_lines"] + ct["lf_lines"]) + 32 * ct["sa_loads"]
-        line["roofline"]["reference_algorithm_bytes_per_read"] = round(ref_bytes / nr, 1)
-        line["roofline"]["reference_seeding_bytes_per_read"] = round(seed_ref / nr, 1)
-        line["roofline"]["reference_algorithm_GBs"] = round(ref_bytes / nr * n_seq / (seed_avg_ms / 1000) / 1e9, 1)
+        reference_algorithm_bytes(line, ix, bases_np, lens_np, n1, paired, max_len, params, n_seq,
+                                  bs2=2 if paired else 0)
     bad = parity_failures(line)
     line["parity_failures"] = bad
     if rank == 0:

@@ -28,7 +28,7 @@ size_t two_stage_scratch_bytes(int64_t n_seq);
 size_t wavefront_scratch_bytes(int64_t n_seq, int loci_per_read);
 int launch_seed_wavefront(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int max_len,
                           const ma_tuning& t, int stage2_blocks, void* scratch, int sm_count, int* d_err,
-                          unsigned long long* d_tally, cudaStream_t st);
+                          unsigned long long* d_tally, WaveTimer* timer, cudaStream_t st);
 int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
                           int stage1_endpoints, int stage1_max_rows, int stage2_blocks, int level,
                           int first_wave, void* scratch, unsigned long long* d_tally, cudaEvent_t mid,
@@ -83,6 +83,8 @@ struct ma_ctx {
     int profiling = 0;           // bit 0: per-kernel events, bit 1: traffic tally
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // pack | stage 1 | stage 2 | rescue
     float kernel_ms[4] = {0, 0, 0, 0};  // pack, seed (both stages), rescue, stage 1 alone
+    WaveTimer wave_timer;              // per-round events of the wavefront form
+    float wave_ms[4] = {0, 0, 0, 0};   // search, eval, finalize (summed over rounds), rounds timed
     uint64_t traffic[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     bool rescue_ran = false;
     DevBuf tally;
@@ -249,7 +251,7 @@ void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const
                                                              : stage2_blocks_per_sm(level, d_tally != nullptr);
         launches += launch_seed_wavefront(idx->dix, R, P, out, static_cast<int>(max_len), ctx->tuning,
                                           bps * ctx->sm_count, seed_scratch->p, ctx->sm_count,
-                                          ctx->err_flag.as<int>(), d_tally, st);
+                                          ctx->err_flag.as<int>(), d_tally, timed ? &ctx->wave_timer : nullptr, st);
     } else {
         seed_scratch->ensure(two_stage_scratch_bytes(n_seq));
         const int bps = ctx->tuning.stage2_blocks_per_sm > 0 ? ctx->tuning.stage2_blocks_per_sm
@@ -358,6 +360,20 @@ void check_err_flag(ma_ctx* ctx, cudaStream_t st) {
         if (!ctx->rescue_ran) ctx->kernel_ms[2] = 0;
         ctx->kernel_ms[3] = ctx->kernel_ms[1];
         if (ctx->tuning.seed_kernel == 1) ck(cudaEventElapsedTime(&ctx->kernel_ms[3], ctx->ev[1], ctx->ev[4]), "elapsed");
+        for (float& v : ctx->wave_ms) v = 0;
+        if (ctx->tuning.seed_kernel == 2) {
+            const WaveTimer& w = ctx->wave_timer;
+            for (int k = 0; k < w.recorded; ++k) {
+                float a = 0, b = 0, c = 0;
+                ck(cudaEventElapsedTime(&a, w.e[3 * k], w.e[3 * k + 1]), "elapsed");
+                ck(cudaEventElapsedTime(&b, w.e[3 * k + 1], w.e[3 * k + 2]), "elapsed");
+                ck(cudaEventElapsedTime(&c, w.e[3 * k + 2], w.e[3 * k + 3]), "elapsed");
+                ctx->wave_ms[0] += a;
+                ctx->wave_ms[1] += b;
+                ctx->wave_ms[2] += c;
+            }
+            ctx->wave_ms[3] = w.complete ? static_cast<float>(w.recorded) : -static_cast<float>(w.recorded);
+        }
     }
     if (ctx->profiling & 2) {
         unsigned long long t[12];
@@ -415,6 +431,8 @@ void ma_ctx_destroy(ma_ctx* ctx) {
     cudaSetDevice(ctx->device);
     drop_graphs(ctx);
     for (cudaEvent_t& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : ctx->wave_timer.e)
         if (e) cudaEventDestroy(e);
     ctx->tally.release();
     ctx->seed_scratch.release();
@@ -1580,6 +1598,8 @@ int ma_ctx_set_profiling(ma_ctx* ctx, int flags) {
         use_device(ctx);
         if ((flags & 1) && !ctx->ev[0])
             for (cudaEvent_t& e : ctx->ev) ck(cudaEventCreate(&e), "cudaEventCreate");
+        if ((flags & 1) && !ctx->wave_timer.e[0])
+            for (cudaEvent_t& e : ctx->wave_timer.e) ck(cudaEventCreate(&e), "cudaEventCreate");
         ctx->profiling = flags;
     });
 }
@@ -1621,6 +1641,12 @@ int ma_ctx_get_pipeline(const ma_ctx* ctx, ma_pipeline* p) {
 int ma_ctx_get_tuning(const ma_ctx* ctx, ma_tuning* t) {
     if (!ctx || !t) return MA_ERR_ARG;
     *t = ctx->tuning;
+    return MA_OK;
+}
+
+int ma_ctx_wave_ms(const ma_ctx* ctx, float* out4) {
+    if (!ctx || !out4) return MA_ERR_ARG;
+    for (int i = 0; i < 4; ++i) out4[i] = ctx->wave_ms[i];
     return MA_OK;
 }
 

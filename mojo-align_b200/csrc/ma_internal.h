@@ -2,6 +2,8 @@
 // libmojoalign_b200.  Nothing here crosses the C ABI.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -74,6 +76,16 @@ struct BwtBuild {
 // fits the device).
 BwtBuild bwt_build_gpu(const std::vector<uint64_t>& text_words, uint64_t n, int sa_intv, uint64_t batch_limit,
                        int device);
+
+// Events around the kernels of each wavefront round (profiling): e[3k]
+// before round k's search, e[3k+1] before its eval, e[3k+2] before its
+// finalize, e[3R] after the last round (rounds past MAX_ROUNDS untimed).
+struct WaveTimer {
+    static constexpr int MAX_ROUNDS = 64;
+    cudaEvent_t e[3 * MAX_ROUNDS + 1] = {};
+    int recorded = 0;  // rounds timed in the last call
+    bool complete = true;
+};
 
 void build_index(const std::string& fasta, const std::string& out_prefix, bool bwameth_c2t,
                  int sa_intv, int device, uint64_t batch_limit = 0);

@@ -43,7 +43,7 @@ size_t two_stage_scratch_bytes(int64_t n_seq);
 size_t wavefront_scratch_bytes(int64_t n_seq, int loci_per_read);
 int launch_seed_wavefront(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int max_len,
                           const ma_tuning& t, int stage2_blocks, void* scratch, int sm_count, int* d_err,
-                          unsigned long long* d_tally, cudaStream_t st);
+                          unsigned long long* d_tally, WaveTimer* timer, cudaStream_t st);
 int launch_seed_two_stage(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out,
                           int stage1_endpoints, int stage1_max_rows, int stage2_blocks, int level,
                           int first_wave, void* scratch, unsigned long long* d_tally, cudaEvent_t mid,
@@ -353,7 +353,7 @@ void issue_group(ma_server* s, Group& g) {
                               t.stage2_first_wave, dev + g.L.scratch, nullptr, nullptr, st);
     } else if (s->seed_kernel() == 2) {
         launch_seed_wavefront(*s->dix, R, P, o, 32 * g.words, t, bps * s->sm_count, dev + g.L.scratch, s->sm_count,
-                              d_err, nullptr, st);
+                              d_err, nullptr, nullptr, st);
     } else {
         launch_seed_extend(*s->dix, R, P, o, nullptr, t.reg_level, st);
     }

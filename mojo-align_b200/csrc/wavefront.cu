@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include "ma_device.cuh"
+#include "ma_internal.h"
 #include "seed_core.cuh"
 
 namespace ma {
@@ -456,7 +457,7 @@ int grid_blocks(K kernel, int sm_count) {
 template <bool S, int MS, int ME>
 int launch_rounds(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, const Wave& w,
                   int max_len, int w0, int wn, int max_rounds, int growth, int sm_count, int* d_err,
-                  unsigned long long* tally, cudaStream_t st) {
+                  unsigned long long* tally, WaveTimer* timer, cudaStream_t st) {
     const int n_end_max = endpoint_count_host(P, max_len);
     // round widths: w0, then wn (doubling from the third round with growth)
     int widths[1100];
@@ -482,11 +483,21 @@ int launch_rounds(const DevIndex& ix, const DevReads& R, const DevParams& P, con
             wf_round_begin_kernel<<<1, 1, 0, st>>>(w);
             ++launches;
         }
+        const bool timed = timer && k < WaveTimer::MAX_ROUNDS;
+        if (timed) cudaEventRecord(timer->e[3 * k], st);
         wf_search_kernel<S, MS><<<g_search, 256, 0, st>>>(ix, R, P, w, act, width, tally);
+        if (timed) cudaEventRecord(timer->e[3 * k + 1], st);
         wf_eval_kernel<S, ME><<<g_eval, 256, 0, st>>>(ix, R, P, w, tally);
+        if (timed) cudaEventRecord(timer->e[3 * k + 2], st);
         wf_finalize_kernel<S><<<g_fin, 256, 0, st>>>(ix, R, P, out, w, act, nxt, width, k == rounds - 1, d_err,
                                                      tally);
         launches += 3;
+    }
+    if (timer) {
+        const int timed = rounds < WaveTimer::MAX_ROUNDS ? rounds : WaveTimer::MAX_ROUNDS;
+        cudaEventRecord(timer->e[3 * timed], st);
+        timer->recorded = timed;
+        timer->complete = rounds <= WaveTimer::MAX_ROUNDS;
     }
     return launches;
 }
@@ -502,7 +513,7 @@ size_t wavefront_scratch_bytes(int64_t n_seq, int loci_per_read) {
 // the number of kernel launches.
 int launch_seed_wavefront(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, int max_len,
                           const ma_tuning& t, int stage2_blocks, void* scratch, int sm_count, int* d_err,
-                          unsigned long long* d_tally, cudaStream_t st) {
+                          unsigned long long* d_tally, WaveTimer* timer, cudaStream_t st) {
     Wave w;
     wave_layout(static_cast<char*>(scratch), R.n_seq, locus_capacity(R.n_seq, t.wave_loci_per_read), &w);
     const int w0 = t.stage1_endpoints > 0 ? t.stage1_endpoints : 1;
@@ -510,13 +521,13 @@ int launch_seed_wavefront(const DevIndex& ix, const DevReads& R, const DevParams
     int launches = 0;
     const int mr = t.wave_max_rounds, gr = t.wave_growth;
     if (d_tally)
-        launches = launch_rounds<true, 1, 1>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, d_tally, st);
+        launches = launch_rounds<true, 1, 1>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, d_tally, timer, st);
     else if (t.reg_level == 1)
-        launches = launch_rounds<false, 5, 4>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, nullptr, st);
+        launches = launch_rounds<false, 5, 4>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, nullptr, timer, st);
     else if (t.reg_level == 2)
-        launches = launch_rounds<false, 6, 5>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, nullptr, st);
+        launches = launch_rounds<false, 6, 5>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, nullptr, timer, st);
     else
-        launches = launch_rounds<false, 1, 1>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, nullptr, st);
+        launches = launch_rounds<false, 1, 1>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, nullptr, timer, st);
     // reads that overflowed the locus list or outlived the rounds
     launches += launch_stage2_pending(ix, R, P, out, w.best_key, w.memo, w.memo_n, w.resume, w.pending,
                                       w.counters + C_HANDOFF, stage2_blocks, t.reg_level, 32, d_tally, st);

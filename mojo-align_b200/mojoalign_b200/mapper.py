@@ -82,6 +82,13 @@ class GpuContext:
         check(lib.ma_ctx_kernel_ms(self.handle, v), self.handle)
         return list(v)
 
+    def wave_ms(self) -> list[float]:
+        """Wavefront search, eval, finalize ms of the last profiled call and
+        the rounds timed (see ma_ctx_wave_ms)."""
+        v = (C.c_float * 4)()
+        check(lib.ma_ctx_wave_ms(self.handle, v), self.handle)
+        return list(v)
+
     def traffic(self) -> list[int]:
         v = (C.c_uint64 * 12)()
         check(lib.ma_ctx_traffic(self.handle, v), self.handle)
