@@ -137,28 +137,57 @@ BwaIndexHost load_bwa_index(const std::string& prefix) {
 }
 
 std::vector<FastaRecord> read_fasta(const std::string& path) {
-    std::ifstream f(path);
-    if (!f) fail(MA_ERR_IO, "cannot open FASTA " + path);
+    // the whole file in memory, lines split with memchr; sequence lines are
+    // appended a line at a time (blanks and tabs inside them dropped)
+    FILE* fp = std::fopen(path.c_str(), "rb");
+    if (!fp) fail(MA_ERR_IO, "cannot open FASTA " + path);
+    std::fseek(fp, 0, SEEK_END);
+    const long size = std::ftell(fp);
+    std::fseek(fp, 0, SEEK_SET);
+    std::string text(size > 0 ? static_cast<size_t>(size) : 0, '\0');
+    if (size > 0 && std::fread(&text[0], 1, text.size(), fp) != text.size()) {
+        std::fclose(fp);
+        fail(MA_ERR_IO, "short read of " + path);
+    }
+    std::fclose(fp);
     std::vector<FastaRecord> recs;
-    std::string line;
-    while (std::getline(f, line)) {
-        if (!line.empty() && line.back() == '\r') line.pop_back();
-        if (line.empty()) continue;
-        if (line[0] == '>') {
-            FastaRecord r;
-            size_t sp = line.find_first_of(" \t", 1);
-            r.name = line.substr(1, sp == std::string::npos ? std::string::npos : sp - 1);
-            if (sp != std::string::npos) {
-                size_t st = line.find_first_not_of(" \t", sp);
-                if (st != std::string::npos) r.anno = line.substr(st);
+    const char* p = text.data();
+    const char* end = p + text.size();
+    // sequence bytes of each record, for one reserve() per record
+    while (p < end) {
+        const char* nl = static_cast<const char*>(std::memchr(p, '\n', static_cast<size_t>(end - p)));
+        const char* le = nl ? nl : end;
+        const char* lend = le;
+        if (lend > p && lend[-1] == '\r') --lend;
+        if (lend > p) {
+            if (*p == '>') {
+                std::string line(p, lend);
+                FastaRecord r;
+                size_t sp = line.find_first_of(" \t", 1);
+                r.name = line.substr(1, sp == std::string::npos ? std::string::npos : sp - 1);
+                if (sp != std::string::npos) {
+                    size_t st = line.find_first_not_of(" \t", sp);
+                    if (st != std::string::npos) r.anno = line.substr(st);
+                }
+                if (r.name.empty()) fail(MA_ERR_FORMAT, "FASTA record without a name in " + path);
+                // room for the record's bases: up to the next header
+                const char* nh = static_cast<const char*>(std::memchr(le, '>', static_cast<size_t>(end - le)));
+                r.seq.reserve(static_cast<size_t>((nh ? nh : end) - le));
+                recs.push_back(std::move(r));
+            } else {
+                if (recs.empty()) fail(MA_ERR_FORMAT, "FASTA sequence before the first header in " + path);
+                std::string& q = recs.back().seq;
+                const char* a = p;
+                for (const char* c = p; c < lend; ++c) {
+                    if (*c == ' ' || *c == '\t') {
+                        q.append(a, c);
+                        a = c + 1;
+                    }
+                }
+                q.append(a, lend);
             }
-            if (r.name.empty()) fail(MA_ERR_FORMAT, "FASTA record without a name in " + path);
-            recs.push_back(std::move(r));
-        } else {
-            if (recs.empty()) fail(MA_ERR_FORMAT, "FASTA sequence before the first header in " + path);
-            for (char ch : line)
-                if (ch != ' ' && ch != '\t') recs.back().seq.push_back(ch);
         }
+        p = nl ? nl + 1 : end;
     }
     if (recs.empty()) fail(MA_ERR_FORMAT, "empty FASTA " + path);
     return recs;
@@ -196,8 +225,12 @@ std::vector<FastaRecord> bwameth_convert(const std::vector<FastaRecord>& in) {
 }
 
 void write_fasta(const std::string& path, const std::vector<FastaRecord>& recs) {
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) fail(MA_ERR_IO, "cannot write " + path);
     std::string buf;
-    for (const auto& r : recs) {
+    for (const auto& r : recs) {  // one record's text at a time
+        buf.clear();
+        buf.reserve(r.seq.size() + r.seq.size() / 80 + r.name.size() + r.anno.size() + 8);
         buf += ">" + r.name;
         if (!r.anno.empty()) buf += " " + r.anno;
         buf += "\n";
@@ -205,8 +238,12 @@ void write_fasta(const std::string& path, const std::vector<FastaRecord>& recs) 
             buf.append(r.seq, i, std::min<size_t>(80, r.seq.size() - i));
             buf += "\n";
         }
+        if (std::fwrite(buf.data(), 1, buf.size(), f) != buf.size()) {
+            std::fclose(f);
+            fail(MA_ERR_IO, "short write of " + path);
+        }
     }
-    write_all(path, buf.data(), buf.size());
+    if (std::fclose(f) != 0) fail(MA_ERR_IO, "close failed for " + path);
 }
 
 }  // namespace
