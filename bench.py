@@ -100,7 +100,8 @@ def parse_args():
                     "(0 = the workload's)")
     ap.add_argument("--genome-chunk", type=int, default=25_000_000, help="reads per device call")
     ap.add_argument("--parity-reads", type=int, default=1_000_000, help="reads checked against the oracle")
-    ap.add_argument("--serve-stream-budget-mb", type=int, default=1536, help="HBM budget of the served stream")
+    ap.add_argument("--serve-stream-budget-mb", type=int, default=512, help="HBM budget of the served stream "
+                    "(below what max_inflight groups need, so that admission waits)")
     ap.add_argument("--gather-sweep", action="store_true", help="print the measured random-gather roofline "
                     "(32- and 64-byte lines, 16 MiB to 32 GiB buffers) as one JSON object and exit")
     ap.add_argument("--prepare-sample", default="", help=argparse.SUPPRESS)

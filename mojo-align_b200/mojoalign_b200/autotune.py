@@ -6,6 +6,12 @@ covers, the round width, the seed kernels' register budget and the
 persistent stage-2 grid, on a sample batch.  Every candidate must produce
 identical outputs (checked here); the fastest by device time wins.
 
+In the wavefront form a round gives every active read `wave_endpoints`
+search threads, so the round width is the warps-per-read choice: 4, 8 and
+16 endpoints pack 8, 4 and 2 reads per warp (64, 32, 16 reads per 256-thread
+CTA), 32, 64 and 128 endpoints give each read 1, 2 and 4 warps (8, 4 and 2
+reads per CTA).  The stage-2 warps take one read each.
+
 The seed stride is not swept: it decides which right endpoints are tried
 (linear_gpu_fm.mojo:1828) and so changes results.
 """
@@ -29,6 +35,9 @@ DEFAULT_CANDIDATES = [
     (2, 1, 0, 0, 1, 1, 4, 4, 0, 1),
     (2, 1, 0, 1, 1, 1, 4, 4, 0, 1),
     (2, 2, 0, 1, 1, 1, 8, 4, 0, 1),
+    (2, 1, 0, 1, 1, 1, 32, 4, 0, 0),   # one warp per read and round
+    (2, 1, 0, 1, 1, 1, 64, 4, 0, 0),   # two warps per read
+    (2, 1, 0, 1, 1, 1, 128, 4, 0, 0),  # four warps per read
 ]
 FIELDS = ("seed_kernel", "stage1_endpoints", "stage2_blocks_per_sm", "reg_level", "stage1_max_rows",
           "stage2_first_wave", "wave_endpoints", "wave_loci_per_read", "wave_max_rounds", "wave_growth")
