@@ -8,13 +8,15 @@
 //   1. one pass counts the suffixes of every bucket; consecutive buckets are
 //      grouped into batches of at most `batch` suffixes;
 //   2. per batch, one pass over the text selects the batch's suffixes with
-//      a 64-bit key (their first 31 symbols, past the end reading as the
-//      smallest symbol, and a low 1 bit), sorted by a radix sort;
-//   3. suffixes with equal keys are refined 31 symbols deeper at a time:
-//      a refinement key is the next 31 symbols, or 0 once the suffix has
-//      ended (an ended suffix is smaller than any suffix it is a prefix
-//      of), ordered within the tie group by a second, stable sort on the
-//      group; groups shrink until no two keys are equal;
+//      a 64-bit key (their first 29 symbols, past the end reading as the
+//      smallest symbol, then how many of the 29 are real, 0..29), sorted by
+//      a radix sort: of two suffixes whose windows read alike, the one that
+//      ends sooner is smaller, as with the sentinel;
+//   3. suffixes with equal keys are refined 29 symbols deeper at a time
+//      (a suffix that has ended has key 0), ordered within the tie group by
+//      a second, stable sort on the group; groups shrink until no two keys
+//      are equal (two suffixes still tied have the same symbols and the same
+//      length so far, so they part before either ends);
 //   4. the batch's rows get their BWT symbol (2 bits per row) and, every
 //      sa_intv rows, their SA sample.
 // Then the bwa .bwt layout (128-position blocks of counts + 8 words, most
@@ -34,7 +36,7 @@ namespace ma {
 namespace {
 
 constexpr int BUCKET_SYMS = 10;  // batching buckets: 4^10
-constexpr int KEY_SYMS = 31;     // symbols per sort key
+constexpr int KEY_SYMS = 29;     // symbols per sort key
 constexpr uint64_t EVEN = 0x5555555555555555ull;
 
 void ck(cudaError_t e, const char* what) {
@@ -52,17 +54,20 @@ __device__ __forceinline__ uint64_t reverse_fields(uint64_t x) {
     return ((y >> 1) & EVEN) | ((y & EVEN) << 1);
 }
 
-// Key of the suffix at i: symbols i .. i+30 (first symbol most significant,
-// 2 bits each; past the end of the text they read as 0), then a 1 bit.  A
-// position at or past the end (an ended suffix) has key 0.  T holds the
-// text LSB first, 32 symbols per word, zero past n, one spare word.
+// Key of the suffix at i: symbols i .. i+28 in bits 63..6 (first symbol
+// most significant, 2 bits each; past the end of the text they read as 0),
+// bit 5 zero, and in bits 4..0 how many of the 29 are in the text
+// (min(n - i, 29)).  A position at or past the end (an ended suffix) has
+// key 0.  T holds the text LSB first, 32 symbols per word, zero past n, one
+// spare word.
 __device__ __forceinline__ uint64_t suffix_key(const uint64_t* __restrict__ T, uint64_t n, uint64_t i) {
     if (i >= n) return 0;
     const uint64_t w = i >> 5;
     const int sh = static_cast<int>(i & 31) * 2;
     const uint64_t lo = __ldg(T + w), hi = __ldg(T + w + 1);
     const uint64_t win = sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
-    return (reverse_fields(win) & ~3ull) | 1ull;
+    const uint64_t real = n - i < KEY_SYMS ? n - i : KEY_SYMS;
+    return (reverse_fields(win) & ~((1ull << 6) - 1)) | real;
 }
 
 __device__ __forceinline__ uint32_t bucket_of(uint64_t key) {
@@ -385,7 +390,7 @@ BwtBuild bwt_build_gpu(const std::vector<uint64_t>& text_words, uint64_t n, int 
             ck(cub::DeviceRadixSort::SortPairs(temp, tb, kk, pp, mi, 0, 64, st), "sort");
             uint64_t* key = kk.Current();
             uint64_t* pos = pp.Current();
-            // refinement of ties, 31 symbols deeper per round
+            // refinement of ties, 29 symbols deeper per round
             tie_flag_kernel<<<grid_of(cnt), 256, 0, st>>>(key, mi, flag);
             ck(cub::DeviceSelect::Flagged(temp, tb, cub::CountingInputIterator<uint32_t>(0), flag, U, d_small + 2,
                                           mi, st), "select ties");
