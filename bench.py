@@ -1498,9 +1498,20 @@ GENOME_WORKLOADS = {
 }
 
 
-def genome_config(args, spec) -> dict:
+def host_capped_reads(n1: int, bytes_per_unit: int, world: int) -> int:
+    """n1, or fewer when `world` ranks' pinned reads would take more than
+    half of the host's memory."""
+    try:
+        total = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES")
+    except (ValueError, OSError):
+        return n1
+    cap = int(total // 2 // max(1, world) // bytes_per_unit)
+    return max(1, min(n1, cap))
+
+
+def genome_config(args, spec, n1: int | None = None) -> dict:
     mb = args.genome_mb_large or spec["genome_mb"]
-    n1 = args.genome_reads or spec["n1"]
+    n1 = n1 or args.genome_reads or spec["n1"]
     n_seq = n1 * (2 if spec["paired"] else 1)
     return {"workload": spec["text"].format(n1=n1, mb=mb), "form": "batched (one device call per chunk)",
             "genome_bp": mb * 1_000_000, "reads_per_gpu": n_seq, "paired": spec["paired"],
@@ -1523,7 +1534,11 @@ def run_genome(args, rank, world, local):
     mb = args.genome_mb_large or spec["genome_mb"]
     n1 = args.genome_reads or spec["n1"]
     paired, max_len = spec["paired"], spec["max_len"]
-    n_seq = n1 * (2 if paired else 1)
+    per = 2 if paired else 1
+    # every rank's reads stay pinned on the host: with several ranks on one
+    # node, at most half of the host memory goes to them
+    n1 = host_capped_reads(n1, per * max_len, world)
+    n_seq = n1 * per
     bs1, bs2 = spec["bs"]
     dev = f"cuda:{local}"
     timings = {}
@@ -1531,16 +1546,21 @@ def run_genome(args, rank, world, local):
     fa, prefix, timings["reference_and_index"] = prepare_reference(
         args, rank, dist, local, genome_mb=mb, repeats=synth.RepeatModel() if spec["repeats"] else None,
         tag="_repeats" if spec["repeats"] else "")
-    t = time.time()
-    pinned = torch.empty((n_seq, max_len), dtype=torch.uint8, pin_memory=True)
-    rb = synth.simulate_reads(fa, synth.ReadModel(**spec["model"]), n1, paired, max_len, seed=shard_seed(rank),
-                              bases_out=pinned.numpy())
-    timings["reads"] = time.time() - t
+    # the ranks of a node simulate their reads and open the index one after
+    # another (each step holds several GB of host memory for a while)
+    for turn in range(world):
+        if turn == rank:
+            t = time.time()
+            pinned = torch.empty((n_seq, max_len), dtype=torch.uint8, pin_memory=True)
+            rb = synth.simulate_reads(fa, synth.ReadModel(**spec["model"]), n1, paired, max_len,
+                                      seed=shard_seed(rank), bases_out=pinned.numpy())
+            timings["reads"] = time.time() - t
+            ctx = GpuContext(local)
+            t = time.time()
+            gi = GpuIndex(ctx, prefix, kmer_k=args.kmer, kmer3_k=args.kmer3)
+            timings["index_open"] = time.time() - t
+        dist.barrier()
     bases_np, lens_np = pinned.numpy(), rb.lens
-    ctx = GpuContext(local)
-    t = time.time()
-    gi = GpuIndex(ctx, prefix, kmer_k=args.kmer, kmer3_k=args.kmer3)
-    timings["index_open"] = time.time() - t
 
     # one stream for the torch copies and the library's calls (the calls
     # launch on the stream they are given), so that they stay ordered
@@ -1702,7 +1722,7 @@ def run_genome(args, rank, world, local):
     line = {"metric": METRIC, "value": round(value, 1), "unit": "reads/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": genome_config(args, spec),
+            "config": genome_config(args, spec, n1),
             "run": {"tuning": tune.tuning, "autotune": tune.all_ms, "kmer_k": args.kmer, "kmer3_k": args.kmer3,
                     "index_hbm_bytes": int(gi.info.device_bytes), "calls_per_step": -(-n1 // chunk),
                     "cuda_graphs": "each device call replays its captured graph (one host launch per call)",
