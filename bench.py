@@ -1474,6 +1474,7 @@ def run_forms(args, ctx, gi, params, fa, local, best_tuning):
         "samples": "8 (CpG retention 0.4-0.9; fixed 150 / lognormal 120 / lognormal 90 length profiles), "
                    f"pools of {args.serve_pool} reads, request sizes log-uniform 1k-2M reads"}
     forms["served_over_plain_1launch"] = round(same_reads_rate / plain_rate, 3)
+    forms["served_over_batched_1call"] = round(same_reads_rate / batched_rate, 3)
     forms["served_over_plain_reference_batches"] = round(same_reads_rate / ref_rate, 3)
     forms["batched_over_plain_1launch"] = round(batched_rate / plain_rate, 3)
     del d_bases, d_lens, pools
