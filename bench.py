@@ -56,6 +56,15 @@ SEED_KERNELS = {
 READ_LEN = 150
 
 
+_T0 = time.time()
+
+
+def log(msg: str) -> None:
+    """One progress line on stderr (the JSON line alone goes to stdout)."""
+    sys.stderr.write(f"[bench +{time.time() - _T0:7.1f}s] {msg}\n")
+    sys.stderr.flush()
+
+
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -191,9 +200,12 @@ def prepare_reference(args, rank, dist: Dist, device: int, genome_mb: int | None
         except ImportError:
             device = -1
         n_contigs = max(1, min(24, genome_mb // 50))
+        log(f"synthetic reference: {genome_mb} Mbp")
         synth.write_reference_model(fa, genome_mb * 1_000_000, n_contigs=n_contigs, gc=0.41, cpg=0.01, seed=0,
                                     repeats=repeats)
+        log("index build")
         build_index(fa, prefix, bwameth_c2t=True, sa_intv=32, device=device)
+        log("index built")
         done.write_text("ok\n")
     dist.barrier()
     return fa, prefix, time.time() - t0
@@ -1060,14 +1072,17 @@ def run_ours(args, rank, world, local):
     n_seq = 2 * args.pairs
     pinned = torch.empty((n_seq, READ_LEN), dtype=torch.uint8, pin_memory=True)
     t = time.time()
+    log("reads")
     rb = simulate(args, fa, rank, bases_out=pinned.numpy())
     sim_s = time.time() - t
     lens_pinned = torch.from_numpy(rb.lens.view(np.int32)).pin_memory()
 
     ctx = GpuContext(local)
     t = time.time()
+    log("index open")
     gi = GpuIndex(ctx, prefix, kmer_k=args.kmer, kmer3_k=args.kmer3)
     open_s = time.time() - t
+    log("autotune")
 
     # ---- result-neutral kernel choices picked on a sample of the batch ----
     from mojoalign_b200.autotune import autotune
@@ -1116,6 +1131,7 @@ def run_ours(args, rank, world, local):
         map_batch_device(ctx, gi, d_bases.data_ptr(), d_lens.data_ptr(), args.pairs, True, READ_LEN, out_ptrs,
                          "C2T", "G2A", params, stream=stream.cuda_stream)
 
+    log(f"tuning {tune.tuning}; counting pass")
     # traffic accounting: one untimed pass of the counting kernel
     _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 2), ctx.handle)
     step()
@@ -1124,6 +1140,7 @@ def run_ours(args, rank, world, local):
     tally = list(tally)
     _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 1), ctx.handle)
 
+    log("timed steps")
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -1152,6 +1169,7 @@ def run_ours(args, rank, world, local):
     ms_max = dist.max(ms)
     value = aggregate_reads_per_s(n_seq, world, ms_max)
 
+    log("end to end")
     # ---- end to end through the host API (pinned host in, host out) ----
     _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 0), ctx.handle)  # per-chunk timing would serialise
     host_out = MapResult.empty(n_seq, debug=False)
@@ -1217,6 +1235,7 @@ def run_ours(args, rank, world, local):
         line["roofline"]["frac_of_gather32"] = round(achieved / line["gather_roofline"]["hbm_32B_GBs"], 4)
         add_gather_fractions(line)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        log("oracle sample")
         ix, o, n, rate, dt = time_oracle(prefix, rb, params, args.cpu_seconds)
         import oracle
 
@@ -1232,24 +1251,30 @@ def run_ours(args, rank, world, local):
         line["parity_sample"] = {"reads": 2 * n, "mismatched_fields": bad}
         reference_algorithm_bytes(line, ix, rb.bases, rb.lens, rb.n1, True, READ_LEN, params, n_seq)
     if rank == 0 and world == 1 and args.bam_pairs > 0:
+        log("stage: BAM pack")
         line["stages"] = {"bam_pack": run_bam_stage(args, ctx, rb, res, local, peaks)}
         if args.sort_batches > 0:
             torch.cuda.empty_cache()
+            log("stage: sort")
             line["stages"]["sort_markdup_gather"] = run_sort_stage(args, ctx, rb, res, local, peaks)
             if args.bgzf_level >= 0 and getattr(args, "_sorted_stream", None) is not None:
                 torch.cuda.empty_cache()
+                log("stage: BGZF")
                 line["stages"]["bgzf"] = run_bgzf_stage(args, ctx, args._sorted_stream, local, peaks)
                 del args._sorted_stream
     if rank == 0 and world == 1 and args.fq2bam_pairs > 0:
         torch.cuda.empty_cache()
         args._prefix = prefix
+        log("stage: FASTQ -> BAM")
         line.setdefault("stages", {})["fq2bam"] = run_fq2bam_stage(args, ctx, gi, rb, local, params)
     if rank == 0 and world == 1 and args.fq2sam_pairs > 0:
         torch.cuda.empty_cache()
         args._prefix = prefix
+        log("stage: FASTQ -> SAM")
         line.setdefault("stages", {})["fq2sam"] = run_fq2sam_stage(args, ctx, gi, rb, local, params, peaks)
     if rank == 0 and world == 1 and args.fastq_pairs > 0:
         torch.cuda.empty_cache()
+        log("stage: FASTQ split")
         line.setdefault("stages", {})["fastq_split"] = run_fastq_stage(args, ctx, rb, local, peaks)
     if rank == 0 and world == 1 and not args.no_forms:
         from mojoalign_b200.autotune import FIELDS as TFIELDS
@@ -1257,6 +1282,7 @@ def run_ours(args, rank, world, local):
         best = tuple(tune.tuning[f] for f in TFIELDS if f in tune.tuning)
         del d_bases, d_lens, d_out
         torch.cuda.empty_cache()
+        log("forms")
         line["forms"] = run_forms(args, ctx, gi, params, fa, local, best)
     bad = parity_failures(line)
     line["parity_failures"] = bad
@@ -1553,8 +1579,10 @@ def run_genome(args, rank, world, local):
         if turn == rank:
             t = time.time()
             pinned = torch.empty((n_seq, max_len), dtype=torch.uint8, pin_memory=True)
+            log(f"reads: {n1} x {per}")
             rb = synth.simulate_reads(fa, synth.ReadModel(**spec["model"]), n1, paired, max_len,
                                       seed=shard_seed(rank), bases_out=pinned.numpy())
+            log("index open")
             timings["reads"] = time.time() - t
             ctx = GpuContext(local)
             t = time.time()
@@ -1610,6 +1638,7 @@ def run_genome(args, rank, world, local):
     from mojoalign_b200.autotune import TuneResult, autotune
 
     ns = min(n1, 1_000_000 if paired else 2_000_000)
+    log("autotune")
     if args.tuning:
         fixed = [int(x) for x in args.tuning.split(",")]
         fixed += [2, 1, 0, 2, 1, 1, 8, 4, 0, 1][len(fixed):]
@@ -1639,6 +1668,7 @@ def run_genome(args, rank, world, local):
         del d_sb, d_sl, s_out, s_dbg, sb, sl
     best = tuple(tune.tuning[f] for f in TFIELDS if f in tune.tuning)
 
+    log(f"tuning {tune.tuning}; counting pass")
     # ---- traffic tally: one untimed pass of the counting kernels ----
     _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 2), ctx.handle)
     tally = [0] * 12
@@ -1665,6 +1695,7 @@ def run_genome(args, rank, world, local):
     seed_ms, wave = seed_ms[1:], wave[1:]
     _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 0), ctx.handle)
 
+    log("timed steps")
     # ---- timed steps: the batched form over every read, each device call
     # replayed from its captured CUDA graph ----
     ctx.set_graphs(True)
@@ -1692,6 +1723,7 @@ def run_genome(args, rank, world, local):
     value = aggregate_reads_per_s(n_seq, world, ms_max)
     batched_out = {f: x.cpu().numpy() for f, x in d_out.items()}
 
+    log("end to end")
     # ---- end to end from pinned host buffers (copies inside) ----
     _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 0), ctx.handle)
     res = MapResult.empty(n_seq, debug=False)
@@ -1745,11 +1777,13 @@ def run_genome(args, rank, world, local):
     if rank == 0 and world == 1 and not args.no_forms and not paired:
         del d_bases
         torch.cuda.empty_cache()
+        log("forms")
         line["forms"] = genome_forms(args, ctx, gi, params, fa, local, best, bases_np, lens_np, n1, max_len,
                                      batched_out, value, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle
 
+        log("oracle sample")
         t = time.perf_counter()
         ix = oracle.OracleIndex(prefix)
         load_s = time.perf_counter() - t
@@ -1881,6 +1915,7 @@ def genome_forms(args, ctx, gi, params, fa, local, best, bases_np, lens_np, n, m
         a = int(rng.integers(0, args.serve_pool - size + 1))
         return b[a:a + size], l[a:a + size], size, ml
 
+    log("served stream")
     budget = args.serve_stream_budget_mb << 20
     with Server(ctx, gi, hbm_budget_bytes=budget, max_group_pairs=group, max_inflight=3) as srv:
         def burst(count):
