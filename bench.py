@@ -107,7 +107,8 @@ def parse_args():
                     "(0 = 3100)")
     ap.add_argument("--genome-reads", type=int, default=0, help="reads (pairs) of the genome workloads "
                     "(0 = the workload's)")
-    ap.add_argument("--genome-chunk", type=int, default=25_000_000, help="reads per device call")
+    ap.add_argument("--genome-chunk", type=int, default=8_000_000, help="reads per device call (the wavefront "
+                    "locus list of a call holds at most 2^27 loci: smaller calls leave room for more loci per read)")
     ap.add_argument("--parity-reads", type=int, default=1_000_000, help="reads checked against the oracle")
     ap.add_argument("--serve-stream-budget-mb", type=int, default=512, help="HBM budget of the served stream "
                     "(below what max_inflight groups need, so that admission waits)")
@@ -729,9 +730,13 @@ def run_fq2bam_stage(args, ctx, gi, rb, local, params):
 
 
 def gzip_content(path) -> bytes:
-    import gzip
+    """The inflated content of a BGZF file, its members inflated on a host
+    thread pool (gzip.decompress copies the rest of the buffer for every
+    member, quadratic in the member count)."""
+    from mojoalign_b200.fqio import BgzfReader
 
-    return gzip.decompress(Path(path).read_bytes())
+    with BgzfReader(str(path)) as fh:
+        return fh.read()
 
 
 def run_fq2sam_stage(args, ctx, gi, rb, local, params, peaks):
@@ -997,20 +1002,28 @@ def parity_failures(obj, path="") -> list:
     return bad
 
 
-def seeding_roofline(tally, wave) -> dict:
-    """The seeding kernels alone (wavefront search: k-mer table, Occ and SA
-    gathers) from the counting pass's tally and the per-round search times."""
+def seeding_roofline(tally, wave, tally2=None, n_seq=0) -> dict:
+    """The seeding kernel alone (wavefront search: k-mer table, Occ and SA
+    gathers) from the counting pass's tallies (the rounds' part: the
+    stage-2 warps' tallies, tally2, taken out) and the per-round search
+    times; the stage-2 warps reported beside it."""
     if not wave or not any(w[0] for w in wave):
         return {}
+    tally2 = tally2 or [0] * 12
     search_ms = statistics.mean(w[0] for w in wave)
-    seed_bytes = 32 * (tally[0] + tally[1] + tally[2])
-    return {"seeding": {"kernel": "wf_search_kernel (all rounds)", "ms": round(search_ms, 3),
-                        "eval_ms": round(statistics.mean(w[1] for w in wave), 3),
-                        "finalize_ms": round(statistics.mean(w[2] for w in wave), 3),
-                        "alg_bytes": int(seed_bytes),
-                        "alg": "32-B sectors of the Occ lines, k-mer table entries and SA entries the search "
-                               "gathers (this implementation's accesses)",
-                        "achieved_GBs": round(seed_bytes / (search_ms / 1000) / 1e9, 1)}}
+    seed_bytes = 32 * sum(tally[i] - tally2[i] for i in range(3))
+    out = {"seeding": {"kernel": "wf_search_kernel (all rounds)", "ms": round(search_ms, 3),
+                       "eval_ms": round(statistics.mean(w[1] for w in wave), 3),
+                       "finalize_ms": round(statistics.mean(w[2] for w in wave), 3),
+                       "alg_bytes": int(seed_bytes),
+                       "alg": "32-B sectors of the Occ lines, k-mer table entries and SA entries the rounds' "
+                              "search gathers (this implementation's accesses)",
+                       "achieved_GBs": round(seed_bytes / (search_ms / 1000) / 1e9, 1)}}
+    if len(wave[0]) > 4:
+        out["seeding"]["stage2_ms"] = round(statistics.mean(w[4] for w in wave), 3)
+        if n_seq:
+            out["seeding"]["stage2_reads_per_read"] = round(tally2[9] / n_seq, 4)
+    return out
 
 
 def add_gather_fractions(line) -> None:
@@ -1138,6 +1151,7 @@ def run_ours(args, rank, world, local):
     tally = (_lib.C.c_uint64 * 12)()
     _lib.lib.ma_ctx_traffic(ctx.handle, tally)
     tally = list(tally)
+    tally2 = ctx.traffic_stage2()
     _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 1), ctx.handle)
 
     log("timed steps")
@@ -1208,7 +1222,7 @@ def run_ours(args, rank, world, local):
                 ["occ_lines_32B", "kmer_loads", "sa_loads", "pac_sectors_32B", "backward_steps", "endpoints",
                  "loci_evaluated", "read_words", "endpoints_skipped", "stage2_reads", "stage2_groups",
                  "shift_evals"], tally)}}
-    roof.update(seeding_roofline(tally, wave))
+    roof.update(seeding_roofline(tally, wave, tally2, n_seq))
     line = {"metric": METRIC, "value": round(value, 1), "unit": "reads/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
@@ -1671,12 +1685,13 @@ def run_genome(args, rank, world, local):
     log(f"tuning {tune.tuning}; counting pass")
     # ---- traffic tally: one untimed pass of the counting kernels ----
     _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 2), ctx.handle)
-    tally = [0] * 12
+    tally, tally2 = [0] * 12, [0] * 12
     for a in range(0, n1, chunk):
         call(a, min(chunk, n1 - a))
         tt = (_lib.C.c_uint64 * 12)()
         _lib.lib.ma_ctx_traffic(ctx.handle, tt)
         tally = [x + y for x, y in zip(tally, tt)]
+        tally2 = [x + y for x, y in zip(tally2, ctx.traffic_stage2())]
     _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 1), ctx.handle)
 
     # ---- per-kernel times of the seed kernels (events around each kernel
@@ -1684,7 +1699,7 @@ def run_genome(args, rank, world, local):
     seed_ms, wave = [], []
     kms = (_lib.C.c_float * 4)()
     for _ in range(2):
-        sm, wv = 0.0, [0.0, 0.0, 0.0, 0.0]
+        sm, wv = 0.0, [0.0] * 5
         for a in range(0, n1, chunk):
             call(a, min(chunk, n1 - a))
             _lib.lib.ma_ctx_kernel_ms(ctx.handle, kms)
@@ -1750,7 +1765,7 @@ def run_genome(args, rank, world, local):
                 ["occ_lines_32B", "kmer_loads", "sa_loads", "pac_sectors_32B", "backward_steps", "endpoints",
                  "loci_evaluated", "read_words", "endpoints_skipped", "stage2_reads", "stage2_groups",
                  "shift_evals"], tally)}}
-    roof.update(seeding_roofline(tally, wave))
+    roof.update(seeding_roofline(tally, wave, tally2, n_seq))
 
     line = {"metric": METRIC, "value": round(value, 1), "unit": "reads/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",

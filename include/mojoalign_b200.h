@@ -779,10 +779,14 @@ int ma_ctx_set_profiling(ma_ctx* ctx, int flags);
  * rescue, and stage 1 alone (equal to seed/extend for seed_kernel 0). */
 int ma_ctx_kernel_ms(const ma_ctx* ctx, float* out4);
 /* Profiling (flag 1), wavefront form: the last call's wf_search, wf_eval and
- * wf_finalize kernel times summed over its rounds (ms), and the rounds timed
+ * wf_finalize kernel times summed over its rounds (ms), the rounds timed
  * (negative when the call had more than 64 rounds: only the first 64 are in
- * the sums). */
-int ma_ctx_wave_ms(const ma_ctx* ctx, float* out4);
+ * the sums), and the time of the stage-2 warps that finish the reads the
+ * rounds left over (ms). */
+int ma_ctx_wave_ms(const ma_ctx* ctx, float* out5);
+/* The part of ma_ctx_traffic's tallies that the wavefront form's stage-2
+ * warps made (counting flag 2; zeros for the other forms). */
+int ma_ctx_traffic_stage2(const ma_ctx* ctx, uint64_t* out12);
 /* Tallies of the last counting call: 32-B Occ lines, k-mer entries, SA
  * entries, distinct 32-B pac sectors per evaluated locus, backward steps,
  * endpoints searched, loci evaluated, read words read, endpoints skipped as

@@ -84,8 +84,9 @@ struct ma_ctx {
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // pack | stage 1 | stage 2 | rescue
     float kernel_ms[4] = {0, 0, 0, 0};  // pack, seed (both stages), rescue, stage 1 alone
     WaveTimer wave_timer;              // per-round events of the wavefront form
-    float wave_ms[4] = {0, 0, 0, 0};   // search, eval, finalize (summed over rounds), rounds timed
+    float wave_ms[5] = {0, 0, 0, 0, 0};  // search, eval, finalize (summed over rounds), rounds timed, stage 2
     uint64_t traffic[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    uint64_t traffic_stage2[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // the part of the wavefront's stage 2
     bool rescue_ran = false;
     DevBuf tally;
     // two-slot pipeline of ma_map_batch: H2D of chunk k+1 on copy_stream
@@ -232,9 +233,9 @@ void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const
     const bool timed = ctx->profiling & 1;
     unsigned long long* d_tally = nullptr;
     if (ctx->profiling & 2) {
-        ctx->tally.ensure(12 * sizeof(unsigned long long));
+        ctx->tally.ensure(24 * sizeof(unsigned long long));  // wavefront rounds, then stage 2
         d_tally = ctx->tally.as<unsigned long long>();
-        ck(cudaMemsetAsync(d_tally, 0, 12 * sizeof(unsigned long long), st), "memset");
+        ck(cudaMemsetAsync(d_tally, 0, 24 * sizeof(unsigned long long), st), "memset");
     }
     if (timed) ck(cudaEventRecord(ctx->ev[0], st), "event");
     launches += launch_pack(d_bases, d_lens, n_seq, n1, static_cast<int>(max_len), words, bs_r1, bs_r2,
@@ -373,12 +374,16 @@ void check_err_flag(ma_ctx* ctx, cudaStream_t st) {
                 ctx->wave_ms[2] += c;
             }
             ctx->wave_ms[3] = w.complete ? static_cast<float>(w.recorded) : -static_cast<float>(w.recorded);
+            ck(cudaEventElapsedTime(&ctx->wave_ms[4], w.s2[0], w.s2[1]), "elapsed");
         }
     }
     if (ctx->profiling & 2) {
-        unsigned long long t[12];
+        unsigned long long t[24];
         ck(cudaMemcpy(t, ctx->tally.p, sizeof t, cudaMemcpyDeviceToHost), "D2H tally");
-        for (int i = 0; i < 12; ++i) ctx->traffic[i] = t[i];
+        for (int i = 0; i < 12; ++i) {
+            ctx->traffic[i] = t[i] + t[12 + i];
+            ctx->traffic_stage2[i] = t[12 + i];
+        }
     }
 }
 
@@ -433,6 +438,8 @@ void ma_ctx_destroy(ma_ctx* ctx) {
     for (cudaEvent_t& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t& e : ctx->wave_timer.e)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : ctx->wave_timer.s2)
         if (e) cudaEventDestroy(e);
     ctx->tally.release();
     ctx->seed_scratch.release();
@@ -1600,6 +1607,8 @@ int ma_ctx_set_profiling(ma_ctx* ctx, int flags) {
             for (cudaEvent_t& e : ctx->ev) ck(cudaEventCreate(&e), "cudaEventCreate");
         if ((flags & 1) && !ctx->wave_timer.e[0])
             for (cudaEvent_t& e : ctx->wave_timer.e) ck(cudaEventCreate(&e), "cudaEventCreate");
+        if ((flags & 1) && !ctx->wave_timer.s2[0])
+            for (cudaEvent_t& e : ctx->wave_timer.s2) ck(cudaEventCreate(&e), "cudaEventCreate");
         ctx->profiling = flags;
     });
 }
@@ -1644,9 +1653,15 @@ int ma_ctx_get_tuning(const ma_ctx* ctx, ma_tuning* t) {
     return MA_OK;
 }
 
-int ma_ctx_wave_ms(const ma_ctx* ctx, float* out4) {
-    if (!ctx || !out4) return MA_ERR_ARG;
-    for (int i = 0; i < 4; ++i) out4[i] = ctx->wave_ms[i];
+int ma_ctx_wave_ms(const ma_ctx* ctx, float* out5) {
+    if (!ctx || !out5) return MA_ERR_ARG;
+    for (int i = 0; i < 5; ++i) out5[i] = ctx->wave_ms[i];
+    return MA_OK;
+}
+
+int ma_ctx_traffic_stage2(const ma_ctx* ctx, uint64_t* out12) {
+    if (!ctx || !out12) return MA_ERR_ARG;
+    for (int i = 0; i < 12; ++i) out12[i] = ctx->traffic_stage2[i];
     return MA_OK;
 }
 

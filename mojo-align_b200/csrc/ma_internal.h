@@ -79,10 +79,12 @@ BwtBuild bwt_build_gpu(const std::vector<uint64_t>& text_words, uint64_t n, int 
 
 // Events around the kernels of each wavefront round (profiling): e[3k]
 // before round k's search, e[3k+1] before its eval, e[3k+2] before its
-// finalize, e[3R] after the last round (rounds past MAX_ROUNDS untimed).
+// finalize, e[3R] after the last round (rounds past MAX_ROUNDS untimed),
+// and around the stage-2 launch after the rounds.
 struct WaveTimer {
     static constexpr int MAX_ROUNDS = 64;
     cudaEvent_t e[3 * MAX_ROUNDS + 1] = {};
+    cudaEvent_t s2[2] = {};  // around the stage-2 warps of the reads left over
     int recorded = 0;  // rounds timed in the last call
     bool complete = true;
 };

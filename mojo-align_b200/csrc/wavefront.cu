@@ -528,9 +528,14 @@ int launch_seed_wavefront(const DevIndex& ix, const DevReads& R, const DevParams
         launches = launch_rounds<false, 6, 5>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, nullptr, timer, st);
     else
         launches = launch_rounds<false, 1, 1>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, nullptr, timer, st);
-    // reads that overflowed the locus list or outlived the rounds
+    // reads that overflowed the locus list or outlived the rounds (their
+    // tallies in the second half of the tally array, their time between
+    // the timer's stage-2 events)
+    if (timer) cudaEventRecord(timer->s2[0], st);
     launches += launch_stage2_pending(ix, R, P, out, w.best_key, w.memo, w.memo_n, w.resume, w.pending,
-                                      w.counters + C_HANDOFF, stage2_blocks, t.reg_level, 32, d_tally, st);
+                                      w.counters + C_HANDOFF, stage2_blocks, t.reg_level, 32,
+                                      d_tally ? d_tally + TALLY_N : nullptr, st);
+    if (timer) cudaEventRecord(timer->s2[1], st);
     return launches;
 }
 

@@ -221,6 +221,7 @@ SIGNATURES = [
     ("ma_ctx_get_pipeline", C.c_int, [C.c_void_p, C.POINTER(ma_pipeline)]),
     ("ma_ctx_kernel_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     ("ma_ctx_wave_ms", C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    ("ma_ctx_traffic_stage2", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     ("ma_ctx_traffic", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     ("ma_bench_gather", C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_uint64, C.POINTER(C.c_double)]),
     ("ma_serve_options_default", None, [C.POINTER(ma_serve_options)]),

@@ -35,6 +35,10 @@ DEFAULT_CANDIDATES = [
     (2, 1, 0, 0, 1, 1, 4, 4, 0, 1),
     (2, 1, 0, 1, 1, 1, 4, 4, 0, 1),
     (2, 2, 0, 1, 1, 1, 8, 4, 0, 1),
+    (2, 1, 0, 1, 1, 1, 8, 8, 0, 1),    # larger locus lists (many multi-row seeds: genome scale)
+    (2, 1, 0, 1, 1, 1, 8, 16, 0, 1),
+    (2, 2, 0, 1, 1, 1, 8, 16, 0, 1),
+    (2, 1, 0, 2, 1, 1, 8, 16, 0, 1),
     (2, 1, 0, 1, 1, 1, 32, 4, 0, 0),   # one warp per read and round
     (2, 1, 0, 1, 1, 1, 64, 4, 0, 0),   # two warps per read
     (2, 1, 0, 1, 1, 1, 128, 4, 0, 0),  # four warps per read

@@ -83,10 +83,16 @@ class GpuContext:
         return list(v)
 
     def wave_ms(self) -> list[float]:
-        """Wavefront search, eval, finalize ms of the last profiled call and
-        the rounds timed (see ma_ctx_wave_ms)."""
-        v = (C.c_float * 4)()
+        """Wavefront search, eval, finalize ms of the last profiled call, the
+        rounds timed and the stage-2 ms (see ma_ctx_wave_ms)."""
+        v = (C.c_float * 5)()
         check(lib.ma_ctx_wave_ms(self.handle, v), self.handle)
+        return list(v)
+
+    def traffic_stage2(self) -> list[int]:
+        """The stage-2 part of traffic() (see ma_ctx_traffic_stage2)."""
+        v = (C.c_uint64 * 12)()
+        check(lib.ma_ctx_traffic_stage2(self.handle, v), self.handle)
         return list(v)
 
     def traffic(self) -> list[int]:

@@ -36,10 +36,12 @@ def test_line_order_puts_contract_and_parity_first():
 
 def test_seeding_roofline_arithmetic():
     tally = [10 ** 9, 5 * 10 ** 8, 2 * 10 ** 8] + [0] * 9
-    wave = [[20.0, 10.0, 5.0, 5.0], [20.0, 10.0, 5.0, 5.0]]
-    r = bench.seeding_roofline(tally, wave)["seeding"]
-    assert r["alg_bytes"] == 32 * 17 * 10 ** 8
-    assert abs(r["achieved_GBs"] - 32 * 17 * 10 ** 8 / 0.020 / 1e9) < 0.1
+    tally2 = [10 ** 8, 0, 0] + [0] * 6 + [500] + [0] * 2
+    wave = [[20.0, 10.0, 5.0, 5.0, 3.0], [20.0, 10.0, 5.0, 5.0, 3.0]]
+    r = bench.seeding_roofline(tally, wave, tally2, 1000)["seeding"]
+    assert r["alg_bytes"] == 32 * 16 * 10 ** 8  # the stage-2 warps' gathers are not the rounds'
+    assert abs(r["achieved_GBs"] - 32 * 16 * 10 ** 8 / 0.020 / 1e9) < 0.1
+    assert r["stage2_ms"] == 3.0 and r["stage2_reads_per_read"] == 0.5
     line = {"roofline": {"seeding": r}, "gather_roofline": {"hbm_32B_GBs": 800.0, "hbm_64B_GBs": 900.0}}
     bench.add_gather_fractions(line)
     assert line["roofline"]["seeding"]["frac_of_gather32"] == round(r["achieved_GBs"] / 800.0, 4)
