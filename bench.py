@@ -1587,18 +1587,18 @@ def run_genome(args, rank, world, local):
     fa, prefix, timings["reference_and_index"] = prepare_reference(
         args, rank, dist, local, genome_mb=mb, repeats=synth.RepeatModel() if spec["repeats"] else None,
         tag="_repeats" if spec["repeats"] else "")
-    # the ranks of a node simulate their reads and open the index one after
-    # another (each step holds several GB of host memory for a while)
+    t = time.time()
+    pinned = torch.empty((n_seq, max_len), dtype=torch.uint8, pin_memory=True)
+    log(f"reads: {n1} x {per}")
+    rb = synth.simulate_reads(fa, synth.ReadModel(**spec["model"]), n1, paired, max_len, seed=shard_seed(rank),
+                              bases_out=pinned.numpy())
+    timings["reads"] = time.time() - t
+    ctx = GpuContext(local)
+    # the ranks of a node open the index one after another: loading the
+    # files holds ~11 GB of host memory per rank for a while
     for turn in range(world):
         if turn == rank:
-            t = time.time()
-            pinned = torch.empty((n_seq, max_len), dtype=torch.uint8, pin_memory=True)
-            log(f"reads: {n1} x {per}")
-            rb = synth.simulate_reads(fa, synth.ReadModel(**spec["model"]), n1, paired, max_len,
-                                      seed=shard_seed(rank), bases_out=pinned.numpy())
             log("index open")
-            timings["reads"] = time.time() - t
-            ctx = GpuContext(local)
             t = time.time()
             gi = GpuIndex(ctx, prefix, kmer_k=args.kmer, kmer3_k=args.kmer3)
             timings["index_open"] = time.time() - t
