@@ -38,13 +38,14 @@ namespace {
 // counters[]
 constexpr int C_ACTIVE = 0;    // reads active in the current round
 constexpr int C_NEXT = 1;      // reads appended to the next round's list
-constexpr int C_LOCI = 2;      // loci appended in the current round
+constexpr int C_LOCI = 4;      // loci appended in the current round: a u64 in counters[4..5]
 constexpr int C_ROUNDS = 3;    // read-rounds processed (tally)
 constexpr int C_HANDOFF = 8;   // [8] reads for stage 2, [9] its work cursor
 constexpr int N_COUNTERS = 16;
 
-constexpr uint64_t LIDX_MASK = (1ull << 27) - 1;  // round keys: nm << 54 | ordinal << 27 | locus index
-constexpr uint64_t MAX_LOCI = LIDX_MASK;          // list capacity limit (indices fit 27 bits)
+// Round keys: nm << (27 + ib) | ordinal << ib | locus index, ib bits of
+// index: what the largest nm of the call leaves of the 64 bits, at most 31.
+constexpr uint64_t MAX_LOCI = (1ull << 31) - 1;  // list capacity limit (indices fit 31 bits)
 
 constexpr uint32_t DEAD_LOCUS = 0xFFFFFFFFu;
 constexpr int PREDICT_MEMO = 4;  // memo loci a duplicate prediction checks besides the best  // WLocus.read of a slot without a locus
@@ -78,9 +79,15 @@ struct Wave {
     uint32_t* pending;    // reads handed to stage 2
     WLocus* loci;
     uint64_t locus_cap;
+    int idx_bits;  // locus-index bits of the round keys
 };
 
 size_t align256(size_t b) { return (b + 255) & ~static_cast<size_t>(255); }
+
+// The round's locus count (64-bit: the rows a round asks for can exceed 2^32).
+__device__ __forceinline__ unsigned long long* loci_count(const Wave& w) {
+    return reinterpret_cast<unsigned long long*>(w.counters + C_LOCI);
+}
 
 // Carves the scratch; returns the bytes used (layout only when p != null).
 size_t wave_layout(char* p, int64_t n_seq, uint64_t locus_cap, Wave* w) {
@@ -144,7 +151,7 @@ __global__ void __launch_bounds__(256) wf_init_kernel(Wave w, DevOut out, const 
 __global__ void wf_round_begin_kernel(Wave w) {
     w.counters[C_ACTIVE] = w.counters[C_NEXT];
     w.counters[C_NEXT] = 0;
-    w.counters[C_LOCI] = 0;
+    *loci_count(w) = 0;
 }
 
 // Whether an SA row of a found seed gives a locus not evaluated before.
@@ -205,8 +212,8 @@ __global__ void __launch_bounds__(256, MINB) wf_search_kernel(DevIndex ix, DevRe
             if (lane >= o) incl += v;
         }
         const uint32_t warp_total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-        uint32_t wbase = 0;
-        if (lane == 31 && warp_total) wbase = atomicAdd(&w.counters[C_LOCI], warp_total);
+        unsigned long long wbase = 0;
+        if (lane == 31 && warp_total) wbase = atomicAdd(loci_count(w), static_cast<unsigned long long>(warp_total));
         wbase = __shfl_sync(0xFFFFFFFFu, wbase, 31);
         // the warp's rows, 32 at a time, one per lane (seeds have 1..16 rows)
         for (uint32_t c0 = 0; c0 < warp_total; c0 += 32) {
@@ -262,7 +269,7 @@ __global__ void __launch_bounds__(256, MINB) wf_search_kernel(DevIndex ix, DevRe
 // Eval: one thread per locus filters its shifts (live_shifts); the shifts
 // left in the warp are spread over its lanes.  Candidates are pruned
 // against the read's best from earlier rounds; the round's minimum key per
-// read is an atomicMin of (nm << 54 | ordinal << 27 | locus index).  The
+// read is an atomicMin of (nm, ordinal, locus index) packed in 64 bits.  The
 // loop over loci is warp-uniform for the redistribution.
 constexpr int EVAL_THREADS = 256;
 
@@ -272,7 +279,7 @@ __global__ void __launch_bounds__(EVAL_THREADS, MINB) wf_eval_kernel(DevIndex ix
     __shared__ WLocus s_loci[EVAL_THREADS];
     constexpr unsigned FULL = 0xFFFFFFFFu;
     Tally t{};
-    uint64_t n_loci = w.counters[C_LOCI];
+    uint64_t n_loci = *loci_count(w);
     if (n_loci > w.locus_cap) n_loci = w.locus_cap;
     const int adj_cap = clamps_for(P, 1 << 20).adj_cap;  // read-independent
     const int lane = threadIdx.x & 31;
@@ -334,7 +341,8 @@ __global__ void __launch_bounds__(EVAL_THREADS, MINB) wf_eval_kernel(DevIndex ix
                     const uint64_t nm = lb.key >> ORD_SHIFT;
                     const uint64_t ord = lb.key & ((1ull << ORD_SHIFT) - 1);
                     atomicMin(reinterpret_cast<unsigned long long*>(w.round_key + r),
-                              static_cast<unsigned long long>((nm << 54) | (ord << 27) | (base + own)));
+                              static_cast<unsigned long long>((nm << (ORD_SHIFT + w.idx_bits)) |
+                                                              (ord << w.idx_bits) | (base + own)));
                 }
             }
         }
@@ -379,10 +387,11 @@ __global__ void __launch_bounds__(256) wf_finalize_kernel(DevIndex ix, DevReads 
                 const uint64_t rk = w.round_key[r];
                 const uint64_t old = w.best_key[r];
                 bool stop = false;
-                if (rk != ~0ull && (rk >> 27) < old) {
+                const uint64_t rkey = rk >> w.idx_bits;  // nm << ORD_SHIFT | ordinal, the best-key format
+                if (rk != ~0ull && rkey < old) {
                     // the new best: recompute its fields from the winning locus and shift
-                    const WLocus L = w.loci[rk & LIDX_MASK];
-                    const uint32_t ord = static_cast<uint32_t>((rk >> 27) & ((1ull << ORD_SHIFT) - 1));
+                    const WLocus L = w.loci[rk & ((1ull << w.idx_bits) - 1)];
+                    const uint32_t ord = static_cast<uint32_t>(rkey & ((1ull << ORD_SHIFT) - 1));
                     const int adj = static_cast<int>(ord / KIND_SPAN) - static_cast<int>(L.ord_row) - 12;
                     const uint64_t bn = old >> ORD_SHIFT;
                     const int prune = bn < (1u << 20) ? static_cast<int>(bn) : (1 << 20);
@@ -397,7 +406,7 @@ __global__ void __launch_bounds__(256) wf_finalize_kernel(DevIndex ix, DevReads 
                     lb.crid = -1;
                     eval_adj<S>(ix, rd, L.b0, L.rev(), adj, cl.budget, cl.clip_cap, L.ord_row, lb, L.uk, L.ul(),
                                 L.us, L.e(), prune, hint, t);
-                    if (lb.key != (rk >> 27)) {
+                    if (lb.key != rkey) {
                         atomicExch(err, 3);  // the recomputed candidate must be the round's minimum
                     } else {
                         write_hit(out, r, lb, qlen);
@@ -516,6 +525,13 @@ int launch_seed_wavefront(const DevIndex& ix, const DevReads& R, const DevParams
                           unsigned long long* d_tally, WaveTimer* timer, cudaStream_t st) {
     Wave w;
     wave_layout(static_cast<char*>(scratch), R.n_seq, locus_capacity(R.n_seq, t.wave_loci_per_read), &w);
+    // an accepted candidate has nm <= its read's budget <= max(2, max_diff)
+    // (and <= 512): the round keys give the rest to the locus index
+    const int max_nm = P.max_diff < 2 ? 2 : (P.max_diff > 512 ? 512 : P.max_diff);
+    int nm_bits = 1;
+    while ((1 << nm_bits) <= max_nm) ++nm_bits;
+    w.idx_bits = 64 - ORD_SHIFT - nm_bits < 31 ? 64 - ORD_SHIFT - nm_bits : 31;
+    if (w.locus_cap > (1ull << w.idx_bits) - 1) w.locus_cap = (1ull << w.idx_bits) - 1;
     const int w0 = t.stage1_endpoints > 0 ? t.stage1_endpoints : 1;
     const int wn = t.wave_endpoints > 0 ? t.wave_endpoints : 1;
     int launches = 0;
