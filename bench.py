@@ -1,21 +1,31 @@
 #!/usr/bin/env python
 """Benchmark of the linear bisulfite seed-and-extend path (reads/s).
 
-Workload (per GPU): a synthetic 250 Mbp reference (GC 0.41, CpG ~1%, seed 0)
-indexed as the bwa-meth dual-strand text, and 10M bisulfite read pairs of
-2x150 bp (fragments N(350, 50), non-CpG conversion 0.99, CpG retention 0.75,
-0.5% substitutions, 5% random reads, seed 1 + rank).  Parameters: the
-reference defaults with seed_len 19 and max_occ 500.  One step maps the
-whole batch through the plain single-launch form (pack -> seed/extend ->
-mate rescue), counting each mate as one read.
+Default workload (`--workload genome`, per GPU): a synthetic 3.1 Gbp
+reference (GC 0.41, CpG ~1%, seed 0) indexed as the bwa-meth dual-strand
+text (12.4 G symbols, the index built on the GPU), and 50 M single-end
+bisulfite reads with lengths lognormal (median 120) clipped to 36-300, half
+of them non-directional (seed 1 + rank).  One step maps every read through
+the batched form (the autotuned wavefront kernels, one device call per 8 M
+reads, each call replayed from a captured CUDA graph).  Beside it: the plain
+single-launch form (the reference's launch shape) and the served form on the
+same reads, a served stream of 8 samples with p50 / p99 / p99.9 latency,
+the oracle on a 1 M-read parity sample, and the file stages (BAM, sort,
+BGZF, FASTQ -> BAM / SAM) on a 250 Mbp reference.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+`--workload chromosome`: 250 Mbp, 10 M pairs 2x150, the plain single-launch
+call; `--workload repeats`: 3.1 Gbp with 45% repeats, 10 M pairs 2x250 at
+non-CpG conversion 0.97.  Parameters: the reference defaults with seed_len
+19 and max_occ 500; each mate counts as one read.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload ...]
 
 Prints one JSON line (rank 0).  `value` is measured with the reads already
 in HBM; `e2e` through the host API (ma_map_batch) with pinned host buffers,
 copies included.  `--impl reference` times the CPU restatement of the
 reference kernels (the oracle; the Mojo reference cannot run here) on all
-host cores over a bounded sample of the same workload.
+host cores over a bounded sample of the same workload.  Progress lines go
+to stderr.
 """
 from __future__ import annotations
 
@@ -79,6 +89,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the oracle timing (profiling runs)")
     ap.add_argument("--no-forms", action="store_true", help="skip the plain / batched / served comparison")
+    ap.add_argument("--no-stages", action="store_true", help="genome workloads: skip the file stages (BAM, sort, "
+                    "BGZF, FASTQ -> BAM / SAM, FASTQ split) on the chromosome-scale reference")
     ap.add_argument("--forms-reads", type=int, default=4_000_000, help="uneven-length reads of the comparison")
     ap.add_argument("--forms-ref-batches", type=int, default=64, help="16384-read batches timed in the "
                     "reference-loop form")
@@ -99,7 +111,7 @@ def parse_args():
                     "stage (0 = skip)")
     ap.add_argument("--fq2sam-pairs", type=int, default=2_000_000, help="read pairs of the FASTQ -> SAM stage "
                     "(0 = skip)")
-    ap.add_argument("--workload", choices=["chromosome", "genome", "repeats"], default="chromosome",
+    ap.add_argument("--workload", choices=["chromosome", "genome", "repeats"], default="genome",
                     help="chromosome: 250 Mbp, 10 M pairs 2x150, plain single-launch (and the file stages); "
                     "genome: 3.1 Gbp, 50 M uneven single-end reads, batched / plain / served forms and the served "
                     "stream; repeats: 3.1 Gbp with 45%% repeats, 10 M pairs 2x250 at conversion 0.97")
@@ -1264,32 +1276,10 @@ def run_ours(args, rank, world, local):
             bad += int((g != o[f]).sum())
         line["parity_sample"] = {"reads": 2 * n, "mismatched_fields": bad}
         reference_algorithm_bytes(line, ix, rb.bases, rb.lens, rb.n1, True, READ_LEN, params, n_seq)
-    if rank == 0 and world == 1 and args.bam_pairs > 0:
-        log("stage: BAM pack")
-        line["stages"] = {"bam_pack": run_bam_stage(args, ctx, rb, res, local, peaks)}
-        if args.sort_batches > 0:
-            torch.cuda.empty_cache()
-            log("stage: sort")
-            line["stages"]["sort_markdup_gather"] = run_sort_stage(args, ctx, rb, res, local, peaks)
-            if args.bgzf_level >= 0 and getattr(args, "_sorted_stream", None) is not None:
-                torch.cuda.empty_cache()
-                log("stage: BGZF")
-                line["stages"]["bgzf"] = run_bgzf_stage(args, ctx, args._sorted_stream, local, peaks)
-                del args._sorted_stream
-    if rank == 0 and world == 1 and args.fq2bam_pairs > 0:
-        torch.cuda.empty_cache()
-        args._prefix = prefix
-        log("stage: FASTQ -> BAM")
-        line.setdefault("stages", {})["fq2bam"] = run_fq2bam_stage(args, ctx, gi, rb, local, params)
-    if rank == 0 and world == 1 and args.fq2sam_pairs > 0:
-        torch.cuda.empty_cache()
-        args._prefix = prefix
-        log("stage: FASTQ -> SAM")
-        line.setdefault("stages", {})["fq2sam"] = run_fq2sam_stage(args, ctx, gi, rb, local, params, peaks)
-    if rank == 0 and world == 1 and args.fastq_pairs > 0:
-        torch.cuda.empty_cache()
-        log("stage: FASTQ split")
-        line.setdefault("stages", {})["fastq_split"] = run_fastq_stage(args, ctx, rb, local, peaks)
+    if rank == 0 and world == 1:
+        stages = stage_block(args, ctx, gi, rb, res, prefix, local, peaks, params)
+        if stages:
+            line["stages"] = stages
     if rank == 0 and world == 1 and not args.no_forms:
         from mojoalign_b200.autotune import FIELDS as TFIELDS
 
@@ -1308,6 +1298,73 @@ def run_ours(args, rank, world, local):
     if bad:
         sys.stderr.write("parity check failed: " + ", ".join(bad) + "\n")
         sys.exit(3)
+
+
+def stage_block(args, ctx, gi, rb, res, prefix, local, peaks, params) -> dict:
+    """The stages either side of the mapping kernels (BAM records, sort +
+    duplicate marking + gather, BGZF, FASTQ -> BAM, FASTQ -> SAM, FASTQ
+    split) on the pairs `rb` and their mapping outputs `res`."""
+    import torch
+
+    stages = {}
+    if args.bam_pairs > 0:
+        log("stage: BAM pack")
+        stages["bam_pack"] = run_bam_stage(args, ctx, rb, res, local, peaks)
+        if args.sort_batches > 0:
+            torch.cuda.empty_cache()
+            log("stage: sort")
+            stages["sort_markdup_gather"] = run_sort_stage(args, ctx, rb, res, local, peaks)
+            if args.bgzf_level >= 0 and getattr(args, "_sorted_stream", None) is not None:
+                torch.cuda.empty_cache()
+                log("stage: BGZF")
+                stages["bgzf"] = run_bgzf_stage(args, ctx, args._sorted_stream, local, peaks)
+                del args._sorted_stream
+    args._prefix = prefix
+    if args.fq2bam_pairs > 0:
+        torch.cuda.empty_cache()
+        log("stage: FASTQ -> BAM")
+        stages["fq2bam"] = run_fq2bam_stage(args, ctx, gi, rb, local, params)
+    if args.fq2sam_pairs > 0:
+        torch.cuda.empty_cache()
+        log("stage: FASTQ -> SAM")
+        stages["fq2sam"] = run_fq2sam_stage(args, ctx, gi, rb, local, params, peaks)
+    if args.fastq_pairs > 0:
+        torch.cuda.empty_cache()
+        log("stage: FASTQ split")
+        stages["fastq_split"] = run_fastq_stage(args, ctx, rb, local, peaks)
+    return stages
+
+
+def chromosome_stages(args, local, params, peaks) -> dict:
+    """The file stages measured beside a genome workload: the chromosome
+    workload's reference (args.genome_mb, 250 Mbp by default) and index,
+    and as many of its 2x150 pairs as the stages use, mapped first."""
+    import torch
+    from mojoalign_b200 import GpuContext, GpuIndex, MapResult, map_batch
+
+    class _Solo(Dist):
+        def __init__(self):
+            super().__init__(1, "gloo")
+
+    fa, prefix, _ = prepare_reference(args, 0, _Solo(), local)
+    pairs = max(args.bam_pairs * max(1, args.sort_batches), args.fq2bam_pairs, args.fq2sam_pairs,
+                args.fastq_pairs, 1)
+    sub = argparse.Namespace(**vars(args))
+    sub.pairs = pairs
+    log(f"stages: {pairs} pairs on the {args.genome_mb} Mbp reference")
+    rb = simulate(sub, fa, 0)
+    ctx = GpuContext(local)
+    gi = GpuIndex(ctx, prefix, kmer_k=args.kmer, kmer3_k=args.kmer3)
+    res = MapResult.empty(rb.n_seq, debug=False)
+    map_batch(ctx, gi, rb.bases, rb.lens, rb.n1, True, READ_LEN, "C2T", "G2A", params, out=res)
+    try:
+        out = stage_block(args, ctx, gi, rb, res, prefix, local, peaks, params)
+        out["reference"] = f"{args.genome_mb} Mbp synthetic bisulfite reference, {pairs} PE 2x{READ_LEN} pairs"
+        return out
+    finally:
+        gi.close()
+        ctx.close()
+        torch.cuda.empty_cache()
 
 
 UNEVEN_MODEL = dict(len_fixed=0, len_lognorm_median=120.0, len_lognorm_sigma=0.35, len_min=36, len_max=300,
@@ -1334,6 +1391,27 @@ def serving_samples():
             ml = 250
         out.append((m, ml))
     return out
+
+
+def sample_pools(args, fa) -> list:
+    """The 8 simulated samples' read pools (pinned host rows), simulated on
+    8 host threads at once (each simulation reads the reference itself)."""
+    import concurrent.futures as cf
+
+    import torch
+    from mojoalign_b200 import synth
+
+    specs = serving_samples()
+    bufs = [torch.empty((args.serve_pool, ml), dtype=torch.uint8, pin_memory=True) for _, ml in specs]
+
+    def one(k):
+        m, ml = specs[k]
+        r = synth.simulate_reads(fa, synth.ReadModel(**m), args.serve_pool, False, ml, seed=200 + k,
+                                 bases_out=bufs[k].numpy())
+        return (bufs[k], bufs[k].numpy(), r.lens, ml)
+
+    with cf.ThreadPoolExecutor(max_workers=len(specs)) as ex:
+        return list(ex.map(one, range(len(specs))))
 
 
 def log_uniform_sizes(rng, n, lo, hi):
@@ -1448,12 +1526,7 @@ def run_forms(args, ctx, gi, params, fa, local, best_tuning):
         del tickets
 
         # 8 samples, each a pool of reads; requests are slices of a pool
-        pools = []
-        for k, (m, ml) in enumerate(serving_samples()):
-            pb = torch.empty((args.serve_pool, ml), dtype=torch.uint8, pin_memory=True)
-            r = synth.simulate_reads(fa, synth.ReadModel(**m), args.serve_pool, False, ml, seed=200 + k,
-                                     bases_out=pb.numpy())
-            pools.append((pb, pb.numpy(), r.lens, ml))
+        pools = sample_pools(args, fa)
 
         def request(k, size):
             _, b, l, ml = pools[k]
@@ -1823,12 +1896,15 @@ def run_genome(args, rank, world, local):
                                 "sample": f"the parity sample ({nr} reads), {dt:.1f} s, index load {load_s:.1f} s"}
         reference_algorithm_bytes(line, ix, bases_np, lens_np, n1, paired, max_len, params, n_seq,
                                   bs2=2 if paired else 0)
+    gi.close()
+    ctx.close()
+    torch.cuda.empty_cache()
+    if rank == 0 and world == 1 and not args.no_stages:
+        line["stages"] = chromosome_stages(args, local, params, peaks)
     bad = parity_failures(line)
     line["parity_failures"] = bad
     if rank == 0:
         print(json.dumps(ordered_line(line)), flush=True)
-    gi.close()
-    ctx.close()
     dist.close()
     if bad:
         sys.stderr.write("parity check failed: " + ", ".join(bad) + "\n")
@@ -1917,12 +1993,7 @@ def genome_forms(args, ctx, gi, params, fa, local, best, bases_np, lens_np, n, m
 
     # served stream: 8 samples, Poisson arrivals at half the burst rate, an
     # HBM budget that admission has to wait on
-    pools = []
-    for k, (mdl, ml) in enumerate(serving_samples()):
-        pb = torch.empty((args.serve_pool, ml), dtype=torch.uint8, pin_memory=True)
-        r = synth.simulate_reads(fa, synth.ReadModel(**mdl), args.serve_pool, False, ml, seed=200 + k,
-                                 bases_out=pb.numpy())
-        pools.append((pb, pb.numpy(), r.lens, ml))
+    pools = sample_pools(args, fa)
 
     def request(k, size):
         _, b, l, ml = pools[k]
