@@ -119,8 +119,8 @@ def parse_args():
                     "(0 = 3100)")
     ap.add_argument("--genome-reads", type=int, default=0, help="reads (pairs) of the genome workloads "
                     "(0 = the workload's)")
-    ap.add_argument("--genome-chunk", type=int, default=8_000_000, help="reads per device call (the wavefront "
-                    "locus list of a call holds at most 2^27 loci: smaller calls leave room for more loci per read)")
+    ap.add_argument("--genome-chunk", type=int, default=8_000_000, help="reads per device call (a wavefront "
+                    "round lists at most 2^31-1 loci: smaller calls leave room for more loci per read)")
     ap.add_argument("--parity-reads", type=int, default=1_000_000, help="reads checked against the oracle")
     ap.add_argument("--serve-stream-budget-mb", type=int, default=512, help="HBM budget of the served stream "
                     "(below what max_inflight groups need, so that admission waits)")
