@@ -62,6 +62,8 @@ SEED_KERNELS = {
     1: "seed/extend: seed_stage1_kernel + seed_stage2_kernel (thread per read, then warp per read)",
     2: "seed/extend: wavefront rounds (wf_search_kernel + wf_eval_kernel + wf_finalize_kernel per round, "
        "seed_stage2_kernel for reads left over)",
+    3: "seed/extend: wavefront rounds with lane refill (wf_search_refill_kernel + wf_eval_kernel + "
+       "wf_finalize_kernel per round, seed_stage2_kernel for reads left over)",
 }
 READ_LEN = 150
 
@@ -1014,7 +1016,7 @@ def parity_failures(obj, path="") -> list:
     return bad
 
 
-def seeding_roofline(tally, wave, tally2=None, n_seq=0) -> dict:
+def seeding_roofline(tally, wave, tally2=None, n_seq=0, seed_kernel=2) -> dict:
     """The seeding kernel alone (wavefront search: k-mer table, Occ and SA
     gathers) from the counting pass's tallies (the rounds' part: the
     stage-2 warps' tallies, tally2, taken out) and the per-round search
@@ -1024,7 +1026,8 @@ def seeding_roofline(tally, wave, tally2=None, n_seq=0) -> dict:
     tally2 = tally2 or [0] * 12
     search_ms = statistics.mean(w[0] for w in wave)
     seed_bytes = 32 * sum(tally[i] - tally2[i] for i in range(3))
-    out = {"seeding": {"kernel": "wf_search_kernel (all rounds)", "ms": round(search_ms, 3),
+    name = "wf_search_refill_kernel" if seed_kernel == 3 else "wf_search_kernel"
+    out = {"seeding": {"kernel": f"{name} (all rounds)", "ms": round(search_ms, 3),
                        "eval_ms": round(statistics.mean(w[1] for w in wave), 3),
                        "finalize_ms": round(statistics.mean(w[2] for w in wave), 3),
                        "alg_bytes": int(seed_bytes),
@@ -1220,7 +1223,7 @@ def run_ours(args, rank, world, local):
     achieved = alg_bytes / (seed_avg_ms / 1000.0) / 1e9
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
             "frac": round(achieved / peaks.get("hbm_gbs"), 4),
-            "traffic": int(alg_bytes * TRAFFIC_OVER_ALG) if tune.tuning.get("seed_kernel") == 2 else None,
+            "traffic": int(alg_bytes * TRAFFIC_OVER_ALG) if tune.tuning.get("seed_kernel") in (2, 3) else None,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the seed kernels of one call "
                               "on the 50 Mbp / 2M-read case, as a ratio to the algorithmic bytes "
                               f"({TRAFFIC_OVER_ALG}), applied to this call's algorithmic bytes",
@@ -1234,7 +1237,7 @@ def run_ours(args, rank, world, local):
                 ["occ_lines_32B", "kmer_loads", "sa_loads", "pac_sectors_32B", "backward_steps", "endpoints",
                  "loci_evaluated", "read_words", "endpoints_skipped", "stage2_reads", "stage2_groups",
                  "shift_evals"], tally)}}
-    roof.update(seeding_roofline(tally, wave, tally2, n_seq))
+    roof.update(seeding_roofline(tally, wave, tally2, n_seq, tune.tuning.get("seed_kernel", 2)))
     line = {"metric": METRIC, "value": round(value, 1), "unit": "reads/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
@@ -1838,7 +1841,7 @@ def run_genome(args, rank, world, local):
                 ["occ_lines_32B", "kmer_loads", "sa_loads", "pac_sectors_32B", "backward_steps", "endpoints",
                  "loci_evaluated", "read_words", "endpoints_skipped", "stage2_reads", "stage2_groups",
                  "shift_evals"], tally)}}
-    roof.update(seeding_roofline(tally, wave, tally2, n_seq))
+    roof.update(seeding_roofline(tally, wave, tally2, n_seq, tune.tuning.get("seed_kernel", 2)))
 
     line = {"metric": METRIC, "value": round(value, 1), "unit": "reads/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",

@@ -281,7 +281,11 @@ int ma_last_launch_count(const ma_ctx* ctx);
  *                         candidate locus and shift), stage1_endpoints
  *                         endpoints in the first round and wave_endpoints in
  *                         each later one; reads left over go to the stage-2
- *                         warps (default).
+ *                         warps (default);
+ *                         3: the wavefront with lane refill in its search
+ *                         pass: each lane steps its own endpoint and takes
+ *                         a new one when its search ends, so lanes do not
+ *                         wait for the longest search of their warp.
  *   stage1_endpoints      endpoints stage 1 (or the first round) covers
  *                         (default 1).
  *   stage2_blocks_per_sm  persistent blocks per SM for stage 2 (0 = the
@@ -290,7 +294,8 @@ int ma_last_launch_count(const ma_ctx* ctx);
  *                         compiler's choice, 1 = 80 registers, 2 = 64
  *                         registers (stage kernels); for the wavefront's
  *                         search / eval kernels 0 = the compiler's choice,
- *                         1 = 5 / 4 blocks of 256 threads per SM, 2 = 6 / 5
+ *                         1 = 5 / 4 blocks of 256 threads per SM, 2 = 6 / 5,
+ *                         and for the lane-refill search 1 = 4, 2 = 5
  *                         (default 2).
  *   stage1_max_rows       stage 1 hands a read to stage 2 as soon as one of
  *                         its seeds has more SA rows than this (1..16,

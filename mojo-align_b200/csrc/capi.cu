@@ -246,7 +246,7 @@ void enqueue_map(ma_ctx* ctx, const ma_index* idx, const uint8_t* d_bases, const
     const int level = ctx->tuning.reg_level;
     if (ctx->tuning.seed_kernel == 0) {
         launches += launch_seed_extend(idx->dix, R, P, out, d_tally, level, st);
-    } else if (ctx->tuning.seed_kernel == 2) {
+    } else if (ctx->tuning.seed_kernel >= 2) {
         seed_scratch->ensure(wavefront_scratch_bytes(n_seq, ctx->tuning.wave_loci_per_read));
         const int bps = ctx->tuning.stage2_blocks_per_sm > 0 ? ctx->tuning.stage2_blocks_per_sm
                                                              : stage2_blocks_per_sm(level, d_tally != nullptr);
@@ -362,7 +362,7 @@ void check_err_flag(ma_ctx* ctx, cudaStream_t st) {
         ctx->kernel_ms[3] = ctx->kernel_ms[1];
         if (ctx->tuning.seed_kernel == 1) ck(cudaEventElapsedTime(&ctx->kernel_ms[3], ctx->ev[1], ctx->ev[4]), "elapsed");
         for (float& v : ctx->wave_ms) v = 0;
-        if (ctx->tuning.seed_kernel == 2) {
+        if (ctx->tuning.seed_kernel >= 2) {
             const WaveTimer& w = ctx->wave_timer;
             for (int k = 0; k < w.recorded; ++k) {
                 float a = 0, b = 0, c = 0;
@@ -1616,7 +1616,7 @@ int ma_ctx_set_profiling(ma_ctx* ctx, int flags) {
 int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t) {
     if (!ctx || !t) return MA_ERR_ARG;
     return guarded(ctx, [&] {
-        if (t->seed_kernel < 0 || t->seed_kernel > 2) fail(MA_ERR_ARG, "seed_kernel must be 0, 1 or 2");
+        if (t->seed_kernel < 0 || t->seed_kernel > 3) fail(MA_ERR_ARG, "seed_kernel must be 0, 1, 2 or 3");
         if (t->stage1_endpoints < 1) fail(MA_ERR_ARG, "stage1_endpoints must be >= 1");
         if (t->stage2_blocks_per_sm < 0 || t->stage2_blocks_per_sm > 64) fail(MA_ERR_ARG, "bad stage2_blocks_per_sm");
         if (t->reg_level < 0 || t->reg_level > 2) fail(MA_ERR_ARG, "reg_level must be 0, 1 or 2");

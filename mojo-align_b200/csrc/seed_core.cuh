@@ -592,15 +592,39 @@ struct Seed {
     bool found;
 };
 
-// Unique-SMEM left extension from right endpoint e (L1235-1385).
+// Unique-SMEM left extension from right endpoint e (L1235-1385), as a
+// start (the table steps) and single backward steps, so that a caller can
+// interleave the steps of many endpoints.  SeedSearch is the state between
+// steps.
+struct SeedSearch {
+    uint64_t k, l, last_k;
+    int s;
+    int last;  // the last interval of <= 16 rows at mlen >= seed_len: its start | (rows - 1) << 16; -1 = none
+};
+
+__device__ __forceinline__ void search_keep(SeedSearch& q, uint64_t k, uint64_t l, int s) {
+    q.last_k = k;
+    q.last = s | static_cast<int>(l - k) << 16;
+}
+
+// The seed a search that stops here returns: the last kept interval, if any.
+__device__ __forceinline__ Seed search_result(const SeedSearch& q) {
+    return q.last >= 0 ? Seed{q.last_k, q.last_k + static_cast<uint64_t>(q.last >> 16), q.last & 0xFFFF, true}
+                       : Seed{0, 0, -1, false};
+}
+
+// Starts the search at endpoint e.  Returns true when backward steps follow
+// (from q.s); false when the search is over, its seed (if any) in `out`.
 template <bool S>
-__device__ __forceinline__ Seed search_endpoint(const DevIndex& ix, const ReadView& rd, int e, const DevParams& P,
-                                                Tally& t) {
+__device__ __forceinline__ bool search_start(const DevIndex& ix, const ReadView& rd, int e, const DevParams& P,
+                                             SeedSearch& q, Seed& out, Tally& t) {
     if constexpr (S) t.endpoints++;
-    uint64_t k = 0, l = ix.seq_len, last_k = 0, last_l = 0;
-    int s = e, last_s = -1;
-    Seed res{0, 0, -1, false};
-    bool stop = false;
+    q.k = 0;
+    q.l = ix.seq_len;
+    q.last_k = 0;
+    q.s = e;
+    q.last = -1;
+    out = Seed{0, 0, -1, false};
     bool have = false;  // a table gave the interval after the first K steps
     int K = 0;
     // Steps before mlen reaches seed_len record nothing, so with K <= seed_len
@@ -610,7 +634,7 @@ __device__ __forceinline__ Seed search_endpoint(const DevIndex& ix, const ReadVi
     const int K3 = ix.kmer3_k;
     if (K3 > 0 && K3 <= P.seed_len) {
         const int s0 = e - K3 + 1;
-        if (window_bits(rd.nf, s0, K3) != 0) return res;
+        if (window_bits(rd.nf, s0, K3) != 0) return false;
         const uint64_t win = window_bits(rd.fwd, s0, K3);
         const uint64_t lo = win & kEven, hi = (win >> 1) & kEven;
         const bool has_c = (lo & ~hi) != 0, has_g = (hi & ~lo) != 0;
@@ -619,7 +643,7 @@ __device__ __forceinline__ Seed search_endpoint(const DevIndex& ix, const ReadVi
             for (int i = 0; i < K3; ++i) idx = idx * 3 + static_cast<uint32_t>(__popcll((win >> (2 * i)) & 3));
             const uint64_t kl = __ldg(ix.kmer3[has_c ? 1 : 0] + idx);
             if constexpr (S) t.kmer_loads++;
-            if (kmer_interval(kl, k, l)) {
+            if (kmer_interval(kl, q.k, q.l)) {
                 have = true;
                 K = K3;
             }
@@ -627,65 +651,96 @@ __device__ __forceinline__ Seed search_endpoint(const DevIndex& ix, const ReadVi
     }
     if (!have && ix.kmer_k > 0 && ix.kmer_k <= P.seed_len) {
         const int s0 = e - ix.kmer_k + 1;
-        if (window_bits(rd.nf, s0, ix.kmer_k) != 0) return res;
+        if (window_bits(rd.nf, s0, ix.kmer_k) != 0) return false;
         const uint64_t win = window_bits(rd.fwd, s0, ix.kmer_k);
         uint32_t idx = 0;
         for (int i = 0; i < ix.kmer_k; ++i) idx = (idx << 2) | static_cast<uint32_t>((win >> (2 * i)) & 3);
         const uint64_t kl = __ldg(ix.kmer + idx);
         if constexpr (S) t.kmer_loads++;
-        if (kmer_interval(kl, k, l)) {  // an untabled entry leaves (k, l) = (0, seq_len)
+        if (kmer_interval(kl, q.k, q.l)) {  // an untabled entry leaves (k, l) = (0, seq_len)
             have = true;
             K = ix.kmer_k;
         }
     }
     if (have) {
         const int s0 = e - K + 1;
-        if (k > l) return res;
+        if (q.k > q.l) return false;
         if (K >= P.seed_len) {
-            const int64_t occ_n = static_cast<int64_t>(l - k + 1);
-            if (occ_n == 1) return Seed{k, l, s0, true};
-            if (occ_n >= 1 && occ_n <= 16) {
-                last_k = k;
-                last_l = l;
-                last_s = s0;
+            const int64_t occ_n = static_cast<int64_t>(q.l - q.k + 1);
+            if (occ_n == 1) {
+                out = Seed{q.k, q.l, s0, true};
+                return false;
             }
-            if (occ_n > P.max_occ) stop = true;
+            if (occ_n >= 1 && occ_n <= 16) search_keep(q, q.k, q.l, s0);
+            if (occ_n > P.max_occ) {
+                out = search_result(q);
+                return false;
+            }
         }
-        s = s0 - 1;
+        q.s = s0 - 1;
     }
-    if (!stop) {
-        while (s >= 0) {
-            const int cc = code_at(rd, s);
-            if (cc > 3) break;
-            uint64_t ok = 0;
-            if constexpr (S) {
-                t.steps++;
-                const int64_t lk = k != 0 ? static_cast<int64_t>((k - 1 - (k - 1 >= ix.primary)) >> 6) : -1;
-                const int64_t ll = l != ix.seq_len ? static_cast<int64_t>((l - (l >= ix.primary)) >> 6) : -2;
-                t.occ_lines += (lk >= 0) + (ll >= 0 && ll != lk);
-            }
-            if (k != 0) ok = occ_row(ix, k - 1, cc);
-            const uint64_t ol = occ_row(ix, l, cc);
-            const uint64_t Lc = ix.L2[cc];
-            k = Lc + ok + 1;
-            l = Lc + ol;
-            if (k > l) break;
-            const int64_t occ_n = static_cast<int64_t>(l - k + 1);
-            const int mlen = e - s + 1;
-            if (mlen >= P.seed_len) {
-                if (occ_n == 1) return Seed{k, l, s, true};
-                if (occ_n <= 16) {
-                    last_k = k;
-                    last_l = l;
-                    last_s = s;
-                }
-                if (occ_n > P.max_occ) break;
-            }
-            --s;
+    if (q.s < 0) {
+        out = search_result(q);
+        return false;
+    }
+    return true;
+}
+
+// One backward step (base q.s).  Returns true when more steps follow; false
+// when the search is over, its seed (if any) in `out`.
+template <bool S>
+__device__ __forceinline__ bool search_next(const DevIndex& ix, const ReadView& rd, int e, const DevParams& P,
+                                            SeedSearch& q, Seed& out, Tally& t) {
+    const int cc = code_at(rd, q.s);
+    if (cc > 3) {
+        out = search_result(q);
+        return false;
+    }
+    uint64_t ok = 0;
+    if constexpr (S) {
+        t.steps++;
+        const int64_t lk = q.k != 0 ? static_cast<int64_t>((q.k - 1 - (q.k - 1 >= ix.primary)) >> 6) : -1;
+        const int64_t ll = q.l != ix.seq_len ? static_cast<int64_t>((q.l - (q.l >= ix.primary)) >> 6) : -2;
+        t.occ_lines += (lk >= 0) + (ll >= 0 && ll != lk);
+    }
+    if (q.k != 0) ok = occ_row(ix, q.k - 1, cc);
+    const uint64_t ol = occ_row(ix, q.l, cc);
+    const uint64_t Lc = ix.L2[cc];
+    q.k = Lc + ok + 1;
+    q.l = Lc + ol;
+    if (q.k > q.l) {
+        out = search_result(q);
+        return false;
+    }
+    const int64_t occ_n = static_cast<int64_t>(q.l - q.k + 1);
+    if (e - q.s + 1 >= P.seed_len) {
+        if (occ_n == 1) {
+            out = Seed{q.k, q.l, q.s, true};
+            return false;
+        }
+        if (occ_n <= 16) search_keep(q, q.k, q.l, q.s);
+        if (occ_n > P.max_occ) {
+            out = search_result(q);
+            return false;
         }
     }
-    if (last_s >= 0) return Seed{last_k, last_l, last_s, true};
-    return res;
+    if (--q.s < 0) {
+        out = search_result(q);
+        return false;
+    }
+    return true;
+}
+
+// The whole search of endpoint e.
+template <bool S>
+__device__ __forceinline__ Seed search_endpoint(const DevIndex& ix, const ReadView& rd, int e, const DevParams& P,
+                                                Tally& t) {
+    SeedSearch q;
+    Seed out;
+    if (search_start<S>(ix, rd, e, P, q, out, t))
+        while (search_next<S>(ix, rd, e, P, q, out, t)) {
+        }
+    return out;
 }
 
 // Per-read clamps of linear_gpu_fm.mojo:1204-1216.

@@ -136,7 +136,7 @@ GroupLayout layout_for(uint32_t n1, bool paired, int words, uint64_t stage_bytes
     o += OffsetArena::kAlign;
     L.scratch = o;
     if (seed_kernel == 1) o += rnd(two_stage_scratch_bytes(static_cast<int64_t>(n_seq)));
-    if (seed_kernel == 2) o += rnd(wavefront_scratch_bytes(static_cast<int64_t>(n_seq), t.wave_loci_per_read));
+    if (seed_kernel >= 2) o += rnd(wavefront_scratch_bytes(static_cast<int64_t>(n_seq), t.wave_loci_per_read));
     L.total = o;
     return L;
 }
@@ -351,7 +351,7 @@ void issue_group(ma_server* s, Group& g) {
     if (s->seed_kernel() == 1) {
         launch_seed_two_stage(*s->dix, R, P, o, t.stage1_endpoints, t.stage1_max_rows, bps * s->sm_count, t.reg_level,
                               t.stage2_first_wave, dev + g.L.scratch, nullptr, nullptr, st);
-    } else if (s->seed_kernel() == 2) {
+    } else if (s->seed_kernel() >= 2) {
         launch_seed_wavefront(*s->dix, R, P, o, 32 * g.words, t, bps * s->sm_count, dev + g.L.scratch, s->sm_count,
                               d_err, nullptr, nullptr, st);
     } else {

@@ -1,4 +1,4 @@
-// wavefront.cu - seed_kernel 2: the seed/extend search as rounds of
+// wavefront.cu - seed_kernels 2 and 3: the seed/extend search as rounds of
 // data-parallel passes over the whole batch (fm_seed_extend_kernel,
 // fq2bam-meth/src/linear_gpu_fm.mojo:1156-1837, with the candidate order
 // and exactness argument of seed_core.cuh).
@@ -47,8 +47,8 @@ constexpr int N_COUNTERS = 16;
 // index: what the largest nm of the call leaves of the 64 bits, at most 31.
 constexpr uint64_t MAX_LOCI = (1ull << 31) - 1;  // list capacity limit (indices fit 31 bits)
 
-constexpr uint32_t DEAD_LOCUS = 0xFFFFFFFFu;
-constexpr int PREDICT_MEMO = 4;  // memo loci a duplicate prediction checks besides the best  // WLocus.read of a slot without a locus
+constexpr uint32_t DEAD_LOCUS = 0xFFFFFFFFu;  // WLocus.read of a slot without a locus
+constexpr int PREDICT_MEMO = 4;  // memo loci a duplicate prediction checks besides the best
 
 // One candidate locus of a round (32 bytes: two per 64-B line).
 struct WLocus {
@@ -266,6 +266,189 @@ __global__ void __launch_bounds__(256, MINB) wf_search_kernel(DevIndex ix, DevRe
     flush_tally<S>(t, tally_out);
 }
 
+// Search with lane refill (seed_kernel 3): the same items as
+// wf_search_kernel, but each lane steps its own endpoint's search and takes
+// a new item when its search ends.  Search lengths differ by two orders of
+// magnitude (a table hit ends at once; a seed in a repeat steps back to the
+// read's start), so a warp that waits for its longest lane runs most steps
+// with few lanes busy.  Here the warp alternates two passes:
+//   refill  when at least REFILL_MIN lanes are idle (or all are), the idle
+//           lanes take the next items of the warp's chunk sequence and run
+//           the duplicate prediction and the table steps;
+//   step    the busy lanes take one backward step each.
+// Seeds found are staged in shared memory and appended to the locus list at
+// least 32 rows at a time (one atomic per flush, one lane per row), as in
+// wf_search_kernel.  Which lane or pass finds a seed does not change the
+// round's result: the eval keys carry the candidate order.
+constexpr int REFILL_MIN = 16;    // idle lanes that trigger a refill pass
+constexpr int REFILL_STAGE = 64;  // staged seeds per warp (flushed above 32)
+constexpr int SEARCH_WARPS = 8;   // 256 threads
+
+struct StagedSeed {  // 24 bytes
+    uint64_t k;
+    uint32_t read, rows_end;  // rows_end: staged rows up to and including this seed
+    uint16_t s, e, ei, qlen;
+};
+
+// Words of read r for the backward steps (qlen is not needed there).
+__device__ __forceinline__ ReadView step_view(const DevReads& R, uint32_t r) {
+    const uint64_t* b = R.packed + static_cast<uint64_t>(r) * 4 * static_cast<uint64_t>(R.words);
+    ReadView v;
+    v.fwd = b;
+    v.rc = nullptr;
+    v.nf = b + 2 * R.words;
+    v.nr = nullptr;
+    v.qlen = 0;
+    return v;
+}
+
+template <bool S, int MINB>
+__global__ void __launch_bounds__(256, MINB) wf_search_refill_kernel(DevIndex ix, DevReads R, DevParams P, Wave w,
+                                                               const uint32_t* __restrict__ act, int width,
+                                                               unsigned long long* __restrict__ tally_out) {
+    __shared__ StagedSeed s_stage[SEARCH_WARPS][REFILL_STAGE];
+    constexpr unsigned FULL = 0xFFFFFFFFu;
+    Tally t{};
+    const uint64_t n_items = static_cast<uint64_t>(w.counters[C_ACTIVE]) * static_cast<uint64_t>(width);
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1;
+    const uint64_t n_warps = static_cast<uint64_t>(gridDim.x) * SEARCH_WARPS;
+    const bool can_predict = ix.summary && ix.kmer3_k > 0 && ix.kmer3_k <= P.seed_len;
+    StagedSeed* stage = s_stage[threadIdx.x >> 5];
+    // the warp's items: chunks of 32 items, warp g takes chunks g, g + n_warps, ...
+    uint64_t chunk = static_cast<uint64_t>(blockIdx.x) * SEARCH_WARPS + (threadIdx.x >> 5);
+    uint32_t off = 0;          // items of the chunk handed out
+    int n_staged = 0;          // warp-uniform
+    uint32_t staged_rows = 0;  // warp-uniform
+    // the lane's search
+    bool busy = false;
+    SeedSearch q;
+    uint32_t r = 0;
+    int e_ei = 0;  // right endpoint | endpoint index << 16
+    for (;;) {
+        const unsigned idle = __ballot_sync(FULL, !busy);
+        const uint64_t cur = chunk * 32 + off;
+        const bool more = off < 32 && cur < n_items;
+        if (!more && idle == FULL && n_staged == 0) break;
+        bool fin = false;  // this lane's search ended in this pass
+        Seed sd{0, 0, -1, false};
+        if (more && (__popc(idle) >= REFILL_MIN || idle == FULL)) {
+            const uint64_t left = min(static_cast<uint64_t>(32 - off), n_items - cur);
+            const unsigned take = min(static_cast<uint64_t>(__popc(idle)), left);
+            const unsigned rank = __popc(idle & lt_mask);
+            if (!busy && rank < take) {
+                const uint64_t item = cur + rank;
+                const uint64_t a = item < (1ull << 32) ? static_cast<uint32_t>(item) / static_cast<uint32_t>(width)
+                                                       : item / static_cast<uint64_t>(width);
+                const int j = static_cast<int>(item - a * static_cast<uint64_t>(width));
+                r = act[a];
+                const ReadView rd = read_view(R, r);
+                const int ei = static_cast<int>(w.resume[r]) + j;
+                fin = true;
+                if (ei < endpoint_count(P, rd.qlen)) {
+                    const int e = P.seed_len - 1 + ei * P.seed_stride;
+                    e_ei = e | ei << 16;
+                    const int n_memo = w.memo_n[r];
+                    const int64_t best_tag = w.best_tag[r];
+                    const bool dup = can_predict && best_tag != -1 &&
+                                     predicted_duplicate<S>(ix, rd, e, P, best_tag, w.memo + r * MEMO1,
+                                                            n_memo < PREDICT_MEMO ? n_memo : PREDICT_MEMO, t);
+                    if constexpr (S) t.skipped += dup;
+                    if (!dup) {
+                        busy = search_start<S>(ix, rd, e, P, q, sd, t);
+                        fin = !busy;
+                    }
+                }
+            }
+            off += take;
+            if (off >= 32 || chunk * 32 + off >= n_items) {  // the warp's next chunk
+                chunk += n_warps;
+                off = 0;
+            }
+        } else if (busy) {
+            busy = search_next<S>(ix, step_view(R, r), e_ei & 0xFFFF, P, q, sd, t);
+            fin = !busy;
+        }
+        // stage the seeds found in this pass (at most 32: n_staged <= 32 here)
+        const bool found = fin && sd.found;
+        const unsigned fb = __ballot_sync(FULL, found);
+        if (fb) {
+            const uint32_t n_rows = found ? static_cast<uint32_t>(sd.l - sd.k + 1) : 0u;
+            uint32_t incl = n_rows;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += v;
+            }
+            if (found) {
+                StagedSeed g;
+                g.k = sd.k;
+                g.read = r;
+                g.rows_end = staged_rows + incl;
+                g.s = static_cast<uint16_t>(sd.s);
+                g.e = static_cast<uint16_t>(e_ei & 0xFFFF);
+                g.ei = static_cast<uint16_t>(e_ei >> 16);
+                g.qlen = static_cast<uint16_t>(__ldg(R.lens + r));
+                stage[n_staged + __popc(fb & lt_mask)] = g;
+            }
+            n_staged += __popc(fb);
+            staged_rows += __shfl_sync(FULL, incl, 31);
+        }
+        if (n_staged == 0) continue;
+        if (staged_rows < 32 && n_staged <= REFILL_STAGE - 32) {
+            // keep staging unless the warp's items are all searched
+            const bool out_of_items = off >= 32 || chunk * 32 + off >= n_items;
+            if (!out_of_items || __ballot_sync(FULL, busy)) continue;
+        }
+        // flush: one list slot per staged row, 32 rows at a time
+        __syncwarp();
+        unsigned long long wbase = 0;
+        if (lane == 0) wbase = atomicAdd(loci_count(w), static_cast<unsigned long long>(staged_rows));
+        wbase = __shfl_sync(FULL, wbase, 0);
+        for (uint32_t idx = lane; idx < staged_rows; idx += 32) {
+            int lo = 0, hi = n_staged - 1;  // first staged seed whose rows_end exceeds idx
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (stage[mid].rows_end > idx) hi = mid;
+                else lo = mid + 1;
+            }
+            const StagedSeed g = stage[lo];
+            const uint32_t first = lo ? stage[lo - 1].rows_end : 0u;
+            const uint64_t row = g.k + (idx - first);
+            const int64_t o_r = g.read;
+            const uint64_t slot = static_cast<uint64_t>(wbase) + idx;
+            if (slot >= w.locus_cap) {
+                w.overflow[o_r] = 1;
+                continue;
+            }
+            const uint64_t sa_pos = sa_at(ix, row);
+            if constexpr (S) t.sa_loads++;
+            WLocus L;
+            int64_t b0;
+            int rev;
+            if (!fresh_locus(ix, w, o_r, w.memo_n[o_r], sa_pos, g.s, g.e, g.qlen, b0, rev)) {
+                L.read = DEAD_LOCUS;
+                w.loci[slot] = L;
+                continue;
+            }
+            L.b0 = b0;
+            L.uk = g.k;
+            L.read = g.read;
+            L.ord_row = (static_cast<uint32_t>(g.ei) * 16 + (idx - first)) * ADJ_SPAN;
+            L.us = g.s;
+            L.e_dl = static_cast<uint16_t>(g.e | ((g.rows_end - first - 1) << 11));
+            L.crid_rev = static_cast<int32_t>(contig_hint(ix, b0).crid) * 2 + rev;
+            w.loci[slot] = L;
+            if constexpr (S) tally_locus(t, b0, clamps_for(P, g.qlen).adj_cap, g.qlen);
+            const uint32_t m = atomicAdd(&w.memo_next[o_r], 1u);
+            if (m < static_cast<uint32_t>(MEMO1)) w.memo[o_r * MEMO1 + m] = static_cast<uint64_t>(b0 * 2 + rev);
+        }
+        __syncwarp();
+        n_staged = 0;
+        staged_rows = 0;
+    }
+    flush_tally<S>(t, tally_out);
+}
+
 // Eval: one thread per locus filters its shifts (live_shifts); the shifts
 // left in the warp are spread over its lanes.  Candidates are pruned
 // against the read's best from earlier rounds; the round's minimum key per
@@ -463,9 +646,9 @@ int grid_blocks(K kernel, int sm_count) {
 
 // Register budget of the search / eval kernels (result-neutral): blocks of
 // 256 threads asked per SM (1 = the compiler's choice).
-template <bool S, int MS, int ME>
+template <bool S, int MS, int ME, int MR>
 int launch_rounds(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, const Wave& w,
-                  int max_len, int w0, int wn, int max_rounds, int growth, int sm_count, int* d_err,
+                  int max_len, int w0, int wn, int max_rounds, int growth, bool refill, int sm_count, int* d_err,
                   unsigned long long* tally, WaveTimer* timer, cudaStream_t st) {
     const int n_end_max = endpoint_count_host(P, max_len);
     // round widths: w0, then wn (doubling from the third round with growth)
@@ -479,6 +662,7 @@ int launch_rounds(const DevIndex& ix, const DevReads& R, const DevParams& P, con
     }
     if (max_rounds > 0 && rounds > max_rounds) rounds = max_rounds;
     static const int g_search = grid_blocks(wf_search_kernel<S, MS>, sm_count);
+    static const int g_refill = grid_blocks(wf_search_refill_kernel<S, MR>, sm_count);
     static const int g_eval = grid_blocks(wf_eval_kernel<S, ME>, sm_count);  // EVAL_THREADS = 256
     static const int g_fin = grid_blocks(wf_finalize_kernel<S>, sm_count);
     const unsigned init_blocks = static_cast<unsigned>((R.n_seq + 255) / 256);
@@ -494,7 +678,8 @@ int launch_rounds(const DevIndex& ix, const DevReads& R, const DevParams& P, con
         }
         const bool timed = timer && k < WaveTimer::MAX_ROUNDS;
         if (timed) cudaEventRecord(timer->e[3 * k], st);
-        wf_search_kernel<S, MS><<<g_search, 256, 0, st>>>(ix, R, P, w, act, width, tally);
+        if (refill) wf_search_refill_kernel<S, MR><<<g_refill, 256, 0, st>>>(ix, R, P, w, act, width, tally);
+        else wf_search_kernel<S, MS><<<g_search, 256, 0, st>>>(ix, R, P, w, act, width, tally);
         if (timed) cudaEventRecord(timer->e[3 * k + 1], st);
         wf_eval_kernel<S, ME><<<g_eval, 256, 0, st>>>(ix, R, P, w, tally);
         if (timed) cudaEventRecord(timer->e[3 * k + 2], st);
@@ -536,14 +721,15 @@ int launch_seed_wavefront(const DevIndex& ix, const DevReads& R, const DevParams
     const int wn = t.wave_endpoints > 0 ? t.wave_endpoints : 1;
     int launches = 0;
     const int mr = t.wave_max_rounds, gr = t.wave_growth;
+    const bool refill = t.seed_kernel == 3;
     if (d_tally)
-        launches = launch_rounds<true, 1, 1>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, d_tally, timer, st);
+        launches = launch_rounds<true, 1, 1, 1>(ix, R, P, out, w, max_len, w0, wn, mr, gr, refill, sm_count, d_err, d_tally, timer, st);
     else if (t.reg_level == 1)
-        launches = launch_rounds<false, 5, 4>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, nullptr, timer, st);
+        launches = launch_rounds<false, 5, 4, 4>(ix, R, P, out, w, max_len, w0, wn, mr, gr, refill, sm_count, d_err, nullptr, timer, st);
     else if (t.reg_level == 2)
-        launches = launch_rounds<false, 6, 5>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, nullptr, timer, st);
+        launches = launch_rounds<false, 6, 5, 5>(ix, R, P, out, w, max_len, w0, wn, mr, gr, refill, sm_count, d_err, nullptr, timer, st);
     else
-        launches = launch_rounds<false, 1, 1>(ix, R, P, out, w, max_len, w0, wn, mr, gr, sm_count, d_err, nullptr, timer, st);
+        launches = launch_rounds<false, 1, 1, 1>(ix, R, P, out, w, max_len, w0, wn, mr, gr, refill, sm_count, d_err, nullptr, timer, st);
     // reads that overflowed the locus list or outlived the rounds (their
     // tallies in the second half of the tally array, their time between
     // the timer's stage-2 events)

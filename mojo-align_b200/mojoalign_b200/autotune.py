@@ -10,7 +10,9 @@ In the wavefront form a round gives every active read `wave_endpoints`
 search threads, so the round width is the warps-per-read choice: 4, 8 and
 16 endpoints pack 8, 4 and 2 reads per warp (64, 32, 16 reads per 256-thread
 CTA), 32, 64 and 128 endpoints give each read 1, 2 and 4 warps (8, 4 and 2
-reads per CTA).  The stage-2 warps take one read each.
+reads per CTA).  The stage-2 warps take one read each.  seed_kernel 3 is the
+wavefront with lane refill in the search pass (each lane takes a new
+endpoint when its search ends).
 
 The seed stride is not swept: it decides which right endpoints are tried
 (linear_gpu_fm.mojo:1828) and so changes results.
@@ -42,6 +44,12 @@ DEFAULT_CANDIDATES = [
     (2, 1, 0, 1, 1, 1, 32, 4, 0, 0),   # one warp per read and round
     (2, 1, 0, 1, 1, 1, 64, 4, 0, 0),   # two warps per read
     (2, 1, 0, 1, 1, 1, 128, 4, 0, 0),  # four warps per read
+    (3, 1, 0, 1, 1, 1, 8, 4, 0, 1),    # lane refill in the search pass
+    (3, 1, 0, 2, 1, 1, 8, 4, 0, 1),
+    (3, 1, 0, 1, 1, 1, 8, 16, 0, 1),
+    (3, 2, 0, 1, 1, 1, 8, 16, 0, 1),
+    (3, 1, 0, 2, 1, 1, 8, 16, 0, 1),
+    (3, 1, 0, 1, 1, 1, 32, 16, 0, 0),
 ]
 FIELDS = ("seed_kernel", "stage1_endpoints", "stage2_blocks_per_sm", "reg_level", "stage1_max_rows",
           "stage2_first_wave", "wave_endpoints", "wave_loci_per_read", "wave_max_rounds", "wave_growth")

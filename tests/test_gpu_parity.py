@@ -41,10 +41,11 @@ def gpu_index(ctx, prefix, k, k3=0):
 # wave_max_rounds): one thread per read; two stages with the first 1, 2 or 3 right endpoints in stage 1, at
 # each register budget; wavefront rounds of several widths, with a locus list too small for the batch (reads
 # overflow to the stage-2 warps), with the rounds cut short (the rest finished by stage 2) and with doubling
-# round widths.
+# round widths; the same with lane refill in the search pass (seed_kernel 3).
 TUNINGS = [(0, 1, 0, 0, 16, 32), (1, 1, 0, 1, 2, 32), (1, 3, 1, 2, 1, 1), (1, 2, 0, 0, 16, 4), (1, 1, 0, 2, 1, 7),
            (2, 1, 0, 1, 2, 32, 32, 4, 0), (2, 2, 0, 2, 1, 1, 5, 1, 0), (2, 1, 0, 0, 2, 32, 3, 4, 2),
-           (2, 1, 0, 1, 1, 1, 4, 2, 0, 1)]
+           (2, 1, 0, 1, 1, 1, 4, 2, 0, 1), (3, 1, 0, 1, 2, 32, 32, 4, 0), (3, 2, 0, 2, 1, 1, 5, 1, 0),
+           (3, 1, 0, 0, 2, 32, 3, 4, 2), (3, 1, 0, 1, 1, 1, 8, 16, 0, 1)]
 
 
 def compare(prefix, ctx, bases, lens, n1, paired, max_len, params, k=12, bs=(1, 2), tunings=TUNINGS, k3=12):

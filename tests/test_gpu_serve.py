@@ -51,7 +51,8 @@ def oracle_map(prefix, req, params):
     return oracle.OracleIndex(prefix).map(bases, lens, n1, paired, ml, bsm[b1], bsm[b2], params.as_list())
 
 
-@pytest.mark.parametrize("tuning", [None, (0, 1, 0, 1, 16, 32), (2, 1, 0, 1, 1, 1, 32, 4, 0)])
+@pytest.mark.parametrize("tuning", [None, (0, 1, 0, 1, 16, 32), (2, 1, 0, 1, 1, 1, 32, 4, 0),
+                                    (3, 1, 0, 2, 1, 1, 8, 4, 0, 1)])
 def test_served_requests_match_oracle(ctx, small_ref, tuning):
     fa, prefix = small_ref
     gi = GpuIndex(ctx, prefix, kmer_k=12, kmer3_k=12)
