@@ -456,6 +456,36 @@ __global__ void __launch_bounds__(256, MINB) wf_search_refill_kernel(DevIndex ix
 // loop over loci is warp-uniform for the redistribution.
 constexpr int EVAL_THREADS = 256;
 
+// One shift (adj) of the locus at list index li: its candidates, pruned
+// against the read's best from earlier rounds, and the atomicMin of the
+// round key.
+template <bool S>
+__device__ __forceinline__ void eval_shift(const DevIndex& ix, const DevReads& R, const DevParams& P, const Wave& w,
+                                           const WLocus& L, uint32_t li, int adj, Tally& t) {
+    const int64_t r = L.read;
+    const ReadView rd = read_view(R, r);
+    const Clamps cl = clamps_for(P, rd.qlen);
+    const uint64_t bn = w.best_key[r] >> ORD_SHIFT;
+    const int prune = bn < (1u << 20) ? static_cast<int>(bn) : (1 << 20);
+    const int crid = L.crid();
+    ContigHint hint{crid, 0, 0};
+    if (crid >= 0) {
+        hint.coff = static_cast<int64_t>(__ldg(ix.coff + crid));
+        hint.clen = static_cast<int64_t>(__ldg(ix.clen + crid));
+    }
+    Best lb;
+    lb.key = ~0ull;
+    lb.crid = -1;
+    eval_adj<S>(ix, rd, L.b0, L.rev(), adj, cl.budget, cl.clip_cap, L.ord_row, lb, L.uk, L.ul(), L.us, L.e(), prune,
+                hint, t);
+    if (lb.key != ~0ull) {
+        const uint64_t nm = lb.key >> ORD_SHIFT;
+        const uint64_t ord = lb.key & ((1ull << ORD_SHIFT) - 1);
+        atomicMin(reinterpret_cast<unsigned long long*>(w.round_key + r),
+                  static_cast<unsigned long long>((nm << (ORD_SHIFT + w.idx_bits)) | (ord << w.idx_bits) | li));
+    }
+}
+
 template <bool S, int MINB>
 __global__ void __launch_bounds__(EVAL_THREADS, MINB) wf_eval_kernel(DevIndex ix, DevReads R, DevParams P, Wave w,
                                                                unsigned long long* __restrict__ tally_out) {
@@ -503,33 +533,86 @@ __global__ void __launch_bounds__(EVAL_THREADS, MINB) wf_eval_kernel(DevIndex ix
             const int o_first = __shfl_sync(FULL, incl - n_live, own);
             if (idx < total) {
                 const int adj = static_cast<int>(__fns(o_live, 0, idx - o_first + 1)) - adj_cap;
-                const WLocus L = wl[own];
-                const int64_t r = L.read;
+                eval_shift<S>(ix, R, P, w, wl[own], base + own, adj, t);
+            }
+        }
+        __syncwarp();
+    }
+    flush_tally<S>(t, tally_out);
+}
+
+// Eval with staged shifts (seed_kernel 3): the filter pass as in
+// wf_eval_kernel, but the live shifts (a fraction of a shift per locus at
+// genome scale) are staged per warp in shared memory and evaluated 32 at a
+// time, so the full compares run with every lane busy.
+constexpr int SHIFT_STAGE = 64;  // staged shifts per warp: locus index << 5 | shift
+
+template <bool S, int MINB>
+__global__ void __launch_bounds__(EVAL_THREADS, MINB) wf_eval_staged_kernel(DevIndex ix, DevReads R, DevParams P,
+                                                                      Wave w,
+                                                                      unsigned long long* __restrict__ tally_out) {
+    __shared__ uint64_t s_shift[EVAL_THREADS / 32][SHIFT_STAGE];
+    constexpr unsigned FULL = 0xFFFFFFFFu;
+    Tally t{};
+    uint64_t n_loci = *loci_count(w);
+    if (n_loci > w.locus_cap) n_loci = w.locus_cap;
+    const int adj_cap = clamps_for(P, 1 << 20).adj_cap;  // read-independent
+    const int lane = threadIdx.x & 31;
+    uint64_t* stage = s_shift[threadIdx.x >> 5];
+    int staged = 0;  // warp-uniform
+    const uint32_t stride = gridDim.x * blockDim.x;
+    // one more pass after the warp's last loci empties the stage
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);; base += stride) {
+        const bool have = base < n_loci;
+        const uint32_t li = base + lane;
+        uint32_t rem = 0;  // the lane's live shifts not yet staged
+        if (have && li < n_loci) {
+            const WLocus L = w.loci[li];
+            const int64_t r = L.read;
+            if (L.read != DEAD_LOCUS && !w.overflow[r]) {
                 const ReadView rd = read_view(R, r);
                 const Clamps cl = clamps_for(P, rd.qlen);
                 const uint64_t bn = w.best_key[r] >> ORD_SHIFT;
                 const int prune = bn < (1u << 20) ? static_cast<int>(bn) : (1 << 20);
-                const int crid = L.crid();
-                ContigHint hint{crid, 0, 0};
-                if (crid >= 0) {
-                    hint.coff = static_cast<int64_t>(__ldg(ix.coff + crid));
-                    hint.clen = static_cast<int64_t>(__ldg(ix.clen + crid));
-                }
-                Best lb;
-                lb.key = ~0ull;
-                lb.crid = -1;
-                eval_adj<S>(ix, rd, L.b0, L.rev(), adj, cl.budget, cl.clip_cap, L.ord_row, lb, L.uk, L.ul(), L.us,
-                            L.e(), prune, hint, t);
-                if (lb.key != ~0ull) {
-                    const uint64_t nm = lb.key >> ORD_SHIFT;
-                    const uint64_t ord = lb.key & ((1ull << ORD_SHIFT) - 1);
-                    atomicMin(reinterpret_cast<unsigned long long*>(w.round_key + r),
-                              static_cast<unsigned long long>((nm << (ORD_SHIFT + w.idx_bits)) |
-                                                              (ord << w.idx_bits) | (base + own)));
-                }
+                rem = live_shifts<S>(ix, rd, L.b0, L.rev(), adj_cap, cl.budget, cl.clip_cap, prune, t);
             }
         }
-        __syncwarp();
+        for (;;) {
+            // stage as many live shifts as fit (lanes in order)
+            if (__ballot_sync(FULL, rem != 0)) {
+                const int n = __popc(rem);
+                int incl = n;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(FULL, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                int at = staged + incl - n;
+                while (rem && at < SHIFT_STAGE) {
+                    stage[at++] = static_cast<uint64_t>(li) << 5 | static_cast<uint32_t>(__ffs(rem) - 1);
+                    rem &= rem - 1;
+                }
+                const int total = staged + __shfl_sync(FULL, incl, 31);
+                staged = total < SHIFT_STAGE ? total : SHIFT_STAGE;
+            }
+            const bool pending = __ballot_sync(FULL, rem != 0) != 0;
+            if (staged < 32 && (have || staged == 0)) break;
+            // evaluate the first 32 (or the last few) staged shifts, one per lane
+            const int n = staged < 32 ? staged : 32;
+            __syncwarp();
+            if (lane < n) {
+                const uint64_t v = stage[lane];
+                const uint32_t sli = static_cast<uint32_t>(v >> 5);
+                eval_shift<S>(ix, R, P, w, w.loci[sli], sli, static_cast<int>(v & 31) - adj_cap, t);
+            }
+            __syncwarp();
+            const uint64_t v = lane < staged - n ? stage[n + lane] : 0;
+            __syncwarp();
+            if (lane < staged - n) stage[lane] = v;
+            staged -= n;
+            __syncwarp();
+            if (!pending && staged < 32 && have) break;
+        }
+        if (!have) break;
     }
     flush_tally<S>(t, tally_out);
 }
@@ -664,6 +747,7 @@ int launch_rounds(const DevIndex& ix, const DevReads& R, const DevParams& P, con
     static const int g_search = grid_blocks(wf_search_kernel<S, MS>, sm_count);
     static const int g_refill = grid_blocks(wf_search_refill_kernel<S, MR>, sm_count);
     static const int g_eval = grid_blocks(wf_eval_kernel<S, ME>, sm_count);  // EVAL_THREADS = 256
+    static const int g_eval_staged = grid_blocks(wf_eval_staged_kernel<S, ME>, sm_count);
     static const int g_fin = grid_blocks(wf_finalize_kernel<S>, sm_count);
     const unsigned init_blocks = static_cast<unsigned>((R.n_seq + 255) / 256);
     wf_init_kernel<<<init_blocks ? init_blocks : 1, 256, 0, st>>>(w, out, R.lens, R.n_seq);
@@ -681,7 +765,8 @@ int launch_rounds(const DevIndex& ix, const DevReads& R, const DevParams& P, con
         if (refill) wf_search_refill_kernel<S, MR><<<g_refill, 256, 0, st>>>(ix, R, P, w, act, width, tally);
         else wf_search_kernel<S, MS><<<g_search, 256, 0, st>>>(ix, R, P, w, act, width, tally);
         if (timed) cudaEventRecord(timer->e[3 * k + 1], st);
-        wf_eval_kernel<S, ME><<<g_eval, 256, 0, st>>>(ix, R, P, w, tally);
+        if (refill) wf_eval_staged_kernel<S, ME><<<g_eval_staged, 256, 0, st>>>(ix, R, P, w, tally);
+        else wf_eval_kernel<S, ME><<<g_eval, 256, 0, st>>>(ix, R, P, w, tally);
         if (timed) cudaEventRecord(timer->e[3 * k + 2], st);
         wf_finalize_kernel<S><<<g_fin, 256, 0, st>>>(ix, R, P, out, w, act, nxt, width, k == rounds - 1, d_err,
                                                      tally);
