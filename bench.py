@@ -77,6 +77,18 @@ def log(msg: str) -> None:
     sys.stderr.flush()
 
 
+def profiled_region(start: bool) -> None:
+    """cudaProfilerStart / cudaProfilerStop around the timed mapping steps:
+    `ncu --profile-from-start off` then captures exactly those launches (no
+    effect without a profiler)."""
+    import torch
+
+    if start:
+        torch.cuda.profiler.start()
+    else:
+        torch.cuda.profiler.stop()
+
+
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1180,6 +1192,7 @@ def run_ours(args, rank, world, local):
     seed_ms, stage1_ms, other_ms = [], [], []
     kms = (_lib.C.c_float * 4)()
     torch.cuda.synchronize()
+    profiled_region(True)
     ev0.record(stream)
     wave = []
     for _ in range(args.steps):
@@ -1191,6 +1204,7 @@ def run_ours(args, rank, world, local):
         wave.append(ctx.wave_ms())
     ev1.record(stream)
     torch.cuda.synchronize()
+    profiled_region(False)
     ms = ev0.elapsed_time(ev1) / args.steps
     clk = clocks.stop()
     dist.barrier()
@@ -1799,6 +1813,7 @@ def run_genome(args, rank, world, local):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     launches = 0
     torch.cuda.synchronize()
+    profiled_region(True)
     ev0.record(stream)
     for _ in range(args.steps):
         for a in range(0, n1, chunk):
@@ -1806,6 +1821,7 @@ def run_genome(args, rank, world, local):
             launches += ctx.last_launch_count()
     ev1.record(stream)
     torch.cuda.synchronize()
+    profiled_region(False)
     ms = ev0.elapsed_time(ev1) / args.steps
     clk = clocks.stop()
     dist.barrier()
