@@ -62,7 +62,9 @@ SEED_KERNELS = {
     1: "seed/extend: seed_stage1_kernel + seed_stage2_kernel (thread per read, then warp per read)",
     2: "seed/extend: wavefront rounds (wf_search_kernel + wf_eval_kernel + wf_finalize_kernel per round, "
        "seed_stage2_kernel for reads left over)",
-    3: "seed/extend: wavefront rounds with lane refill (wf_search_refill_kernel + wf_eval_kernel + "
+    3: "seed/extend: wavefront rounds with lane refill (wf_search_refill_kernel + wf_eval_staged_kernel + "
+       "wf_finalize_kernel per round, seed_stage2_kernel for reads left over)",
+    4: "seed/extend: wavefront rounds with staged eval (wf_search_kernel + wf_eval_staged_kernel + "
        "wf_finalize_kernel per round, seed_stage2_kernel for reads left over)",
 }
 READ_LEN = 150
@@ -1237,7 +1239,7 @@ def run_ours(args, rank, world, local):
     achieved = alg_bytes / (seed_avg_ms / 1000.0) / 1e9
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
             "frac": round(achieved / peaks.get("hbm_gbs"), 4),
-            "traffic": int(alg_bytes * TRAFFIC_OVER_ALG) if tune.tuning.get("seed_kernel") in (2, 3) else None,
+            "traffic": int(alg_bytes * TRAFFIC_OVER_ALG) if tune.tuning.get("seed_kernel") in (2, 3, 4) else None,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the seed kernels of one call "
                               "on the 50 Mbp / 2M-read case, as a ratio to the algorithmic bytes "
                               f"({TRAFFIC_OVER_ALG}), applied to this call's algorithmic bytes",

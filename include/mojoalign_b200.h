@@ -285,7 +285,12 @@ int ma_last_launch_count(const ma_ctx* ctx);
  *                         3: the wavefront with lane refill in its search
  *                         pass: each lane steps its own endpoint and takes
  *                         a new one when its search ends, so lanes do not
- *                         wait for the longest search of their warp.
+ *                         wait for the longest search of their warp, and
+ *                         staged shifts in its eval pass: the live shifts
+ *                         of a warp's loci are gathered in shared memory
+ *                         and evaluated 32 at a time, every lane busy;
+ *                         4: the wavefront with the search pass of 2 and
+ *                         the staged eval pass of 3.
  *   stage1_endpoints      endpoints stage 1 (or the first round) covers
  *                         (default 1).
  *   stage2_blocks_per_sm  persistent blocks per SM for stage 2 (0 = the
@@ -347,11 +352,14 @@ int ma_ctx_set_graphs(ma_ctx* ctx, int enable);
  * Chunking of ma_map_batch's copy / compute pipeline (result-neutral; no
  * reference counterpart: _fm_fire_batch runs fixed 16384-pair batches two
  * deep, linear_gpu_fm.mojo:2438-3094).  Chunk k+1 is copied in and chunk k-1
- * copied out while chunk k computes.
+ * copied out while chunk k computes.  Host arrays that are not page-locked
+ * (lengths, outputs) are staged through page-locked buffers of the context,
+ * so that their copies do not hold the calling thread; page-locked reads
+ * (bases) let their copies overlap the kernels as well.
  *   first_chunk_pairs  pairs of the first chunk (0 = max(65536, n1 / 64))
  *   growth_percent     each chunk is this much larger than the one before
  *                      (default 50)
- *   max_chunk_pairs    chunk size cap (0 = min(400000, max(131072, n1 / 4)))
+ *   max_chunk_pairs    chunk size cap (0 = min(2000000, max(131072, n1 / 16)))
  *   compute_streams    1: chunks compute in turn on the context's stream;
  *                      2 or 3 (default): consecutive chunks compute on that
  *                      many streams with their own work buffers, so one

@@ -73,6 +73,39 @@ struct DevBuf {
     T* as() const { return static_cast<T*>(p); }
 };
 
+// A grow-only page-locked host buffer (staging of host arrays that are
+// not page-locked, so that their copies can run asynchronously).
+struct HostBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    void ensure(size_t n) {
+        if (n <= cap) return;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        ck(cudaHostAlloc(&p, n ? n : 1, cudaHostAllocDefault), "cudaHostAlloc staging");
+        cap = n;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <typename T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// Whether a host pointer is ordinary pageable memory (a copy from or to it
+// is synchronous for the calling thread).
+bool pageable(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered;
+}
+
 }  // namespace
 
 struct ma_ctx {
@@ -96,6 +129,7 @@ struct ma_ctx {
     cudaEvent_t h2d_done[NSLOT] = {}, slot_free[NSLOT] = {}, comp_done[NSLOT] = {};
     struct Slot {
         DevBuf bases, lens, out[12];
+        HostBuf h_lens, h_out[12];  // staging of pageable caller arrays
     } slot[NSLOT];
     struct Lane {  // a second compute stream with its own work buffers
         DevBuf packed, seed_scratch;
@@ -447,6 +481,8 @@ void ma_ctx_destroy(ma_ctx* ctx) {
         sl.bases.release();
         sl.lens.release();
         for (DevBuf& b : sl.out) b.release();
+        sl.h_lens.release();
+        for (HostBuf& b : sl.h_out) b.release();
     }
     for (auto& ln : ctx->lane) {
         ln.packed.release();
@@ -661,12 +697,18 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
         // chunk k computes: three slots, three or four streams (ma_pipeline).
         // Chunks grow from a small first one (the pipeline fills quickly,
         // while large later chunks keep the kernels' per-call overhead
-        // small).
+        // small).  Caller arrays that are not page-locked (lengths,
+        // outputs) go through page-locked staging buffers of the slot: a
+        // copy from or to pageable memory would hold the calling thread
+        // until the chunk's kernels end and serialise the pipeline.  A
+        // slot's staged outputs are copied out when the slot is reused and
+        // after the last chunk.
         const ma_pipeline& pl = ctx->pipeline;
         const uint32_t first = std::min<uint32_t>(
             n1, pl.first_chunk_pairs ? pl.first_chunk_pairs : std::max<uint32_t>(65536u, n1 / 64));
         const uint32_t cap = std::max<uint32_t>(
-            first, pl.max_chunk_pairs ? pl.max_chunk_pairs : std::min<uint32_t>(400000u, std::max<uint32_t>(131072u, n1 / 4)));
+            first, pl.max_chunk_pairs ? pl.max_chunk_pairs
+                                      : std::min<uint32_t>(2000000u, std::max<uint32_t>(131072u, n1 / 16)));
         const int lanes = static_cast<int>(pl.compute_streams);
         const bool two = lanes > 1;
         const int mates = paired ? 2 : 1;
@@ -675,16 +717,44 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
                               want_dbg ? dbg->us : nullptr, want_dbg ? dbg->e : nullptr,
                               want_dbg ? dbg->score : nullptr};
         const size_t width[12] = {4, 4, 4, 4, 4, 4, 4, 8, 8, 4, 4, 4};
+        const bool stage_lens = pageable(lens);
+        bool stage_out[12];
+        bool any_stage = stage_lens;
+        for (int f = 0; f < 12; ++f) {
+            stage_out[f] = host_out[f] && pageable(host_out[f]);
+            any_stage = any_stage || stage_out[f];
+        }
         int k = 0;
         float acc_ms[4] = {0, 0, 0, 0};
-        // both slots sized for the largest chunk before any copy starts
+        // every slot sized for the largest chunk before any copy starts
         // (growing a buffer later would free memory still in use)
         for (auto& sl : ctx->slot) {
             const int64_t cs = static_cast<int64_t>(std::min(cap, n1)) * mates;
             sl.bases.ensure(static_cast<size_t>(cs) * max_len);
             sl.lens.ensure(cs * 4);
             for (int f = 0; f < 12; ++f) sl.out[f].ensure(cs * width[f]);
+            if (stage_lens) sl.h_lens.ensure(cs * 4);
+            for (int f = 0; f < 12; ++f)
+                if (stage_out[f]) sl.h_out[f].ensure(cs * width[f]);
         }
+        // the chunk (first pair, pairs) whose staged outputs slot i holds
+        uint32_t pend_a[ma_ctx::NSLOT], pend_c[ma_ctx::NSLOT];
+        bool pend[ma_ctx::NSLOT] = {};
+        auto drain = [&](int si) {  // the slot's previous chunk done: staged outputs out
+            if (!pend[si]) return;
+            ck(cudaEventSynchronize(ctx->slot_free[si]), "cudaEventSynchronize");
+            pend[si] = false;
+            const ma_ctx::Slot& sl = ctx->slot[si];
+            for (int f = 0; f < 12; ++f) {
+                if (!stage_out[f]) continue;
+                for (int m = 0; m < mates; ++m) {
+                    const size_t row0 = static_cast<size_t>(m) * n1 + pend_a[si];
+                    std::memcpy(static_cast<char*>(host_out[f]) + row0 * width[f],
+                                sl.h_out[f].as<char>() + static_cast<size_t>(m) * pend_c[si] * width[f],
+                                pend_c[si] * width[f]);
+                }
+            }
+        };
         // one error word for the call, cleared before any chunk computes
         ctx->err_flag.ensure(sizeof(int));
         ck(cudaMemsetAsync(ctx->err_flag.p, 0, sizeof(int), st), "memset");
@@ -704,13 +774,21 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
             ma_ctx::Lane& ln = ctx->lane[k % (lanes > 1 ? lanes : 1)];
             cudaStream_t cst = two ? ln.stream : st;
             // copy: wait until the slot's previous chunk has been read back
+            // (on the host too when its staging buffers are reused)
+            drain(si);
             ck(cudaStreamWaitEvent(ctx->copy_stream, ctx->slot_free[si], 0), "cudaStreamWaitEvent");
             for (int m = 0; m < mates; ++m) {
                 const size_t row0 = static_cast<size_t>(m) * n1 + a;
                 ck(cudaMemcpyAsync(sl.bases.as<uint8_t>() + static_cast<size_t>(m) * c * max_len,
                                    bases + row0 * max_len, static_cast<size_t>(c) * max_len, cudaMemcpyHostToDevice,
                                    ctx->copy_stream), "H2D bases");
-                ck(cudaMemcpyAsync(sl.lens.as<uint32_t>() + static_cast<size_t>(m) * c, lens + row0, c * 4,
+                const uint32_t* lsrc = lens + row0;
+                if (stage_lens) {
+                    uint32_t* h = sl.h_lens.as<uint32_t>() + static_cast<size_t>(m) * c;
+                    std::memcpy(h, lsrc, c * 4);
+                    lsrc = h;
+                }
+                ck(cudaMemcpyAsync(sl.lens.as<uint32_t>() + static_cast<size_t>(m) * c, lsrc, c * 4,
                                    cudaMemcpyHostToDevice, ctx->copy_stream), "H2D lens");
             }
             ck(cudaEventRecord(ctx->h2d_done[si], ctx->copy_stream), "cudaEventRecord");
@@ -742,6 +820,11 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
             ck(cudaStreamWaitEvent(ctx->d2h_stream, ctx->comp_done[si], 0), "cudaStreamWaitEvent");
             for (int f = 0; f < 12; ++f) {
                 if (!host_out[f]) continue;
+                if (stage_out[f]) {  // one copy of the chunk into the staging buffer
+                    ck(cudaMemcpyAsync(sl.h_out[f].p, sl.out[f].p, static_cast<size_t>(mates) * c * width[f],
+                                       cudaMemcpyDeviceToHost, ctx->d2h_stream), "D2H");
+                    continue;
+                }
                 for (int m = 0; m < mates; ++m) {
                     const size_t row0 = static_cast<size_t>(m) * n1 + a;
                     ck(cudaMemcpyAsync(static_cast<char*>(host_out[f]) + row0 * width[f],
@@ -750,10 +833,14 @@ int ma_map_batch(ma_ctx* ctx, const ma_index* idx, const uint8_t* bases, const u
                 }
             }
             ck(cudaEventRecord(ctx->slot_free[si], ctx->d2h_stream), "cudaEventRecord");
+            pend[si] = any_stage;
+            pend_a[si] = a;
+            pend_c[si] = c;
         }
         // the error word after the last copies back
         ck(cudaStreamWaitEvent(st, ctx->slot_free[(k - 1) % ma_ctx::NSLOT], 0), "cudaStreamWaitEvent");
         check_err_flag(ctx, st);
+        for (int i = 0; i < ma_ctx::NSLOT; ++i) drain(i);
         if (ctx->profiling & 1)
             for (int i = 0; i < 4; ++i) ctx->kernel_ms[i] = acc_ms[i];
     });
@@ -1616,7 +1703,7 @@ int ma_ctx_set_profiling(ma_ctx* ctx, int flags) {
 int ma_ctx_set_tuning(ma_ctx* ctx, const ma_tuning* t) {
     if (!ctx || !t) return MA_ERR_ARG;
     return guarded(ctx, [&] {
-        if (t->seed_kernel < 0 || t->seed_kernel > 3) fail(MA_ERR_ARG, "seed_kernel must be 0, 1, 2 or 3");
+        if (t->seed_kernel < 0 || t->seed_kernel > 4) fail(MA_ERR_ARG, "seed_kernel must be 0, 1, 2, 3 or 4");
         if (t->stage1_endpoints < 1) fail(MA_ERR_ARG, "stage1_endpoints must be >= 1");
         if (t->stage2_blocks_per_sm < 0 || t->stage2_blocks_per_sm > 64) fail(MA_ERR_ARG, "bad stage2_blocks_per_sm");
         if (t->reg_level < 0 || t->reg_level > 2) fail(MA_ERR_ARG, "reg_level must be 0, 1 or 2");

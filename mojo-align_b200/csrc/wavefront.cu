@@ -1,4 +1,4 @@
-// wavefront.cu - seed_kernels 2 and 3: the seed/extend search as rounds of
+// wavefront.cu - seed_kernels 2, 3 and 4: the seed/extend search as rounds of
 // data-parallel passes over the whole batch (fm_seed_extend_kernel,
 // fq2bam-meth/src/linear_gpu_fm.mojo:1156-1837, with the candidate order
 // and exactness argument of seed_core.cuh).
@@ -541,7 +541,7 @@ __global__ void __launch_bounds__(EVAL_THREADS, MINB) wf_eval_kernel(DevIndex ix
     flush_tally<S>(t, tally_out);
 }
 
-// Eval with staged shifts (seed_kernel 3): the filter pass as in
+// Eval with staged shifts (seed_kernels 3 and 4): the filter pass as in
 // wf_eval_kernel, but the live shifts (a fraction of a shift per locus at
 // genome scale) are staged per warp in shared memory and evaluated 32 at a
 // time, so the full compares run with every lane busy.
@@ -731,7 +731,8 @@ int grid_blocks(K kernel, int sm_count) {
 // 256 threads asked per SM (1 = the compiler's choice).
 template <bool S, int MS, int ME, int MR>
 int launch_rounds(const DevIndex& ix, const DevReads& R, const DevParams& P, const DevOut& out, const Wave& w,
-                  int max_len, int w0, int wn, int max_rounds, int growth, bool refill, int sm_count, int* d_err,
+                  int max_len, int w0, int wn, int max_rounds, int growth, bool refill, bool staged, int sm_count,
+                  int* d_err,
                   unsigned long long* tally, WaveTimer* timer, cudaStream_t st) {
     const int n_end_max = endpoint_count_host(P, max_len);
     // round widths: w0, then wn (doubling from the third round with growth)
@@ -765,7 +766,7 @@ int launch_rounds(const DevIndex& ix, const DevReads& R, const DevParams& P, con
         if (refill) wf_search_refill_kernel<S, MR><<<g_refill, 256, 0, st>>>(ix, R, P, w, act, width, tally);
         else wf_search_kernel<S, MS><<<g_search, 256, 0, st>>>(ix, R, P, w, act, width, tally);
         if (timed) cudaEventRecord(timer->e[3 * k + 1], st);
-        if (refill) wf_eval_staged_kernel<S, ME><<<g_eval_staged, 256, 0, st>>>(ix, R, P, w, tally);
+        if (staged) wf_eval_staged_kernel<S, ME><<<g_eval_staged, 256, 0, st>>>(ix, R, P, w, tally);
         else wf_eval_kernel<S, ME><<<g_eval, 256, 0, st>>>(ix, R, P, w, tally);
         if (timed) cudaEventRecord(timer->e[3 * k + 2], st);
         wf_finalize_kernel<S><<<g_fin, 256, 0, st>>>(ix, R, P, out, w, act, nxt, width, k == rounds - 1, d_err,
@@ -806,15 +807,16 @@ int launch_seed_wavefront(const DevIndex& ix, const DevReads& R, const DevParams
     const int wn = t.wave_endpoints > 0 ? t.wave_endpoints : 1;
     int launches = 0;
     const int mr = t.wave_max_rounds, gr = t.wave_growth;
-    const bool refill = t.seed_kernel == 3;
+    const bool refill = t.seed_kernel == 3;                         // lane-refill search
+    const bool staged = t.seed_kernel == 3 || t.seed_kernel == 4;  // staged-shift eval
     if (d_tally)
-        launches = launch_rounds<true, 1, 1, 1>(ix, R, P, out, w, max_len, w0, wn, mr, gr, refill, sm_count, d_err, d_tally, timer, st);
+        launches = launch_rounds<true, 1, 1, 1>(ix, R, P, out, w, max_len, w0, wn, mr, gr, refill, staged, sm_count, d_err, d_tally, timer, st);
     else if (t.reg_level == 1)
-        launches = launch_rounds<false, 5, 4, 4>(ix, R, P, out, w, max_len, w0, wn, mr, gr, refill, sm_count, d_err, nullptr, timer, st);
+        launches = launch_rounds<false, 5, 4, 4>(ix, R, P, out, w, max_len, w0, wn, mr, gr, refill, staged, sm_count, d_err, nullptr, timer, st);
     else if (t.reg_level == 2)
-        launches = launch_rounds<false, 6, 5, 5>(ix, R, P, out, w, max_len, w0, wn, mr, gr, refill, sm_count, d_err, nullptr, timer, st);
+        launches = launch_rounds<false, 6, 5, 5>(ix, R, P, out, w, max_len, w0, wn, mr, gr, refill, staged, sm_count, d_err, nullptr, timer, st);
     else
-        launches = launch_rounds<false, 1, 1, 1>(ix, R, P, out, w, max_len, w0, wn, mr, gr, refill, sm_count, d_err, nullptr, timer, st);
+        launches = launch_rounds<false, 1, 1, 1>(ix, R, P, out, w, max_len, w0, wn, mr, gr, refill, staged, sm_count, d_err, nullptr, timer, st);
     // reads that overflowed the locus list or outlived the rounds (their
     // tallies in the second half of the tally array, their time between
     // the timer's stage-2 events)

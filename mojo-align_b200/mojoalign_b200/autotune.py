@@ -12,7 +12,9 @@ search threads, so the round width is the warps-per-read choice: 4, 8 and
 CTA), 32, 64 and 128 endpoints give each read 1, 2 and 4 warps (8, 4 and 2
 reads per CTA).  The stage-2 warps take one read each.  seed_kernel 3 is the
 wavefront with lane refill in the search pass (each lane takes a new
-endpoint when its search ends).
+endpoint when its search ends) and staged shifts in the eval pass (the live
+shifts of a warp's loci evaluated 32 at a time); seed_kernel 4 combines the
+plain search pass with the staged eval pass.
 
 The seed stride is not swept: it decides which right endpoints are tried
 (linear_gpu_fm.mojo:1828) and so changes results.
@@ -50,6 +52,12 @@ DEFAULT_CANDIDATES = [
     (3, 2, 0, 1, 1, 1, 8, 16, 0, 1),
     (3, 1, 0, 2, 1, 1, 8, 16, 0, 1),
     (3, 1, 0, 1, 1, 1, 32, 16, 0, 0),
+    (4, 1, 0, 1, 1, 1, 8, 4, 0, 1),    # plain search, staged eval
+    (4, 1, 0, 1, 1, 1, 8, 16, 0, 1),
+    (4, 2, 0, 1, 1, 1, 8, 16, 0, 1),
+    (4, 2, 0, 2, 1, 1, 8, 16, 0, 1),
+    (2, 2, 0, 1, 1, 1, 8, 32, 0, 1),   # locus lists of 32 per read
+    (4, 2, 0, 1, 1, 1, 8, 32, 0, 1),
 ]
 FIELDS = ("seed_kernel", "stage1_endpoints", "stage2_blocks_per_sm", "reg_level", "stage1_max_rows",
           "stage2_first_wave", "wave_endpoints", "wave_loci_per_read", "wave_max_rounds", "wave_growth")

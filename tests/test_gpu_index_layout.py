@@ -31,7 +31,8 @@ def ctx():
 def _check(ctx, fa, prefix, layout, paired, max_len, seed, **model):
     rb = synth.simulate_reads(fa, synth.ReadModel(**model), 4000, paired, max_len, seed=seed)
     o = oracle.OracleIndex(prefix).map(rb.bases, rb.lens, rb.n1, paired, max_len, 1, 2, BENCH_PARAMS.as_list())
-    for tuning in ((0, 1, 0, 0, 16, 32), (2, 1, 0, 1, 2, 32, 8, 4, 0, 1), (3, 1, 0, 1, 2, 32, 8, 16, 0, 1)):
+    for tuning in ((0, 1, 0, 0, 16, 32), (2, 1, 0, 1, 2, 32, 8, 4, 0, 1), (3, 1, 0, 1, 2, 32, 8, 16, 0, 1),
+                   (4, 1, 0, 1, 2, 32, 8, 16, 0, 1)):
         ctx.set_tuning(*tuning)
         with GpuIndex(ctx, prefix, kmer_k=12, kmer3_k=19, **layout) as gi:
             g = map_batch(ctx, gi, rb.bases, rb.lens, rb.n1, paired, max_len, 1, 2, BENCH_PARAMS, debug=True)

@@ -41,11 +41,13 @@ def gpu_index(ctx, prefix, k, k3=0):
 # wave_max_rounds): one thread per read; two stages with the first 1, 2 or 3 right endpoints in stage 1, at
 # each register budget; wavefront rounds of several widths, with a locus list too small for the batch (reads
 # overflow to the stage-2 warps), with the rounds cut short (the rest finished by stage 2) and with doubling
-# round widths; the same with lane refill in the search pass (seed_kernel 3).
+# round widths; the same with lane refill in the search pass and staged eval (seed_kernel 3), and with the
+# staged eval alone (seed_kernel 4).
 TUNINGS = [(0, 1, 0, 0, 16, 32), (1, 1, 0, 1, 2, 32), (1, 3, 1, 2, 1, 1), (1, 2, 0, 0, 16, 4), (1, 1, 0, 2, 1, 7),
            (2, 1, 0, 1, 2, 32, 32, 4, 0), (2, 2, 0, 2, 1, 1, 5, 1, 0), (2, 1, 0, 0, 2, 32, 3, 4, 2),
            (2, 1, 0, 1, 1, 1, 4, 2, 0, 1), (3, 1, 0, 1, 2, 32, 32, 4, 0), (3, 2, 0, 2, 1, 1, 5, 1, 0),
-           (3, 1, 0, 0, 2, 32, 3, 4, 2), (3, 1, 0, 1, 1, 1, 8, 16, 0, 1)]
+           (3, 1, 0, 0, 2, 32, 3, 4, 2), (3, 1, 0, 1, 1, 1, 8, 16, 0, 1), (4, 1, 0, 1, 2, 32, 32, 4, 0),
+           (4, 2, 0, 2, 1, 1, 5, 1, 0), (4, 1, 0, 0, 2, 32, 3, 4, 2), (4, 2, 0, 1, 1, 1, 8, 16, 0, 1)]
 
 
 def compare(prefix, ctx, bases, lens, n1, paired, max_len, params, k=12, bs=(1, 2), tunings=TUNINGS, k3=12):
@@ -247,6 +249,51 @@ def test_host_batch_pipeline_matches_device_batch(ctx, small_ref):
     torch.cuda.synchronize()
     for f in FIELDS:
         assert np.array_equal(out[f].cpu().numpy(), getattr(host, f).view(out[f].cpu().numpy().dtype)), f
+
+
+@pytest.mark.parametrize("chunking", [(0, 50, 0, 3), (7000, 0, 7000, 1), (5000, 50, 60000, 2), (1, 100, 3, 3)])
+def test_host_batch_pinned_and_pageable_arrays(ctx, small_ref, chunking):
+    """ma_map_batch with page-locked lengths and outputs (copied directly)
+    and with pageable ones (staged through the context's page-locked
+    buffers): equal outputs for every chunking of the pipeline, pairs and
+    single-end, the staged outputs of every slot delivered."""
+    torch = pytest.importorskip("torch")
+    from mojoalign_b200 import MapResult, map_batch_device
+
+    fa, prefix = small_ref
+    gi = gpu_index(ctx, prefix, 12, 12)
+    dev = torch.device("cuda:0")
+    for paired, n in ((True, 20_000), (False, 30_011)):
+        rb = sim(fa, n, paired, seed=41 + paired, sub_rate=0.01)
+        if chunking[2] == 3:
+            rb = sim(fa, 40, paired, seed=43, sub_rate=0.01)  # chunks of 1, 2, 3 pairs
+        # the device-resident call is the reference
+        d_bases = torch.from_numpy(rb.bases.reshape(-1)).to(dev)
+        d_lens = torch.from_numpy(rb.lens.view(np.int32)).to(dev)
+        d_out = {f: torch.empty(rb.n_seq, dtype=torch.int64 if f in ("uk", "ul") else torch.int32, device=dev)
+                 for f in FIELDS}
+        map_batch_device(ctx, gi, d_bases.data_ptr(), d_lens.data_ptr(), rb.n1, paired, 150,
+                         {f: d_out[f].data_ptr() for f in MapResult.FIELDS}, "C2T", "G2A", BENCH_PARAMS,
+                         d_debug={f: d_out[f].data_ptr() for f in MapResult.DEBUG},
+                         stream=torch.cuda.current_stream(dev).cuda_stream)
+        torch.cuda.synchronize()
+        ref = {f: d_out[f].cpu().numpy() for f in FIELDS}
+        ctx.set_pipeline(*chunking)
+        try:
+            want = map_batch(ctx, gi, rb.bases, rb.lens, rb.n1, paired, 150, "C2T", "G2A", BENCH_PARAMS, debug=True)
+            pin = MapResult.empty(rb.n_seq, debug=True)
+            for f in FIELDS:
+                a = getattr(pin, f)
+                t = torch.empty(a.size, dtype=torch.int64 if a.itemsize == 8 else torch.int32, pin_memory=True)
+                setattr(pin, f, t.numpy().view(a.dtype))
+            lens = torch.from_numpy(rb.lens.view(np.int32).copy()).pin_memory().numpy().view(np.uint32)
+            bases = torch.from_numpy(rb.bases.copy()).pin_memory().numpy()
+            got = map_batch(ctx, gi, bases, lens, rb.n1, paired, 150, "C2T", "G2A", BENCH_PARAMS, out=pin)
+        finally:
+            ctx.set_pipeline()
+        for f in FIELDS:
+            assert np.array_equal(getattr(want, f).view(ref[f].dtype), ref[f]), ("pageable", paired, f)
+            assert np.array_equal(getattr(got, f).view(ref[f].dtype), ref[f]), ("page-locked", paired, f)
 
 
 @pytest.fixture(scope="module")

@@ -52,7 +52,7 @@ def oracle_map(prefix, req, params):
 
 
 @pytest.mark.parametrize("tuning", [None, (0, 1, 0, 1, 16, 32), (2, 1, 0, 1, 1, 1, 32, 4, 0),
-                                    (3, 1, 0, 2, 1, 1, 8, 4, 0, 1)])
+                                    (3, 1, 0, 2, 1, 1, 8, 4, 0, 1), (4, 1, 0, 2, 1, 1, 8, 4, 0, 1)])
 def test_served_requests_match_oracle(ctx, small_ref, tuning):
     fa, prefix = small_ref
     gi = GpuIndex(ctx, prefix, kmer_k=12, kmer3_k=12)
