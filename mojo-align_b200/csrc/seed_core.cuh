@@ -420,7 +420,10 @@ __device__ void eval_adj(const DevIndex& ix, const ReadView& rd, int64_t b0, int
 // acceptable compare; the deletion probe of shift 0 (forward) has
 // nm_d >= 1 + popc(M0 & M1) (shift 0 and +1 mismatch bits, any part of the
 // read), so it is dropped only when that bound reaches the same cap too.
-// Loci of a read shorter than the core halves keep every shift.
+// The per-shift count leaves out the read's N bases (an N mismatches every
+// text base, so leaving it out only lowers the count: the filter stays a
+// lower bound and keeps every shift that can win).  Loci of a read shorter
+// than the core halves keep every shift.
 template <bool S>
 __device__ uint32_t live_shifts(const DevIndex& ix, const ReadView& rd, int64_t b0, int is_rev, int adj_cap,
                                 int budget, int clip_cap, int prune_nm, Tally& t) {
@@ -447,43 +450,53 @@ __device__ uint32_t live_shifts(const DevIndex& ix, const ReadView& rd, int64_t 
     const uint32_t w3 = __ldg(p32 + wlo + 3), w4 = __ldg(p32 + wlo + 4), w5 = __ldg(p32 + wlo + 5);
     const uint32_t* q32 = reinterpret_cast<const uint32_t*>(q);
     const uint32_t* n32 = reinterpret_cast<const uint32_t*>(qn);
-    const uint32_t qa = q32[h0], na = n32[h0], ma = range_mask16(h0, c0, c1);
-    const uint32_t qb = nh > 1 ? q32[h0 + 1] : 0u, nb = nh > 1 ? n32[h0 + 1] : 0u;
-    const uint32_t mb = nh > 1 ? range_mask16(h0 + 1, c0, c1) : 0u;
-    const uint32_t qc = nh > 2 ? q32[h0 + 2] : 0u, nc = nh > 2 ? n32[h0 + 2] : 0u;
-    const uint32_t mc = nh > 2 ? range_mask16(h0 + 2, c0, c1) : 0u;
-    // mismatch bits of the three halves for the shift starting `off` bases in
-    auto halves = [&](int off, uint32_t& xa, uint32_t& xb, uint32_t& xc) {
-        const int k = off >> 4;
-        const uint32_t sh = static_cast<uint32_t>(off & 15) * 2;
+    const uint32_t qa = q32[h0], ma = range_mask16(h0, c0, c1);
+    const uint32_t qb = nh > 1 ? q32[h0 + 1] : 0u, mb = nh > 1 ? range_mask16(h0 + 1, c0, c1) : 0u;
+    const uint32_t qc = nh > 2 ? q32[h0 + 2] : 0u, mc = nh > 2 ? range_mask16(h0 + 2, c0, c1) : 0u;
+    if constexpr (S) t.read_words += 6;
+    // Mismatch bits of half b go to the odd bit positions (the halves' masks
+    // hold even bits), so halves a and b share one popcount.  Shifts run in
+    // three segments of 16 offsets, each with its own four text words.
+    const uint32_t mb_odd = mb << 1;
+    uint32_t live = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
         const uint32_t a = k == 0 ? w0 : (k == 1 ? w1 : w2);
         const uint32_t b = k == 0 ? w1 : (k == 1 ? w2 : w3);
         const uint32_t c = k == 0 ? w2 : (k == 1 ? w3 : w4);
         const uint32_t d = k == 0 ? w3 : (k == 1 ? w4 : w5);
-        const uint32_t ta = qa ^ __funnelshift_r(a, b, sh), tb = qb ^ __funnelshift_r(b, c, sh);
-        const uint32_t tc = qc ^ __funnelshift_r(c, d, sh);
-        xa = (((ta | (ta >> 1)) & 0x55555555u) | na) & ma;
-        xb = (((tb | (tb >> 1)) & 0x55555555u) | nb) & mb;
-        xc = (((tc | (tc >> 1)) & 0x55555555u) | nc) & mc;
-    };
-    if constexpr (S) t.read_words += 6;
-    uint32_t live = 0, z0a = 0, z0b = 0, z0c = 0, z1a = 0, z1b = 0, z1c = 0;  // shift 0 and +1 bits
-    for (int i = 0; i < A; ++i) {
-        uint32_t xa, xb, xc;
-        halves(s0 + i, xa, xb, xc);
-        if (__popc(xa) + __popc(xb) + __popc(xc) < cap) live |= 1u << i;
-        if (i == adj_cap) {
-            z0a = xa;
-            z0b = xb;
-            z0c = xc;
-        } else if (i == adj_cap + 1) {
-            z1a = xa;
-            z1b = xb;
-            z1c = xc;
+        const int lo = s0 > 16 * k ? s0 : 16 * k;
+        const int hi = s0 + A < 16 * k + 16 ? s0 + A : 16 * k + 16;
+        for (int off = lo; off < hi; ++off) {
+            const uint32_t sh = static_cast<uint32_t>(off - 16 * k) * 2;
+            const uint32_t ta = qa ^ __funnelshift_r(a, b, sh);
+            const uint32_t tb = qb ^ __funnelshift_r(b, c, sh);
+            const uint32_t tc = qc ^ __funnelshift_r(c, d, sh);
+            const uint32_t xab = ((ta | (ta >> 1)) & ma) | ((tb | (tb << 1)) & mb_odd);
+            const uint32_t xc = (tc | (tc >> 1)) & mc;
+            if (__popc(xab) + __popc(xc) < cap) live |= 1u << (off - s0);
         }
     }
     if (!is_rev && !((live >> adj_cap) & 1u)) {
-        if (adj_cap == 0) halves(s0 + 1, z1a, z1b, z1c);
+        // the deletion probe's bound from the exact mismatch bits (N bases
+        // included) of shifts 0 and +1
+        const uint32_t na = n32[h0], nb = nh > 1 ? n32[h0 + 1] : 0u, nc = nh > 2 ? n32[h0 + 2] : 0u;
+        auto halves = [&](int off, uint32_t& xa, uint32_t& xb, uint32_t& xc) {
+            const int k = off >> 4;
+            const uint32_t sh = static_cast<uint32_t>(off & 15) * 2;
+            const uint32_t a = k == 0 ? w0 : (k == 1 ? w1 : w2);
+            const uint32_t b = k == 0 ? w1 : (k == 1 ? w2 : w3);
+            const uint32_t c = k == 0 ? w2 : (k == 1 ? w3 : w4);
+            const uint32_t d = k == 0 ? w3 : (k == 1 ? w4 : w5);
+            const uint32_t ta = qa ^ __funnelshift_r(a, b, sh), tb = qb ^ __funnelshift_r(b, c, sh);
+            const uint32_t tc = qc ^ __funnelshift_r(c, d, sh);
+            xa = (((ta | (ta >> 1)) & 0x55555555u) | na) & ma;
+            xb = (((tb | (tb >> 1)) & 0x55555555u) | nb) & mb;
+            xc = (((tc | (tc >> 1)) & 0x55555555u) | nc) & mc;
+        };
+        uint32_t z0a, z0b, z0c, z1a, z1b, z1c;
+        halves(s0 + adj_cap, z0a, z0b, z0c);
+        halves(s0 + adj_cap + 1, z1a, z1b, z1c);
         if (1 + __popc(z0a & z1a) + __popc(z0b & z1b) + __popc(z0c & z1c) < cap) live |= 1u << adj_cap;
     }
     return live;
