@@ -1217,11 +1217,12 @@ def run_ours(args, rank, world, local):
     log("end to end")
     # ---- end to end through the host API (pinned host in, host out) ----
     _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 0), ctx.handle)  # per-chunk timing would serialise
-    host_out = MapResult.empty(n_seq, debug=False)
-    pin_out = {f: torch.empty(n_seq, dtype=torch.int32, pin_memory=True) for f in MapResult.FIELDS}
-    res = MapResult(*[pin_out[f].numpy().view(getattr(host_out, f).dtype) for f in MapResult.FIELDS])
+    from mojoalign_b200.mapper import page_locked
+
+    res = MapResult.empty(n_seq, debug=False, pinned=True)
     bases_np = pinned.numpy()
-    lens_np = rb.lens
+    lens_np = page_locked(n_seq, np.uint32)
+    lens_np[:] = rb.lens
     map_batch(ctx, gi, bases_np, lens_np, args.pairs, True, READ_LEN, "C2T", "G2A", params, out=res)
     dist.barrier()
     t = time.perf_counter()
@@ -1835,12 +1836,16 @@ def run_genome(args, rank, world, local):
     log("end to end")
     # ---- end to end from pinned host buffers (copies inside) ----
     _lib.check(_lib.lib.ma_ctx_set_profiling(ctx.handle, 0), ctx.handle)
-    res = MapResult.empty(n_seq, debug=False)
-    map_batch(ctx, gi, bases_np, lens_np, n1, paired, max_len, bs1, bs2, params, out=res)
+    from mojoalign_b200.mapper import page_locked
+
+    res = MapResult.empty(n_seq, debug=False, pinned=True)
+    lens_pin = page_locked(n_seq, np.uint32)
+    lens_pin[:] = lens_np
+    map_batch(ctx, gi, bases_np, lens_pin, n1, paired, max_len, bs1, bs2, params, out=res)
     dist.barrier()
     t = time.perf_counter()
     for _ in range(args.steps):
-        map_batch(ctx, gi, bases_np, lens_np, n1, paired, max_len, bs1, bs2, params, out=res)
+        map_batch(ctx, gi, bases_np, lens_pin, n1, paired, max_len, bs1, bs2, params, out=res)
     e2e_s = dist.max((time.perf_counter() - t) / args.steps)
     e2e_same = all(np.array_equal(getattr(res, f).view(np.int32), batched_out[f]) for f in MapResult.FIELDS)
 

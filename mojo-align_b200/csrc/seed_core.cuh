@@ -454,40 +454,41 @@ __device__ uint32_t live_shifts(const DevIndex& ix, const ReadView& rd, int64_t 
     const uint32_t qb = nh > 1 ? q32[h0 + 1] : 0u, mb = nh > 1 ? range_mask16(h0 + 1, c0, c1) : 0u;
     const uint32_t qc = nh > 2 ? q32[h0 + 2] : 0u, mc = nh > 2 ? range_mask16(h0 + 2, c0, c1) : 0u;
     if constexpr (S) t.read_words += 6;
-    // Mismatch bits of half b go to the odd bit positions (the halves' masks
-    // hold even bits), so halves a and b share one popcount.  Shifts run in
-    // three segments of 16 offsets, each with its own four text words.
+    // The text words realigned so that shift i starts i bases into them:
+    // the offset of a shift's words and its funnel-shift amount are then the
+    // same for every lane (no divergence between loci whose windows start at
+    // different bases).  Mismatch bits of half b go to the odd bit
+    // positions (the halves' masks hold even bits), so halves a and b share
+    // one popcount.
+    const uint32_t sa = static_cast<uint32_t>(s0) * 2;
+    const uint32_t W0 = __funnelshift_r(w0, w1, sa), W1 = __funnelshift_r(w1, w2, sa);
+    const uint32_t W2 = __funnelshift_r(w2, w3, sa), W3 = __funnelshift_r(w3, w4, sa);
+    const uint32_t W4 = __funnelshift_r(w4, w5, sa);
     const uint32_t mb_odd = mb << 1;
     uint32_t live = 0;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const uint32_t a = k == 0 ? w0 : (k == 1 ? w1 : w2);
-        const uint32_t b = k == 0 ? w1 : (k == 1 ? w2 : w3);
-        const uint32_t c = k == 0 ? w2 : (k == 1 ? w3 : w4);
-        const uint32_t d = k == 0 ? w3 : (k == 1 ? w4 : w5);
-        const int lo = s0 > 16 * k ? s0 : 16 * k;
-        const int hi = s0 + A < 16 * k + 16 ? s0 + A : 16 * k + 16;
-        for (int off = lo; off < hi; ++off) {
-            const uint32_t sh = static_cast<uint32_t>(off - 16 * k) * 2;
+    for (int k = 0; k < 2; ++k) {  // A <= 25: shifts 0..15 and 16..A-1
+        const uint32_t a = k == 0 ? W0 : W1, b = k == 0 ? W1 : W2;
+        const uint32_t c = k == 0 ? W2 : W3, d = k == 0 ? W3 : W4;
+        const int hi = A < 16 * k + 16 ? A : 16 * k + 16;
+        for (int i = 16 * k; i < hi; ++i) {
+            const uint32_t sh = static_cast<uint32_t>(i - 16 * k) * 2;
             const uint32_t ta = qa ^ __funnelshift_r(a, b, sh);
             const uint32_t tb = qb ^ __funnelshift_r(b, c, sh);
             const uint32_t tc = qc ^ __funnelshift_r(c, d, sh);
             const uint32_t xab = ((ta | (ta >> 1)) & ma) | ((tb | (tb << 1)) & mb_odd);
             const uint32_t xc = (tc | (tc >> 1)) & mc;
-            if (__popc(xab) + __popc(xc) < cap) live |= 1u << (off - s0);
+            if (__popc(xab) + __popc(xc) < cap) live |= 1u << i;
         }
     }
     if (!is_rev && !((live >> adj_cap) & 1u)) {
         // the deletion probe's bound from the exact mismatch bits (N bases
         // included) of shifts 0 and +1
         const uint32_t na = n32[h0], nb = nh > 1 ? n32[h0 + 1] : 0u, nc = nh > 2 ? n32[h0 + 2] : 0u;
-        auto halves = [&](int off, uint32_t& xa, uint32_t& xb, uint32_t& xc) {
-            const int k = off >> 4;
-            const uint32_t sh = static_cast<uint32_t>(off & 15) * 2;
-            const uint32_t a = k == 0 ? w0 : (k == 1 ? w1 : w2);
-            const uint32_t b = k == 0 ? w1 : (k == 1 ? w2 : w3);
-            const uint32_t c = k == 0 ? w2 : (k == 1 ? w3 : w4);
-            const uint32_t d = k == 0 ? w3 : (k == 1 ? w4 : w5);
+        auto halves = [&](int i, uint32_t& xa, uint32_t& xb, uint32_t& xc) {
+            const bool hi16 = i >= 16;
+            const uint32_t sh = static_cast<uint32_t>(i & 15) * 2;
+            const uint32_t a = hi16 ? W1 : W0, b = hi16 ? W2 : W1, c = hi16 ? W3 : W2, d = hi16 ? W4 : W3;
             const uint32_t ta = qa ^ __funnelshift_r(a, b, sh), tb = qb ^ __funnelshift_r(b, c, sh);
             const uint32_t tc = qc ^ __funnelshift_r(c, d, sh);
             xa = (((ta | (ta >> 1)) & 0x55555555u) | na) & ma;
@@ -495,8 +496,8 @@ __device__ uint32_t live_shifts(const DevIndex& ix, const ReadView& rd, int64_t 
             xc = (((tc | (tc >> 1)) & 0x55555555u) | nc) & mc;
         };
         uint32_t z0a, z0b, z0c, z1a, z1b, z1c;
-        halves(s0 + adj_cap, z0a, z0b, z0c);
-        halves(s0 + adj_cap + 1, z1a, z1b, z1c);
+        halves(adj_cap, z0a, z0b, z0c);
+        halves(adj_cap + 1, z1a, z1b, z1c);
         if (1 + __popc(z0a & z1a) + __popc(z0b & z1b) + __popc(z0c & z1c) < cap) live |= 1u << adj_cap;
     }
     return live;

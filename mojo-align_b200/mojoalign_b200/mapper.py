@@ -172,6 +172,17 @@ class GpuIndex:
             pass
 
 
+def page_locked(n: int, dtype) -> np.ndarray:
+    """A page-locked host array of n elements (its memory stays valid while
+    the array, or a view of it, lives)."""
+    import torch
+
+    dt = np.dtype(dtype)
+    t = torch.empty(n * dt.itemsize, dtype=torch.uint8, pin_memory=True)
+    a = t.numpy().view(dt)
+    return a
+
+
 @dataclass
 class MapResult:
     rid: np.ndarray
@@ -191,15 +202,18 @@ class MapResult:
     DEBUG = ("uk", "ul", "us", "e", "score")
 
     @classmethod
-    def empty(cls, n: int, debug: bool) -> "MapResult":
-        r = cls(np.empty(n, np.int32), np.empty(n, np.uint32), np.empty(n, np.uint32), np.empty(n, np.int32),
-                np.empty(n, np.uint32), np.empty(n, np.uint32), np.empty(n, np.uint32))
+    def empty(cls, n: int, debug: bool, pinned: bool = False) -> "MapResult":
+        """Output arrays for n reads; pinned=True allocates them page-locked,
+        so that map_batch copies the results straight into them."""
+        alloc = page_locked if pinned else np.empty
+        r = cls(alloc(n, np.int32), alloc(n, np.uint32), alloc(n, np.uint32), alloc(n, np.int32),
+                alloc(n, np.uint32), alloc(n, np.uint32), alloc(n, np.uint32))
         if debug:
-            r.uk = np.empty(n, np.uint64)
-            r.ul = np.empty(n, np.uint64)
-            r.us = np.empty(n, np.int32)
-            r.e = np.empty(n, np.int32)
-            r.score = np.empty(n, np.int32)
+            r.uk = alloc(n, np.uint64)
+            r.ul = alloc(n, np.uint64)
+            r.us = alloc(n, np.int32)
+            r.e = alloc(n, np.int32)
+            r.score = alloc(n, np.int32)
         return r
 
     def hits(self) -> ma_hits:
