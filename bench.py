@@ -55,6 +55,7 @@ METRIC = "reads/s seed+extend"
 # tuning, and null otherwise.
 GENOME_SEED_DRAM_BYTES_PER_READ = 27486
 GENOME_SEED_DRAM_TUNING = (4, 2, 0, 1, 1, 1, 8, 32, 0, 1)
+GENOME_SEED_DRAM_AT_K = 0  # the capture's A/T window table (0: none)
 # The workload parameters: the reference defaults with seed_len 19 and
 # max_occ 500 (mojoalign_b200.params.BENCH_PARAMS holds the same values; the
 # reference arm takes them from here so that it loads nothing of the
@@ -105,6 +106,8 @@ def parse_args():
     ap.add_argument("--pairs", type=int, default=10_000_000, help="read pairs per GPU")
     ap.add_argument("--kmer", type=int, default=12)
     ap.add_argument("--kmer3", type=int, default=19, help="converted-alphabet k-mer tables (<= seed_len)")
+    ap.add_argument("--at-k", type=int, default=28, help="A/T window outcome table: window length (0 = none); "
+                    "built for the workload's seed length")
     ap.add_argument("--workdir", default=os.environ.get("MOJOALIGN_BENCH_DIR", tempfile.gettempdir()))
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the oracle timing (profiling runs)")
@@ -1126,7 +1129,8 @@ def run_ours(args, rank, world, local):
     ctx = GpuContext(local)
     t = time.time()
     log("index open")
-    gi = GpuIndex(ctx, prefix, kmer_k=args.kmer, kmer3_k=args.kmer3)
+    gi = GpuIndex(ctx, prefix, kmer_k=args.kmer, kmer3_k=args.kmer3, at_k=args.at_k,
+                  at_seed_len=params.seed_len if args.at_k else 0)
     open_s = time.time() - t
     log("autotune")
 
@@ -1263,7 +1267,7 @@ def run_ours(args, rank, world, local):
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": workload_config(args),
             "run": {"tuning": tune.tuning, "autotune_sample_reads": 2 * ns, "kmer_k": args.kmer,
-                    "kmer3_k": args.kmer3, "index_hbm_bytes": int(gi.info.device_bytes),
+                    "kmer3_k": args.kmer3, "at_k": args.at_k, "index_hbm_bytes": int(gi.info.device_bytes),
                     "mapped_frac": round(mapped, 4)},
             "e2e": {"value": round(e2e_value, 1), "unit": "reads/s",
                     "h2d_bytes_per_step": int(n_seq * READ_LEN + n_seq * 4),
@@ -1377,7 +1381,8 @@ def chromosome_stages(args, local, params, peaks) -> dict:
     log(f"stages: {pairs} pairs on the {args.genome_mb} Mbp reference")
     rb = simulate(sub, fa, 0)
     ctx = GpuContext(local)
-    gi = GpuIndex(ctx, prefix, kmer_k=args.kmer, kmer3_k=args.kmer3)
+    gi = GpuIndex(ctx, prefix, kmer_k=args.kmer, kmer3_k=args.kmer3, at_k=args.at_k,
+                  at_seed_len=params.seed_len if args.at_k else 0)
     res = MapResult.empty(rb.n_seq, debug=False)
     map_batch(ctx, gi, rb.bases, rb.lens, rb.n1, True, READ_LEN, "C2T", "G2A", params, out=res)
     try:
@@ -1696,7 +1701,8 @@ def run_genome(args, rank, world, local):
         if turn == rank:
             log("index open")
             t = time.time()
-            gi = GpuIndex(ctx, prefix, kmer_k=args.kmer, kmer3_k=args.kmer3)
+            gi = GpuIndex(ctx, prefix, kmer_k=args.kmer, kmer3_k=args.kmer3, at_k=args.at_k,
+                          at_seed_len=params.seed_len if args.at_k else 0)
             timings["index_open"] = time.time() - t
         dist.barrier()
     bases_np, lens_np = pinned.numpy(), rb.lens
@@ -1869,7 +1875,7 @@ def run_genome(args, rank, world, local):
                  "shift_evals"], tally)}}
     roof.update(seeding_roofline(tally, wave, tally2, n_seq, tune.tuning.get("seed_kernel", 2)))
     if (GENOME_SEED_DRAM_BYTES_PER_READ and spec is GENOME_WORKLOADS["genome"] and mb == spec["genome_mb"]
-            and n1 == spec["n1"] and tuple(best) == GENOME_SEED_DRAM_TUNING):
+            and n1 == spec["n1"] and tuple(best) == GENOME_SEED_DRAM_TUNING and args.at_k == GENOME_SEED_DRAM_AT_K):
         roof["traffic"] = int(GENOME_SEED_DRAM_BYTES_PER_READ * n_seq)
         roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the seed kernels of one timed "
                                   "step of this workload and tuning (one-pass capture of this build), per read x reads")
@@ -1880,7 +1886,7 @@ def run_genome(args, rank, world, local):
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": genome_config(args, spec, n1),
             "run": {"tuning": tune.tuning, "autotune": tune.all_ms, "kmer_k": args.kmer, "kmer3_k": args.kmer3,
-                    "index_hbm_bytes": int(gi.info.device_bytes), "calls_per_step": -(-n1 // chunk),
+                    "at_k": args.at_k, "index_hbm_bytes": int(gi.info.device_bytes), "calls_per_step": -(-n1 // chunk),
                     "cuda_graphs": "each device call replays its captured graph (one host launch per call)",
                     "mapped_frac": round(float((batched_out["rid"] >= 0).mean()), 4)},
             "e2e": {"value": round(aggregate_reads_per_s(n_seq, world, e2e_s * 1000.0), 1), "unit": "reads/s",

@@ -129,6 +129,16 @@ typedef struct ma_index_info {
  *             lines count symbols from the start of their superblock.
  *   prep_chunk_rows   SA rows per preparation pass of the k-mer tables and
  *             the seed summary (0 = 2^30; at least 512).
+ *   at_k, at_seed_len   A/T window outcome table: for every read window of
+ *             at_k bases that holds only A and T (2^at_k windows, 16 bytes
+ *             each; 0 = none, else at_seed_len..30), the whole outcome of
+ *             the backward search over it for seed length at_seed_len (the
+ *             seed it returns, none, or the interval it continues from).
+ *             Reads from the strand the conversion does not match are
+ *             nearly all A/T after conversion, and their searches step back
+ *             several bases past the k-mer tables; a search whose last
+ *             at_k bases are A/T starts from this one lookup instead.  Used
+ *             only by calls whose seed_len equals at_seed_len.
  * A table is used by a mapping call only when its k <= seed_len.  Texts of
  * up to 2^35 - 2 symbols (seq_len) are supported.
  */
@@ -139,6 +149,8 @@ typedef struct ma_index_options {
     int32_t wide_rows;
     int32_t occ_super_shift;
     uint64_t prep_chunk_rows;
+    int32_t at_k;
+    int32_t at_seed_len;
 } ma_index_options;
 void ma_index_options_default(ma_index_options* o);
 

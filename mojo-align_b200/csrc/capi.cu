@@ -547,6 +547,8 @@ void ma_index_options_default(ma_index_options* o) {
     o->wide_rows = 0;
     o->occ_super_shift = 0;
     o->prep_chunk_rows = 0;
+    o->at_k = 0;
+    o->at_seed_len = 0;
 }
 
 namespace {
@@ -557,6 +559,8 @@ LayoutOptions layout_of(const ma_index_options& o) {
     lo.wide_rows = o.wide_rows != 0;
     lo.occ_super_shift = o.occ_super_shift ? o.occ_super_shift : OCC_SUPER_SHIFT;
     lo.prep_chunk_rows = o.prep_chunk_rows;
+    lo.at_k = o.at_k;
+    lo.at_seed_len = o.at_seed_len;
     return lo;
 }
 }  // namespace

@@ -173,6 +173,61 @@ __global__ void build_kmer_kernel(DevIndex ix, int K, uint64_t n_kmers, uint64_t
     out[idx] = kmer_entry(k, l - k + 1);
 }
 
+// A/T window outcome table: one thread per window W of K bases over A/T
+// (index bit i set where base i of W is T).  The backward search over W
+// from its last base with seed length sl and no max_occ stop, as
+// search_start / search_next in seed_core.cuh run it: the first length
+// >= sl with one row ends it with that seed; an empty interval ends it
+// with the last interval of <= 16 rows at a length >= sl, if any; else it
+// continues past W from the rows of all of W.
+__global__ void build_atw_kernel(DevIndex ix, int K, int sl, uint64_t n, uint4* __restrict__ out) {
+    const uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (idx >= n) return;
+    uint64_t k = 0, l = ix.seq_len, c_sl = 0;
+    uint64_t kept_k = 0, kept_n = 0;
+    int kept_o = -1;
+    uint64_t lo = 0, hi = 0;  // kind 0 unless set below
+    bool done = false;
+    for (int t = 0; t < K && !done; ++t) {
+        const int c = (idx >> (K - 1 - t)) & 1 ? 3 : 0;  // base K-1-t of W
+        const uint64_t ok = k != 0 ? occ_row(ix, k - 1, c) : 0;
+        const uint64_t ol = occ_row(ix, l, c);
+        k = ix.L2[c] + ok + 1;
+        l = ix.L2[c] + ol;
+        const int mlen = t + 1;
+        if (k > l) {
+            if (kept_o >= 0) {
+                lo = kept_k | static_cast<uint64_t>(kept_o) << 35 | 1ull << 40;
+                hi = kept_n;
+            }
+            done = true;
+            break;
+        }
+        const uint64_t rows = l - k + 1;
+        if (mlen == sl) c_sl = rows < ATW_COUNT_CAP ? rows : ATW_COUNT_CAP;
+        if (mlen >= sl) {
+            if (rows == 1) {
+                lo = k | static_cast<uint64_t>(mlen - 1) << 35 | 1ull << 40;
+                hi = 1;
+                done = true;
+                break;
+            }
+            if (rows <= 16) {
+                kept_k = k;
+                kept_n = rows;
+                kept_o = mlen - 1;
+            }
+        }
+    }
+    if (!done) {  // continues from the rows of W (>= 2 of them)
+        lo = k | 2ull << 40;
+        hi = l - k + 1;
+    }
+    hi |= c_sl << 35;
+    out[idx] = make_uint4(static_cast<uint32_t>(lo), static_cast<uint32_t>(lo >> 32), static_cast<uint32_t>(hi),
+                          static_cast<uint32_t>(hi >> 32));
+}
+
 // 2-bit codes of text T[p, p+K) (T = the pac followed by its reverse
 // complement), first base most significant; ~0 when p + K > seq_len.
 __device__ uint64_t text_kmer(const DevIndex& ix, uint64_t p, int K) {
@@ -377,6 +432,7 @@ uint64_t device_index_bytes(const BwaIndexHost& h, const LayoutOptions& lo) {
     b += ((h.l_pac + 31) / 32 + 2 * PAC_PAD) * 8;
     if (lo.kmer_k > 0) b += (1ull << (2 * lo.kmer_k)) * 8;
     if (lo.kmer3_k > 0) b += 2 * pow3(lo.kmer3_k) * 8 + h.seq_len * 2;
+    if (lo.at_k > 0) b += (1ull << lo.at_k) * 16;
     b += h.contigs.size() * 12;
     return b;
 }
@@ -398,6 +454,8 @@ DevIndex build_device_index(const BwaIndexHost& h, const LayoutOptions& lo, cuda
     if (lo.kmer_k < 0 || lo.kmer_k > 14) fail(MA_ERR_ARG, "kmer_k must be in 0..14");
     if (lo.kmer3_k < 0 || lo.kmer3_k > 20) fail(MA_ERR_ARG, "kmer3_k must be in 0..20");
     if (lo.occ_super_shift < 7 || lo.occ_super_shift > 31) fail(MA_ERR_ARG, "occ superblock shift must be in 7..31");
+    if (lo.at_k < 0 || lo.at_k > ATW_MAX_K || (lo.at_k > 0 && (lo.at_seed_len < 1 || lo.at_seed_len > lo.at_k)))
+        fail(MA_ERR_ARG, "at_k must be 0 or in at_seed_len..30, at_seed_len >= 1");
     const int kmer_k = lo.kmer_k, kmer3_k = lo.kmer3_k;
     const uint64_t n_lines = (h.seq_len + 63) / 64;
     const uint64_t n_pacw = (h.l_pac + 31) / 32 + 2 * PAC_PAD;
@@ -521,6 +579,15 @@ DevIndex build_device_index(const BwaIndexHost& h, const LayoutOptions& lo, cuda
             check(cudaGetLastError(), "build_kmer launch");
             ix.kmer = bufs.kmer;
         }
+        if (lo.at_k > 0) {
+            const uint64_t na = 1ull << lo.at_k;
+            check(cudaMalloc(&bufs.atw, na * 16), "cudaMalloc A/T window table");
+            build_atw_kernel<<<grid_for(na, 256), 256, 0, st>>>(ix, lo.at_k, lo.at_seed_len, na, bufs.atw);
+            check(cudaGetLastError(), "build_atw launch");
+            ix.atw = bufs.atw;
+            ix.at_k = lo.at_k;
+            ix.at_seed_len = lo.at_seed_len;
+        }
         if (kmer3_k > 0) {
             const uint64_t n3 = pow3(kmer3_k);
             const uint64_t C = chunk_rows(h, lo);
@@ -582,6 +649,7 @@ void free_device_index(DeviceIndexBuffers& b) {
     cudaFree(b.kmer3[0]);
     cudaFree(b.kmer3[1]);
     cudaFree(b.summary);
+    cudaFree(b.atw);
     cudaFree(b.coff);
     cudaFree(b.clen);
     b = DeviceIndexBuffers{};

@@ -31,6 +31,17 @@
 //         occurrences of the kmer3_k-mer ending at x (capped at 255).  T is
 //         its own reverse complement, so these are the shortest unique prefix
 //         and the k-mer count of the suffix starting at 2*l_pac-1-x.
+//   atw   for every read window W of at_k bases over A and T alone (bit i
+//         of the index set where base i of W, first base at bit 0, is T),
+//         the outcome of the backward search from W's last base over W
+//         with seed length at_seed_len and no max_occ stop, 16 bytes:
+//         lo = k (bits 0-34) | o (35-39) | kind (40-41),
+//         hi = n (bits 0-34) | c (35-63), where kind 0: the search ends with
+//         no seed; kind 1: it ends with the seed of rows [k, k+n) whose
+//         pattern is the last o+1 bases of W; kind 2: it continues past W
+//         from the n >= 2 rows [k, k+n) of all of W; c = the rows at
+//         length at_seed_len (0 when empty before it, capped at 2^29 - 1),
+//         which decides the max_occ stop at run time.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -59,6 +70,8 @@ constexpr uint64_t KMER_MAX_COUNT = (1ull << (64 - KMER_K_BITS)) - 2;
 constexpr uint64_t KMER_UNTABLED = ~0ull;
 constexpr uint64_t SA40_UNSET = (1ull << 40) - 1;
 constexpr int OCC_SUPER_SHIFT = 31;  // default superblock: 2^31 positions
+constexpr int ATW_MAX_K = 30;                            // longest A/T window of the outcome table
+constexpr uint64_t ATW_COUNT_CAP = (1ull << 29) - 1;     // rows at the seed length, saturated
 
 struct DevIndex {
     const OccLine* occ;
@@ -79,6 +92,9 @@ struct DevIndex {
     uint64_t sa_reject_below;  // sa_pos below this is rejected (see seed kernel)
     int32_t kmer_k;
     int32_t kmer3_k;
+    const uint4* atw;         // A/T window outcome table (see "atw" above), or null
+    int32_t at_k;             // window length of atw (0: no table)
+    int32_t at_seed_len;      // seed length the outcomes hold for
 };
 
 // Mapping parameters after the reference's clamps are applied per read.
@@ -220,6 +236,7 @@ struct DeviceIndexBuffers {
     uint64_t* kmer = nullptr;
     uint64_t* kmer3[2] = {nullptr, nullptr};
     uint16_t* summary = nullptr;
+    uint4* atw = nullptr;
     uint64_t* coff = nullptr;
     uint32_t* clen = nullptr;
     uint64_t bytes = 0;
@@ -232,6 +249,8 @@ struct LayoutOptions {
     bool wide_rows = false;         // 40-bit SA rows even when u32 would do
     int occ_super_shift = OCC_SUPER_SHIFT;
     uint64_t prep_chunk_rows = 0;   // rows per preparation pass (0 = automatic)
+    int at_k = 0;                   // A/T window outcome table: window length (0 = none)
+    int at_seed_len = 0;            // and the seed length its outcomes hold for
 };
 
 struct BwaIndexHost;

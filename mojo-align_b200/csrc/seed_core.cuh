@@ -86,6 +86,17 @@ __device__ __forceinline__ uint64_t window_bits(const uint64_t* words, int s, in
     return n >= 32 ? v : (v & ((1ull << (2 * n)) - 1));
 }
 
+// Bits 0, 2, 4, ... of x gathered into bits 0, 1, 2, ...
+__device__ __forceinline__ uint32_t compact_even(uint64_t x) {
+    x &= kEven;
+    x = (x | (x >> 1)) & 0x3333333333333333ull;
+    x = (x | (x >> 2)) & 0x0F0F0F0F0F0F0F0Full;
+    x = (x | (x >> 4)) & 0x00FF00FF00FF00FFull;
+    x = (x | (x >> 8)) & 0x0000FFFF0000FFFFull;
+    x = (x | (x >> 16)) & 0x00000000FFFFFFFFull;
+    return static_cast<uint32_t>(x);
+}
+
 // Per-thread traffic tally of the counting kernel variant (S = true).  The
 // timed kernel is the S = false instantiation, where every tally compiles
 // away.
@@ -641,6 +652,44 @@ __device__ __forceinline__ bool search_start(const DevIndex& ix, const ReadView&
     out = Seed{0, 0, -1, false};
     bool have = false;  // a table gave the interval after the first K steps
     int K = 0;
+    // A/T window outcome table: the whole search over the last at_k bases
+    // in one lookup when they are all A or T.  Counts never grow as the
+    // pattern extends, so the max_occ stop can only come at seed_len: with
+    // c rows there (c > max_occ) the search stops with no seed, unless
+    // c <= 16 made that interval the kept one (then the steps below run).
+    const int AK = ix.at_k;
+    if (AK > 0 && P.seed_len == ix.at_seed_len && e >= AK - 1) {
+        const int s0 = e - AK + 1;
+        const uint64_t win = window_bits(rd.fwd, s0, AK);
+        const uint64_t lo = win & kEven, hi = (win >> 1) & kEven;
+        if (lo == hi && window_bits(rd.nf, s0, AK) == 0) {
+            const uint4 v = __ldg(ix.atw + compact_even(lo));
+            if constexpr (S) t.kmer_loads++;
+            const uint64_t elo = static_cast<uint64_t>(v.x) | static_cast<uint64_t>(v.y) << 32;
+            const uint64_t ehi = static_cast<uint64_t>(v.z) | static_cast<uint64_t>(v.w) << 32;
+            const uint64_t c_sl = ehi >> 35;
+            const uint64_t rk = elo & KMER_K_MASK, rn = ehi & KMER_K_MASK;
+            const int kind = static_cast<int>(elo >> 40) & 3;
+            if (c_sl > static_cast<uint64_t>(P.max_occ)) {
+                if (c_sl > 16) return false;  // stopped at seed_len, nothing kept
+            } else if (kind == 0) {
+                return false;
+            } else if (kind == 1) {
+                out = Seed{rk, rk + rn - 1, e - static_cast<int>((elo >> 35) & 31), true};
+                return false;
+            } else {
+                q.k = rk;
+                q.l = rk + rn - 1;
+                if (rn <= 16) search_keep(q, q.k, q.l, s0);
+                q.s = s0 - 1;
+                if (q.s < 0) {
+                    out = search_result(q);
+                    return false;
+                }
+                return true;
+            }
+        }
+    }
     // Steps before mlen reaches seed_len record nothing, so with K <= seed_len
     // a window holding a non-ACGT base, or an empty interval, ends the search
     // with no seed, and otherwise the interval after K steps is all that is

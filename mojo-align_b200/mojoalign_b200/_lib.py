@@ -96,7 +96,8 @@ class ma_index_info(C.Structure):
 
 class ma_index_options(C.Structure):
     _fields_ = [("kmer_k", C.c_int32), ("kmer3_k", C.c_int32), ("hbm_budget_bytes", C.c_uint64),
-                ("wide_rows", C.c_int32), ("occ_super_shift", C.c_int32), ("prep_chunk_rows", C.c_uint64)]
+                ("wide_rows", C.c_int32), ("occ_super_shift", C.c_int32), ("prep_chunk_rows", C.c_uint64),
+                ("at_k", C.c_int32), ("at_seed_len", C.c_int32)]
 
 
 class ma_tuning(C.Structure):

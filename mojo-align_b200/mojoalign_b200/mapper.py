@@ -134,14 +134,17 @@ class GpuIndex:
     """A bwa 0.7 FM-index made resident in HBM (FmIndex.load + upload)."""
 
     def __init__(self, ctx: GpuContext, prefix, kmer_k: int = 12, kmer3_k: int = 0, hbm_budget_bytes: int = 0,
-                 wide_rows: bool = False, occ_super_shift: int = 0, prep_chunk_rows: int = 0):
+                 wide_rows: bool = False, occ_super_shift: int = 0, prep_chunk_rows: int = 0, at_k: int = 0,
+                 at_seed_len: int = 0):
         """Layout options (result-neutral): wide_rows stores 40-bit SA rows
         even for short texts, occ_super_shift sets the Occ superblock
         (log2 positions, 0 = 31), prep_chunk_rows the SA rows per
-        preparation pass (0 = 2^30)."""
+        preparation pass (0 = 2^30), at_k / at_seed_len the A/T window
+        outcome table (windows of at_k bases, used by calls with seed_len
+        at_seed_len; 0 = none)."""
         h = C.c_void_p()
         opt = _lib.ma_index_options(kmer_k, kmer3_k, hbm_budget_bytes, int(wide_rows), occ_super_shift,
-                                    prep_chunk_rows)
+                                    prep_chunk_rows, at_k, at_seed_len)
         check(lib.ma_index_open(ctx.handle, fspath(prefix), C.byref(opt), C.byref(h)), ctx.handle)
         self.handle = h
         self.ctx = ctx

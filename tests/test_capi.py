@@ -49,6 +49,26 @@ def test_ctypes_signatures_match_the_header():
             assert len(args) == arity[name], f"{name}: {len(args)} ctypes arguments, header declares {arity[name]}"
 
 
+def declared_struct_fields(name: str) -> list[str]:
+    """Field names of `typedef struct name { ... } name;` in the header."""
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    m = re.search(r"typedef struct " + name + r"\s*\{(.*?)\}\s*" + name + r"\s*;", text, flags=re.S)
+    assert m, name
+    return [re.sub(r"\[.*\]", "", d.split()[-1]) for d in m.group(1).split(";") if d.strip()]
+
+
+@pytest.mark.parametrize("name", ["ma_index_options", "ma_index_info", "ma_params", "ma_tuning"])
+def test_ctypes_structs_match_the_header(name):
+    assert [f[0] for f in getattr(_lib, name)._fields_] == declared_struct_fields(name)
+
+
+def test_index_options_default():
+    o = _lib.ma_index_options()
+    _lib.lib.ma_index_options_default(o)
+    assert (o.kmer_k, o.kmer3_k, o.hbm_budget_bytes, o.wide_rows, o.occ_super_shift, o.prep_chunk_rows,
+            o.at_k, o.at_seed_len) == (12, 0, 0, 0, 0, 0, 0, 0)
+
+
 def test_params_default_are_the_reference_defaults():
     p = _lib.ma_params()
     _lib.lib.ma_params_default(p)
