@@ -53,9 +53,9 @@ METRIC = "reads/s seed+extend"
 # reads), from a one-pass ncu capture of that step on this build with the
 # tuning below; roofline.traffic reports it for runs of that workload and
 # tuning, and null otherwise.
-GENOME_SEED_DRAM_BYTES_PER_READ = 27486
+GENOME_SEED_DRAM_BYTES_PER_READ = 24660
 GENOME_SEED_DRAM_TUNING = (4, 2, 0, 1, 1, 1, 8, 32, 0, 1)
-GENOME_SEED_DRAM_AT_K = 0  # the capture's A/T window table (0: none)
+GENOME_SEED_DRAM_AT_K = 28  # the capture's A/T window table (0: none)
 # The workload parameters: the reference defaults with seed_len 19 and
 # max_occ 500 (mojoalign_b200.params.BENCH_PARAMS holds the same values; the
 # reference arm takes them from here so that it loads nothing of the

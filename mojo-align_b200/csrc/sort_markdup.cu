@@ -8,9 +8,10 @@
 // key, each with a host round trip) and marks duplicates and gathers the
 // records on the host.  Here everything stays in HBM:
 //   - the three stable 64-bit key sorts (coordinate; dlo, then dhi carried
-//     into that order) are CUB onesweep radix sorts carrying u32 record
-//     indices; a stable LSD sort gives exactly the reference's order, ties
-//     broken by record index;
+//     into that order) are LSD radix sorts of 8-bit digits carrying u32
+//     record indices (radix_sort.cuh; digits that are equal in every key
+//     are skipped); a stable LSD sort gives exactly the reference's order,
+//     ties broken by record index;
 //   - mark_dups_kernel: one thread per position of the duplicate-key order;
 //     the first record of every run of equal (dhi, dlo) walks its run, picks
 //     the best (highest score, then lowest pair id) and marks every record
@@ -18,12 +19,12 @@
 //   - the gather is a size pass + scan + one warp per output record that
 //     copies the record and sets flag 0x400 on duplicates (_or_dup_flag,
 //     L408-420).
-#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include <string>
 
 #include "ma_internal.h"
+#include "radix_sort.cuh"
 #include "sort_markdup.h"
 
 namespace ma {
@@ -94,13 +95,7 @@ struct SortScratch {
     size_t temp_bytes;
 };
 
-size_t radix_temp_bytes(uint64_t n) {
-    size_t t = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, t, static_cast<const uint64_t*>(nullptr), static_cast<uint64_t*>(nullptr),
-                                    static_cast<const uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
-                                    static_cast<int64_t>(n));
-    return t;
-}
+size_t radix_temp_bytes(uint64_t n) { return radix::scratch_bytes(n); }
 
 SortScratch carve(void* scratch, size_t bytes, uint64_t n) {
     uint8_t* s = static_cast<uint8_t*>(scratch);
@@ -118,12 +113,12 @@ SortScratch carve(void* scratch, size_t bytes, uint64_t n) {
     return r;
 }
 
-void radix(const SortScratch& sc, const uint64_t* keys, uint64_t* keys_out, const uint32_t* vals, uint32_t* vals_out,
-           uint64_t n, cudaStream_t st) {
-    size_t tb = sc.temp_bytes;
-    check_launch(cub::DeviceRadixSort::SortPairs(sc.temp, tb, keys, keys_out, vals, vals_out, static_cast<int64_t>(n),
-                                                 0, 64, st),
-                 "radix sort");
+int radix_sort(const SortScratch& sc, const uint64_t* keys, uint64_t* keys_out, const uint32_t* vals,
+               uint32_t* vals_out, uint64_t n, cudaStream_t st) {
+    if (sc.temp_bytes < radix::scratch_bytes(n)) fail(MA_ERR_INTERNAL, "radix sort scratch too small");
+    const int k = radix::sort_pairs(keys, vals, keys_out, vals_out, n, sc.temp, 0, st);
+    check_launch(cudaGetLastError(), "radix sort");
+    return k;
 }
 
 // ---- gather -------------------------------------------------------------
@@ -192,18 +187,17 @@ int enqueue_sort_markdup(const SortDev& s, void* scratch, size_t scratch_bytes, 
     if (s.marked) check_launch(cudaMemsetAsync(s.marked, 0, sizeof(unsigned long long), st), "memset");
     // coordinate order (L469-525)
     iota_kernel<<<grid_for(n), THREADS, 0, st>>>(sc.idx_a, n);
-    radix(sc, s.coord, sc.keys_out, sc.idx_a, s.perm, n, st);
-    launches += 1 + 2;
+    launches += 1 + radix_sort(sc, s.coord, sc.keys_out, sc.idx_a, s.perm, n, st);
     if (s.do_markdup) {
         // duplicate-key order: dlo, then dhi carried along (L311-360)
         iota_kernel<<<grid_for(n), THREADS, 0, st>>>(sc.idx_a, n);
-        radix(sc, s.dlo, sc.keys_out, sc.idx_a, sc.idx_b, n, st);
+        launches += 1 + radix_sort(sc, s.dlo, sc.keys_out, sc.idx_a, sc.idx_b, n, st);
         permute_kernel<<<grid_for(n), THREADS, 0, st>>>(s.dhi, sc.idx_b, sc.key2, n);
         uint32_t* merged = s.dup_perm ? s.dup_perm : sc.idx_a;
-        radix(sc, sc.key2, sc.keys_out, sc.idx_b, merged, n, st);
+        launches += 1 + radix_sort(sc, sc.key2, sc.keys_out, sc.idx_b, merged, n, st);
         mark_dups_kernel<<<grid_for(n), THREADS, 0, st>>>(sc.keys_out, merged, s.dlo, s.score, s.pair, s.is_dup, n,
                                                           s.marked);
-        launches += 1 + 2 + 1 + 2 + 1;
+        launches += 1;
     } else {
         check_launch(cudaMemsetAsync(s.is_dup, 0, n * sizeof(uint32_t), st), "memset");
         if (s.dup_perm) {

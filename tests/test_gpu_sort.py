@@ -43,6 +43,33 @@ def test_sort_markdup_matches_oracle(ctx, seed, n, do_markdup):
     assert got.n_marked == want[3]
 
 
+def _key_pattern(kind, n, rng):
+    if kind == "all_equal":        # no digit varies: the input is copied
+        return np.full(n, 0x0123456789ABCDEF, np.uint64)
+    if kind == "one_digit":        # one active pass
+        return (np.uint64(0x5500000000000000) | (rng.integers(0, 256, n, dtype=np.uint64) << np.uint64(24)))
+    if kind == "top_bits":         # the sign bit and the top digit
+        return rng.integers(0, 4, n, dtype=np.uint64) << np.uint64(62)
+    if kind == "few_values":       # long runs of equal keys (stability)
+        return rng.integers(0, 7, n, dtype=np.uint64) * np.uint64(0x0101010101010101)
+    return rng.integers(0, 2**64 - 1, n, dtype=np.uint64, endpoint=True)  # every digit varies
+
+
+@pytest.mark.parametrize("kind", ["all_equal", "one_digit", "top_bits", "few_values", "random"])
+@pytest.mark.parametrize("n", [1, 4095, 4096, 4097, 1_000_003])
+def test_coordinate_order_is_a_stable_sort(ctx, kind, n):
+    """The radix passes give numpy's stable order for key patterns that
+    skip no digit, some digits or all of them, at tile-size edges."""
+    rng = np.random.default_rng(n)
+    m = random_tile_meta(11, n, dup_rate=0.2)
+    m["coord"] = _key_pattern(kind, n, rng)
+    got = sort_markdup(ctx, _tile(m), do_markdup=True, dup_perm=True)
+    np.testing.assert_array_equal(got.perm, np.argsort(m["coord"], kind="stable").astype(np.uint32))
+    want = oracle.sort_markdup(**m, do_markdup=True)
+    np.testing.assert_array_equal(got.is_dup, want[0])
+    np.testing.assert_array_equal(got.dup_perm, want[2])
+
+
 def test_deep_duplicate_group(ctx):
     n = 200_000
     m = random_tile_meta(7, n, dup_rate=0.0)
