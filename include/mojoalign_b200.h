@@ -205,7 +205,9 @@ int ma_index_open(ma_ctx* ctx, const char* prefix, const ma_index_options* opt,
 void ma_index_close(ma_index* idx);
 /* Host-only preflight of prefix.{bwt,sa,pac,ann}: the checks of
  * FmIndex.load (linear_fm_index.mojo:88-175) without a GPU; device_bytes
- * reports the HBM ma_index_open would need (resident + staging). */
+ * reports the HBM ma_index_open would need (resident + staging) with these
+ * k-mer tables and no A/T window outcome table (that table adds
+ * 2^at_k * 16 bytes). */
 int ma_index_probe(const char* prefix, int kmer_k, int kmer3_k, ma_index_info* out);
 int ma_index_get_info(const ma_index* idx, ma_index_info* out);
 /* Contig record i of the .ann (FmIndex.contig_name/offset/length,
