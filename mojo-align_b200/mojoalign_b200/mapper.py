@@ -263,10 +263,16 @@ def map_batch_device(ctx: GpuContext, index: GpuIndex, d_bases: int, d_lens: int
     check(rc, ctx.handle)
 
 
-def probe_index(prefix, kmer_k: int = 12, kmer3_k: int = 0) -> ma_index_info:
-    """Validates a bwa index on the host (no GPU) and reports its HBM need."""
+def probe_index(prefix, kmer_k: int = 12, kmer3_k: int = 0, at_k: int = 0) -> ma_index_info:
+    """Validates a bwa index on the host (no GPU) and reports its HBM need,
+    with the A/T window outcome table of at_k bases (2^at_k entries of 16
+    bytes) when at_k > 0."""
+    if at_k < 0 or at_k > 30:
+        raise _lib.MojoAlignError(_lib.MA_ERR_ARG, "at_k must be in 0..30")
     info = ma_index_info()
     check(lib.ma_index_probe(fspath(prefix), kmer_k, kmer3_k, C.byref(info)))
+    if at_k:
+        info.device_bytes += (1 << at_k) * 16
     return info
 
 

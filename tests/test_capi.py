@@ -88,6 +88,14 @@ def test_context_without_sm100_gpu_fails_closed():
     assert _lib.last_error()
 
 
+def test_probe_counts_the_at_window_table(small_ref):
+    _, prefix = small_ref
+    base = probe_index(prefix, kmer_k=10, kmer3_k=9).device_bytes
+    assert probe_index(prefix, kmer_k=10, kmer3_k=9, at_k=20).device_bytes == base + (1 << 20) * 16
+    with pytest.raises(MojoAlignError):
+        probe_index(prefix, at_k=31)
+
+
 def test_probe_matches_oracle_header(small_ref):
     _, prefix = small_ref
     info = probe_index(prefix, kmer_k=10, kmer3_k=9)
